@@ -1,0 +1,603 @@
+"""ctypes binding of the oracle (TEST INFRASTRUCTURE ONLY).
+
+The oracle is the CPU restatement of ragtux/LAPSTACK's stacking path
+(crates/lapstack-core/src/{pyramid,fuse,align,brightness,depth,stack}.rs),
+built from oracle/*.hpp into oracle/_build/liblsb_oracle.so. It is the
+checker the CUDA engine is compared against. Only tests/, smoke() and
+bench.py's CPU legs may import this module; the engine never does.
+
+Parameter blocks follow the reference's defaults (fuse.rs:94-107,
+align.rs:66-70, depth.rs:93-109, stack.rs:106-120).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+from dataclasses import dataclass, field
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_build", "liblsb_oracle.so")
+
+_lib = None
+
+
+def build(force: bool = False) -> str:
+    """Compile the oracle with its Makefile (g++, no GPU needed)."""
+    if force or not os.path.exists(LIB_PATH):
+        subprocess.run(["make", "-C", HERE], check=True, capture_output=True)
+    return LIB_PATH
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        build()
+        _lib = C.CDLL(LIB_PATH)
+        _declare(_lib)
+    return _lib
+
+
+P = C.c_void_p
+F32 = np.float32
+F64 = np.float64
+
+
+def _ptr(a):
+    return a.ctypes.data_as(C.c_void_p) if a is not None else None
+
+
+def _declare(L):
+    sz = C.c_size_t
+    for name, res, args in [
+        ("orc_reflect", sz, [C.c_long, sz]),
+        ("orc_auto_levels", sz, [sz, sz, sz]),
+        ("orc_reduce_f", None, [P, sz, sz, P]),
+        ("orc_expand_f", None, [P, sz, sz, sz, sz, P]),
+        ("orc_build_collapse_f", None, [P, sz, sz, sz, P]),
+        ("orc_binomial_f", None, [sz, P]),
+        ("orc_window_sum_f", None, [P, sz, sz, P, sz, P]),
+        ("orc_region_energy_f", None, [P, sz, sz, sz, C.c_int, P]),
+        ("orc_halo_weight", C.c_float, [C.c_float, C.c_float]),
+        ("orc_winner_shares", None, [P, P, sz, sz, P]),
+        ("orc_deviation_entropy_f", None, [P, sz, sz, sz, sz, P, P]),
+        ("orc_fuse_residuals_f", None, [P, sz, sz, sz, P, P]),
+        ("orc_sim_matrix", None, [P, sz, sz, P]),
+        ("orc_mat_inverse", None, [P, P]),
+        ("orc_interp_weights", C.c_int, [C.c_int, C.c_double, P]),
+        ("orc_spline4f", None, [C.c_float, P]),
+        ("orc_warp_plane_f", None, [P, sz, sz, P, sz, sz, C.c_int, P, P]),
+        ("orc_warp_cost_f", C.c_double, [P, sz, sz, P, sz, sz, P]),
+        ("orc_reduce_burt_f", None, [P, sz, sz, P]),
+        ("orc_gauss_levels_f", sz, [P, sz, sz, P, P]),
+        ("orc_level_steps", None, [P, sz, sz, sz, sz, P, P]),
+        ("orc_multiscale_align_f", None, [P, P, sz, sz, P, P, sz, P, P]),
+        ("orc_common_area", None, [P, sz, sz, sz, C.c_int, P]),
+        ("orc_brightness_gains_f", None, [P, P, sz, sz, P, P]),
+        ("orc_brightness_gains_to_f", None, [P, P, sz, sz, P]),
+        ("orc_box_mean_f", None, [P, sz, sz, sz, P]),
+        ("orc_guided_filter_f", None, [P, P, sz, sz, sz, C.c_float, P]),
+        ("orc_rdf_taps_f", sz, [sz, sz, P]),
+        ("orc_focus_measure_f", None, [P, sz, sz, P, P]),
+        ("orc_focus_slice_f", None, [P, sz, sz, P, P]),
+        ("orc_block_mean_f", None, [P, sz, sz, sz, P]),
+        ("orc_upsample_bilinear_f", None, [P, sz, sz, sz, sz, sz, P]),
+        ("orc_peak_track_f", None, [P, sz, sz, C.c_float, P, P, P, P]),
+        ("orc_normalize_conf_f", C.c_float, [P, sz]),
+        ("orc_median3_f", None, [P, sz, sz, P]),
+        ("orc_wls_solve_f", None, [P, P, P, sz, sz, C.c_float, C.c_float, sz, P, P, P]),
+        ("orc_wls_solve_d", None, [P, P, P, sz, sz, C.c_double, C.c_double, sz, P, P, P]),
+        ("orc_wls_levels_f", sz, [P, sz, sz]),
+        ("orc_depth_from_slices_f", None, [P, sz, sz, P, sz, sz, P, P, P, P, P]),
+        ("orc_depth_from_slices_d", None, [P, sz, sz, P, sz, sz, P, P, P, P, P]),
+        ("orc_run_stack", P, [P, sz, sz, sz, P, C.c_int]),
+        ("orc_stack_free", None, [P]),
+        ("orc_stack_image", None, [P, P, P]),
+        ("orc_stack_winner", None, [P, P]),
+        ("orc_stack_depth", None, [P, P, P, P]),
+        ("orc_stack_stats", None, [P, P]),
+        ("orc_stack_sims", None, [P, P, P, P]),
+    ]:
+        f = getattr(L, name)
+        f.restype = res
+        f.argtypes = args
+    for s in ("f", "d"):
+        getattr(L, f"orc_fuser_new_{s}").restype = P
+        getattr(L, f"orc_fuser_new_{s}").argtypes = [sz, sz, P]
+        getattr(L, f"orc_fuser_levels_{s}").restype = sz
+        getattr(L, f"orc_fuser_levels_{s}").argtypes = [P]
+        getattr(L, f"orc_fuser_push_{s}").argtypes = [P, P]
+        getattr(L, f"orc_fuser_shares_{s}").restype = sz
+        getattr(L, f"orc_fuser_shares_{s}").argtypes = [P, P]
+        getattr(L, f"orc_fuser_winner_{s}").argtypes = [P, P]
+        getattr(L, f"orc_fuser_finish_{s}").argtypes = [P, P, P]
+        getattr(L, f"orc_fuser_free_{s}").argtypes = [P]
+
+
+# ----------------------------------------------------------------- parameters
+TOP_RULES = {"de": 0, "dev": 1, "avg": 2}
+INTERPS = ["nearest", "bilinear", "bicubic", "spline4x4", "spline6x6", "lanczos3"]
+MODELS = ["similarity", "affine", "projective"]
+
+
+@dataclass
+class FuseParams:  # fuse.rs:70-107
+    levels: int = 0  # 0 = auto (residual short side >= 32)
+    energy_radius: int = 1
+    top_rule: str = "de"
+    top_radius: int = 2
+    entropy_bins: int = 256
+    use_chroma: bool = False
+    depth_level: int = 2
+    halo: float = 0.0
+
+    def arr(self):
+        return [self.levels, self.energy_radius, TOP_RULES[self.top_rule], self.top_radius, self.entropy_bins,
+                float(self.use_chroma), self.depth_level, self.halo]
+
+
+@dataclass
+class AlignParams:  # align.rs:52-70
+    shift: bool = True
+    scale: bool = True
+    rotation: bool = True
+    model: str = "similarity"
+    coarsen: int = 0
+    interp: str = "spline4x4"
+
+    def arr(self):
+        return [float(self.shift), float(self.scale), float(self.rotation), MODELS.index(self.model), self.coarsen,
+                INTERPS.index(self.interp)]
+
+    def free(self):
+        a, p = self.model != "similarity", self.model == "projective"
+        return [self.shift, self.shift, self.scale, self.rotation, a, a, p, p]
+
+
+@dataclass
+class DepthParams:  # depth.rs:69-109
+    scale: int = 1
+    focus: str = "rdf"
+    r_in: int = 1
+    r_out: int = 3
+    sml_step: int = 1
+    agg_radius: int = 3
+    agg_eps: float = 1e-4
+    lam: float = 3.0
+    sigma_c: float = 0.04
+    cg_iters: int = 200
+    median: bool = True
+    upsample: str = "guided"
+    up_radius: int = 2
+    up_eps: float = 1e-2
+    gate: float = 1.0
+    robust: float = 1.0
+
+    def arr(self):
+        return [self.scale, 0 if self.focus == "rdf" else 1, self.r_in, self.r_out, self.sml_step, self.agg_radius,
+                self.agg_eps, self.lam, self.sigma_c, self.cg_iters, float(self.median),
+                0 if self.upsample == "bilinear" else 1, self.up_radius, self.up_eps, self.gate, self.robust]
+
+
+@dataclass
+class StackParams:  # stack.rs:27-71 (the hot-path subset)
+    fuse: FuseParams = field(default_factory=FuseParams)
+    align: AlignParams | None = field(default_factory=AlignParams)
+    depth: DepthParams | None = field(default_factory=DepthParams)
+    brightness: bool = True
+    crop: bool = True
+
+    def arr(self):
+        a = self.fuse.arr() + (self.align or AlignParams()).arr() + (self.depth or DepthParams()).arr()
+        a += [float(self.align is not None), float(self.depth is not None), float(self.brightness), float(self.crop)]
+        return np.asarray(a, dtype=F64)
+
+
+def _arr(v):
+    return np.ascontiguousarray(np.asarray(v, dtype=F64))
+
+
+def c32(a):
+    return np.ascontiguousarray(a, dtype=F32)
+
+
+# ------------------------------------------------------------------- pyramid
+def reflect(i, n):
+    return lib().orc_reflect(i, n)
+
+
+def auto_levels(w, h, min_top=32):
+    return lib().orc_auto_levels(w, h, min_top)
+
+
+def half(n):
+    return (n + 1) // 2
+
+
+def reduce(src):
+    src = c32(src)
+    h, w = src.shape
+    out = np.empty((half(h), half(w)), F32)
+    lib().orc_reduce_f(_ptr(src), w, h, _ptr(out))
+    return out
+
+
+def expand(coarse, ow, oh):
+    coarse = c32(coarse)
+    ch, cw = coarse.shape
+    out = np.empty((oh, ow), F32)
+    lib().orc_expand_f(_ptr(coarse), cw, ch, ow, oh, _ptr(out))
+    return out
+
+
+def build_collapse(planes, levels):
+    planes = c32(planes)
+    _, h, w = planes.shape
+    out = np.empty_like(planes)
+    lib().orc_build_collapse_f(_ptr(planes), w, h, levels, _ptr(out))
+    return out
+
+
+# ---------------------------------------------------------------------- fuse
+def binomial(r):
+    out = np.empty(2 * r + 1, F32)
+    lib().orc_binomial_f(r, _ptr(out))
+    return out
+
+
+def window_sum(src, wt):
+    src, wt = c32(src), c32(wt)
+    h, w = src.shape
+    out = np.empty_like(src)
+    lib().orc_window_sum_f(_ptr(src), w, h, _ptr(wt), len(wt), _ptr(out))
+    return out
+
+
+def region_energy(planes, radius=1, use_chroma=False):
+    planes = c32(planes)
+    _, h, w = planes.shape
+    out = np.empty((h, w), F32)
+    lib().orc_region_energy_f(_ptr(planes), w, h, radius, int(use_chroma), _ptr(out))
+    return out
+
+
+def halo_weight(re, p):
+    return lib().orc_halo_weight(re, p)
+
+
+def winner_shares(win, best, frames):
+    win = np.ascontiguousarray(win, dtype=np.uint16)
+    best = c32(best)
+    out = np.empty(frames, F32)
+    lib().orc_winner_shares(_ptr(win), _ptr(best), win.size, frames, _ptr(out))
+    return out
+
+
+def deviation_entropy(y, radius=2, bins=256):
+    y = c32(y)
+    h, w = y.shape
+    d, e = np.empty_like(y), np.empty_like(y)
+    lib().orc_deviation_entropy_f(_ptr(y), w, h, radius, bins, _ptr(d), _ptr(e))
+    return d, e
+
+
+def fuse_residuals(tops, params: FuseParams):
+    tops = c32(tops)
+    n, _, h, w = tops.shape
+    out = np.empty((3, h, w), F32)
+    lib().orc_fuse_residuals_f(_ptr(tops), n, w, h, _ptr(_arr(params.arr())), _ptr(out))
+    return out
+
+
+class Fuser:
+    """fuse.rs:349 `Fuser`: push planar RGB frames, then shares / finish."""
+
+    def __init__(self, w, h, params: FuseParams | None = None, fp64=False):
+        self.w, self.h, self.s = w, h, ("d" if fp64 else "f")
+        self.dt = F64 if fp64 else F32
+        self._p = _arr((params or FuseParams()).arr())
+        self._h = getattr(lib(), f"orc_fuser_new_{self.s}")(w, h, _ptr(self._p))
+        self.levels = getattr(lib(), f"orc_fuser_levels_{self.s}")(self._h)
+        self.count = 0
+
+    def push(self, planes):
+        planes = np.ascontiguousarray(planes, dtype=self.dt)
+        assert planes.shape == (3, self.h, self.w)
+        getattr(lib(), f"orc_fuser_push_{self.s}")(self._h, _ptr(planes))
+        self.count += 1
+
+    def shares(self):
+        out = np.empty(max(self.count, 1), F32)
+        n = getattr(lib(), f"orc_fuser_shares_{self.s}")(self._h, _ptr(out))
+        return out[:n]
+
+    def winner(self, dw, dh):
+        out = np.empty((dh, dw), np.uint16)
+        getattr(lib(), f"orc_fuser_winner_{self.s}")(self._h, _ptr(out))
+        return out
+
+    def finish(self):
+        img = np.empty((3, self.h, self.w), self.dt)
+        depth = np.empty((self.h, self.w), F32)
+        getattr(lib(), f"orc_fuser_finish_{self.s}")(self._h, _ptr(img), _ptr(depth))
+        return img, depth
+
+    def __del__(self):
+        try:
+            getattr(lib(), f"orc_fuser_free_{self.s}")(self._h)
+        except Exception:
+            pass
+
+
+# --------------------------------------------------------------------- align
+SIM_ID = [0.0, 0.0, 1.0, 0.0, 1.0, 0.0, 0.0, 0.0]
+
+
+def sim_matrix(sim, w, h):
+    m = np.empty(9, F64)
+    lib().orc_sim_matrix(_ptr(_arr(sim)), w, h, _ptr(m))
+    return m.reshape(3, 3)
+
+
+def mat_inverse(m):
+    inv = np.empty(9, F64)
+    lib().orc_mat_inverse(_ptr(_arr(m).reshape(9)), _ptr(inv))
+    return inv.reshape(3, 3)
+
+
+def interp_weights(kind, t):
+    w = np.zeros(6, F64)
+    n = lib().orc_interp_weights(INTERPS.index(kind), t, _ptr(w))
+    return w[:n]
+
+
+def warp_plane(src, sim, interp="spline4x4", ow=None, oh=None):
+    src = c32(src)
+    h, w = src.shape
+    ow, oh = ow or w, oh or h
+    out = np.empty((oh, ow), F32)
+    valid = np.empty((oh, ow), np.uint8)
+    lib().orc_warp_plane_f(_ptr(src), w, h, _ptr(_arr(sim)), ow, oh, INTERPS.index(interp), _ptr(out), _ptr(valid))
+    return out, valid
+
+
+def warp_cost(rf, tgt, sim):
+    rf, tgt = c32(rf), c32(tgt)
+    ah, aw = rf.shape
+    th, tw = tgt.shape
+    return lib().orc_warp_cost_f(_ptr(rf), aw, ah, _ptr(tgt), tw, th, _ptr(_arr(sim)))
+
+
+def reduce_burt(src):
+    src = c32(src)
+    h, w = src.shape
+    out = np.empty((half(h), half(w)), F32)
+    lib().orc_reduce_burt_f(_ptr(src), w, h, _ptr(out))
+    return out
+
+
+def gauss_levels(y):
+    y = c32(y)
+    h, w = y.shape
+    dims = np.zeros(128, np.uint64)
+    n = lib().orc_gauss_levels_f(_ptr(y), w, h, _ptr(dims), None)
+    total = sum(int(dims[2 * l]) * int(dims[2 * l + 1]) for l in range(n))
+    buf = np.empty(total, F32)
+    lib().orc_gauss_levels_f(_ptr(y), w, h, _ptr(dims), _ptr(buf))
+    out, o = [], 0
+    for l in range(n):
+        lw, lh = int(dims[2 * l]), int(dims[2 * l + 1])
+        out.append(buf[o:o + lw * lh].reshape(lh, lw))
+        o += lw * lh
+    return out
+
+
+def level_steps(free_idx, lvl, w, h):
+    fi = np.asarray(free_idx, np.uint64)
+    step, tol = np.empty(len(fi), F64), np.empty(len(fi), F64)
+    lib().orc_level_steps(_ptr(fi), len(fi), lvl, w, h, _ptr(step), _ptr(tol))
+    return step, tol
+
+
+def multiscale_align(rf, tg, init=None, free=None, coarsen=0):
+    rf, tg = c32(rf), c32(tg)
+    h, w = rf.shape
+    out = np.empty(8, F64)
+    ev = C.c_size_t(0)
+    fr = np.asarray(free if free is not None else AlignParams().free(), np.uint8)
+    lib().orc_multiscale_align_f(_ptr(rf), _ptr(tg), w, h, _ptr(_arr(init or SIM_ID)), _ptr(fr), coarsen, _ptr(out),
+                                 C.byref(ev))
+    return out, ev.value
+
+
+def common_area(sims, w, h, interp="spline4x4"):
+    s = _arr(sims).reshape(-1, 8)
+    r = np.empty(4, np.uint64)
+    lib().orc_common_area(_ptr(s), len(s), w, h, INTERPS.index(interp), _ptr(r))
+    return tuple(int(v) for v in r)
+
+
+def brightness_gains(ref3, frame3, sim):
+    ref3, frame3 = c32(ref3), c32(frame3)
+    _, h, w = ref3.shape
+    g = np.empty(3, F32)
+    lib().orc_brightness_gains_f(_ptr(ref3), _ptr(frame3), w, h, _ptr(_arr(sim)), _ptr(g))
+    return g
+
+
+def brightness_gains_to(ref3, frame3):
+    ref3, frame3 = c32(ref3), c32(frame3)
+    _, h, w = ref3.shape
+    g = np.empty(3, F32)
+    lib().orc_brightness_gains_to_f(_ptr(ref3), _ptr(frame3), w, h, _ptr(g))
+    return g
+
+
+# --------------------------------------------------------------------- depth
+def box_mean(src, r):
+    src = c32(src)
+    h, w = src.shape
+    out = np.empty_like(src)
+    lib().orc_box_mean_f(_ptr(src), w, h, r, _ptr(out))
+    return out
+
+
+def guided_filter(guide, p, r, eps):
+    guide, p = c32(guide), c32(p)
+    h, w = guide.shape
+    out = np.empty_like(p)
+    lib().orc_guided_filter_f(_ptr(guide), _ptr(p), w, h, r, eps, _ptr(out))
+    return out
+
+
+def rdf_taps(r_in=1, r_out=3):
+    buf = np.empty(3 * (2 * r_out + 1) ** 2, F32)
+    n = lib().orc_rdf_taps_f(r_in, r_out, _ptr(buf))
+    return buf[:3 * n].reshape(n, 3)
+
+
+def focus_measure(y, params: DepthParams | None = None):
+    y = c32(y)
+    h, w = y.shape
+    out = np.empty_like(y)
+    lib().orc_focus_measure_f(_ptr(y), w, h, _ptr(_arr((params or DepthParams()).arr())), _ptr(out))
+    return out
+
+
+def blocks(n, k):
+    return (n + k - 1) // k
+
+
+def focus_slice(planes, params: DepthParams | None = None):
+    p = params or DepthParams()
+    planes = c32(planes)
+    _, h, w = planes.shape
+    k = 1 << p.scale
+    out = np.empty((blocks(h, k), blocks(w, k)), F32)
+    lib().orc_focus_slice_f(_ptr(planes), w, h, _ptr(_arr(p.arr())), _ptr(out))
+    return out
+
+
+def block_mean(src, k):
+    src = c32(src)
+    h, w = src.shape
+    out = np.empty((blocks(h, k), blocks(w, k)), F32)
+    lib().orc_block_mean_f(_ptr(src), w, h, k, _ptr(out))
+    return out
+
+
+def upsample_bilinear(g, w, h, k):
+    g = c32(g)
+    dh, dw = g.shape
+    out = np.empty((h, w), F32)
+    lib().orc_upsample_bilinear_f(_ptr(g), dw, dh, w, h, k, _ptr(out))
+    return out
+
+
+def peak_track(slices, gate=1.0):
+    s = c32(slices)
+    n = s.shape[0]
+    m = s[0].size
+    d, c, mins = np.empty(m, F32), np.empty(m, F32), np.empty(m, F32)
+    fl = C.c_float(0)
+    lib().orc_peak_track_f(_ptr(s), n, m, gate, _ptr(d), _ptr(c), _ptr(mins), C.byref(fl))
+    shp = s.shape[1:]
+    return d.reshape(shp), c.reshape(shp), mins.reshape(shp), fl.value
+
+
+def normalize_conf(conf):
+    c = c32(conf).copy()
+    p = lib().orc_normalize_conf_f(_ptr(c), c.size)
+    return c, p
+
+
+def median3(src):
+    src = c32(src)
+    h, w = src.shape
+    out = np.empty_like(src)
+    lib().orc_median3_f(_ptr(src), w, h, _ptr(out))
+    return out
+
+
+def wls_solve(d, conf, guide, lam, sigma_c, max_iters, fp64=False):
+    dt, s = (F64, "d") if fp64 else (F32, "f")
+    d, conf, guide = (np.ascontiguousarray(x, dtype=dt) for x in (d, conf, guide))
+    h, w = d.shape
+    u = np.empty_like(d)
+    rel = (C.c_double if fp64 else C.c_float)(0)
+    it = C.c_size_t(0)
+    getattr(lib(), f"orc_wls_solve_{s}")(_ptr(d), _ptr(conf), _ptr(guide), w, h, lam, sigma_c, max_iters, _ptr(u),
+                                         C.byref(rel), C.byref(it))
+    return u, rel.value, it.value
+
+
+def wls_levels(guide):
+    g = c32(guide)
+    h, w = g.shape
+    return lib().orc_wls_levels_f(_ptr(g), w, h)
+
+
+def depth_from_slices(slices, fused, params: DepthParams | None = None, fp64=False):
+    p = params or DepthParams()
+    dt, s = (F64, "d") if fp64 else (F32, "f")
+    sl = np.ascontiguousarray(slices, dtype=dt)
+    fused = np.ascontiguousarray(fused, dtype=dt)
+    _, h, w = fused.shape
+    n = sl.shape[0]
+    m = sl[0].size
+    depth, conf = np.empty((h, w), dt), np.empty((h, w), dt)
+    floor_cells = np.empty(m, dt)
+    st = np.empty(7, F64)
+    getattr(lib(), f"orc_depth_from_slices_{s}")(_ptr(sl), n, m, _ptr(fused), w, h, _ptr(_arr(p.arr())), _ptr(depth),
+                                                 _ptr(conf), _ptr(floor_cells), _ptr(st))
+    stats = dict(floor=st[0], p90=st[1], rel=st[2], iters=int(st[3]), iters_first=int(st[4]), dw=int(st[5]),
+                 dh=int(st[6]))
+    return depth, conf, floor_cells.reshape(int(st[6]), int(st[5])), stats
+
+
+# --------------------------------------------------------------------- stack
+@dataclass
+class StackResult:
+    image: np.ndarray  # (3, h, w) float64 (exact copy of the f32 or f64 result)
+    image_u16: np.ndarray  # (h, w, 3) uint16
+    winner: np.ndarray  # (h, w) float32 (the fuse winner map, upsampled)
+    depth: np.ndarray | None
+    conf: np.ndarray | None
+    floor_cells: np.ndarray | None
+    sims: np.ndarray  # (n, 8)
+    gains: np.ndarray  # (n, 3)
+    shares: np.ndarray
+    stats: dict
+
+
+def run_stack(frames_u16, params: StackParams | None = None, fp64=False) -> StackResult:
+    """stack.rs run_with over in-memory interleaved RGB u16 frames (n, h, w, 3)."""
+    p = params or StackParams()
+    fr = np.ascontiguousarray(frames_u16, dtype=np.uint16)
+    n, h, w, _ = fr.shape
+    L = lib()
+    r = L.orc_run_stack(_ptr(fr), n, w, h, _ptr(p.arr()), int(fp64))
+    try:
+        img = np.empty((3, h, w), F64)
+        u16 = np.empty((h, w, 3), np.uint16)
+        L.orc_stack_image(r, _ptr(img), _ptr(u16))
+        win = np.empty((h, w), F32)
+        L.orc_stack_winner(r, _ptr(win))
+        st = np.empty(13, F64)
+        L.orc_stack_stats(r, _ptr(st))
+        stats = dict(levels=int(st[0]), dw=int(st[1]), dh=int(st[2]), floor=st[3], p90=st[4], rel=st[5],
+                     iters=int(st[6]), iters_first=int(st[7]), align_evals=int(st[8]),
+                     crop=(int(st[9]), int(st[10]), int(st[11]), int(st[12])))
+        depth = conf = floor_cells = None
+        if p.depth is not None:
+            depth, conf = np.empty((h, w), F64), np.empty((h, w), F64)
+            floor_cells = np.empty((stats["dh"], stats["dw"]), F64)
+            L.orc_stack_depth(r, _ptr(depth), _ptr(conf), _ptr(floor_cells))
+        sims, gains = np.empty((n, 8), F64), np.empty((n, 3), F32)
+        shares = np.zeros(n, F32)
+        L.orc_stack_sims(r, _ptr(sims), _ptr(gains), _ptr(shares))
+        return StackResult(img, u16, win, depth, conf, floor_cells, sims, gains, shares, stats)
+    finally:
+        L.orc_stack_free(r)

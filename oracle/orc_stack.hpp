@@ -1,0 +1,127 @@
+// Oracle (test infrastructure only; see orc_core.hpp): the per-frame
+// sequence of stack.rs for in-memory 16-bit frames — AlignedFrames::get /
+// register (stack.rs:513-530, 638-706), LazyFrames brightness (stack.rs:
+// 276-437), fuse_range (stack.rs:740-826), fuse_and_depth (stack.rs:833-853)
+// and the common-area crop of run_with (stack.rs:1047-1060).
+#pragma once
+#include "orc_align.hpp"
+#include "orc_depth.hpp"
+
+namespace orc {
+
+struct StackParams {
+    FuseParams fuse;
+    bool align = true;
+    AlignParams al;
+    bool depth = true;
+    DepthParams dp;
+    bool brightness = true;
+    bool crop = true;
+};
+
+template <class T>
+struct StackOutput {
+    Img3<T> image;                 // fused, clamped, full frame (before the crop)
+    std::vector<float> winner;     // fuse winner map, upsampled (stack.rs:244 Output::depth when depth is off)
+    DepthMap<T> dm;                // depth pass
+    std::vector<Sim> sims;
+    std::vector<std::array<float, 3>> gains;
+    std::vector<float> shares;
+    Rect crop;                     // the common area (full frame when nothing is cut)
+    size_t levels = 0;
+    size_t align_evals = 0;
+};
+
+// io.rs:89-94 u16 -> f32 as v * (1/65535) (an f32 multiply by the f32 reciprocal)
+template <class T>
+Img3<T> img_of_u16(const uint16_t* rgb, size_t w, size_t h) {
+    Img3<T> im(w, h);
+    const T inv = std::is_same<T, float>::value ? (T)(1.0f / 65535.0f) : (T)(1.0 / 65535.0);
+    for (int c = 0; c < 3; c++)
+        for (size_t i = 0; i < w * h; i++) im.p[c][i] = (T)rgb[3 * i + c] * inv;
+    return im;
+}
+
+// io.rs:287 f32 -> u16 as (clamp01 * 65535 + 0.5) as u16
+template <class T>
+inline uint16_t u16_of(T v) {
+    T c = rclamp(v, T(0), T(1));
+    return (uint16_t)(c * LIT(65535.0) + LIT(0.5));
+}
+
+template <class T>
+StackOutput<T> run_stack(const uint16_t* const* frames, size_t n, size_t w, size_t h, const StackParams& sp) {
+    StackOutput<T> out;
+    Fuser<T> fuser(w, h, sp.fuse);
+    out.levels = fuser.levels;
+    std::vector<std::vector<T>> slices;
+    bool aligned = sp.align && n > 1;
+    bool freem[8];
+    free_mask(sp.al, freem);
+    std::vector<T> prev_ref;
+    BReference<T> bref;
+    double ref_means[3] = {0, 0, 0};
+    for (size_t i = 0; i < n; i++) {
+        Img3<T> img = img_of_u16<T>(frames[i], w, h);
+        Sim sim;
+        std::array<float, 3> gain{1.0f, 1.0f, 1.0f};
+        if (aligned) {
+            // stack.rs:513 `register`
+            std::vector<T> y = luma(img);
+            if (i > 0) sim = multiscale_align<T>(prev_ref.data(), y.data(), w, h, out.sims.back(), freem, sp.al.coarsen, &out.align_evals);
+            if (i + 1 < n) {
+                if (sim.is_id()) prev_ref = y;
+                else warp_plane<T>(y.data(), w, h, sim, w, h, sp.al.interp, prev_ref, nullptr);
+            }
+            // stack.rs:662-679: warp, the pixel as shot where the source leaves the frame
+            if (!sim.is_id()) {
+                std::vector<uint8_t> valid;
+                Img3<T> warped(w, h);
+                warp_plane<T>(img.p[0].data(), w, h, sim, w, h, sp.al.interp, warped.p[0], &valid);
+                warp_plane<T>(img.p[1].data(), w, h, sim, w, h, sp.al.interp, warped.p[1], nullptr);
+                warp_plane<T>(img.p[2].data(), w, h, sim, w, h, sp.al.interp, warped.p[2], nullptr);
+                for (int c = 0; c < 3; c++)
+                    for (size_t k = 0; k < w * h; k++)
+                        if (!valid[k]) warped.p[c][k] = img.p[c][k];
+                img = std::move(warped);
+            }
+            // stack.rs:680-690 brightness against frame 0 over the covered pixels
+            if (sp.brightness) {
+                if (i == 0) {
+                    bref.init(img);
+                } else {
+                    double sf[3], so[3];
+                    size_t cnt;
+                    bsums<T>(img, &bref, sim, sf, so, cnt);
+                    bratio(so, sf, cnt, gain.data());
+                    bapply<T>(img, gain.data());
+                }
+            }
+        } else if (sp.brightness) {
+            // stack.rs LazyFrames: frame 0's channel means, gains_to for the others
+            if (i == 0) {
+                bmeans<T>(img, ref_means);
+            } else {
+                double m[3];
+                bmeans<T>(img, m);
+                bratio(ref_means, m, (size_t)-1, gain.data());
+                bapply<T>(img, gain.data());
+            }
+        }
+        out.sims.push_back(sim);
+        out.gains.push_back(gain);
+        fuser.push(img);
+        if (sp.depth) {
+            size_t dw, dh;
+            slices.push_back(focus_slice<T>(img, sp.dp, dw, dh));
+        }
+    }
+    out.shares = fuser.shares();
+    fuser.finish(out.image, out.winner);
+    if (sp.depth) out.dm = depth_from_slices<T>(slices, out.image, sp.dp);
+    out.crop = Rect{0, 0, w, h};
+    if (aligned && sp.crop) out.crop = common_area(out.sims, w, h, sp.al.interp);
+    return out;
+}
+
+}  // namespace orc
