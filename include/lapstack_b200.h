@@ -1,0 +1,183 @@
+/* lapstack-b200: the stacking-engine hot path of ragtux/LAPSTACK
+ * (crates/lapstack-core) as a B200-native CUDA library behind a C ABI.
+ *
+ * Conventions follow the reference's one C ABI, crates/lapstack-raw/src/
+ * ffi.rs:66-152: an ABI-version function, plain #[repr(C)]-style structs,
+ * functions that return NULL on success or a heap error string (free it
+ * with lsb_free_str), explicit free functions, no unwinding across the
+ * boundary. A handle is used from one thread at a time; an engine owns one
+ * CUDA stream and every stack made from it runs on that stream.
+ *
+ * What each entry point replaces in the reference (crates/lapstack-core/src):
+ *   lsb_engine_create      gpu.rs:308 `available` + the NVRTC/context set-up of
+ *                          gpu.rs:312-324 (GpuFuser::new, GpuFrames::new)
+ *   lsb_stack_begin        stack.rs:740 `fuse_range` creating the fuser
+ *                          (AnyFuser, stack.rs:123-201) and stack.rs:481
+ *                          AlignedFrames::open for one stack
+ *   lsb_stack_push_u16     stack.rs:785-821 one frame of the fold loop:
+ *                          FrameSource::get_gpu (stack.rs:623) + GpuFrames::
+ *                          process (gpu.rs:751) + GpuFuser::push_device
+ *                          (gpu.rs:451), from the decoded 16-bit frame
+ *   lsb_stack_push_f32     AnyFuser::push(&Img3) (stack.rs:152, gpu.rs:435)
+ *   lsb_stack_shares       AnyFuser::shares (stack.rs:167, gpu.rs:505)
+ *   lsb_stack_finish       AnyFuser::finish (stack.rs:178, gpu.rs:517) +
+ *                          fuse_and_depth (stack.rs:833) with
+ *                          gpu::depth_from_slices (gpu.rs:1327) + the
+ *                          common-area crop rectangle (align.rs:344)
+ *   lsb_depth_from_slices  gpu::depth_from_slices (gpu.rs:1327)
+ *   lsb_wls_solve          depth::wls_solve (depth.rs:1081) / DWls (gpu.rs:1154)
+ *   lsb_align_pair         align::multiscale_align (align.rs:896) /
+ *                          GpuFrames::search (gpu.rs:692)
+ *   lsb_warp_cost          align::warp_cost (align.rs:581) / the warp_cost
+ *                          kernel (gpu.rs:148)
+ */
+#ifndef LAPSTACK_B200_H
+#define LAPSTACK_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define LSB_ABI_VERSION 1u
+
+typedef struct lsb_engine lsb_engine;
+typedef struct lsb_stack lsb_stack;
+
+typedef void (*lsb_log_fn)(const char* line, void* user);
+
+typedef struct {
+    int32_t device;        /* CUDA device ordinal */
+    int32_t fp16_storage;  /* store pyramid levels >= 1 and the focus slices in FP16 */
+    int32_t grid_limit;    /* CTAs of the persistent kernels; 0 = 2 x the SM count */
+    int32_t reserved;
+    lsb_log_fn log;        /* optional progress lines (stack.rs:1014 `log`) */
+    void* user;
+} lsb_config;
+
+/* fuse.rs:70-107 FuseParams */
+typedef struct {
+    uint32_t levels;        /* band-pass levels; 0 = auto (residual short side >= 32) */
+    uint32_t energy_radius; /* 0..2 (1 = 3x3 binomial) */
+    uint32_t top_rule;      /* 0 dev-entropy, 1 deviation, 2 average */
+    uint32_t top_radius;    /* 0..4 */
+    uint32_t entropy_bins;
+    uint32_t use_chroma;
+    uint32_t depth_level;
+    float halo;             /* halo control hardness; 0 = off */
+} lsb_fuse_params;
+
+/* align.rs:52-70 AlignParams (enabled = 0: stack.rs's no-align path) */
+typedef struct {
+    uint32_t enabled;
+    uint32_t shift, scale, rotation;
+    uint32_t model;   /* 0 similarity, 1 affine, 2 projective */
+    uint32_t coarsen; /* skip the N finest registration levels */
+    uint32_t interp;  /* align.rs Interp id: 0 nearest .. 3 spline4x4 .. 5 lanczos3 */
+    uint32_t reserved;
+} lsb_align_params;
+
+/* depth.rs:69-109 DepthParams (enabled = 0: report the fuse winner map) */
+typedef struct {
+    uint32_t enabled;
+    uint32_t scale;     /* working grid 1/2^scale */
+    uint32_t focus;     /* 0 ring difference filter, 1 sum-modified Laplacian */
+    uint32_t r_in, r_out, sml_step;
+    uint32_t agg_radius;
+    float agg_eps;
+    float lambda, sigma_c;
+    uint32_t cg_iters;
+    uint32_t median;
+    uint32_t upsample;  /* 0 bilinear, 1 guided */
+    uint32_t up_radius;
+    float up_eps;
+    float gate, robust;
+    uint32_t edge_mode; /* 0 exp(-|dI|/sigma_c) (reference); 1 exp(-dI^2/(2 sigma_c^2)) */
+    uint32_t vcycle_mode; /* 0 FP32 V-cycle (reference); 1 BF16 smoother + restriction */
+} lsb_depth_params;
+
+/* Results of lsb_stack_finish; buffers owned by the library until lsb_result_free. */
+typedef struct {
+    uint32_t w, h, n_frames, levels, dw, dh;
+    uint16_t* image_u16; /* w*h*3 interleaved, io.rs:287 quantisation */
+    float* image_f32;    /* 3*w*h planar, clamped to [0,1] */
+    float* winner;       /* w*h, fuse winner map at depth_level, upsampled (fuse.rs:336) */
+    float* depth;        /* w*h fractional frame index, or NULL without the depth pass */
+    float* conf;         /* w*h */
+    float* floor_cells;  /* dw*dh per-cell noise floor (depth.rs:151 DepthMap::floor) */
+    double* sims;        /* n*8 align.rs:200 Sim vectors */
+    float* gains;        /* n*3 */
+    float* shares;       /* n, fuse.rs:315 winner_shares */
+    uint32_t crop[4];    /* x, y, w, h of the common area (align.rs:344) */
+    float floor_value, p90, wls_rel;
+    uint32_t wls_iters, wls_iters_first, align_evals;
+    double wls_rel64;
+    double ms[8];        /* device time per stage: align, gains, fold, residual+collapse, focus agg, wls, upsample, total */
+} lsb_result;
+
+/* Seeded synthetic stack description (no reference counterpart; the benchmark inputs). */
+typedef struct {
+    uint32_t w, h, n;
+    uint32_t warp;          /* 1: a seeded similarity warp per frame */
+    uint64_t seed;
+    float mag_step;         /* frame k magnified by 1 + mag_step*k */
+    float noise_std;
+    float blur_px;          /* defocus sigma = blur_px * |z - f_k| */
+    float warp_scale;       /* scale 1 + U(-a, a) */
+    float warp_rot_deg;     /* rotation U(-a, a) degrees */
+    float warp_shift;       /* translation U(-a, a) px */
+} lsb_synth_desc;
+
+uint32_t lsb_abi(void);
+void lsb_free_str(char* s);
+
+char* lsb_engine_create(const lsb_config* cfg, lsb_engine** out);
+void lsb_engine_destroy(lsb_engine* e);
+/* The engine's CUDA stream (cudaStream_t), for callers that share it. */
+void* lsb_engine_stream(lsb_engine* e);
+
+char* lsb_stack_begin(lsb_engine* e, uint32_t w, uint32_t h, uint32_t n_frames, const lsb_fuse_params* fuse,
+                      const lsb_align_params* align, const lsb_depth_params* depth, int32_t brightness, int32_t crop,
+                      lsb_stack** out);
+/* One decoded frame: interleaved RGB u16, rows stride_px pixels apart (host or device pointer). */
+char* lsb_stack_push_u16(lsb_stack* s, const uint16_t* rgb, size_t stride_px);
+/* One frame as three planar f32 planes in [0,1] (host or device pointers); the frame is folded as given. */
+char* lsb_stack_push_f32(lsb_stack* s, const float* const planes[3]);
+/* The device buffer frames are pushed into ([n][h][w][3] u16), and a way to declare
+   frames written there directly (count = frames now present). */
+char* lsb_stack_frames_device(lsb_stack* s, uint16_t** frames_dev);
+char* lsb_stack_set_count(lsb_stack* s, uint32_t count);
+/* fuse.rs:315 shares of the frames pushed so far (runs the fold when needed); out_n holds n floats. */
+char* lsb_stack_shares(lsb_stack* s, float* out_n);
+/* Align, fold, depth: the whole pipeline over the frames pushed; may be called again. */
+char* lsb_stack_finish(lsb_stack* s, lsb_result* out);
+/* lsb_stack_finish without copying results back (device-resident benchmarking). */
+char* lsb_stack_run(lsb_stack* s, double* ms_out8);
+void lsb_stack_destroy(lsb_stack* s);
+void lsb_result_free(lsb_result* r);
+
+/* gpu.rs:1327 depth_from_slices: slices [n][dh][dw] f32, fused [3][h][w] f32 (host pointers). */
+char* lsb_depth_from_slices(lsb_engine* e, const float* slices, uint32_t n, const float* fused, uint32_t w, uint32_t h,
+                            const lsb_depth_params* p, lsb_result* out);
+/* depth.rs:1081 wls_solve on the device (host pointers, w*h each). */
+char* lsb_wls_solve(lsb_engine* e, const float* d, const float* conf, const float* guide, uint32_t w, uint32_t h, float lambda,
+                    float sigma_c, uint32_t max_iters, uint32_t edge_mode, uint32_t vcycle_mode, float* u, float* rel,
+                    uint32_t* iters, double* ms);
+/* align.rs:896 multiscale_align of luma planes tg onto rf (host pointers, w*h f32). */
+char* lsb_align_pair(lsb_engine* e, const float* rf, const float* tg, uint32_t w, uint32_t h, const double* init8,
+                     const uint8_t* free8, uint32_t coarsen, double* out8, uint32_t* evals);
+/* align.rs:581 warp_cost of tgt (tw x th) warped by sim onto rf (aw x ah), host pointers. */
+char* lsb_warp_cost(lsb_engine* e, const float* rf, uint32_t aw, uint32_t ah, const float* tgt, uint32_t tw, uint32_t th,
+                    const double* sim8, double* cost);
+
+/* Synthetic stacks: [n][h][w][3] u16 into host memory (OpenMP) or device memory. truth (n*4, may be NULL):
+   per frame scale, rotation (rad), tx, ty (px) applied. */
+const char* lsb_synth_stack_host(const lsb_synth_desc* d, uint16_t* out, double* truth);
+const char* lsb_synth_stack_device(const lsb_synth_desc* d, uint16_t* out_dev, double* truth, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

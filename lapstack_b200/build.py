@@ -1,0 +1,82 @@
+"""Compile the engine's CUDA sources for sm_100a into an in-tree shared library.
+
+Output: lapstack_b200/_build/liblapstack_b200.so (git-ignored; it travels with
+the working tree). Every translation unit is compiled with -fmad=false: the
+kernels that must match the reference FP32 path bit for bit spell out their
+rounding with intrinsics, and nothing else is left for the compiler to
+contract. Objects are rebuilt only when a source or header is newer.
+"""
+from __future__ import annotations
+
+import concurrent.futures as cf
+import glob
+import os
+import shutil
+import subprocess
+import sys
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(PKG)
+CSRC = os.path.join(PKG, "csrc")
+OUT_DIR = os.path.join(PKG, "_build")
+LIB = os.path.join(OUT_DIR, "liblapstack_b200.so")
+SOURCES = ["lsb_fold.cu", "lsb_depth.cu", "lsb_wls.cu", "lsb_align.cu", "lsb_synth.cu", "lsb_api.cu"]
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+
+
+def _nvcc():
+    for cand in (os.environ.get("CUDA_HOME", ""), "/usr/local/cuda"):
+        p = os.path.join(cand, "bin", "nvcc") if cand else ""
+        if p and os.path.exists(p):
+            return p
+    p = shutil.which("nvcc")
+    if not p:
+        raise RuntimeError("nvcc not found: the lapstack-b200 engine is CUDA-only")
+    return p
+
+
+def _flags():
+    f = ["-O3", "-std=c++17", "-lineinfo", "-fmad=false", "-Xcompiler", "-fPIC,-fopenmp,-O3",
+         "-I", os.path.join(ROOT, "include"), "-I", CSRC] + ARCH
+    if os.path.exists("/usr/bin/g++"):
+        f = ["-ccbin", "/usr/bin/g++"] + f
+    return f
+
+
+def _stale(obj, deps):
+    if not os.path.exists(obj):
+        return True
+    t = os.path.getmtime(obj)
+    return any(os.path.getmtime(d) > t for d in deps)
+
+
+def build(force: bool = False, verbose: bool = False) -> str:
+    os.makedirs(OUT_DIR, exist_ok=True)
+    nvcc = _nvcc()
+    headers = glob.glob(os.path.join(CSRC, "*.h")) + glob.glob(os.path.join(CSRC, "*.cuh")) + \
+        glob.glob(os.path.join(ROOT, "include", "*.h"))
+    jobs = []
+    objs = []
+    for src in SOURCES:
+        s = os.path.join(CSRC, src)
+        o = os.path.join(OUT_DIR, src.replace(".cu", ".o"))
+        objs.append(o)
+        if force or _stale(o, [s] + headers):
+            jobs.append([nvcc, *_flags(), "-c", s, "-o", o])
+
+    def run(cmd):
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError(f"nvcc failed: {' '.join(cmd)}\n{r.stdout}\n{r.stderr}")
+        if verbose and (r.stdout or r.stderr):
+            print(r.stdout, r.stderr, file=sys.stderr)
+
+    with cf.ThreadPoolExecutor(max_workers=min(8, max(1, len(jobs)))) as ex:
+        list(ex.map(run, jobs))
+    if force or jobs or _stale(LIB, objs):
+        run([nvcc, *ARCH, "-shared", "-o", LIB, *objs, "-Xcompiler", "-fopenmp", "-lgomp"])
+    return LIB
+
+
+if __name__ == "__main__":
+    print(build(force="--force" in sys.argv, verbose=True))

@@ -1,0 +1,493 @@
+// Registration on the device (crates/lapstack-core/src/align.rs): the luma
+// registration pyramid (align.rs:674 `reduce_burt`, a = 0.33, border-
+// renormalised), the DC-removed RMS cost of a warped target (align.rs:581
+// `warp_cost`: f64 source points and sums, f32 Spline4x4 taps) evaluated for
+// a BATCH of candidate transforms per launch, the full-frame luma warp that
+// becomes the next frame's reference (align.rs:542 `warp_plane`), and the
+// brightness sums of every aligned frame against frame 0 (brightness.rs:67).
+//
+// The bounded Nelder-Mead search (align.rs:796) runs on the host on this
+// schedule, with one launch and one small read-back per simplex iteration:
+// the reflection, expansion and contraction points of an iteration are all
+// evaluated in the same launch (the search then takes the branch the
+// reference takes), and a shrink's n points in one more.
+#include <algorithm>
+#include <cmath>
+#include <functional>
+#include <vector>
+
+#include "lsb_align.h"
+#include "lsb_common.cuh"
+#include "lsb_interp.cuh"
+
+namespace lsb {
+
+// ------------------------------------------------------------------ kernels
+__global__ void luma_u16_kernel(const uint16_t* __restrict__ f, size_t n, float* __restrict__ y) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        const uint16_t* p = f + 3 * i;
+        y[i] = lsb_luma(__fmul_rn((float)p[0], LSB_INV16), __fmul_rn((float)p[1], LSB_INV16), __fmul_rn((float)p[2], LSB_INV16));
+    }
+}
+
+// align.rs:650 Burt's kernel, a = 0.33: [c, b, a, b, c]
+__device__ __forceinline__ float burt_k(int t) {
+    const float a = 0.33f, b = 0.25f, c = __fsub_rn(0.25f, __fdiv_rn(a, 2.0f));
+    return t == 2 ? a : ((t == 1 || t == 3) ? b : c);
+}
+// align.rs:658 `norm_full`: the in-bounds taps summed in order
+__device__ __forceinline__ float burt_norm(int i, int n) {
+    float s = 0.f;
+    for (int t = 0; t < 5; t++) {
+        int x = i + t - 2;
+        if (x >= 0 && x < n) s = __fadd_rn(s, burt_k(t));
+    }
+    return s;
+}
+// align.rs:674 `reduce_burt`, one output sample: the horizontal in-bounds sums
+// of the five rows, the vertical in-bounds sum, then / (row norm * column norm).
+__global__ void reduce_burt_kernel(const float* __restrict__ src, int w, int h, float* __restrict__ out, int ow, int oh) {
+    const int oj = blockIdx.x * blockDim.x + threadIdx.x, oi = blockIdx.y * blockDim.y + threadIdx.y;
+    if (oj >= ow || oi >= oh) return;
+    const int cx = 2 * oj, cy = 2 * oi;
+    float v = 0.f;
+    for (int t = 0; t < 5; t++) {
+        const int y = cy + t - 2;
+        if (y < 0 || y >= h) continue;
+        const float* row = src + (size_t)y * w;
+        float a = 0.f;
+        for (int u = 0; u < 5; u++) {
+            const int x = cx + u - 2;
+            if (x >= 0 && x < w) a = __fadd_rn(a, __fmul_rn(burt_k(u), row[x]));
+        }
+        v = __fadd_rn(v, __fmul_rn(burt_k(t), a));
+    }
+    out[(size_t)oi * ow + oj] = __fdiv_rn(v, __fmul_rn(burt_norm(cy, h), burt_norm(cx, w)));
+}
+
+// align.rs:639 `spline4f`
+__device__ __forceinline__ void spline4f(float t, float w[4]) {
+    w[0] = __fmul_rn(__fsub_rn(__fmul_rn(__fadd_rn(__fmul_rn(-1.0f / 3.0f, t), 0.8f), t), 0.46666667f), t);
+    w[1] = __fadd_rn(__fmul_rn(__fsub_rn(__fmul_rn(__fsub_rn(t, 1.8f), t), 0.2f), t), 1.0f);
+    w[2] = __fmul_rn(__fadd_rn(__fmul_rn(__fsub_rn(1.2f, t), t), 0.8f), t);
+    w[3] = __fmul_rn(__fsub_rn(__fmul_rn(__fsub_rn(__fmul_rn(1.0f / 3.0f, t), 0.2f), t), 0.13333334f), t);
+}
+
+// align.rs:485 `affine_row` + align.rs:291 `map`
+__device__ __forceinline__ void src_point(const double* m, bool aff, double x, double y, double& sx, double& sy) {
+    if (aff) {
+        sx = __dadd_rn(__dadd_rn(__dmul_rn(m[1], y), m[2]), __dmul_rn(m[0], x));
+        sy = __dadd_rn(__dadd_rn(__dmul_rn(m[4], y), m[5]), __dmul_rn(m[3], x));
+    } else {
+        const double d = __dadd_rn(__dadd_rn(__dmul_rn(m[6], x), __dmul_rn(m[7], y)), m[8]);
+        sx = __ddiv_rn(__dadd_rn(__dadd_rn(__dmul_rn(m[0], x), __dmul_rn(m[1], y)), m[2]), d);
+        sy = __ddiv_rn(__dadd_rn(__dadd_rn(__dmul_rn(m[3], x), __dmul_rn(m[4], y)), m[5]), d);
+    }
+}
+
+// align.rs:581 `warp_cost` for up to MAX_CAND candidates (blockIdx.y): per
+// block f64 partial sums of d, d^2 and the count, tree-reduced in a fixed order.
+__global__ void cost_kernel(const float* __restrict__ rf, int aw, int ah, const float* __restrict__ tgt, int tw, int th,
+                            const CostBatch cb, double* __restrict__ part) {
+    const int k = blockIdx.y;
+    const double* m = cb.inv[k];
+    const bool aff = m[6] == 0.0 && m[7] == 0.0 && m[8] == 1.0;
+    const double xmax = (double)(tw - 1), ymax = (double)(th - 1);
+    double sd = 0.0, sd2 = 0.0, cnt = 0.0;
+    const size_t n = (size_t)aw * ah;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        const int x = (int)(i % aw), y = (int)(i / aw);
+        double sx, sy;
+        src_point(m, aff, (double)x, (double)y, sx, sy);
+        if (!(sx >= 0.0 && sx <= xmax && sy >= 0.0 && sy <= ymax)) continue;
+        const double fx = floor(sx), fy = floor(sy);
+        const int x0 = (int)fx, y0 = (int)fy;
+        float wx[4], wy[4];
+        spline4f((float)__dsub_rn(sx, fx), wx);
+        spline4f((float)__dsub_rn(sy, fy), wy);
+        float acc = 0.f;
+        for (int j = 0; j < 4; j++) {
+            const float* row = tgt + (size_t)min(max(y0 + j - 1, 0), th - 1) * tw;
+            float r = 0.f;
+            for (int u = 0; u < 4; u++) r = __fadd_rn(r, __fmul_rn(wx[u], row[min(max(x0 + u - 1, 0), tw - 1)]));
+            acc = __fadd_rn(acc, __fmul_rn(wy[j], r));
+        }
+        const double d = (double)__fsub_rn(rf[i], acc);
+        sd += d;
+        sd2 += d * d;
+        cnt += 1.0;
+    }
+    __shared__ double red[3][256];
+    red[0][threadIdx.x] = sd;
+    red[1][threadIdx.x] = sd2;
+    red[2][threadIdx.x] = cnt;
+    __syncthreads();
+    for (int st = blockDim.x / 2; st > 0; st >>= 1) {
+        if (threadIdx.x < st)
+            for (int q = 0; q < 3; q++) red[q][threadIdx.x] += red[q][threadIdx.x + st];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0)
+        for (int q = 0; q < 3; q++) part[((size_t)k * gridDim.x + blockIdx.x) * 3 + q] = red[q][0];
+}
+__global__ void cost_final_kernel(const double* __restrict__ part, int nblocks, int ncand, double* __restrict__ out) {
+    const int k = threadIdx.x;
+    if (k >= ncand) return;
+    double s[3] = {0.0, 0.0, 0.0};
+    for (int b = 0; b < nblocks; b++)
+        for (int q = 0; q < 3; q++) s[q] += part[((size_t)k * nblocks + b) * 3 + q];
+    for (int q = 0; q < 3; q++) out[3 * k + q] = s[q];
+}
+
+// align.rs:489 `warp_with` on an f32 plane (edge-clamped; no fallback), the
+// interpolation weights as in the fold's level-0 warp.
+__global__ void warp_plane_kernel(const float* __restrict__ src, int w, int h, const WarpXform xf, float* __restrict__ out) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
+    if (x >= w || y >= h) return;
+    double sx, sy;
+    src_point(xf.inv, xf.affine, (double)x, (double)y, sx, sy);
+    const double fx = floor(sx), fy = floor(sy);
+    const int x0 = (int)fx, y0 = (int)fy;
+    float wx[6], wy[6];
+    const int n = interp_w(xf.interp, __dsub_rn(sx, fx), wx);
+    interp_w(xf.interp, __dsub_rn(sy, fy), wy);
+    const int start = 1 - n / 2;
+    float acc = 0.f;
+    for (int j = 0; j < n; j++) {
+        const float* row = src + (size_t)min(max(y0 + start + j, 0), h - 1) * w;
+        float r = 0.f;
+        for (int i = 0; i < n; i++) r = __fadd_rn(r, __fmul_rn(wx[i], row[min(max(x0 + start + i, 0), w - 1)]));
+        acc = __fadd_rn(acc, __fmul_rn(wy[j], r));
+    }
+    out[(size_t)y * w + x] = acc;
+}
+
+// brightness.rs:67 `sums` of every aligned frame against frame 0: over the
+// stride-4 grid points that the frame's map (align.rs:291) keeps inside,
+// the warped frame's channels (the pixel as shot where the warp leaves the
+// frame) and frame 0's; f64 partials per block, then in order.
+__global__ void bright_kernel(const uint16_t* __restrict__ frames, int w, int h, const BrightXform* __restrict__ xf, int interp,
+                              int nparts, double* __restrict__ part) {
+    const int k = blockIdx.y + 1, pi = blockIdx.x;
+    const int gw = (w + 3) / 4, gh = (h + 3) / 4, ng = gw * gh;
+    const int per = (ng + nparts - 1) / nparts, lo = pi * per, hi = min(ng, lo + per);
+    const uint16_t* f = frames + (size_t)k * w * h * 3;
+    const BrightXform X = xf[k];
+    double s[7] = {0, 0, 0, 0, 0, 0, 0};
+    for (int g = lo + threadIdx.x; g < hi; g += blockDim.x) {
+        const int x = (g % gw) * 4, y = (g / gw) * 4;
+        if (!X.ident) {
+            const double* m = X.inv;
+            const double d = __dadd_rn(__dadd_rn(__dmul_rn(m[6], (double)x), __dmul_rn(m[7], (double)y)), m[8]);
+            const double sx = __ddiv_rn(__dadd_rn(__dadd_rn(__dmul_rn(m[0], (double)x), __dmul_rn(m[1], (double)y)), m[2]), d);
+            const double sy = __ddiv_rn(__dadd_rn(__dadd_rn(__dmul_rn(m[3], (double)x), __dmul_rn(m[4], (double)y)), m[5]), d);
+            if (!(sx >= 0.0 && sx <= (double)(w - 1) && sy >= 0.0 && sy <= (double)(h - 1))) continue;
+        }
+        float v[3];
+        load_px_core(f, X.inv, !X.ident, X.affine, interp, w, h, x, y, v);
+        const uint16_t* r = frames + ((size_t)y * w + x) * 3;
+        for (int c = 0; c < 3; c++) {
+            s[c] += (double)v[c];
+            s[3 + c] += (double)__fmul_rn((float)r[c], LSB_INV16);
+        }
+        s[6] += 1.0;
+    }
+    __shared__ double red[7][128];
+    for (int q = 0; q < 7; q++) red[q][threadIdx.x] = s[q];
+    __syncthreads();
+    for (int st = blockDim.x / 2; st > 0; st >>= 1) {
+        if (threadIdx.x < st)
+            for (int q = 0; q < 7; q++) red[q][threadIdx.x] += red[q][threadIdx.x + st];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0)
+        for (int q = 0; q < 7; q++) part[((size_t)k * nparts + pi) * 7 + q] = red[q][0];
+}
+
+// ------------------------------------------------------------------- host
+static int gsz(size_t n) { return (int)std::min<size_t>((n + 255) / 256, 148 * 16); }
+
+cudaError_t luma_u16(const uint16_t* f, int w, int h, float* y, cudaStream_t s) {
+    size_t n = (size_t)w * h;
+    luma_u16_kernel<<<gsz(n), 256, 0, s>>>(f, n, y);
+    return cudaGetLastError();
+}
+
+void gauss_dims(int w, int h, std::vector<std::pair<int, int>>& dims) {
+    dims.clear();
+    int cw = w, ch = h;
+    while (ch > 64 && cw > 8) {
+        cw = (cw + 1) / 2;
+        ch = (ch + 1) / 2;
+        dims.push_back({cw, ch});
+    }
+}
+
+cudaError_t gauss_levels(const float* y, int w, int h, const std::vector<float*>& lv, cudaStream_t s) {
+    std::vector<std::pair<int, int>> dims;
+    gauss_dims(w, h, dims);
+    const float* src = y;
+    int cw = w, ch = h;
+    for (size_t l = 0; l < dims.size() && l < lv.size(); l++) {
+        dim3 b(32, 8), g((dims[l].first + 31) / 32, (dims[l].second + 7) / 8);
+        reduce_burt_kernel<<<g, b, 0, s>>>(src, cw, ch, lv[l], dims[l].first, dims[l].second);
+        src = lv[l];
+        cw = dims[l].first;
+        ch = dims[l].second;
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t warp_plane(const float* src, int w, int h, const WarpXform& xf, float* out, cudaStream_t s) {
+    dim3 b(32, 8), g((w + 31) / 32, (h + 7) / 8);
+    warp_plane_kernel<<<g, b, 0, s>>>(src, w, h, xf, out);
+    return cudaGetLastError();
+}
+
+cudaError_t bright_sums(const uint16_t* frames, int n, int w, int h, const BrightXform* xf_dev, int interp, int nparts, double* part,
+                        cudaStream_t s) {
+    if (n < 2) return cudaSuccess;
+    dim3 g(nparts, n - 1);
+    bright_kernel<<<g, 128, 0, s>>>(frames, w, h, xf_dev, interp, nparts, part);
+    return cudaGetLastError();
+}
+
+// --------------------------------------------------- the search (host side)
+// align.rs:200-294 Sim::matrix and inverse, exactly as the reference.
+void sim_matrix(const double* v, int w, int h, double m[9]) {
+    const double cx = (double)w / 2.0, cy = (double)h / 2.0;
+    const double c = std::cos(v[3]), sn = std::sin(v[3]);
+    const double sc = v[2], shear = v[5], aspect = v[4];
+    const double a = sc * c, b = sc * (c * shear - sn * aspect), d = sc * sn, e = sc * (sn * shear + c * aspect);
+    const double gx = v[6] / (double)w, gy = v[7] / (double)h;
+    const double a2 = a + cx * gx, b2 = b + cx * gy, d2 = d + cy * gx, e2 = e + cy * gy;
+    m[0] = a2;
+    m[1] = b2;
+    m[2] = cx + v[0] * (double)w - (a2 * cx + b2 * cy);
+    m[3] = d2;
+    m[4] = e2;
+    m[5] = cy + v[1] * (double)h - (d2 * cx + e2 * cy);
+    m[6] = gx;
+    m[7] = gy;
+    m[8] = 1.0 - gx * cx - gy * cy;
+}
+void mat_inverse(const double m[9], double inv[9]) {
+    if (m[6] == 0.0 && m[7] == 0.0 && m[8] == 1.0) {
+        const double a = m[0], b = m[1], tx = m[2], d = m[3], e = m[4], ty = m[5];
+        const double det = a * e - b * d;
+        const double ia = e / det, ib = -b / det, id = -d / det, ie = a / det;
+        inv[0] = ia;
+        inv[1] = ib;
+        inv[2] = -(ia * tx + ib * ty);
+        inv[3] = id;
+        inv[4] = ie;
+        inv[5] = -(id * tx + ie * ty);
+        inv[6] = 0.0;
+        inv[7] = 0.0;
+        inv[8] = 1.0;
+        return;
+    }
+    auto M = [&](int i, int j) { return m[3 * i + j]; };
+    auto cof = [&](int i, int j) {
+        const int r0 = (i + 1) % 3, r1 = (i + 2) % 3, c0 = (j + 1) % 3, c1 = (j + 2) % 3;
+        return M(r0, c0) * M(r1, c1) - M(r0, c1) * M(r1, c0);
+    };
+    for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) inv[3 * i + j] = cof(j, i);
+    const double k = inv[8];
+    for (int i = 0; i < 9; i++) inv[i] /= k;
+}
+bool sim_is_id(const double* v) {
+    static const double id[8] = {0.0, 0.0, 1.0, 0.0, 1.0, 0.0, 0.0, 0.0};
+    for (int k = 0; k < 8; k++)
+        if (v[k] != id[k]) return false;
+    return true;
+}
+
+// align.rs:581's cost for a batch of full Sim vectors on one level pair.
+static cudaError_t eval_batch(AlignCtx& C, const float* rf, int aw, int ah, const float* tg, int tw, int th,
+                              const std::vector<std::vector<double>>& sims, std::vector<double>& costs) {
+    costs.assign(sims.size(), 0.0);
+    for (size_t b0 = 0; b0 < sims.size(); b0 += MAX_CAND) {
+        const int nc = (int)std::min<size_t>(MAX_CAND, sims.size() - b0);
+        CostBatch cb;
+        for (int k = 0; k < nc; k++) {
+            double m[9];
+            sim_matrix(sims[b0 + k].data(), tw, th, m);
+            mat_inverse(m, cb.inv[k]);
+        }
+        const size_t npx = (size_t)aw * ah;
+        const int nblocks = (int)std::min<size_t>(std::max<size_t>((npx + 255) / 256, 1), 296);
+        dim3 g(nblocks, nc);
+        cost_kernel<<<g, 256, 0, C.s>>>(rf, aw, ah, tg, tw, th, cb, C.part);
+        cost_final_kernel<<<1, 32, 0, C.s>>>(C.part, nblocks, nc, C.sums_dev);
+        cudaMemcpyAsync(C.sums_host, C.sums_dev, sizeof(double) * 3 * nc, cudaMemcpyDeviceToHost, C.s);
+        cudaError_t e = cudaStreamSynchronize(C.s);
+        if (e != cudaSuccess) return e;
+        C.launches++;
+        for (int k = 0; k < nc; k++) {
+            const double sd = C.sums_host[3 * k], sd2 = C.sums_host[3 * k + 1], cnt = C.sums_host[3 * k + 2];
+            costs[b0 + k] = cnt < 16.0 ? 1e9 : std::sqrt(std::max((sd2 - sd * sd / cnt) / cnt, 0.0));
+        }
+    }
+    return cudaSuccess;
+}
+
+// align.rs:796 `nelder_mead`, evaluations batched per iteration.
+static cudaError_t nelder_mead_dev(AlignCtx& C, const std::function<cudaError_t(const std::vector<std::vector<double>>&, std::vector<double>&)>& F,
+                                   const std::vector<double>& x0, const std::vector<double>& lo, const std::vector<double>& hi,
+                                   const std::vector<double>& step, const std::vector<double>& tol, std::vector<double>& out) {
+    const size_t n = x0.size();
+    out = x0;
+    if (n == 0) return cudaSuccess;
+    auto clampv = [&](std::vector<double>& v) {
+        for (size_t k = 0; k < n; k++) v[k] = std::min(std::max(v[k], lo[k]), hi[k]);
+    };
+    std::vector<std::vector<double>> simplex{x0};
+    for (size_t k = 0; k < n; k++) {
+        std::vector<double> v = x0;
+        v[k] += step[k];
+        clampv(v);
+        simplex.push_back(v);
+    }
+    std::vector<double> fv;
+    cudaError_t e = F(simplex, fv);
+    if (e != cudaSuccess) return e;
+    C.evals += n + 1;
+    const double alpha = 1.0, gamma = 2.0, rho = 0.5, sigma = 0.5;
+    for (int it = 0; it < 200; it++) {
+        std::vector<size_t> idx(n + 1);
+        for (size_t i = 0; i <= n; i++) idx[i] = i;
+        std::stable_sort(idx.begin(), idx.end(), [&](size_t a, size_t b) { return fv[a] < fv[b]; });
+        std::vector<std::vector<double>> s2;
+        std::vector<double> f2;
+        for (size_t i : idx) {
+            s2.push_back(simplex[i]);
+            f2.push_back(fv[i]);
+        }
+        simplex.swap(s2);
+        fv.swap(f2);
+        // align.rs:888 `converged`
+        bool conv = std::fabs(fv[n] - fv[0]) <= 1e-4 * (1.0 + std::fabs(fv[0]));
+        for (size_t i = 1; conv && i <= n; i++)
+            for (size_t k = 0; k < n; k++)
+                if (!(std::fabs(simplex[i][k] - simplex[0][k]) <= tol[k])) {
+                    conv = false;
+                    break;
+                }
+        if (conv) break;
+        std::vector<double> c(n, 0.0);
+        for (size_t i = 0; i < n; i++)
+            for (size_t k = 0; k < n; k++) c[k] += simplex[i][k];
+        for (size_t k = 0; k < n; k++) c[k] /= (double)n;
+        std::vector<double> xr(n), xe(n), xc(n);
+        for (size_t k = 0; k < n; k++) xr[k] = c[k] + alpha * (c[k] - simplex[n][k]);
+        clampv(xr);
+        for (size_t k = 0; k < n; k++) xe[k] = c[k] + gamma * (xr[k] - c[k]);
+        clampv(xe);
+        for (size_t k = 0; k < n; k++) xc[k] = c[k] + rho * (simplex[n][k] - c[k]);
+        clampv(xc);
+        std::vector<double> f3;
+        e = F({xr, xe, xc}, f3);
+        if (e != cudaSuccess) return e;
+        const double fr = f3[0], fe = f3[1], fc = f3[2];
+        C.evals += 1;
+        if (fr < fv[0]) {
+            C.evals += 1;
+            if (fe < fr) {
+                simplex[n] = xe;
+                fv[n] = fe;
+            } else {
+                simplex[n] = xr;
+                fv[n] = fr;
+            }
+        } else if (fr < fv[n - 1]) {
+            simplex[n] = xr;
+            fv[n] = fr;
+        } else {
+            C.evals += 1;
+            if (fc < fv[n]) {
+                simplex[n] = xc;
+                fv[n] = fc;
+            } else {
+                std::vector<std::vector<double>> pts;
+                for (size_t i = 1; i <= n; i++) {
+                    for (size_t k = 0; k < n; k++) simplex[i][k] = simplex[0][k] + sigma * (simplex[i][k] - simplex[0][k]);
+                    clampv(simplex[i]);
+                    pts.push_back(simplex[i]);
+                }
+                std::vector<double> fs;
+                e = F(pts, fs);
+                if (e != cudaSuccess) return e;
+                C.evals += n;
+                for (size_t i = 1; i <= n; i++) fv[i] = fs[i - 1];
+            }
+        }
+    }
+    size_t best = 0;
+    for (size_t i = 1; i <= n; i++)
+        if (fv[i] < fv[best]) best = i;
+    out = simplex[best];
+    return cudaSuccess;
+}
+
+// align.rs:896 `multiscale_align`: rf/tg full-res planes with their levels.
+cudaError_t multiscale_align(AlignCtx& C, const float* rf, const std::vector<float*>& pr, const float* tg,
+                             const std::vector<float*>& pt, int w, int h, const double init[8], const bool freem[8], int coarsen,
+                             double out[8]) {
+    std::vector<std::pair<int, int>> dims;
+    gauss_dims(w, h, dims);
+    const size_t n = dims.size() + 1;
+    static const double SPAN[8] = {0.10, 0.10, 0.10, 0.087266462599716474, 0.05, 0.05, 0.05, 0.05};
+    std::vector<size_t> free_idx;
+    for (size_t k = 0; k < 8; k++)
+        if (freem[k]) free_idx.push_back(k);
+    std::vector<double> lo_f, hi_f;
+    for (size_t k : free_idx) {
+        lo_f.push_back(init[k] - SPAN[k]);
+        hi_f.push_back(init[k] + SPAN[k]);
+    }
+    std::vector<double> cur(init, init + 8);
+    const size_t finest = std::min((size_t)coarsen, n - 1);
+    for (size_t lvl = n; lvl-- > finest;) {
+        const float* a_d = lvl == 0 ? rf : pr[lvl - 1];
+        const float* t_d = lvl == 0 ? tg : pt[lvl - 1];
+        const int lw = lvl == 0 ? w : dims[lvl - 1].first, lh = lvl == 0 ? h : dims[lvl - 1].second;
+        const std::vector<double> snap = cur;
+        auto F = [&](const std::vector<std::vector<double>>& xs, std::vector<double>& fs) {
+            std::vector<std::vector<double>> sims;
+            for (auto& xf : xs) {
+                std::vector<double> v = snap;
+                for (size_t k = 0; k < free_idx.size(); k++) v[free_idx[k]] = xf[k];
+                sims.push_back(v);
+            }
+            return eval_batch(C, a_d, lw, lh, t_d, lw, lh, sims, fs);
+        };
+        std::vector<double> x0, step, tol;
+        for (size_t k : free_idx) x0.push_back(cur[k]);
+        // align.rs:784 `level_steps`
+        const double wf = w, hf = h, r = std::max(wf, hf) / 2.0;
+        const double gain[8] = {wf, hf, r, r, hf / 2.0, hf / 2.0, wf / 4.0, hf / 4.0};
+        const double px = (double)((uint64_t)1 << lvl);
+        for (size_t k : free_idx) {
+            step.push_back(1.0 * px / gain[k]);
+            tol.push_back(0.1 * px / gain[k]);
+        }
+        std::vector<double> best;
+        cudaError_t e = nelder_mead_dev(C, F, x0, lo_f, hi_f, step, tol, best);
+        if (e != cudaSuccess) return e;
+        for (size_t k = 0; k < free_idx.size(); k++) cur[free_idx[k]] = best[k];
+    }
+    for (int k = 0; k < 8; k++) out[k] = cur[k];
+    return cudaSuccess;
+}
+
+cudaError_t cost_single(AlignCtx& C, const float* rf, int aw, int ah, const float* tg, int tw, int th, const double sim[8],
+                        double* cost) {
+    std::vector<double> fs;
+    cudaError_t e = eval_batch(C, rf, aw, ah, tg, tw, th, {std::vector<double>(sim, sim + 8)}, fs);
+    *cost = fs.empty() ? 0.0 : fs[0];
+    return e;
+}
+
+}  // namespace lsb

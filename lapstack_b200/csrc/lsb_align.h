@@ -1,0 +1,50 @@
+// Internal interfaces of the registration kernels (host side).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <utility>
+#include <vector>
+
+namespace lsb {
+
+constexpr int MAX_CAND = 9;
+
+// The inverse homographies of a batch of candidate transforms (row-major 3x3).
+struct CostBatch {
+    double inv[MAX_CAND][9];
+};
+struct WarpXform {
+    double inv[9];
+    int affine, interp;
+};
+struct BrightXform {
+    double inv[9];
+    int ident, affine;
+};
+
+// Search state: the stream, scratch for the cost partials and counters.
+struct AlignCtx {
+    cudaStream_t s;
+    double* part;      // device, MAX_CAND * 296 * 3
+    double* sums_dev;  // device, MAX_CAND * 3
+    double* sums_host; // pinned, MAX_CAND * 3
+    size_t evals = 0, launches = 0;
+};
+
+cudaError_t luma_u16(const uint16_t* f, int w, int h, float* y, cudaStream_t s);
+void gauss_dims(int w, int h, std::vector<std::pair<int, int>>& dims);
+cudaError_t gauss_levels(const float* y, int w, int h, const std::vector<float*>& lv, cudaStream_t s);
+cudaError_t warp_plane(const float* src, int w, int h, const WarpXform& xf, float* out, cudaStream_t s);
+cudaError_t bright_sums(const uint16_t* frames, int n, int w, int h, const BrightXform* xf_dev, int interp, int nparts, double* part,
+                        cudaStream_t s);
+void sim_matrix(const double* v, int w, int h, double m[9]);
+void mat_inverse(const double m[9], double inv[9]);
+bool sim_is_id(const double* v);
+cudaError_t multiscale_align(AlignCtx& C, const float* rf, const std::vector<float*>& pr, const float* tg,
+                             const std::vector<float*>& pt, int w, int h, const double init[8], const bool freem[8], int coarsen,
+                             double out[8]);
+cudaError_t cost_single(AlignCtx& C, const float* rf, int aw, int ah, const float* tg, int tw, int th, const double sim[8],
+                        double* cost);
+
+}  // namespace lsb

@@ -1,0 +1,1033 @@
+// The C ABI of include/lapstack_b200.h: engine, stack and the standalone
+// depth / WLS / registration entry points. A stack runs the reference's
+// pipeline order (stack.rs:1011 `run_with` for in-memory frames): register
+// every frame to the previous aligned one, equalise brightness, fold all
+// frames level by level, fuse the residuals, collapse, take the shares, then
+// the depth pass on the focus slices the fold took.
+#include <math.h>
+#include <stdarg.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include <algorithm>
+#include <array>
+#include <string>
+#include <vector>
+
+#include "lapstack_b200.h"
+#include "lsb_align.h"
+#include "lsb_depth.h"
+#include "lsb_internal.h"
+
+using namespace lsb;
+
+static char* dup_err(const std::string& s) {
+    char* p = (char*)malloc(s.size() + 1);
+    memcpy(p, s.c_str(), s.size() + 1);
+    return p;
+}
+static std::string fmt(const char* f, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, f);
+    vsnprintf(buf, sizeof buf, f, ap);
+    va_end(ap);
+    return buf;
+}
+#define TRY(expr)                                                                                  \
+    do {                                                                                           \
+        cudaError_t _e = (expr);                                                                   \
+        if (_e != cudaSuccess) return dup_err(fmt("%s: %s (%s:%d)", #expr, cudaGetErrorString(_e), __FILE__, __LINE__)); \
+    } while (0)
+
+struct DevPool {
+    std::vector<void*> ptrs;
+    template <class T>
+    cudaError_t get(T** p, size_t n) {
+        void* q = nullptr;
+        cudaError_t e = cudaMalloc(&q, std::max<size_t>(n, 1) * sizeof(T));
+        if (e == cudaSuccess) ptrs.push_back(q);
+        *p = (T*)q;
+        return e;
+    }
+    void release() {
+        for (void* p : ptrs) cudaFree(p);
+        ptrs.clear();
+    }
+    ~DevPool() { release(); }
+};
+
+struct lsb_engine {
+    lsb_config cfg;
+    int device, sms, grid;
+    cudaStream_t s;
+    DevPool pool;
+    unsigned *hist, *sel;
+    float* scal;  // [floor, p90, max, ...]
+    AlignCtx actx;
+    cudaEvent_t ev[10];
+    void log(const std::string& line) {
+        if (cfg.log) cfg.log(line.c_str(), cfg.user);
+    }
+};
+
+struct lsb_stack {
+    lsb_engine* e;
+    uint32_t w, h, n, count;
+    lsb_fuse_params fp;
+    lsb_align_params ap;
+    lsb_depth_params dp;
+    bool brightness, crop, fp16, f32src;
+    int levels, depth_level;
+    std::vector<int> lw, lh;  // level dims 0..levels
+    DevPool pool;
+    uint16_t* frames = nullptr;
+    float* frames_f32 = nullptr;
+    std::vector<void*> g;      // G storage per level 1..levels (index l)
+    std::vector<float*> acc, best;
+    uint16_t* winner = nullptr;
+    void* slices = nullptr;
+    int dw = 0, dh = 0, bk = 1;
+    FrameXform* xf_dev = nullptr;
+    std::vector<FrameXform> xf;
+    std::vector<double> sims;   // n*8
+    std::vector<float> gains;   // n*3
+    float* top = nullptr;       // fused residual [3][ht][wt]
+    float *dev_s = nullptr, *ent_s = nullptr, *lnp = nullptr;
+    float *img = nullptr, *img_tmp = nullptr;
+    uint16_t* img_u16 = nullptr;
+    unsigned* counts = nullptr;
+    float* mx = nullptr;
+    double *mpart = nullptr, *means = nullptr;
+    int* status = nullptr;
+    // registration scratch
+    float *yt = nullptr, *yr = nullptr;
+    std::vector<float*> pt, pr;
+    BrightXform* bx_dev = nullptr;
+    double* bpart = nullptr;
+    // depth scratch
+    float *yfull = nullptr, *guide = nullptr, *mi = nullptr, *vi = nullptr, *tmp = nullptr, *state = nullptr;
+    float *draw = nullptr, *dmed = nullptr, *conf = nullptr, *mins = nullptr, *u = nullptr, *w2 = nullptr;
+    float *t0 = nullptr, *t1 = nullptr, *t2 = nullptr, *abar = nullptr, *bbar = nullptr, *dfull = nullptr, *cfull = nullptr;
+    bool folded = false;
+    size_t align_evals = 0;
+    float floor_v = 0.f, p90 = 0.f, rel = 0.f;
+    double rel64 = 0.0;
+    int iters = 0, iters_first = 0;
+    double ms[8] = {0};
+};
+
+extern "C" {
+
+uint32_t lsb_abi(void) { return LSB_ABI_VERSION; }
+void lsb_free_str(char* s) { free(s); }
+
+char* lsb_engine_create(const lsb_config* cfg, lsb_engine** out) {
+    *out = nullptr;
+    lsb_engine* e = new lsb_engine();
+    e->cfg = cfg ? *cfg : lsb_config{0, 0, 0, 0, nullptr, nullptr};
+    e->device = e->cfg.device;
+    int ndev = 0;
+    cudaError_t r = cudaGetDeviceCount(&ndev);
+    if (r != cudaSuccess || ndev == 0) {
+        delete e;
+        return dup_err(fmt("lapstack-b200 needs a CUDA device: %s", r != cudaSuccess ? cudaGetErrorString(r) : "none found"));
+    }
+    TRY(cudaSetDevice(e->device));
+    cudaDeviceProp prop;
+    TRY(cudaGetDeviceProperties(&prop, e->device));
+    if (prop.major < 10) {
+        delete e;
+        return dup_err(fmt("lapstack-b200 is built for sm_100a; device %d is sm_%d%d", e->device, prop.major, prop.minor));
+    }
+    e->sms = prop.multiProcessorCount;
+    e->grid = e->cfg.grid_limit > 0 ? e->cfg.grid_limit : 2 * e->sms;
+    TRY(cudaStreamCreateWithFlags(&e->s, cudaStreamNonBlocking));
+    TRY(e->pool.get(&e->hist, 65536));
+    TRY(e->pool.get(&e->sel, 4));
+    TRY(e->pool.get(&e->scal, 16));
+    e->actx.s = e->s;
+    TRY(e->pool.get(&e->actx.part, MAX_CAND * 296 * 3));
+    TRY(e->pool.get(&e->actx.sums_dev, MAX_CAND * 3));
+    TRY(cudaHostAlloc((void**)&e->actx.sums_host, sizeof(double) * MAX_CAND * 3, cudaHostAllocDefault));
+    for (auto& v : e->ev) TRY(cudaEventCreate(&v));
+    *out = e;
+    return nullptr;
+}
+
+void lsb_engine_destroy(lsb_engine* e) {
+    if (!e) return;
+    cudaStreamSynchronize(e->s);
+    for (auto& v : e->ev) cudaEventDestroy(v);
+    cudaFreeHost(e->actx.sums_host);
+    e->pool.release();
+    cudaStreamDestroy(e->s);
+    delete e;
+}
+
+void* lsb_engine_stream(lsb_engine* e) { return e ? (void*)e->s : nullptr; }
+
+}  // extern "C"
+
+static size_t gs_bytes(const lsb_stack* s) { return s->fp16 ? 2 : 4; }
+
+// depth.rs:454 `rdf_taps` in depth.rs:417 `conv_sparse`'s per-pixel order
+static std::vector<float> focus_taps(uint32_t r_in, uint32_t r_out) {
+    std::vector<std::array<int, 2>> disk, ring;
+    int ri2 = (int)(r_in * r_in), ro2 = (int)(r_out * r_out), r = (int)r_out;
+    for (int dy = -r; dy <= r; dy++)
+        for (int dx = -r; dx <= r; dx++) {
+            int d2 = dx * dx + dy * dy;
+            if (d2 <= ri2) disk.push_back({dy, dx});
+            else if (d2 <= ro2) ring.push_back({dy, dx});
+        }
+    float wd = 1.0f / (float)disk.size(), wr = -1.0f / (float)std::max<size_t>(ring.size(), 1);
+    std::vector<std::array<float, 3>> list;
+    for (auto& p : disk) list.push_back({(float)p[0], (float)p[1], wd});
+    for (auto& p : ring) list.push_back({(float)p[0], (float)p[1], wr});
+    std::vector<float> dys, out;
+    for (auto& t : list)
+        if (std::find(dys.begin(), dys.end(), t[0]) == dys.end()) dys.push_back(t[0]);
+    for (float dy : dys)
+        for (auto& t : list)
+            if (t[0] == dy) out.insert(out.end(), {t[0], t[1], t[2]});
+    return out;
+}
+
+static char* stack_alloc(lsb_stack* s) {
+    DevPool& P = s->pool;
+    const size_t W = s->w, H = s->h, N = s->n;
+    TRY(P.get(&s->frames, N * W * H * 3));
+    s->g.assign(s->levels + 1, nullptr);
+    s->acc.assign(s->levels, nullptr);
+    s->best.assign(s->levels, nullptr);
+    for (int l = 1; l <= s->levels; l++) {
+        void* p = nullptr;
+        TRY(cudaMalloc(&p, N * 3 * (size_t)s->lw[l] * s->lh[l] * gs_bytes(s)));
+        P.ptrs.push_back(p);
+        s->g[l] = p;
+    }
+    for (int l = 0; l < s->levels; l++) {
+        TRY(P.get(&s->acc[l], 3 * (size_t)s->lw[l] * s->lh[l]));
+        TRY(P.get(&s->best[l], (size_t)s->lw[l] * s->lh[l]));
+    }
+    TRY(P.get(&s->winner, (size_t)s->lw[s->depth_level] * s->lh[s->depth_level]));
+    const size_t nt = (size_t)s->lw[s->levels] * s->lh[s->levels];
+    TRY(P.get(&s->top, 3 * nt));
+    TRY(P.get(&s->dev_s, N * nt));
+    TRY(P.get(&s->ent_s, N * nt));
+    TRY(P.get(&s->lnp, 128));
+    TRY(P.get(&s->img, 3 * W * H));
+    TRY(P.get(&s->img_tmp, 3 * W * H));
+    TRY(P.get(&s->img_u16, 3 * W * H));
+    TRY(P.get(&s->counts, N));
+    TRY(P.get(&s->mx, 4));
+    TRY(P.get(&s->mpart, N * 64 * 3));
+    TRY(P.get(&s->means, N * 3));
+    TRY(P.get(&s->status, 4));
+    TRY(P.get(&s->xf_dev, N));
+    if (s->dp.enabled) {
+        s->bk = 1 << s->dp.scale;
+        s->dw = (int)((W + s->bk - 1) / s->bk);
+        s->dh = (int)((H + s->bk - 1) / s->bk);
+        const size_t m = (size_t)s->dw * s->dh;
+        void* p = nullptr;
+        TRY(cudaMalloc(&p, N * m * (s->fp16 ? 2 : 4)));
+        P.ptrs.push_back(p);
+        s->slices = p;
+        for (float** q : {&s->guide, &s->mi, &s->vi, &s->tmp, &s->draw, &s->dmed, &s->conf, &s->mins, &s->u, &s->w2, &s->t0,
+                          &s->t1, &s->t2, &s->abar, &s->bbar})
+            TRY(P.get(q, m));
+        TRY(P.get(&s->state, 9 * m));
+        TRY(P.get(&s->yfull, W * H));
+        TRY(P.get(&s->dfull, W * H));
+        TRY(P.get(&s->cfull, W * H));
+    }
+    if (s->ap.enabled && N > 1) {
+        TRY(P.get(&s->yt, W * H));
+        TRY(P.get(&s->yr, W * H));
+        std::vector<std::pair<int, int>> dims;
+        gauss_dims((int)W, (int)H, dims);
+        for (auto& d : dims) {
+            float *a, *b;
+            TRY(P.get(&a, (size_t)d.first * d.second));
+            TRY(P.get(&b, (size_t)d.first * d.second));
+            s->pt.push_back(a);
+            s->pr.push_back(b);
+        }
+        TRY(P.get(&s->bx_dev, N));
+        TRY(P.get(&s->bpart, N * 64 * 7));
+    }
+    return nullptr;
+}
+
+extern "C" char* lsb_stack_begin(lsb_engine* e, uint32_t w, uint32_t h, uint32_t n_frames, const lsb_fuse_params* fuse,
+                                 const lsb_align_params* align, const lsb_depth_params* depth, int32_t brightness, int32_t crop,
+                                 lsb_stack** out) {
+    *out = nullptr;
+    if (!e) return dup_err("no engine");
+    if (w == 0 || h == 0 || n_frames == 0) return dup_err("a stack needs a size and at least one frame");
+    if (n_frames > 65535) return dup_err("at most 65535 frames (the winner map is u16)");
+    lsb_stack* s = new lsb_stack();
+    s->e = e;
+    s->w = w;
+    s->h = h;
+    s->n = n_frames;
+    s->count = 0;
+    s->fp = fuse ? *fuse : lsb_fuse_params{0, 1, 0, 2, 256, 0, 2, 0.f};
+    s->ap = align ? *align : lsb_align_params{0, 1, 1, 1, 0, 0, 3, 0};
+    s->dp = depth ? *depth : lsb_depth_params{};
+    s->brightness = brightness != 0;
+    s->crop = crop != 0;
+    s->fp16 = e->cfg.fp16_storage != 0;
+    s->f32src = false;
+    if (s->fp.halo > 0.f) {
+        delete s;
+        return dup_err("halo control (FuseParams::halo > 0) is not on the device path");
+    }
+    if (s->fp.energy_radius > 2) {
+        delete s;
+        return dup_err("energy_radius must be 0..2");
+    }
+    if (s->fp.top_radius > 4) {
+        delete s;
+        return dup_err("top_radius must be 0..4");
+    }
+    if (s->dp.enabled) {
+        const char* bad = nullptr;
+        if (s->dp.scale > 2) bad = "depth scale must be 0..2";
+        else if (s->dp.focus == 0 && (s->dp.r_out > 3 || s->dp.r_out <= s->dp.r_in)) bad = "rdf radii: r_in < r_out <= 3";
+        else if (s->dp.focus == 1 && (s->dp.sml_step < 1 || s->dp.sml_step > 3)) bad = "sml step must be 1..3";
+        else if (aggregate_smem_bytes((int)s->dp.agg_radius) > 227 * 1024) bad = "agg_radius too large";
+        if (bad) {
+            delete s;
+            return dup_err(bad);
+        }
+    }
+    // pyramid.rs:191 auto_levels(w, h, 32); fuse.rs:372-373
+    uint32_t levels = s->fp.levels;
+    if (levels == 0) {
+        size_t cw = w, ch = h, k = 0;
+        while ((cw > 1 || ch > 1) && std::min((cw + 1) / 2, (ch + 1) / 2) >= 32) {
+            cw = (cw + 1) / 2;
+            ch = (ch + 1) / 2;
+            k++;
+        }
+        levels = (uint32_t)std::max<size_t>(k, 1);
+    }
+    s->levels = (int)levels;
+    s->depth_level = (int)std::min(s->fp.depth_level, levels - 1);
+    s->lw.push_back((int)w);
+    s->lh.push_back((int)h);
+    for (int l = 1; l <= s->levels; l++) {
+        s->lw.push_back((s->lw.back() + 1) / 2);
+        s->lh.push_back((s->lh.back() + 1) / 2);
+    }
+    char* err = stack_alloc(s);
+    if (err) {
+        delete s;
+        return err;
+    }
+    s->sims.assign((size_t)n_frames * 8, 0.0);
+    for (uint32_t k = 0; k < n_frames; k++) {
+        s->sims[8 * k + 2] = 1.0;
+        s->sims[8 * k + 4] = 1.0;
+    }
+    s->gains.assign((size_t)n_frames * 3, 1.f);
+    *out = s;
+    return nullptr;
+}
+
+static bool is_device_ptr(const void* p) {
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+
+extern "C" char* lsb_stack_push_u16(lsb_stack* s, const uint16_t* rgb, size_t stride_px) {
+    if (!s || !rgb) return dup_err("null argument");
+    if (s->f32src) return dup_err("this stack takes f32 frames");
+    if (s->count >= s->n) return dup_err(fmt("the stack holds %u frames", s->n));
+    if (stride_px == 0) stride_px = s->w;
+    if (stride_px < s->w) return dup_err("stride_px < width");
+    uint16_t* dst = s->frames + (size_t)s->count * s->w * s->h * 3;
+    cudaMemcpyKind kind = is_device_ptr(rgb) ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+    if (stride_px == s->w) TRY(cudaMemcpyAsync(dst, rgb, sizeof(uint16_t) * 3 * (size_t)s->w * s->h, kind, s->e->s));
+    else TRY(cudaMemcpy2DAsync(dst, 6 * (size_t)s->w, rgb, 6 * stride_px, 6 * (size_t)s->w, s->h, kind, s->e->s));
+    s->count++;
+    s->folded = false;
+    return nullptr;
+}
+
+extern "C" char* lsb_stack_push_f32(lsb_stack* s, const float* const planes[3]) {
+    if (!s || !planes) return dup_err("null argument");
+    if (s->count >= s->n) return dup_err(fmt("the stack holds %u frames", s->n));
+    if (s->ap.enabled && s->n > 1) return dup_err("f32 frames are folded as given: disable alignment");
+    if (!s->frames_f32) {
+        if (s->count > 0) return dup_err("this stack takes u16 frames");
+        void* p = nullptr;
+        TRY(cudaMalloc(&p, sizeof(float) * 3 * (size_t)s->n * s->w * s->h));
+        s->pool.ptrs.push_back(p);
+        s->frames_f32 = (float*)p;
+        s->f32src = true;
+    }
+    const size_t np = (size_t)s->w * s->h;
+    for (int c = 0; c < 3; c++) {
+        cudaMemcpyKind kind = is_device_ptr(planes[c]) ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+        TRY(cudaMemcpyAsync(s->frames_f32 + ((size_t)s->count * 3 + c) * np, planes[c], sizeof(float) * np, kind, s->e->s));
+    }
+    s->count++;
+    s->folded = false;
+    return nullptr;
+}
+
+extern "C" char* lsb_stack_frames_device(lsb_stack* s, uint16_t** frames_dev) {
+    if (!s || !frames_dev) return dup_err("null argument");
+    *frames_dev = s->frames;
+    return nullptr;
+}
+
+extern "C" char* lsb_stack_set_count(lsb_stack* s, uint32_t count) {
+    if (!s) return dup_err("null argument");
+    if (count > s->n) return dup_err("count exceeds the stack's frames");
+    s->count = count;
+    s->folded = false;
+    return nullptr;
+}
+
+// ------------------------------------------------------------- pipeline
+static char* run_align(lsb_stack* s) {
+    lsb_engine* e = s->e;
+    const int W = (int)s->w, H = (int)s->h, n = (int)s->count;
+    AlignCtx& C = e->actx;
+    C.evals = 0;
+    bool freem[8];
+    {
+        bool aff = s->ap.model != 0, proj = s->ap.model == 2;
+        bool m[8] = {s->ap.shift != 0, s->ap.shift != 0, s->ap.scale != 0, s->ap.rotation != 0, aff, aff, proj, proj};
+        memcpy(freem, m, sizeof m);
+    }
+    for (int i = 0; i < n; i++) {
+        const uint16_t* f = s->frames + (size_t)i * W * H * 3;
+        double* sim = &s->sims[8 * (size_t)i];
+        const double id[8] = {0, 0, 1, 0, 1, 0, 0, 0};
+        memcpy(sim, id, sizeof id);
+        TRY(luma_u16(f, W, H, s->yt, e->s));
+        if (i > 0) {
+            TRY(gauss_levels(s->yt, W, H, s->pt, e->s));
+            TRY(multiscale_align(C, s->yr, s->pr, s->yt, s->pt, W, H, &s->sims[8 * (size_t)(i - 1)], freem, (int)s->ap.coarsen, sim));
+        }
+        if (i + 1 < n) {
+            // the next frame's reference: this frame's luma as aligned (stack.rs:527)
+            if (sim_is_id(sim)) {
+                TRY(cudaMemcpyAsync(s->yr, s->yt, sizeof(float) * W * H, cudaMemcpyDeviceToDevice, e->s));
+            } else {
+                WarpXform wx;
+                double m[9];
+                sim_matrix(sim, W, H, m);
+                mat_inverse(m, wx.inv);
+                wx.affine = wx.inv[6] == 0.0 && wx.inv[7] == 0.0 && wx.inv[8] == 1.0;
+                wx.interp = (int)s->ap.interp;
+                TRY(warp_plane(s->yt, W, H, wx, s->yr, e->s));
+            }
+            TRY(gauss_levels(s->yr, W, H, s->pr, e->s));
+        }
+    }
+    s->align_evals = C.evals;
+    return nullptr;
+}
+
+// brightness.rs:93 `ratio`
+static void bratio(const double ref[3], const double frame[3], size_t n, float g[3]) {
+    for (int c = 0; c < 3; c++) {
+        if (n < 64) {
+            g[c] = 1.0f;
+            continue;
+        }
+        float v = frame[c] > 1e-9 ? (float)(ref[c] / frame[c]) : 1.0f;
+        g[c] = std::min(std::max(v, 0.25f), 4.0f);
+    }
+}
+
+static char* run_gains(lsb_stack* s, bool aligned) {
+    lsb_engine* e = s->e;
+    const int W = (int)s->w, H = (int)s->h, n = (int)s->count;
+    for (int k = 0; k < n; k++)
+        for (int c = 0; c < 3; c++) s->gains[3 * k + c] = 1.f;
+    if (!s->brightness || n < 2 || s->f32src) return nullptr;
+    if (aligned) {
+        std::vector<BrightXform> bx(n);
+        for (int k = 0; k < n; k++) {
+            double m[9];
+            sim_matrix(&s->sims[8 * (size_t)k], W, H, m);
+            mat_inverse(m, bx[k].inv);
+            bx[k].ident = sim_is_id(&s->sims[8 * (size_t)k]);
+            bx[k].affine = bx[k].inv[6] == 0.0 && bx[k].inv[7] == 0.0 && bx[k].inv[8] == 1.0;
+        }
+        TRY(cudaMemcpyAsync(s->bx_dev, bx.data(), sizeof(BrightXform) * n, cudaMemcpyHostToDevice, e->s));
+        TRY(bright_sums(s->frames, n, W, H, s->bx_dev, (int)s->ap.interp, 64, s->bpart, e->s));
+        std::vector<double> part((size_t)n * 64 * 7);
+        TRY(cudaMemcpyAsync(part.data(), s->bpart, sizeof(double) * part.size(), cudaMemcpyDeviceToHost, e->s));
+        TRY(cudaStreamSynchronize(e->s));
+        for (int k = 1; k < n; k++) {
+            double sm[7] = {0, 0, 0, 0, 0, 0, 0};
+            for (int p = 0; p < 64; p++)
+                for (int q = 0; q < 7; q++) sm[q] += part[((size_t)k * 64 + p) * 7 + q];
+            double sf[3] = {sm[0], sm[1], sm[2]}, so[3] = {sm[3], sm[4], sm[5]};
+            bratio(so, sf, (size_t)sm[6], &s->gains[3 * (size_t)k]);
+        }
+    } else {
+        // stack.rs LazyFrames: gains_to(means(frame 0), frame)
+        TRY(frame_means(s->frames, n, W, H, s->mpart, 64, s->means, e->s));
+        std::vector<double> m((size_t)n * 3);
+        TRY(cudaMemcpyAsync(m.data(), s->means, sizeof(double) * m.size(), cudaMemcpyDeviceToHost, e->s));
+        TRY(cudaStreamSynchronize(e->s));
+        for (int k = 1; k < n; k++) bratio(&m[0], &m[3 * (size_t)k], (size_t)-1, &s->gains[3 * (size_t)k]);
+    }
+    return nullptr;
+}
+
+static float ms_between(cudaEvent_t a, cudaEvent_t b) {
+    float t = 0.f;
+    cudaEventElapsedTime(&t, a, b);
+    return t;
+}
+
+static char* run_pipeline(lsb_stack* s) {
+    lsb_engine* e = s->e;
+    cudaStream_t st = e->s;
+    const int W = (int)s->w, H = (int)s->h, n = (int)s->count;
+    if (n == 0) return dup_err("no frames pushed");
+    const bool aligned = s->ap.enabled && n > 1 && !s->f32src;
+    cudaEvent_t* ev = e->ev;
+    TRY(cudaEventRecord(ev[0], st));
+    if (aligned) {
+        char* err = run_align(s);
+        if (err) return err;
+    }
+    TRY(cudaEventRecord(ev[1], st));
+    {
+        char* err = run_gains(s, aligned);
+        if (err) return err;
+    }
+    // per-frame level-0 transforms
+    s->xf.assign(n, FrameXform{});
+    for (int k = 0; k < n; k++) {
+        FrameXform& X = s->xf[k];
+        const double* sim = &s->sims[8 * (size_t)k];
+        X.warp = aligned && !sim_is_id(sim);
+        if (X.warp) {
+            double m[9];
+            sim_matrix(sim, W, H, m);
+            mat_inverse(m, X.inv);
+        }
+        X.affine = X.inv[6] == 0.0 && X.inv[7] == 0.0 && X.inv[8] == 1.0;
+        X.gain_on = 0;
+        for (int c = 0; c < 3; c++) {
+            X.gain[c] = s->gains[3 * (size_t)k + c];
+            if (fabsf(X.gain[c] - 1.0f) > 1e-6f) X.gain_on |= 1 << c;
+        }
+    }
+    TRY(cudaMemcpyAsync(s->xf_dev, s->xf.data(), sizeof(FrameXform) * n, cudaMemcpyHostToDevice, st));
+    TRY(cudaMemsetAsync(s->status, 0, sizeof(int), st));
+    TRY(cudaEventRecord(ev[2], st));
+    // ---- the fold, level by level over all frames
+    const bool depth_on = s->dp.enabled != 0;
+    if (depth_on && s->dp.focus == 0) {
+        std::vector<float> taps = focus_taps(s->dp.r_in, s->dp.r_out);
+        TRY(set_focus_taps(taps.data(), (int)(taps.size() / 3), st));
+    }
+    for (int l = 0; l < s->levels; l++) {
+        FoldArgs a{};
+        a.level = l;
+        a.nframes = n;
+        a.W = s->lw[l];
+        a.H = s->lh[l];
+        a.W1 = s->lw[l + 1];
+        a.H1 = s->lh[l + 1];
+        a.tiles_x = (a.W + 63) / 64;
+        a.tiles_y = (a.H + 31) / 32;
+        a.ntiles = a.tiles_x * a.tiles_y;
+        a.src_u16 = s->frames;
+        a.src_f32 = s->frames_f32;
+        a.xf = s->xf_dev;
+        a.interp = (int)s->ap.interp;
+        a.src_g = l > 0 ? s->g[l] : nullptr;
+        a.dst_g = s->g[l + 1];
+        a.acc = s->acc[l];
+        a.best = s->best[l];
+        a.winner = l == s->depth_level ? s->winner : nullptr;
+        a.use_chroma = (int)s->fp.use_chroma;
+        a.status = s->status;
+        const bool focus = depth_on && l == 0;
+        if (focus) {
+            a.slice = s->slices;
+            a.dw = s->dw;
+            a.dh = s->dh;
+            a.bk = s->bk;
+            a.focus_kind = (int)s->dp.focus;
+            a.sml_step = (int)s->dp.sml_step;
+            a.ntaps = (int)focus_taps(s->dp.r_in, s->dp.r_out).size() / 3;
+        }
+        const int src = l > 0 ? SRC_G : (s->f32src ? SRC_F32 : SRC_U16);
+        TRY(fold_level(a, src, s->fp16, (int)s->fp.energy_radius, focus, s->fp16, st, e->grid));
+    }
+    TRY(cudaEventRecord(ev[3], st));
+    // ---- residual, collapse
+    {
+        const int wt = s->lw[s->levels], ht = s->lh[s->levels];
+        const int r = (int)s->fp.top_radius, nwin = (2 * r + 1) * (2 * r + 1);
+        std::vector<float> lnp(128, 0.f);
+        const float inv_n = 1.0f / (float)nwin;
+        for (int c = 1; c <= nwin; c++) lnp[c] = logf((float)c * inv_n);
+        TRY(cudaMemcpyAsync(s->lnp, lnp.data(), sizeof(float) * 128, cudaMemcpyHostToDevice, st));
+        ResidualArgs ra{s->g[s->levels], n, wt, ht, (int)s->fp.top_rule, r, (int)s->fp.entropy_bins, s->dev_s, s->ent_s, s->top};
+        TRY(fuse_residuals(ra, s->fp16, s->lnp, st));
+        const float* coarse = s->top;
+        for (int l = s->levels - 1; l >= 0; l--) {
+            // even levels land in img, odd ones in img_tmp: a level never overwrites its coarser input
+            float* out = (l % 2 == 0) ? s->img : s->img_tmp;
+            TRY(collapse_level(s->acc[l], coarse, out, s->lw[l], s->lh[l], s->lw[l + 1], s->lh[l + 1], l == 0, s->img_u16, st));
+            coarse = out;
+        }
+    }
+    TRY(cudaEventRecord(ev[4], st));
+    s->folded = true;
+    // ---- depth
+    if (depth_on) {
+        const int k = s->bk, dw = s->dw, dh = s->dh;
+        const size_t m = (size_t)dw * dh;
+        TRY(luma_and_guide(s->img, W, H, k, s->yfull, s->guide, dw, dh, st));
+        if (s->dp.agg_radius > 0) gf_stats(s->guide, dw, dh, (int)s->dp.agg_radius, s->tmp, s->mi, s->vi, st);
+        AggArgs ag{s->slices, n, dw, dh, (int)s->dp.agg_radius, s->dp.agg_eps, s->guide, s->mi, s->vi, s->state, 0, 0};
+        TRY(aggregate_peaks(ag, s->fp16, st, e->grid));
+        TRY(cudaEventRecord(ev[5], st));
+        const size_t cnt = (m + 6) / 7;
+        TRY(select_kth(s->state + 7 * m, cnt, 7, cnt / 2, e->hist, e->sel, e->scal + 0, st));
+        TRY(peak_finish(s->state, m, n, e->scal + 0, s->dp.gate, s->draw, s->conf, s->mins, st));
+        if (s->dp.median) TRY(median3(s->draw, s->dmed, dw, dh, st));
+        else TRY(cudaMemcpyAsync(s->dmed, s->draw, sizeof(float) * m, cudaMemcpyDeviceToDevice, st));
+        TRY(select_kth(s->conf, cnt, 7, std::min(cnt * 9 / 10, cnt - 1), e->hist, e->sel, e->scal + 1, st));
+        TRY(conf_scale(s->conf, m, e->scal + 1, st));
+        s->iters = s->iters_first = 0;
+        s->rel = 0.f;
+        s->rel64 = 0.0;
+        const float* dsol = s->dmed;
+        if (s->dp.lambda > 0.f) {
+            cudaError_t ce;
+            WlsSolver* ws = wls_create(s->guide, dw, dh, s->dp.lambda, s->dp.sigma_c, (int)s->dp.edge_mode, st, &ce);
+            if (ce != cudaSuccess) {
+                wls_destroy(ws);
+                return dup_err(fmt("wls: %s", cudaGetErrorString(ce)));
+            }
+            cudaError_t r1 = wls_set_weights(ws, s->conf, st);
+            float rel = 0.f;
+            int it = 0;
+            if (r1 == cudaSuccess) r1 = wls_solve(ws, s->dmed, (int)s->dp.cg_iters, s->u, &rel, &it, st, (int)s->dp.vcycle_mode, false, &s->rel64);
+            s->iters_first = it;
+            if (r1 == cudaSuccess && s->dp.robust > 0.f) {
+                r1 = robust_weights(s->conf, s->dmed, s->u, s->dp.robust, s->w2, m, st);
+                if (r1 == cudaSuccess) r1 = wls_set_weights(ws, s->w2, st);
+                if (r1 == cudaSuccess) r1 = wls_solve(ws, s->dmed, (int)s->dp.cg_iters, s->u, &rel, &it, st, (int)s->dp.vcycle_mode, false, &s->rel64);
+            }
+            wls_destroy(ws);
+            if (r1 != cudaSuccess) return dup_err(fmt("wls: %s", cudaGetErrorString(r1)));
+            s->rel = rel;
+            s->iters = it;
+            dsol = s->u;
+        }
+        TRY(cudaEventRecord(ev[6], st));
+        const float max_d = (float)(n - 1);
+        if (s->dp.upsample == 1) {
+            gf_stats(s->guide, dw, dh, (int)s->dp.up_radius, s->tmp, s->mi, s->vi, st);
+            gf_coeffs(s->guide, s->mi, s->vi, dsol, dw, dh, (int)s->dp.up_radius, s->dp.up_eps, s->t0, s->t1, s->t2, s->tmp, s->abar,
+                      s->bbar, st);
+            TRY(upsample(s->abar, s->bbar, s->yfull, s->guide, s->conf, W, H, dw, dh, k, max_d, true, s->dfull, s->cfull, st));
+        } else {
+            TRY(upsample(nullptr, dsol, s->yfull, s->guide, s->conf, W, H, dw, dh, k, max_d, false, s->dfull, s->cfull, st));
+        }
+    } else {
+        TRY(cudaEventRecord(ev[5], st));
+        TRY(cudaEventRecord(ev[6], st));
+    }
+    TRY(cudaEventRecord(ev[7], st));
+    TRY(cudaEventSynchronize(ev[7]));
+    int status = 0;
+    TRY(cudaMemcpy(&status, s->status, sizeof(int), cudaMemcpyDeviceToHost));
+    if (status) return dup_err(fmt("device status 0x%x (a kernel met a shape it was not built for)", status));
+    if (depth_on) {
+        float sc[2];
+        TRY(cudaMemcpy(sc, e->scal, sizeof sc, cudaMemcpyDeviceToHost));
+        s->floor_v = sc[0];
+        s->p90 = sc[1];
+    }
+    s->ms[0] = ms_between(ev[0], ev[1]);
+    s->ms[1] = ms_between(ev[1], ev[2]);
+    s->ms[2] = ms_between(ev[2], ev[3]);
+    s->ms[3] = ms_between(ev[3], ev[4]);
+    s->ms[4] = ms_between(ev[4], ev[5]);
+    s->ms[5] = ms_between(ev[5], ev[6]);
+    s->ms[6] = ms_between(ev[6], ev[7]);
+    s->ms[7] = ms_between(ev[0], ev[7]);
+    return nullptr;
+}
+
+extern "C" char* lsb_stack_run(lsb_stack* s, double* ms_out8) {
+    if (!s) return dup_err("null stack");
+    char* err = run_pipeline(s);
+    if (err) return err;
+    if (ms_out8) memcpy(ms_out8, s->ms, sizeof s->ms);
+    return nullptr;
+}
+
+// fuse.rs:315 from the device counts
+static char* shares_of(lsb_stack* s, float* out) {
+    const int dl = s->depth_level;
+    const int cells = s->lw[dl] * s->lh[dl];
+    TRY(winner_counts(s->winner, s->best[dl], cells, (int)s->count, s->counts, s->mx, s->e->s));
+    std::vector<unsigned> c(s->count);
+    TRY(cudaMemcpyAsync(c.data(), s->counts, sizeof(unsigned) * s->count, cudaMemcpyDeviceToHost, s->e->s));
+    TRY(cudaStreamSynchronize(s->e->s));
+    size_t total = 0;
+    for (unsigned v : c) total += v;
+    for (uint32_t k = 0; k < s->count; k++) out[k] = total > 0 ? (float)c[k] / (float)total : 0.0f;
+    return nullptr;
+}
+
+extern "C" char* lsb_stack_shares(lsb_stack* s, float* out_n) {
+    if (!s || !out_n) return dup_err("null argument");
+    if (!s->folded) {
+        char* err = run_pipeline(s);
+        if (err) return err;
+    }
+    return shares_of(s, out_n);
+}
+
+// align.rs:344 `common_area` (host, on the transforms found)
+static void common_area(const std::vector<double>& sims, int n, int w, int h, int interp, uint32_t rect[4]) {
+    rect[0] = 0;
+    rect[1] = 0;
+    rect[2] = w;
+    rect[3] = h;
+    std::vector<std::array<double, 9>> invs;
+    for (int k = 0; k < n; k++) {
+        if (sim_is_id(&sims[8 * (size_t)k])) continue;
+        double m[9];
+        std::array<double, 9> inv;
+        sim_matrix(&sims[8 * (size_t)k], w, h, m);
+        mat_inverse(m, inv.data());
+        invs.push_back(inv);
+    }
+    if (invs.empty()) return;
+    const double mg = (double)((interp == 0 ? 1 : interp == 1 ? 2 : interp <= 3 ? 4 : 6) / 2);
+    const double xmax = (double)(w - 1) - mg, ymax = (double)(h - 1) - mg;
+    std::vector<std::pair<long, long>> rows;
+    for (int y = 0; y < h; y++) {
+        double lo = 0.0, hi = (double)(w - 1), yf = (double)y;
+        for (auto& inv : invs) {
+            double g = inv[6], d = inv[7] * yf + inv[8];
+            if (d <= 0.0 || g * (double)(w - 1) + d <= 0.0) {
+                lo = 1.0;
+                hi = 0.0;
+                break;
+            }
+            double A[2] = {inv[0], inv[3]}, K[2] = {inv[1] * yf + inv[2], inv[4] * yf + inv[5]};
+            double smin[2] = {mg, mg}, smax[2] = {xmax, ymax};
+            for (int ax = 0; ax < 2; ax++) {
+                double a = A[ax], kk = K[ax];
+                double pq[2][2] = {{a - smin[ax] * g, kk - smin[ax] * d}, {smax[ax] * g - a, smax[ax] * d - kk}};
+                for (int t = 0; t < 2; t++) {
+                    double p = pq[t][0], q = pq[t][1];
+                    if (fabs(p) < 1e-12) {
+                        if (q < 0.0) {
+                            lo = 1.0;
+                            hi = 0.0;
+                        }
+                    } else if (p > 0.0) {
+                        lo = std::max(lo, -q / p);
+                    } else {
+                        hi = std::min(hi, -q / p);
+                    }
+                }
+            }
+        }
+        rows.push_back(lo <= hi ? std::make_pair((long)ceil(lo), (long)floor(hi)) : std::make_pair(1L, 0L));
+    }
+    size_t bx = 0, by = 0, bw = 0, bh = 0;
+    for (int y0 = 0; y0 < h; y0++) {
+        long lo = rows[y0].first, hi = rows[y0].second;
+        for (int y1 = y0; y1 < h; y1++) {
+            lo = std::max(lo, rows[y1].first);
+            hi = std::min(hi, rows[y1].second);
+            if (lo > hi) break;
+            size_t rw = (size_t)(hi - lo + 1), rh = (size_t)(y1 - y0 + 1);
+            if (rw * rh > bw * bh) {
+                bx = (size_t)lo;
+                by = (size_t)y0;
+                bw = rw;
+                bh = rh;
+            }
+        }
+    }
+    if (bw * bh > 0) {
+        rect[0] = (uint32_t)bx;
+        rect[1] = (uint32_t)by;
+        rect[2] = (uint32_t)bw;
+        rect[3] = (uint32_t)bh;
+    }
+}
+
+extern "C" char* lsb_stack_finish(lsb_stack* s, lsb_result* r) {
+    if (!s || !r) return dup_err("null argument");
+    memset(r, 0, sizeof *r);
+    char* err = run_pipeline(s);
+    if (err) return err;
+    const size_t W = s->w, H = s->h, N = s->count;
+    cudaStream_t st = s->e->s;
+    r->w = s->w;
+    r->h = s->h;
+    r->n_frames = s->count;
+    r->levels = s->levels;
+    r->image_u16 = (uint16_t*)malloc(sizeof(uint16_t) * 3 * W * H);
+    r->image_f32 = (float*)malloc(sizeof(float) * 3 * W * H);
+    r->winner = (float*)malloc(sizeof(float) * W * H);
+    r->sims = (double*)malloc(sizeof(double) * 8 * N);
+    r->gains = (float*)malloc(sizeof(float) * 3 * N);
+    r->shares = (float*)malloc(sizeof(float) * N);
+    TRY(cudaMemcpyAsync(r->image_u16, s->img_u16, sizeof(uint16_t) * 3 * W * H, cudaMemcpyDeviceToHost, st));
+    TRY(cudaMemcpyAsync(r->image_f32, s->img, sizeof(float) * 3 * W * H, cudaMemcpyDeviceToHost, st));
+    const int dl = s->depth_level, dwl = s->lw[dl], dhl = s->lh[dl];
+    std::vector<uint16_t> win((size_t)dwl * dhl);
+    TRY(cudaMemcpyAsync(win.data(), s->winner, sizeof(uint16_t) * win.size(), cudaMemcpyDeviceToHost, st));
+    if (s->dp.enabled) {
+        const size_t m = (size_t)s->dw * s->dh;
+        r->dw = s->dw;
+        r->dh = s->dh;
+        r->depth = (float*)malloc(sizeof(float) * W * H);
+        r->conf = (float*)malloc(sizeof(float) * W * H);
+        r->floor_cells = (float*)malloc(sizeof(float) * m);
+        TRY(cudaMemcpyAsync(r->depth, s->dfull, sizeof(float) * W * H, cudaMemcpyDeviceToHost, st));
+        TRY(cudaMemcpyAsync(r->conf, s->cfull, sizeof(float) * W * H, cudaMemcpyDeviceToHost, st));
+        TRY(cudaMemcpyAsync(r->floor_cells, s->mins, sizeof(float) * m, cudaMemcpyDeviceToHost, st));
+    }
+    TRY(cudaStreamSynchronize(st));
+    // fuse.rs:336 upsample_index
+    const size_t scale = (size_t)1 << dl;
+    for (size_t y = 0; y < H; y++) {
+        const size_t sy = std::min(y / scale, (size_t)dhl - 1);
+        for (size_t x = 0; x < W; x++) r->winner[y * W + x] = (float)win[sy * dwl + std::min(x / scale, (size_t)dwl - 1)];
+    }
+    memcpy(r->sims, s->sims.data(), sizeof(double) * 8 * N);
+    memcpy(r->gains, s->gains.data(), sizeof(float) * 3 * N);
+    err = shares_of(s, r->shares);
+    if (err) return err;
+    r->crop[0] = 0;
+    r->crop[1] = 0;
+    r->crop[2] = s->w;
+    r->crop[3] = s->h;
+    if (s->ap.enabled && N > 1 && s->crop) common_area(s->sims, (int)N, (int)W, (int)H, (int)s->ap.interp, r->crop);
+    r->floor_value = s->floor_v;
+    r->p90 = s->p90;
+    r->wls_rel = s->rel;
+    r->wls_rel64 = s->rel64;
+    r->wls_iters = s->iters;
+    r->wls_iters_first = s->iters_first;
+    r->align_evals = (uint32_t)s->align_evals;
+    memcpy(r->ms, s->ms, sizeof s->ms);
+    return nullptr;
+}
+
+extern "C" void lsb_stack_destroy(lsb_stack* s) {
+    if (!s) return;
+    cudaStreamSynchronize(s->e->s);
+    delete s;
+}
+
+extern "C" void lsb_result_free(lsb_result* r) {
+    if (!r) return;
+    free(r->image_u16);
+    free(r->image_f32);
+    free(r->winner);
+    free(r->depth);
+    free(r->conf);
+    free(r->floor_cells);
+    free(r->sims);
+    free(r->gains);
+    free(r->shares);
+    memset(r, 0, sizeof *r);
+}
+
+// ------------------------------------------------- standalone entry points
+extern "C" char* lsb_depth_from_slices(lsb_engine* e, const float* slices, uint32_t n, const float* fused, uint32_t w, uint32_t h,
+                                       const lsb_depth_params* p, lsb_result* out) {
+    if (!e || !slices || !fused || !p || !out) return dup_err("null argument");
+    // a stack with the fold skipped: its depth buffers, the fused image and the slices uploaded
+    lsb_fuse_params fp{1, 1, 2, 2, 256, 0, 0, 0.f};
+    lsb_depth_params dp = *p;
+    dp.enabled = 1;
+    lsb_stack* s = nullptr;
+    lsb_config saved = e->cfg;
+    e->cfg.fp16_storage = 0;
+    char* err = lsb_stack_begin(e, w, h, n, &fp, nullptr, &dp, 0, 0, &s);
+    e->cfg = saved;
+    if (err) return err;
+    cudaStream_t st = e->s;
+    const int k = s->bk, dw = s->dw, dh = s->dh;
+    const size_t m = (size_t)dw * dh;
+    memset(out, 0, sizeof *out);
+    auto fail = [&](char* m_) {
+        lsb_stack_destroy(s);
+        return m_;
+    };
+#define TRYS(x)                                                                                        \
+    do {                                                                                               \
+        cudaError_t _e = (x);                                                                          \
+        if (_e != cudaSuccess) return fail(dup_err(fmt("%s: %s", #x, cudaGetErrorString(_e))));       \
+    } while (0)
+    TRYS(cudaMemcpyAsync(s->img, fused, sizeof(float) * 3 * w * h, cudaMemcpyHostToDevice, st));
+    TRYS(cudaMemcpyAsync(s->slices, slices, sizeof(float) * n * m, cudaMemcpyHostToDevice, st));
+    TRYS(luma_and_guide(s->img, (int)w, (int)h, k, s->yfull, s->guide, dw, dh, st));
+    if (dp.agg_radius > 0) gf_stats(s->guide, dw, dh, (int)dp.agg_radius, s->tmp, s->mi, s->vi, st);
+    AggArgs ag{s->slices, (int)n, dw, dh, (int)dp.agg_radius, dp.agg_eps, s->guide, s->mi, s->vi, s->state, 0, 0};
+    TRYS(aggregate_peaks(ag, false, st, e->grid));
+    const size_t cnt = (m + 6) / 7;
+    TRYS(select_kth(s->state + 7 * m, cnt, 7, cnt / 2, e->hist, e->sel, e->scal + 0, st));
+    TRYS(peak_finish(s->state, m, (int)n, e->scal + 0, dp.gate, s->draw, s->conf, s->mins, st));
+    if (dp.median) TRYS(median3(s->draw, s->dmed, dw, dh, st));
+    else TRYS(cudaMemcpyAsync(s->dmed, s->draw, sizeof(float) * m, cudaMemcpyDeviceToDevice, st));
+    TRYS(select_kth(s->conf, cnt, 7, std::min(cnt * 9 / 10, cnt - 1), e->hist, e->sel, e->scal + 1, st));
+    TRYS(conf_scale(s->conf, m, e->scal + 1, st));
+    const float* dsol = s->dmed;
+    float rel = 0.f;
+    int it = 0, it1 = 0;
+    double rel64 = 0.0;
+    if (dp.lambda > 0.f) {
+        cudaError_t ce;
+        WlsSolver* ws = wls_create(s->guide, dw, dh, dp.lambda, dp.sigma_c, (int)dp.edge_mode, st, &ce);
+        if (ce == cudaSuccess) ce = wls_set_weights(ws, s->conf, st);
+        if (ce == cudaSuccess) ce = wls_solve(ws, s->dmed, (int)dp.cg_iters, s->u, &rel, &it, st, (int)dp.vcycle_mode, false, &rel64);
+        it1 = it;
+        if (ce == cudaSuccess && dp.robust > 0.f) {
+            ce = robust_weights(s->conf, s->dmed, s->u, dp.robust, s->w2, m, st);
+            if (ce == cudaSuccess) ce = wls_set_weights(ws, s->w2, st);
+            if (ce == cudaSuccess) ce = wls_solve(ws, s->dmed, (int)dp.cg_iters, s->u, &rel, &it, st, (int)dp.vcycle_mode, false, &rel64);
+        }
+        wls_destroy(ws);
+        if (ce != cudaSuccess) return fail(dup_err(fmt("wls: %s", cudaGetErrorString(ce))));
+        dsol = s->u;
+    }
+    const float max_d = (float)(n - 1);
+    if (dp.upsample == 1) {
+        gf_stats(s->guide, dw, dh, (int)dp.up_radius, s->tmp, s->mi, s->vi, st);
+        gf_coeffs(s->guide, s->mi, s->vi, dsol, dw, dh, (int)dp.up_radius, dp.up_eps, s->t0, s->t1, s->t2, s->tmp, s->abar, s->bbar, st);
+        TRYS(upsample(s->abar, s->bbar, s->yfull, s->guide, s->conf, (int)w, (int)h, dw, dh, k, max_d, true, s->dfull, s->cfull, st));
+    } else {
+        TRYS(upsample(nullptr, dsol, s->yfull, s->guide, s->conf, (int)w, (int)h, dw, dh, k, max_d, false, s->dfull, s->cfull, st));
+    }
+    out->w = w;
+    out->h = h;
+    out->n_frames = n;
+    out->dw = dw;
+    out->dh = dh;
+    out->depth = (float*)malloc(sizeof(float) * w * h);
+    out->conf = (float*)malloc(sizeof(float) * w * h);
+    out->floor_cells = (float*)malloc(sizeof(float) * m);
+    TRYS(cudaMemcpyAsync(out->depth, s->dfull, sizeof(float) * w * h, cudaMemcpyDeviceToHost, st));
+    TRYS(cudaMemcpyAsync(out->conf, s->cfull, sizeof(float) * w * h, cudaMemcpyDeviceToHost, st));
+    TRYS(cudaMemcpyAsync(out->floor_cells, s->mins, sizeof(float) * m, cudaMemcpyDeviceToHost, st));
+    float sc[2];
+    TRYS(cudaMemcpyAsync(sc, e->scal, sizeof sc, cudaMemcpyDeviceToHost, st));
+    TRYS(cudaStreamSynchronize(st));
+    out->floor_value = sc[0];
+    out->p90 = sc[1];
+    out->wls_rel = rel;
+    out->wls_rel64 = rel64;
+    out->wls_iters = it;
+    out->wls_iters_first = it1;
+    lsb_stack_destroy(s);
+    return nullptr;
+#undef TRYS
+}
+
+extern "C" char* lsb_wls_solve(lsb_engine* e, const float* d, const float* conf, const float* guide, uint32_t w, uint32_t h,
+                               float lambda, float sigma_c, uint32_t max_iters, uint32_t edge_mode, uint32_t vcycle_mode, float* u,
+                               float* rel, uint32_t* iters, double* ms) {
+    if (!e || !d || !conf || !guide || !u) return dup_err("null argument");
+    cudaStream_t st = e->s;
+    const size_t m = (size_t)w * h;
+    DevPool P;
+    float *dd, *cc, *gg, *uu;
+    TRY(P.get(&dd, m));
+    TRY(P.get(&cc, m));
+    TRY(P.get(&gg, m));
+    TRY(P.get(&uu, m));
+    TRY(cudaMemcpyAsync(dd, d, sizeof(float) * m, cudaMemcpyHostToDevice, st));
+    TRY(cudaMemcpyAsync(cc, conf, sizeof(float) * m, cudaMemcpyHostToDevice, st));
+    TRY(cudaMemcpyAsync(gg, guide, sizeof(float) * m, cudaMemcpyHostToDevice, st));
+    TRY(cudaMemsetAsync(uu, 0, sizeof(float) * m, st));
+    TRY(cudaEventRecord(e->ev[0], st));
+    cudaError_t ce;
+    WlsSolver* ws = wls_create(gg, (int)w, (int)h, lambda, sigma_c, (int)edge_mode, st, &ce);
+    if (ce == cudaSuccess) ce = wls_set_weights(ws, cc, st);
+    float r = 0.f;
+    int it = 0;
+    if (ce == cudaSuccess) ce = wls_solve(ws, dd, (int)max_iters, uu, &r, &it, st, (int)vcycle_mode, false, nullptr);
+    TRY(cudaEventRecord(e->ev[1], st));
+    wls_destroy(ws);
+    if (ce != cudaSuccess) return dup_err(fmt("wls: %s", cudaGetErrorString(ce)));
+    TRY(cudaMemcpyAsync(u, uu, sizeof(float) * m, cudaMemcpyDeviceToHost, st));
+    TRY(cudaStreamSynchronize(st));
+    if (rel) *rel = r;
+    if (iters) *iters = (uint32_t)it;
+    if (ms) *ms = ms_between(e->ev[0], e->ev[1]);
+    return nullptr;
+}
+
+extern "C" char* lsb_align_pair(lsb_engine* e, const float* rf, const float* tg, uint32_t w, uint32_t h, const double* init8,
+                                const uint8_t* free8, uint32_t coarsen, double* out8, uint32_t* evals) {
+    if (!e || !rf || !tg || !out8) return dup_err("null argument");
+    cudaStream_t st = e->s;
+    DevPool P;
+    float *a, *b;
+    TRY(P.get(&a, (size_t)w * h));
+    TRY(P.get(&b, (size_t)w * h));
+    TRY(cudaMemcpyAsync(a, rf, sizeof(float) * w * h, cudaMemcpyHostToDevice, st));
+    TRY(cudaMemcpyAsync(b, tg, sizeof(float) * w * h, cudaMemcpyHostToDevice, st));
+    std::vector<std::pair<int, int>> dims;
+    gauss_dims((int)w, (int)h, dims);
+    std::vector<float*> pr, pt;
+    for (auto& dd : dims) {
+        float *x, *y;
+        TRY(P.get(&x, (size_t)dd.first * dd.second));
+        TRY(P.get(&y, (size_t)dd.first * dd.second));
+        pr.push_back(x);
+        pt.push_back(y);
+    }
+    TRY(gauss_levels(a, (int)w, (int)h, pr, st));
+    TRY(gauss_levels(b, (int)w, (int)h, pt, st));
+    const double id[8] = {0, 0, 1, 0, 1, 0, 0, 0};
+    bool fr[8];
+    for (int k = 0; k < 8; k++) fr[k] = free8 ? free8[k] != 0 : (k < 4);
+    e->actx.evals = 0;
+    TRY(multiscale_align(e->actx, a, pr, b, pt, (int)w, (int)h, init8 ? init8 : id, fr, (int)coarsen, out8));
+    if (evals) *evals = (uint32_t)e->actx.evals;
+    return nullptr;
+}
+
+extern "C" char* lsb_warp_cost(lsb_engine* e, const float* rf, uint32_t aw, uint32_t ah, const float* tgt, uint32_t tw, uint32_t th,
+                               const double* sim8, double* cost) {
+    if (!e || !rf || !tgt || !sim8 || !cost) return dup_err("null argument");
+    cudaStream_t st = e->s;
+    DevPool P;
+    float *a, *b;
+    TRY(P.get(&a, (size_t)aw * ah));
+    TRY(P.get(&b, (size_t)tw * th));
+    TRY(cudaMemcpyAsync(a, rf, sizeof(float) * aw * ah, cudaMemcpyHostToDevice, st));
+    TRY(cudaMemcpyAsync(b, tgt, sizeof(float) * tw * th, cudaMemcpyHostToDevice, st));
+    TRY(cost_single(e->actx, a, (int)aw, (int)ah, b, (int)tw, (int)th, sim8, cost));
+    return nullptr;
+}

@@ -1,0 +1,69 @@
+// Shared device helpers of the lapstack-b200 engine (sm_100a).
+//
+// Arithmetic that must be bit-identical to the reference's FP32 CPU path
+// (crates/lapstack-core/src/pyramid.rs, fuse.rs) is written with explicit
+// __fmul_rn / __fadd_rn / __fsub_rn so that no a*b+c is contracted into an
+// FMA whatever the compiler flags: the reference's rustc build never fuses.
+#pragma once
+#include <cuda_fp16.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#define LSB_HD __host__ __device__ __forceinline__
+
+// Reflect-101 into [0, n) (pyramid.rs:51 `reflect`): period 2(n-1); n == 1 maps to 0.
+LSB_HD int lsb_reflect(int i, int n) {
+    if (n == 1) return 0;
+    if (i >= 0 && i < n) return i;
+    int p = 2 * (n - 1);
+    i %= p;
+    if (i < 0) i += p;
+    return i < n ? i : p - i;
+}
+
+// BT.601 luma with the reference's f32 literals and left-to-right order
+// (fuse.rs:160, depth.rs:163, align.rs:567).
+__device__ __forceinline__ float lsb_luma(float r, float g, float b) {
+    return __fadd_rn(__fadd_rn(__fmul_rn(0.299f, r), __fmul_rn(0.587f, g)), __fmul_rn(0.114f, b));
+}
+
+// u16 -> [0,1] as v * (1/65535) in f32 (io.rs:89-94).
+#define LSB_INV16 (1.0f / 65535.0f)
+
+// pyramid.rs:46 KERNEL and pyramid.rs:124-125 EVEN / ODD.
+#define LSB_K0 (1.0f / 16.0f)
+#define LSB_K1 (4.0f / 16.0f)
+#define LSB_K2 (6.0f / 16.0f)
+#define LSB_E0 (2.0f * LSB_K0)
+#define LSB_E1 (2.0f * LSB_K2)
+#define LSB_OD (2.0f * LSB_K1)
+
+// a5 = ((((k0*s0 + k1*s1) + k2*s2) + k1*s3) + k0*s4), the order of pyramid.rs:95/111.
+__device__ __forceinline__ float lsb_tap5(float s0, float s1, float s2, float s3, float s4) {
+    float a = __fmul_rn(LSB_K0, s0);
+    a = __fadd_rn(a, __fmul_rn(LSB_K1, s1));
+    a = __fadd_rn(a, __fmul_rn(LSB_K2, s2));
+    a = __fadd_rn(a, __fmul_rn(LSB_K1, s3));
+    return __fadd_rn(a, __fmul_rn(LSB_K0, s4));
+}
+// EXPAND taps (pyramid.rs:128-166): even = E0*a + E1*b + E0*c, odd = OD*(a + b).
+__device__ __forceinline__ float lsb_exp_even(float a, float b, float c) {
+    return __fadd_rn(__fadd_rn(__fmul_rn(LSB_E0, a), __fmul_rn(LSB_E1, b)), __fmul_rn(LSB_E0, c));
+}
+__device__ __forceinline__ float lsb_exp_odd(float a, float b) { return __fmul_rn(LSB_OD, __fadd_rn(a, b)); }
+
+template <class S>
+__device__ __forceinline__ float lsb_ld(const S* p);
+template <>
+__device__ __forceinline__ float lsb_ld<float>(const float* p) { return *p; }
+template <>
+__device__ __forceinline__ float lsb_ld<__half>(const __half* p) { return __half2float(*p); }
+template <class S>
+__device__ __forceinline__ void lsb_st(S* p, float v);
+template <>
+__device__ __forceinline__ void lsb_st<float>(float* p, float v) { *p = v; }
+template <>
+__device__ __forceinline__ void lsb_st<__half>(__half* p, float v) { *p = __float2half_rn(v); }
+
+// Error flag bits a kernel may raise in the engine's device status word.
+enum { LSB_ERR_BOUNDS = 1, LSB_ERR_TIMEOUT = 2, LSB_ERR_SHAPE = 4 };

@@ -1,0 +1,519 @@
+// The depth-from-focus pass (crates/lapstack-core/src/depth.rs:1119
+// `depth_from_slices`) on the device.
+//
+// * The guided-filter aggregation of every slice (depth.rs:352 GuidedFilter,
+//   r = agg_radius) and the streamed peak tracker (depth.rs:533 PeakTracker)
+//   run as ONE persistent kernel: a CTA owns a tile of the working grid, keeps
+//   the guide's statistics for it in shared memory, walks the N slices in
+//   order and keeps every cell's profile state in registers, so a slice is read
+//   from HBM once (plus its halo) and the tracker state never round-trips.
+// * Box sums follow depth.rs:285 `BoxFilter::sum_into`: border-clipped, f64
+//   sums rounded to f32 after the horizontal and after the vertical pass; the
+//   window sums are formed directly in f64 (equal to the reference's f64
+//   running sums whenever those are exact, which they are unless a window
+//   spans more than 2^29 in magnitude).
+// * The two medians of a subsample (noise floor depth.rs:578, p90
+//   depth.rs:616) are exact k-th-value selections on the device (two 16-bit
+//   radix passes over the total-order key of each float).
+#include <algorithm>
+
+#include "lsb_common.cuh"
+#include "lsb_depth.h"
+
+namespace lsb {
+
+// ------------------------------------------------------------------ helpers
+__global__ void luma_kernel(const float* __restrict__ img, float* __restrict__ y, size_t n) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        y[i] = lsb_luma(img[i], img[n + i], img[2 * n + i]);
+}
+
+// depth.rs:174 `block_mean`: per row of the block the row sum, added in order, then / count.
+__global__ void block_mean_kernel(const float* __restrict__ src, int w, int h, int k, float* __restrict__ out, int dw, int dh) {
+    const int ox = blockIdx.x * blockDim.x + threadIdx.x, oy = blockIdx.y * blockDim.y + threadIdx.y;
+    if (ox >= dw || oy >= dh) return;
+    const int x0 = ox * k, x1 = min(x0 + k, w), y0 = oy * k, y1 = min(y0 + k, h);
+    float o = 0.f;
+    for (int y = y0; y < y1; y++) {
+        float rs = 0.f;
+        for (int x = x0; x < x1; x++) rs = __fadd_rn(rs, src[(size_t)y * w + x]);
+        o = __fadd_rn(o, rs);
+    }
+    out[(size_t)oy * dw + ox] = __fdiv_rn(o, (float)((y1 - y0) * (x1 - x0)));
+}
+
+__device__ __forceinline__ float box_inv_count(int x, int y, int w, int h, int r) {
+    const float cy = (float)(min(y + r + 1, h) - max(y - r, 0));
+    const float cx = (float)(min(x + r + 1, w) - max(x - r, 0));
+    return __fdiv_rn(1.f, __fmul_rn(cy, cx));
+}
+
+// Horizontal box sums (optionally of a*b), f64 window sum rounded to f32.
+__global__ void box_h_kernel(const float* __restrict__ a, const float* __restrict__ b, float* __restrict__ out, int w, int h, int r) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
+    if (x >= w || y >= h) return;
+    const float* ra = a + (size_t)y * w;
+    const float* rb = b ? b + (size_t)y * w : nullptr;
+    double s = 0.0;
+    for (int t = max(x - r, 0); t <= min(x + r, w - 1); t++) s += rb ? (double)__fmul_rn(ra[t], rb[t]) : (double)ra[t];
+    out[(size_t)y * w + x] = (float)s;
+}
+// Vertical box sums of the horizontal sums, rounded to f32, times the inverse count.
+__global__ void box_v_kernel(const float* __restrict__ hs, float* __restrict__ out, int w, int h, int r) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
+    if (x >= w || y >= h) return;
+    double s = 0.0;
+    for (int t = max(y - r, 0); t <= min(y + r, h - 1); t++) s += (double)hs[(size_t)t * w + x];
+    out[(size_t)y * w + x] = __fmul_rn((float)s, box_inv_count(x, y, w, h, r));
+}
+
+static void box_mean(const float* a, const float* b, float* tmp, float* out, int w, int h, int r, cudaStream_t s) {
+    dim3 blk(128), g((w + 127) / 128, h);
+    box_h_kernel<<<g, blk, 0, s>>>(a, b, tmp, w, h, r);
+    box_v_kernel<<<g, blk, 0, s>>>(tmp, out, w, h, r);
+}
+
+// depth.rs:363 GuidedFilter::new: var_i = max(mean(I*I) - mean_i^2, 0)
+__global__ void gf_var_kernel(const float* __restrict__ mean_i, float* __restrict__ var_i, size_t n) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        var_i[i] = fmaxf(__fsub_rn(var_i[i], __fmul_rn(mean_i[i], mean_i[i])), 0.f);
+}
+// depth.rs:385: a = (corr - mean_i * mean_p) / (var_i + eps), b = mean_p - a * mean_i
+__global__ void gf_ab_kernel(const float* __restrict__ mp, const float* __restrict__ corr, const float* __restrict__ mi,
+                             const float* __restrict__ vi, float eps, float* __restrict__ a, float* __restrict__ b, size_t n) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        const float av = __fdiv_rn(__fsub_rn(corr[i], __fmul_rn(mi[i], mp[i])), __fadd_rn(vi[i], eps));
+        a[i] = av;
+        b[i] = __fsub_rn(mp[i], __fmul_rn(av, mi[i]));
+    }
+}
+
+static int grid1(size_t n) { return (int)std::min<size_t>((n + 255) / 256, 148 * 16); }
+
+void gf_stats(const float* guide, int w, int h, int r, float* tmp, float* mean_i, float* var_i, cudaStream_t s) {
+    box_mean(guide, nullptr, tmp, mean_i, w, h, r, s);
+    box_mean(guide, guide, tmp, var_i, w, h, r, s);
+    gf_var_kernel<<<grid1((size_t)w * h), 256, 0, s>>>(mean_i, var_i, (size_t)w * h);
+}
+
+// depth.rs:379 `coeffs_into` for one plane p: a-bar into abar, b-bar into bbar.
+void gf_coeffs(const float* guide, const float* mean_i, const float* var_i, const float* p, int w, int h, int r, float eps,
+               float* t0, float* t1, float* t2, float* tmp, float* abar, float* bbar, cudaStream_t s) {
+    size_t n = (size_t)w * h;
+    box_mean(p, nullptr, tmp, t0, w, h, r, s);    // mean_p
+    box_mean(guide, p, tmp, t1, w, h, r, s);      // corr_Ip (I*p formed inside)
+    gf_ab_kernel<<<grid1(n), 256, 0, s>>>(t0, t1, mean_i, var_i, eps, t2, t1, n);  // a -> t2, b -> t1
+    box_mean(t2, nullptr, tmp, abar, w, h, r, s);
+    box_mean(t1, nullptr, tmp, bbar, w, h, r, s);
+}
+
+// --------------------------------------------- fused aggregation + peaks
+struct PeakState {
+    float c1, l1, r1, c2, prev, prev2, sum, cmin;
+    int i1;
+};
+__device__ __forceinline__ void peak_reg(PeakState& p, float val, int idx, float l, float r) {
+    if (val > p.c1) {
+        if (p.c1 >= 0.f) p.c2 = p.c1;
+        p.c1 = val;
+        p.i1 = idx;
+        p.l1 = l;
+        p.r1 = r;
+    } else if (val > p.c2) {
+        p.c2 = val;
+    }
+}
+// depth.rs:547 `push` of slice m
+__device__ __forceinline__ void peak_push(PeakState& p, float v, int m) {
+    if (m >= 1) {
+        const bool is_peak = (m == 1 || p.prev >= p.prev2) && p.prev > v;
+        if (is_peak) peak_reg(p, p.prev, m - 1, m >= 2 ? p.prev2 : -1.f, v);
+    }
+    p.sum = __fadd_rn(p.sum, v);
+    p.cmin = fminf(p.cmin, v);
+    p.prev2 = p.prev;
+    p.prev = v;
+}
+
+template <int TWD, int THD, class SS>
+__global__ void __launch_bounds__(256, 2) aggregate_kernel(const AggArgs a) {
+    constexpr int CPT = TWD * THD / 256;
+    extern __shared__ float sm[];
+    const int R = a.r, w = a.dw, h = a.dh, tid = threadIdx.x;
+    const int PW = TWD + 4 * R, PH = THD + 4 * R, QW = TWD + 2 * R, QH = THD + 2 * R;
+    float* P = sm;                 // [PH][PW] slice over tile +- 2R
+    float* I = P + PW * PH;        // [PH][PW] guide
+    float* MI = I + PW * PH;       // [QH][QW] mean_i
+    float* VI = MI + QW * QH;      // [QH][QW] var_i
+    float* HP = VI + QW * QH;      // [PH][QW] horizontal sums of p, then of a
+    float* HQ = HP + PH * QW;      // [PH][QW] horizontal sums of I*p, then of b
+    float* A = HQ + PH * QW;       // [QH][QW]
+    float* B = A + QW * QH;        // [QH][QW]
+    for (int tile = blockIdx.x; tile < a.ntiles; tile += gridDim.x) {
+        const int x0 = (tile % a.tiles_x) * TWD, y0 = (tile / a.tiles_x) * THD;
+        const int px0 = x0 - 2 * R, py0 = y0 - 2 * R, qx0 = x0 - R, qy0 = y0 - R;
+        for (int i = tid; i < PW * PH; i += 256) {
+            const int x = px0 + i % PW, y = py0 + i / PW;
+            I[i] = (x >= 0 && x < w && y >= 0 && y < h) ? a.guide[(size_t)y * w + x] : 0.f;
+        }
+        for (int i = tid; i < QW * QH; i += 256) {
+            const int x = qx0 + i % QW, y = qy0 + i / QW;
+            const bool in = x >= 0 && x < w && y >= 0 && y < h;
+            MI[i] = in ? a.mean_i[(size_t)y * w + x] : 0.f;
+            VI[i] = in ? a.var_i[(size_t)y * w + x] : 0.f;
+        }
+        PeakState st[CPT];
+#pragma unroll
+        for (int j = 0; j < CPT; j++) st[j] = PeakState{-1.f, -1.f, -1.f, -1.f, 0.f, 0.f, 0.f, __int_as_float(0x7f800000), 0};
+        for (int m = 0; m < a.n; m++) {
+            const SS* sl = (const SS*)a.slices + (size_t)m * w * h;
+            __syncthreads();
+            for (int i = tid; i < PW * PH; i += 256) {
+                const int x = px0 + i % PW, y = py0 + i / PW;
+                P[i] = (x >= 0 && x < w && y >= 0 && y < h) ? lsb_ld<SS>(sl + (size_t)y * w + x) : 0.f;
+            }
+            __syncthreads();
+            // horizontal sums of p and I*p over rows of tile +- 2R, columns of tile +- R
+            for (int i = tid; i < PH * QW; i += 256) {
+                const int r = i / QW, c = i % QW, x = qx0 + c;
+                double sp = 0.0, sq = 0.0;
+                const int lo = max(x - R, 0) - px0, hi = min(x + R, w - 1) - px0;
+                for (int t = lo; t <= hi; t++) {
+                    const float pv = P[r * PW + t];
+                    sp += (double)pv;
+                    sq += (double)__fmul_rn(I[r * PW + t], pv);
+                }
+                HP[i] = (float)sp;
+                HQ[i] = (float)sq;
+            }
+            __syncthreads();
+            // vertical: mean_p, corr_Ip -> a, b over tile +- R
+            for (int i = tid; i < QW * QH; i += 256) {
+                const int r = i / QW, c = i % QW, x = qx0 + c, y = qy0 + r;
+                if (x < 0 || x >= w || y < 0 || y >= h) {
+                    A[i] = 0.f;
+                    B[i] = 0.f;
+                    continue;
+                }
+                double sp = 0.0, sq = 0.0;
+                const int lo = max(y - R, 0) - py0, hi = min(y + R, h - 1) - py0;
+                for (int t = lo; t <= hi; t++) {
+                    sp += (double)HP[t * QW + c];
+                    sq += (double)HQ[t * QW + c];
+                }
+                const float ic = box_inv_count(x, y, w, h, R);
+                const float mp = __fmul_rn((float)sp, ic), corr = __fmul_rn((float)sq, ic);
+                const float av = __fdiv_rn(__fsub_rn(corr, __fmul_rn(MI[i], mp)), __fadd_rn(VI[i], a.eps));
+                A[i] = av;
+                B[i] = __fsub_rn(mp, __fmul_rn(av, MI[i]));
+            }
+            __syncthreads();
+            // horizontal sums of a and b over rows of tile +- R, the tile's columns
+            for (int i = tid; i < QH * TWD; i += 256) {
+                const int r = i / TWD, c = i % TWD, x = x0 + c;
+                if (x >= w) continue;
+                double sa = 0.0, sb = 0.0;
+                const int lo = max(x - R, 0) - qx0, hi = min(x + R, w - 1) - qx0;
+                for (int t = lo; t <= hi; t++) {
+                    sa += (double)A[r * QW + t];
+                    sb += (double)B[r * QW + t];
+                }
+                HP[i] = (float)sa;
+                HQ[i] = (float)sb;
+            }
+            __syncthreads();
+#pragma unroll
+            for (int j = 0; j < CPT; j++) {
+                const int p = tid + 256 * j, c = p % TWD, r = p / TWD, x = x0 + c, y = y0 + r;
+                if (x >= w || y >= h) continue;
+                double sa = 0.0, sb = 0.0;
+                const int lo = max(y - R, 0) - qy0, hi = min(y + R, h - 1) - qy0;
+                for (int t = lo; t <= hi; t++) {
+                    sa += (double)HP[t * TWD + c];
+                    sb += (double)HQ[t * TWD + c];
+                }
+                const float ic = box_inv_count(x, y, w, h, R);
+                const float abar = __fmul_rn((float)sa, ic), bbar = __fmul_rn((float)sb, ic);
+                // depth.rs:404 q = a-bar * I + b-bar, then depth.rs:1146 max(q, 0)
+                const float q = fmaxf(__fadd_rn(__fmul_rn(abar, I[(r + 2 * R) * PW + c + 2 * R]), bbar), 0.f);
+                peak_push(st[j], q, m);
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < CPT; j++) {
+            const int p = tid + 256 * j, c = p % TWD, r = p / TWD, x = x0 + c, y = y0 + r;
+            if (x >= w || y >= h) continue;
+            const size_t o = (size_t)y * w + x, m = (size_t)w * h;
+            float* S = a.state;
+            S[o] = st[j].c1;
+            S[m + o] = st[j].l1;
+            S[2 * m + o] = st[j].r1;
+            S[3 * m + o] = st[j].c2;
+            S[4 * m + o] = st[j].prev;
+            S[5 * m + o] = st[j].prev2;
+            S[6 * m + o] = st[j].sum;
+            S[7 * m + o] = st[j].cmin;
+            S[8 * m + o] = __int_as_float(st[j].i1);
+        }
+        __syncthreads();
+    }
+}
+
+// Without aggregation (agg_radius 0) the slices go to the tracker as they are.
+template <class SS>
+__global__ void peaks_raw_kernel(const SS* __restrict__ slices, int n, size_t m, float* __restrict__ S) {
+    for (size_t o = blockIdx.x * (size_t)blockDim.x + threadIdx.x; o < m; o += (size_t)gridDim.x * blockDim.x) {
+        PeakState st{-1.f, -1.f, -1.f, -1.f, 0.f, 0.f, 0.f, __int_as_float(0x7f800000), 0};
+        for (int k = 0; k < n; k++) peak_push(st, lsb_ld<SS>(slices + (size_t)k * m + o), k);
+        S[o] = st.c1;
+        S[m + o] = st.l1;
+        S[2 * m + o] = st.r1;
+        S[3 * m + o] = st.c2;
+        S[4 * m + o] = st.prev;
+        S[5 * m + o] = st.prev2;
+        S[6 * m + o] = st.sum;
+        S[7 * m + o] = st.cmin;
+        S[8 * m + o] = __int_as_float(st.i1);
+    }
+}
+
+size_t aggregate_smem_bytes(int r) {
+    const int TWD = r <= 4 ? 64 : 32, THD = 32;
+    const int PW = TWD + 4 * r, PH = THD + 4 * r, QW = TWD + 2 * r, QH = THD + 2 * r;
+    return sizeof(float) * (size_t)(2 * PW * PH + 4 * QW * QH + 2 * PH * QW);
+}
+
+cudaError_t aggregate_peaks(AggArgs a, bool slice_fp16, cudaStream_t s, int grid_limit) {
+    size_t m = (size_t)a.dw * a.dh;
+    if (a.r == 0) {
+        if (slice_fp16) peaks_raw_kernel<__half><<<grid1(m), 256, 0, s>>>((const __half*)a.slices, a.n, m, a.state);
+        else peaks_raw_kernel<float><<<grid1(m), 256, 0, s>>>((const float*)a.slices, a.n, m, a.state);
+        return cudaGetLastError();
+    }
+    const int TWD = a.r <= 4 ? 64 : 32, THD = 32;
+    a.tiles_x = (a.dw + TWD - 1) / TWD;
+    a.ntiles = a.tiles_x * ((a.dh + THD - 1) / THD);
+    size_t smem = aggregate_smem_bytes(a.r);
+    if (smem > 227 * 1024) return cudaErrorInvalidValue;
+    int grid = std::min(a.ntiles, std::max(1, grid_limit));
+    cudaError_t e;
+#define LAUNCH_AGG(TWV, SST)                                                                               \
+    {                                                                                                      \
+        auto k = aggregate_kernel<TWV, 32, SST>;                                                           \
+        e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);               \
+        if (e != cudaSuccess) return e;                                                                    \
+        k<<<grid, 256, smem, s>>>(a);                                                                      \
+    }
+    if (TWD == 64) {
+        if (slice_fp16) LAUNCH_AGG(64, __half) else LAUNCH_AGG(64, float)
+    } else {
+        if (slice_fp16) LAUNCH_AGG(32, __half) else LAUNCH_AGG(32, float)
+    }
+#undef LAUNCH_AGG
+    return cudaGetLastError();
+}
+
+// ------------------------------------------------------------- k-th value
+// The key of a float in the total order (total_cmp): monotone as u32.
+__device__ __forceinline__ unsigned fkey(float f) {
+    unsigned b = __float_as_uint(f);
+    return (b & 0x80000000u) ? ~b : (b | 0x80000000u);
+}
+__device__ __forceinline__ float fkey_inv(unsigned k) {
+    return __uint_as_float((k & 0x80000000u) ? (k & 0x7fffffffu) : ~k);
+}
+__global__ void hist_kernel(const float* __restrict__ v, size_t cnt, int stride, unsigned* hist, const unsigned* sel, int pass) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < cnt; i += (size_t)gridDim.x * blockDim.x) {
+        const unsigned k = fkey(v[i * stride]);
+        if (pass == 0) atomicAdd(&hist[k >> 16], 1u);
+        else if ((k >> 16) == sel[0]) atomicAdd(&hist[k & 0xffffu], 1u);
+    }
+}
+// One block: find the bin holding rank sel[1] (pass 0) / sel[2] (pass 1).
+__global__ void scan_kernel(const unsigned* hist, unsigned* sel, int pass, float* out) {
+    __shared__ unsigned part[1024];
+    const int t = threadIdx.x;
+    unsigned s = 0;
+    for (int b = t * 64; b < t * 64 + 64; b++) s += hist[b];
+    part[t] = s;
+    __syncthreads();
+    if (t == 0) {
+        unsigned want = pass == 0 ? sel[1] : sel[2], acc = 0;
+        int chunk = 0;
+        while (chunk < 1023 && acc + part[chunk] <= want) acc += part[chunk++];
+        int b = chunk * 64;
+        while (b < chunk * 64 + 63 && acc + hist[b] <= want) acc += hist[b++];
+        if (pass == 0) {
+            sel[0] = (unsigned)b;
+            sel[2] = want - acc;
+        } else {
+            *out = fkey_inv((sel[0] << 16) | (unsigned)b);
+        }
+    }
+}
+__global__ void set_rank_kernel(unsigned* sel, unsigned rank) { sel[1] = rank; }
+
+cudaError_t select_kth(const float* v, size_t cnt, int stride, size_t rank, unsigned* hist, unsigned* sel, float* out,
+                       cudaStream_t s) {
+    cudaMemsetAsync(hist, 0, sizeof(unsigned) * 65536, s);
+    set_rank_kernel<<<1, 1, 0, s>>>(sel, (unsigned)rank);
+    hist_kernel<<<grid1(cnt), 256, 0, s>>>(v, cnt, stride, hist, sel, 0);
+    scan_kernel<<<1, 1024, 0, s>>>(hist, sel, 0, out);
+    cudaMemsetAsync(hist, 0, sizeof(unsigned) * 65536, s);
+    hist_kernel<<<grid1(cnt), 256, 0, s>>>(v, cnt, stride, hist, sel, 1);
+    scan_kernel<<<1, 1024, 0, s>>>(hist, sel, 1, out);
+    return cudaGetLastError();
+}
+
+// ------------------------------------------------------------ peak finish
+// depth.rs:568 `finish`: the last slice's peak, the log-parabola offset, the
+// confidence (prominence x peak ratio x noise gate) and the profile minimum.
+__global__ void peak_finish_kernel(const float* __restrict__ S, size_t m, int n, const float* __restrict__ floor_p, float gate,
+                                   float* __restrict__ depth, float* __restrict__ conf, float* __restrict__ mins) {
+    const float fl = *floor_p;
+    const float inv_n = __fdiv_rn(1.f, (float)n);
+    for (size_t o = blockIdx.x * (size_t)blockDim.x + threadIdx.x; o < m; o += (size_t)gridDim.x * blockDim.x) {
+        PeakState p{S[o], S[m + o], S[2 * m + o], S[3 * m + o], S[4 * m + o], S[5 * m + o], S[6 * m + o], S[7 * m + o],
+                    __float_as_int(S[8 * m + o])};
+        if (n == 1 || p.prev >= p.prev2) peak_reg(p, p.prev, n - 1, n >= 2 ? p.prev2 : -1.f, -1.f);
+        const float c1 = p.c1, l = p.l1, r = p.r1;
+        float delta = 0.f;
+        if (l >= 0.f && r >= 0.f && c1 > 0.f) {
+            const float ll = logf(fmaxf(l, 1e-12f)), lc = logf(c1), lr = logf(fmaxf(r, 1e-12f));
+            const float den = __fadd_rn(__fsub_rn(ll, __fmul_rn(2.f, lc)), lr);
+            if (den < 0.f) delta = fminf(fmaxf(__fdiv_rn(__fmul_rn(0.5f, __fsub_rn(ll, lr)), den), -0.5f), 0.5f);
+        }
+        depth[o] = __fadd_rn((float)p.i1, delta);
+        float c = 0.f;
+        if (c1 > 0.f) {
+            const float mean = __fmul_rn(p.sum, inv_n);
+            const float prom = fminf(fmaxf(__fsub_rn(1.f, __fdiv_rn(mean, c1)), 0.f), 1.f);
+            const float pkr = p.c2 >= 0.f ? fminf(fmaxf(__fsub_rn(1.f, __fdiv_rn(p.c2, c1)), 0.f), 1.f) : 1.f;
+            const float g = (gate > 0.f && fl > 0.f) ? fminf(fmaxf(__fdiv_rn(__fsub_rn(c1, fl), __fmul_rn(gate, fl)), 0.f), 1.f) : 1.f;
+            c = __fmul_rn(__fmul_rn(prom, pkr), g);
+        }
+        conf[o] = c;
+        mins[o] = isfinite(p.cmin) ? p.cmin : 0.f;
+    }
+}
+cudaError_t peak_finish(const float* state, size_t m, int n, const float* floor_p, float gate, float* depth, float* conf,
+                        float* mins, cudaStream_t s) {
+    peak_finish_kernel<<<grid1(m), 256, 0, s>>>(state, m, n, floor_p, gate, depth, conf, mins);
+    return cudaGetLastError();
+}
+
+// depth.rs:628 `median3`: 3x3 median, reflect-101.
+__device__ __forceinline__ void cswap(float& a, float& b) {
+    const float lo = fminf(a, b), hi = fmaxf(a, b);
+    a = lo;
+    b = hi;
+}
+__global__ void median3_kernel(const float* __restrict__ src, float* __restrict__ out, int w, int h) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
+    if (x >= w || y >= h) return;
+    float v[9];
+    int k = 0;
+    for (int dy = -1; dy <= 1; dy++) {
+        const float* row = src + (size_t)lsb_reflect(y + dy, h) * w;
+        for (int dx = -1; dx <= 1; dx++) v[k++] = row[lsb_reflect(x + dx, w)];
+    }
+    // a sorting network, then the middle element
+    for (int i = 0; i < 9; i++)
+        for (int j = 0; j < 8 - i; j++) cswap(v[j], v[j + 1]);
+    out[(size_t)y * w + x] = v[4];
+}
+cudaError_t median3(const float* src, float* out, int w, int h, cudaStream_t s) {
+    dim3 b(32, 8), g((w + 31) / 32, (h + 7) / 8);
+    median3_kernel<<<g, b, 0, s>>>(src, out, w, h);
+    return cudaGetLastError();
+}
+
+// depth.rs:615 `normalize_conf`: c = min(c / p90, 1) when p90 > 1e-6
+__global__ void conf_scale_kernel(float* conf, size_t m, const float* p90) {
+    const float p = *p90;
+    if (!(p > 1e-6f)) return;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < m; i += (size_t)gridDim.x * blockDim.x)
+        conf[i] = fminf(__fdiv_rn(conf[i], p), 1.f);
+}
+cudaError_t conf_scale(float* conf, size_t m, const float* p90, cudaStream_t s) {
+    conf_scale_kernel<<<grid1(m), 256, 0, s>>>(conf, m, p90);
+    return cudaGetLastError();
+}
+
+// depth.rs:1168 robust reweighting: w2 = c * min(tau / |d - u|, 1)
+__global__ void robust_kernel(const float* __restrict__ conf, const float* __restrict__ d, const float* __restrict__ u,
+                              float tau, float* __restrict__ w2, size_t m) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < m; i += (size_t)gridDim.x * blockDim.x)
+        w2[i] = __fmul_rn(conf[i], fminf(__fdiv_rn(tau, fabsf(__fsub_rn(d[i], u[i]))), 1.f));
+}
+cudaError_t robust_weights(const float* conf, const float* d, const float* u, float tau, float* w2, size_t m, cudaStream_t s) {
+    robust_kernel<<<grid1(m), 256, 0, s>>>(conf, d, u, tau, w2, m);
+    return cudaGetLastError();
+}
+
+// ----------------------------------------------------------------- upsample
+// depth.rs:201 `upsample_bilinear` weights for an axis position.
+__device__ __forceinline__ void bil_axis(int x, float inv, int dn, int& x0, int& x1, float& t) {
+    const float f = fminf(fmaxf(__fsub_rn(__fmul_rn(__fadd_rn((float)x, 0.5f), inv), 0.5f), 0.f), (float)(dn - 1));
+    x0 = (int)f;
+    x1 = min(x0 + 1, dn - 1);
+    t = __fsub_rn(f, (float)x0);
+}
+__device__ __forceinline__ float bil(const float* g, int dw, int x0, int x1, int y0, int y1, float tx, float ty) {
+    const float* r0 = g + (size_t)y0 * dw;
+    const float* r1 = g + (size_t)y1 * dw;
+    const float top = __fadd_rn(r0[x0], __fmul_rn(__fsub_rn(r0[x1], r0[x0]), tx));
+    const float bot = __fadd_rn(r1[x0], __fmul_rn(__fsub_rn(r1[x1], r1[x0]), tx));
+    return __fadd_rn(top, __fmul_rn(__fsub_rn(bot, top), ty));
+}
+// depth.rs:1183-1197: depth = clamp(a-bar(x) * Y + b-bar(x), 0, n-1) with the
+// coefficients bilinear from the grid (a = 0, b = u for bilinear upsampling);
+// the confidence bilinear too.
+__global__ void upsample_kernel(const float* __restrict__ abar, const float* __restrict__ bbar, const float* __restrict__ yfull,
+                                const float* __restrict__ conf, int w, int h, int dw, int dh, int k, float max_d, int guided,
+                                float* __restrict__ depth, float* __restrict__ conf_full) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
+    if (x >= w || y >= h) return;
+    const float inv = __fdiv_rn(1.f, (float)k);
+    int x0, x1, y0, y1;
+    float tx, ty;
+    bil_axis(x, inv, dw, x0, x1, tx);
+    bil_axis(y, inv, dh, y0, y1, ty);
+    const size_t o = (size_t)y * w + x;
+    float d;
+    if (guided) d = __fadd_rn(__fmul_rn(bil(abar, dw, x0, x1, y0, y1, tx, ty), yfull[o]), bil(bbar, dw, x0, x1, y0, y1, tx, ty));
+    else d = bil(bbar, dw, x0, x1, y0, y1, tx, ty);
+    depth[o] = fminf(fmaxf(d, 0.f), max_d);
+    conf_full[o] = bil(conf, dw, x0, x1, y0, y1, tx, ty);
+}
+// The k == 1 case: q = a-bar * I + b-bar on the grid itself, clamped.
+__global__ void apply_grid_kernel(const float* __restrict__ abar, const float* __restrict__ bbar, const float* __restrict__ guide,
+                                  size_t m, float max_d, int guided, float* __restrict__ depth) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < m; i += (size_t)gridDim.x * blockDim.x) {
+        const float d = guided ? __fadd_rn(__fmul_rn(abar[i], guide[i]), bbar[i]) : bbar[i];
+        depth[i] = fminf(fmaxf(d, 0.f), max_d);
+    }
+}
+
+cudaError_t upsample(const float* abar, const float* bbar, const float* yfull, const float* guide, const float* conf, int w,
+                     int h, int dw, int dh, int k, float max_d, bool guided, float* depth, float* conf_full, cudaStream_t s) {
+    if (k == 1) {
+        apply_grid_kernel<<<grid1((size_t)dw * dh), 256, 0, s>>>(abar, bbar, guide, (size_t)dw * dh, max_d, guided ? 1 : 0, depth);
+        cudaMemcpyAsync(conf_full, conf, sizeof(float) * dw * dh, cudaMemcpyDeviceToDevice, s);
+        return cudaGetLastError();
+    }
+    dim3 b(32, 8), g((w + 31) / 32, (h + 7) / 8);
+    upsample_kernel<<<g, b, 0, s>>>(abar, bbar, yfull, conf, w, h, dw, dh, k, max_d, guided ? 1 : 0, depth, conf_full);
+    return cudaGetLastError();
+}
+
+cudaError_t luma_and_guide(const float* img, int w, int h, int k, float* yfull, float* guide, int dw, int dh, cudaStream_t s) {
+    size_t n = (size_t)w * h;
+    luma_kernel<<<grid1(n), 256, 0, s>>>(img, yfull, n);
+    if (k == 1) return cudaMemcpyAsync(guide, yfull, sizeof(float) * n, cudaMemcpyDeviceToDevice, s);
+    dim3 b(32, 8), g((dw + 31) / 32, (dh + 7) / 8);
+    block_mean_kernel<<<g, b, 0, s>>>(yfull, w, h, k, guide, dw, dh);
+    return cudaGetLastError();
+}
+
+}  // namespace lsb

@@ -1,0 +1,81 @@
+// Internal interfaces between the engine's translation units (host side).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+namespace lsb {
+
+// Per-frame level-0 source transform: the inverse homography that maps an
+// aligned pixel to its source point (align.rs:258 `inverse` of the frame's
+// Sim::matrix) and the brightness gains (brightness.rs:124 `apply`).
+struct FrameXform {
+    double inv[9];
+    float gain[3];
+    int warp;      // 1: resample through `inv` (the pixel as shot where it leaves the frame)
+    int affine;    // inv's last row is [0, 0, 1] (align.rs:485 `affine_row`)
+    int gain_on;   // bit c: multiply channel c by gain[c] (|g - 1| > 1e-6)
+    int pad;
+};
+
+enum SrcKind { SRC_U16 = 0, SRC_F32 = 1, SRC_G = 2 };
+
+// One pyramid level's fold over all frames of a stack.
+struct FoldArgs {
+    int level, nframes;
+    int W, H, W1, H1;
+    int tiles_x, tiles_y, ntiles;
+    // level-0 sources: interleaved u16 [n][H][W][3] or planar f32 [n][3][H][W]
+    const uint16_t* src_u16;
+    const float* src_f32;
+    const FrameXform* xf;  // per frame, level 0 only
+    int interp;            // align.rs Interp id for the warp
+    // level >= 1 source and every level's output: planar [n][3][h][w] in the storage type
+    const void* src_g;
+    void* dst_g;
+    // accumulator of this level: acc [3][H][W], best [H][W], winner [H][W] (depth level only)
+    float* acc;
+    float* best;
+    uint16_t* winner;
+    int use_chroma;
+    // focus slices (level 0): [n][dh][dw], block k, measure
+    void* slice;
+    int dw, dh, bk;
+    int focus_kind;  // 0 RDF, 1 SML
+    int sml_step;
+    int ntaps;
+    int* status;  // device error word
+};
+
+// Launchers (lsb_fold.cu).
+cudaError_t fold_level(const FoldArgs& a, int src_kind, bool fp16, int radius, bool focus, bool slice_fp16,
+                       cudaStream_t s, int grid_limit);
+cudaError_t set_focus_taps(const float* taps3, int ntaps, cudaStream_t s);
+size_t fold_smem_bytes(int radius, bool focus);
+
+// Residual (top) level: fuse.rs:248 `fuse_residuals` over all frames' tops.
+struct ResidualArgs {
+    const void* tops;  // [n][3][h][w] storage type
+    int n, w, h;
+    int top_rule, radius, bins;
+    float* dev;  // scratch [n][h][w]
+    float* ent;  // scratch [n][h][w]
+    float* out;  // [3][h][w]
+};
+cudaError_t fuse_residuals(const ResidualArgs& a, bool fp16, const float* lnp, cudaStream_t s);
+
+// Collapse: out_l = acc_l + EXPAND(coarse) (pyramid.rs:219); at level 0 also clamp and pack.
+cudaError_t collapse_level(const float* acc, const float* coarse, float* out, int w, int h, int cw, int ch, bool last,
+                           uint16_t* rgb_out, cudaStream_t s);
+
+// winner_shares (fuse.rs:315) on the device: counts[frames] of detail cells.
+cudaError_t winner_counts(const uint16_t* win, const float* best, int cells, int frames, unsigned int* counts,
+                          float* scratch_max, cudaStream_t s);
+
+// brightness.rs:107 `means` of every frame on the stride-4 grid (unwarped u16).
+cudaError_t frame_means(const uint16_t* frames, int n, int w, int h, double* partial, int nparts, double* means,
+                        cudaStream_t s);
+
+}  // namespace lsb

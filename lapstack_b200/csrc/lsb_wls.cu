@@ -1,0 +1,406 @@
+// The confidence-weighted, edge-aware WLS depth solve (crates/lapstack-core/
+// src/depth.rs:958 `WlsSolver`) on the device: the separable fast-global-
+// smoother guess (depth.rs:677/707 Thomas sweeps, depth.rs:1022-1034
+// schedule), then CG on (W + lambda L) u = W d preconditioned by one V-cycle
+// of the 2x2-aggregation multigrid hierarchy (depth.rs:753-947), stopping at
+// a relative residual of 1e-5. The f32 stencil, smoother, restriction and
+// prolongation follow the reference's operation order; the CG dot products
+// are f64 sums in a fixed two-stage order.
+#include <cuda_bf16.h>
+
+#include <algorithm>
+#include <vector>
+
+#include "lsb_common.cuh"
+#include "lsb_depth.h"
+
+namespace lsb {
+
+constexpr float MG_OMEGA = 0.8f;
+constexpr int MG_COARSE = 32, MG_MIN = 16;
+constexpr int DOT_BLOCKS = 592;
+
+struct WlsSolver {
+    int w, h;
+    float lambda;
+    float *ex, *ey;
+    std::vector<WlsLevel> lv;
+    float *cp, *dp, *f, *r, *z, *p, *ap, *ones;
+    double *part, *scal;  // scal: [rz, pap, rr, bnorm2, rz_new]
+    float* alpha_beta;    // [alpha, beta]
+    float* host_rel;      // pinned: [rel, stop]
+    std::vector<void*> allocs;
+    float* alloc(size_t n, cudaError_t* e) {
+        void* p = nullptr;
+        cudaError_t r = cudaMalloc(&p, n * sizeof(float));
+        if (r != cudaSuccess) *e = r;
+        else allocs.push_back(p);
+        return (float*)p;
+    }
+};
+
+static int g1(size_t n) { return (int)std::min<size_t>((n + 255) / 256, 148 * 16); }
+static dim3 g2(int w, int h) { return dim3((w + 31) / 32, (h + 7) / 8); }
+static const dim3 B2(32, 8);
+
+// depth.rs:653 `edge_weights`: e = exp(-|dI| / sigma) right and below (mode 0);
+// mode 1, the Gaussian-of-gradient weight exp(-dI^2 / (2 sigma^2)).
+__global__ void edge_kernel(const float* __restrict__ g, int w, int h, float inv, float inv2s2, int mode, float lambda,
+                            float* ex, float* ey, float* ax, float* ay) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
+    if (x >= w || y >= h) return;
+    const size_t k = (size_t)y * w + x;
+    float vx = 0.f, vy = 0.f;
+    if (x + 1 < w) {
+        const float d = fabsf(__fsub_rn(g[k], g[k + 1]));
+        vx = mode == 0 ? expf(__fmul_rn(d, inv)) : expf(-__fmul_rn(__fmul_rn(d, d), inv2s2));
+    }
+    if (y + 1 < h) {
+        const float d = fabsf(__fsub_rn(g[k], g[k + w]));
+        vy = mode == 0 ? expf(__fmul_rn(d, inv)) : expf(-__fmul_rn(__fmul_rn(d, d), inv2s2));
+    }
+    ex[k] = vx;
+    ey[k] = vy;
+    ax[k] = __fmul_rn(lambda, vx);
+    ay[k] = __fmul_rn(lambda, vy);
+}
+
+// depth.rs:852 `coarsen` (edges) and :886 `coarsen_wd_into` (data weights)
+__global__ void coarsen_edges_kernel(const float* __restrict__ ax, const float* __restrict__ ay, int w, int h, float* cax,
+                                     float* cay, int cw, int ch) {
+    const int xx = blockIdx.x * blockDim.x + threadIdx.x, yy = blockIdx.y * blockDim.y + threadIdx.y;
+    if (xx >= cw || yy >= ch) return;
+    float a = 0.f;
+    if (xx + 1 < cw)
+        for (int y = 2 * yy; y < min(2 * yy + 2, h); y++) a = __fadd_rn(a, ax[(size_t)y * w + 2 * xx + 1]);
+    cax[(size_t)yy * cw + xx] = a;
+    float b = 0.f;
+    if (yy + 1 < ch) {
+        const int y = 2 * yy + 1;
+        for (int x = 2 * xx; x < min(2 * xx + 2, w); x++) b = __fadd_rn(b, ay[(size_t)y * w + x]);
+    }
+    cay[(size_t)yy * cw + xx] = b;
+}
+// b_c = P^T r (depth.rs:911 `restrict`), the same block sum as the data weights
+__global__ void block_sum_kernel(const float* __restrict__ src, int w, int h, float* __restrict__ dst, int cw, int ch) {
+    const int xx = blockIdx.x * blockDim.x + threadIdx.x, yy = blockIdx.y * blockDim.y + threadIdx.y;
+    if (xx >= cw || yy >= ch) return;
+    float o = 0.f;
+    for (int y = 2 * yy; y < min(2 * yy + 2, h); y++) {
+        float rs = 0.f;
+        for (int x = 2 * xx; x < min(2 * xx + 2, w); x++) rs = __fadd_rn(rs, src[(size_t)y * w + x]);
+        o = __fadd_rn(o, rs);
+    }
+    dst[(size_t)yy * cw + xx] = o;
+}
+// depth.rs:812 `set_dinv`
+__global__ void dinv_kernel(const float* __restrict__ wd, const float* __restrict__ ax, const float* __restrict__ ay, int w, int h,
+                            float* __restrict__ dinv) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
+    if (x >= w || y >= h) return;
+    const size_t k = (size_t)y * w + x;
+    float v = wd[k];
+    if (x > 0) v = __fadd_rn(v, ax[k - 1]);
+    if (x + 1 < w) v = __fadd_rn(v, ax[k]);
+    if (y > 0) v = __fadd_rn(v, ay[k - w]);
+    if (y + 1 < h) v = __fadd_rn(v, ay[k]);
+    dinv[k] = __fdiv_rn(1.f, fmaxf(v, 1e-12f));
+}
+// depth.rs:786 `apply`: mode 0 out = A x; 1 out = b - A x; 2 out = x + w D^-1 (b - A x)
+__global__ void stencil_kernel(const float* __restrict__ x, const float* __restrict__ b, const float* __restrict__ wd,
+                               const float* __restrict__ ax, const float* __restrict__ ay, const float* __restrict__ dinv,
+                               float* __restrict__ out, int w, int h, int mode) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
+    if (i >= w || y >= h) return;
+    const size_t k = (size_t)y * w + i;
+    const float xk = x[k];
+    float v = __fmul_rn(wd[k], xk);
+    if (i > 0) v = __fadd_rn(v, __fmul_rn(ax[k - 1], __fsub_rn(xk, x[k - 1])));
+    if (i + 1 < w) v = __fadd_rn(v, __fmul_rn(ax[k], __fsub_rn(xk, x[k + 1])));
+    if (y > 0) v = __fadd_rn(v, __fmul_rn(ay[k - w], __fsub_rn(xk, x[k - w])));
+    if (y + 1 < h) v = __fadd_rn(v, __fmul_rn(ay[k], __fsub_rn(xk, x[k + w])));
+    if (mode == 0) out[k] = v;
+    else if (mode == 1) out[k] = __fsub_rn(b[k], v);
+    else out[k] = __fadd_rn(xk, __fmul_rn(__fmul_rn(MG_OMEGA, dinv[k]), __fsub_rn(b[k], v)));
+}
+// depth.rs:840 zero-start Jacobi: x = w * D^-1 * b
+__global__ void jac0_kernel(const float* __restrict__ b, const float* __restrict__ dinv, float* __restrict__ x, size_t n) {
+    for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x)
+        x[k] = __fmul_rn(__fmul_rn(MG_OMEGA, dinv[k]), b[k]);
+}
+// depth.rs:901 `prolong_add`
+__global__ void prolong_kernel(float* __restrict__ x, int w, int h, const float* __restrict__ xc, int cw) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
+    if (i >= w || y >= h) return;
+    const size_t k = (size_t)y * w + i;
+    x[k] = __fadd_rn(x[k], xc[(size_t)(y / 2) * cw + i / 2]);
+}
+// depth.rs:994 wd = max(conf, 0) + 1e-4
+__global__ void wd_kernel(const float* __restrict__ conf, float* __restrict__ wd, size_t n) {
+    for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x)
+        wd[k] = __fadd_rn(fmaxf(conf[k], 0.f), 1e-4f);
+}
+
+// depth.rs:677 `solve_rows` / :707 `solve_cols`: the Thomas algorithm along
+// every line, one thread per line (stride 1: rows; stride w: columns).
+__global__ void thomas_kernel(float* __restrict__ u, const float* __restrict__ f, const float* __restrict__ wd, int unit_wd,
+                              const float* __restrict__ a, int nlines, int len, size_t line_step, size_t stride, float lam,
+                              float* __restrict__ cp, float* __restrict__ dp) {
+    const int li = blockIdx.x * blockDim.x + threadIdx.x;
+    if (li >= nlines) return;
+    const size_t base = (size_t)li * line_step;
+    float prev_a = 0.f, cprev = 0.f, dprev = 0.f;
+    const float nl = -lam;
+    for (int i = 0; i < len; i++) {
+        const size_t k = base + (size_t)i * stride;
+        const float ai = i + 1 < len ? a[k] : 0.f;
+        const float wdi = unit_wd ? 1.f : wd[k];
+        const float diag = __fadd_rn(wdi, __fmul_rn(lam, __fadd_rn(prev_a, ai)));
+        const float lower = __fmul_rn(nl, prev_a), upper = __fmul_rn(nl, ai);
+        float m = __fsub_rn(diag, __fmul_rn(lower, i > 0 ? cprev : 0.f));
+        if (fabsf(m) < 1e-12f) m = 1e-12f;
+        cprev = __fdiv_rn(upper, m);
+        dprev = __fdiv_rn(__fsub_rn(__fmul_rn(wdi, f[k]), __fmul_rn(lower, i > 0 ? dprev : 0.f)), m);
+        cp[k] = cprev;
+        dp[k] = dprev;
+        prev_a = ai;
+    }
+    float nxt = dp[base + (size_t)(len - 1) * stride];
+    u[base + (size_t)(len - 1) * stride] = nxt;
+    for (int i = len - 2; i >= 0; i--) {
+        const size_t k = base + (size_t)i * stride;
+        nxt = __fsub_rn(dp[k], __fmul_rn(cp[k], nxt));
+        u[k] = nxt;
+    }
+}
+
+// f64 dot products: per-block partials, then the partials in order.
+__global__ void dot_partial_kernel(const float* __restrict__ a, const float* __restrict__ b, size_t n, double* part) {
+    double s = 0.0;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        s += (double)a[i] * (double)b[i];
+    __shared__ double red[256];
+    red[threadIdx.x] = s;
+    __syncthreads();
+    for (int st = 128; st > 0; st >>= 1) {
+        if (threadIdx.x < st) red[threadIdx.x] += red[threadIdx.x + st];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) part[blockIdx.x] = red[0];
+}
+// mode: 0 rz; 1 pap -> alpha; 2 rz_new -> beta; 3 rr -> rel; 4 bb -> bnorm
+__global__ void dot_final_kernel(const double* part, int nparts, double* scal, float* ab, float* host_rel, int mode) {
+    if (threadIdx.x != 0) return;
+    double s = 0.0;
+    for (int i = 0; i < nparts; i++) s += part[i];
+    if (mode == 0) scal[0] = s;
+    else if (mode == 1) {
+        scal[1] = s;
+        host_rel[1] = s <= 0.0 ? 1.f : 0.f;
+        ab[0] = s <= 0.0 ? 0.f : (float)(scal[0] / s);
+    } else if (mode == 2) {
+        ab[1] = (float)(s / scal[0]);
+        scal[0] = s;
+    } else if (mode == 3) {
+        scal[2] = s;
+        host_rel[0] = (float)(sqrt(s) / scal[3]);
+        host_rel[2] = 0.f;
+        ((double*)(host_rel + 4))[0] = sqrt(s) / scal[3];
+    } else {
+        scal[3] = fmax(sqrt(s), 1e-30);
+    }
+}
+__global__ void axpy2_kernel(float* __restrict__ u, const float* __restrict__ p, float* __restrict__ r, const float* __restrict__ ap,
+                             const float* ab, size_t n) {
+    const float alpha = ab[0];
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        u[i] = __fadd_rn(u[i], __fmul_rn(alpha, p[i]));
+        r[i] = __fsub_rn(r[i], __fmul_rn(alpha, ap[i]));
+    }
+}
+__global__ void pupd_kernel(float* __restrict__ p, const float* __restrict__ z, const float* ab, size_t n) {
+    const float beta = ab[1];
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        p[i] = __fadd_rn(z[i], __fmul_rn(beta, p[i]));
+}
+__global__ void mul_kernel(const float* __restrict__ a, const float* __restrict__ b, float* __restrict__ o, size_t n) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        o[i] = __fmul_rn(a[i], b[i]);
+}
+__global__ void fill_kernel(float* o, float v, size_t n) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) o[i] = v;
+}
+
+WlsSolver* wls_create(const float* guide, int w, int h, float lambda, float sigma_c, int edge_mode, cudaStream_t s,
+                      cudaError_t* err) {
+    *err = cudaSuccess;
+    WlsSolver* S = new WlsSolver();
+    S->w = w;
+    S->h = h;
+    S->lambda = lambda;
+    size_t n = (size_t)w * h;
+    S->ex = S->alloc(n, err);
+    S->ey = S->alloc(n, err);
+    int cw = w, ch = h;
+    while (true) {
+        WlsLevel L;
+        L.w = cw;
+        L.h = ch;
+        size_t m = (size_t)cw * ch;
+        L.wd = S->alloc(m, err);
+        L.ax = S->alloc(m, err);
+        L.ay = S->alloc(m, err);
+        L.dinv = S->alloc(m, err);
+        L.x = S->alloc(m, err);
+        L.b = S->alloc(m, err);
+        L.r = S->alloc(m, err);
+        S->lv.push_back(L);
+        if (std::max(cw, ch) <= MG_MIN) break;
+        cw = (cw + 1) / 2;
+        ch = (ch + 1) / 2;
+    }
+    S->cp = S->alloc(n, err);
+    S->dp = S->alloc(n, err);
+    S->f = S->alloc(n, err);
+    S->r = S->alloc(n, err);
+    S->z = S->alloc(n, err);
+    S->p = S->alloc(n, err);
+    S->ap = S->alloc(n, err);
+    S->ones = S->alloc(n, err);
+    S->part = (double*)S->alloc(2 * DOT_BLOCKS, err);
+    S->scal = (double*)S->alloc(16, err);
+    S->alpha_beta = S->alloc(4, err);
+    if (cudaHostAlloc((void**)&S->host_rel, 64, cudaHostAllocDefault) != cudaSuccess) *err = cudaErrorMemoryAllocation;
+    if (*err != cudaSuccess) return S;
+    const float inv = -1.0f / std::max(sigma_c, 1e-6f);
+    const float inv2s2 = 1.0f / (2.0f * sigma_c * sigma_c);
+    edge_kernel<<<g2(w, h), B2, 0, s>>>(guide, w, h, inv, inv2s2, edge_mode, lambda, S->ex, S->ey, S->lv[0].ax, S->lv[0].ay);
+    for (size_t l = 1; l < S->lv.size(); l++) {
+        const WlsLevel &F = S->lv[l - 1], &C = S->lv[l];
+        coarsen_edges_kernel<<<g2(C.w, C.h), B2, 0, s>>>(F.ax, F.ay, F.w, F.h, C.ax, C.ay, C.w, C.h);
+    }
+    fill_kernel<<<g1(n), 256, 0, s>>>(S->ones, 1.f, n);
+    *err = cudaGetLastError();
+    return S;
+}
+
+void wls_destroy(WlsSolver* s) {
+    if (!s) return;
+    for (void* p : s->allocs) cudaFree(p);
+    if (s->host_rel) cudaFreeHost(s->host_rel);
+    delete s;
+}
+
+int wls_levels(const WlsSolver* s) { return (int)s->lv.size(); }
+
+cudaError_t wls_set_weights(WlsSolver* S, const float* conf, cudaStream_t s) {
+    wd_kernel<<<g1((size_t)S->w * S->h), 256, 0, s>>>(conf, S->lv[0].wd, (size_t)S->w * S->h);
+    for (size_t l = 0; l < S->lv.size(); l++) {
+        const WlsLevel& C = S->lv[l];
+        if (l > 0) {
+            const WlsLevel& F = S->lv[l - 1];
+            block_sum_kernel<<<g2(C.w, C.h), B2, 0, s>>>(F.wd, F.w, F.h, C.wd, C.w, C.h);
+        }
+        dinv_kernel<<<g2(C.w, C.h), B2, 0, s>>>(C.wd, C.ax, C.ay, C.w, C.h, C.dinv);
+    }
+    return cudaGetLastError();
+}
+
+static void jacobi(WlsLevel& L, bool zero, cudaStream_t s) {
+    if (zero) {
+        jac0_kernel<<<g1((size_t)L.w * L.h), 256, 0, s>>>(L.b, L.dinv, L.x, (size_t)L.w * L.h);
+        return;
+    }
+    stencil_kernel<<<g2(L.w, L.h), B2, 0, s>>>(L.x, L.b, L.wd, L.ax, L.ay, L.dinv, L.r, L.w, L.h, 2);
+    std::swap(L.x, L.r);
+}
+
+// depth.rs:924 `vcycle`
+static void vcycle(WlsSolver* S, size_t l, cudaStream_t s) {
+    WlsLevel& T = S->lv[l];
+    if (l + 1 == S->lv.size()) {
+        for (int k = 0; k < MG_COARSE; k++) jacobi(T, k == 0, s);
+        return;
+    }
+    jacobi(T, true, s);
+    stencil_kernel<<<g2(T.w, T.h), B2, 0, s>>>(T.x, T.b, T.wd, T.ax, T.ay, T.dinv, T.r, T.w, T.h, 1);
+    WlsLevel& C = S->lv[l + 1];
+    block_sum_kernel<<<g2(C.w, C.h), B2, 0, s>>>(T.r, T.w, T.h, C.b, C.w, C.h);
+    vcycle(S, l + 1, s);
+    prolong_kernel<<<g2(T.w, T.h), B2, 0, s>>>(T.x, T.w, T.h, C.x, C.w);
+    jacobi(T, false, s);
+}
+
+static void dot(WlsSolver* S, const float* a, const float* b, size_t n, int mode, cudaStream_t s) {
+    int nb = (int)std::min<size_t>(DOT_BLOCKS, (n + 255) / 256);
+    dot_partial_kernel<<<nb, 256, 0, s>>>(a, b, n, S->part);
+    dot_final_kernel<<<1, 32, 0, s>>>(S->part, nb, S->scal, S->alpha_beta, S->host_rel, mode);
+}
+
+cudaError_t wls_solve(WlsSolver* S, const float* d, int max_iters, float* u, float* rel_out, int* iters_out, cudaStream_t s,
+                      int mode, bool x0_given, double* rel64) {
+    (void)mode;
+    const int w = S->w, h = S->h;
+    const size_t n = (size_t)w * h;
+    WlsLevel& L0 = S->lv[0];
+    if (w == 1 || h == 1) {
+        if (h == 1) thomas_kernel<<<1, 32, 0, s>>>(u, d, L0.wd, 0, S->ex, 1, w, 0, 1, S->lambda, S->cp, S->dp);
+        else thomas_kernel<<<1, 32, 0, s>>>(u, d, L0.wd, 0, S->ey, 1, h, 0, (size_t)w, S->lambda, S->cp, S->dp);
+        *rel_out = 0.f;
+        *iters_out = 0;
+        if (rel64) *rel64 = 0.0;
+        return cudaGetLastError();
+    }
+    if (!x0_given) {
+        // depth.rs:1022-1034: three separable sweeps, the first confidence-weighted
+        cudaMemcpyAsync(S->f, d, n * sizeof(float), cudaMemcpyDeviceToDevice, s);
+        for (int t = 1; t <= 3; t++) {
+            float p4 = 1.f;
+            for (int q = 0; q < 3 - t; q++) p4 *= 4.f;
+            const float lam_t = (1.5f * S->lambda * p4) / (64.f - 1.f);
+            thomas_kernel<<<(h + 127) / 128, 128, 0, s>>>(u, S->f, L0.wd, t == 1 ? 0 : 1, S->ex, h, w, (size_t)w, 1, lam_t, S->cp, S->dp);
+            cudaMemcpyAsync(S->f, u, n * sizeof(float), cudaMemcpyDeviceToDevice, s);
+            thomas_kernel<<<(w + 127) / 128, 128, 0, s>>>(u, S->f, L0.wd, 1, S->ey, w, h, 1, (size_t)w, lam_t, S->cp, S->dp);
+            cudaMemcpyAsync(S->f, u, n * sizeof(float), cudaMemcpyDeviceToDevice, s);
+        }
+    }
+    // b = W d, |b|, r = b - A u, z = M r, p = z
+    mul_kernel<<<g1(n), 256, 0, s>>>(L0.wd, d, S->f, n);
+    dot(S, S->f, S->f, n, 4, s);
+    stencil_kernel<<<g2(w, h), B2, 0, s>>>(u, S->f, L0.wd, L0.ax, L0.ay, L0.dinv, S->r, w, h, 1);
+    auto precond = [&]() {
+        cudaMemcpyAsync(L0.b, S->r, n * sizeof(float), cudaMemcpyDeviceToDevice, s);
+        vcycle(S, 0, s);
+        cudaMemcpyAsync(S->z, S->lv[0].x, n * sizeof(float), cudaMemcpyDeviceToDevice, s);
+    };
+    precond();
+    cudaMemcpyAsync(S->p, S->z, n * sizeof(float), cudaMemcpyDeviceToDevice, s);
+    dot(S, S->r, S->z, n, 0, s);
+    dot(S, S->r, S->r, n, 3, s);
+    cudaError_t e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return e;
+    float rel = S->host_rel[0];
+    int iters = 0;
+    for (int it = 0; it < max_iters; it++) {
+        if (rel < 1e-5f) break;
+        iters++;
+        stencil_kernel<<<g2(w, h), B2, 0, s>>>(S->p, S->f, L0.wd, L0.ax, L0.ay, L0.dinv, S->ap, w, h, 0);
+        dot(S, S->p, S->ap, n, 1, s);
+        axpy2_kernel<<<g1(n), 256, 0, s>>>(u, S->p, S->r, S->ap, S->alpha_beta, n);
+        dot(S, S->r, S->r, n, 3, s);
+        e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) return e;
+        if (S->host_rel[1] != 0.f) break;  // p.Ap <= 0: alpha was 0, u and r are unchanged (depth.rs:1060)
+        rel = S->host_rel[0];
+        if (rel < 1e-5f) break;
+        precond();
+        dot(S, S->r, S->z, n, 2, s);
+        pupd_kernel<<<g1(n), 256, 0, s>>>(S->p, S->z, S->alpha_beta, n);
+    }
+    *rel_out = rel;
+    *iters_out = iters;
+    if (rel64) *rel64 = ((double*)(S->host_rel + 4))[0];
+    return cudaGetLastError();
+}
+
+}  // namespace lsb

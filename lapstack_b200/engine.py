@@ -1,0 +1,405 @@
+"""Host-side mirror of lapstack-core's stacking interface over the C ABI.
+
+Names and argument meaning follow the reference (crates/lapstack-core/src):
+FuseParams / AlignParams / DepthParams carry its defaults (fuse.rs:94-107,
+align.rs:66-70, depth.rs:93-109); `GpuFuser` has the new / push / shares /
+finish contract of gpu.rs:326 (and stack.rs:123 AnyFuser); `depth_from_slices`
+is gpu.rs:1327; `Stack` runs stack.rs:1011 `run_with` for in-memory 16-bit
+frames. Errors are raised as LsbError with the library's message, the way
+the reference returns Result<_, String>.
+
+Inputs may be numpy arrays (host memory) or CUDA tensors (device memory).
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from ._lib import (AlignParamsC, Config, DepthParamsC, FuseParamsC, LOG_FN, LsbError, Result, SynthDesc, check, load)
+
+TOP_RULES = {"de": 0, "dev": 1, "avg": 2}
+INTERPS = ["nearest", "bilinear", "bicubic", "spline4x4", "spline6x6", "lanczos3"]
+MODELS = ["similarity", "affine", "projective"]
+
+
+@dataclass
+class FuseParams:  # fuse.rs:70-107
+    levels: int = 0
+    energy_radius: int = 1
+    top_rule: str = "de"
+    top_radius: int = 2
+    entropy_bins: int = 256
+    use_chroma: bool = False
+    depth_level: int = 2
+    halo: float = 0.0
+
+    def c(self):
+        return FuseParamsC(self.levels, self.energy_radius, TOP_RULES[self.top_rule], self.top_radius, self.entropy_bins,
+                           int(self.use_chroma), self.depth_level, self.halo)
+
+
+@dataclass
+class AlignParams:  # align.rs:52-70
+    shift: bool = True
+    scale: bool = True
+    rotation: bool = True
+    model: str = "similarity"
+    coarsen: int = 0
+    interp: str = "spline4x4"
+
+    def c(self, enabled=True):
+        return AlignParamsC(int(enabled), int(self.shift), int(self.scale), int(self.rotation), MODELS.index(self.model),
+                            self.coarsen, INTERPS.index(self.interp), 0)
+
+    def free(self):
+        a, p = self.model != "similarity", self.model == "projective"
+        return [self.shift, self.shift, self.scale, self.rotation, a, a, p, p]
+
+
+@dataclass
+class DepthParams:  # depth.rs:69-109
+    scale: int = 1
+    focus: str = "rdf"
+    r_in: int = 1
+    r_out: int = 3
+    sml_step: int = 1
+    agg_radius: int = 3
+    agg_eps: float = 1e-4
+    lam: float = 3.0
+    sigma_c: float = 0.04
+    cg_iters: int = 200
+    median: bool = True
+    upsample: str = "guided"
+    up_radius: int = 2
+    up_eps: float = 1e-2
+    gate: float = 1.0
+    robust: float = 1.0
+    edge_mode: int = 0  # 0: exp(-|dI|/sigma_c) as the reference; 1: exp(-dI^2/(2 sigma_c^2))
+    vcycle_mode: int = 0  # 0: FP32 V-cycle as the reference; 1: BF16 smoother and restriction
+
+    def c(self, enabled=True):
+        return DepthParamsC(int(enabled), self.scale, 0 if self.focus == "rdf" else 1, self.r_in, self.r_out, self.sml_step,
+                            self.agg_radius, self.agg_eps, self.lam, self.sigma_c, self.cg_iters, int(self.median),
+                            0 if self.upsample == "bilinear" else 1, self.up_radius, self.up_eps, self.gate, self.robust,
+                            self.edge_mode, self.vcycle_mode)
+
+
+@dataclass
+class DepthMap:  # depth.rs:141
+    depth: np.ndarray
+    conf: np.ndarray
+    w: int
+    h: int
+    dw: int
+    dh: int
+    floor: np.ndarray
+    floor_value: float = 0.0
+    p90: float = 0.0
+    wls_rel: float = 0.0
+    wls_rel64: float = 0.0
+    wls_iters: int = 0
+    wls_iters_first: int = 0
+
+
+@dataclass
+class Output:  # stack.rs:244 Output (the hot-path part)
+    image: np.ndarray  # (3, h, w) float32 in [0, 1]
+    image_u16: np.ndarray  # (h, w, 3) uint16
+    winner: np.ndarray  # (h, w) float32
+    depth: DepthMap | None
+    align: np.ndarray  # (n, 8) Sim vectors
+    gains: np.ndarray  # (n, 3)
+    shares: np.ndarray
+    levels: int
+    crop: tuple
+    align_evals: int = 0
+    ms: dict = field(default_factory=dict)
+
+
+STAGES = ["align", "gains", "fold", "collapse", "aggregate", "wls", "upsample", "total"]
+
+
+def _ptr(a):
+    """A host numpy array or a CUDA tensor -> (void*, keep-alive)."""
+    if isinstance(a, np.ndarray):
+        a = np.ascontiguousarray(a)
+        return C.c_void_p(a.ctypes.data), a
+    if hasattr(a, "data_ptr"):
+        if not a.is_contiguous():
+            a = a.contiguous()
+        return C.c_void_p(a.data_ptr()), a
+    raise TypeError(f"expected a numpy array or a tensor, got {type(a)}")
+
+
+class Engine:
+    """lsb_engine: one CUDA device, one stream (gpu.rs:308-324's set-up, once)."""
+
+    def __init__(self, device: int = 0, fp16_storage: bool = False, grid_limit: int = 0, log=None):
+        self._L = load()
+        self._logcb = LOG_FN(lambda line, _u: log(line.decode())) if log else LOG_FN()
+        cfg = Config(device, int(fp16_storage), grid_limit, 0, self._logcb, None)
+        h = C.c_void_p()
+        check(self._L.lsb_engine_create(C.byref(cfg), C.byref(h)))
+        self._h = h
+        self.fp16_storage = fp16_storage
+
+    @property
+    def stream(self):
+        return self._L.lsb_engine_stream(self._h)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._L.lsb_engine_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def stack(self, w, h, n, fuse=None, align=None, depth=None, brightness=True, crop=True):
+        return Stack(self, w, h, n, fuse, align, depth, brightness, crop)
+
+
+_default = None
+
+
+def default_engine() -> Engine:
+    global _default
+    if _default is None:
+        _default = Engine()
+    return _default
+
+
+def _arr(ptr, n, dt):
+    return np.ctypeslib.as_array(ptr, shape=(n,)).astype(dt, copy=True)
+
+
+class Stack:
+    """One stack: push frames (host or device), then finish (stack.rs:1011 run_with)."""
+
+    def __init__(self, engine: Engine, w, h, n, fuse=None, align=None, depth=None, brightness=True, crop=True):
+        self.e, self.w, self.h, self.n = engine, w, h, n
+        self._L = engine._L
+        self.fuse = fuse or FuseParams()
+        self.align = align
+        self.depth = depth
+        fp = self.fuse.c()
+        ap = (align or AlignParams()).c(enabled=align is not None)
+        dp = (depth or DepthParams()).c(enabled=depth is not None)
+        hnd = C.c_void_p()
+        check(self._L.lsb_stack_begin(engine._h, w, h, n, C.byref(fp), C.byref(ap), C.byref(dp), int(brightness), int(crop),
+                                      C.byref(hnd)))
+        self._h = hnd
+        self._keep = []
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._L.lsb_stack_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def push_u16(self, rgb, stride_px: int = 0):
+        """One decoded frame, (h, w, 3) uint16 (numpy or CUDA tensor)."""
+        p, keep = _ptr(rgb)
+        check(self._L.lsb_stack_push_u16(self._h, p, stride_px))
+        self._keep.append(keep)  # async copies from host memory complete before the next sync
+
+    def push_f32(self, planes):
+        """AnyFuser::push(&Img3): (3, h, w) float32 planes in [0, 1]."""
+        ps = []
+        for c in range(3):
+            p, keep = _ptr(planes[c])
+            ps.append(p)
+            self._keep.append(keep)
+        arr = (C.c_void_p * 3)(*ps)
+        check(self._L.lsb_stack_push_f32(self._h, arr))
+
+    push = push_f32
+
+    def frames_device(self):
+        p = C.c_void_p()
+        check(self._L.lsb_stack_frames_device(self._h, C.byref(p)))
+        return p.value
+
+    def set_count(self, count):
+        check(self._L.lsb_stack_set_count(self._h, count))
+
+    def shares(self):
+        out = np.zeros(self.n, np.float32)
+        check(self._L.lsb_stack_shares(self._h, C.c_void_p(out.ctypes.data)))
+        self._keep.clear()
+        return out
+
+    def run(self):
+        """The whole pipeline, results left on the device; per-stage device ms."""
+        ms = np.zeros(8, np.float64)
+        check(self._L.lsb_stack_run(self._h, C.c_void_p(ms.ctypes.data)))
+        self._keep.clear()
+        return dict(zip(STAGES, ms.tolist()))
+
+    def finish(self) -> Output:
+        r = Result()
+        check(self._L.lsb_stack_finish(self._h, C.byref(r)))
+        self._keep.clear()
+        try:
+            w, h, n = r.w, r.h, r.n_frames
+            img = _arr(r.image_f32, 3 * w * h, np.float32).reshape(3, h, w)
+            u16 = _arr(r.image_u16, 3 * w * h, np.uint16).reshape(h, w, 3)
+            win = _arr(r.winner, w * h, np.float32).reshape(h, w)
+            dm = None
+            if r.depth:
+                dm = DepthMap(_arr(r.depth, w * h, np.float32).reshape(h, w), _arr(r.conf, w * h, np.float32).reshape(h, w), w,
+                              h, r.dw, r.dh, _arr(r.floor_cells, r.dw * r.dh, np.float32).reshape(r.dh, r.dw), r.floor_value,
+                              r.p90, r.wls_rel, r.wls_rel64, r.wls_iters, r.wls_iters_first)
+            return Output(img, u16, win, dm, _arr(r.sims, 8 * n, np.float64).reshape(n, 8),
+                          _arr(r.gains, 3 * n, np.float32).reshape(n, 3), _arr(r.shares, n, np.float32), r.levels,
+                          tuple(r.crop), r.align_evals, dict(zip(STAGES, list(r.ms))))
+        finally:
+            self._L.lsb_result_free(C.byref(r))
+
+
+class GpuFuser:
+    """gpu.rs:326 `GpuFuser` (the AnyFuser contract of stack.rs:123): push
+    aligned, equalised RGB frames as (3, h, w) float32 planes, then shares /
+    finish. finish returns the fused image (clamped) and the winner map of
+    depth_level upsampled to full resolution, as fuse.rs:499 `finish`."""
+
+    def __init__(self, w, h, params: FuseParams | None = None, n_max: int = 64, engine: Engine | None = None):
+        self.w, self.h = w, h
+        self.params = params or FuseParams()
+        self._s = Stack(engine or default_engine(), w, h, n_max, self.params, None, None, brightness=False, crop=False)
+        self.count = 0
+
+    @property
+    def levels(self):
+        return _levels_of(self.w, self.h, self.params)
+
+    def push(self, planes):
+        self._s.push_f32(planes)
+        self.count += 1
+
+    def shares(self):
+        return self._s.shares()[:self.count]
+
+    def finish(self):
+        o = self._s.finish()
+        return o.image, o.winner
+
+
+def _levels_of(w, h, p: FuseParams):
+    if p.levels:
+        return p.levels
+    cw, ch, k = w, h, 0
+    while (cw > 1 or ch > 1) and min((cw + 1) // 2, (ch + 1) // 2) >= 32:
+        cw, ch, k = (cw + 1) // 2, (ch + 1) // 2, k + 1
+    return max(k, 1)
+
+
+def depth_from_slices(slices, fused, params: DepthParams | None = None, engine: Engine | None = None) -> DepthMap:
+    """gpu.rs:1327: slices (n, dh, dw) float32, fused (3, h, w) float32 -> DepthMap."""
+    e = engine or default_engine()
+    p = params or DepthParams()
+    sl = np.ascontiguousarray(slices, dtype=np.float32)
+    fu = np.ascontiguousarray(fused, dtype=np.float32)
+    _, h, w = fu.shape
+    dp = p.c()
+    r = Result()
+    check(e._L.lsb_depth_from_slices(e._h, C.c_void_p(sl.ctypes.data), sl.shape[0], C.c_void_p(fu.ctypes.data), w, h,
+                                     C.byref(dp), C.byref(r)))
+    try:
+        return DepthMap(_arr(r.depth, w * h, np.float32).reshape(h, w), _arr(r.conf, w * h, np.float32).reshape(h, w), w, h, r.dw,
+                        r.dh, _arr(r.floor_cells, r.dw * r.dh, np.float32).reshape(r.dh, r.dw), r.floor_value, r.p90, r.wls_rel,
+                        r.wls_rel64, r.wls_iters, r.wls_iters_first)
+    finally:
+        e._L.lsb_result_free(C.byref(r))
+
+
+def wls_solve(d, conf, guide, lam, sigma_c, max_iters=200, edge_mode=0, vcycle_mode=0, engine: Engine | None = None):
+    """depth.rs:1081 `wls_solve`: (u, rel, iters, device ms)."""
+    e = engine or default_engine()
+    d, conf, guide = (np.ascontiguousarray(x, dtype=np.float32) for x in (d, conf, guide))
+    h, w = d.shape
+    u = np.empty_like(d)
+    rel, it, ms = C.c_float(0), C.c_uint32(0), C.c_double(0)
+    check(e._L.lsb_wls_solve(e._h, C.c_void_p(d.ctypes.data), C.c_void_p(conf.ctypes.data), C.c_void_p(guide.ctypes.data), w, h,
+                             lam, sigma_c, max_iters, edge_mode, vcycle_mode, C.c_void_p(u.ctypes.data), C.byref(rel),
+                             C.byref(it), C.byref(ms)))
+    return u, rel.value, it.value, ms.value
+
+
+def multiscale_align(rf, tg, init=None, free=None, coarsen=0, engine: Engine | None = None):
+    """align.rs:896 `multiscale_align` of luma plane tg onto rf: (Sim vector, evaluations)."""
+    e = engine or default_engine()
+    rf, tg = (np.ascontiguousarray(x, dtype=np.float32) for x in (rf, tg))
+    h, w = rf.shape
+    init = np.asarray(init if init is not None else [0, 0, 1, 0, 1, 0, 0, 0], np.float64)
+    fr = np.asarray(free if free is not None else AlignParams().free(), np.uint8)
+    out = np.empty(8, np.float64)
+    ev = C.c_uint32(0)
+    check(e._L.lsb_align_pair(e._h, C.c_void_p(rf.ctypes.data), C.c_void_p(tg.ctypes.data), w, h, C.c_void_p(init.ctypes.data),
+                              C.c_void_p(fr.ctypes.data), coarsen, C.c_void_p(out.ctypes.data), C.byref(ev)))
+    return out, ev.value
+
+
+def warp_cost(rf, tgt, sim, engine: Engine | None = None):
+    """align.rs:581 `warp_cost` on the device."""
+    e = engine or default_engine()
+    rf, tgt = (np.ascontiguousarray(x, dtype=np.float32) for x in (rf, tgt))
+    s = np.asarray(sim, np.float64)
+    out = C.c_double(0)
+    check(e._L.lsb_warp_cost(e._h, C.c_void_p(rf.ctypes.data), rf.shape[1], rf.shape[0], C.c_void_p(tgt.ctypes.data), tgt.shape[1],
+                             tgt.shape[0], C.c_void_p(s.ctypes.data), C.byref(out)))
+    return out.value
+
+
+# ---------------------------------------------------------------- synthetic
+@dataclass
+class SynthSpec:
+    """A seeded synthetic focus stack (the benchmark inputs)."""
+    w: int
+    h: int
+    n: int
+    seed: int = 0x1A957ACC
+    mag_step: float = 0.002
+    noise_std: float = 0.003
+    blur_px: float = 6.0
+    warp: bool = False
+    warp_scale: float = 0.004
+    warp_rot_deg: float = 0.2
+    warp_shift: float = 8.0
+
+    def c(self):
+        return SynthDesc(self.w, self.h, self.n, int(self.warp), self.seed, self.mag_step, self.noise_std, self.blur_px,
+                         self.warp_scale, self.warp_rot_deg, self.warp_shift)
+
+
+def synth_stack(spec: SynthSpec):
+    """(n, h, w, 3) uint16 frames made on the host (OpenMP) and the applied transforms (n, 4)."""
+    L = load()
+    out = np.empty((spec.n, spec.h, spec.w, 3), np.uint16)
+    truth = np.empty((spec.n, 4), np.float64)
+    d = spec.c()
+    err = L.lsb_synth_stack_host(C.byref(d), C.c_void_p(out.ctypes.data), C.c_void_p(truth.ctypes.data))
+    if err:
+        raise LsbError(err.decode())
+    return out, truth
+
+
+def synth_stack_device(spec: SynthSpec, dst_ptr: int, stream=None):
+    """Generate the stack straight into device memory at dst_ptr ([n][h][w][3] u16)."""
+    L = load()
+    truth = np.empty((spec.n, 4), np.float64)
+    d = spec.c()
+    err = L.lsb_synth_stack_device(C.byref(d), C.c_void_p(dst_ptr), C.c_void_p(truth.ctypes.data), C.c_void_p(stream or 0))
+    if err:
+        raise LsbError(err.decode())
+    return truth

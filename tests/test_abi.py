@@ -1,0 +1,61 @@
+"""The C ABI library loads without a GPU and exports every entry point
+include/lapstack_b200.h declares; compute entry points fail loudly (no CPU
+fallback) when no CUDA device is present. CPU only."""
+import ctypes as C
+import os
+import re
+
+import numpy as np
+import pytest
+
+import lapstack_b200 as L
+from lapstack_b200 import _lib
+
+HEADER = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "include", "lapstack_b200.h")
+
+
+def declared():
+    src = open(HEADER).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return sorted(set(re.findall(r"\b(lsb_[a-z0-9_]+)\s*\(", src)))
+
+
+def test_header_declares_the_boundary():
+    names = declared()
+    for must in ["lsb_abi", "lsb_engine_create", "lsb_stack_begin", "lsb_stack_push_u16", "lsb_stack_push_f32",
+                 "lsb_stack_shares", "lsb_stack_finish", "lsb_result_free", "lsb_free_str", "lsb_engine_destroy",
+                 "lsb_depth_from_slices", "lsb_wls_solve", "lsb_align_pair", "lsb_warp_cost"]:
+        assert must in names
+
+
+def test_library_exports_every_declared_symbol():
+    lib = L.load()
+    for name in declared():
+        assert hasattr(lib, name), name
+    assert set(declared()) == set(_lib.SIGNATURES), "the ctypes table covers the header exactly"
+    assert lib.lsb_abi() == _lib.ABI_VERSION
+
+
+def test_no_cpu_fallback_without_a_device():
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a CUDA device is present")
+    with pytest.raises(L.LsbError, match="CUDA"):
+        L.Engine()
+
+
+def test_host_synthetic_stack_is_seeded():
+    a, ta = L.synth_stack(L.SynthSpec(96, 64, 3, seed=7))
+    b, tb = L.synth_stack(L.SynthSpec(96, 64, 3, seed=7))
+    c, _ = L.synth_stack(L.SynthSpec(96, 64, 3, seed=8))
+    assert a.shape == (3, 64, 96, 3) and a.dtype == np.uint16
+    assert np.array_equal(a, b) and np.array_equal(ta, tb)
+    assert not np.array_equal(a, c)
+    m = a.astype(np.float64) / 65535
+    assert 0.35 < m.mean() < 0.55 and 0.05 < m.std() < 0.3
+
+
+def test_warped_synthetic_stack_records_its_transforms():
+    _, t = L.synth_stack(L.SynthSpec(96, 64, 4, warp=True, mag_step=0.0))
+    assert np.allclose(t[0], [1, 0, 0, 0])
+    assert np.all(np.abs(t[1:, 0] - 1) <= 0.004 + 1e-12) and np.all(np.abs(t[1:, 2:]) <= 8.0)
