@@ -1,0 +1,338 @@
+#!/usr/bin/env python
+"""Benchmark: stack MP-frames/s (align + fuse + depth) on seeded synthetic stacks.
+
+One step = the whole stacking path over one stack: registration of every
+frame to the previous aligned one (Nelder-Mead on the device cost), the
+brightness gains, the level-by-level fold over all frames, the residual
+rule and collapse, and the depth pass (guided-filter aggregation, peaks,
+median, WLS, upsampling). `value` times steps whose 16-bit frames are
+already in HBM; `e2e` times the public API (Stack.push_u16 from pinned host
+memory, Stack.finish reading the results back) per step.
+
+Workloads (seeded synthetic stacks with the shapes of the reference's
+published runs):
+  c3  100 x 8256x5504 RGB u16, per-frame similarity warps, alignment at
+      coarsen 3, 7 levels, 16-bit (UNORM16) pyramid storage   [default]
+  c2  30 x 6000x4000, no alignment, 8 levels, aggregation radius 8, FP32
+  c1  8 x 1024x768, no alignment, 6 levels, FP32
+
+--impl reference times the CPU restatement of the reference's path (the
+oracle; the Rust reference cannot be built here) on a bounded sample of the
+same workload with all host threads.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "stack MP-frames/s (align+fuse+depth)"
+UNIT = "MP-frames/s"
+# the reference's CUDA run of 100 x 45.7 MP frames (RTX 3060), 26 s wall
+PUBLISHED_MPFS = 175.8
+
+CONFIGS = {
+    "c3": dict(w=8256, h=5504, n=100, warp=True, mag_step=0.0, noise_std=0.002, levels=0, align=True, coarsen=3,
+               agg_radius=3, storage="unorm16", sample=2),
+    "c2": dict(w=6000, h=4000, n=30, warp=False, mag_step=0.001, noise_std=0.002, levels=8, align=False, coarsen=0,
+               agg_radius=8, storage="f32", sample=2),
+    "c1": dict(w=1024, h=768, n=8, warp=False, mag_step=0.002, noise_std=0.003, levels=6, align=False, coarsen=0,
+               agg_radius=3, storage="f32", sample=8),
+}
+
+
+def params_of(cfg, mod):
+    fuse = mod.FuseParams(levels=cfg["levels"])
+    align = mod.AlignParams(coarsen=cfg["coarsen"]) if cfg["align"] else None
+    depth = mod.DepthParams(agg_radius=cfg["agg_radius"])
+    return fuse, align, depth
+
+
+def workload_name(c, name):
+    return (f"{name}: {c['n']} x {c['w']}x{c['h']} RGB u16 seeded synthetic focus stack"
+            f"{', per-frame similarity warps, alignment coarsen ' + str(c['coarsen']) if c['align'] else ', no alignment'}, "
+            f"{'auto' if not c['levels'] else c['levels']} levels, guided-filter DfF r={c['agg_radius']}, WLS MG-PCG, "
+            f"{c['storage']} pyramid storage")
+
+
+def spec_of(c, n=None, seed=0x1A957ACC):
+    import lapstack_b200 as L
+    return L.SynthSpec(c["w"], c["h"], n or c["n"], seed=seed, mag_step=c["mag_step"], noise_std=c["noise_std"],
+                       warp=c["warp"])
+
+
+# ------------------------------------------------------------------ clocks
+class Clocks:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index, self.p, self.path = index, None, f"/tmp/lsb_clocks_{os.getpid()}.csv"
+
+    def __enter__(self):
+        try:
+            self.f = open(self.path, "w")
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                       "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+        return self
+
+    def __exit__(self, *a):
+        if self.p:
+            self.p.terminate()
+            try:
+                self.p.wait(5)
+            except Exception:
+                self.p.kill()
+            self.f.close()
+
+    def summary(self):
+        try:
+            rows = [r.split(",") for r in open(self.path).read().strip().splitlines() if r.strip()]
+        except Exception:
+            return None
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows]
+        mx = max(float(r[2]) for r in rows)
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].strip().lower() == "active"})
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": reasons, "samples": len(rows)}
+
+
+# ------------------------------------------------------------- reference
+def run_oracle(frames, c, threads=None):
+    from oracle import oracle as O
+    fuse, align, depth = params_of(c, O)
+    sp = O.StackParams(fuse=fuse, align=align, depth=depth)
+    t0 = time.perf_counter()
+    O.run_stack(frames, sp)
+    return time.perf_counter() - t0
+
+
+def sample_frames(c):
+    """A bounded sample of the workload: c['sample'] frames of the same size and recipe."""
+    import lapstack_b200 as L
+    n = c["sample"]
+    spec = spec_of(c, n=n, seed=0x1A957ACC ^ 0x5A)
+    try:
+        import torch
+        if torch.cuda.is_available():
+            buf = torch.empty((n, c["h"], c["w"], 3), dtype=torch.int16, device="cuda")
+            L.synth_stack_device(spec, buf.data_ptr())
+            torch.cuda.synchronize()
+            return buf.cpu().numpy().view(np.uint16)
+    except Exception:
+        pass
+    return L.synth_stack(spec)[0]
+
+
+def cpu_baseline(c, frames=None):
+    frames = frames if frames is not None else sample_frames(c)
+    t = run_oracle(frames, c)
+    n = frames.shape[0]
+    mp = n * c["w"] * c["h"] / 1e6
+    return {"value": mp / t, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
+            "sample": f"{n} of the workload's frames ({c['w']}x{c['h']}), the whole path (align+fold+depth) in {t:.1f} s "
+                      f"on the oracle (C++ restatement of the reference's CPU path, OpenMP)"}
+
+
+def reference_arm(args, c, name):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    frames = sample_frames(c)
+    n = frames.shape[0]
+    mp = n * c["w"] * c["h"] / 1e6
+    for _ in range(args.warmup):
+        run_oracle(frames, c)
+    ts = [run_oracle(frames, c) for _ in range(args.steps)]
+    t = sum(ts) / len(ts)
+    v = mp / t
+    line = {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": t * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": v / PUBLISHED_MPFS,
+            "dtype": "f32", "data": "synthetic (seeded)", "impl": "reference",
+            "config": {"workload": workload_name(c, name), "sample_frames": n},
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
+                             "sample": f"{n} frames of {c['w']}x{c['h']}, whole path per step"},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ------------------------------------------------------------------- ours
+def traffic_per_px_frame(name):
+    """DRAM bytes per pixel-frame of the level-0 fold kernel from its committed ncu summary."""
+    p = os.path.join(ROOT, "profiles", f"fold_level0_{name}.md")
+    try:
+        for line in open(p):
+            if line.startswith("TRAFFIC_BYTES_PER_PIXEL_FRAME"):
+                return float(line.split("=")[1])
+    except Exception:
+        return None
+    return None
+
+
+def peaks():
+    try:
+        return json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))), "measured"
+    except Exception:
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "fallback"
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--config", default="c3", choices=sorted(CONFIGS))
+    ap.add_argument("--storage", default=None, choices=["f32", "unorm16", "f16"])
+    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    c = dict(CONFIGS[args.config])
+    if args.storage:
+        c["storage"] = args.storage
+    if args.impl == "reference":
+        return reference_arm(args, c, args.config)
+
+    import torch
+    import lapstack_b200 as L
+
+    rank, world = int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+
+    def barrier():
+        if dist:
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if not dist:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    eng = L.Engine(device=local, storage=c["storage"])
+    fuse, align, depth = params_of(c, L)
+    W, H, N = c["w"], c["h"], c["n"]
+    st = eng.stack(W, H, N, fuse, align, depth)
+    # independent stacks per rank (replicas): each its own seed
+    L.synth_stack_device(spec_of(c, seed=0x1A957ACC ^ rank), st.frames_device(), eng.stream)
+    st.set_count(N)
+    stream = torch.cuda.ExternalStream(eng.stream)
+
+    for _ in range(args.warmup):
+        st.run()
+    l0 = L.load().lsb_launch_count()
+    stages = []
+    barrier()
+    torch.cuda.synchronize()
+    with Clocks(local) as clk:
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            stages.append(st.run())
+        e1.record(stream)
+        e1.synchronize()
+    torch.cuda.synchronize()
+    barrier()
+    launches = L.load().lsb_launch_count() - l0
+    ms = max_over_ranks(e0.elapsed_time(e1) / args.steps)
+    mp_step = N * W * H / 1e6
+    value = world * mp_step / (ms / 1e3)
+    fold0 = statistics.mean(s["fold_level0"] for s in stages)
+    stage_ms = {k: statistics.mean(s[k] for s in stages) for k in stages[0]}
+
+    # ---- end to end through the public API: pinned host frames in, results out
+    host = torch.empty((N, H, W, 3), dtype=torch.int16, pin_memory=True)
+    host.copy_(_frames_tensor(st, N, H, W))
+    hnp = host.numpy().view(np.uint16)
+    e2e_ms = []
+    for _ in range(max(1, args.e2e_steps)):
+        barrier()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        st.set_count(0)
+        for k in range(N):
+            st.push_u16(hnp[k])
+        out = st.finish()
+        torch.cuda.synchronize()
+        e2e_ms.append(max_over_ranks((time.perf_counter() - t0) * 1e3))
+    e2e_t = statistics.median(e2e_ms)
+    h2d = N * W * H * 6
+    m = out.depth.dw * out.depth.dh if out.depth else 0
+    d2h = W * H * (6 + 12 + 4) + (W * H * 8 + m * 4 if out.depth else 0)
+
+    if rank == 0:
+        pk, pk_kind = peaks()
+        gs = {"f32": 4, "unorm16": 2, "f16": 2}[c["storage"]]
+        ss = gs  # slices share the storage width
+        bk = 1 << depth.scale
+        # level-0 fold: the u16 frames read once, G_1 written once, the focus slice written once,
+        # the level's accumulator (3 x f32 + best f32) written once
+        alg_bytes = N * W * H * (6 + 3 * gs / 4 + ss / (bk * bk)) + W * H * 16
+        achieved = alg_bytes / (fold0 / 1e3) / 1e9
+        tr = traffic_per_px_frame(args.config)
+        cb = None
+        if not args.no_cpu_baseline:
+            try:
+                cb = cpu_baseline(c)
+            except Exception as ex:  # the baseline is reported, never the product
+                cb = {"value": None, "unit": UNIT, "cores": os.cpu_count(), "kind": "port", "sample": f"failed: {ex}"}
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": value / PUBLISHED_MPFS,
+            "dtype": "f32", "data": "synthetic (seeded generator: height field, band-limited texture, per-pixel defocus)",
+            "config": {"workload": workload_name(c, args.config), "global_batch": N * world, "parallelism": f"replicas x{world}",
+                       "l2": "inputs (frames) larger than L2 every step"},
+            "e2e": {"value": world * mp_step / (e2e_t / 1e3), "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                    "ms_per_step": e2e_t},
+            "gpu_launches": launches,
+            "roofline": {"bound": "hbm", "kernel": "fold_level_kernel (level 0)", "achieved": achieved,
+                         "peak": pk["hbm_gbs"], "unit": "GB/s", "frac": achieved / pk["hbm_gbs"], "peak_kind": pk_kind,
+                         "traffic": (tr * N * W * H if tr else None), "algorithmic_bytes": alg_bytes, "kernel_ms": fold0},
+            "stages_ms": stage_ms,
+            "align_evals": out.align_evals,
+            "wls": {"iters": out.depth.wls_iters if out.depth else 0, "rel": out.depth.wls_rel if out.depth else 0.0},
+            "cpu_baseline": cb,
+            "clocks": clk.summary(),
+        }
+        print(json.dumps(line), flush=True)
+    st.close()
+    eng.close()
+    if dist:
+        dist.destroy_process_group()
+    return 0
+
+
+def _frames_tensor(st, n, h, w):
+    """The stack's device frame store as a torch tensor (no copy)."""
+    import torch
+
+    class _Cuda:
+        def __init__(self, ptr, shape):
+            self.__cuda_array_interface__ = {"data": (ptr, False), "shape": shape, "typestr": "<i2", "version": 3}
+    return torch.as_tensor(_Cuda(st.frames_device(), (n, h, w, 3)), device="cuda")
+
+
+if __name__ == "__main__":
+    sys.exit(main())

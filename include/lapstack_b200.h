@@ -50,7 +50,8 @@ typedef void (*lsb_log_fn)(const char* line, void* user);
 
 typedef struct {
     int32_t device;        /* CUDA device ordinal */
-    int32_t fp16_storage;  /* store pyramid levels >= 1 and the focus slices in FP16 */
+    int32_t storage;       /* Gaussian levels >= 1 and focus slices: 0 FP32 (bit-exact with the reference
+                              FP32 path); 1 16-bit: UNORM16 levels, FP16 slices; 2 FP16 levels and slices */
     int32_t grid_limit;    /* CTAs of the persistent kernels; 0 = 2 x the SM count */
     int32_t reserved;
     lsb_log_fn log;        /* optional progress lines (stack.rs:1014 `log`) */
@@ -114,7 +115,8 @@ typedef struct {
     float floor_value, p90, wls_rel;
     uint32_t wls_iters, wls_iters_first, align_evals;
     double wls_rel64;
-    double ms[8];        /* device time per stage: align, gains, fold, residual+collapse, focus agg, wls, upsample, total */
+    double ms[12];       /* device ms per stage: align, gains, fold, residual+collapse, focus agg, wls, upsample,
+                            total, fold level 0; 3 spare */
 } lsb_result;
 
 /* Seeded synthetic stack description (no reference counterpart; the benchmark inputs). */
@@ -132,6 +134,8 @@ typedef struct {
 
 uint32_t lsb_abi(void);
 void lsb_free_str(char* s);
+/* Kernel launches the library has issued since it was loaded. */
+uint64_t lsb_launch_count(void);
 
 char* lsb_engine_create(const lsb_config* cfg, lsb_engine** out);
 void lsb_engine_destroy(lsb_engine* e);
@@ -154,7 +158,7 @@ char* lsb_stack_shares(lsb_stack* s, float* out_n);
 /* Align, fold, depth: the whole pipeline over the frames pushed; may be called again. */
 char* lsb_stack_finish(lsb_stack* s, lsb_result* out);
 /* lsb_stack_finish without copying results back (device-resident benchmarking). */
-char* lsb_stack_run(lsb_stack* s, double* ms_out8);
+char* lsb_stack_run(lsb_stack* s, double* ms_out12);
 void lsb_stack_destroy(lsb_stack* s);
 void lsb_result_free(lsb_result* r);
 

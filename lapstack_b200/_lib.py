@@ -25,7 +25,7 @@ LOG_FN = C.CFUNCTYPE(None, C.c_char_p, C.c_void_p)
 
 
 class Config(C.Structure):
-    _fields_ = [("device", C.c_int32), ("fp16_storage", C.c_int32), ("grid_limit", C.c_int32), ("reserved", C.c_int32),
+    _fields_ = [("device", C.c_int32), ("storage", C.c_int32), ("grid_limit", C.c_int32), ("reserved", C.c_int32),
                 ("log", LOG_FN), ("user", C.c_void_p)]
 
 
@@ -54,7 +54,7 @@ class Result(C.Structure):
                 ("floor_cells", C.POINTER(C.c_float)), ("sims", C.POINTER(C.c_double)), ("gains", C.POINTER(C.c_float)),
                 ("shares", C.POINTER(C.c_float)), ("crop", C.c_uint32 * 4), ("floor_value", C.c_float), ("p90", C.c_float),
                 ("wls_rel", C.c_float), ("wls_iters", C.c_uint32), ("wls_iters_first", C.c_uint32),
-                ("align_evals", C.c_uint32), ("wls_rel64", C.c_double), ("ms", C.c_double * 8)]
+                ("align_evals", C.c_uint32), ("wls_rel64", C.c_double), ("ms", C.c_double * 12)]
 
 
 class SynthDesc(C.Structure):
@@ -70,6 +70,7 @@ ERR = C.c_void_p  # char* owned by the library until lsb_free_str
 SIGNATURES = {
     "lsb_abi": (C.c_uint32, []),
     "lsb_free_str": (None, [P]),
+    "lsb_launch_count": (C.c_uint64, []),
     "lsb_engine_create": (ERR, [C.POINTER(Config), C.POINTER(P)]),
     "lsb_engine_destroy": (None, [P]),
     "lsb_engine_stream": (P, [P]),

@@ -209,7 +209,7 @@ static int gsz(size_t n) { return (int)std::min<size_t>((n + 255) / 256, 148 * 1
 
 cudaError_t luma_u16(const uint16_t* f, int w, int h, float* y, cudaStream_t s) {
     size_t n = (size_t)w * h;
-    luma_u16_kernel<<<gsz(n), 256, 0, s>>>(f, n, y);
+    lsb_launched(), luma_u16_kernel<<<gsz(n), 256, 0, s>>>(f, n, y);
     return cudaGetLastError();
 }
 
@@ -230,7 +230,7 @@ cudaError_t gauss_levels(const float* y, int w, int h, const std::vector<float*>
     int cw = w, ch = h;
     for (size_t l = 0; l < dims.size() && l < lv.size(); l++) {
         dim3 b(32, 8), g((dims[l].first + 31) / 32, (dims[l].second + 7) / 8);
-        reduce_burt_kernel<<<g, b, 0, s>>>(src, cw, ch, lv[l], dims[l].first, dims[l].second);
+        lsb_launched(), reduce_burt_kernel<<<g, b, 0, s>>>(src, cw, ch, lv[l], dims[l].first, dims[l].second);
         src = lv[l];
         cw = dims[l].first;
         ch = dims[l].second;
@@ -240,7 +240,7 @@ cudaError_t gauss_levels(const float* y, int w, int h, const std::vector<float*>
 
 cudaError_t warp_plane(const float* src, int w, int h, const WarpXform& xf, float* out, cudaStream_t s) {
     dim3 b(32, 8), g((w + 31) / 32, (h + 7) / 8);
-    warp_plane_kernel<<<g, b, 0, s>>>(src, w, h, xf, out);
+    lsb_launched(), warp_plane_kernel<<<g, b, 0, s>>>(src, w, h, xf, out);
     return cudaGetLastError();
 }
 
@@ -248,7 +248,7 @@ cudaError_t bright_sums(const uint16_t* frames, int n, int w, int h, const Brigh
                         cudaStream_t s) {
     if (n < 2) return cudaSuccess;
     dim3 g(nparts, n - 1);
-    bright_kernel<<<g, 128, 0, s>>>(frames, w, h, xf_dev, interp, nparts, part);
+    lsb_launched(), bright_kernel<<<g, 128, 0, s>>>(frames, w, h, xf_dev, interp, nparts, part);
     return cudaGetLastError();
 }
 
@@ -319,8 +319,8 @@ static cudaError_t eval_batch(AlignCtx& C, const float* rf, int aw, int ah, cons
         const size_t npx = (size_t)aw * ah;
         const int nblocks = (int)std::min<size_t>(std::max<size_t>((npx + 255) / 256, 1), 296);
         dim3 g(nblocks, nc);
-        cost_kernel<<<g, 256, 0, C.s>>>(rf, aw, ah, tg, tw, th, cb, C.part);
-        cost_final_kernel<<<1, 32, 0, C.s>>>(C.part, nblocks, nc, C.sums_dev);
+        lsb_launched(), cost_kernel<<<g, 256, 0, C.s>>>(rf, aw, ah, tg, tw, th, cb, C.part);
+        lsb_launched(), cost_final_kernel<<<1, 32, 0, C.s>>>(C.part, nblocks, nc, C.sums_dev);
         cudaMemcpyAsync(C.sums_host, C.sums_dev, sizeof(double) * 3 * nc, cudaMemcpyDeviceToHost, C.s);
         cudaError_t e = cudaStreamSynchronize(C.s);
         if (e != cudaSuccess) return e;

@@ -12,6 +12,7 @@
 
 #include <algorithm>
 #include <array>
+#include <atomic>
 #include <string>
 #include <vector>
 
@@ -21,6 +22,10 @@
 #include "lsb_internal.h"
 
 using namespace lsb;
+
+static std::atomic<unsigned long long> g_launches{0};
+void lsb_launched() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+extern "C" uint64_t lsb_launch_count(void) { return g_launches.load(); }
 
 static char* dup_err(const std::string& s) {
     char* p = (char*)malloc(s.size() + 1);
@@ -78,7 +83,8 @@ struct lsb_stack {
     lsb_fuse_params fp;
     lsb_align_params ap;
     lsb_depth_params dp;
-    bool brightness, crop, fp16, f32src;
+    bool brightness, crop, f32src;
+    int storage;  // lsb::Storage of the Gaussian levels >= 1 and the slices
     int levels, depth_level;
     std::vector<int> lw, lh;  // level dims 0..levels
     DevPool pool;
@@ -115,7 +121,7 @@ struct lsb_stack {
     float floor_v = 0.f, p90 = 0.f, rel = 0.f;
     double rel64 = 0.0;
     int iters = 0, iters_first = 0;
-    double ms[8] = {0};
+    double ms[12] = {0};
 };
 
 extern "C" {
@@ -170,7 +176,7 @@ void* lsb_engine_stream(lsb_engine* e) { return e ? (void*)e->s : nullptr; }
 
 }  // extern "C"
 
-static size_t gs_bytes(const lsb_stack* s) { return s->fp16 ? 2 : 4; }
+static size_t gs_bytes(const lsb_stack* s) { return s->storage == STORE_F32 ? 4 : 2; }
 
 // depth.rs:454 `rdf_taps` in depth.rs:417 `conv_sparse`'s per-pixel order
 static std::vector<float> focus_taps(uint32_t r_in, uint32_t r_out) {
@@ -233,7 +239,7 @@ static char* stack_alloc(lsb_stack* s) {
         s->dh = (int)((H + s->bk - 1) / s->bk);
         const size_t m = (size_t)s->dw * s->dh;
         void* p = nullptr;
-        TRY(cudaMalloc(&p, N * m * (s->fp16 ? 2 : 4)));
+        TRY(cudaMalloc(&p, N * m * gs_bytes(s)));
         P.ptrs.push_back(p);
         s->slices = p;
         for (float** q : {&s->guide, &s->mi, &s->vi, &s->tmp, &s->draw, &s->dmed, &s->conf, &s->mins, &s->u, &s->w2, &s->t0,
@@ -280,7 +286,11 @@ extern "C" char* lsb_stack_begin(lsb_engine* e, uint32_t w, uint32_t h, uint32_t
     s->dp = depth ? *depth : lsb_depth_params{};
     s->brightness = brightness != 0;
     s->crop = crop != 0;
-    s->fp16 = e->cfg.fp16_storage != 0;
+    s->storage = e->cfg.storage;
+    if (s->storage < 0 || s->storage > 2) {
+        delete s;
+        return dup_err("storage must be 0 (FP32), 1 (UNORM16 levels, FP16 slices) or 2 (FP16)");
+    }
     s->f32src = false;
     if (s->fp.halo > 0.f) {
         delete s;
@@ -541,6 +551,12 @@ static char* run_pipeline(lsb_stack* s) {
         std::vector<float> taps = focus_taps(s->dp.r_in, s->dp.r_out);
         TRY(set_focus_taps(taps.data(), (int)(taps.size() / 3), st));
     }
+    // the fixed-point storage spans [0, the largest gain]: every Gaussian level
+    // is a convex combination of gained inputs in [0, 1]
+    float maxg = 1.f;
+    for (float g : s->gains) maxg = std::max(maxg, g);
+    if (s->f32src) maxg = 1.f;
+    const float gscale = (float)(65535.0 / maxg), ginv = (float)(maxg / 65535.0);
     for (int l = 0; l < s->levels; l++) {
         FoldArgs a{};
         a.level = l;
@@ -573,8 +589,12 @@ static char* run_pipeline(lsb_stack* s) {
             a.sml_step = (int)s->dp.sml_step;
             a.ntaps = (int)focus_taps(s->dp.r_in, s->dp.r_out).size() / 3;
         }
+        a.gscale = gscale;
+        a.ginv = ginv;
         const int src = l > 0 ? SRC_G : (s->f32src ? SRC_F32 : SRC_U16);
-        TRY(fold_level(a, src, s->fp16, (int)s->fp.energy_radius, focus, s->fp16, st, e->grid));
+        if (l == 0) TRY(cudaEventRecord(ev[8], st));
+        TRY(fold_level(a, src, s->storage, (int)s->fp.energy_radius, focus, st, e->grid));
+        if (l == 0) TRY(cudaEventRecord(ev[9], st));
     }
     TRY(cudaEventRecord(ev[3], st));
     // ---- residual, collapse
@@ -585,8 +605,8 @@ static char* run_pipeline(lsb_stack* s) {
         const float inv_n = 1.0f / (float)nwin;
         for (int c = 1; c <= nwin; c++) lnp[c] = logf((float)c * inv_n);
         TRY(cudaMemcpyAsync(s->lnp, lnp.data(), sizeof(float) * 128, cudaMemcpyHostToDevice, st));
-        ResidualArgs ra{s->g[s->levels], n, wt, ht, (int)s->fp.top_rule, r, (int)s->fp.entropy_bins, s->dev_s, s->ent_s, s->top};
-        TRY(fuse_residuals(ra, s->fp16, s->lnp, st));
+        ResidualArgs ra{s->g[s->levels], n, wt, ht, (int)s->fp.top_rule, r, (int)s->fp.entropy_bins, s->dev_s, s->ent_s, s->top, ginv};
+        TRY(fuse_residuals(ra, s->storage, s->lnp, st));
         const float* coarse = s->top;
         for (int l = s->levels - 1; l >= 0; l--) {
             // even levels land in img, odd ones in img_tmp: a level never overwrites its coarser input
@@ -604,7 +624,7 @@ static char* run_pipeline(lsb_stack* s) {
         TRY(luma_and_guide(s->img, W, H, k, s->yfull, s->guide, dw, dh, st));
         if (s->dp.agg_radius > 0) gf_stats(s->guide, dw, dh, (int)s->dp.agg_radius, s->tmp, s->mi, s->vi, st);
         AggArgs ag{s->slices, n, dw, dh, (int)s->dp.agg_radius, s->dp.agg_eps, s->guide, s->mi, s->vi, s->state, 0, 0};
-        TRY(aggregate_peaks(ag, s->fp16, st, e->grid));
+        TRY(aggregate_peaks(ag, s->storage != STORE_F32, st, e->grid));
         TRY(cudaEventRecord(ev[5], st));
         const size_t cnt = (m + 6) / 7;
         TRY(select_kth(s->state + 7 * m, cnt, 7, cnt / 2, e->hist, e->sel, e->scal + 0, st));
@@ -673,14 +693,15 @@ static char* run_pipeline(lsb_stack* s) {
     s->ms[5] = ms_between(ev[5], ev[6]);
     s->ms[6] = ms_between(ev[6], ev[7]);
     s->ms[7] = ms_between(ev[0], ev[7]);
+    s->ms[8] = ms_between(ev[8], ev[9]);
     return nullptr;
 }
 
-extern "C" char* lsb_stack_run(lsb_stack* s, double* ms_out8) {
+extern "C" char* lsb_stack_run(lsb_stack* s, double* ms_out12) {
     if (!s) return dup_err("null stack");
     char* err = run_pipeline(s);
     if (err) return err;
-    if (ms_out8) memcpy(ms_out8, s->ms, sizeof s->ms);
+    if (ms_out12) memcpy(ms_out12, s->ms, sizeof s->ms);
     return nullptr;
 }
 
@@ -843,7 +864,7 @@ extern "C" char* lsb_stack_finish(lsb_stack* s, lsb_result* r) {
 
 extern "C" void lsb_stack_destroy(lsb_stack* s) {
     if (!s) return;
-    cudaStreamSynchronize(s->e->s);
+    // cudaFree waits for the device; the engine (and its stream) may already be gone
     delete s;
 }
 
@@ -871,7 +892,7 @@ extern "C" char* lsb_depth_from_slices(lsb_engine* e, const float* slices, uint3
     dp.enabled = 1;
     lsb_stack* s = nullptr;
     lsb_config saved = e->cfg;
-    e->cfg.fp16_storage = 0;
+    e->cfg.storage = 0;
     char* err = lsb_stack_begin(e, w, h, n, &fp, nullptr, &dp, 0, 0, &s);
     e->cfg = saved;
     if (err) return err;

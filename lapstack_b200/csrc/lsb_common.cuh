@@ -11,6 +11,9 @@
 
 #define LSB_HD __host__ __device__ __forceinline__
 
+// Every kernel launch of the engine counts itself (lsb_launch_count in the C ABI).
+void lsb_launched();
+
 // Reflect-101 into [0, n) (pyramid.rs:51 `reflect`): period 2(n-1); n == 1 maps to 0.
 LSB_HD int lsb_reflect(int i, int n) {
     if (n == 1) return 0;
@@ -51,6 +54,40 @@ __device__ __forceinline__ float lsb_exp_even(float a, float b, float c) {
     return __fadd_rn(__fadd_rn(__fmul_rn(LSB_E0, a), __fmul_rn(LSB_E1, b)), __fmul_rn(LSB_E0, c));
 }
 __device__ __forceinline__ float lsb_exp_odd(float a, float b) { return __fmul_rn(LSB_OD, __fadd_rn(a, b)); }
+
+// 16-bit fixed point over [0, 1/inv]: the Gaussian levels are convex
+// combinations of 16-bit inputs, so UNORM16 keeps them at the inputs' own
+// quantisation step (IEEE half would round them to 11 bits).
+struct unorm16 {
+    uint16_t v;
+};
+
+// Load / store a pyramid sample in its storage type; `sc` = (scale, 1/scale)
+// of the fixed-point format (unused by the floating-point ones).
+template <class S>
+struct Store;
+template <>
+struct Store<float> {
+    static __device__ __forceinline__ float ld(const float* p, float2) { return *p; }
+    static __device__ __forceinline__ void st(float* p, float v, float2) { *p = v; }
+    static __device__ __forceinline__ float as_stored(float v, float2) { return v; }
+};
+template <>
+struct Store<__half> {
+    static __device__ __forceinline__ float ld(const __half* p, float2) { return __half2float(*p); }
+    static __device__ __forceinline__ void st(__half* p, float v, float2) { *p = __float2half_rn(v); }
+    static __device__ __forceinline__ float as_stored(float v, float2) { return __half2float(__float2half_rn(v)); }
+};
+template <>
+struct Store<unorm16> {
+    static __device__ __forceinline__ uint16_t enc(float v, float2 sc) {
+        return (uint16_t)fminf(fmaxf(__fadd_rn(__fmul_rn(v, sc.x), 0.5f), 0.f), 65535.f);
+    }
+    static __device__ __forceinline__ float dec(uint16_t u, float2 sc) { return __fmul_rn((float)u, sc.y); }
+    static __device__ __forceinline__ float ld(const unorm16* p, float2 sc) { return dec(p->v, sc); }
+    static __device__ __forceinline__ void st(unorm16* p, float v, float2 sc) { p->v = enc(v, sc); }
+    static __device__ __forceinline__ float as_stored(float v, float2 sc) { return dec(enc(v, sc), sc); }
+};
 
 template <class S>
 __device__ __forceinline__ float lsb_ld(const S* p);

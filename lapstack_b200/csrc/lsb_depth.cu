@@ -69,8 +69,8 @@ __global__ void box_v_kernel(const float* __restrict__ hs, float* __restrict__ o
 
 static void box_mean(const float* a, const float* b, float* tmp, float* out, int w, int h, int r, cudaStream_t s) {
     dim3 blk(128), g((w + 127) / 128, h);
-    box_h_kernel<<<g, blk, 0, s>>>(a, b, tmp, w, h, r);
-    box_v_kernel<<<g, blk, 0, s>>>(tmp, out, w, h, r);
+    lsb_launched(), box_h_kernel<<<g, blk, 0, s>>>(a, b, tmp, w, h, r);
+    lsb_launched(), box_v_kernel<<<g, blk, 0, s>>>(tmp, out, w, h, r);
 }
 
 // depth.rs:363 GuidedFilter::new: var_i = max(mean(I*I) - mean_i^2, 0)
@@ -93,7 +93,7 @@ static int grid1(size_t n) { return (int)std::min<size_t>((n + 255) / 256, 148 *
 void gf_stats(const float* guide, int w, int h, int r, float* tmp, float* mean_i, float* var_i, cudaStream_t s) {
     box_mean(guide, nullptr, tmp, mean_i, w, h, r, s);
     box_mean(guide, guide, tmp, var_i, w, h, r, s);
-    gf_var_kernel<<<grid1((size_t)w * h), 256, 0, s>>>(mean_i, var_i, (size_t)w * h);
+    lsb_launched(), gf_var_kernel<<<grid1((size_t)w * h), 256, 0, s>>>(mean_i, var_i, (size_t)w * h);
 }
 
 // depth.rs:379 `coeffs_into` for one plane p: a-bar into abar, b-bar into bbar.
@@ -102,7 +102,7 @@ void gf_coeffs(const float* guide, const float* mean_i, const float* var_i, cons
     size_t n = (size_t)w * h;
     box_mean(p, nullptr, tmp, t0, w, h, r, s);    // mean_p
     box_mean(guide, p, tmp, t1, w, h, r, s);      // corr_Ip (I*p formed inside)
-    gf_ab_kernel<<<grid1(n), 256, 0, s>>>(t0, t1, mean_i, var_i, eps, t2, t1, n);  // a -> t2, b -> t1
+    lsb_launched(), gf_ab_kernel<<<grid1(n), 256, 0, s>>>(t0, t1, mean_i, var_i, eps, t2, t1, n);  // a -> t2, b -> t1
     box_mean(t2, nullptr, tmp, abar, w, h, r, s);
     box_mean(t1, nullptr, tmp, bbar, w, h, r, s);
 }
@@ -286,8 +286,8 @@ size_t aggregate_smem_bytes(int r) {
 cudaError_t aggregate_peaks(AggArgs a, bool slice_fp16, cudaStream_t s, int grid_limit) {
     size_t m = (size_t)a.dw * a.dh;
     if (a.r == 0) {
-        if (slice_fp16) peaks_raw_kernel<__half><<<grid1(m), 256, 0, s>>>((const __half*)a.slices, a.n, m, a.state);
-        else peaks_raw_kernel<float><<<grid1(m), 256, 0, s>>>((const float*)a.slices, a.n, m, a.state);
+        if (slice_fp16) lsb_launched(), peaks_raw_kernel<__half><<<grid1(m), 256, 0, s>>>((const __half*)a.slices, a.n, m, a.state);
+        else lsb_launched(), peaks_raw_kernel<float><<<grid1(m), 256, 0, s>>>((const float*)a.slices, a.n, m, a.state);
         return cudaGetLastError();
     }
     const int TWD = a.r <= 4 ? 64 : 32, THD = 32;
@@ -302,7 +302,7 @@ cudaError_t aggregate_peaks(AggArgs a, bool slice_fp16, cudaStream_t s, int grid
         auto k = aggregate_kernel<TWV, 32, SST>;                                                           \
         e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);               \
         if (e != cudaSuccess) return e;                                                                    \
-        k<<<grid, 256, smem, s>>>(a);                                                                      \
+        lsb_launched(), k<<<grid, 256, smem, s>>>(a);                                                                      \
     }
     if (TWD == 64) {
         if (slice_fp16) LAUNCH_AGG(64, __half) else LAUNCH_AGG(64, float)
@@ -356,12 +356,12 @@ __global__ void set_rank_kernel(unsigned* sel, unsigned rank) { sel[1] = rank; }
 cudaError_t select_kth(const float* v, size_t cnt, int stride, size_t rank, unsigned* hist, unsigned* sel, float* out,
                        cudaStream_t s) {
     cudaMemsetAsync(hist, 0, sizeof(unsigned) * 65536, s);
-    set_rank_kernel<<<1, 1, 0, s>>>(sel, (unsigned)rank);
-    hist_kernel<<<grid1(cnt), 256, 0, s>>>(v, cnt, stride, hist, sel, 0);
-    scan_kernel<<<1, 1024, 0, s>>>(hist, sel, 0, out);
+    lsb_launched(), set_rank_kernel<<<1, 1, 0, s>>>(sel, (unsigned)rank);
+    lsb_launched(), hist_kernel<<<grid1(cnt), 256, 0, s>>>(v, cnt, stride, hist, sel, 0);
+    lsb_launched(), scan_kernel<<<1, 1024, 0, s>>>(hist, sel, 0, out);
     cudaMemsetAsync(hist, 0, sizeof(unsigned) * 65536, s);
-    hist_kernel<<<grid1(cnt), 256, 0, s>>>(v, cnt, stride, hist, sel, 1);
-    scan_kernel<<<1, 1024, 0, s>>>(hist, sel, 1, out);
+    lsb_launched(), hist_kernel<<<grid1(cnt), 256, 0, s>>>(v, cnt, stride, hist, sel, 1);
+    lsb_launched(), scan_kernel<<<1, 1024, 0, s>>>(hist, sel, 1, out);
     return cudaGetLastError();
 }
 
@@ -398,7 +398,7 @@ __global__ void peak_finish_kernel(const float* __restrict__ S, size_t m, int n,
 }
 cudaError_t peak_finish(const float* state, size_t m, int n, const float* floor_p, float gate, float* depth, float* conf,
                         float* mins, cudaStream_t s) {
-    peak_finish_kernel<<<grid1(m), 256, 0, s>>>(state, m, n, floor_p, gate, depth, conf, mins);
+    lsb_launched(), peak_finish_kernel<<<grid1(m), 256, 0, s>>>(state, m, n, floor_p, gate, depth, conf, mins);
     return cudaGetLastError();
 }
 
@@ -424,7 +424,7 @@ __global__ void median3_kernel(const float* __restrict__ src, float* __restrict_
 }
 cudaError_t median3(const float* src, float* out, int w, int h, cudaStream_t s) {
     dim3 b(32, 8), g((w + 31) / 32, (h + 7) / 8);
-    median3_kernel<<<g, b, 0, s>>>(src, out, w, h);
+    lsb_launched(), median3_kernel<<<g, b, 0, s>>>(src, out, w, h);
     return cudaGetLastError();
 }
 
@@ -436,7 +436,7 @@ __global__ void conf_scale_kernel(float* conf, size_t m, const float* p90) {
         conf[i] = fminf(__fdiv_rn(conf[i], p), 1.f);
 }
 cudaError_t conf_scale(float* conf, size_t m, const float* p90, cudaStream_t s) {
-    conf_scale_kernel<<<grid1(m), 256, 0, s>>>(conf, m, p90);
+    lsb_launched(), conf_scale_kernel<<<grid1(m), 256, 0, s>>>(conf, m, p90);
     return cudaGetLastError();
 }
 
@@ -447,7 +447,7 @@ __global__ void robust_kernel(const float* __restrict__ conf, const float* __res
         w2[i] = __fmul_rn(conf[i], fminf(__fdiv_rn(tau, fabsf(__fsub_rn(d[i], u[i]))), 1.f));
 }
 cudaError_t robust_weights(const float* conf, const float* d, const float* u, float tau, float* w2, size_t m, cudaStream_t s) {
-    robust_kernel<<<grid1(m), 256, 0, s>>>(conf, d, u, tau, w2, m);
+    lsb_launched(), robust_kernel<<<grid1(m), 256, 0, s>>>(conf, d, u, tau, w2, m);
     return cudaGetLastError();
 }
 
@@ -498,21 +498,21 @@ __global__ void apply_grid_kernel(const float* __restrict__ abar, const float* _
 cudaError_t upsample(const float* abar, const float* bbar, const float* yfull, const float* guide, const float* conf, int w,
                      int h, int dw, int dh, int k, float max_d, bool guided, float* depth, float* conf_full, cudaStream_t s) {
     if (k == 1) {
-        apply_grid_kernel<<<grid1((size_t)dw * dh), 256, 0, s>>>(abar, bbar, guide, (size_t)dw * dh, max_d, guided ? 1 : 0, depth);
+        lsb_launched(), apply_grid_kernel<<<grid1((size_t)dw * dh), 256, 0, s>>>(abar, bbar, guide, (size_t)dw * dh, max_d, guided ? 1 : 0, depth);
         cudaMemcpyAsync(conf_full, conf, sizeof(float) * dw * dh, cudaMemcpyDeviceToDevice, s);
         return cudaGetLastError();
     }
     dim3 b(32, 8), g((w + 31) / 32, (h + 7) / 8);
-    upsample_kernel<<<g, b, 0, s>>>(abar, bbar, yfull, conf, w, h, dw, dh, k, max_d, guided ? 1 : 0, depth, conf_full);
+    lsb_launched(), upsample_kernel<<<g, b, 0, s>>>(abar, bbar, yfull, conf, w, h, dw, dh, k, max_d, guided ? 1 : 0, depth, conf_full);
     return cudaGetLastError();
 }
 
 cudaError_t luma_and_guide(const float* img, int w, int h, int k, float* yfull, float* guide, int dw, int dh, cudaStream_t s) {
     size_t n = (size_t)w * h;
-    luma_kernel<<<grid1(n), 256, 0, s>>>(img, yfull, n);
+    lsb_launched(), luma_kernel<<<grid1(n), 256, 0, s>>>(img, yfull, n);
     if (k == 1) return cudaMemcpyAsync(guide, yfull, sizeof(float) * n, cudaMemcpyDeviceToDevice, s);
     dim3 b(32, 8), g((dw + 31) / 32, (dh + 7) / 8);
-    block_mean_kernel<<<g, b, 0, s>>>(yfull, w, h, k, guide, dw, dh);
+    lsb_launched(), block_mean_kernel<<<g, b, 0, s>>>(yfull, w, h, k, guide, dw, dh);
     return cudaGetLastError();
 }
 

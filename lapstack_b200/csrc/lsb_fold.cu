@@ -64,7 +64,7 @@ __global__ void __launch_bounds__(NT, 2) fold_level_kernel(const FoldArgs a) {
     float* lo = yb + YB_MAX;            // [3][TH][TW] L at the tile's own pixels
     const int tid = threadIdx.x;
     const int W = a.W, H = a.H, W1 = a.W1, H1 = a.H1;
-    const bool fp16g = sizeof(GS) == 2;
+    const float2 sc = make_float2(a.gscale, a.ginv);
 
     for (int tile = blockIdx.x; tile < a.ntiles; tile += gridDim.x) {
         const int x0 = (tile % a.tiles_x) * TW, y0 = (tile / a.tiles_x) * TH;
@@ -114,7 +114,7 @@ __global__ void __launch_bounds__(NT, 2) fold_level_kernel(const FoldArgs a) {
                 const GS* f = (const GS*)a.src_g + (size_t)k * 3 * W * H;
                 for (int c = 0; c < 3; c++)
                     for (int i = tid; i < gh * gw; i += NT)
-                        g0[c * G0_MAX + i] = lsb_ld<GS>(f + ((size_t)c * H + yG0 + i / gw) * W + xG0 + i % gw);
+                        g0[c * G0_MAX + i] = Store<GS>::ld(f + ((size_t)c * H + yG0 + i / gw) * W + xG0 + i % gw, sc);
             }
             __syncthreads();
 
@@ -186,10 +186,9 @@ __global__ void __launch_bounds__(NT, 2) fold_level_kernel(const FoldArgs a) {
                                        col[lsb_reflect(cc + 1, H) * aw], col[lsb_reflect(cc + 2, H) * aw]);
                     const int gx = xA0 + jx;
                     if (gx >= (x0 >> 1) && gx < ((x0 + TW) >> 1) && iy >= (y0 >> 1) && iy < ((y0 + TH) >> 1))
-                        lsb_st<GS>(dst + (size_t)iy * W1 + gx, v);
-                    // the coarse level as stored: with FP16 storage the next level sees the rounded value
-                    if (fp16g) v = __half2float(__float2half_rn(v));
-                    g1[i] = v;
+                        Store<GS>::st(dst + (size_t)iy * W1 + gx, v, sc);
+                    // the coarse level as stored: with 16-bit storage the next level sees the rounded value
+                    g1[i] = Store<GS>::as_stored(v, sc);
                 }
                 __syncthreads();
                 for (int i = tid; i < ah * lw; i += NT) {
@@ -287,40 +286,43 @@ static cudaError_t launch_fold(const FoldArgs& a, cudaStream_t s, int grid_limit
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     int grid = std::min(a.ntiles, std::max(grid_limit, 1));
-    k<<<grid, NT, smem, s>>>(a);
+    lsb_launched(), k<<<grid, NT, smem, s>>>(a);
     return cudaGetLastError();
 }
 
 template <int SRC, class GS, int R>
-static cudaError_t pick_focus(const FoldArgs& a, bool focus, bool slice_fp16, cudaStream_t s, int gl) {
+static cudaError_t pick_focus(const FoldArgs& a, bool focus, cudaStream_t s, int gl) {
     if (!focus) return launch_fold<SRC, GS, R, false, float>(a, s, gl);
-    return slice_fp16 ? launch_fold<SRC, GS, R, true, __half>(a, s, gl) : launch_fold<SRC, GS, R, true, float>(a, s, gl);
+    // 16-bit storage keeps the focus slices in FP16 (relative precision is what the peak search needs)
+    if (sizeof(GS) == 2) return launch_fold<SRC, GS, R, true, __half>(a, s, gl);
+    return launch_fold<SRC, GS, R, true, float>(a, s, gl);
 }
 
 template <int SRC, class GS>
-static cudaError_t pick_r(const FoldArgs& a, int r, bool focus, bool sf16, cudaStream_t s, int gl) {
+static cudaError_t pick_r(const FoldArgs& a, int r, bool focus, cudaStream_t s, int gl) {
     switch (r) {
-        case 0: return pick_focus<SRC, GS, 0>(a, focus, sf16, s, gl);
-        case 1: return pick_focus<SRC, GS, 1>(a, focus, sf16, s, gl);
-        case 2: return pick_focus<SRC, GS, 2>(a, focus, sf16, s, gl);
+        case 0: return pick_focus<SRC, GS, 0>(a, focus, s, gl);
+        case 1: return pick_focus<SRC, GS, 1>(a, focus, s, gl);
+        case 2: return pick_focus<SRC, GS, 2>(a, focus, s, gl);
         default: return cudaErrorInvalidValue;
     }
 }
 
-cudaError_t fold_level(const FoldArgs& a, int src_kind, bool fp16, int radius, bool focus, bool slice_fp16, cudaStream_t s,
-                       int grid_limit) {
-    if (a.ntiles <= 0) return cudaSuccess;
-    if (fp16) {
-        switch (src_kind) {
-            case SRC_U16: return pick_r<SRC_U16, __half>(a, radius, focus, slice_fp16, s, grid_limit);
-            case SRC_F32: return pick_r<SRC_F32, __half>(a, radius, focus, slice_fp16, s, grid_limit);
-            default: return pick_r<SRC_G, __half>(a, radius, false, slice_fp16, s, grid_limit);
-        }
-    }
+template <class GS>
+static cudaError_t pick_src(const FoldArgs& a, int src_kind, int r, bool focus, cudaStream_t s, int gl) {
     switch (src_kind) {
-        case SRC_U16: return pick_r<SRC_U16, float>(a, radius, focus, slice_fp16, s, grid_limit);
-        case SRC_F32: return pick_r<SRC_F32, float>(a, radius, focus, slice_fp16, s, grid_limit);
-        default: return pick_r<SRC_G, float>(a, radius, false, slice_fp16, s, grid_limit);
+        case SRC_U16: return pick_r<SRC_U16, GS>(a, r, focus, s, gl);
+        case SRC_F32: return pick_r<SRC_F32, GS>(a, r, focus, s, gl);
+        default: return pick_r<SRC_G, GS>(a, r, false, s, gl);
+    }
+}
+
+cudaError_t fold_level(const FoldArgs& a, int src_kind, int storage, int radius, bool focus, cudaStream_t s, int grid_limit) {
+    if (a.ntiles <= 0) return cudaSuccess;
+    switch (storage) {
+        case STORE_UNORM16: return pick_src<unorm16>(a, src_kind, radius, focus, s, grid_limit);
+        case STORE_F16: return pick_src<__half>(a, src_kind, radius, focus, s, grid_limit);
+        default: return pick_src<float>(a, src_kind, radius, focus, s, grid_limit);
     }
 }
 
@@ -345,7 +347,8 @@ __global__ void dev_ent_kernel(const ResidualArgs a, const float* __restrict__ l
         const int yy = lsb_reflect(i + dy, a.h);
         for (int dx = -r; dx <= r; dx++) {
             const int o = yy * a.w + lsb_reflect(j + dx, a.w);
-            const float v = lsb_luma(lsb_ld<GS>(t + o), lsb_ld<GS>(t + n2 + o), lsb_ld<GS>(t + 2 * n2 + o));
+            const float2 sc = make_float2(0.f, a.ginv);
+            const float v = lsb_luma(Store<GS>::ld(t + o, sc), Store<GS>::ld(t + n2 + o, sc), Store<GS>::ld(t + 2 * n2 + o, sc));
             s = __fadd_rn(s, v);
             s2 = __fadd_rn(s2, __fmul_rn(v, v));
             const float vc = fminf(fmaxf(v, 0.f), 1.f);
@@ -376,10 +379,11 @@ __global__ void pareto_kernel(const ResidualArgs a) {
     if (pix >= n2) return;
     float o[3] = {0.f, 0.f, 0.f};
     const GS* t = (const GS*)a.tops;
+    const float2 sc = make_float2(0.f, a.ginv);
     if (a.n == 1 || a.top_rule == 2) {
         const float inv = __fdiv_rn(1.f, (float)a.n);
         for (int k = 0; k < a.n; k++)
-            for (int c = 0; c < 3; c++) o[c] = __fadd_rn(o[c], __fmul_rn(lsb_ld<GS>(t + ((size_t)k * 3 + c) * n2 + pix), inv));
+            for (int c = 0; c < 3; c++) o[c] = __fadd_rn(o[c], __fmul_rn(Store<GS>::ld(t + ((size_t)k * 3 + c) * n2 + pix, sc), inv));
     } else {
         const bool ent = a.top_rule == 0;
         auto dominated = [&](int x) {
@@ -397,21 +401,22 @@ __global__ void pareto_kernel(const ResidualArgs a) {
         const float inv = __fdiv_rn(1.f, (float)max(kept, 1));
         for (int x = 0; x < a.n; x++)
             if (!dominated(x))
-                for (int c = 0; c < 3; c++) o[c] = __fadd_rn(o[c], __fmul_rn(lsb_ld<GS>(t + ((size_t)x * 3 + c) * n2 + pix), inv));
+                for (int c = 0; c < 3; c++) o[c] = __fadd_rn(o[c], __fmul_rn(Store<GS>::ld(t + ((size_t)x * 3 + c) * n2 + pix, sc), inv));
     }
     for (int c = 0; c < 3; c++) a.out[(size_t)c * n2 + pix] = o[c];
 }
 
-cudaError_t fuse_residuals(const ResidualArgs& a, bool fp16, const float* lnp, cudaStream_t s) {
+template <class GS>
+static void residual_launch(const ResidualArgs& a, const float* lnp, cudaStream_t s) {
     const int n2 = a.w * a.h;
-    if (a.n > 1 && a.top_rule != 2) {
-        if (a.radius > 4) return cudaErrorInvalidValue;
-        const int tot = a.n * n2;
-        if (fp16) dev_ent_kernel<__half><<<(tot + 127) / 128, 128, 0, s>>>(a, lnp);
-        else dev_ent_kernel<float><<<(tot + 127) / 128, 128, 0, s>>>(a, lnp);
-    }
-    if (fp16) pareto_kernel<__half><<<(n2 + 127) / 128, 128, 0, s>>>(a);
-    else pareto_kernel<float><<<(n2 + 127) / 128, 128, 0, s>>>(a);
+    if (a.n > 1 && a.top_rule != 2) lsb_launched(), dev_ent_kernel<GS><<<(a.n * n2 + 127) / 128, 128, 0, s>>>(a, lnp);
+    lsb_launched(), pareto_kernel<GS><<<(n2 + 127) / 128, 128, 0, s>>>(a);
+}
+cudaError_t fuse_residuals(const ResidualArgs& a, int storage, const float* lnp, cudaStream_t s) {
+    if (a.radius > 4) return cudaErrorInvalidValue;
+    if (storage == STORE_UNORM16) residual_launch<unorm16>(a, lnp, s);
+    else if (storage == STORE_F16) residual_launch<__half>(a, lnp, s);
+    else residual_launch<float>(a, lnp, s);
     return cudaGetLastError();
 }
 
@@ -451,7 +456,7 @@ __global__ void collapse_kernel(const float* __restrict__ acc, const float* __re
 cudaError_t collapse_level(const float* acc, const float* coarse, float* out, int w, int h, int cw, int ch, bool last,
                            uint16_t* rgb_out, cudaStream_t s) {
     dim3 b(32, 8), g((w + 31) / 32, (h + 7) / 8);
-    collapse_kernel<<<g, b, 0, s>>>(acc, coarse, out, w, h, cw, ch, last ? 1 : 0, rgb_out);
+    lsb_launched(), collapse_kernel<<<g, b, 0, s>>>(acc, coarse, out, w, h, cw, ch, last ? 1 : 0, rgb_out);
     return cudaGetLastError();
 }
 
@@ -473,8 +478,8 @@ cudaError_t winner_counts(const uint16_t* win, const float* best, int cells, int
     cudaMemsetAsync(mx, 0, sizeof(float), s);
     cudaMemsetAsync(counts, 0, sizeof(unsigned int) * frames, s);
     int g = std::min((cells + 255) / 256, 4096);
-    max_kernel<<<g, 256, 0, s>>>(best, cells, mx);
-    count_kernel<<<g, 256, 0, s>>>(win, best, cells, frames, mx, counts);
+    lsb_launched(), max_kernel<<<g, 256, 0, s>>>(best, cells, mx);
+    lsb_launched(), count_kernel<<<g, 256, 0, s>>>(win, best, cells, frames, mx, counts);
     return cudaGetLastError();
 }
 
@@ -513,9 +518,9 @@ __global__ void means_final_kernel(const double* partial, int n, int nparts, int
 }
 cudaError_t frame_means(const uint16_t* frames, int n, int w, int h, double* partial, int nparts, double* means, cudaStream_t s) {
     dim3 g(nparts, n);
-    means_partial_kernel<<<g, 256, 0, s>>>(frames, w, h, nparts, partial);
+    lsb_launched(), means_partial_kernel<<<g, 256, 0, s>>>(frames, w, h, nparts, partial);
     const int count = ((w + 3) / 4) * ((h + 3) / 4);
-    means_final_kernel<<<(n + 127) / 128, 128, 0, s>>>(partial, n, nparts, count, means);
+    lsb_launched(), means_final_kernel<<<(n + 127) / 128, 128, 0, s>>>(partial, n, nparts, count, means);
     return cudaGetLastError();
 }
 

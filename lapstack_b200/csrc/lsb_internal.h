@@ -47,11 +47,14 @@ struct FoldArgs {
     int sml_step;
     int ntaps;
     int* status;  // device error word
+    float gscale, ginv;  // the 16-bit fixed-point storage's scale and its inverse
 };
 
+// Storage of the Gaussian levels >= 1 and the focus slices.
+enum Storage { STORE_F32 = 0, STORE_UNORM16 = 1, STORE_F16 = 2 };
+
 // Launchers (lsb_fold.cu).
-cudaError_t fold_level(const FoldArgs& a, int src_kind, bool fp16, int radius, bool focus, bool slice_fp16,
-                       cudaStream_t s, int grid_limit);
+cudaError_t fold_level(const FoldArgs& a, int src_kind, int storage, int radius, bool focus, cudaStream_t s, int grid_limit);
 cudaError_t set_focus_taps(const float* taps3, int ntaps, cudaStream_t s);
 size_t fold_smem_bytes(int radius, bool focus);
 
@@ -63,8 +66,9 @@ struct ResidualArgs {
     float* dev;  // scratch [n][h][w]
     float* ent;  // scratch [n][h][w]
     float* out;  // [3][h][w]
+    float ginv;  // fixed-point storage inverse scale
 };
-cudaError_t fuse_residuals(const ResidualArgs& a, bool fp16, const float* lnp, cudaStream_t s);
+cudaError_t fuse_residuals(const ResidualArgs& a, int storage, const float* lnp, cudaStream_t s);
 
 // Collapse: out_l = acc_l + EXPAND(coarse) (pyramid.rs:219); at level 0 also clamp and pack.
 cudaError_t collapse_level(const float* acc, const float* coarse, float* out, int w, int h, int cw, int ch, bool last,

@@ -265,18 +265,18 @@ const char* lsb_synth_stack_device(const lsb_synth_desc* d, uint16_t* out_dev, d
         cudaMemcpyAsync(dp, hp, sizeof(SynthPlan), cudaMemcpyHostToDevice, s);
         unsigned init[2] = {0x7f7fffffu, 0u};
         cudaMemcpyAsync(mm, init, 8, cudaMemcpyHostToDevice, s);
-        zraw_kernel<<<gsz(n), 256, 0, s>>>(dp, z);
-        minmax_kernel<<<gsz(n), 256, 0, s>>>(z, n, mm);
-        znorm_kernel<<<gsz(n), 256, 0, s>>>(z, n, mm);
-        noise_kernel<<<gsz(3 * n), 256, 0, s>>>(dp, t);
+        lsb_launched(), zraw_kernel<<<gsz(n), 256, 0, s>>>(dp, z);
+        lsb_launched(), minmax_kernel<<<gsz(n), 256, 0, s>>>(z, n, mm);
+        lsb_launched(), znorm_kernel<<<gsz(n), 256, 0, s>>>(z, n, mm);
+        lsb_launched(), noise_kernel<<<gsz(3 * n), 256, 0, s>>>(dp, t);
         for (int j = 0; j < hp->nb; j++) {
             const float* src = j == 0 ? t : B;
             float* tmp = j == 0 ? B + 3 * n : t;  // scratch: level 1's slot (not yet written) / the spent noise
             float sc = j == 0 ? hp->tex_scale : 1.f, off = j == 0 ? 0.45f : 0.f;
-            blur_kernel<<<gsz(3 * n), 256, 0, s>>>(dp, src, tmp, j, 0, 1.f, 0.f);
-            blur_kernel<<<gsz(3 * n), 256, 0, s>>>(dp, tmp, B + (size_t)j * 3 * n, j, 1, sc, off);
+            lsb_launched(), blur_kernel<<<gsz(3 * n), 256, 0, s>>>(dp, src, tmp, j, 0, 1.f, 0.f);
+            lsb_launched(), blur_kernel<<<gsz(3 * n), 256, 0, s>>>(dp, tmp, B + (size_t)j * 3 * n, j, 1, sc, off);
         }
-        frames_kernel<<<gsz(n * hp->n * 3), 256, 0, s>>>(dp, *d, z, B, out_dev);
+        lsb_launched(), frames_kernel<<<gsz(n * hp->n * 3), 256, 0, s>>>(dp, *d, z, B, out_dev);
         if (cudaStreamSynchronize(s) != cudaSuccess) err = "synth: device generation failed";
     }
     cudaFree(dp);

@@ -274,12 +274,12 @@ WlsSolver* wls_create(const float* guide, int w, int h, float lambda, float sigm
     if (*err != cudaSuccess) return S;
     const float inv = -1.0f / std::max(sigma_c, 1e-6f);
     const float inv2s2 = 1.0f / (2.0f * sigma_c * sigma_c);
-    edge_kernel<<<g2(w, h), B2, 0, s>>>(guide, w, h, inv, inv2s2, edge_mode, lambda, S->ex, S->ey, S->lv[0].ax, S->lv[0].ay);
+    lsb_launched(), edge_kernel<<<g2(w, h), B2, 0, s>>>(guide, w, h, inv, inv2s2, edge_mode, lambda, S->ex, S->ey, S->lv[0].ax, S->lv[0].ay);
     for (size_t l = 1; l < S->lv.size(); l++) {
         const WlsLevel &F = S->lv[l - 1], &C = S->lv[l];
-        coarsen_edges_kernel<<<g2(C.w, C.h), B2, 0, s>>>(F.ax, F.ay, F.w, F.h, C.ax, C.ay, C.w, C.h);
+        lsb_launched(), coarsen_edges_kernel<<<g2(C.w, C.h), B2, 0, s>>>(F.ax, F.ay, F.w, F.h, C.ax, C.ay, C.w, C.h);
     }
-    fill_kernel<<<g1(n), 256, 0, s>>>(S->ones, 1.f, n);
+    lsb_launched(), fill_kernel<<<g1(n), 256, 0, s>>>(S->ones, 1.f, n);
     *err = cudaGetLastError();
     return S;
 }
@@ -294,24 +294,24 @@ void wls_destroy(WlsSolver* s) {
 int wls_levels(const WlsSolver* s) { return (int)s->lv.size(); }
 
 cudaError_t wls_set_weights(WlsSolver* S, const float* conf, cudaStream_t s) {
-    wd_kernel<<<g1((size_t)S->w * S->h), 256, 0, s>>>(conf, S->lv[0].wd, (size_t)S->w * S->h);
+    lsb_launched(), wd_kernel<<<g1((size_t)S->w * S->h), 256, 0, s>>>(conf, S->lv[0].wd, (size_t)S->w * S->h);
     for (size_t l = 0; l < S->lv.size(); l++) {
         const WlsLevel& C = S->lv[l];
         if (l > 0) {
             const WlsLevel& F = S->lv[l - 1];
-            block_sum_kernel<<<g2(C.w, C.h), B2, 0, s>>>(F.wd, F.w, F.h, C.wd, C.w, C.h);
+            lsb_launched(), block_sum_kernel<<<g2(C.w, C.h), B2, 0, s>>>(F.wd, F.w, F.h, C.wd, C.w, C.h);
         }
-        dinv_kernel<<<g2(C.w, C.h), B2, 0, s>>>(C.wd, C.ax, C.ay, C.w, C.h, C.dinv);
+        lsb_launched(), dinv_kernel<<<g2(C.w, C.h), B2, 0, s>>>(C.wd, C.ax, C.ay, C.w, C.h, C.dinv);
     }
     return cudaGetLastError();
 }
 
 static void jacobi(WlsLevel& L, bool zero, cudaStream_t s) {
     if (zero) {
-        jac0_kernel<<<g1((size_t)L.w * L.h), 256, 0, s>>>(L.b, L.dinv, L.x, (size_t)L.w * L.h);
+        lsb_launched(), jac0_kernel<<<g1((size_t)L.w * L.h), 256, 0, s>>>(L.b, L.dinv, L.x, (size_t)L.w * L.h);
         return;
     }
-    stencil_kernel<<<g2(L.w, L.h), B2, 0, s>>>(L.x, L.b, L.wd, L.ax, L.ay, L.dinv, L.r, L.w, L.h, 2);
+    lsb_launched(), stencil_kernel<<<g2(L.w, L.h), B2, 0, s>>>(L.x, L.b, L.wd, L.ax, L.ay, L.dinv, L.r, L.w, L.h, 2);
     std::swap(L.x, L.r);
 }
 
@@ -323,18 +323,18 @@ static void vcycle(WlsSolver* S, size_t l, cudaStream_t s) {
         return;
     }
     jacobi(T, true, s);
-    stencil_kernel<<<g2(T.w, T.h), B2, 0, s>>>(T.x, T.b, T.wd, T.ax, T.ay, T.dinv, T.r, T.w, T.h, 1);
+    lsb_launched(), stencil_kernel<<<g2(T.w, T.h), B2, 0, s>>>(T.x, T.b, T.wd, T.ax, T.ay, T.dinv, T.r, T.w, T.h, 1);
     WlsLevel& C = S->lv[l + 1];
-    block_sum_kernel<<<g2(C.w, C.h), B2, 0, s>>>(T.r, T.w, T.h, C.b, C.w, C.h);
+    lsb_launched(), block_sum_kernel<<<g2(C.w, C.h), B2, 0, s>>>(T.r, T.w, T.h, C.b, C.w, C.h);
     vcycle(S, l + 1, s);
-    prolong_kernel<<<g2(T.w, T.h), B2, 0, s>>>(T.x, T.w, T.h, C.x, C.w);
+    lsb_launched(), prolong_kernel<<<g2(T.w, T.h), B2, 0, s>>>(T.x, T.w, T.h, C.x, C.w);
     jacobi(T, false, s);
 }
 
 static void dot(WlsSolver* S, const float* a, const float* b, size_t n, int mode, cudaStream_t s) {
     int nb = (int)std::min<size_t>(DOT_BLOCKS, (n + 255) / 256);
-    dot_partial_kernel<<<nb, 256, 0, s>>>(a, b, n, S->part);
-    dot_final_kernel<<<1, 32, 0, s>>>(S->part, nb, S->scal, S->alpha_beta, S->host_rel, mode);
+    lsb_launched(), dot_partial_kernel<<<nb, 256, 0, s>>>(a, b, n, S->part);
+    lsb_launched(), dot_final_kernel<<<1, 32, 0, s>>>(S->part, nb, S->scal, S->alpha_beta, S->host_rel, mode);
 }
 
 cudaError_t wls_solve(WlsSolver* S, const float* d, int max_iters, float* u, float* rel_out, int* iters_out, cudaStream_t s,
@@ -344,8 +344,8 @@ cudaError_t wls_solve(WlsSolver* S, const float* d, int max_iters, float* u, flo
     const size_t n = (size_t)w * h;
     WlsLevel& L0 = S->lv[0];
     if (w == 1 || h == 1) {
-        if (h == 1) thomas_kernel<<<1, 32, 0, s>>>(u, d, L0.wd, 0, S->ex, 1, w, 0, 1, S->lambda, S->cp, S->dp);
-        else thomas_kernel<<<1, 32, 0, s>>>(u, d, L0.wd, 0, S->ey, 1, h, 0, (size_t)w, S->lambda, S->cp, S->dp);
+        if (h == 1) lsb_launched(), thomas_kernel<<<1, 32, 0, s>>>(u, d, L0.wd, 0, S->ex, 1, w, 0, 1, S->lambda, S->cp, S->dp);
+        else lsb_launched(), thomas_kernel<<<1, 32, 0, s>>>(u, d, L0.wd, 0, S->ey, 1, h, 0, (size_t)w, S->lambda, S->cp, S->dp);
         *rel_out = 0.f;
         *iters_out = 0;
         if (rel64) *rel64 = 0.0;
@@ -358,16 +358,16 @@ cudaError_t wls_solve(WlsSolver* S, const float* d, int max_iters, float* u, flo
             float p4 = 1.f;
             for (int q = 0; q < 3 - t; q++) p4 *= 4.f;
             const float lam_t = (1.5f * S->lambda * p4) / (64.f - 1.f);
-            thomas_kernel<<<(h + 127) / 128, 128, 0, s>>>(u, S->f, L0.wd, t == 1 ? 0 : 1, S->ex, h, w, (size_t)w, 1, lam_t, S->cp, S->dp);
+            lsb_launched(), thomas_kernel<<<(h + 127) / 128, 128, 0, s>>>(u, S->f, L0.wd, t == 1 ? 0 : 1, S->ex, h, w, (size_t)w, 1, lam_t, S->cp, S->dp);
             cudaMemcpyAsync(S->f, u, n * sizeof(float), cudaMemcpyDeviceToDevice, s);
-            thomas_kernel<<<(w + 127) / 128, 128, 0, s>>>(u, S->f, L0.wd, 1, S->ey, w, h, 1, (size_t)w, lam_t, S->cp, S->dp);
+            lsb_launched(), thomas_kernel<<<(w + 127) / 128, 128, 0, s>>>(u, S->f, L0.wd, 1, S->ey, w, h, 1, (size_t)w, lam_t, S->cp, S->dp);
             cudaMemcpyAsync(S->f, u, n * sizeof(float), cudaMemcpyDeviceToDevice, s);
         }
     }
     // b = W d, |b|, r = b - A u, z = M r, p = z
-    mul_kernel<<<g1(n), 256, 0, s>>>(L0.wd, d, S->f, n);
+    lsb_launched(), mul_kernel<<<g1(n), 256, 0, s>>>(L0.wd, d, S->f, n);
     dot(S, S->f, S->f, n, 4, s);
-    stencil_kernel<<<g2(w, h), B2, 0, s>>>(u, S->f, L0.wd, L0.ax, L0.ay, L0.dinv, S->r, w, h, 1);
+    lsb_launched(), stencil_kernel<<<g2(w, h), B2, 0, s>>>(u, S->f, L0.wd, L0.ax, L0.ay, L0.dinv, S->r, w, h, 1);
     auto precond = [&]() {
         cudaMemcpyAsync(L0.b, S->r, n * sizeof(float), cudaMemcpyDeviceToDevice, s);
         vcycle(S, 0, s);
@@ -384,9 +384,9 @@ cudaError_t wls_solve(WlsSolver* S, const float* d, int max_iters, float* u, flo
     for (int it = 0; it < max_iters; it++) {
         if (rel < 1e-5f) break;
         iters++;
-        stencil_kernel<<<g2(w, h), B2, 0, s>>>(S->p, S->f, L0.wd, L0.ax, L0.ay, L0.dinv, S->ap, w, h, 0);
+        lsb_launched(), stencil_kernel<<<g2(w, h), B2, 0, s>>>(S->p, S->f, L0.wd, L0.ax, L0.ay, L0.dinv, S->ap, w, h, 0);
         dot(S, S->p, S->ap, n, 1, s);
-        axpy2_kernel<<<g1(n), 256, 0, s>>>(u, S->p, S->r, S->ap, S->alpha_beta, n);
+        lsb_launched(), axpy2_kernel<<<g1(n), 256, 0, s>>>(u, S->p, S->r, S->ap, S->alpha_beta, n);
         dot(S, S->r, S->r, n, 3, s);
         e = cudaStreamSynchronize(s);
         if (e != cudaSuccess) return e;
@@ -395,7 +395,7 @@ cudaError_t wls_solve(WlsSolver* S, const float* d, int max_iters, float* u, flo
         if (rel < 1e-5f) break;
         precond();
         dot(S, S->r, S->z, n, 2, s);
-        pupd_kernel<<<g1(n), 256, 0, s>>>(S->p, S->z, S->alpha_beta, n);
+        lsb_launched(), pupd_kernel<<<g1(n), 256, 0, s>>>(S->p, S->z, S->alpha_beta, n);
     }
     *rel_out = rel;
     *iters_out = iters;

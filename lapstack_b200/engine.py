@@ -12,7 +12,10 @@ Inputs may be numpy arrays (host memory) or CUDA tensors (device memory).
 """
 from __future__ import annotations
 
+import atexit
 import ctypes as C
+import sys
+import weakref
 from dataclasses import dataclass, field
 
 import numpy as np
@@ -118,7 +121,20 @@ class Output:  # stack.rs:244 Output (the hot-path part)
     ms: dict = field(default_factory=dict)
 
 
-STAGES = ["align", "gains", "fold", "collapse", "aggregate", "wls", "upsample", "total"]
+STAGES = ["align", "gains", "fold", "collapse", "aggregate", "wls", "upsample", "total", "fold_level0"]
+
+# Live handles, released stacks-first at interpreter exit while the CUDA
+# runtime is still up (a finaliser run during shutdown does nothing).
+_live_stacks: "weakref.WeakSet" = weakref.WeakSet()
+_live_engines: "weakref.WeakSet" = weakref.WeakSet()
+
+
+@atexit.register
+def _release_all():
+    for s in list(_live_stacks):
+        s.close()
+    for e in list(_live_engines):
+        e.close()
 
 
 def _ptr(a):
@@ -136,14 +152,19 @@ def _ptr(a):
 class Engine:
     """lsb_engine: one CUDA device, one stream (gpu.rs:308-324's set-up, once)."""
 
-    def __init__(self, device: int = 0, fp16_storage: bool = False, grid_limit: int = 0, log=None):
+    STORAGE = {"f32": 0, "unorm16": 1, "f16": 2}
+
+    def __init__(self, device: int = 0, storage: str = "f32", grid_limit: int = 0, log=None):
+        """storage: "f32" (bit-exact with the reference FP32 path), "unorm16" (16-bit
+        Gaussian levels, FP16 slices) or "f16" (IEEE half levels and slices)."""
         self._L = load()
         self._logcb = LOG_FN(lambda line, _u: log(line.decode())) if log else LOG_FN()
-        cfg = Config(device, int(fp16_storage), grid_limit, 0, self._logcb, None)
+        cfg = Config(device, self.STORAGE[storage], grid_limit, 0, self._logcb, None)
         h = C.c_void_p()
         check(self._L.lsb_engine_create(C.byref(cfg), C.byref(h)))
         self._h = h
-        self.fp16_storage = fp16_storage
+        self.storage = storage
+        _live_engines.add(self)
 
     @property
     def stream(self):
@@ -155,6 +176,8 @@ class Engine:
             self._h = None
 
     def __del__(self):
+        if sys.is_finalizing():
+            return
         try:
             self.close()
         except Exception:
@@ -195,6 +218,7 @@ class Stack:
                                       C.byref(hnd)))
         self._h = hnd
         self._keep = []
+        _live_stacks.add(self)
 
     def close(self):
         if getattr(self, "_h", None):
@@ -202,6 +226,8 @@ class Stack:
             self._h = None
 
     def __del__(self):
+        if sys.is_finalizing():
+            return
         try:
             self.close()
         except Exception:
@@ -241,7 +267,7 @@ class Stack:
 
     def run(self):
         """The whole pipeline, results left on the device; per-stage device ms."""
-        ms = np.zeros(8, np.float64)
+        ms = np.zeros(12, np.float64)
         check(self._L.lsb_stack_run(self._h, C.c_void_p(ms.ctypes.data)))
         self._keep.clear()
         return dict(zip(STAGES, ms.tolist()))
