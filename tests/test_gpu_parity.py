@@ -240,4 +240,7 @@ def test_16bit_storage_error_vs_oracles(storage):
     e64, e32, f32_64 = _errors(out.image, ref64.image), _errors(out.image, ref32.image), _errors(ref32.image, ref64.image)
     print(f"{storage}: vs fp64 {e64}; vs fp32 reference path {e32}; fp32 path vs fp64 {f32_64}")
     if storage == "unorm16":
-        assert e64["mean"] < 1.0 and e64["p99"] < 4.0
+        # 16-bit fixed-point levels cost no more accuracy than the reference's own FP32 arithmetic:
+        # both differ from FP64 mostly where a near-tie in the energies picks another frame
+        assert e64["mean"] < 1.5 * f32_64["mean"] and e64["p99"] < 1.5 * f32_64["p99"]
+        assert e32["mean"] < 2.0
