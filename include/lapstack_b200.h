@@ -176,6 +176,21 @@ char* lsb_align_pair(lsb_engine* e, const float* rf, const float* tg, uint32_t w
 char* lsb_warp_cost(lsb_engine* e, const float* rf, uint32_t aw, uint32_t ah, const float* tgt, uint32_t tw, uint32_t th,
                     const double* sim8, double* cost);
 
+/* lsb_warp_cost without any allocation (no counterpart in the reference). For a
+ * host that runs the Nelder-Mead search itself and keeps its level planes in
+ * device memory it manages -- an allocator arena, a pool it sized up front,
+ * or a process where a new device allocation mid-search would stall or fail
+ * (a cudaMalloc synchronises the device and may not be available at all to a
+ * caller that only ever borrows memory). rf_dev (aw x ah) and tgt_dev
+ * (tw x th) are device f32 planes; sims8 holds n_sims (1..9) Sim vectors;
+ * costs (host, n_sims) receives the align.rs:581 costs. The scratch is a
+ * fixed 64.9 KB array in the library's device image, per GPU: its address is
+ * looked up on the first call on each device, so make that first call before
+ * any stream capture. Calls that overlap on the GPU race on that scratch.
+ * Returns NULL or a static error string (do not free it). */
+const char* lsb_warp_cost_noalloc(const float* rf_dev, uint32_t aw, uint32_t ah, const float* tgt_dev, uint32_t tw,
+                                  uint32_t th, const double* sims8, uint32_t n_sims, double* costs, void* stream);
+
 /* Synthetic stacks: [n][h][w][3] u16 into host memory (OpenMP) or device memory. truth (n*4, may be NULL):
    per frame scale, rotation (rad), tx, ty (px) applied. */
 const char* lsb_synth_stack_host(const lsb_synth_desc* d, uint16_t* out, double* truth);

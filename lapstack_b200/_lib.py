@@ -90,6 +90,7 @@ SIGNATURES = {
                             P, P]),
     "lsb_align_pair": (ERR, [P, P, P, C.c_uint32, C.c_uint32, P, P, C.c_uint32, P, P]),
     "lsb_warp_cost": (ERR, [P, P, C.c_uint32, C.c_uint32, P, C.c_uint32, C.c_uint32, P, P]),
+    "lsb_warp_cost_noalloc": (C.c_char_p, [P, C.c_uint32, C.c_uint32, P, C.c_uint32, C.c_uint32, P, C.c_uint32, P, P]),
     "lsb_synth_stack_host": (C.c_char_p, [C.POINTER(SynthDesc), P, P]),
     "lsb_synth_stack_device": (C.c_char_p, [C.POINTER(SynthDesc), P, P, P]),
 }

@@ -12,6 +12,7 @@
 // evaluated in the same launch (the search then takes the branch the
 // reference takes), and a shrink's n points in one more.
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <functional>
 #include <vector>
@@ -490,4 +491,69 @@ cudaError_t cost_single(AlignCtx& C, const float* rf, int aw, int ah, const floa
     return e;
 }
 
+// ------------------------------------------ the cost without any allocation
+// Scratch of lsb_warp_cost_noalloc: the per-block partial sums (MAX_CAND
+// candidates x NOALLOC_BLOCKS blocks x 3 doubles) and the reduced sums
+// (MAX_CAND x 3): 64.9 KB, held by every GPU that loads the library until
+// the process exits. Each call writes every partial it later reads, so
+// nothing has to start at zero; calls that overlap on the GPU race on it.
+constexpr int NOALLOC_BLOCKS = 296;
+constexpr size_t NOALLOC_PARTS = (size_t)MAX_CAND * NOALLOC_BLOCKS * 3;
+static __device__ __align__(256) double g_noalloc_scratch[NOALLOC_PARTS + MAX_CAND * 3];
+
+// The array's device address, looked up once per device with that device
+// current (in host code its name is only a host-side stand-in).
+static double* g_noalloc_dev[128];
+static std::atomic<int> g_noalloc_ready[128];
+
+static const char* noalloc_scratch(double** out) {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return "lsb_warp_cost_noalloc: no current CUDA device";
+    if (dev < 0 || dev >= 128) return "lsb_warp_cost_noalloc: device ordinal out of range";
+    if (g_noalloc_ready[dev].load(std::memory_order_acquire) == 0) {
+        void* p = nullptr;
+        if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || p == nullptr)
+            return "lsb_warp_cost_noalloc: cudaGetSymbolAddress of the scratch failed";
+        g_noalloc_dev[dev] = (double*)p;
+        g_noalloc_ready[dev].store(1, std::memory_order_release);
+    }
+    *out = g_noalloc_dev[dev];
+    return nullptr;
+}
+
 }  // namespace lsb
+
+using namespace lsb;
+
+// align.rs:581 warp_cost of device planes for up to MAX_CAND transforms, using
+// only the static scratch above. The error string, when one is returned, is
+// static: do not free it.
+extern "C" const char* lsb_warp_cost_noalloc(const float* rf_dev, uint32_t aw, uint32_t ah, const float* tgt_dev, uint32_t tw,
+                                             uint32_t th, const double* sims8, uint32_t n_sims, double* costs, void* stream) {
+    if (!rf_dev || !tgt_dev || !sims8 || !costs) return "lsb_warp_cost_noalloc: null argument";
+    if (aw == 0 || ah == 0 || tw == 0 || th == 0) return "lsb_warp_cost_noalloc: empty plane";
+    if (n_sims == 0 || n_sims > (uint32_t)MAX_CAND) return "lsb_warp_cost_noalloc: 1 to 9 transforms per call";
+    double* scratch = nullptr;
+    if (const char* e = noalloc_scratch(&scratch)) return e;
+    cudaStream_t s = (cudaStream_t)stream;
+    CostBatch cb;
+    for (uint32_t k = 0; k < n_sims; k++) {
+        double m[9];
+        sim_matrix(sims8 + 8 * k, (int)tw, (int)th, m);
+        mat_inverse(m, cb.inv[k]);
+    }
+    const size_t npx = (size_t)aw * ah;
+    const int nblocks = (int)std::min<size_t>(std::max<size_t>((npx + 255) / 256, 1), NOALLOC_BLOCKS);
+    dim3 g(nblocks, n_sims);
+    lsb_launched(), cost_kernel<<<g, 256, 0, s>>>(rf_dev, (int)aw, (int)ah, tgt_dev, (int)tw, (int)th, cb, scratch);
+    lsb_launched(), cost_final_kernel<<<1, 32, 0, s>>>(scratch, nblocks, (int)n_sims, scratch + NOALLOC_PARTS);
+    double sums[MAX_CAND * 3];
+    if (cudaMemcpyAsync(sums, scratch + NOALLOC_PARTS, sizeof(double) * 3 * n_sims, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+        cudaStreamSynchronize(s) != cudaSuccess)
+        return "lsb_warp_cost_noalloc: the cost kernels failed";
+    for (uint32_t k = 0; k < n_sims; k++) {
+        const double sd = sums[3 * k], sd2 = sums[3 * k + 1], cnt = sums[3 * k + 2];
+        costs[k] = cnt < 16.0 ? 1e9 : std::sqrt(std::max((sd2 - sd * sd / cnt) / cnt, 0.0));
+    }
+    return nullptr;
+}
