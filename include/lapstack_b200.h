@@ -77,7 +77,8 @@ typedef struct {
     uint32_t model;   /* 0 similarity, 1 affine, 2 projective */
     uint32_t coarsen; /* skip the N finest registration levels */
     uint32_t interp;  /* align.rs Interp id: 0 nearest .. 3 spline4x4 .. 5 lanczos3 */
-    uint32_t reserved;
+    uint32_t host_search; /* 0: each frame's whole Nelder-Mead search in one cooperative launch;
+                             1: the host drives it, one launch and read-back per simplex step */
 } lsb_align_params;
 
 /* depth.rs:69-109 DepthParams (enabled = 0: report the fuse winner map) */

@@ -36,7 +36,7 @@ class FuseParamsC(C.Structure):
 
 class AlignParamsC(C.Structure):
     _fields_ = [("enabled", C.c_uint32), ("shift", C.c_uint32), ("scale", C.c_uint32), ("rotation", C.c_uint32),
-                ("model", C.c_uint32), ("coarsen", C.c_uint32), ("interp", C.c_uint32), ("reserved", C.c_uint32)]
+                ("model", C.c_uint32), ("coarsen", C.c_uint32), ("interp", C.c_uint32), ("host_search", C.c_uint32)]
 
 
 class DepthParamsC(C.Structure):

@@ -6,11 +6,15 @@
 // becomes the next frame's reference (align.rs:542 `warp_plane`), and the
 // brightness sums of every aligned frame against frame 0 (brightness.rs:67).
 //
-// The bounded Nelder-Mead search (align.rs:796) runs on the host on this
-// schedule, with one launch and one small read-back per simplex iteration:
-// the reflection, expansion and contraction points of an iteration are all
-// evaluated in the same launch (the search then takes the branch the
-// reference takes), and a shrink's n points in one more.
+// The bounded Nelder-Mead search (align.rs:796) evaluates the reflection,
+// expansion and contraction points of an iteration together (the search then
+// takes the branch the reference takes), and a shrink's n points together.
+// By default the whole multi-level search of a frame runs in one cooperative
+// launch (`multiscale_align_dev`); the host-driven form, one launch and one
+// small read-back per simplex step, stays for a device without cooperative
+// launch and as the cross-check of the device search.
+#include <cooperative_groups.h>
+
 #include <algorithm>
 #include <atomic>
 #include <cmath>
@@ -22,6 +26,11 @@
 #include "lsb_interp.cuh"
 
 namespace lsb {
+namespace cg = cooperative_groups;
+
+// align.rs:220 `Sim::SPAN`: the search box around the initial transform, per parameter.
+static const double SPAN[8] = {0.10, 0.10, 0.10, 0.087266462599716474, 0.05, 0.05, 0.05, 0.05};
+__constant__ double c_span[8] = {0.10, 0.10, 0.10, 0.087266462599716474, 0.05, 0.05, 0.05, 0.05};
 
 // ------------------------------------------------------------------ kernels
 __global__ void luma_u16_kernel(const uint16_t* __restrict__ f, size_t n, float* __restrict__ y) {
@@ -131,13 +140,24 @@ __global__ void cost_kernel(const float* __restrict__ rf, int aw, int ah, const 
     if (threadIdx.x == 0)
         for (int q = 0; q < 3; q++) part[((size_t)k * gridDim.x + blockIdx.x) * 3 + q] = red[q][0];
 }
+// The per-block partials of every candidate summed in a fixed order: one
+// block per candidate, each thread a fixed stride of blocks, then a tree.
 __global__ void cost_final_kernel(const double* __restrict__ part, int nblocks, int ncand, double* __restrict__ out) {
-    const int k = threadIdx.x;
+    const int k = blockIdx.x;
     if (k >= ncand) return;
     double s[3] = {0.0, 0.0, 0.0};
-    for (int b = 0; b < nblocks; b++)
+    for (int b = threadIdx.x; b < nblocks; b += blockDim.x)
         for (int q = 0; q < 3; q++) s[q] += part[((size_t)k * nblocks + b) * 3 + q];
-    for (int q = 0; q < 3; q++) out[3 * k + q] = s[q];
+    __shared__ double red[3][128];
+    for (int q = 0; q < 3; q++) red[q][threadIdx.x] = s[q];
+    __syncthreads();
+    for (int st = blockDim.x / 2; st > 0; st >>= 1) {
+        if (threadIdx.x < st)
+            for (int q = 0; q < 3; q++) red[q][threadIdx.x] += red[q][threadIdx.x + st];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0)
+        for (int q = 0; q < 3; q++) out[3 * k + q] = red[q][0];
 }
 
 // align.rs:489 `warp_with` on an f32 plane (edge-clamped; no fallback), the
@@ -321,7 +341,7 @@ static cudaError_t eval_batch(AlignCtx& C, const float* rf, int aw, int ah, cons
         const int nblocks = (int)std::min<size_t>(std::max<size_t>((npx + 255) / 256, 1), 296);
         dim3 g(nblocks, nc);
         lsb_launched(), cost_kernel<<<g, 256, 0, C.s>>>(rf, aw, ah, tg, tw, th, cb, C.part);
-        lsb_launched(), cost_final_kernel<<<1, 32, 0, C.s>>>(C.part, nblocks, nc, C.sums_dev);
+        lsb_launched(), cost_final_kernel<<<nc, 128, 0, C.s>>>(C.part, nblocks, nc, C.sums_dev);
         cudaMemcpyAsync(C.sums_host, C.sums_dev, sizeof(double) * 3 * nc, cudaMemcpyDeviceToHost, C.s);
         cudaError_t e = cudaStreamSynchronize(C.s);
         if (e != cudaSuccess) return e;
@@ -432,14 +452,14 @@ static cudaError_t nelder_mead_dev(AlignCtx& C, const std::function<cudaError_t(
     return cudaSuccess;
 }
 
-// align.rs:896 `multiscale_align`: rf/tg full-res planes with their levels.
-cudaError_t multiscale_align(AlignCtx& C, const float* rf, const std::vector<float*>& pr, const float* tg,
+// align.rs:896 `multiscale_align`: rf/tg full-res planes with their levels,
+// the search driven from the host.
+static cudaError_t multiscale_align_host(AlignCtx& C, const float* rf, const std::vector<float*>& pr, const float* tg,
                              const std::vector<float*>& pt, int w, int h, const double init[8], const bool freem[8], int coarsen,
                              double out[8]) {
     std::vector<std::pair<int, int>> dims;
     gauss_dims(w, h, dims);
     const size_t n = dims.size() + 1;
-    static const double SPAN[8] = {0.10, 0.10, 0.10, 0.087266462599716474, 0.05, 0.05, 0.05, 0.05};
     std::vector<size_t> free_idx;
     for (size_t k = 0; k < 8; k++)
         if (freem[k]) free_idx.push_back(k);
@@ -489,6 +509,377 @@ cudaError_t cost_single(AlignCtx& C, const float* rf, int aw, int ah, const floa
     cudaError_t e = eval_batch(C, rf, aw, ah, tg, tw, th, {std::vector<double>(sim, sim + 8)}, fs);
     *cost = fs.empty() ? 0.0 : fs[0];
     return e;
+}
+
+// ------------------------------------------- the search on the device
+// align.rs:896 `multiscale_align` for one frame in ONE cooperative launch:
+// every block evaluates the current candidates over the level (the cost of
+// align.rs:581, f64 partials per block), block 0 sums the partials in a fixed
+// order and its thread 0 advances the bounded Nelder-Mead of align.rs:796
+// (the reflection, expansion and contraction of an iteration evaluated
+// together, a shrink's n points together), and grid-wide barriers separate
+// the two. No host round trip per iteration.
+struct NmLevel {
+    const float* rf;
+    const float* tg;
+    int w, h, lvl;
+};
+struct NmJob {
+    NmLevel lv[24];
+    int nlv;   // levels searched, coarsest first
+    int W, H;  // full resolution
+    double init[8];
+    int free_idx[8], nfree;
+    double* part;  // [MAX_CAND][gridDim.x][3]
+    double* cand;  // [MAX_CAND][9] candidate inverses (written by block 0)
+    int* ctl;      // [0] candidates pending, [1] evaluations (the reference's count)
+    double* out;   // the transform found [8]
+};
+
+__device__ void dev_sim_matrix(const double* v, int w, int h, double m[9]) {
+    const double cx = (double)w / 2.0, cy = (double)h / 2.0;
+    const double c = cos(v[3]), sn = sin(v[3]);
+    const double sc = v[2], shear = v[5], aspect = v[4];
+    const double a = __dmul_rn(sc, c), b = __dmul_rn(sc, __dsub_rn(__dmul_rn(c, shear), __dmul_rn(sn, aspect)));
+    const double d = __dmul_rn(sc, sn), e = __dmul_rn(sc, __dadd_rn(__dmul_rn(sn, shear), __dmul_rn(c, aspect)));
+    const double gx = __ddiv_rn(v[6], (double)w), gy = __ddiv_rn(v[7], (double)h);
+    const double a2 = __dadd_rn(a, __dmul_rn(cx, gx)), b2 = __dadd_rn(b, __dmul_rn(cx, gy));
+    const double d2 = __dadd_rn(d, __dmul_rn(cy, gx)), e2 = __dadd_rn(e, __dmul_rn(cy, gy));
+    m[0] = a2;
+    m[1] = b2;
+    m[2] = __dsub_rn(__dadd_rn(cx, __dmul_rn(v[0], (double)w)), __dadd_rn(__dmul_rn(a2, cx), __dmul_rn(b2, cy)));
+    m[3] = d2;
+    m[4] = e2;
+    m[5] = __dsub_rn(__dadd_rn(cy, __dmul_rn(v[1], (double)h)), __dadd_rn(__dmul_rn(d2, cx), __dmul_rn(e2, cy)));
+    m[6] = gx;
+    m[7] = gy;
+    m[8] = __dsub_rn(__dsub_rn(1.0, __dmul_rn(gx, cx)), __dmul_rn(gy, cy));
+}
+__device__ void dev_mat_inverse(const double m[9], double inv[9]) {
+    if (m[6] == 0.0 && m[7] == 0.0 && m[8] == 1.0) {
+        const double a = m[0], b = m[1], tx = m[2], d = m[3], e = m[4], ty = m[5];
+        const double det = __dsub_rn(__dmul_rn(a, e), __dmul_rn(b, d));
+        const double ia = __ddiv_rn(e, det), ib = __ddiv_rn(-b, det), id = __ddiv_rn(-d, det), ie = __ddiv_rn(a, det);
+        inv[0] = ia;
+        inv[1] = ib;
+        inv[2] = -__dadd_rn(__dmul_rn(ia, tx), __dmul_rn(ib, ty));
+        inv[3] = id;
+        inv[4] = ie;
+        inv[5] = -__dadd_rn(__dmul_rn(id, tx), __dmul_rn(ie, ty));
+        inv[6] = 0.0;
+        inv[7] = 0.0;
+        inv[8] = 1.0;
+        return;
+    }
+    for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) {
+            const int r0 = (j + 1) % 3, r1 = (j + 2) % 3, c0 = (i + 1) % 3, c1 = (i + 2) % 3;
+            inv[3 * i + j] = __dsub_rn(__dmul_rn(m[3 * r0 + c0], m[3 * r1 + c1]), __dmul_rn(m[3 * r0 + c1], m[3 * r1 + c0]));
+        }
+    const double k = inv[8];
+    for (int i = 0; i < 9; i++) inv[i] = __ddiv_rn(inv[i], k);
+}
+
+// The NM state block 0's thread 0 keeps between grid barriers.
+struct NmState {
+    double cur[8], snap[8], simplex[9][8], fv[9], lo[8], hi[8], step[8], tol[8], xr[8], xe[8], xc[8];
+    int it, phase, level, evals;
+};
+enum { NM_INIT = 0, NM_RXC = 1, NM_SHRINK = 2 };
+
+__device__ void nm_put_cand(const NmJob& J, const NmState& S, int k, const double* x, int tw, int th) {
+    double v[8], m[9];
+    for (int q = 0; q < 8; q++) v[q] = S.snap[q];
+    for (int q = 0; q < J.nfree; q++) v[J.free_idx[q]] = x[q];
+    dev_sim_matrix(v, tw, th, m);
+    dev_mat_inverse(m, J.cand + 9 * k);
+}
+__device__ void nm_clamp(const NmState& S, int n, double* v) {
+    for (int q = 0; q < n; q++) v[q] = fmin(fmax(v[q], S.lo[q]), S.hi[q]);
+}
+// Start level L: the first simplex (align.rs:806-813). Returns the candidates pending.
+__device__ int nm_level_start(const NmJob& J, NmState& S, int L) {
+    const int n = J.nfree;
+    const NmLevel& lv = J.lv[L];
+    for (int q = 0; q < 8; q++) S.snap[q] = S.cur[q];
+    const double wf = J.W, hf = J.H, r = fmax(wf, hf) / 2.0;
+    const double gain[8] = {wf, hf, r, r, hf / 2.0, hf / 2.0, wf / 4.0, hf / 4.0};
+    const double px = (double)(1ull << lv.lvl);
+    for (int q = 0; q < n; q++) {
+        S.step[q] = __ddiv_rn(__dmul_rn(1.0, px), gain[J.free_idx[q]]);
+        S.tol[q] = __ddiv_rn(__dmul_rn(0.1, px), gain[J.free_idx[q]]);
+    }
+    for (int q = 0; q < n; q++) S.simplex[0][q] = S.cur[J.free_idx[q]];
+    for (int k = 0; k < n; k++) {
+        for (int q = 0; q < n; q++) S.simplex[k + 1][q] = S.simplex[0][q];
+        S.simplex[k + 1][k] = __dadd_rn(S.simplex[k + 1][k], S.step[k]);
+        nm_clamp(S, n, S.simplex[k + 1]);
+    }
+    for (int k = 0; k <= n; k++) nm_put_cand(J, S, k, S.simplex[k], lv.w, lv.h);
+    S.phase = NM_INIT;
+    S.it = 0;
+    return n + 1;
+}
+// The top of align.rs:815's loop: returns the candidates pending, 0 when the level is done.
+__device__ int nm_iterate(const NmJob& J, NmState& S, int L) {
+    const int n = J.nfree;
+    const NmLevel& lv = J.lv[L];
+    bool done = S.it >= 200;
+    if (!done) {
+        S.it++;
+        // stable sort by fv (align.rs:817)
+        for (int i = 1; i <= n; i++) {
+            double f = S.fv[i], v[8];
+            for (int q = 0; q < n; q++) v[q] = S.simplex[i][q];
+            int j = i - 1;
+            while (j >= 0 && S.fv[j] > f) {
+                S.fv[j + 1] = S.fv[j];
+                for (int q = 0; q < n; q++) S.simplex[j + 1][q] = S.simplex[j][q];
+                j--;
+            }
+            S.fv[j + 1] = f;
+            for (int q = 0; q < n; q++) S.simplex[j + 1][q] = v[q];
+        }
+        // align.rs:888 `converged`
+        bool conv = fabs(__dsub_rn(S.fv[n], S.fv[0])) <= __dmul_rn(1e-4, __dadd_rn(1.0, fabs(S.fv[0])));
+        for (int i = 1; conv && i <= n; i++)
+            for (int q = 0; q < n; q++)
+                if (!(fabs(__dsub_rn(S.simplex[i][q], S.simplex[0][q])) <= S.tol[q])) {
+                    conv = false;
+                    break;
+                }
+        done = conv;
+    }
+    if (done) {
+        int best = 0;
+        for (int i = 1; i <= n; i++)
+            if (S.fv[i] < S.fv[best]) best = i;
+        for (int q = 0; q < n; q++) S.cur[J.free_idx[q]] = S.simplex[best][q];
+        return 0;
+    }
+    double c[8];
+    for (int q = 0; q < n; q++) c[q] = 0.0;
+    for (int i = 0; i < n; i++)
+        for (int q = 0; q < n; q++) c[q] = __dadd_rn(c[q], S.simplex[i][q]);
+    for (int q = 0; q < n; q++) c[q] = __ddiv_rn(c[q], (double)n);
+    for (int q = 0; q < n; q++) S.xr[q] = __dadd_rn(c[q], __dmul_rn(1.0, __dsub_rn(c[q], S.simplex[n][q])));
+    nm_clamp(S, n, S.xr);
+    for (int q = 0; q < n; q++) S.xe[q] = __dadd_rn(c[q], __dmul_rn(2.0, __dsub_rn(S.xr[q], c[q])));
+    nm_clamp(S, n, S.xe);
+    for (int q = 0; q < n; q++) S.xc[q] = __dadd_rn(c[q], __dmul_rn(0.5, __dsub_rn(S.simplex[n][q], c[q])));
+    nm_clamp(S, n, S.xc);
+    nm_put_cand(J, S, 0, S.xr, lv.w, lv.h);
+    nm_put_cand(J, S, 1, S.xe, lv.w, lv.h);
+    nm_put_cand(J, S, 2, S.xc, lv.w, lv.h);
+    S.phase = NM_RXC;
+    return 3;
+}
+// Take the costs of the pending candidates; returns the candidates pending next.
+__device__ int nm_advance(const NmJob& J, NmState& S, int L, const double* cost) {
+    const int n = J.nfree;
+    const NmLevel& lv = J.lv[L];
+    if (S.phase == NM_INIT) {
+        for (int i = 0; i <= n; i++) S.fv[i] = cost[i];
+        S.evals += n + 1;
+        return nm_iterate(J, S, L);
+    }
+    if (S.phase == NM_SHRINK) {
+        for (int i = 1; i <= n; i++) S.fv[i] = cost[i - 1];
+        S.evals += n;
+        return nm_iterate(J, S, L);
+    }
+    const double fr = cost[0], fe = cost[1], fc = cost[2];
+    S.evals += 1;
+    if (fr < S.fv[0]) {
+        S.evals += 1;
+        if (fe < fr) {
+            for (int q = 0; q < n; q++) S.simplex[n][q] = S.xe[q];
+            S.fv[n] = fe;
+        } else {
+            for (int q = 0; q < n; q++) S.simplex[n][q] = S.xr[q];
+            S.fv[n] = fr;
+        }
+    } else if (fr < S.fv[n - 1]) {
+        for (int q = 0; q < n; q++) S.simplex[n][q] = S.xr[q];
+        S.fv[n] = fr;
+    } else {
+        S.evals += 1;
+        if (fc < S.fv[n]) {
+            for (int q = 0; q < n; q++) S.simplex[n][q] = S.xc[q];
+            S.fv[n] = fc;
+        } else {
+            for (int i = 1; i <= n; i++) {
+                for (int q = 0; q < n; q++)
+                    S.simplex[i][q] = __dadd_rn(S.simplex[0][q], __dmul_rn(0.5, __dsub_rn(S.simplex[i][q], S.simplex[0][q])));
+                nm_clamp(S, n, S.simplex[i]);
+                nm_put_cand(J, S, i - 1, S.simplex[i], lv.w, lv.h);
+            }
+            S.phase = NM_SHRINK;
+            return n;
+        }
+    }
+    return nm_iterate(J, S, L);
+}
+
+__global__ void __launch_bounds__(256) nm_search_kernel(const NmJob J) {
+    cg::grid_group grid = cg::this_grid();
+    __shared__ NmState S;
+    __shared__ double red[3][256];
+    __shared__ double cost[MAX_CAND];
+    const bool lead = blockIdx.x == 0 && threadIdx.x == 0;
+    if (lead) {
+        for (int q = 0; q < 8; q++) S.cur[q] = J.init[q];
+        for (int q = 0; q < J.nfree; q++) {
+            S.lo[q] = __dsub_rn(J.init[J.free_idx[q]], c_span[J.free_idx[q]]);
+            S.hi[q] = __dadd_rn(J.init[J.free_idx[q]], c_span[J.free_idx[q]]);
+        }
+        S.evals = 0;
+    }
+    for (int L = 0; L < J.nlv; L++) {
+        if (L > 0) grid.sync();  // every block has read the previous level's final 0
+        if (lead) J.ctl[0] = J.nfree > 0 ? nm_level_start(J, S, L) : 0;
+        grid.sync();
+        const NmLevel lv = J.lv[L];
+        const double xmax = (double)(lv.w - 1), ymax = (double)(lv.h - 1);
+        const unsigned npx = (unsigned)lv.w * lv.h;  // < 2^32 (the host checks)
+        int passes = 0;
+        while (true) {
+            const int nc = *(volatile int*)J.ctl;
+            if (nc == 0) break;
+            for (int k = 0; k < nc; k++) {
+                double m[9];
+                for (int q = 0; q < 9; q++) m[q] = J.cand[9 * k + q];
+                const bool aff = m[6] == 0.0 && m[7] == 0.0 && m[8] == 1.0;
+                double sd = 0.0, sd2 = 0.0, cnt = 0.0;
+                for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < npx; i += gridDim.x * blockDim.x) {
+                    const int y = (int)(i / (unsigned)lv.w), x = (int)(i - (unsigned)y * lv.w);
+                    double sx, sy;
+                    src_point(m, aff, (double)x, (double)y, sx, sy);
+                    if (!(sx >= 0.0 && sx <= xmax && sy >= 0.0 && sy <= ymax)) continue;
+                    const double fx = floor(sx), fy = floor(sy);
+                    const int x0 = (int)fx, y0 = (int)fy;
+                    float wx[4], wy[4];
+                    spline4f((float)__dsub_rn(sx, fx), wx);
+                    spline4f((float)__dsub_rn(sy, fy), wy);
+                    float acc = 0.f;
+                    for (int j = 0; j < 4; j++) {
+                        const float* row = lv.tg + (size_t)min(max(y0 + j - 1, 0), lv.h - 1) * lv.w;
+                        float r = 0.f;
+                        for (int u = 0; u < 4; u++) r = __fadd_rn(r, __fmul_rn(wx[u], row[min(max(x0 + u - 1, 0), lv.w - 1)]));
+                        acc = __fadd_rn(acc, __fmul_rn(wy[j], r));
+                    }
+                    const double d = (double)__fsub_rn(lv.rf[i], acc);
+                    sd += d;
+                    sd2 += d * d;
+                    cnt += 1.0;
+                }
+                red[0][threadIdx.x] = sd;
+                red[1][threadIdx.x] = sd2;
+                red[2][threadIdx.x] = cnt;
+                __syncthreads();
+                for (int st = blockDim.x / 2; st > 0; st >>= 1) {
+                    if (threadIdx.x < st)
+                        for (int q = 0; q < 3; q++) red[q][threadIdx.x] += red[q][threadIdx.x + st];
+                    __syncthreads();
+                }
+                if (threadIdx.x == 0)
+                    for (int q = 0; q < 3; q++) J.part[((size_t)k * gridDim.x + blockIdx.x) * 3 + q] = red[q][0];
+                __syncthreads();
+            }
+            grid.sync();
+            if (blockIdx.x == 0) {
+                for (int k = 0; k < nc; k++) {
+                    double s[3] = {0.0, 0.0, 0.0};
+                    for (int b = threadIdx.x; b < (int)gridDim.x; b += blockDim.x)
+                        for (int q = 0; q < 3; q++) s[q] += J.part[((size_t)k * gridDim.x + b) * 3 + q];
+                    for (int q = 0; q < 3; q++) red[q][threadIdx.x] = s[q];
+                    __syncthreads();
+                    for (int st = blockDim.x / 2; st > 0; st >>= 1) {
+                        if (threadIdx.x < st)
+                            for (int q = 0; q < 3; q++) red[q][threadIdx.x] += red[q][threadIdx.x + st];
+                        __syncthreads();
+                    }
+                    if (threadIdx.x == 0) {
+                        const double sdv = red[0][0], sd2v = red[1][0], cn = red[2][0];
+                        cost[k] = cn < 16.0 ? 1e9 : sqrt(fmax(__ddiv_rn(__dsub_rn(sd2v, __ddiv_rn(__dmul_rn(sdv, sdv), cn)), cn), 0.0));
+                    }
+                    __syncthreads();
+                }
+                if (lead) {
+                    // <= 200 iterations of at most two batches each, plus the first simplex
+                    const int nx = nm_advance(J, S, L, cost);
+                    J.ctl[0] = ++passes > 402 ? 0 : nx;
+                }
+            }
+            grid.sync();
+        }
+    }
+    if (lead) {
+        for (int q = 0; q < 8; q++) J.out[q] = S.cur[q];
+        J.ctl[1] = S.evals;
+    }
+}
+
+static int g_nm_blocks = 0;
+
+static cudaError_t multiscale_align_dev(AlignCtx& C, const float* rf, const std::vector<float*>& pr, const float* tg,
+                                 const std::vector<float*>& pt, int w, int h, const double init[8], const bool freem[8], int coarsen,
+                                 double out[8]) {
+    std::vector<std::pair<int, int>> dims;
+    gauss_dims(w, h, dims);
+    const int n = (int)dims.size() + 1;
+    const int finest = std::min(coarsen, n - 1);
+    NmJob J;
+    memset(&J, 0, sizeof J);
+    J.nlv = 0;
+    for (int lvl = n - 1; lvl >= finest && J.nlv < 24; lvl--) {
+        NmLevel& L = J.lv[J.nlv++];
+        L.rf = lvl == 0 ? rf : pr[lvl - 1];
+        L.tg = lvl == 0 ? tg : pt[lvl - 1];
+        L.w = lvl == 0 ? w : dims[lvl - 1].first;
+        L.h = lvl == 0 ? h : dims[lvl - 1].second;
+        L.lvl = lvl;
+    }
+    if ((uint64_t)w * h >= (1ull << 32)) return cudaErrorInvalidValue;
+    J.W = w;
+    J.H = h;
+    for (int q = 0; q < 8; q++) J.init[q] = init[q];
+    J.nfree = 0;
+    for (int q = 0; q < 8; q++)
+        if (freem[q]) J.free_idx[J.nfree++] = q;
+    if (g_nm_blocks == 0) {
+        int dev = 0, sms = 0, per = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, nm_search_kernel, 256, 0);
+        if (e != cudaSuccess) return e;
+        g_nm_blocks = std::max(1, std::min(per, 4)) * sms;
+    }
+    if (g_nm_blocks > NM_MAX_BLOCKS) g_nm_blocks = NM_MAX_BLOCKS;
+    J.part = C.nm_part;
+    J.cand = C.nm_cand;
+    J.ctl = C.nm_ctl;
+    J.out = C.nm_out;
+    void* args[] = {(void*)&J};
+    lsb_launched();
+    cudaError_t e = cudaLaunchCooperativeKernel((void*)nm_search_kernel, dim3(g_nm_blocks), dim3(256), args, 0, C.s);
+    if (e != cudaSuccess) return e;
+    cudaMemcpyAsync(C.sums_host, C.nm_out, sizeof(double) * 8, cudaMemcpyDeviceToHost, C.s);
+    int ev[2] = {0, 0};
+    cudaMemcpyAsync(ev, C.nm_ctl, sizeof ev, cudaMemcpyDeviceToHost, C.s);
+    e = cudaStreamSynchronize(C.s);
+    if (e != cudaSuccess) return e;
+    for (int q = 0; q < 8; q++) out[q] = C.sums_host[q];
+    C.evals += ev[1];
+    C.launches++;
+    return cudaSuccess;
+}
+
+cudaError_t multiscale_align(AlignCtx& C, const float* rf, const std::vector<float*>& pr, const float* tg,
+                             const std::vector<float*>& pt, int w, int h, const double init[8], const bool freem[8], int coarsen,
+                             double out[8]) {
+    if (C.device_search) return multiscale_align_dev(C, rf, pr, tg, pt, w, h, init, freem, coarsen, out);
+    return multiscale_align_host(C, rf, pr, tg, pt, w, h, init, freem, coarsen, out);
 }
 
 // ------------------------------------------ the cost without any allocation
@@ -546,7 +937,7 @@ extern "C" const char* lsb_warp_cost_noalloc(const float* rf_dev, uint32_t aw, u
     const int nblocks = (int)std::min<size_t>(std::max<size_t>((npx + 255) / 256, 1), NOALLOC_BLOCKS);
     dim3 g(nblocks, n_sims);
     lsb_launched(), cost_kernel<<<g, 256, 0, s>>>(rf_dev, (int)aw, (int)ah, tgt_dev, (int)tw, (int)th, cb, scratch);
-    lsb_launched(), cost_final_kernel<<<1, 32, 0, s>>>(scratch, nblocks, (int)n_sims, scratch + NOALLOC_PARTS);
+    lsb_launched(), cost_final_kernel<<<n_sims, 128, 0, s>>>(scratch, nblocks, (int)n_sims, scratch + NOALLOC_PARTS);
     double sums[MAX_CAND * 3];
     if (cudaMemcpyAsync(sums, scratch + NOALLOC_PARTS, sizeof(double) * 3 * n_sims, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
         cudaStreamSynchronize(s) != cudaSuccess)

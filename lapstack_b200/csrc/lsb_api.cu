@@ -66,6 +66,7 @@ struct DevPool {
 struct lsb_engine {
     lsb_config cfg;
     int device, sms, grid;
+    int coop = 0;  // cooperative launch: the registration search runs on the device
     cudaStream_t s;
     DevPool pool;
     unsigned *hist, *sel;
@@ -90,6 +91,7 @@ struct lsb_stack {
     DevPool pool;
     uint16_t* frames = nullptr;
     float* frames_f32 = nullptr;
+    void* warped = nullptr;  // aligned frames, written once before the fold (f32 planar or u16 interleaved)
     std::vector<void*> g;      // G storage per level 1..levels (index l)
     std::vector<float*> acc, best;
     uint16_t* winner = nullptr;
@@ -157,6 +159,15 @@ char* lsb_engine_create(const lsb_config* cfg, lsb_engine** out) {
     TRY(e->pool.get(&e->actx.part, MAX_CAND * 296 * 3));
     TRY(e->pool.get(&e->actx.sums_dev, MAX_CAND * 3));
     TRY(cudaHostAlloc((void**)&e->actx.sums_host, sizeof(double) * MAX_CAND * 3, cudaHostAllocDefault));
+    TRY(e->pool.get(&e->actx.nm_part, (size_t)MAX_CAND * NM_MAX_BLOCKS * 3));
+    TRY(e->pool.get(&e->actx.nm_cand, MAX_CAND * 9));
+    TRY(e->pool.get(&e->actx.nm_ctl, 2));
+    TRY(e->pool.get(&e->actx.nm_out, 8));
+    {
+        int coop = 0;
+        TRY(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, e->cfg.device));
+        e->coop = coop;
+    }
     for (auto& v : e->ev) TRY(cudaEventCreate(&v));
     *out = e;
     return nullptr;
@@ -251,6 +262,12 @@ static char* stack_alloc(lsb_stack* s) {
         TRY(P.get(&s->cfull, W * H));
     }
     if (s->ap.enabled && N > 1) {
+        {
+            void* p = nullptr;
+            TRY(cudaMalloc(&p, N * W * H * (s->storage == STORE_F32 ? 3 * sizeof(float) : 3 * sizeof(uint16_t))));
+            P.ptrs.push_back(p);
+            s->warped = p;
+        }
         TRY(P.get(&s->yt, W * H));
         TRY(P.get(&s->yr, W * H));
         std::vector<std::pair<int, int>> dims;
@@ -429,6 +446,7 @@ static char* run_align(lsb_stack* s) {
         TRY(luma_u16(f, W, H, s->yt, e->s));
         if (i > 0) {
             TRY(gauss_levels(s->yt, W, H, s->pt, e->s));
+            C.device_search = s->ap.host_search ? 0 : e->coop;
             TRY(multiscale_align(C, s->yr, s->pr, s->yt, s->pt, W, H, &s->sims[8 * (size_t)(i - 1)], freem, (int)s->ap.coarsen, sim));
         }
         if (i + 1 < n) {
@@ -543,6 +561,9 @@ static char* run_pipeline(lsb_stack* s) {
         }
     }
     TRY(cudaMemcpyAsync(s->xf_dev, s->xf.data(), sizeof(FrameXform) * n, cudaMemcpyHostToDevice, st));
+    // the aligned frames, written once (align.rs:489 with stack.rs:668's fallback); the fold reads them
+    const bool warped = aligned;
+    if (warped) TRY(warp_frames(s->frames, s->xf_dev, (int)s->ap.interp, W, H, n, s->storage != STORE_F32, s->warped, st));
     TRY(cudaMemsetAsync(s->status, 0, sizeof(int), st));
     TRY(cudaEventRecord(ev[2], st));
     // ---- the fold, level by level over all frames
@@ -568,8 +589,8 @@ static char* run_pipeline(lsb_stack* s) {
         a.tiles_x = (a.W + 63) / 64;
         a.tiles_y = (a.H + 31) / 32;
         a.ntiles = a.tiles_x * a.tiles_y;
-        a.src_u16 = s->frames;
-        a.src_f32 = s->frames_f32;
+        a.src_u16 = warped && s->storage != STORE_F32 ? (const uint16_t*)s->warped : s->frames;
+        a.src_f32 = warped && s->storage == STORE_F32 ? (const float*)s->warped : s->frames_f32;
         a.xf = s->xf_dev;
         a.interp = (int)s->ap.interp;
         a.src_g = l > 0 ? s->g[l] : nullptr;
@@ -591,7 +612,7 @@ static char* run_pipeline(lsb_stack* s) {
         }
         a.gscale = gscale;
         a.ginv = ginv;
-        const int src = l > 0 ? SRC_G : (s->f32src ? SRC_F32 : SRC_U16);
+        const int src = l > 0 ? SRC_G : ((s->f32src || (warped && s->storage == STORE_F32)) ? SRC_F32 : SRC_U16);
         if (l == 0) TRY(cudaEventRecord(ev[8], st));
         TRY(fold_level(a, src, s->storage, (int)s->fp.energy_radius, focus, st, e->grid));
         if (l == 0) TRY(cudaEventRecord(ev[9], st));
@@ -1034,6 +1055,7 @@ extern "C" char* lsb_align_pair(lsb_engine* e, const float* rf, const float* tg,
     bool fr[8];
     for (int k = 0; k < 8; k++) fr[k] = free8 ? free8[k] != 0 : (k < 4);
     e->actx.evals = 0;
+    e->actx.device_search = e->coop;
     TRY(multiscale_align(e->actx, a, pr, b, pt, (int)w, (int)h, init8 ? init8 : id, fr, (int)coarsen, out8));
     if (evals) *evals = (uint32_t)e->actx.evals;
     return nullptr;

@@ -30,272 +30,41 @@
 
 namespace lsb {
 
-constexpr int TW = 64, TH = 32, NT = 256, PPT = (TW * TH) / NT;
-constexpr int RMAX = 2;
-constexpr int LW_MAX = TW + 2 * RMAX, LH_MAX = TH + 2 * RMAX;
-constexpr int AW_MAX = LW_MAX / 2 + 5, AH_MAX = LH_MAX / 2 + 5;
-constexpr int GW_MAX = 2 * AW_MAX + 4, GH_MAX = 2 * AH_MAX + 4;
-constexpr int G0_MAX = GW_MAX * GH_MAX;
-constexpr int SCR_MAX = GH_MAX * AW_MAX + AH_MAX * AW_MAX + AH_MAX * LW_MAX;
-constexpr int YB_MAX = LW_MAX * LH_MAX;
-constexpr int FOC_R = 3;
-static_assert((TW + 2 * FOC_R) * (TH + 2 * FOC_R) <= SCR_MAX, "focus window must fit the scratch");
-static_assert(LH_MAX * TW <= SCR_MAX, "window scratch must fit");
-constexpr int SMEM_FLOATS = 3 * G0_MAX + SCR_MAX + YB_MAX + 3 * TW * TH;
+#include "lsb_level.cuh"
 
-// conv_sparse taps (depth.rs:417) in the per-pixel accumulation order: rows
-// grouped by dy in order of first appearance, within a row in list order.
-__constant__ float c_taps[3 * 64];
-
-// binomial(R) of fuse.rs:139: C(2R, t) / 4^R, exact in f32.
-template <int R>
-__device__ __forceinline__ float binw(int t) {
-    if (R == 1) return t == 1 ? 0.5f : 0.25f;
-    if (R == 2) return t == 2 ? 0.375f : (t == 1 || t == 3 ? 0.25f : 0.0625f);
-    return 1.f;
-}
-
-template <int SRC, class GS, int R, bool FOCUS, class SS>
-__global__ void __launch_bounds__(NT, 2) fold_level_kernel(const FoldArgs a) {
-    extern __shared__ float sm[];
-    float* g0 = sm;                     // [3][gh][gw]
-    float* scr = g0 + 3 * G0_MAX;       // per-channel scratch / focus luma / window rows
-    float* yb = scr + SCR_MAX;          // [lh][lw] luma (then energy) of L
-    float* lo = yb + YB_MAX;            // [3][TH][TW] L at the tile's own pixels
-    const int tid = threadIdx.x;
-    const int W = a.W, H = a.H, W1 = a.W1, H1 = a.H1;
-    const float2 sc = make_float2(a.gscale, a.ginv);
-
-    for (int tile = blockIdx.x; tile < a.ntiles; tile += gridDim.x) {
-        const int x0 = (tile % a.tiles_x) * TW, y0 = (tile / a.tiles_x) * TH;
-        const int xL0 = max(0, x0 - R), xL1 = min(W, x0 + TW + R);
-        const int yL0 = max(0, y0 - R), yL1 = min(H, y0 + TH + R);
-        const int xA0 = max(0, (xL0 >> 1) - 1), xA1 = min(W1, ((xL1 - 1) >> 1) + 2);
-        const int yA0 = max(0, (yL0 >> 1) - 1), yA1 = min(H1, ((yL1 - 1) >> 1) + 2);
-        const int xG0 = max(0, 2 * xA0 - 2), xG1 = min(W, 2 * xA1 + 1);
-        const int yG0 = max(0, 2 * yA0 - 2), yG1 = min(H, 2 * yA1 + 1);
-        const int gw = xG1 - xG0, gh = yG1 - yG0, aw = xA1 - xA0, ah = yA1 - yA0, lw = xL1 - xL0, lh = yL1 - yL0;
-        if (gw > GW_MAX || gh > GH_MAX || aw > AW_MAX || ah > AH_MAX) {
-            if (tid == 0) atomicOr(a.status, LSB_ERR_SHAPE);
-            return;
-        }
-        float* tmph = scr;                       // [gh][aw]
-        float* g1 = tmph + GH_MAX * AW_MAX;      // [ah][aw]
-        float* exph = g1 + AH_MAX * AW_MAX;      // [ah][lw]
-        const int ox1 = min(TW, W - x0), oy1 = min(TH, H - y0);  // the tile's own extent
-
-        float best[PPT], acc[PPT][3];
-        int win[PPT];
-#pragma unroll
-        for (int j = 0; j < PPT; j++) {
-            best[j] = -1.f;  // any energy (>= 0) beats it: frame 0 fills the accumulator (fuse.rs:409-412)
-            acc[j][0] = acc[j][1] = acc[j][2] = 0.f;
-            win[j] = 0;
-        }
-
-        for (int k = 0; k < a.nframes; k++) {
-            // ---- stage G_l over the window, three channels
-            if (SRC == SRC_U16) {
-                const uint16_t* f = a.src_u16 + (size_t)k * W * H * 3;
-                const FrameXform xf = a.xf[k];
-                for (int i = tid; i < gh * gw; i += NT) {
-                    float v[3];
-                    load_u16_px(f, xf, a.interp, W, H, xG0 + i % gw, yG0 + i / gw, v);
-                    g0[i] = v[0];
-                    g0[G0_MAX + i] = v[1];
-                    g0[2 * G0_MAX + i] = v[2];
-                }
-            } else if (SRC == SRC_F32) {
-                const float* f = a.src_f32 + (size_t)k * 3 * W * H;
-                for (int c = 0; c < 3; c++)
-                    for (int i = tid; i < gh * gw; i += NT)
-                        g0[c * G0_MAX + i] = f[((size_t)c * H + yG0 + i / gw) * W + xG0 + i % gw];
-            } else {
-                const GS* f = (const GS*)a.src_g + (size_t)k * 3 * W * H;
-                for (int c = 0; c < 3; c++)
-                    for (int i = tid; i < gh * gw; i += NT)
-                        g0[c * G0_MAX + i] = Store<GS>::ld(f + ((size_t)c * H + yG0 + i / gw) * W + xG0 + i % gw, sc);
-            }
-            __syncthreads();
-
-            // ---- the focus slice of this frame (level 0): depth.rs:1097 focus_slice
-            if (FOCUS) {
-                const int xF0 = max(0, x0 - FOC_R), xF1 = min(W, x0 + TW + FOC_R);
-                const int yF0 = max(0, y0 - FOC_R), yF1 = min(H, y0 + TH + FOC_R);
-                const int fw = xF1 - xF0, fh = yF1 - yF0;
-                float* yl = scr;
-                for (int i = tid; i < fw * fh; i += NT) {
-                    int gi = (yF0 + i / fw - yG0) * gw + (xF0 + i % fw - xG0);
-                    yl[i] = lsb_luma(g0[gi], g0[G0_MAX + gi], g0[2 * G0_MAX + gi]);
-                }
-                __syncthreads();
-                const int bk = a.bk;
-                const int cx0 = x0 / bk, cy0 = y0 / bk;
-                const int cw = min(TW / bk, a.dw - cx0), chh = min(TH / bk, a.dh - cy0);
-                for (int i = tid; i < cw * chh; i += NT) {
-                    const int cx = cx0 + i % cw, cy = cy0 + i / cw;
-                    const int px0 = cx * bk, px1 = min(px0 + bk, W), py0 = cy * bk, py1 = min(py0 + bk, H);
-                    float o = 0.f;
-                    for (int y = py0; y < py1; y++) {
-                        float rs = 0.f;
-                        for (int x = px0; x < px1; x++) {
-                            float m;
-                            if (a.focus_kind == 0) {
-                                float s = 0.f;
-                                for (int t = 0; t < a.ntaps; t++) {
-                                    int yy = lsb_reflect(y + (int)c_taps[3 * t], H) - yF0;
-                                    int xx = lsb_reflect(x + (int)c_taps[3 * t + 1], W) - xF0;
-                                    s = __fadd_rn(s, __fmul_rn(c_taps[3 * t + 2], yl[yy * fw + xx]));
-                                }
-                                m = fabsf(s);
-                            } else {
-                                const int st = a.sml_step;
-                                float c = yl[(y - yF0) * fw + x - xF0];
-                                float l = yl[(y - yF0) * fw + lsb_reflect(x - st, W) - xF0];
-                                float r = yl[(y - yF0) * fw + lsb_reflect(x + st, W) - xF0];
-                                float u = yl[(lsb_reflect(y - st, H) - yF0) * fw + x - xF0];
-                                float d = yl[(lsb_reflect(y + st, H) - yF0) * fw + x - xF0];
-                                float c2 = __fmul_rn(2.f, c);
-                                m = __fadd_rn(fabsf(__fsub_rn(__fsub_rn(c2, l), r)), fabsf(__fsub_rn(__fsub_rn(c2, u), d)));
-                            }
-                            rs = __fadd_rn(rs, m);
-                        }
-                        o = __fadd_rn(o, rs);
-                    }
-                    o = __fdiv_rn(o, (float)((py1 - py0) * (px1 - px0)));
-                    lsb_st<SS>((SS*)a.slice + ((size_t)k * a.dh + cy) * a.dw + cx, o);
-                }
-                __syncthreads();
-            }
-
-            // ---- per channel: REDUCE to G_{l+1}, EXPAND back, L = G - EXPAND(G_{l+1})
-            for (int c = 0; c < 3; c++) {
-                const float* G = g0 + c * G0_MAX;
-                for (int i = tid; i < gh * aw; i += NT) {
-                    const int r = i / aw, cc = 2 * (xA0 + i % aw);
-                    const float* row = G + r * gw - xG0;
-                    tmph[i] = lsb_tap5(row[lsb_reflect(cc - 2, W)], row[lsb_reflect(cc - 1, W)], row[lsb_reflect(cc, W)],
-                                       row[lsb_reflect(cc + 1, W)], row[lsb_reflect(cc + 2, W)]);
-                }
-                __syncthreads();
-                GS* dst = (GS*)a.dst_g + ((size_t)k * 3 + c) * W1 * H1;
-                for (int i = tid; i < ah * aw; i += NT) {
-                    const int iy = yA0 + i / aw, jx = i % aw, cc = 2 * iy;
-                    const float* col = tmph + jx - yG0 * aw;
-                    float v = lsb_tap5(col[lsb_reflect(cc - 2, H) * aw], col[lsb_reflect(cc - 1, H) * aw], col[lsb_reflect(cc, H) * aw],
-                                       col[lsb_reflect(cc + 1, H) * aw], col[lsb_reflect(cc + 2, H) * aw]);
-                    const int gx = xA0 + jx;
-                    if (gx >= (x0 >> 1) && gx < ((x0 + TW) >> 1) && iy >= (y0 >> 1) && iy < ((y0 + TH) >> 1))
-                        Store<GS>::st(dst + (size_t)iy * W1 + gx, v, sc);
-                    // the coarse level as stored: with 16-bit storage the next level sees the rounded value
-                    g1[i] = Store<GS>::as_stored(v, sc);
-                }
-                __syncthreads();
-                for (int i = tid; i < ah * lw; i += NT) {
-                    const int r = i / lw, x = xL0 + i % lw, cx = x >> 1;
-                    const float* row = g1 + r * aw - xA0;
-                    exph[i] = (x & 1) == 0 ? lsb_exp_even(row[lsb_reflect(cx - 1, W1)], row[lsb_reflect(cx, W1)], row[lsb_reflect(cx + 1, W1)])
-                                           : lsb_exp_odd(row[lsb_reflect(cx, W1)], row[lsb_reflect(cx + 1, W1)]);
-                }
-                __syncthreads();
-                for (int i = tid; i < lh * lw; i += NT) {
-                    const int y = yL0 + i / lw, xi = i % lw, x = xL0 + xi, cy = y >> 1;
-                    const float* col = exph + xi - yA0 * lw;
-                    const float up = (y & 1) == 0 ? lsb_exp_even(col[lsb_reflect(cy - 1, H1) * lw], col[lsb_reflect(cy, H1) * lw], col[lsb_reflect(cy + 1, H1) * lw])
-                                                   : lsb_exp_odd(col[lsb_reflect(cy, H1) * lw], col[lsb_reflect(cy + 1, H1) * lw]);
-                    const float L = __fsub_rn(G[(y - yG0) * gw + x - xG0], up);
-                    if (a.use_chroma) {
-                        const float q = __fmul_rn(L, L);
-                        yb[i] = c == 0 ? q : __fadd_rn(yb[i], q);
-                    } else {
-                        const float q = __fmul_rn(c == 0 ? 0.299f : (c == 1 ? 0.587f : 0.114f), L);
-                        yb[i] = c == 0 ? q : __fadd_rn(yb[i], q);
-                    }
-                    if (x >= x0 && x < x0 + TW && y >= y0 && y < y0 + TH) lo[(c * TH + y - y0) * TW + x - x0] = L;
-                }
-                __syncthreads();
-            }
-
-            // ---- region energy: e = Y^2, the separable binomial window (fuse.rs:168)
-            if (!a.use_chroma)
-                for (int i = tid; i < lh * lw; i += NT) yb[i] = __fmul_rn(yb[i], yb[i]);
-            float* eh = scr;  // [lh][TW]
-            if (R > 0) {
-                __syncthreads();
-                for (int i = tid; i < lh * TW; i += NT) {
-                    const int r = i / TW, xo = i % TW;
-                    if (xo >= ox1) continue;
-                    const float* row = yb + r * lw - xL0;
-                    float s = 0.f;
-#pragma unroll
-                    for (int t = 0; t <= 2 * R; t++) s = __fadd_rn(s, __fmul_rn(binw<R>(t), row[lsb_reflect(x0 + xo + t - R, W)]));
-                    eh[i] = s;
-                }
-            }
-            __syncthreads();
-#pragma unroll
-            for (int j = 0; j < PPT; j++) {
-                const int p = tid + NT * j, px = p % TW, py = p / TW;
-                if (px >= ox1 || py >= oy1) continue;
-                float e;
-                if (R > 0) {
-                    e = 0.f;
-#pragma unroll
-                    for (int t = 0; t <= 2 * R; t++)
-                        e = __fadd_rn(e, __fmul_rn(binw<R>(t), eh[(lsb_reflect(y0 + py + t - R, H) - yL0) * TW + px]));
-                } else {
-                    e = yb[(y0 + py - yL0) * lw + x0 + px - xL0];
-                }
-                if (e > best[j]) {
-                    best[j] = e;
-                    acc[j][0] = lo[(0 * TH + py) * TW + px];
-                    acc[j][1] = lo[(1 * TH + py) * TW + px];
-                    acc[j][2] = lo[(2 * TH + py) * TW + px];
-                    win[j] = k;
-                }
-            }
-            __syncthreads();
-        }
-
-        // ---- the level's accumulator, written once
-#pragma unroll
-        for (int j = 0; j < PPT; j++) {
-            const int p = tid + NT * j, px = p % TW, py = p / TW;
-            if (px >= ox1 || py >= oy1) continue;
-            const size_t o = (size_t)(y0 + py) * W + x0 + px;
-            a.acc[o] = acc[j][0];
-            a.acc[(size_t)W * H + o] = acc[j][1];
-            a.acc[2 * (size_t)W * H + o] = acc[j][2];
-            a.best[o] = best[j];
-            if (a.winner) a.winner[o] = (uint16_t)win[j];
-        }
-    }
-}
-
-size_t fold_smem_bytes(int, bool) { return (size_t)SMEM_FLOATS * sizeof(float); }
+size_t fold_smem_bytes(int, bool) { return (size_t)SEL_FLOATS * sizeof(float); }
 
 cudaError_t set_focus_taps(const float* taps3, int ntaps, cudaStream_t s) {
     if (ntaps > 64) return cudaErrorInvalidValue;
     return cudaMemcpyToSymbolAsync(c_taps, taps3, sizeof(float) * 3 * ntaps, 0, cudaMemcpyHostToDevice, s);
 }
 
+template <class K>
+static cudaError_t with_smem(K k, size_t smem) {
+    return cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+}
+
+// One level: REDUCE every frame (and take the focus slices at level 0), then select.
 template <int SRC, class GS, int R, bool FOCUS, class SS>
-static cudaError_t launch_fold(const FoldArgs& a, cudaStream_t s, int grid_limit) {
-    auto k = fold_level_kernel<SRC, GS, R, FOCUS, SS>;
-    size_t smem = fold_smem_bytes(R, FOCUS);
-    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+static cudaError_t launch_level(const FoldArgs& a, cudaStream_t s, int grid_limit) {
+    const size_t rsm = (size_t)RED_FLOATS * sizeof(float), ssm = (size_t)SEL_FLOATS * sizeof(float);
+    auto kr = reduce_level_kernel<SRC, GS, FOCUS, SS>;
+    auto ks = select_level_kernel<SRC, GS, R>;
+    cudaError_t e = with_smem(kr, rsm);
+    if (e == cudaSuccess) e = with_smem(ks, ssm);
     if (e != cudaSuccess) return e;
-    int grid = std::min(a.ntiles, std::max(grid_limit, 1));
-    lsb_launched(), k<<<grid, NT, smem, s>>>(a);
+    const int rtiles = ((a.W1 + RW - 1) / RW) * ((a.H1 + RH - 1) / RH);
+    lsb_launched(), kr<<<dim3(rtiles, a.nframes), NT, rsm, s>>>(a);
+    lsb_launched(), ks<<<std::min(a.ntiles, std::max(grid_limit, 1)), NT, ssm, s>>>(a);
     return cudaGetLastError();
 }
 
 template <int SRC, class GS, int R>
 static cudaError_t pick_focus(const FoldArgs& a, bool focus, cudaStream_t s, int gl) {
-    if (!focus) return launch_fold<SRC, GS, R, false, float>(a, s, gl);
+    if (!focus) return launch_level<SRC, GS, R, false, float>(a, s, gl);
     // 16-bit storage keeps the focus slices in FP16 (relative precision is what the peak search needs)
-    if (sizeof(GS) == 2) return launch_fold<SRC, GS, R, true, __half>(a, s, gl);
-    return launch_fold<SRC, GS, R, true, float>(a, s, gl);
+    if (sizeof(GS) == 2) return launch_level<SRC, GS, R, true, __half>(a, s, gl);
+    return launch_level<SRC, GS, R, true, float>(a, s, gl);
 }
 
 template <int SRC, class GS>
@@ -324,6 +93,14 @@ cudaError_t fold_level(const FoldArgs& a, int src_kind, int storage, int radius,
         case STORE_F16: return pick_src<__half>(a, src_kind, radius, focus, s, grid_limit);
         default: return pick_src<float>(a, src_kind, radius, focus, s, grid_limit);
     }
+}
+
+cudaError_t warp_frames(const uint16_t* frames, const FrameXform* xf, int interp, int w, int h, int n, bool u16_out, void* out,
+                        cudaStream_t s) {
+    dim3 g((w + 31) / 32, (h + 7) / 8, n);
+    if (u16_out) lsb_launched(), warp_frames_kernel<true><<<g, NT, 0, s>>>(frames, xf, interp, w, h, out);
+    else lsb_launched(), warp_frames_kernel<false><<<g, NT, 0, s>>>(frames, xf, interp, w, h, out);
+    return cudaGetLastError();
 }
 
 // ------------------------------------------------------------ residual level

@@ -55,6 +55,10 @@ enum Storage { STORE_F32 = 0, STORE_UNORM16 = 1, STORE_F16 = 2 };
 
 // Launchers (lsb_fold.cu).
 cudaError_t fold_level(const FoldArgs& a, int src_kind, int storage, int radius, bool focus, cudaStream_t s, int grid_limit);
+// Every frame through its warp (the pixel as shot where it leaves the frame):
+// f32 planar [n][3][h][w], or u16 interleaved [n][h][w][3] rounded to the u16 step.
+cudaError_t warp_frames(const uint16_t* frames, const FrameXform* xf, int interp, int w, int h, int n, bool u16_out, void* out,
+                        cudaStream_t s);
 cudaError_t set_focus_taps(const float* taps3, int ntaps, cudaStream_t s);
 size_t fold_smem_bytes(int radius, bool focus);
 

@@ -1,0 +1,400 @@
+// The fold kernels (one pyramid level, all frames) -- included by lsb_fold.cu
+// inside namespace lsb.
+//
+// Level l of the fold runs as two kernels:
+//  * reduce_level_kernel, one CTA per (frame, 32x16 tile of G_{l+1}): stages
+//    the tile's G_l window, REDUCEs rows then columns (pyramid.rs:86) and
+//    writes G_{l+1} once; at level 0 it also takes the frame's focus slice
+//    (depth.rs:1097: luma -> ring difference filter -> block mean) from the
+//    same staged window. Parallel over frames, so even the coarse levels fill
+//    the GPU.
+//  * select_level_kernel, persistent over 64x32 tiles of level l: walks the
+//    frames in order, stages G_l over the tile +- R and G_{l+1} over what
+//    EXPAND needs, forms L = G - EXPAND(G_{l+1}) (pyramid.rs:143/209), the
+//    luma energy and its binomial window (fuse.rs:152/168) and keeps the
+//    strict-> selection (fuse.rs:429) in registers: thread (tx, ty) owns
+//    the tile pixels (tx + 32a, ty + 8b), a < 2, b < 4.
+// Tiles whose windows never reach the border index without reflect-101
+// (IN = true); border tiles reflect as pyramid.rs:51 does. Every float op is
+// an explicit round-to-nearest intrinsic in the reference's order.
+#pragma once
+
+constexpr int NT = 256;
+// select: tile, own pixels per thread, windows
+constexpr int TW = 64, TH = 32, PPT = (TW * TH) / NT;
+constexpr int RMAX = 2;
+constexpr int LW_MAX = TW + 2 * RMAX, LH_MAX = TH + 2 * RMAX;
+constexpr int AW_MAX = LW_MAX / 2 + 5, AH_MAX = LH_MAX / 2 + 5;
+constexpr int SEL_GL = LW_MAX * LH_MAX;  // per channel
+constexpr int SEL_G1 = AW_MAX * AH_MAX;
+constexpr int SEL_EXP = AH_MAX * LW_MAX;
+constexpr int SEL_FLOATS = 3 * (SEL_GL + SEL_G1 + SEL_EXP) + LW_MAX * LH_MAX;
+static_assert(LH_MAX * TW <= 3 * SEL_EXP, "the window rows fit the EXPAND scratch");
+// reduce: tile of G_{l+1}, G_l window with the focus halo
+constexpr int RW = 32, RH = 16, FOC_R = 3;
+constexpr int RGW = 2 * RW + 2 * FOC_R, RGH = 2 * RH + 2 * FOC_R;  // 70 x 38
+constexpr int RED_FLOATS = 3 * RGW * RGH + RGW * RGH + 3 * RGH * RW;
+
+// conv_sparse taps (depth.rs:417) in the per-pixel accumulation order: rows
+// grouped by dy in order of first appearance, within a row in list order.
+__constant__ float c_taps[3 * 64];
+
+// binomial(R) of fuse.rs:139: C(2R, t) / 4^R, exact in f32.
+template <int R>
+__device__ __forceinline__ float binw(int t) {
+    if (R == 1) return t == 1 ? 0.5f : 0.25f;
+    if (R == 2) return t == 2 ? 0.375f : (t == 1 || t == 3 ? 0.25f : 0.0625f);
+    return 1.f;
+}
+
+// The level-l value of (x, y), three channels, from the level's source:
+// level 0 the frame (u16 interleaved or f32 planar) times its gains
+// (brightness.rs:124); above, the stored Gaussian level.
+template <int SRC, class GS>
+__device__ __forceinline__ void level_px(const FoldArgs& a, int k, int x, int y, float v[3]) {
+    const size_t np = (size_t)a.W * a.H, o = (size_t)y * a.W + x;
+    if (SRC == SRC_U16) {
+        const uint16_t* p = a.src_u16 + (size_t)k * np * 3 + o * 3;
+        v[0] = __fmul_rn((float)p[0], LSB_INV16);
+        v[1] = __fmul_rn((float)p[1], LSB_INV16);
+        v[2] = __fmul_rn((float)p[2], LSB_INV16);
+    } else if (SRC == SRC_F32) {
+        const float* p = a.src_f32 + (size_t)k * 3 * np + o;
+        v[0] = p[0];
+        v[1] = p[np];
+        v[2] = p[2 * np];
+    } else {
+        const float2 sc = make_float2(a.gscale, a.ginv);
+        const GS* p = (const GS*)a.src_g + (size_t)k * 3 * np + o;
+        v[0] = Store<GS>::ld(p, sc);
+        v[1] = Store<GS>::ld(p + np, sc);
+        v[2] = Store<GS>::ld(p + 2 * np, sc);
+        return;
+    }
+    const int gon = a.xf[k].gain_on;
+    if (gon) {
+        for (int c = 0; c < 3; c++)
+            if (gon & (1 << c)) v[c] = __fmul_rn(v[c], a.xf[k].gain[c]);
+    }
+}
+
+// ------------------------------------------------------------------ REDUCE
+template <int SRC, class GS, bool FOCUS, class SS, bool IN>
+__device__ __forceinline__ void reduce_tile(const FoldArgs& a, float* __restrict__ sm, int k, int gx0, int gy0) {
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+    const int W = a.W, H = a.H, W1 = a.W1, H1 = a.H1;
+#define RX(i) (IN ? (i) : lsb_reflect((i), W))
+#define RY(i) (IN ? (i) : lsb_reflect((i), H))
+    float* g0 = sm;                      // [3][wh][ww]
+    float* yl = g0 + 3 * RGW * RGH;      // [wh][ww] focus luma
+    float* tmph = yl + RGW * RGH;        // [3][wh][RW]
+    const int xw0 = max(0, 2 * gx0 - FOC_R), xw1 = min(W, 2 * gx0 + 2 * RW + FOC_R);
+    const int yw0 = max(0, 2 * gy0 - FOC_R), yw1 = min(H, 2 * gy0 + 2 * RH + FOC_R);
+    const int ww = xw1 - xw0, wh = yw1 - yw0;
+    for (int r = ty; r < wh; r += 8)
+        for (int c = tx; c < ww; c += 32) {
+            float v[3];
+            level_px<SRC, GS>(a, k, xw0 + c, yw0 + r, v);
+            const int i = r * ww + c;
+            g0[i] = v[0];
+            g0[RGW * RGH + i] = v[1];
+            g0[2 * RGW * RGH + i] = v[2];
+            if (FOCUS) yl[i] = lsb_luma(v[0], v[1], v[2]);
+        }
+    __syncthreads();
+    const int ow = min(RW, W1 - gx0), oh = min(RH, H1 - gy0);
+    // rows (pyramid.rs:90)
+    for (int r = ty; r < wh; r += 8)
+        for (int j = tx; j < ow; j += 32) {
+            const int cc = 2 * (gx0 + j);
+            const int i0 = RX(cc - 2) - xw0, i1 = RX(cc - 1) - xw0, i2 = RX(cc) - xw0, i3 = RX(cc + 1) - xw0, i4 = RX(cc + 2) - xw0;
+#pragma unroll
+            for (int c = 0; c < 3; c++) {
+                const float* row = g0 + c * RGW * RGH + r * ww;
+                tmph[(c * RGH + r) * RW + j] = lsb_tap5(row[i0], row[i1], row[i2], row[i3], row[i4]);
+            }
+        }
+    if (FOCUS) {
+        const int bk = a.bk;
+        const int cx0 = (2 * gx0) / bk, cy0 = (2 * gy0) / bk;
+        const int cw = min(2 * RW / bk, a.dw - cx0), chh = min(2 * RH / bk, a.dh - cy0);
+        for (int cyy = ty; cyy < chh; cyy += 8)
+            for (int cxx = tx; cxx < cw; cxx += 32) {
+                const int cx = cx0 + cxx, cy = cy0 + cyy;
+                const int px0 = cx * bk, px1 = min(px0 + bk, W), py0 = cy * bk, py1 = min(py0 + bk, H);
+                float o = 0.f;
+                for (int y = py0; y < py1; y++) {
+                    float rs = 0.f;
+                    for (int x = px0; x < px1; x++) {
+                        float m;
+                        if (a.focus_kind == 0) {
+                            float s = 0.f;
+                            for (int q = 0; q < a.ntaps; q++) {
+                                const int yy = RY(y + (int)c_taps[3 * q]) - yw0, xx = RX(x + (int)c_taps[3 * q + 1]) - xw0;
+                                s = __fadd_rn(s, __fmul_rn(c_taps[3 * q + 2], yl[yy * ww + xx]));
+                            }
+                            m = fabsf(s);
+                        } else {
+                            const int st = a.sml_step;
+                            const float c = yl[(y - yw0) * ww + x - xw0];
+                            const float l = yl[(y - yw0) * ww + RX(x - st) - xw0], r = yl[(y - yw0) * ww + RX(x + st) - xw0];
+                            const float u = yl[(RY(y - st) - yw0) * ww + x - xw0], d = yl[(RY(y + st) - yw0) * ww + x - xw0];
+                            const float c2 = __fmul_rn(2.f, c);
+                            m = __fadd_rn(fabsf(__fsub_rn(__fsub_rn(c2, l), r)), fabsf(__fsub_rn(__fsub_rn(c2, u), d)));
+                        }
+                        rs = __fadd_rn(rs, m);
+                    }
+                    o = __fadd_rn(o, rs);
+                }
+                lsb_st<SS>((SS*)a.slice + ((size_t)k * a.dh + cy) * a.dw + cx, __fdiv_rn(o, (float)((py1 - py0) * (px1 - px0))));
+            }
+    }
+    __syncthreads();
+    // columns (pyramid.rs:104) -> G_{l+1}
+    const float2 sc = make_float2(a.gscale, a.ginv);
+    for (int i = ty; i < oh; i += 8) {
+        const int cy = 2 * (gy0 + i);
+        const int r0 = RY(cy - 2) - yw0, r1 = RY(cy - 1) - yw0, r2 = RY(cy) - yw0, r3 = RY(cy + 1) - yw0, r4 = RY(cy + 2) - yw0;
+        for (int j = tx; j < ow; j += 32) {
+#pragma unroll
+            for (int c = 0; c < 3; c++) {
+                const float* col = tmph + c * RGH * RW + j;
+                const float v = lsb_tap5(col[r0 * RW], col[r1 * RW], col[r2 * RW], col[r3 * RW], col[r4 * RW]);
+                Store<GS>::st((GS*)a.dst_g + (((size_t)k * 3 + c) * H1 + gy0 + i) * W1 + gx0 + j, v, sc);
+            }
+        }
+    }
+#undef RX
+#undef RY
+}
+
+template <int SRC, class GS, bool FOCUS, class SS>
+__global__ void __launch_bounds__(NT) reduce_level_kernel(const FoldArgs a) {
+    extern __shared__ float sm[];
+    const int tiles_x = (a.W1 + RW - 1) / RW;
+    const int gx0 = (blockIdx.x % tiles_x) * RW, gy0 = (blockIdx.x / tiles_x) * RH;
+    const int k = blockIdx.y;
+    const bool interior = 2 * gx0 - FOC_R >= 0 && 2 * gx0 + 2 * RW + FOC_R <= a.W && 2 * gy0 - FOC_R >= 0 &&
+                          2 * gy0 + 2 * RH + FOC_R <= a.H;
+    if (interior) reduce_tile<SRC, GS, FOCUS, SS, true>(a, sm, k, gx0, gy0);
+    else reduce_tile<SRC, GS, FOCUS, SS, false>(a, sm, k, gx0, gy0);
+}
+
+// ------------------------------------------------------------------ select
+struct TileWin {
+    int x0, y0, xL0, xL1, yL0, yL1, xA0, xA1, yA0, yA1, lw, lh, aw, ah, ox1, oy1;
+};
+
+template <int SRC, class GS, int R, bool IN>
+__device__ __forceinline__ void select_frame(const FoldArgs& a, float* __restrict__ sm, int k, const TileWin& t,
+                                             float (&best)[PPT], float (&acc)[PPT][3], int (&win)[PPT]) {
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+    const int W = a.W, H = a.H, W1 = a.W1, H1 = a.H1;
+#define RX(i) (IN ? (i) : lsb_reflect((i), W))
+#define RY(i) (IN ? (i) : lsb_reflect((i), H))
+#define RX1(i) (IN ? (i) : lsb_reflect((i), W1))
+#define RY1(i) (IN ? (i) : lsb_reflect((i), H1))
+    float* gl = sm;                      // [3][lh][lw]   G_l over the tile +- R
+    float* g1 = gl + 3 * SEL_GL;         // [3][ah][aw]   G_{l+1} as stored
+    float* exph = g1 + 3 * SEL_G1;       // [3][ah][lw]   EXPAND along rows
+    float* yb = exph + 3 * SEL_EXP;      // [lh][lw]      node energy
+    const int lw = t.lw, lh = t.lh, aw = t.aw, ah = t.ah;
+    const float2 sc = make_float2(a.gscale, a.ginv);
+
+    // ---- 1: stage G_l and G_{l+1}
+    for (int r = ty; r < lh; r += 8)
+        for (int c = tx; c < lw; c += 32) {
+            float v[3];
+            level_px<SRC, GS>(a, k, t.xL0 + c, t.yL0 + r, v);
+            const int i = r * lw + c;
+            gl[i] = v[0];
+            gl[SEL_GL + i] = v[1];
+            gl[2 * SEL_GL + i] = v[2];
+        }
+    {
+        const GS* f = (const GS*)a.dst_g + (size_t)k * 3 * W1 * H1;
+        for (int c = 0; c < 3; c++)
+            for (int r = ty; r < ah; r += 8) {
+                const GS* row = f + ((size_t)c * H1 + t.yA0 + r) * W1 + t.xA0;
+                for (int x = tx; x < aw; x += 32) g1[c * SEL_G1 + r * aw + x] = Store<GS>::ld(row + x, sc);
+            }
+    }
+    __syncthreads();
+
+    // ---- 2: EXPAND along rows (pyramid.rs:147)
+    for (int i = ty; i < ah; i += 8)
+        for (int xi = tx; xi < lw; xi += 32) {
+            const int x = t.xL0 + xi, cx = x >> 1;
+            const bool even = (x & 1) == 0;
+            const int ja = RX1(cx - 1) - t.xA0, jb = RX1(cx) - t.xA0, jc = RX1(cx + 1) - t.xA0;
+#pragma unroll
+            for (int c = 0; c < 3; c++) {
+                const float* row = g1 + c * SEL_G1 + i * aw;
+                exph[c * SEL_EXP + i * lw + xi] = even ? lsb_exp_even(row[ja], row[jb], row[jc]) : lsb_exp_odd(row[jb], row[jc]);
+            }
+        }
+    __syncthreads();
+
+    // ---- 3: EXPAND along columns, L = G - EXPAND(G_{l+1}), node energy (fuse.rs:152)
+    auto lpoint = [&](int x, int y, float L[3]) -> float {
+        const int xi = x - t.xL0, cy = y >> 1;
+        const bool even = (y & 1) == 0;
+        const int ra = (RY1(cy - 1) - t.yA0) * lw, rb = (RY1(cy) - t.yA0) * lw, rc = (RY1(cy + 1) - t.yA0) * lw;
+        const int gi = (y - t.yL0) * lw + xi;
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+            const float* col = exph + c * SEL_EXP + xi;
+            const float up = even ? lsb_exp_even(col[ra], col[rb], col[rc]) : lsb_exp_odd(col[rb], col[rc]);
+            L[c] = __fsub_rn(gl[c * SEL_GL + gi], up);
+        }
+        if (a.use_chroma) return __fadd_rn(__fadd_rn(__fmul_rn(L[0], L[0]), __fmul_rn(L[1], L[1])), __fmul_rn(L[2], L[2]));
+        const float Y = lsb_luma(L[0], L[1], L[2]);
+        return __fmul_rn(Y, Y);
+    };
+    float Lr[PPT][3];
+#pragma unroll
+    for (int j = 0; j < PPT; j++) {
+        const int px = tx + 32 * (j & 1), py = ty + 8 * (j >> 1);
+        Lr[j][0] = Lr[j][1] = Lr[j][2] = 0.f;
+        if (px < t.ox1 && py < t.oy1) {
+            const int x = t.x0 + px, y = t.y0 + py;
+            yb[(y - t.yL0) * lw + x - t.xL0] = lpoint(x, y, Lr[j]);
+        }
+    }
+    if (R > 0) {
+        // the window's halo ring around the tile: energy only
+        const int left = t.x0 - t.xL0, right = t.xL1 - (t.x0 + t.ox1);
+        for (int yi = ty; yi < lh; yi += 8) {
+            const int y = t.yL0 + yi;
+            float L[3];
+            if (y < t.y0 || y >= t.y0 + t.oy1) {
+                for (int xi = tx; xi < lw; xi += 32) yb[yi * lw + xi] = lpoint(t.xL0 + xi, y, L);
+            } else if (tx < left + right) {
+                const int xi = tx < left ? tx : (lw - right) + (tx - left);
+                yb[yi * lw + xi] = lpoint(t.xL0 + xi, y, L);
+            }
+        }
+    }
+    __syncthreads();
+
+    // ---- 4: the binomial window (fuse.rs:168) along rows, then columns + the selection
+    float* eh = exph;
+    if (R > 0) {
+        for (int r = ty; r < lh; r += 8)
+            for (int xo = tx; xo < t.ox1; xo += 32) {
+                const float* row = yb + r * lw - t.xL0;
+                float s = 0.f;
+#pragma unroll
+                for (int q = 0; q <= 2 * R; q++) s = __fadd_rn(s, __fmul_rn(binw<R>(q), row[RX(t.x0 + xo + q - R)]));
+                eh[r * TW + xo] = s;
+            }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int j = 0; j < PPT; j++) {
+        const int px = tx + 32 * (j & 1), py = ty + 8 * (j >> 1);
+        if (px >= t.ox1 || py >= t.oy1) continue;
+        float e;
+        if (R > 0) {
+            e = 0.f;
+#pragma unroll
+            for (int q = 0; q <= 2 * R; q++) e = __fadd_rn(e, __fmul_rn(binw<R>(q), eh[(RY(t.y0 + py + q - R) - t.yL0) * TW + px]));
+        } else {
+            e = yb[(py + t.y0 - t.yL0) * lw + px + t.x0 - t.xL0];
+        }
+        if (e > best[j]) {
+            best[j] = e;
+            acc[j][0] = Lr[j][0];
+            acc[j][1] = Lr[j][1];
+            acc[j][2] = Lr[j][2];
+            win[j] = k;
+        }
+    }
+    __syncthreads();  // the next frame restages gl / g1 / exph
+#undef RX
+#undef RY
+#undef RX1
+#undef RY1
+}
+
+template <int SRC, class GS, int R>
+__global__ void __launch_bounds__(NT, 2) select_level_kernel(const FoldArgs a) {
+    extern __shared__ float sm[];
+    const int W = a.W, H = a.H, W1 = a.W1, H1 = a.H1;
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+    for (int tile = blockIdx.x; tile < a.ntiles; tile += gridDim.x) {
+        TileWin t;
+        t.x0 = (tile % a.tiles_x) * TW;
+        t.y0 = (tile / a.tiles_x) * TH;
+        const int uxL0 = t.x0 - R, uxL1 = t.x0 + TW + R, uyL0 = t.y0 - R, uyL1 = t.y0 + TH + R;
+        const bool interior = ((uxL0 >> 1) - 1) >= 0 && uxL1 <= W && ((uxL1 - 1) >> 1) + 2 <= W1 && ((uyL0 >> 1) - 1) >= 0 &&
+                              uyL1 <= H && ((uyL1 - 1) >> 1) + 2 <= H1;
+        t.xL0 = max(0, uxL0);
+        t.xL1 = min(W, uxL1);
+        t.yL0 = max(0, uyL0);
+        t.yL1 = min(H, uyL1);
+        t.xA0 = max(0, (t.xL0 >> 1) - 1);
+        t.xA1 = min(W1, ((t.xL1 - 1) >> 1) + 2);
+        t.yA0 = max(0, (t.yL0 >> 1) - 1);
+        t.yA1 = min(H1, ((t.yL1 - 1) >> 1) + 2);
+        t.lw = t.xL1 - t.xL0;
+        t.lh = t.yL1 - t.yL0;
+        t.aw = t.xA1 - t.xA0;
+        t.ah = t.yA1 - t.yA0;
+        t.ox1 = min(TW, W - t.x0);
+        t.oy1 = min(TH, H - t.y0);
+        if (t.lw > LW_MAX || t.lh > LH_MAX || t.aw > AW_MAX || t.ah > AH_MAX) {
+            if (threadIdx.x == 0) atomicOr(a.status, LSB_ERR_SHAPE);
+            return;
+        }
+        float best[PPT], acc[PPT][3];
+        int win[PPT];
+#pragma unroll
+        for (int j = 0; j < PPT; j++) {
+            best[j] = -1.f;  // any energy (>= 0) beats it: frame 0 fills the accumulator (fuse.rs:409-412)
+            acc[j][0] = acc[j][1] = acc[j][2] = 0.f;
+            win[j] = 0;
+        }
+        for (int k = 0; k < a.nframes; k++) {
+            if (interior) select_frame<SRC, GS, R, true>(a, sm, k, t, best, acc, win);
+            else select_frame<SRC, GS, R, false>(a, sm, k, t, best, acc, win);
+        }
+#pragma unroll
+        for (int j = 0; j < PPT; j++) {
+            const int px = tx + 32 * (j & 1), py = ty + 8 * (j >> 1);
+            if (px >= t.ox1 || py >= t.oy1) continue;
+            const size_t o = (size_t)(t.y0 + py) * W + t.x0 + px;
+            a.acc[o] = acc[j][0];
+            a.acc[(size_t)W * H + o] = acc[j][1];
+            a.acc[2 * (size_t)W * H + o] = acc[j][2];
+            a.best[o] = best[j];
+            if (a.winner) a.winner[o] = (uint16_t)win[j];
+        }
+    }
+}
+
+// --------------------------------------------------------------------- warp
+// align.rs:489 `warp_with` of every aligned frame (stack.rs:662-679: the pixel
+// as shot where the source point leaves the frame), written once: f32 planar
+// (FP32 storage) or u16 interleaved (16-bit storage, rounded to the u16 step).
+template <bool U16OUT>
+__global__ void __launch_bounds__(NT) warp_frames_kernel(const uint16_t* __restrict__ frames, const FrameXform* __restrict__ xf,
+                                                         int interp, int W, int H, void* __restrict__ out) {
+    const int k = blockIdx.z;
+    const int x = blockIdx.x * 32 + (threadIdx.x & 31), y = blockIdx.y * 8 + (threadIdx.x >> 5);
+    if (x >= W || y >= H) return;
+    const size_t np = (size_t)W * H;
+    const FrameXform X = xf[k];
+    float v[3];
+    load_px_core(frames + (size_t)k * np * 3, X.inv, X.warp, X.affine, interp, W, H, x, y, v);
+    const size_t o = (size_t)y * W + x;
+    if (U16OUT) {
+        uint16_t* p = (uint16_t*)out + ((size_t)k * np + o) * 3;
+        for (int c = 0; c < 3; c++) p[c] = (uint16_t)fminf(fmaxf(__fadd_rn(__fmul_rn(v[c], 65535.f), 0.5f), 0.f), 65535.f);
+    } else {
+        float* p = (float*)out + (size_t)k * 3 * np + o;
+        p[0] = v[0];
+        p[np] = v[1];
+        p[2 * np] = v[2];
+    }
+}

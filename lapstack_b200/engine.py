@@ -51,10 +51,11 @@ class AlignParams:  # align.rs:52-70
     model: str = "similarity"
     coarsen: int = 0
     interp: str = "spline4x4"
+    host_search: bool = False  # True: the host drives Nelder-Mead, one launch per simplex step
 
     def c(self, enabled=True):
         return AlignParamsC(int(enabled), int(self.shift), int(self.scale), int(self.rotation), MODELS.index(self.model),
-                            self.coarsen, INTERPS.index(self.interp), 0)
+                            self.coarsen, INTERPS.index(self.interp), int(self.host_search))
 
     def free(self):
         a, p = self.model != "similarity", self.model == "projective"

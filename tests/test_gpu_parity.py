@@ -217,6 +217,26 @@ def test_aligned_stack_matches_oracle():
     assert frac <= 1e-3
 
 
+@pytest.mark.parametrize("model", ["similarity", "affine"])
+def test_device_search_matches_host_search(model):
+    """The one-launch search on the device and the host-driven one take the
+    same Nelder-Mead branches: same transforms (to the f64 summation order of
+    the cost) and the same evaluation count."""
+    fr, _ = L.synth_stack(L.SynthSpec(320, 240, 4, warp=True, mag_step=0.01, seed=23))
+    outs = []
+    for host in (False, True):
+        st = L.default_engine().stack(320, 240, 4, L.FuseParams(), L.AlignParams(model=model, host_search=host), None)
+        for f in fr:
+            st.push_u16(f)
+        outs.append(st.finish())
+    assert np.max(np.abs(outs[0].align - outs[1].align)) < 1e-9, (outs[0].align, outs[1].align)
+    assert outs[0].align_evals == outs[1].align_evals
+    assert_same(outs[0].image_u16, outs[1].image_u16, "fused u16")
+    ap = O.AlignParams(model=model)
+    ref = O.run_stack(fr, O.StackParams(align=ap, depth=None))
+    assert np.max(np.abs(outs[0].align - ref.sims)) < 1e-9
+
+
 # ---------------------------------------------------------------- precision
 def _errors(img, ref):
     e = np.abs(img.astype(np.float64) - ref.astype(np.float64)) * 65535
