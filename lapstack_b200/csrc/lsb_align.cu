@@ -512,13 +512,17 @@ cudaError_t cost_single(AlignCtx& C, const float* rf, int aw, int ah, const floa
 }
 
 // ------------------------------------------- the search on the device
-// align.rs:896 `multiscale_align` for one frame in ONE cooperative launch:
-// every block evaluates the current candidates over the level (the cost of
-// align.rs:581, f64 partials per block), block 0 sums the partials in a fixed
-// order and its thread 0 advances the bounded Nelder-Mead of align.rs:796
-// (the reflection, expansion and contraction of an iteration evaluated
-// together, a shrink's n points together), and grid-wide barriers separate
-// the two. No host round trip per iteration.
+// align.rs:896 `multiscale_align` for one frame in ONE cooperative launch.
+// Every block keeps its own copy of the Nelder-Mead state (align.rs:796).
+// Per batch it evaluates the pending candidates over its share of the
+// level's pixels (the cost of align.rs:581: f64 sums of d, d^2 and the
+// count), publishes its partial sums, meets the other blocks at a grid
+// barrier, sums every block's partials in one fixed order and advances its
+// copy of the search. Every copy sees the same sums and takes the same
+// branches, so one barrier per batch suffices; the partials alternate
+// between two buffers, so a batch's writes never meet a slower block's reads
+// of the batch before. The barrier's wait is bounded: on a timeout the
+// kernel records an error and every block returns.
 struct NmLevel {
     const float* rf;
     const float* tg;
@@ -530,10 +534,10 @@ struct NmJob {
     int W, H;  // full resolution
     double init[8];
     int free_idx[8], nfree;
-    double* part;  // [MAX_CAND][gridDim.x][3]
-    double* cand;  // [MAX_CAND][9] candidate inverses (written by block 0)
-    int* ctl;      // [0] candidates pending, [1] evaluations (the reference's count)
-    double* out;   // the transform found [8]
+    double* part;   // [2][MAX_CAND][gridDim.x][3]
+    unsigned* bar;  // [0] arrivals, [1] generation; zero at launch
+    int* ctl;       // [0] error: 1 barrier timeout, 2 batch limit; [1] evaluations (the reference's count)
+    double* out;    // the transform found [8]
 };
 
 __device__ void dev_sim_matrix(const double* v, int w, int h, double m[9]) {
@@ -580,19 +584,17 @@ __device__ void dev_mat_inverse(const double m[9], double inv[9]) {
     for (int i = 0; i < 9; i++) inv[i] = __ddiv_rn(inv[i], k);
 }
 
-// The NM state block 0's thread 0 keeps between grid barriers.
+// A block's copy of the search: the simplex, its costs, the box and steps of
+// the level, and the points of the batch in flight.
 struct NmState {
     double cur[8], snap[8], simplex[9][8], fv[9], lo[8], hi[8], step[8], tol[8], xr[8], xe[8], xc[8];
-    int it, phase, level, evals;
+    double pts[MAX_CAND][8];  // the pending candidates (free coordinates)
+    int it, phase, evals;
 };
 enum { NM_INIT = 0, NM_RXC = 1, NM_SHRINK = 2 };
 
-__device__ void nm_put_cand(const NmJob& J, const NmState& S, int k, const double* x, int tw, int th) {
-    double v[8], m[9];
-    for (int q = 0; q < 8; q++) v[q] = S.snap[q];
-    for (int q = 0; q < J.nfree; q++) v[J.free_idx[q]] = x[q];
-    dev_sim_matrix(v, tw, th, m);
-    dev_mat_inverse(m, J.cand + 9 * k);
+__device__ __forceinline__ void nm_put(NmState& S, int n, int k, const double* x) {
+    for (int q = 0; q < n; q++) S.pts[k][q] = x[q];
 }
 __device__ void nm_clamp(const NmState& S, int n, double* v) {
     for (int q = 0; q < n; q++) v[q] = fmin(fmax(v[q], S.lo[q]), S.hi[q]);
@@ -600,11 +602,11 @@ __device__ void nm_clamp(const NmState& S, int n, double* v) {
 // Start level L: the first simplex (align.rs:806-813). Returns the candidates pending.
 __device__ int nm_level_start(const NmJob& J, NmState& S, int L) {
     const int n = J.nfree;
-    const NmLevel& lv = J.lv[L];
     for (int q = 0; q < 8; q++) S.snap[q] = S.cur[q];
+    // align.rs:784 `level_steps`
     const double wf = J.W, hf = J.H, r = fmax(wf, hf) / 2.0;
     const double gain[8] = {wf, hf, r, r, hf / 2.0, hf / 2.0, wf / 4.0, hf / 4.0};
-    const double px = (double)(1ull << lv.lvl);
+    const double px = (double)(1ull << J.lv[L].lvl);
     for (int q = 0; q < n; q++) {
         S.step[q] = __ddiv_rn(__dmul_rn(1.0, px), gain[J.free_idx[q]]);
         S.tol[q] = __ddiv_rn(__dmul_rn(0.1, px), gain[J.free_idx[q]]);
@@ -615,19 +617,18 @@ __device__ int nm_level_start(const NmJob& J, NmState& S, int L) {
         S.simplex[k + 1][k] = __dadd_rn(S.simplex[k + 1][k], S.step[k]);
         nm_clamp(S, n, S.simplex[k + 1]);
     }
-    for (int k = 0; k <= n; k++) nm_put_cand(J, S, k, S.simplex[k], lv.w, lv.h);
+    for (int k = 0; k <= n; k++) nm_put(S, n, k, S.simplex[k]);
     S.phase = NM_INIT;
     S.it = 0;
     return n + 1;
 }
 // The top of align.rs:815's loop: returns the candidates pending, 0 when the level is done.
-__device__ int nm_iterate(const NmJob& J, NmState& S, int L) {
+__device__ int nm_iterate(const NmJob& J, NmState& S) {
     const int n = J.nfree;
-    const NmLevel& lv = J.lv[L];
     bool done = S.it >= 200;
     if (!done) {
         S.it++;
-        // stable sort by fv (align.rs:817)
+        // stable sort by cost (align.rs:817)
         for (int i = 1; i <= n; i++) {
             double f = S.fv[i], v[8];
             for (int q = 0; q < n; q++) v[q] = S.simplex[i][q];
@@ -668,25 +669,24 @@ __device__ int nm_iterate(const NmJob& J, NmState& S, int L) {
     nm_clamp(S, n, S.xe);
     for (int q = 0; q < n; q++) S.xc[q] = __dadd_rn(c[q], __dmul_rn(0.5, __dsub_rn(S.simplex[n][q], c[q])));
     nm_clamp(S, n, S.xc);
-    nm_put_cand(J, S, 0, S.xr, lv.w, lv.h);
-    nm_put_cand(J, S, 1, S.xe, lv.w, lv.h);
-    nm_put_cand(J, S, 2, S.xc, lv.w, lv.h);
+    nm_put(S, n, 0, S.xr);
+    nm_put(S, n, 1, S.xe);
+    nm_put(S, n, 2, S.xc);
     S.phase = NM_RXC;
     return 3;
 }
 // Take the costs of the pending candidates; returns the candidates pending next.
-__device__ int nm_advance(const NmJob& J, NmState& S, int L, const double* cost) {
+__device__ int nm_advance(const NmJob& J, NmState& S, const double* cost) {
     const int n = J.nfree;
-    const NmLevel& lv = J.lv[L];
     if (S.phase == NM_INIT) {
         for (int i = 0; i <= n; i++) S.fv[i] = cost[i];
         S.evals += n + 1;
-        return nm_iterate(J, S, L);
+        return nm_iterate(J, S);
     }
     if (S.phase == NM_SHRINK) {
         for (int i = 1; i <= n; i++) S.fv[i] = cost[i - 1];
         S.evals += n;
-        return nm_iterate(J, S, L);
+        return nm_iterate(J, S);
     }
     const double fr = cost[0], fe = cost[1], fc = cost[2];
     S.evals += 1;
@@ -712,22 +712,65 @@ __device__ int nm_advance(const NmJob& J, NmState& S, int L, const double* cost)
                 for (int q = 0; q < n; q++)
                     S.simplex[i][q] = __dadd_rn(S.simplex[0][q], __dmul_rn(0.5, __dsub_rn(S.simplex[i][q], S.simplex[0][q])));
                 nm_clamp(S, n, S.simplex[i]);
-                nm_put_cand(J, S, i - 1, S.simplex[i], lv.w, lv.h);
+                nm_put(S, n, i - 1, S.simplex[i]);
             }
             S.phase = NM_SHRINK;
             return n;
         }
     }
-    return nm_iterate(J, S, L);
+    return nm_iterate(J, S);
 }
 
-__global__ void __launch_bounds__(256) nm_search_kernel(const NmJob J) {
-    cg::grid_group grid = cg::this_grid();
+// A grid barrier with a bounded wait (at least ~1 s of polling before it
+// gives up). Returns false when the wait ran out here or in another block.
+constexpr long long NM_SPIN_LIMIT = 1ll << 21;
+__device__ bool nm_barrier(unsigned* bar, int* err) {
+    __shared__ int ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        volatile unsigned* gen = bar + 1;
+        volatile int* verr = err;
+        int good = *verr == 0;
+        if (good) {
+            const unsigned g = *gen;
+            __threadfence();
+            if (atomicAdd(bar, 1u) == gridDim.x - 1) {
+                atomicExch(bar, 0u);
+                __threadfence();
+                atomicAdd(bar + 1, 1u);
+            } else {
+                long long t = 0;
+                while (*gen == g) {
+                    if (*verr != 0 || ++t > NM_SPIN_LIMIT) {
+                        good = 0;
+                        break;
+                    }
+                    __nanosleep(256);
+                }
+                if (!good) atomicCAS(err, 0, 1);
+            }
+            __threadfence();
+        }
+        ok = good;
+    }
+    __syncthreads();
+    return ok != 0;
+}
+
+__device__ __forceinline__ double warp_sum(double v) {
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    return v;
+}
+
+constexpr int NM_THREADS = 256, NM_WARPS = NM_THREADS / 32;
+__global__ void __launch_bounds__(NM_THREADS) nm_search_kernel(const NmJob J) {
     __shared__ NmState S;
-    __shared__ double red[3][256];
+    __shared__ double cand[MAX_CAND][9];
+    __shared__ double wred[MAX_CAND][3][NM_WARPS];
     __shared__ double cost[MAX_CAND];
-    const bool lead = blockIdx.x == 0 && threadIdx.x == 0;
-    if (lead) {
+    __shared__ int pending;
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    if (tid == 0) {
         for (int q = 0; q < 8; q++) S.cur[q] = J.init[q];
         for (int q = 0; q < J.nfree; q++) {
             S.lo[q] = __dsub_rn(J.init[J.free_idx[q]], c_span[J.free_idx[q]]);
@@ -735,86 +778,124 @@ __global__ void __launch_bounds__(256) nm_search_kernel(const NmJob J) {
         }
         S.evals = 0;
     }
+    int batch = 0;
+    const unsigned stride = gridDim.x * NM_THREADS;
     for (int L = 0; L < J.nlv; L++) {
-        if (L > 0) grid.sync();  // every block has read the previous level's final 0
-        if (lead) J.ctl[0] = J.nfree > 0 ? nm_level_start(J, S, L) : 0;
-        grid.sync();
         const NmLevel lv = J.lv[L];
+        __syncthreads();
+        if (tid == 0) pending = J.nfree > 0 ? nm_level_start(J, S, L) : 0;
+        __syncthreads();
         const double xmax = (double)(lv.w - 1), ymax = (double)(lv.h - 1);
         const unsigned npx = (unsigned)lv.w * lv.h;  // < 2^32 (the host checks)
+        const unsigned sdy = stride / (unsigned)lv.w, sdx = stride - sdy * (unsigned)lv.w;
+        const unsigned i0 = blockIdx.x * NM_THREADS + tid;
+        const int y0s = (int)(i0 / (unsigned)lv.w), x0s = (int)(i0 - (unsigned)y0s * lv.w);
         int passes = 0;
-        while (true) {
-            const int nc = *(volatile int*)J.ctl;
-            if (nc == 0) break;
+        while (pending > 0) {
+            const int nc = pending;
+            if (tid < nc) {
+                double v[8], m[9];
+                for (int q = 0; q < 8; q++) v[q] = S.snap[q];
+                for (int q = 0; q < J.nfree; q++) v[J.free_idx[q]] = S.pts[tid][q];
+                dev_sim_matrix(v, lv.w, lv.h, m);
+                dev_mat_inverse(m, cand[tid]);
+            }
+            __syncthreads();
             for (int k = 0; k < nc; k++) {
                 double m[9];
-                for (int q = 0; q < 9; q++) m[q] = J.cand[9 * k + q];
+                for (int q = 0; q < 9; q++) m[q] = cand[k][q];
                 const bool aff = m[6] == 0.0 && m[7] == 0.0 && m[8] == 1.0;
                 double sd = 0.0, sd2 = 0.0, cnt = 0.0;
-                for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < npx; i += gridDim.x * blockDim.x) {
-                    const int y = (int)(i / (unsigned)lv.w), x = (int)(i - (unsigned)y * lv.w);
+                int x = x0s, y = y0s;
+                for (unsigned i = i0; i < npx; i += stride) {
                     double sx, sy;
                     src_point(m, aff, (double)x, (double)y, sx, sy);
-                    if (!(sx >= 0.0 && sx <= xmax && sy >= 0.0 && sy <= ymax)) continue;
-                    const double fx = floor(sx), fy = floor(sy);
-                    const int x0 = (int)fx, y0 = (int)fy;
-                    float wx[4], wy[4];
-                    spline4f((float)__dsub_rn(sx, fx), wx);
-                    spline4f((float)__dsub_rn(sy, fy), wy);
-                    float acc = 0.f;
-                    for (int j = 0; j < 4; j++) {
-                        const float* row = lv.tg + (size_t)min(max(y0 + j - 1, 0), lv.h - 1) * lv.w;
-                        float r = 0.f;
-                        for (int u = 0; u < 4; u++) r = __fadd_rn(r, __fmul_rn(wx[u], row[min(max(x0 + u - 1, 0), lv.w - 1)]));
-                        acc = __fadd_rn(acc, __fmul_rn(wy[j], r));
+                    if (sx >= 0.0 && sx <= xmax && sy >= 0.0 && sy <= ymax) {
+                        const double fx = floor(sx), fy = floor(sy);
+                        const int xa = (int)fx, ya = (int)fy;
+                        float wx[4], wy[4];
+                        spline4f((float)__dsub_rn(sx, fx), wx);
+                        spline4f((float)__dsub_rn(sy, fy), wy);
+                        float acc = 0.f;
+                        for (int j = 0; j < 4; j++) {
+                            const float* row = lv.tg + (size_t)min(max(ya + j - 1, 0), lv.h - 1) * lv.w;
+                            float r = 0.f;
+                            for (int u = 0; u < 4; u++) r = __fadd_rn(r, __fmul_rn(wx[u], row[min(max(xa + u - 1, 0), lv.w - 1)]));
+                            acc = __fadd_rn(acc, __fmul_rn(wy[j], r));
+                        }
+                        const double d = (double)__fsub_rn(lv.rf[i], acc);
+                        sd += d;
+                        sd2 += d * d;
+                        cnt += 1.0;
                     }
-                    const double d = (double)__fsub_rn(lv.rf[i], acc);
-                    sd += d;
-                    sd2 += d * d;
-                    cnt += 1.0;
-                }
-                red[0][threadIdx.x] = sd;
-                red[1][threadIdx.x] = sd2;
-                red[2][threadIdx.x] = cnt;
-                __syncthreads();
-                for (int st = blockDim.x / 2; st > 0; st >>= 1) {
-                    if (threadIdx.x < st)
-                        for (int q = 0; q < 3; q++) red[q][threadIdx.x] += red[q][threadIdx.x + st];
-                    __syncthreads();
-                }
-                if (threadIdx.x == 0)
-                    for (int q = 0; q < 3; q++) J.part[((size_t)k * gridDim.x + blockIdx.x) * 3 + q] = red[q][0];
-                __syncthreads();
-            }
-            grid.sync();
-            if (blockIdx.x == 0) {
-                for (int k = 0; k < nc; k++) {
-                    double s[3] = {0.0, 0.0, 0.0};
-                    for (int b = threadIdx.x; b < (int)gridDim.x; b += blockDim.x)
-                        for (int q = 0; q < 3; q++) s[q] += J.part[((size_t)k * gridDim.x + b) * 3 + q];
-                    for (int q = 0; q < 3; q++) red[q][threadIdx.x] = s[q];
-                    __syncthreads();
-                    for (int st = blockDim.x / 2; st > 0; st >>= 1) {
-                        if (threadIdx.x < st)
-                            for (int q = 0; q < 3; q++) red[q][threadIdx.x] += red[q][threadIdx.x + st];
-                        __syncthreads();
+                    x += (int)sdx;
+                    y += (int)sdy;
+                    if (x >= lv.w) {
+                        x -= lv.w;
+                        y++;
                     }
-                    if (threadIdx.x == 0) {
-                        const double sdv = red[0][0], sd2v = red[1][0], cn = red[2][0];
-                        cost[k] = cn < 16.0 ? 1e9 : sqrt(fmax(__ddiv_rn(__dsub_rn(sd2v, __ddiv_rn(__dmul_rn(sdv, sdv), cn)), cn), 0.0));
-                    }
-                    __syncthreads();
                 }
-                if (lead) {
-                    // <= 200 iterations of at most two batches each, plus the first simplex
-                    const int nx = nm_advance(J, S, L, cost);
-                    J.ctl[0] = ++passes > 402 ? 0 : nx;
+                sd = warp_sum(sd);
+                sd2 = warp_sum(sd2);
+                cnt = warp_sum(cnt);
+                if (lane == 0) {
+                    wred[k][0][wid] = sd;
+                    wred[k][1][wid] = sd2;
+                    wred[k][2][wid] = cnt;
                 }
             }
-            grid.sync();
+            __syncthreads();
+            double* P = J.part + (size_t)(batch & 1) * MAX_CAND * gridDim.x * 3;
+            if (tid < 3 * nc) {
+                const int k = tid / 3, q = tid % 3;
+                double s = 0.0;
+                for (int w8 = 0; w8 < NM_WARPS; w8++) s += wred[k][q][w8];
+                P[((size_t)k * gridDim.x + blockIdx.x) * 3 + q] = s;
+            }
+            if (!nm_barrier(J.bar, J.ctl)) return;
+            // every block: every block's partials, in block order, then a fixed tree
+            for (int k = 0; k < nc; k++) {
+                double s0 = 0.0, s1 = 0.0, s2 = 0.0;
+                for (int b = tid; b < (int)gridDim.x; b += NM_THREADS) {
+                    const double* p = P + ((size_t)k * gridDim.x + b) * 3;
+                    s0 += __ldcg(p);
+                    s1 += __ldcg(p + 1);
+                    s2 += __ldcg(p + 2);
+                }
+                s0 = warp_sum(s0);
+                s1 = warp_sum(s1);
+                s2 = warp_sum(s2);
+                if (lane == 0) {
+                    wred[k][0][wid] = s0;
+                    wred[k][1][wid] = s1;
+                    wred[k][2][wid] = s2;
+                }
+            }
+            __syncthreads();
+            if (tid < nc) {
+                double sdv = 0.0, sd2v = 0.0, cn = 0.0;
+                for (int w8 = 0; w8 < NM_WARPS; w8++) {
+                    sdv += wred[tid][0][w8];
+                    sd2v += wred[tid][1][w8];
+                    cn += wred[tid][2][w8];
+                }
+                cost[tid] = cn < 16.0 ? 1e9 : sqrt(fmax(__ddiv_rn(__dsub_rn(sd2v, __ddiv_rn(__dmul_rn(sdv, sdv), cn)), cn), 0.0));
+            }
+            __syncthreads();
+            if (tid == 0) {
+                int nx = nm_advance(J, S, cost);
+                // <= 200 iterations of at most two batches each, plus the first simplex
+                if (++passes > 402 && nx > 0) {
+                    nx = 0;
+                    if (blockIdx.x == 0) atomicCAS(J.ctl, 0, 2);
+                }
+                pending = nx;
+            }
+            batch++;
+            __syncthreads();
         }
     }
-    if (lead) {
+    if (blockIdx.x == 0 && tid == 0) {
         for (int q = 0; q < 8; q++) J.out[q] = S.cur[q];
         J.ctl[1] = S.evals;
     }
@@ -823,8 +904,8 @@ __global__ void __launch_bounds__(256) nm_search_kernel(const NmJob J) {
 static int g_nm_blocks = 0;
 
 static cudaError_t multiscale_align_dev(AlignCtx& C, const float* rf, const std::vector<float*>& pr, const float* tg,
-                                 const std::vector<float*>& pt, int w, int h, const double init[8], const bool freem[8], int coarsen,
-                                 double out[8]) {
+                                        const std::vector<float*>& pt, int w, int h, const double init[8], const bool freem[8],
+                                        int coarsen, double out[8]) {
     std::vector<std::pair<int, int>> dims;
     gauss_dims(w, h, dims);
     const int n = (int)dims.size() + 1;
@@ -840,7 +921,7 @@ static cudaError_t multiscale_align_dev(AlignCtx& C, const float* rf, const std:
         L.h = lvl == 0 ? h : dims[lvl - 1].second;
         L.lvl = lvl;
     }
-    if ((uint64_t)w * h >= (1ull << 32)) return cudaErrorInvalidValue;
+    if ((uint64_t)w * h >= (1ull << 31)) return cudaErrorInvalidValue;
     J.W = w;
     J.H = h;
     for (int q = 0; q < 8; q++) J.init[q] = init[q];
@@ -851,26 +932,30 @@ static cudaError_t multiscale_align_dev(AlignCtx& C, const float* rf, const std:
         int dev = 0, sms = 0, per = 0;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, nm_search_kernel, 256, 0);
+        cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, nm_search_kernel, NM_THREADS, 0);
         if (e != cudaSuccess) return e;
-        g_nm_blocks = std::max(1, std::min(per, 4)) * sms;
+        if (per < 1) return cudaErrorCooperativeLaunchTooLarge;
+        g_nm_blocks = std::min(std::min(per, 2) * sms, NM_MAX_BLOCKS);
     }
-    if (g_nm_blocks > NM_MAX_BLOCKS) g_nm_blocks = NM_MAX_BLOCKS;
     J.part = C.nm_part;
-    J.cand = C.nm_cand;
+    J.bar = (unsigned*)C.nm_ctl + 2;
     J.ctl = C.nm_ctl;
     J.out = C.nm_out;
+    cudaError_t e = cudaMemsetAsync(C.nm_ctl, 0, sizeof(int) * 4, C.s);
+    if (e != cudaSuccess) return e;
     void* args[] = {(void*)&J};
     lsb_launched();
-    cudaError_t e = cudaLaunchCooperativeKernel((void*)nm_search_kernel, dim3(g_nm_blocks), dim3(256), args, 0, C.s);
+    e = cudaLaunchCooperativeKernel((void*)nm_search_kernel, dim3(g_nm_blocks), dim3(NM_THREADS), args, 0, C.s);
     if (e != cudaSuccess) return e;
     cudaMemcpyAsync(C.sums_host, C.nm_out, sizeof(double) * 8, cudaMemcpyDeviceToHost, C.s);
-    int ev[2] = {0, 0};
-    cudaMemcpyAsync(ev, C.nm_ctl, sizeof ev, cudaMemcpyDeviceToHost, C.s);
+    cudaMemcpyAsync(C.sums_host + 8, C.nm_ctl, sizeof(int) * 2, cudaMemcpyDeviceToHost, C.s);
     e = cudaStreamSynchronize(C.s);
     if (e != cudaSuccess) return e;
+    int ctl[2];
+    memcpy(ctl, C.sums_host + 8, sizeof ctl);
+    if (ctl[0] != 0) return cudaErrorLaunchTimeout;  // a barrier wait or the batch limit ran out
     for (int q = 0; q < 8; q++) out[q] = C.sums_host[q];
-    C.evals += ev[1];
+    C.evals += ctl[1];
     C.launches++;
     return cudaSuccess;
 }

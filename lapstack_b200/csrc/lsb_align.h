@@ -9,7 +9,7 @@
 namespace lsb {
 
 constexpr int MAX_CAND = 9;
-constexpr int NM_MAX_BLOCKS = 148 * 4;
+constexpr int NM_MAX_BLOCKS = 148 * 2;
 
 // The inverse homographies of a batch of candidate transforms (row-major 3x3).
 struct CostBatch {
@@ -31,9 +31,8 @@ struct AlignCtx {
     double* sums_dev;  // device, MAX_CAND * 3
     double* sums_host; // pinned, MAX_CAND * 3
     // the search on the device (one cooperative launch per frame)
-    double* nm_part;   // device, MAX_CAND * NM_MAX_BLOCKS * 3
-    double* nm_cand;   // device, MAX_CAND * 9
-    int* nm_ctl;       // device, 2
+    double* nm_part;   // device, 2 * MAX_CAND * NM_MAX_BLOCKS * 3
+    int* nm_ctl;       // device, 4: error, evaluations, barrier arrivals and generation
     double* nm_out;    // device, 8
     int device_search = 1;  // 0: the host drives the search, one launch per simplex step
     size_t evals = 0, launches = 0;

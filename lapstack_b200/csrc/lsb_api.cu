@@ -124,7 +124,29 @@ struct lsb_stack {
     double rel64 = 0.0;
     int iters = 0, iters_first = 0;
     double ms[12] = {0};
+    WlsSolver* ws = nullptr;  // planes of the depth grid's solve, kept across runs
+    ~lsb_stack() { wls_destroy(ws); }
 };
+
+// The stack's WLS solver for a dw x dh grid and this run's guide: planes
+// allocated on the first run, edge weights recomputed every run.
+static WlsSolver* stack_solver(lsb_stack* s, int dw, int dh, const lsb_depth_params& dp, cudaStream_t st, cudaError_t* ce) {
+    *ce = cudaSuccess;
+    if (s->ws && (wls_width(s->ws) != dw || wls_height(s->ws) != dh)) {
+        wls_destroy(s->ws);
+        s->ws = nullptr;
+    }
+    if (!s->ws) {
+        s->ws = wls_alloc(dw, dh, ce);
+        if (*ce != cudaSuccess) {
+            wls_destroy(s->ws);
+            s->ws = nullptr;
+            return nullptr;
+        }
+    }
+    *ce = wls_prepare(s->ws, s->guide, dp.lambda, dp.sigma_c, (int)dp.edge_mode, st);
+    return s->ws;
+}
 
 extern "C" {
 
@@ -159,9 +181,8 @@ char* lsb_engine_create(const lsb_config* cfg, lsb_engine** out) {
     TRY(e->pool.get(&e->actx.part, MAX_CAND * 296 * 3));
     TRY(e->pool.get(&e->actx.sums_dev, MAX_CAND * 3));
     TRY(cudaHostAlloc((void**)&e->actx.sums_host, sizeof(double) * MAX_CAND * 3, cudaHostAllocDefault));
-    TRY(e->pool.get(&e->actx.nm_part, (size_t)MAX_CAND * NM_MAX_BLOCKS * 3));
-    TRY(e->pool.get(&e->actx.nm_cand, MAX_CAND * 9));
-    TRY(e->pool.get(&e->actx.nm_ctl, 2));
+    TRY(e->pool.get(&e->actx.nm_part, (size_t)2 * MAX_CAND * NM_MAX_BLOCKS * 3));
+    TRY(e->pool.get(&e->actx.nm_ctl, 4));
     TRY(e->pool.get(&e->actx.nm_out, 8));
     {
         int coop = 0;
@@ -660,11 +681,8 @@ static char* run_pipeline(lsb_stack* s) {
         const float* dsol = s->dmed;
         if (s->dp.lambda > 0.f) {
             cudaError_t ce;
-            WlsSolver* ws = wls_create(s->guide, dw, dh, s->dp.lambda, s->dp.sigma_c, (int)s->dp.edge_mode, st, &ce);
-            if (ce != cudaSuccess) {
-                wls_destroy(ws);
-                return dup_err(fmt("wls: %s", cudaGetErrorString(ce)));
-            }
+            WlsSolver* ws = stack_solver(s, dw, dh, s->dp, st, &ce);
+            if (ce != cudaSuccess) return dup_err(fmt("wls: %s", cudaGetErrorString(ce)));
             cudaError_t r1 = wls_set_weights(ws, s->conf, st);
             float rel = 0.f;
             int it = 0;
@@ -675,7 +693,6 @@ static char* run_pipeline(lsb_stack* s) {
                 if (r1 == cudaSuccess) r1 = wls_set_weights(ws, s->w2, st);
                 if (r1 == cudaSuccess) r1 = wls_solve(ws, s->dmed, (int)s->dp.cg_iters, s->u, &rel, &it, st, (int)s->dp.vcycle_mode, false, &s->rel64);
             }
-            wls_destroy(ws);
             if (r1 != cudaSuccess) return dup_err(fmt("wls: %s", cudaGetErrorString(r1)));
             s->rel = rel;
             s->iters = it;
@@ -949,7 +966,7 @@ extern "C" char* lsb_depth_from_slices(lsb_engine* e, const float* slices, uint3
     double rel64 = 0.0;
     if (dp.lambda > 0.f) {
         cudaError_t ce;
-        WlsSolver* ws = wls_create(s->guide, dw, dh, dp.lambda, dp.sigma_c, (int)dp.edge_mode, st, &ce);
+        WlsSolver* ws = stack_solver(s, dw, dh, dp, st, &ce);
         if (ce == cudaSuccess) ce = wls_set_weights(ws, s->conf, st);
         if (ce == cudaSuccess) ce = wls_solve(ws, s->dmed, (int)dp.cg_iters, s->u, &rel, &it, st, (int)dp.vcycle_mode, false, &rel64);
         it1 = it;
@@ -958,7 +975,6 @@ extern "C" char* lsb_depth_from_slices(lsb_engine* e, const float* slices, uint3
             if (ce == cudaSuccess) ce = wls_set_weights(ws, s->w2, st);
             if (ce == cudaSuccess) ce = wls_solve(ws, s->dmed, (int)dp.cg_iters, s->u, &rel, &it, st, (int)dp.vcycle_mode, false, &rel64);
         }
-        wls_destroy(ws);
         if (ce != cudaSuccess) return fail(dup_err(fmt("wls: %s", cudaGetErrorString(ce))));
         dsol = s->u;
     }

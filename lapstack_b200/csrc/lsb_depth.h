@@ -42,6 +42,12 @@ struct WlsLevel {
 struct WlsSolver;
 WlsSolver* wls_create(const float* guide, int w, int h, float lambda, float sigma_c, int edge_mode, cudaStream_t s,
                       cudaError_t* err);
+// The planes of a w x h solver (allocated once, reused by every solve of that size) ...
+WlsSolver* wls_alloc(int w, int h, cudaError_t* err);
+// ... and the edge weights of one guide (depth.rs:653), down the hierarchy.
+cudaError_t wls_prepare(WlsSolver* s, const float* guide, float lambda, float sigma_c, int edge_mode, cudaStream_t st);
+int wls_width(const WlsSolver* s);
+int wls_height(const WlsSolver* s);
 void wls_destroy(WlsSolver* s);
 // wd = max(conf, 0) + 1e-4, aggregated down the hierarchy, diagonals taken
 cudaError_t wls_set_weights(WlsSolver* s, const float* conf, cudaStream_t st);

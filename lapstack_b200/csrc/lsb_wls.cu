@@ -25,7 +25,7 @@ struct WlsSolver {
     float lambda;
     float *ex, *ey;
     std::vector<WlsLevel> lv;
-    float *cp, *dp, *f, *r, *z, *p, *ap, *ones;
+    float *cp, *dp, *f, *r, *z, *p, *ap;
     double *part, *scal;  // scal: [rz, pap, rr, bnorm2, rz_new]
     float* alpha_beta;    // [alpha, beta]
     float* host_rel;      // pinned: [rel, stop]
@@ -142,36 +142,109 @@ __global__ void wd_kernel(const float* __restrict__ conf, float* __restrict__ wd
 }
 
 // depth.rs:677 `solve_rows` / :707 `solve_cols`: the Thomas algorithm along
-// every line, one thread per line (stride 1: rows; stride w: columns).
-__global__ void thomas_kernel(float* __restrict__ u, const float* __restrict__ f, const float* __restrict__ wd, int unit_wd,
-                              const float* __restrict__ a, int nlines, int len, size_t line_step, size_t stride, float lam,
-                              float* __restrict__ cp, float* __restrict__ dp) {
-    const int li = blockIdx.x * blockDim.x + threadIdx.x;
-    if (li >= nlines) return;
-    const size_t base = (size_t)li * line_step;
+// every line, one thread per line, 32 lines per warp. The warp stages 32x32
+// tiles of the coefficients through shared memory with coalesced row-segment
+// loads (ROWS: a line is an image row, the tile is [line][element]; else a
+// line is a column, the tile is [element][line]); each thread then walks its
+// line's 32 elements of the tile in the reference's order and arithmetic.
+constexpr int TT = 32;
+template <bool ROWS>
+__device__ __forceinline__ float& tl(float (*t)[TT + 1], int line, int e) {
+    return ROWS ? t[line][e] : t[e][line];
+}
+template <bool ROWS>
+__global__ void __launch_bounds__(32) thomas_kernel(float* __restrict__ u, const float* __restrict__ f, const float* __restrict__ wd,
+                                                    int unit_wd, const float* __restrict__ a, int w, int h, float lam,
+                                                    float* __restrict__ cp, float* __restrict__ dp) {
+    __shared__ float ta[TT][TT + 1], tw[TT][TT + 1], tf[TT][TT + 1], tc[TT][TT + 1], td[TT][TT + 1];
+    const int lane = threadIdx.x;
+    const int nlines = ROWS ? h : w, len = ROWS ? w : h;
+    const int l0 = blockIdx.x * TT;
+    const int li = l0 + lane;
+    // global index of (line l0 + ln, element e)
+    auto gi = [&](int ln, int e) -> size_t { return ROWS ? (size_t)(l0 + ln) * w + e : (size_t)e * w + (l0 + ln); };
+    // the warp moves tile row q (q = line for ROWS, element otherwise): lane walks the contiguous axis
     float prev_a = 0.f, cprev = 0.f, dprev = 0.f;
     const float nl = -lam;
-    for (int i = 0; i < len; i++) {
-        const size_t k = base + (size_t)i * stride;
-        const float ai = i + 1 < len ? a[k] : 0.f;
-        const float wdi = unit_wd ? 1.f : wd[k];
-        const float diag = __fadd_rn(wdi, __fmul_rn(lam, __fadd_rn(prev_a, ai)));
-        const float lower = __fmul_rn(nl, prev_a), upper = __fmul_rn(nl, ai);
-        float m = __fsub_rn(diag, __fmul_rn(lower, i > 0 ? cprev : 0.f));
-        if (fabsf(m) < 1e-12f) m = 1e-12f;
-        cprev = __fdiv_rn(upper, m);
-        dprev = __fdiv_rn(__fsub_rn(__fmul_rn(wdi, f[k]), __fmul_rn(lower, i > 0 ? dprev : 0.f)), m);
-        cp[k] = cprev;
-        dp[k] = dprev;
-        prev_a = ai;
+    for (int e0 = 0; e0 < len; e0 += TT) {
+        const int ne = min(TT, len - e0);
+        for (int q = 0; q < TT; q++) {
+            int ln, e;
+            if (ROWS) ln = q, e = e0 + lane;
+            else ln = lane, e = e0 + q;
+            const bool ok = l0 + ln < nlines && e < e0 + ne;
+            const size_t k = ok ? gi(ln, e) : 0;
+            tl<ROWS>(ta, ln, e - e0) = ok && e + 1 < len ? a[k] : 0.f;
+            tl<ROWS>(tf, ln, e - e0) = ok ? f[k] : 0.f;
+            tl<ROWS>(tw, ln, e - e0) = ok && !unit_wd ? wd[k] : 1.f;
+        }
+        __syncwarp();
+        if (li < nlines)
+            for (int j = 0; j < ne; j++) {
+                const int i = e0 + j;
+                const float ai = tl<ROWS>(ta, lane, j);
+                const float wdi = tl<ROWS>(tw, lane, j);
+                const float diag = __fadd_rn(wdi, __fmul_rn(lam, __fadd_rn(prev_a, ai)));
+                const float lower = __fmul_rn(nl, prev_a), upper = __fmul_rn(nl, ai);
+                float m = __fsub_rn(diag, __fmul_rn(lower, i > 0 ? cprev : 0.f));
+                if (fabsf(m) < 1e-12f) m = 1e-12f;
+                cprev = __fdiv_rn(upper, m);
+                dprev = __fdiv_rn(__fsub_rn(__fmul_rn(wdi, tl<ROWS>(tf, lane, j)), __fmul_rn(lower, i > 0 ? dprev : 0.f)), m);
+                tl<ROWS>(tc, lane, j) = cprev;
+                tl<ROWS>(td, lane, j) = dprev;
+                prev_a = ai;
+            }
+        __syncwarp();
+        for (int q = 0; q < TT; q++) {
+            int ln, e;
+            if (ROWS) ln = q, e = e0 + lane;
+            else ln = lane, e = e0 + q;
+            if (l0 + ln < nlines && e < e0 + ne) {
+                const size_t k = gi(ln, e);
+                cp[k] = tl<ROWS>(tc, ln, e - e0);
+                dp[k] = tl<ROWS>(td, ln, e - e0);
+            }
+        }
+        __syncwarp();
     }
-    float nxt = dp[base + (size_t)(len - 1) * stride];
-    u[base + (size_t)(len - 1) * stride] = nxt;
-    for (int i = len - 2; i >= 0; i--) {
-        const size_t k = base + (size_t)i * stride;
-        nxt = __fsub_rn(dp[k], __fmul_rn(cp[k], nxt));
-        u[k] = nxt;
+    // back substitution, tiles from the end; the last chunk's cp/dp are still in shared memory
+    float nxt = 0.f;
+    const int last0 = ((len - 1) / TT) * TT;
+    for (int e0 = last0; e0 >= 0; e0 -= TT) {
+        const int ne = min(TT, len - e0);
+        if (e0 != last0) {
+            for (int q = 0; q < TT; q++) {
+                int ln, e;
+                if (ROWS) ln = q, e = e0 + lane;
+                else ln = lane, e = e0 + q;
+                const bool ok = l0 + ln < nlines;
+                const size_t k = ok ? gi(ln, e) : 0;
+                tl<ROWS>(tc, ln, e - e0) = ok ? cp[k] : 0.f;
+                tl<ROWS>(td, ln, e - e0) = ok ? dp[k] : 0.f;
+            }
+            __syncwarp();
+        }
+        if (li < nlines)
+            for (int j = ne - 1; j >= 0; j--) {
+                const int i = e0 + j;
+                nxt = i == len - 1 ? tl<ROWS>(td, lane, j) : __fsub_rn(tl<ROWS>(td, lane, j), __fmul_rn(tl<ROWS>(tc, lane, j), nxt));
+                tl<ROWS>(tf, lane, j) = nxt;
+            }
+        __syncwarp();
+        for (int q = 0; q < TT; q++) {
+            int ln, e;
+            if (ROWS) ln = q, e = e0 + lane;
+            else ln = lane, e = e0 + q;
+            if (l0 + ln < nlines && e < e0 + ne) u[gi(ln, e)] = tl<ROWS>(tf, ln, e - e0);
+        }
+        __syncwarp();
     }
+}
+static void thomas(bool rows, float* u, const float* f, const float* wd, int unit_wd, const float* a, int w, int h, float lam,
+                   float* cp, float* dp, cudaStream_t s) {
+    const int nlines = rows ? h : w;
+    if (rows) lsb_launched(), thomas_kernel<true><<<(nlines + TT - 1) / TT, TT, 0, s>>>(u, f, wd, unit_wd, a, w, h, lam, cp, dp);
+    else lsb_launched(), thomas_kernel<false><<<(nlines + TT - 1) / TT, TT, 0, s>>>(u, f, wd, unit_wd, a, w, h, lam, cp, dp);
 }
 
 // f64 dot products: per-block partials, then the partials in order.
@@ -231,13 +304,11 @@ __global__ void fill_kernel(float* o, float v, size_t n) {
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) o[i] = v;
 }
 
-WlsSolver* wls_create(const float* guide, int w, int h, float lambda, float sigma_c, int edge_mode, cudaStream_t s,
-                      cudaError_t* err) {
+WlsSolver* wls_alloc(int w, int h, cudaError_t* err) {
     *err = cudaSuccess;
     WlsSolver* S = new WlsSolver();
     S->w = w;
     S->h = h;
-    S->lambda = lambda;
     size_t n = (size_t)w * h;
     S->ex = S->alloc(n, err);
     S->ey = S->alloc(n, err);
@@ -266,12 +337,16 @@ WlsSolver* wls_create(const float* guide, int w, int h, float lambda, float sigm
     S->z = S->alloc(n, err);
     S->p = S->alloc(n, err);
     S->ap = S->alloc(n, err);
-    S->ones = S->alloc(n, err);
     S->part = (double*)S->alloc(2 * DOT_BLOCKS, err);
     S->scal = (double*)S->alloc(16, err);
     S->alpha_beta = S->alloc(4, err);
     if (cudaHostAlloc((void**)&S->host_rel, 64, cudaHostAllocDefault) != cudaSuccess) *err = cudaErrorMemoryAllocation;
-    if (*err != cudaSuccess) return S;
+    return S;
+}
+
+cudaError_t wls_prepare(WlsSolver* S, const float* guide, float lambda, float sigma_c, int edge_mode, cudaStream_t s) {
+    const int w = S->w, h = S->h;
+    S->lambda = lambda;
     const float inv = -1.0f / std::max(sigma_c, 1e-6f);
     const float inv2s2 = 1.0f / (2.0f * sigma_c * sigma_c);
     lsb_launched(), edge_kernel<<<g2(w, h), B2, 0, s>>>(guide, w, h, inv, inv2s2, edge_mode, lambda, S->ex, S->ey, S->lv[0].ax, S->lv[0].ay);
@@ -279,10 +354,19 @@ WlsSolver* wls_create(const float* guide, int w, int h, float lambda, float sigm
         const WlsLevel &F = S->lv[l - 1], &C = S->lv[l];
         lsb_launched(), coarsen_edges_kernel<<<g2(C.w, C.h), B2, 0, s>>>(F.ax, F.ay, F.w, F.h, C.ax, C.ay, C.w, C.h);
     }
-    lsb_launched(), fill_kernel<<<g1(n), 256, 0, s>>>(S->ones, 1.f, n);
-    *err = cudaGetLastError();
+    return cudaGetLastError();
+}
+
+WlsSolver* wls_create(const float* guide, int w, int h, float lambda, float sigma_c, int edge_mode, cudaStream_t s,
+                      cudaError_t* err) {
+    WlsSolver* S = wls_alloc(w, h, err);
+    if (*err != cudaSuccess) return S;
+    *err = wls_prepare(S, guide, lambda, sigma_c, edge_mode, s);
     return S;
 }
+
+int wls_width(const WlsSolver* s) { return s->w; }
+int wls_height(const WlsSolver* s) { return s->h; }
 
 void wls_destroy(WlsSolver* s) {
     if (!s) return;
@@ -344,8 +428,8 @@ cudaError_t wls_solve(WlsSolver* S, const float* d, int max_iters, float* u, flo
     const size_t n = (size_t)w * h;
     WlsLevel& L0 = S->lv[0];
     if (w == 1 || h == 1) {
-        if (h == 1) lsb_launched(), thomas_kernel<<<1, 32, 0, s>>>(u, d, L0.wd, 0, S->ex, 1, w, 0, 1, S->lambda, S->cp, S->dp);
-        else lsb_launched(), thomas_kernel<<<1, 32, 0, s>>>(u, d, L0.wd, 0, S->ey, 1, h, 0, (size_t)w, S->lambda, S->cp, S->dp);
+        if (h == 1) thomas(true, u, d, L0.wd, 0, S->ex, w, h, S->lambda, S->cp, S->dp, s);
+        else thomas(false, u, d, L0.wd, 0, S->ey, w, h, S->lambda, S->cp, S->dp, s);
         *rel_out = 0.f;
         *iters_out = 0;
         if (rel64) *rel64 = 0.0;
@@ -358,9 +442,9 @@ cudaError_t wls_solve(WlsSolver* S, const float* d, int max_iters, float* u, flo
             float p4 = 1.f;
             for (int q = 0; q < 3 - t; q++) p4 *= 4.f;
             const float lam_t = (1.5f * S->lambda * p4) / (64.f - 1.f);
-            lsb_launched(), thomas_kernel<<<(h + 127) / 128, 128, 0, s>>>(u, S->f, L0.wd, t == 1 ? 0 : 1, S->ex, h, w, (size_t)w, 1, lam_t, S->cp, S->dp);
+            thomas(true, u, S->f, L0.wd, t == 1 ? 0 : 1, S->ex, w, h, lam_t, S->cp, S->dp, s);
             cudaMemcpyAsync(S->f, u, n * sizeof(float), cudaMemcpyDeviceToDevice, s);
-            lsb_launched(), thomas_kernel<<<(w + 127) / 128, 128, 0, s>>>(u, S->f, L0.wd, 1, S->ey, w, h, 1, (size_t)w, lam_t, S->cp, S->dp);
+            thomas(false, u, S->f, L0.wd, 1, S->ey, w, h, lam_t, S->cp, S->dp, s);
             cudaMemcpyAsync(S->f, u, n * sizeof(float), cudaMemcpyDeviceToDevice, s);
         }
     }
