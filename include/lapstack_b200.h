@@ -117,7 +117,7 @@ typedef struct {
     uint32_t wls_iters, wls_iters_first, align_evals;
     double wls_rel64;
     double ms[12];       /* device ms per stage: align, gains, fold, residual+collapse, focus agg, wls, upsample,
-                            total, fold level 0; 3 spare */
+                            total, fold level 0, its select kernel, its REDUCE kernel; 1 spare */
 } lsb_result;
 
 /* Seeded synthetic stack description (no reference counterpart; the benchmark inputs). */

@@ -72,7 +72,7 @@ struct lsb_engine {
     unsigned *hist, *sel;
     float* scal;  // [floor, p90, max, ...]
     AlignCtx actx;
-    cudaEvent_t ev[10];
+    cudaEvent_t ev[12];
     void log(const std::string& line) {
         if (cfg.log) cfg.log(line.c_str(), cfg.user);
     }
@@ -634,6 +634,7 @@ static char* run_pipeline(lsb_stack* s) {
         a.gscale = gscale;
         a.ginv = ginv;
         const int src = l > 0 ? SRC_G : ((s->f32src || (warped && s->storage == STORE_F32)) ? SRC_F32 : SRC_U16);
+        a.between = l == 0 ? ev[10] : nullptr;
         if (l == 0) TRY(cudaEventRecord(ev[8], st));
         TRY(fold_level(a, src, s->storage, (int)s->fp.energy_radius, focus, st, e->grid));
         if (l == 0) TRY(cudaEventRecord(ev[9], st));
@@ -732,6 +733,8 @@ static char* run_pipeline(lsb_stack* s) {
     s->ms[6] = ms_between(ev[6], ev[7]);
     s->ms[7] = ms_between(ev[0], ev[7]);
     s->ms[8] = ms_between(ev[8], ev[9]);
+    s->ms[9] = ms_between(ev[10], ev[9]);   // select, level 0
+    s->ms[10] = ms_between(ev[8], ev[10]);  // REDUCE (+ focus slices), level 0
     return nullptr;
 }
 

@@ -55,6 +55,7 @@ static cudaError_t launch_level(const FoldArgs& a, cudaStream_t s, int grid_limi
     if (e != cudaSuccess) return e;
     const int rtiles = ((a.W1 + RW - 1) / RW) * ((a.H1 + RH - 1) / RH);
     lsb_launched(), kr<<<dim3(rtiles, a.nframes), NT, rsm, s>>>(a);
+    if (a.between) cudaEventRecord(a.between, s);
     lsb_launched(), ks<<<std::min(a.ntiles, std::max(grid_limit, 1)), NT, ssm, s>>>(a);
     return cudaGetLastError();
 }

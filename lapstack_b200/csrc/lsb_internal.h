@@ -48,6 +48,7 @@ struct FoldArgs {
     int ntaps;
     int* status;  // device error word
     float gscale, ginv;  // the 16-bit fixed-point storage's scale and its inverse
+    cudaEvent_t between;  // host side: recorded between the REDUCE and the select launch (may be null)
 };
 
 // Storage of the Gaussian levels >= 1 and the focus slices.

@@ -122,7 +122,8 @@ class Output:  # stack.rs:244 Output (the hot-path part)
     ms: dict = field(default_factory=dict)
 
 
-STAGES = ["align", "gains", "fold", "collapse", "aggregate", "wls", "upsample", "total", "fold_level0"]
+STAGES = ["align", "gains", "fold", "collapse", "aggregate", "wls", "upsample", "total", "fold_level0", "select_level0",
+          "reduce_level0"]
 
 # Live handles, released stacks-first at interpreter exit while the CUDA
 # runtime is still up (a finaliser run during shutdown does nothing).
