@@ -117,7 +117,8 @@ typedef struct {
     uint32_t wls_iters, wls_iters_first, align_evals;
     double wls_rel64;
     double ms[12];       /* device ms per stage: align, gains, fold, residual+collapse, focus agg, wls, upsample,
-                            total, fold level 0, its select kernel, its REDUCE kernel; 1 spare */
+                            total, fold level 0, its select kernel, its REDUCE kernel, the WLS solves
+                            (warm start included) */
 } lsb_result;
 
 /* Seeded synthetic stack description (no reference counterpart; the benchmark inputs). */
@@ -196,6 +197,38 @@ const char* lsb_warp_cost_noalloc(const float* rf_dev, uint32_t aw, uint32_t ah,
    per frame scale, rotation (rad), tx, ty (px) applied. */
 const char* lsb_synth_stack_host(const lsb_synth_desc* d, uint16_t* out, double* truth);
 const char* lsb_synth_stack_device(const lsb_synth_desc* d, uint16_t* out_dev, double* truth, void* stream);
+
+/* The learned warm start of the WLS solve (no counterpart in the reference):
+ * a 4-level U-Net, 32 base channels, BF16 weights and activations with FP32
+ * accumulation, mapping the quarter-resolution (guide luma, raw depth / dmax,
+ * confidence) to the WLS solution / dmax. Weights: [tap][cout][cin] per layer,
+ * 15 layers; the input layer reads 3 live channels of 32, the output layer
+ * writes channel 0 of 32. Trained by its own forward/backward/Adam kernels. */
+typedef struct lsb_unet lsb_unet;
+char* lsb_unet_create(int32_t device, uint64_t seed, lsb_unet** out);
+void lsb_unet_destroy(lsb_unet* u);
+void lsb_unet_sizes(const lsb_unet* u, uint64_t* n_weights, uint64_t* n_biases);
+/* host copies of the FP32 master weights/biases and of the last step's gradients (any may be NULL) */
+char* lsb_unet_get_params(lsb_unet* u, float* w, float* b, float* gw, float* gb);
+char* lsb_unet_set_params(lsb_unet* u, const float* w, const float* b);
+/* network grid of a dw x dh depth grid: ceil(d/2) rounded up to a multiple of 8 */
+void lsb_unet_grid(uint32_t dw, uint32_t dh, uint32_t* H, uint32_t* W);
+/* device planes (dw x dh) -> batch entry b of in_dev [B][H][W][32] bf16 and d_in_dev [B][H][W] f32 (= d / dmax) */
+char* lsb_unet_prepare(const float* guide, const float* d, const float* conf, uint32_t dw, uint32_t dh, float dmax, void* in_dev,
+                       float* d_in_dev, uint32_t b, void* stream);
+/* out0_dev [B][H][W]: the network's correction; the prediction is d_in + out0 */
+char* lsb_unet_forward(lsb_unet* u, const void* in_dev, const float* d_in_dev, uint32_t B, uint32_t H, uint32_t W, float* out0_dev);
+/* forward, MSE of d_in + out0 against target_dev [B][H][W], backward, and Adam when lr > 0 */
+char* lsb_unet_train_step(lsb_unet* u, const void* in_dev, const float* d_in_dev, const float* target_dev, uint32_t B, uint32_t H,
+                          uint32_t W, float lr, double* loss_out);
+/* Use the network's prediction as the x0 of this stack's WLS solves (NULL: the
+ * reference's FGS start). The stack does not own the network. */
+char* lsb_stack_set_warm_start(lsb_stack* s, lsb_unet* u);
+/* Device planes of the last run's depth grid (dw x dh, valid until the next
+ * run): the guide luma, the median-filtered raw depth, the normalised
+ * confidence and the WLS solution -- the network's inputs and target. */
+char* lsb_stack_depth_planes(lsb_stack* s, const float** guide, const float** d, const float** conf, const float** u,
+                             uint32_t* dw, uint32_t* dh);
 
 #ifdef __cplusplus
 }

@@ -93,6 +93,18 @@ SIGNATURES = {
     "lsb_warp_cost_noalloc": (C.c_char_p, [P, C.c_uint32, C.c_uint32, P, C.c_uint32, C.c_uint32, P, C.c_uint32, P, P]),
     "lsb_synth_stack_host": (C.c_char_p, [C.POINTER(SynthDesc), P, P]),
     "lsb_synth_stack_device": (C.c_char_p, [C.POINTER(SynthDesc), P, P, P]),
+    "lsb_unet_create": (ERR, [C.c_int32, C.c_uint64, C.POINTER(P)]),
+    "lsb_unet_destroy": (None, [P]),
+    "lsb_unet_sizes": (None, [P, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
+    "lsb_unet_get_params": (ERR, [P, P, P, P, P]),
+    "lsb_unet_set_params": (ERR, [P, P, P]),
+    "lsb_unet_grid": (None, [C.c_uint32, C.c_uint32, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]),
+    "lsb_unet_prepare": (ERR, [P, P, P, C.c_uint32, C.c_uint32, C.c_float, P, P, C.c_uint32, P]),
+    "lsb_unet_forward": (ERR, [P, P, P, C.c_uint32, C.c_uint32, C.c_uint32, P]),
+    "lsb_unet_train_step": (ERR, [P, P, P, P, C.c_uint32, C.c_uint32, C.c_uint32, C.c_float, C.POINTER(C.c_double)]),
+    "lsb_stack_set_warm_start": (ERR, [P, P]),
+    "lsb_stack_depth_planes": (ERR, [P, C.POINTER(P), C.POINTER(P), C.POINTER(P), C.POINTER(P), C.POINTER(C.c_uint32),
+                                     C.POINTER(C.c_uint32)]),
 }
 
 _lib = None

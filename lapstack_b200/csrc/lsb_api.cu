@@ -125,8 +125,38 @@ struct lsb_stack {
     int iters = 0, iters_first = 0;
     double ms[12] = {0};
     WlsSolver* ws = nullptr;  // planes of the depth grid's solve, kept across runs
-    ~lsb_stack() { wls_destroy(ws); }
+    lsb_unet* net = nullptr;  // learned warm start of the solves (not owned)
+    float* x0 = nullptr;      // its prediction on the depth grid
+    size_t x0_cells = 0;
+    ~lsb_stack() {
+        wls_destroy(ws);
+        if (x0) cudaFree(x0);
+    }
 };
+
+namespace lsb {
+cudaError_t unet_warm_start(lsb_unet* u, const float* guide, const float* d, const float* conf, int dw, int dh, float dmax, float* x0,
+                            cudaStream_t st);
+}
+
+// The x0 of this run's solves: the network's prediction (learned warm start)
+// or none (the reference's FGS start).
+static cudaError_t warm_start(lsb_stack* s, int dw, int dh, int n, cudaStream_t st, bool* given) {
+    *given = false;
+    if (!s->net) return cudaSuccess;
+    const size_t m = (size_t)dw * dh;
+    if (s->x0_cells < m) {
+        if (s->x0) cudaFree(s->x0);
+        s->x0 = nullptr;
+        s->x0_cells = 0;
+        cudaError_t e = cudaMalloc(&s->x0, m * sizeof(float));
+        if (e != cudaSuccess) return e;
+        s->x0_cells = m;
+    }
+    cudaError_t e = lsb::unet_warm_start(s->net, s->guide, s->dmed, s->conf, dw, dh, (float)std::max(n - 1, 1), s->x0, st);
+    if (e == cudaSuccess) *given = true;
+    return e;
+}
 
 // The stack's WLS solver for a dw x dh grid and this run's guide: planes
 // allocated on the first run, edge weights recomputed every run.
@@ -680,19 +710,27 @@ static char* run_pipeline(lsb_stack* s) {
         s->rel = 0.f;
         s->rel64 = 0.0;
         const float* dsol = s->dmed;
+        TRY(cudaEventRecord(ev[11], st));
         if (s->dp.lambda > 0.f) {
             cudaError_t ce;
             WlsSolver* ws = stack_solver(s, dw, dh, s->dp, st, &ce);
             if (ce != cudaSuccess) return dup_err(fmt("wls: %s", cudaGetErrorString(ce)));
-            cudaError_t r1 = wls_set_weights(ws, s->conf, st);
+            bool given = false;
+            cudaError_t r1 = warm_start(s, dw, dh, n, st, &given);
+            auto start = [&]() {
+                return given ? cudaMemcpyAsync(s->u, s->x0, sizeof(float) * m, cudaMemcpyDeviceToDevice, st) : cudaSuccess;
+            };
+            if (r1 == cudaSuccess) r1 = wls_set_weights(ws, s->conf, st);
             float rel = 0.f;
             int it = 0;
-            if (r1 == cudaSuccess) r1 = wls_solve(ws, s->dmed, (int)s->dp.cg_iters, s->u, &rel, &it, st, (int)s->dp.vcycle_mode, false, &s->rel64);
+            if (r1 == cudaSuccess) r1 = start();
+            if (r1 == cudaSuccess) r1 = wls_solve(ws, s->dmed, (int)s->dp.cg_iters, s->u, &rel, &it, st, (int)s->dp.vcycle_mode, given, &s->rel64);
             s->iters_first = it;
             if (r1 == cudaSuccess && s->dp.robust > 0.f) {
                 r1 = robust_weights(s->conf, s->dmed, s->u, s->dp.robust, s->w2, m, st);
                 if (r1 == cudaSuccess) r1 = wls_set_weights(ws, s->w2, st);
-                if (r1 == cudaSuccess) r1 = wls_solve(ws, s->dmed, (int)s->dp.cg_iters, s->u, &rel, &it, st, (int)s->dp.vcycle_mode, false, &s->rel64);
+                if (r1 == cudaSuccess) r1 = start();
+                if (r1 == cudaSuccess) r1 = wls_solve(ws, s->dmed, (int)s->dp.cg_iters, s->u, &rel, &it, st, (int)s->dp.vcycle_mode, given, &s->rel64);
             }
             if (r1 != cudaSuccess) return dup_err(fmt("wls: %s", cudaGetErrorString(r1)));
             s->rel = rel;
@@ -711,6 +749,7 @@ static char* run_pipeline(lsb_stack* s) {
         }
     } else {
         TRY(cudaEventRecord(ev[5], st));
+        TRY(cudaEventRecord(ev[11], st));
         TRY(cudaEventRecord(ev[6], st));
     }
     TRY(cudaEventRecord(ev[7], st));
@@ -735,6 +774,7 @@ static char* run_pipeline(lsb_stack* s) {
     s->ms[8] = ms_between(ev[8], ev[9]);
     s->ms[9] = ms_between(ev[10], ev[9]);   // select, level 0
     s->ms[10] = ms_between(ev[8], ev[10]);  // REDUCE (+ focus slices), level 0
+    s->ms[11] = ms_between(ev[11], ev[6]);  // the WLS solves (warm start included)
     return nullptr;
 }
 
@@ -1091,5 +1131,23 @@ extern "C" char* lsb_warp_cost(lsb_engine* e, const float* rf, uint32_t aw, uint
     TRY(cudaMemcpyAsync(a, rf, sizeof(float) * aw * ah, cudaMemcpyHostToDevice, st));
     TRY(cudaMemcpyAsync(b, tgt, sizeof(float) * tw * th, cudaMemcpyHostToDevice, st));
     TRY(cost_single(e->actx, a, (int)aw, (int)ah, b, (int)tw, (int)th, sim8, cost));
+    return nullptr;
+}
+
+extern "C" char* lsb_stack_set_warm_start(lsb_stack* s, lsb_unet* u) {
+    if (!s) return dup_err("lsb_stack_set_warm_start: null stack");
+    s->net = u;
+    return nullptr;
+}
+
+extern "C" char* lsb_stack_depth_planes(lsb_stack* s, const float** guide, const float** d, const float** conf, const float** u,
+                                        uint32_t* dw, uint32_t* dh) {
+    if (!s || !s->folded || !s->dp.enabled) return dup_err("lsb_stack_depth_planes: run the stack with the depth pass first");
+    *guide = s->guide;
+    *d = s->dmed;
+    *conf = s->conf;
+    *u = s->dp.lambda > 0.f ? s->u : s->dmed;
+    *dw = (uint32_t)s->dw;
+    *dh = (uint32_t)s->dh;
     return nullptr;
 }

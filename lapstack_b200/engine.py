@@ -123,7 +123,7 @@ class Output:  # stack.rs:244 Output (the hot-path part)
 
 
 STAGES = ["align", "gains", "fold", "collapse", "aggregate", "wls", "upsample", "total", "fold_level0", "select_level0",
-          "reduce_level0"]
+          "reduce_level0", "wls_solve"]
 
 # Live handles, released stacks-first at interpreter exit while the CUDA
 # runtime is still up (a finaliser run during shutdown does nothing).
@@ -252,6 +252,18 @@ class Stack:
         check(self._L.lsb_stack_push_f32(self._h, arr))
 
     push = push_f32
+
+    def set_warm_start(self, net):
+        """Start this stack's WLS solves from the U-Net's prediction (None: the reference's FGS start)."""
+        check(self._L.lsb_stack_set_warm_start(self._h, net._h if net is not None else None))
+        self._net = net  # the stack does not own the network; keep it alive
+
+    def depth_planes(self):
+        """Device pointers of the last run's depth-grid planes: guide, d, conf, u, and (dw, dh)."""
+        ps = [C.c_void_p() for _ in range(4)]
+        dw, dh = C.c_uint32(), C.c_uint32()
+        check(self._L.lsb_stack_depth_planes(self._h, *[C.byref(p) for p in ps], C.byref(dw), C.byref(dh)))
+        return [p.value for p in ps], (dw.value, dh.value)
 
     def frames_device(self):
         p = C.c_void_p()
