@@ -38,6 +38,8 @@ cudaError_t upsample(const float* abar, const float* bbar, const float* yfull, c
 struct WlsLevel {
     int w, h;
     float *wd, *ax, *ay, *dinv, *x, *b, *r;
+    // BF16 copies the mixed-precision V-cycle (vcycle_mode 1) works on
+    uint16_t *hwd, *hax, *hay, *hdinv, *hx, *hb, *hr;
 };
 struct WlsSolver;
 WlsSolver* wls_create(const float* guide, int w, int h, float lambda, float sigma_c, int edge_mode, cudaStream_t s,

@@ -18,6 +18,8 @@ namespace lsb {
 
 constexpr float MG_OMEGA = 0.8f;
 constexpr int MG_COARSE = 32, MG_MIN = 16;
+// the BF16 V-cycle: levels, and Jacobi sweeps before and after the coarse correction
+constexpr int MG_H_LEVELS = 6, MG_H_SWEEPS = 2;
 constexpr int DOT_BLOCKS = 592;
 
 struct WlsSolver {
@@ -247,6 +249,55 @@ static void thomas(bool rows, float* u, const float* f, const float* wd, int uni
     else lsb_launched(), thomas_kernel<false><<<(nlines + TT - 1) / TT, TT, 0, s>>>(u, f, wd, unit_wd, a, w, h, lam, cp, dp);
 }
 
+// ------------------------------------------------ the BF16 V-cycle (mode 1)
+// The preconditioner's smoother, residual, restriction and prolongation on
+// BF16 copies of the level operators and vectors, arithmetic in FP32; the
+// outer CG stays FP32 with FP64 dot products.
+typedef __nv_bfloat16 bf;
+__device__ __forceinline__ float ldh(const uint16_t* p, size_t k) { return __bfloat162float(((const bf*)p)[k]); }
+__device__ __forceinline__ void sth(uint16_t* p, size_t k, float v) { ((bf*)p)[k] = __float2bfloat16_rn(v); }
+
+__global__ void to_bf16_kernel(const float* __restrict__ a, uint16_t* __restrict__ o, size_t n) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) sth(o, i, a[i]);
+}
+__global__ void from_bf16_kernel(const uint16_t* __restrict__ a, float* __restrict__ o, size_t n) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) o[i] = ldh(a, i);
+}
+// mode 1: out = b - A x; mode 2: out = x + w D^-1 (b - A x)
+__global__ void stencil_h_kernel(const uint16_t* __restrict__ x, const uint16_t* __restrict__ b, const uint16_t* __restrict__ wd,
+                                 const uint16_t* __restrict__ ax, const uint16_t* __restrict__ ay, const uint16_t* __restrict__ dinv,
+                                 uint16_t* __restrict__ out, int w, int h, int mode) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
+    if (i >= w || y >= h) return;
+    const size_t k = (size_t)y * w + i;
+    const float xk = ldh(x, k);
+    float v = ldh(wd, k) * xk;
+    if (i > 0) v += ldh(ax, k - 1) * (xk - ldh(x, k - 1));
+    if (i + 1 < w) v += ldh(ax, k) * (xk - ldh(x, k + 1));
+    if (y > 0) v += ldh(ay, k - w) * (xk - ldh(x, k - w));
+    if (y + 1 < h) v += ldh(ay, k) * (xk - ldh(x, k + w));
+    const float r = ldh(b, k) - v;
+    sth(out, k, mode == 1 ? r : xk + MG_OMEGA * ldh(dinv, k) * r);
+}
+__global__ void jac0_h_kernel(const uint16_t* __restrict__ b, const uint16_t* __restrict__ dinv, uint16_t* __restrict__ x, size_t n) {
+    for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x)
+        sth(x, k, MG_OMEGA * ldh(dinv, k) * ldh(b, k));
+}
+__global__ void block_sum_h_kernel(const uint16_t* __restrict__ src, int w, int h, uint16_t* __restrict__ dst, int cw, int ch) {
+    const int xx = blockIdx.x * blockDim.x + threadIdx.x, yy = blockIdx.y * blockDim.y + threadIdx.y;
+    if (xx >= cw || yy >= ch) return;
+    float o = 0.f;
+    for (int y = 2 * yy; y < min(2 * yy + 2, h); y++)
+        for (int x = 2 * xx; x < min(2 * xx + 2, w); x++) o += ldh(src, (size_t)y * w + x);
+    sth(dst, (size_t)yy * cw + xx, o);
+}
+__global__ void prolong_h_kernel(uint16_t* __restrict__ x, int w, int h, const uint16_t* __restrict__ xc, int cw) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
+    if (i >= w || y >= h) return;
+    const size_t k = (size_t)y * w + i;
+    sth(x, k, ldh(x, k) + ldh(xc, (size_t)(y / 2) * cw + i / 2));
+}
+
 // f64 dot products: per-block partials, then the partials in order.
 __global__ void dot_partial_kernel(const float* __restrict__ a, const float* __restrict__ b, size_t n, double* part) {
     double s = 0.0;
@@ -325,6 +376,8 @@ WlsSolver* wls_alloc(int w, int h, cudaError_t* err) {
         L.x = S->alloc(m, err);
         L.b = S->alloc(m, err);
         L.r = S->alloc(m, err);
+        uint16_t** hs[7] = {&L.hwd, &L.hax, &L.hay, &L.hdinv, &L.hx, &L.hb, &L.hr};
+        for (uint16_t** h : hs) *h = (uint16_t*)S->alloc((m + 1) / 2, err);
         S->lv.push_back(L);
         if (std::max(cw, ch) <= MG_MIN) break;
         cw = (cw + 1) / 2;
@@ -387,6 +440,14 @@ cudaError_t wls_set_weights(WlsSolver* S, const float* conf, cudaStream_t s) {
         }
         lsb_launched(), dinv_kernel<<<g2(C.w, C.h), B2, 0, s>>>(C.wd, C.ax, C.ay, C.w, C.h, C.dinv);
     }
+    // the BF16 V-cycle's operators (levels 0 .. MG_H_LEVELS-1)
+    for (size_t l = 0; l < S->lv.size() && l < (size_t)MG_H_LEVELS; l++) {
+        const WlsLevel& C = S->lv[l];
+        const size_t m = (size_t)C.w * C.h;
+        const float* src[4] = {C.wd, C.ax, C.ay, C.dinv};
+        uint16_t* dst[4] = {C.hwd, C.hax, C.hay, C.hdinv};
+        for (int q = 0; q < 4; q++) lsb_launched(), to_bf16_kernel<<<g1(m), 256, 0, s>>>(src[q], dst[q], m);
+    }
     return cudaGetLastError();
 }
 
@@ -415,6 +476,32 @@ static void vcycle(WlsSolver* S, size_t l, cudaStream_t s) {
     jacobi(T, false, s);
 }
 
+static void jacobi_h(WlsLevel& L, bool zero, cudaStream_t s) {
+    if (zero) {
+        lsb_launched(), jac0_h_kernel<<<g1((size_t)L.w * L.h), 256, 0, s>>>(L.hb, L.hdinv, L.hx, (size_t)L.w * L.h);
+        return;
+    }
+    lsb_launched(), stencil_h_kernel<<<g2(L.w, L.h), B2, 0, s>>>(L.hx, L.hb, L.hwd, L.hax, L.hay, L.hdinv, L.hr, L.w, L.h, 2);
+    std::swap(L.hx, L.hr);
+}
+// the mixed-precision V-cycle: MG_H_SWEEPS pre/post sweeps, MG_H_LEVELS levels,
+// MG_COARSE sweeps on the coarsest
+static void vcycle_h(WlsSolver* S, size_t l, cudaStream_t s) {
+    WlsLevel& T = S->lv[l];
+    const size_t last = std::min(S->lv.size(), (size_t)MG_H_LEVELS) - 1;
+    if (l == last) {
+        for (int k = 0; k < MG_COARSE; k++) jacobi_h(T, k == 0, s);
+        return;
+    }
+    for (int k = 0; k < MG_H_SWEEPS; k++) jacobi_h(T, k == 0, s);
+    lsb_launched(), stencil_h_kernel<<<g2(T.w, T.h), B2, 0, s>>>(T.hx, T.hb, T.hwd, T.hax, T.hay, T.hdinv, T.hr, T.w, T.h, 1);
+    WlsLevel& C = S->lv[l + 1];
+    lsb_launched(), block_sum_h_kernel<<<g2(C.w, C.h), B2, 0, s>>>(T.hr, T.w, T.h, C.hb, C.w, C.h);
+    vcycle_h(S, l + 1, s);
+    lsb_launched(), prolong_h_kernel<<<g2(T.w, T.h), B2, 0, s>>>(T.hx, T.w, T.h, C.hx, C.w);
+    for (int k = 0; k < MG_H_SWEEPS; k++) jacobi_h(T, false, s);
+}
+
 static void dot(WlsSolver* S, const float* a, const float* b, size_t n, int mode, cudaStream_t s) {
     int nb = (int)std::min<size_t>(DOT_BLOCKS, (n + 255) / 256);
     lsb_launched(), dot_partial_kernel<<<nb, 256, 0, s>>>(a, b, n, S->part);
@@ -423,7 +510,6 @@ static void dot(WlsSolver* S, const float* a, const float* b, size_t n, int mode
 
 cudaError_t wls_solve(WlsSolver* S, const float* d, int max_iters, float* u, float* rel_out, int* iters_out, cudaStream_t s,
                       int mode, bool x0_given, double* rel64) {
-    (void)mode;
     const int w = S->w, h = S->h;
     const size_t n = (size_t)w * h;
     WlsLevel& L0 = S->lv[0];
@@ -453,6 +539,12 @@ cudaError_t wls_solve(WlsSolver* S, const float* d, int max_iters, float* u, flo
     dot(S, S->f, S->f, n, 4, s);
     lsb_launched(), stencil_kernel<<<g2(w, h), B2, 0, s>>>(u, S->f, L0.wd, L0.ax, L0.ay, L0.dinv, S->r, w, h, 1);
     auto precond = [&]() {
+        if (mode == 1) {
+            lsb_launched(), to_bf16_kernel<<<g1(n), 256, 0, s>>>(S->r, L0.hb, n);
+            vcycle_h(S, 0, s);
+            lsb_launched(), from_bf16_kernel<<<g1(n), 256, 0, s>>>(S->lv[0].hx, S->z, n);
+            return;
+        }
         cudaMemcpyAsync(L0.b, S->r, n * sizeof(float), cudaMemcpyDeviceToDevice, s);
         vcycle(S, 0, s);
         cudaMemcpyAsync(S->z, S->lv[0].x, n * sizeof(float), cudaMemcpyDeviceToDevice, s);

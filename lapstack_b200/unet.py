@@ -165,3 +165,26 @@ def train(net: UNet, inp, d_in, tgt, steps=300, batch=8, crop=128, lr=1e-3, seed
         if log and (it % 50 == 0 or it == steps - 1):
             log(f"step {it} loss {losses[-1]:.3e} ({time.perf_counter() - t0:.1f} s)")
     return losses
+
+
+def compare_warm_start(net: UNet, w, h, n, seeds, engine: Engine | None = None, depth: DepthParams | None = None, repeats=2):
+    """Plain (the reference's FGS start) against learned (the network's x0)
+    WLS solves on seeded stacks: per seed, per mode, the iterations of both
+    solves, the solve time (device ms, warm start included), the final
+    relative residual and the depth map."""
+    eng = engine or default_engine()
+    dp = depth or DepthParams()
+    out = []
+    for seed in seeds:
+        st = eng.stack(w, h, n, FuseParams(), None, dp)
+        synth_stack_device(SynthSpec(w, h, n, seed=seed, mag_step=0.002, noise_std=0.003), st.frames_device(), eng.stream)
+        st.set_count(n)
+        row = {}
+        for mode in ("plain", "learned") * repeats:
+            st.set_warm_start(net if mode == "learned" else None)
+            o = st.finish()
+            row[mode] = dict(iters_first=o.depth.wls_iters_first, iters=o.depth.wls_iters, ms=o.ms["wls_solve"],
+                             rel=o.depth.wls_rel64, depth=o.depth.depth)
+        st.close()
+        out.append(row)
+    return out

@@ -87,8 +87,8 @@ def _declare(L):
         ("orc_peak_track_f", None, [P, sz, sz, C.c_float, P, P, P, P]),
         ("orc_normalize_conf_f", C.c_float, [P, sz]),
         ("orc_median3_f", None, [P, sz, sz, P]),
-        ("orc_wls_solve_f", None, [P, P, P, sz, sz, C.c_float, C.c_float, sz, P, P, P]),
-        ("orc_wls_solve_d", None, [P, P, P, sz, sz, C.c_double, C.c_double, sz, P, P, P]),
+        ("orc_wls_solve_f", None, [P, P, P, sz, sz, C.c_float, C.c_float, sz, P, P, P, C.c_int]),
+        ("orc_wls_solve_d", None, [P, P, P, sz, sz, C.c_double, C.c_double, sz, P, P, P, C.c_int]),
         ("orc_wls_levels_f", sz, [P, sz, sz]),
         ("orc_depth_from_slices_f", None, [P, sz, sz, P, sz, sz, P, P, P, P, P]),
         ("orc_depth_from_slices_d", None, [P, sz, sz, P, sz, sz, P, P, P, P, P]),
@@ -521,7 +521,7 @@ def median3(src):
     return out
 
 
-def wls_solve(d, conf, guide, lam, sigma_c, max_iters, fp64=False):
+def wls_solve(d, conf, guide, lam, sigma_c, max_iters, fp64=False, edge_mode=0):
     dt, s = (F64, "d") if fp64 else (F32, "f")
     d, conf, guide = (np.ascontiguousarray(x, dtype=dt) for x in (d, conf, guide))
     h, w = d.shape
@@ -529,7 +529,7 @@ def wls_solve(d, conf, guide, lam, sigma_c, max_iters, fp64=False):
     rel = (C.c_double if fp64 else C.c_float)(0)
     it = C.c_size_t(0)
     getattr(lib(), f"orc_wls_solve_{s}")(_ptr(d), _ptr(conf), _ptr(guide), w, h, lam, sigma_c, max_iters, _ptr(u),
-                                         C.byref(rel), C.byref(it))
+                                         C.byref(rel), C.byref(it), int(edge_mode))
     return u, rel.value, it.value
 
 

@@ -299,8 +299,8 @@ void orc_median3_f(const float* src, size_t w, size_t h, float* out) {
 }
 #define WLS_API(S, T)                                                                                                   \
     void orc_wls_solve_##S(const T* d, const T* conf, const T* guide, size_t w, size_t h, T lambda, T sigma_c, size_t iters, \
-                           T* u, T* rel, size_t* it) {                                                                  \
-        WlsSolver<T> s(guide, w, h, lambda, sigma_c);                                                                   \
+                           T* u, T* rel, size_t* it, int edge_mode) {                                                   \
+        WlsSolver<T> s(guide, w, h, lambda, sigma_c, edge_mode);                                                        \
         s.set_weights(conf);                                                                                            \
         std::fill(u, u + w * h, T(0));                                                                                  \
         auto r = s.solve(d, iters, u);                                                                                  \

@@ -394,16 +394,23 @@ std::vector<T> median3(const T* src, size_t w, size_t h) {
     return out;
 }
 
-// depth.rs:653 `edge_weights`: exp(-|dI| / sigma) to the right and below.
+// depth.rs:653 `edge_weights`: exp(-|dI| / sigma) to the right and below
+// (edge_mode 0). edge_mode 1 is not in the reference: the Gaussian of the
+// guide gradient, exp(-dI^2 / (2 sigma^2)), the large-grid solve's weights.
 template <class T>
-void edge_weights(const T* g, size_t w, size_t h, T sigma, std::vector<T>& ax, std::vector<T>& ay) {
+void edge_weights(const T* g, size_t w, size_t h, T sigma, std::vector<T>& ax, std::vector<T>& ay, int edge_mode = 0) {
     T inv = T(-1) / rmax(sigma, LIT(1e-6));
+    T inv2s2 = T(1) / (T(2) * sigma * sigma);
+    auto wgt = [&](T a, T b) {
+        T d = std::fabs(a - b);
+        return edge_mode == 0 ? std::exp(d * inv) : std::exp(-(d * d * inv2s2));
+    };
     ax.assign(w * h, T(0));
     ay.assign(w * h, T(0));
     for (size_t y = 0; y < h; y++)
-        for (size_t x = 0; x + 1 < w; x++) ax[y * w + x] = std::exp(std::fabs(g[y * w + x] - g[y * w + x + 1]) * inv);
+        for (size_t x = 0; x + 1 < w; x++) ax[y * w + x] = wgt(g[y * w + x], g[y * w + x + 1]);
     for (size_t y = 0; y + 1 < h; y++)
-        for (size_t x = 0; x < w; x++) ay[y * w + x] = std::exp(std::fabs(g[y * w + x] - g[(y + 1) * w + x]) * inv);
+        for (size_t x = 0; x < w; x++) ay[y * w + x] = wgt(g[y * w + x], g[(y + 1) * w + x]);
 }
 
 // depth.rs:677 `solve_rows` (Thomas algorithm per row) and :707 `solve_cols`,
@@ -591,8 +598,8 @@ struct WlsSolver {
     std::vector<T> ex, ey;
     std::vector<MgLevel<T>> levels;
     std::vector<T> r, z, p, ap, f;
-    WlsSolver(const T* guide, size_t w_, size_t h_, T lambda_, T sigma_c) : w(w_), h(h_), lambda(lambda_) {
-        edge_weights<T>(guide, w, h, sigma_c, ex, ey);
+    WlsSolver(const T* guide, size_t w_, size_t h_, T lambda_, T sigma_c, int edge_mode = 0) : w(w_), h(h_), lambda(lambda_) {
+        edge_weights<T>(guide, w, h, sigma_c, ex, ey, edge_mode);
         MgLevel<T> top(w, h);
         for (size_t i = 0; i < w * h; i++) {
             top.ax[i] = lambda * ex[i];

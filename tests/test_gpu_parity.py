@@ -177,6 +177,28 @@ def test_wls_matches_oracle():
     assert np.max(np.abs(du - ru)) < 1e-3 * (d.max() - d.min())
 
 
+@pytest.mark.parametrize("edge_mode,lam,sigma", [(0, 3.0, 0.04), (1, 0.5, 0.02)])
+def test_wls_bf16_vcycle_reaches_the_same_solution(edge_mode, lam, sigma):
+    """vcycle_mode 1 (BF16 smoother/restriction, 2 pre/post sweeps, 6 levels,
+    inside the FP32 CG with FP64 dots) reaches the solver's 1e-5 relative
+    residual and the FP32 V-cycle's solution, with the reference's edge
+    weights and with the Gaussian-of-gradient ones; the FP32 path also
+    matches the oracle's FP64 solve of the same system."""
+    w, h = 640, 480
+    rng = np.random.default_rng(9)
+    y, x = np.mgrid[0:h, 0:w]
+    guide = (0.5 + 0.3 * np.sin(x / 37.0) * np.cos(y / 29.0) + 0.01 * rng.random((h, w))).astype(np.float32)
+    d = (4.0 + 3.0 * np.sin(x / 53.0) * np.cos(y / 41.0) + rng.normal(0, 0.4, (h, w))).astype(np.float32)
+    conf = rng.random((h, w)).astype(np.float32)
+    u0, r0, i0, _ = L.wls_solve(d, conf, guide, lam, sigma, 200, edge_mode=edge_mode, vcycle_mode=0)
+    u1, r1, i1, _ = L.wls_solve(d, conf, guide, lam, sigma, 200, edge_mode=edge_mode, vcycle_mode=1)
+    ru, rrel, _ = O.wls_solve(d, conf, guide, lam, sigma, 200, fp64=True, edge_mode=edge_mode)
+    span = float(d.max() - d.min())
+    assert r0 < 1e-5 and r1 < 1e-5 and i1 < 200
+    assert np.max(np.abs(u1 - u0)) < 1e-3 * span
+    assert np.max(np.abs(u0 - ru)) < 1e-3 * span
+
+
 # ------------------------------------------------------------ registration
 def test_warp_cost_matches_oracle():
     w, h = 96, 72
