@@ -43,7 +43,7 @@ PUBLISHED_MPFS = 175.8
 
 CONFIGS = {
     "c3": dict(w=8256, h=5504, n=100, warp=True, mag_step=0.0, noise_std=0.002, levels=0, align=True, coarsen=3,
-               agg_radius=3, storage="unorm16", sample=2),
+               agg_radius=3, storage="unorm16", sample=2, wls_report=True),
     "c2": dict(w=6000, h=4000, n=30, warp=False, mag_step=0.001, noise_std=0.002, levels=8, align=False, coarsen=0,
                agg_radius=8, storage="f32", sample=2),
     "c1": dict(w=1024, h=768, n=8, warp=False, mag_step=0.002, noise_std=0.003, levels=6, align=False, coarsen=0,
@@ -188,6 +188,56 @@ def traffic_per_px_frame(name):
     return None
 
 
+def _device_plane(ptr, h, w):
+    """A float32 device plane as a torch tensor (no copy)."""
+    import torch
+
+    class _Cuda:
+        def __init__(self):
+            self.__cuda_array_interface__ = {"data": (ptr, False), "shape": (h, w), "typestr": "<f4", "version": 3}
+    return torch.as_tensor(_Cuda(), device="cuda")
+
+
+def wls_report(L, eng, st, c):
+    """WLS ms to rel-res 1e-5 on this stack's depth grid: the reference's FP32
+    MG-PCG against the BF16 V-cycle, with the reference's edge weights and with
+    the large-grid Gaussian ones (lambda 0.5, sigma 0.02); and this stack's
+    solves started from the trained U-Net against the reference's FGS start."""
+    import torch
+    from lapstack_b200 import unet as U
+    (g, d, cf, _), (dw, dh) = st.depth_planes()
+    torch.cuda.synchronize()
+    d_h, cf_h, g_h = (_device_plane(p, dh, dw).cpu().numpy() for p in (d, cf, g))
+    out = {"grid": [dw, dh]}
+    for name, (em, lam, sg) in {"reference_edges": (0, 3.0, 0.04), "gaussian_edges": (1, 0.5, 0.02)}.items():
+        row = {}
+        for mode, tag in ((0, "fp32_vcycle"), (1, "bf16_vcycle")):
+            L.wls_solve(d_h, cf_h, g_h, lam, sg, 200, edge_mode=em, vcycle_mode=mode, engine=eng)  # warm
+            _, rel, it, ms = L.wls_solve(d_h, cf_h, g_h, lam, sg, 200, edge_mode=em, vcycle_mode=mode, engine=eng)
+            row[tag] = {"ms": ms, "iters": it, "rel": rel}
+        out[name] = row
+    # learned warm start: trained on solver pairs of this resolution, then this stack's own solves
+    t0 = time.perf_counter()
+    inp, d_in, tgt, _ = U.solver_pairs(6, c["w"], c["h"], frames=(8, 12), engine=eng,
+                                      depth=L.DepthParams(agg_radius=c["agg_radius"]))
+    net = U.UNet(seed=0)
+    losses = U.train(net, inp, d_in, tgt, steps=300, batch=8, crop=256, lr=1e-3)
+    train_s = time.perf_counter() - t0
+    del inp, d_in, tgt
+    res = {}
+    for mode in ("plain", "learned", "plain", "learned"):
+        st.set_warm_start(net if mode == "learned" else None)
+        o = st.finish()
+        res[mode] = {"ms": o.ms["wls_solve"], "iters": [o.depth.wls_iters_first, o.depth.wls_iters], "rel": o.depth.wls_rel64}
+    st.set_warm_start(None)
+    out["learned_vs_plain"] = {"plain": res["plain"], "learned": res["learned"],
+                               "speedup": res["plain"]["ms"] / max(res["learned"]["ms"], 1e-9),
+                               "train": {"stacks": 6, "steps": 300, "seconds": train_s,
+                                         "loss_first": float(np.mean(losses[:10])), "loss_last": float(np.mean(losses[-10:]))}}
+    net.close()
+    return out
+
+
 def peaks():
     try:
         return json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))), "measured"
@@ -205,6 +255,7 @@ def main():
     ap.add_argument("--storage", default=None, choices=["f32", "unorm16", "f16"])
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-wls-report", action="store_true")
     args = ap.parse_args()
     c = dict(CONFIGS[args.config])
     if args.storage:
@@ -286,6 +337,12 @@ def main():
     m = out.depth.dw * out.depth.dh if out.depth else 0
     d2h = W * H * (6 + 12 + 4) + (W * H * 8 + m * 4 if out.depth else 0)
 
+    wls = None
+    if rank == 0 and c.get("wls_report") and not args.no_wls_report:
+        try:
+            wls = wls_report(L, eng, st, c)
+        except Exception as ex:  # reported, never the product
+            wls = {"error": str(ex)}
     if rank == 0:
         pk, pk_kind = peaks()
         gs = {"f32": 4, "unorm16": 2, "f16": 2}[c["storage"]]
@@ -315,7 +372,8 @@ def main():
                          "traffic": (tr * N * W * H if tr else None), "algorithmic_bytes": alg_bytes, "kernel_ms": sel0},
             "stages_ms": stage_ms,
             "align_evals": out.align_evals,
-            "wls": {"iters": out.depth.wls_iters if out.depth else 0, "rel": out.depth.wls_rel if out.depth else 0.0},
+            "wls": {"iters": out.depth.wls_iters if out.depth else 0, "rel": out.depth.wls_rel if out.depth else 0.0,
+                    "ms_to_rel_1e-5": wls},
             "cpu_baseline": cb,
             "clocks": clk.summary(),
         }

@@ -167,7 +167,8 @@ void lsb_result_free(lsb_result* r);
 /* gpu.rs:1327 depth_from_slices: slices [n][dh][dw] f32, fused [3][h][w] f32 (host pointers). */
 char* lsb_depth_from_slices(lsb_engine* e, const float* slices, uint32_t n, const float* fused, uint32_t w, uint32_t h,
                             const lsb_depth_params* p, lsb_result* out);
-/* depth.rs:1081 wls_solve on the device (host pointers, w*h each). */
+/* depth.rs:1081 wls_solve on the device (host pointers, w*h each). ms: device time from the edge
+   weights to the converged solution (FGS guess and MG-PCG), the solver's planes allocated first. */
 char* lsb_wls_solve(lsb_engine* e, const float* d, const float* conf, const float* guide, uint32_t w, uint32_t h, float lambda,
                     float sigma_c, uint32_t max_iters, uint32_t edge_mode, uint32_t vcycle_mode, float* u, float* rel,
                     uint32_t* iters, double* ms);

@@ -162,16 +162,15 @@ __global__ void cost_final_kernel(const double* __restrict__ part, int nblocks, 
 
 // align.rs:489 `warp_with` on an f32 plane (edge-clamped; no fallback), the
 // interpolation weights as in the fold's level-0 warp.
-__global__ void warp_plane_kernel(const float* __restrict__ src, int w, int h, const WarpXform xf, float* __restrict__ out) {
-    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
-    if (x >= w || y >= h) return;
+__device__ __forceinline__ float warp_plane_px(const float* __restrict__ src, int w, int h, const double* inv, bool affine, int interp,
+                                               int x, int y) {
     double sx, sy;
-    src_point(xf.inv, xf.affine, (double)x, (double)y, sx, sy);
+    src_point(inv, affine, (double)x, (double)y, sx, sy);
     const double fx = floor(sx), fy = floor(sy);
     const int x0 = (int)fx, y0 = (int)fy;
     float wx[6], wy[6];
-    const int n = interp_w(xf.interp, __dsub_rn(sx, fx), wx);
-    interp_w(xf.interp, __dsub_rn(sy, fy), wy);
+    const int n = interp_w(interp, __dsub_rn(sx, fx), wx);
+    interp_w(interp, __dsub_rn(sy, fy), wy);
     const int start = 1 - n / 2;
     float acc = 0.f;
     for (int j = 0; j < n; j++) {
@@ -180,7 +179,28 @@ __global__ void warp_plane_kernel(const float* __restrict__ src, int w, int h, c
         for (int i = 0; i < n; i++) r = __fadd_rn(r, __fmul_rn(wx[i], row[min(max(x0 + start + i, 0), w - 1)]));
         acc = __fadd_rn(acc, __fmul_rn(wy[j], r));
     }
-    out[(size_t)y * w + x] = acc;
+    return acc;
+}
+__global__ void warp_plane_kernel(const float* __restrict__ src, int w, int h, const WarpXform xf, float* __restrict__ out) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
+    if (x >= w || y >= h) return;
+    out[(size_t)y * w + x] = warp_plane_px(src, w, h, xf.inv, xf.affine, xf.interp, x, y);
+}
+// The same with the warp a search left in device memory: inverse [9],
+// affine flag, identity flag (an identity result copies the plane, as the
+// host path does).
+__global__ void warp_plane_dev_kernel(const float* __restrict__ src, int w, int h, const double* __restrict__ wd, int interp,
+                                      float* __restrict__ out) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
+    if (x >= w || y >= h) return;
+    const size_t k = (size_t)y * w + x;
+    if (wd[10] != 0.0) {
+        out[k] = src[k];
+        return;
+    }
+    double inv[9];
+    for (int q = 0; q < 9; q++) inv[q] = wd[q];
+    out[k] = warp_plane_px(src, w, h, inv, wd[9] != 0.0, interp, x, y);
 }
 
 // brightness.rs:67 `sums` of every aligned frame against frame 0: over the
@@ -262,6 +282,12 @@ cudaError_t gauss_levels(const float* y, int w, int h, const std::vector<float*>
 cudaError_t warp_plane(const float* src, int w, int h, const WarpXform& xf, float* out, cudaStream_t s) {
     dim3 b(32, 8), g((w + 31) / 32, (h + 7) / 8);
     lsb_launched(), warp_plane_kernel<<<g, b, 0, s>>>(src, w, h, xf, out);
+    return cudaGetLastError();
+}
+
+cudaError_t warp_plane_dev(const float* src, int w, int h, const double* warp_dev, int interp, float* out, cudaStream_t s) {
+    dim3 b(32, 8), g((w + 31) / 32, (h + 7) / 8);
+    lsb_launched(), warp_plane_dev_kernel<<<g, b, 0, s>>>(src, w, h, warp_dev, interp, out);
     return cudaGetLastError();
 }
 
@@ -536,8 +562,12 @@ struct NmJob {
     int free_idx[8], nfree;
     double* part;   // [2][MAX_CAND][gridDim.x][3]
     unsigned* bar;  // [0] arrivals, [1] generation; zero at launch
-    int* ctl;       // [0] error: 1 barrier timeout, 2 batch limit; [1] evaluations (the reference's count)
+    int* ctl;       // [0] error (sticky): 1 barrier timeout, 2 batch limit; [1] evaluations (the reference's count)
     double* out;    // the transform found [8]
+    // chained searches (no host round trip between frames):
+    const double* init_dev;        // if set, the initial transform (the previous frame's result) instead of init
+    double* warp_dev;              // if set, the full-resolution warp of the result: inverse [9], affine, identity
+    unsigned long long* evals_dev; // if set, evaluations are added here
 };
 
 __device__ void dev_sim_matrix(const double* v, int w, int h, double m[9]) {
@@ -771,10 +801,10 @@ __global__ void __launch_bounds__(NM_THREADS) nm_search_kernel(const NmJob J) {
     __shared__ int pending;
     const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
     if (tid == 0) {
-        for (int q = 0; q < 8; q++) S.cur[q] = J.init[q];
+        for (int q = 0; q < 8; q++) S.cur[q] = J.init_dev ? J.init_dev[q] : J.init[q];
         for (int q = 0; q < J.nfree; q++) {
-            S.lo[q] = __dsub_rn(J.init[J.free_idx[q]], c_span[J.free_idx[q]]);
-            S.hi[q] = __dadd_rn(J.init[J.free_idx[q]], c_span[J.free_idx[q]]);
+            S.lo[q] = __dsub_rn(S.cur[J.free_idx[q]], c_span[J.free_idx[q]]);
+            S.hi[q] = __dadd_rn(S.cur[J.free_idx[q]], c_span[J.free_idx[q]]);
         }
         S.evals = 0;
     }
@@ -898,21 +928,32 @@ __global__ void __launch_bounds__(NM_THREADS) nm_search_kernel(const NmJob J) {
     if (blockIdx.x == 0 && tid == 0) {
         for (int q = 0; q < 8; q++) J.out[q] = S.cur[q];
         J.ctl[1] = S.evals;
+        if (J.evals_dev) atomicAdd(J.evals_dev, (unsigned long long)S.evals);
+        if (J.warp_dev) {
+            // align.rs:258: the inverse of the frame's matrix, as the warp of the next reference reads it
+            const double id[8] = {0.0, 0.0, 1.0, 0.0, 1.0, 0.0, 0.0, 0.0};
+            bool ident = true;
+            for (int q = 0; q < 8; q++) ident = ident && S.cur[q] == id[q];
+            double m[9], inv[9];
+            dev_sim_matrix(S.cur, J.W, J.H, m);
+            dev_mat_inverse(m, inv);
+            for (int q = 0; q < 9; q++) J.warp_dev[q] = inv[q];
+            J.warp_dev[9] = inv[6] == 0.0 && inv[7] == 0.0 && inv[8] == 1.0 ? 1.0 : 0.0;
+            J.warp_dev[10] = ident ? 1.0 : 0.0;
+        }
     }
 }
 
 static int g_nm_blocks = 0;
 
-static cudaError_t multiscale_align_dev(AlignCtx& C, const float* rf, const std::vector<float*>& pr, const float* tg,
-                                        const std::vector<float*>& pt, int w, int h, const double init[8], const bool freem[8],
-                                        int coarsen, double out[8]) {
+// One frame's search job: the levels searched (coarsest first) and the free parameters.
+static cudaError_t nm_job(AlignCtx& C, const float* rf, const std::vector<float*>& pr, const float* tg, const std::vector<float*>& pt,
+                          int w, int h, const bool freem[8], int coarsen, NmJob& J) {
     std::vector<std::pair<int, int>> dims;
     gauss_dims(w, h, dims);
     const int n = (int)dims.size() + 1;
     const int finest = std::min(coarsen, n - 1);
-    NmJob J;
     memset(&J, 0, sizeof J);
-    J.nlv = 0;
     for (int lvl = n - 1; lvl >= finest && J.nlv < 24; lvl--) {
         NmLevel& L = J.lv[J.nlv++];
         L.rf = lvl == 0 ? rf : pr[lvl - 1];
@@ -924,8 +965,6 @@ static cudaError_t multiscale_align_dev(AlignCtx& C, const float* rf, const std:
     if ((uint64_t)w * h >= (1ull << 31)) return cudaErrorInvalidValue;
     J.W = w;
     J.H = h;
-    for (int q = 0; q < 8; q++) J.init[q] = init[q];
-    J.nfree = 0;
     for (int q = 0; q < 8; q++)
         if (freem[q]) J.free_idx[J.nfree++] = q;
     if (g_nm_blocks == 0) {
@@ -941,11 +980,25 @@ static cudaError_t multiscale_align_dev(AlignCtx& C, const float* rf, const std:
     J.bar = (unsigned*)C.nm_ctl + 2;
     J.ctl = C.nm_ctl;
     J.out = C.nm_out;
-    cudaError_t e = cudaMemsetAsync(C.nm_ctl, 0, sizeof(int) * 4, C.s);
+    return cudaSuccess;
+}
+static cudaError_t nm_launch(AlignCtx& C, NmJob& J) {
+    cudaError_t e = cudaMemsetAsync(C.nm_ctl + 2, 0, sizeof(int) * 2, C.s);  // the barrier; the error word stays sticky
     if (e != cudaSuccess) return e;
     void* args[] = {(void*)&J};
     lsb_launched();
-    e = cudaLaunchCooperativeKernel((void*)nm_search_kernel, dim3(g_nm_blocks), dim3(NM_THREADS), args, 0, C.s);
+    return cudaLaunchCooperativeKernel((void*)nm_search_kernel, dim3(g_nm_blocks), dim3(NM_THREADS), args, 0, C.s);
+}
+
+static cudaError_t multiscale_align_dev(AlignCtx& C, const float* rf, const std::vector<float*>& pr, const float* tg,
+                                        const std::vector<float*>& pt, int w, int h, const double init[8], const bool freem[8],
+                                        int coarsen, double out[8]) {
+    NmJob J;
+    cudaError_t e = nm_job(C, rf, pr, tg, pt, w, h, freem, coarsen, J);
+    if (e != cudaSuccess) return e;
+    for (int q = 0; q < 8; q++) J.init[q] = init[q];
+    e = cudaMemsetAsync(C.nm_ctl, 0, sizeof(int) * 2, C.s);
+    if (e == cudaSuccess) e = nm_launch(C, J);
     if (e != cudaSuccess) return e;
     cudaMemcpyAsync(C.sums_host, C.nm_out, sizeof(double) * 8, cudaMemcpyDeviceToHost, C.s);
     cudaMemcpyAsync(C.sums_host + 8, C.nm_ctl, sizeof(int) * 2, cudaMemcpyDeviceToHost, C.s);
@@ -957,6 +1010,36 @@ static cudaError_t multiscale_align_dev(AlignCtx& C, const float* rf, const std:
     for (int q = 0; q < 8; q++) out[q] = C.sums_host[q];
     C.evals += ctl[1];
     C.launches++;
+    return cudaSuccess;
+}
+
+cudaError_t align_chain_begin(AlignCtx& C, unsigned long long* evals_dev) {
+    cudaError_t e = cudaMemsetAsync(C.nm_ctl, 0, sizeof(int) * 4, C.s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(evals_dev, 0, sizeof(unsigned long long), C.s);
+    return e;
+}
+cudaError_t multiscale_align_chain(AlignCtx& C, const float* rf, const std::vector<float*>& pr, const float* tg,
+                                   const std::vector<float*>& pt, int w, int h, const double* init_dev, const bool freem[8], int coarsen,
+                                   double* out_dev, double* warp_dev, unsigned long long* evals_dev) {
+    NmJob J;
+    cudaError_t e = nm_job(C, rf, pr, tg, pt, w, h, freem, coarsen, J);
+    if (e != cudaSuccess) return e;
+    J.init_dev = init_dev;
+    J.out = out_dev;
+    J.warp_dev = warp_dev;
+    J.evals_dev = evals_dev;
+    C.launches++;
+    return nm_launch(C, J);
+}
+cudaError_t align_chain_end(AlignCtx& C, const unsigned long long* evals_dev, size_t* evals) {
+    int err = 0;
+    unsigned long long ev = 0;
+    cudaError_t e = cudaMemcpyAsync(&err, C.nm_ctl, sizeof err, cudaMemcpyDeviceToHost, C.s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&ev, evals_dev, sizeof ev, cudaMemcpyDeviceToHost, C.s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(C.s);
+    if (e != cudaSuccess) return e;
+    if (err != 0) return cudaErrorLaunchTimeout;
+    *evals = (size_t)ev;
     return cudaSuccess;
 }
 

@@ -50,6 +50,17 @@ bool sim_is_id(const double* v);
 cudaError_t multiscale_align(AlignCtx& C, const float* rf, const std::vector<float*>& pr, const float* tg,
                              const std::vector<float*>& pt, int w, int h, const double init[8], const bool freem[8], int coarsen,
                              double out[8]);
+// Chained searches, one frame after another with no host round trip: the
+// search of frame i starts from the device-resident result of frame i-1,
+// leaves its transform and full-resolution warp in device memory and adds its
+// evaluation count on the device; the error word is sticky until the end.
+cudaError_t align_chain_begin(AlignCtx& C, unsigned long long* evals_dev);
+cudaError_t multiscale_align_chain(AlignCtx& C, const float* rf, const std::vector<float*>& pr, const float* tg,
+                                   const std::vector<float*>& pt, int w, int h, const double* init_dev, const bool freem[8], int coarsen,
+                                   double* out_dev, double* warp_dev, unsigned long long* evals_dev);
+cudaError_t align_chain_end(AlignCtx& C, const unsigned long long* evals_dev, size_t* evals);
+// warp_plane with the warp a chained search left on the device (inverse [9], affine, identity)
+cudaError_t warp_plane_dev(const float* src, int w, int h, const double* warp_dev, int interp, float* out, cudaStream_t s);
 cudaError_t cost_single(AlignCtx& C, const float* rf, int aw, int ah, const float* tg, int tw, int th, const double sim[8],
                         double* cost);
 

@@ -68,6 +68,8 @@ struct lsb_engine {
     int device, sms, grid;
     int coop = 0;  // cooperative launch: the registration search runs on the device
     cudaStream_t s;
+    cudaStream_t cs = nullptr;  // host -> device frame copies, overlapped with the work on s
+    cudaEvent_t s_mark = nullptr;  // recorded on s so that cs can wait for the work queued before it
     DevPool pool;
     unsigned *hist, *sel;
     float* scal;  // [floor, p90, max, ...]
@@ -124,6 +126,12 @@ struct lsb_stack {
     double rel64 = 0.0;
     int iters = 0, iters_first = 0;
     double ms[12] = {0};
+    // registration chained on the device: per-frame transforms, the last warp, evaluations
+    double* sims_dev = nullptr;  // n*8
+    double* warp_dev = nullptr;  // inverse [9], affine, identity
+    unsigned long long* evals_dev = nullptr;
+    int aligned_upto = 0;        // frames already registered (at push time)
+    std::vector<cudaEvent_t> copied;  // per frame: its host -> device copy is done
     WlsSolver* ws = nullptr;  // planes of the depth grid's solve, kept across runs
     lsb_unet* net = nullptr;  // learned warm start of the solves (not owned)
     float* x0 = nullptr;      // its prediction on the depth grid
@@ -131,6 +139,7 @@ struct lsb_stack {
     ~lsb_stack() {
         wls_destroy(ws);
         if (x0) cudaFree(x0);
+        for (auto& v : copied) cudaEventDestroy(v);
     }
 };
 
@@ -157,6 +166,9 @@ static cudaError_t warm_start(lsb_stack* s, int dw, int dh, int n, cudaStream_t 
     if (e == cudaSuccess) *given = true;
     return e;
 }
+
+static bool chained(const lsb_stack* s);
+static char* align_frame(lsb_stack* s, int i);
 
 // The stack's WLS solver for a dw x dh grid and this run's guide: planes
 // allocated on the first run, edge weights recomputed every run.
@@ -204,6 +216,8 @@ char* lsb_engine_create(const lsb_config* cfg, lsb_engine** out) {
     e->sms = prop.multiProcessorCount;
     e->grid = e->cfg.grid_limit > 0 ? e->cfg.grid_limit : 2 * e->sms;
     TRY(cudaStreamCreateWithFlags(&e->s, cudaStreamNonBlocking));
+    TRY(cudaStreamCreateWithFlags(&e->cs, cudaStreamNonBlocking));
+    TRY(cudaEventCreateWithFlags(&e->s_mark, cudaEventDisableTiming));
     TRY(e->pool.get(&e->hist, 65536));
     TRY(e->pool.get(&e->sel, 4));
     TRY(e->pool.get(&e->scal, 16));
@@ -230,6 +244,8 @@ void lsb_engine_destroy(lsb_engine* e) {
     for (auto& v : e->ev) cudaEventDestroy(v);
     cudaFreeHost(e->actx.sums_host);
     e->pool.release();
+    if (e->cs) cudaStreamSynchronize(e->cs), cudaStreamDestroy(e->cs);
+    if (e->s_mark) cudaEventDestroy(e->s_mark);
     cudaStreamDestroy(e->s);
     delete e;
 }
@@ -332,7 +348,12 @@ static char* stack_alloc(lsb_stack* s) {
         }
         TRY(P.get(&s->bx_dev, N));
         TRY(P.get(&s->bpart, N * 64 * 7));
+        TRY(P.get(&s->sims_dev, (size_t)N * 8));
+        TRY(P.get(&s->warp_dev, 16));
+        TRY(P.get(&s->evals_dev, 1));
     }
+    s->copied.assign(N, nullptr);
+    for (auto& v : s->copied) TRY(cudaEventCreateWithFlags(&v, cudaEventDisableTiming));
     return nullptr;
 }
 
@@ -434,10 +455,22 @@ extern "C" char* lsb_stack_push_u16(lsb_stack* s, const uint16_t* rgb, size_t st
     if (stride_px < s->w) return dup_err("stride_px < width");
     uint16_t* dst = s->frames + (size_t)s->count * s->w * s->h * 3;
     cudaMemcpyKind kind = is_device_ptr(rgb) ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
-    if (stride_px == s->w) TRY(cudaMemcpyAsync(dst, rgb, sizeof(uint16_t) * 3 * (size_t)s->w * s->h, kind, s->e->s));
-    else TRY(cudaMemcpy2DAsync(dst, 6 * (size_t)s->w, rgb, 6 * stride_px, 6 * (size_t)s->w, s->h, kind, s->e->s));
+    // the copy runs on the engine's copy stream; the work on this frame waits for it
+    lsb_engine* e = s->e;
+    const int i = (int)s->count;
+    if (i == 0) {  // the frame store is rewritten: wait for whatever still reads it on the work stream
+        TRY(cudaEventRecord(e->s_mark, e->s));
+        TRY(cudaStreamWaitEvent(e->cs, e->s_mark, 0));
+    }
+    if (stride_px == s->w) TRY(cudaMemcpyAsync(dst, rgb, sizeof(uint16_t) * 3 * (size_t)s->w * s->h, kind, e->cs));
+    else TRY(cudaMemcpy2DAsync(dst, 6 * (size_t)s->w, rgb, 6 * stride_px, 6 * (size_t)s->w, s->h, kind, e->cs));
+    TRY(cudaEventRecord(s->copied[i], e->cs));
+    TRY(cudaStreamWaitEvent(e->s, s->copied[i], 0));
     s->count++;
     s->folded = false;
+    // register this frame now, behind the copy of the next one (stack.rs:785-821 does it per frame too)
+    if (s->ap.enabled && s->n > 1 && chained(s) && s->aligned_upto == i)
+        if (char* er = align_frame(s, i)) return er;
     return nullptr;
 }
 
@@ -474,11 +507,64 @@ extern "C" char* lsb_stack_set_count(lsb_stack* s, uint32_t count) {
     if (count > s->n) return dup_err("count exceeds the stack's frames");
     s->count = count;
     s->folded = false;
+    s->aligned_upto = 0;
     return nullptr;
 }
 
 // ------------------------------------------------------------- pipeline
+static void free_mask(const lsb_stack* s, bool freem[8]) {
+    const bool aff = s->ap.model != 0, proj = s->ap.model == 2;
+    const bool m[8] = {s->ap.shift != 0, s->ap.shift != 0, s->ap.scale != 0, s->ap.rotation != 0, aff, aff, proj, proj};
+    memcpy(freem, m, sizeof m);
+}
+// Registration chained on the device (stack.rs:513-530 per frame): frame i's
+// luma and pyramid, its search from frame i-1's transform against frame
+// i-1's aligned luma, then its own aligned luma as frame i+1's reference.
+// Nothing returns to the host between frames.
+static bool chained(const lsb_stack* s) { return !s->ap.host_search && s->e->coop; }
+static char* run_align_host(lsb_stack* s);
+static char* align_frame(lsb_stack* s, int i) {
+    lsb_engine* e = s->e;
+    AlignCtx& C = e->actx;
+    const int W = (int)s->w, H = (int)s->h, n = (int)s->n;
+    const uint16_t* f = s->frames + (size_t)i * W * H * 3;
+    if (i == 0) {
+        static const double id[8] = {0, 0, 1, 0, 1, 0, 0, 0};
+        TRY(align_chain_begin(C, s->evals_dev));
+        TRY(cudaMemcpyAsync(s->sims_dev, id, sizeof id, cudaMemcpyHostToDevice, e->s));
+        TRY(luma_u16(f, W, H, s->yr, e->s));
+        TRY(gauss_levels(s->yr, W, H, s->pr, e->s));
+    } else {
+        bool freem[8];
+        free_mask(s, freem);
+        TRY(luma_u16(f, W, H, s->yt, e->s));
+        TRY(gauss_levels(s->yt, W, H, s->pt, e->s));
+        TRY(multiscale_align_chain(C, s->yr, s->pr, s->yt, s->pt, W, H, s->sims_dev + 8 * (size_t)(i - 1), freem, (int)s->ap.coarsen,
+                                   s->sims_dev + 8 * (size_t)i, s->warp_dev, s->evals_dev));
+        if (i + 1 < n) {
+            TRY(warp_plane_dev(s->yt, W, H, s->warp_dev, (int)s->ap.interp, s->yr, e->s));
+            TRY(gauss_levels(s->yr, W, H, s->pr, e->s));
+        }
+    }
+    s->aligned_upto = i + 1;
+    return nullptr;
+}
+
 static char* run_align(lsb_stack* s) {
+    if (chained(s)) {
+        for (int i = s->aligned_upto; i < (int)s->count; i++)
+            if (char* er = align_frame(s, i)) return er;
+        size_t evals = 0;
+        TRY(align_chain_end(s->e->actx, s->evals_dev, &evals));
+        TRY(cudaMemcpy(s->sims.data(), s->sims_dev, sizeof(double) * 8 * s->count, cudaMemcpyDeviceToHost));
+        s->align_evals = evals;
+        s->aligned_upto = 0;  // a later run registers the frames again
+        return nullptr;
+    }
+    return run_align_host(s);
+}
+
+static char* run_align_host(lsb_stack* s) {
     lsb_engine* e = s->e;
     const int W = (int)s->w, H = (int)s->h, n = (int)s->count;
     AlignCtx& C = e->actx;
@@ -1070,9 +1156,10 @@ extern "C" char* lsb_wls_solve(lsb_engine* e, const float* d, const float* conf,
     TRY(cudaMemcpyAsync(cc, conf, sizeof(float) * m, cudaMemcpyHostToDevice, st));
     TRY(cudaMemcpyAsync(gg, guide, sizeof(float) * m, cudaMemcpyHostToDevice, st));
     TRY(cudaMemsetAsync(uu, 0, sizeof(float) * m, st));
-    TRY(cudaEventRecord(e->ev[0], st));
     cudaError_t ce;
-    WlsSolver* ws = wls_create(gg, (int)w, (int)h, lambda, sigma_c, (int)edge_mode, st, &ce);
+    WlsSolver* ws = wls_alloc((int)w, (int)h, &ce);  // planes first: the timed part is the solve
+    if (ce == cudaSuccess) ce = cudaEventRecord(e->ev[0], st);
+    if (ce == cudaSuccess) ce = wls_prepare(ws, gg, lambda, sigma_c, (int)edge_mode, st);
     if (ce == cudaSuccess) ce = wls_set_weights(ws, cc, st);
     float r = 0.f;
     int it = 0;
