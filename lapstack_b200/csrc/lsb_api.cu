@@ -13,7 +13,10 @@
 #include <algorithm>
 #include <array>
 #include <atomic>
+#include <map>
+#include <mutex>
 #include <string>
+#include <unordered_map>
 #include <vector>
 
 #include "lapstack_b200.h"
@@ -135,6 +138,7 @@ struct lsb_stack {
     WlsSolver* ws = nullptr;  // planes of the depth grid's solve, kept across runs
     lsb_unet* net = nullptr;  // learned warm start of the solves (not owned)
     float* x0 = nullptr;      // its prediction on the depth grid
+    float* winner_full = nullptr;  // the winner map at full size (finish)
     size_t x0_cells = 0;
     ~lsb_stack() {
         wls_destroy(ws);
@@ -969,6 +973,55 @@ static void common_area(const std::vector<double>& sims, int n, int w, int h, in
     }
 }
 
+// Page-locked host blocks for the large result planes: the device -> host
+// copies run at the link's speed, and a freed result's blocks serve the next
+// result of the same size instead of being pinned again (at most
+// HB_CACHE_BYTES are kept unused).
+static std::mutex g_hb_mu;
+static std::multimap<size_t, void*> g_hb_free;
+static std::unordered_map<void*, size_t> g_hb_size;
+static size_t g_hb_cached = 0;
+constexpr size_t HB_CACHE_BYTES = (size_t)8 << 30;
+static void* hb_get(size_t bytes) {
+    {
+        std::lock_guard<std::mutex> lk(g_hb_mu);
+        auto it = g_hb_free.find(bytes);
+        if (it != g_hb_free.end()) {
+            void* p = it->second;
+            g_hb_free.erase(it);
+            g_hb_cached -= bytes;
+            return p;
+        }
+    }
+    void* p = nullptr;
+    if (cudaHostAlloc(&p, bytes, cudaHostAllocDefault) != cudaSuccess) {
+        cudaGetLastError();
+        return malloc(bytes);  // pageable: slower copies, same results
+    }
+    std::lock_guard<std::mutex> lk(g_hb_mu);
+    g_hb_size[p] = bytes;
+    return p;
+}
+static void hb_release(void* p) {
+    if (!p) return;
+    {
+        std::lock_guard<std::mutex> lk(g_hb_mu);
+        auto it = g_hb_size.find(p);
+        if (it != g_hb_size.end()) {
+            if (g_hb_cached + it->second <= HB_CACHE_BYTES) {
+                g_hb_free.emplace(it->second, p);
+                g_hb_cached += it->second;
+                return;
+            }
+            g_hb_size.erase(it);
+        } else {
+            free(p);
+            return;
+        }
+    }
+    cudaFreeHost(p);
+}
+
 extern "C" char* lsb_stack_finish(lsb_stack* s, lsb_result* r) {
     if (!s || !r) return dup_err("null argument");
     memset(r, 0, sizeof *r);
@@ -980,35 +1033,30 @@ extern "C" char* lsb_stack_finish(lsb_stack* s, lsb_result* r) {
     r->h = s->h;
     r->n_frames = s->count;
     r->levels = s->levels;
-    r->image_u16 = (uint16_t*)malloc(sizeof(uint16_t) * 3 * W * H);
-    r->image_f32 = (float*)malloc(sizeof(float) * 3 * W * H);
-    r->winner = (float*)malloc(sizeof(float) * W * H);
+    r->image_u16 = (uint16_t*)hb_get(sizeof(uint16_t) * 3 * W * H);
+    r->image_f32 = (float*)hb_get(sizeof(float) * 3 * W * H);
+    r->winner = (float*)hb_get(sizeof(float) * W * H);
     r->sims = (double*)malloc(sizeof(double) * 8 * N);
     r->gains = (float*)malloc(sizeof(float) * 3 * N);
     r->shares = (float*)malloc(sizeof(float) * N);
     TRY(cudaMemcpyAsync(r->image_u16, s->img_u16, sizeof(uint16_t) * 3 * W * H, cudaMemcpyDeviceToHost, st));
     TRY(cudaMemcpyAsync(r->image_f32, s->img, sizeof(float) * 3 * W * H, cudaMemcpyDeviceToHost, st));
     const int dl = s->depth_level, dwl = s->lw[dl], dhl = s->lh[dl];
-    std::vector<uint16_t> win((size_t)dwl * dhl);
-    TRY(cudaMemcpyAsync(win.data(), s->winner, sizeof(uint16_t) * win.size(), cudaMemcpyDeviceToHost, st));
+    if (!s->winner_full) TRY(s->pool.get(&s->winner_full, W * H));
+    TRY(upsample_index(s->winner, dwl, dhl, 1 << dl, (int)W, (int)H, s->winner_full, st));
+    TRY(cudaMemcpyAsync(r->winner, s->winner_full, sizeof(float) * W * H, cudaMemcpyDeviceToHost, st));
     if (s->dp.enabled) {
         const size_t m = (size_t)s->dw * s->dh;
         r->dw = s->dw;
         r->dh = s->dh;
-        r->depth = (float*)malloc(sizeof(float) * W * H);
-        r->conf = (float*)malloc(sizeof(float) * W * H);
+        r->depth = (float*)hb_get(sizeof(float) * W * H);
+        r->conf = (float*)hb_get(sizeof(float) * W * H);
         r->floor_cells = (float*)malloc(sizeof(float) * m);
         TRY(cudaMemcpyAsync(r->depth, s->dfull, sizeof(float) * W * H, cudaMemcpyDeviceToHost, st));
         TRY(cudaMemcpyAsync(r->conf, s->cfull, sizeof(float) * W * H, cudaMemcpyDeviceToHost, st));
         TRY(cudaMemcpyAsync(r->floor_cells, s->mins, sizeof(float) * m, cudaMemcpyDeviceToHost, st));
     }
     TRY(cudaStreamSynchronize(st));
-    // fuse.rs:336 upsample_index
-    const size_t scale = (size_t)1 << dl;
-    for (size_t y = 0; y < H; y++) {
-        const size_t sy = std::min(y / scale, (size_t)dhl - 1);
-        for (size_t x = 0; x < W; x++) r->winner[y * W + x] = (float)win[sy * dwl + std::min(x / scale, (size_t)dwl - 1)];
-    }
     memcpy(r->sims, s->sims.data(), sizeof(double) * 8 * N);
     memcpy(r->gains, s->gains.data(), sizeof(float) * 3 * N);
     err = shares_of(s, r->shares);
@@ -1037,11 +1085,11 @@ extern "C" void lsb_stack_destroy(lsb_stack* s) {
 
 extern "C" void lsb_result_free(lsb_result* r) {
     if (!r) return;
-    free(r->image_u16);
-    free(r->image_f32);
-    free(r->winner);
-    free(r->depth);
-    free(r->conf);
+    hb_release(r->image_u16);
+    hb_release(r->image_f32);
+    hb_release(r->winner);
+    hb_release(r->depth);
+    hb_release(r->conf);
     free(r->floor_cells);
     free(r->sims);
     free(r->gains);

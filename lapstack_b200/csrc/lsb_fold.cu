@@ -231,6 +231,18 @@ __global__ void collapse_kernel(const float* __restrict__ acc, const float* __re
     }
 }
 
+// fuse.rs:336 `upsample_index`: the depth level's winner map, nearest, to full size (clamped at the edge)
+__global__ void upsample_index_kernel(const uint16_t* __restrict__ win, int dwl, int dhl, int scale, int w, int h, float* __restrict__ out) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
+    if (x >= w || y >= h) return;
+    out[(size_t)y * w + x] = (float)win[(size_t)min(y / scale, dhl - 1) * dwl + min(x / scale, dwl - 1)];
+}
+cudaError_t upsample_index(const uint16_t* win, int dwl, int dhl, int scale, int w, int h, float* out, cudaStream_t s) {
+    dim3 b(32, 8), g((w + 31) / 32, (h + 7) / 8);
+    lsb_launched(), upsample_index_kernel<<<g, b, 0, s>>>(win, dwl, dhl, scale, w, h, out);
+    return cudaGetLastError();
+}
+
 cudaError_t collapse_level(const float* acc, const float* coarse, float* out, int w, int h, int cw, int ch, bool last,
                            uint16_t* rgb_out, cudaStream_t s) {
     dim3 b(32, 8), g((w + 31) / 32, (h + 7) / 8);

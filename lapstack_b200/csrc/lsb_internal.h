@@ -79,6 +79,9 @@ cudaError_t fuse_residuals(const ResidualArgs& a, int storage, const float* lnp,
 cudaError_t collapse_level(const float* acc, const float* coarse, float* out, int w, int h, int cw, int ch, bool last,
                            uint16_t* rgb_out, cudaStream_t s);
 
+// fuse.rs:336 upsample_index of the depth level's winner map to w x h (f32 frame indices).
+cudaError_t upsample_index(const uint16_t* win, int dwl, int dhl, int scale, int w, int h, float* out, cudaStream_t s);
+
 // winner_shares (fuse.rs:315) on the device: counts[frames] of detail cells.
 cudaError_t winner_counts(const uint16_t* win, const float* best, int cells, int frames, unsigned int* counts,
                           float* scratch_max, cudaStream_t s);

@@ -203,6 +203,27 @@ def _arr(ptr, n, dt):
     return np.ctypeslib.as_array(ptr, shape=(n,)).astype(dt, copy=True)
 
 
+class _ResultOwner:
+    """Frees an lsb_result once no array viewing its buffers is left."""
+
+    def __init__(self, lib, r):
+        self._lib, self._r = lib, r
+
+    def __del__(self):
+        try:
+            self._lib.lsb_result_free(C.byref(self._r))
+        except Exception:
+            pass
+
+
+def _view(owner, ptr, n, dt):
+    """A numpy view of a result buffer (no copy) that keeps the result alive."""
+    ct = np.ctypeslib.as_ctypes_type(np.dtype(dt))
+    buf = (ct * n).from_address(C.cast(ptr, C.c_void_p).value)
+    buf._owner = owner
+    return np.frombuffer(buf, dtype=dt)
+
+
 class Stack:
     """One stack: push frames (host or device), then finish (stack.rs:1011 run_with)."""
 
@@ -290,21 +311,19 @@ class Stack:
         r = Result()
         check(self._L.lsb_stack_finish(self._h, C.byref(r)))
         self._keep.clear()
-        try:
-            w, h, n = r.w, r.h, r.n_frames
-            img = _arr(r.image_f32, 3 * w * h, np.float32).reshape(3, h, w)
-            u16 = _arr(r.image_u16, 3 * w * h, np.uint16).reshape(h, w, 3)
-            win = _arr(r.winner, w * h, np.float32).reshape(h, w)
-            dm = None
-            if r.depth:
-                dm = DepthMap(_arr(r.depth, w * h, np.float32).reshape(h, w), _arr(r.conf, w * h, np.float32).reshape(h, w), w,
-                              h, r.dw, r.dh, _arr(r.floor_cells, r.dw * r.dh, np.float32).reshape(r.dh, r.dw), r.floor_value,
-                              r.p90, r.wls_rel, r.wls_rel64, r.wls_iters, r.wls_iters_first)
-            return Output(img, u16, win, dm, _arr(r.sims, 8 * n, np.float64).reshape(n, 8),
-                          _arr(r.gains, 3 * n, np.float32).reshape(n, 3), _arr(r.shares, n, np.float32), r.levels,
-                          tuple(r.crop), r.align_evals, dict(zip(STAGES, list(r.ms))))
-        finally:
-            self._L.lsb_result_free(C.byref(r))
+        own = _ResultOwner(self._L, r)  # the large planes are views of the library's buffers
+        w, h, n = r.w, r.h, r.n_frames
+        img = _view(own, r.image_f32, 3 * w * h, np.float32).reshape(3, h, w)
+        u16 = _view(own, r.image_u16, 3 * w * h, np.uint16).reshape(h, w, 3)
+        win = _view(own, r.winner, w * h, np.float32).reshape(h, w)
+        dm = None
+        if r.depth:
+            dm = DepthMap(_view(own, r.depth, w * h, np.float32).reshape(h, w), _view(own, r.conf, w * h, np.float32).reshape(h, w),
+                          w, h, r.dw, r.dh, _arr(r.floor_cells, r.dw * r.dh, np.float32).reshape(r.dh, r.dw), r.floor_value,
+                          r.p90, r.wls_rel, r.wls_rel64, r.wls_iters, r.wls_iters_first)
+        return Output(img, u16, win, dm, _arr(r.sims, 8 * n, np.float64).reshape(n, 8),
+                      _arr(r.gains, 3 * n, np.float32).reshape(n, 3), _arr(r.shares, n, np.float32), r.levels,
+                      tuple(r.crop), r.align_evals, dict(zip(STAGES, list(r.ms))))
 
 
 class GpuFuser:
