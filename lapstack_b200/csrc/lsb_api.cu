@@ -99,6 +99,7 @@ struct lsb_stack {
     void* warped = nullptr;  // aligned frames, written once before the fold (f32 planar or u16 interleaved)
     std::vector<void*> g;      // G storage per level 1..levels (index l)
     std::vector<float*> acc, best;
+    std::vector<float*> halo_w;  // halo control: each frame's weights at the guide level and the coarser ones
     uint16_t* winner = nullptr;
     void* slices = nullptr;
     int dw = 0, dh = 0, bk = 1;
@@ -385,10 +386,6 @@ extern "C" char* lsb_stack_begin(lsb_engine* e, uint32_t w, uint32_t h, uint32_t
         return dup_err("storage must be 0 (FP32), 1 (UNORM16 levels, FP16 slices) or 2 (FP16)");
     }
     s->f32src = false;
-    if (s->fp.halo > 0.f) {
-        delete s;
-        return dup_err("halo control (FuseParams::halo > 0) is not on the device path");
-    }
     if (s->fp.energy_radius > 2) {
         delete s;
         return dup_err("energy_radius must be 0..2");
@@ -719,9 +716,22 @@ static char* run_pipeline(lsb_stack* s) {
     for (float g : s->gains) maxg = std::max(maxg, g);
     if (s->f32src) maxg = 1.f;
     const float gscale = (float)(65535.0 / maxg), ginv = (float)(maxg / 65535.0);
+    // fuse.rs:120 halo_guide: the guide level and the hardness, when on (fuse.rs:112 HALO_MAX = 8)
+    const bool halo = s->fp.halo > 0.f;
+    const int guide = std::min((int)s->fp.depth_level, s->levels - 1);
+    if (halo && s->halo_w.empty()) {
+        s->halo_w.assign(s->levels + 1, nullptr);
+        for (int l = guide; l <= s->levels; l++) TRY(s->pool.get(&s->halo_w[l], (size_t)s->n * s->lw[l] * s->lh[l]));
+    }
     for (int l = 0; l < s->levels; l++) {
         FoldArgs a{};
         a.level = l;
+        if (halo && l >= guide) {
+            a.halo_mode = l == guide ? 1 : 2;
+            a.halo_p = std::min(s->fp.halo, 8.0f);
+            a.halo_w = s->halo_w[l];
+            if (l > guide) TRY(reduce_weights(s->halo_w[l - 1], s->lw[l - 1], s->lh[l - 1], n, s->halo_w[l], s->lw[l], s->lh[l], st));
+        }
         a.nframes = n;
         a.W = s->lw[l];
         a.H = s->lh[l];
@@ -768,8 +778,17 @@ static char* run_pipeline(lsb_stack* s) {
         const float inv_n = 1.0f / (float)nwin;
         for (int c = 1; c <= nwin; c++) lnp[c] = logf((float)c * inv_n);
         TRY(cudaMemcpyAsync(s->lnp, lnp.data(), sizeof(float) * 128, cudaMemcpyHostToDevice, st));
-        ResidualArgs ra{s->g[s->levels], n, wt, ht, (int)s->fp.top_rule, r, (int)s->fp.entropy_bins, s->dev_s, s->ent_s, s->top, ginv};
-        TRY(fuse_residuals(ra, s->storage, s->lnp, st));
+        if (halo) {
+            // fuse.rs:453-475 below the guide, fuse.rs:505-510 the weighted means
+            const int L = s->levels;
+            TRY(reduce_weights(s->halo_w[L - 1], s->lw[L - 1], s->lh[L - 1], n, s->halo_w[L], wt, ht, st));
+            TRY(halo_top(s->g[L], s->storage, ginv, s->halo_w[L], n, wt, ht, s->top, s->dev_s, st));
+            TRY(halo_divide(s->top, s->dev_s, wt, ht, st));
+            for (int l = guide + 1; l < L; l++) TRY(halo_divide(s->acc[l], s->best[l], s->lw[l], s->lh[l], st));
+        } else {
+            ResidualArgs ra{s->g[s->levels], n, wt, ht, (int)s->fp.top_rule, r, (int)s->fp.entropy_bins, s->dev_s, s->ent_s, s->top, ginv};
+            TRY(fuse_residuals(ra, s->storage, s->lnp, st));
+        }
         const float* coarse = s->top;
         for (int l = s->levels - 1; l >= 0; l--) {
             // even levels land in img, odd ones in img_tmp: a level never overwrites its coarser input

@@ -198,6 +198,66 @@ cudaError_t fuse_residuals(const ResidualArgs& a, int storage, const float* lnp,
     return cudaGetLastError();
 }
 
+// ------------------------------------------------------------- halo control
+// pyramid.rs:86 REDUCE of one f32 plane per frame: the 5 reflected rows each
+// reduced along x (the row pass), then those 5 values along y (the column
+// pass) -- the same operations, in the same order, as the two passes.
+__global__ void reduce_weights_kernel(const float* __restrict__ src, int w, int h, float* __restrict__ dst, int w1, int h1) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x, i = blockIdx.y * blockDim.y + threadIdx.y, k = blockIdx.z;
+    if (j >= w1 || i >= h1) return;
+    const float* p = src + (size_t)k * w * h;
+    float r[5];
+    for (int t = 0; t < 5; t++) {
+        const float* row = p + (size_t)lsb_reflect(2 * i + t - 2, h) * w;
+        r[t] = lsb_tap5(row[lsb_reflect(2 * j - 2, w)], row[lsb_reflect(2 * j - 1, w)], row[lsb_reflect(2 * j, w)],
+                        row[lsb_reflect(2 * j + 1, w)], row[lsb_reflect(2 * j + 2, w)]);
+    }
+    dst[(size_t)k * w1 * h1 + (size_t)i * w1 + j] = lsb_tap5(r[0], r[1], r[2], r[3], r[4]);
+}
+cudaError_t reduce_weights(const float* src, int w, int h, int n, float* dst, int w1, int h1, cudaStream_t s) {
+    dim3 b(32, 8), g((w1 + 31) / 32, (h1 + 7) / 8, n);
+    lsb_launched(), reduce_weights_kernel<<<g, b, 0, s>>>(src, w, h, dst, w1, h1);
+    return cudaGetLastError();
+}
+// fuse.rs:466-470 at the top level: acc = G * w for frame 0, then acc += w * G; best = sum w
+template <class GS>
+__global__ void halo_top_kernel(const GS* __restrict__ tops, float ginv, const float* __restrict__ wts, int n, int w, int h,
+                                float* __restrict__ acc, float* __restrict__ best) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
+    if (x >= w || y >= h) return;
+    const size_t n2 = (size_t)w * h, o = (size_t)y * w + x;
+    const float2 sc = make_float2(1.f / ginv, ginv);
+    float a[3] = {0.f, 0.f, 0.f}, b = 0.f;
+    for (int k = 0; k < n; k++) {
+        const float wv = wts[(size_t)k * n2 + o];
+        for (int c = 0; c < 3; c++) {
+            const float g = Store<GS>::ld(tops + ((size_t)k * 3 + c) * n2 + o, sc);
+            a[c] = k == 0 ? __fmul_rn(g, wv) : __fadd_rn(a[c], __fmul_rn(wv, g));
+        }
+        b = k == 0 ? wv : __fadd_rn(b, wv);
+    }
+    for (int c = 0; c < 3; c++) acc[c * n2 + o] = a[c];
+    best[o] = b;
+}
+cudaError_t halo_top(const void* tops, int storage, float ginv, const float* wts, int n, int w, int h, float* acc, float* best,
+                     cudaStream_t s) {
+    dim3 b(32, 8), g((w + 31) / 32, (h + 7) / 8);
+    if (storage == STORE_UNORM16) lsb_launched(), halo_top_kernel<unorm16><<<g, b, 0, s>>>((const unorm16*)tops, ginv, wts, n, w, h, acc, best);
+    else if (storage == STORE_F16) lsb_launched(), halo_top_kernel<__half><<<g, b, 0, s>>>((const __half*)tops, ginv, wts, n, w, h, acc, best);
+    else lsb_launched(), halo_top_kernel<float><<<g, b, 0, s>>>((const float*)tops, ginv, wts, n, w, h, acc, best);
+    return cudaGetLastError();
+}
+// fuse.rs:508: the weighted means
+__global__ void halo_divide_kernel(float* __restrict__ acc, const float* __restrict__ best, size_t n2) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n2; i += (size_t)gridDim.x * blockDim.x)
+        for (int c = 0; c < 3; c++) acc[c * n2 + i] = __fdiv_rn(acc[c * n2 + i], best[i]);
+}
+cudaError_t halo_divide(float* acc, const float* best, int w, int h, cudaStream_t s) {
+    const size_t n2 = (size_t)w * h;
+    lsb_launched(), halo_divide_kernel<<<(int)std::min<size_t>((n2 + 255) / 256, 148 * 8), 256, 0, s>>>(acc, best, n2);
+    return cudaGetLastError();
+}
+
 // ------------------------------------------------------------------ collapse
 // pyramid.rs:219: G_l = L_l + EXPAND(G_{l+1}), EXPAND horizontal then
 // vertical (pyramid.rs:143) evaluated per output pixel with the same taps;

@@ -48,6 +48,12 @@ struct FoldArgs {
     int ntaps;
     int* status;  // device error word
     float gscale, ginv;  // the 16-bit fixed-point storage's scale and its inverse
+    // halo control (fuse.rs:112-136, 453-475): 1 at the guide level (select, and write each frame's
+    // weight plane halo_w [n][H][W]); 2 at coarser levels (no selection: acc = sum w*L, best = sum w,
+    // frames in order, with halo_w the weights REDUCEd to this level)
+    int halo_mode;
+    float halo_p;
+    float* halo_w;
     cudaEvent_t between;  // host side: recorded between the REDUCE and the select launch (may be null)
 };
 
@@ -78,6 +84,15 @@ cudaError_t fuse_residuals(const ResidualArgs& a, int storage, const float* lnp,
 // Collapse: out_l = acc_l + EXPAND(coarse) (pyramid.rs:219); at level 0 also clamp and pack.
 cudaError_t collapse_level(const float* acc, const float* coarse, float* out, int w, int h, int cw, int ch, bool last,
                            uint16_t* rgb_out, cudaStream_t s);
+
+// Halo control's coarse part: each frame's weight plane REDUCEd one level
+// (pyramid.rs:86, planes [n][h][w] -> [n][h1][w1]); the weighted sums of the
+// top Gaussian level (acc [3][h][w] = sum w*G, best = sum w, frames in order);
+// and the weighted means acc /= best.
+cudaError_t reduce_weights(const float* src, int w, int h, int n, float* dst, int w1, int h1, cudaStream_t s);
+cudaError_t halo_top(const void* tops, int storage, float ginv, const float* wts, int n, int w, int h, float* acc, float* best,
+                     cudaStream_t s);
+cudaError_t halo_divide(float* acc, const float* best, int w, int h, cudaStream_t s);
 
 // fuse.rs:336 upsample_index of the depth level's winner map to w x h (f32 frame indices).
 cudaError_t upsample_index(const uint16_t* win, int dwl, int dhl, int scale, int w, int h, float* out, cudaStream_t s);

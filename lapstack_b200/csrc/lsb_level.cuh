@@ -47,6 +47,12 @@ __device__ __forceinline__ float binw(int t) {
     return 1.f;
 }
 
+// fuse.rs:127 `halo_weight`: exp(clamp(p * ln((E + 1e-8) / 1e-4), -60, 60))
+__device__ __forceinline__ float halo_weight(float e, float p) {
+    const float v = __fmul_rn(p, logf(__fdiv_rn(__fadd_rn(e, 1e-8f), 1e-4f)));
+    return expf(fminf(fmaxf(v, -60.f), 60.f));
+}
+
 // The level-l value of (x, y), three channels, from the level's source:
 // level 0 the frame (u16 interleaved or f32 planar) times its gains
 // (brightness.rs:124); above, the stored Gaussian level.
@@ -261,7 +267,7 @@ __device__ __forceinline__ void select_frame(const FoldArgs& a, float* __restric
             yb[(y - t.yL0) * lw + x - t.xL0] = lpoint(x, y, Lr[j]);
         }
     }
-    if (R > 0) {
+    if (R > 0 && a.halo_mode != 2) {
         // the window's halo ring around the tile: energy only
         const int left = t.x0 - t.xL0, right = t.xL1 - (t.x0 + t.ox1);
         for (int yi = ty; yi < lh; yi += 8) {
@@ -278,6 +284,21 @@ __device__ __forceinline__ void select_frame(const FoldArgs& a, float* __restric
     __syncthreads();
 
     // ---- 4: the binomial window (fuse.rs:168) along rows, then columns + the selection
+    if (a.halo_mode == 2) {
+        // halo control below the guide (fuse.rs:466-470): acc = L * w for the first frame,
+        // then acc += w * L; best = the sum of the weights
+#pragma unroll
+        for (int j = 0; j < PPT; j++) {
+            const int px = tx + 32 * (j & 1), py = ty + 8 * (j >> 1);
+            if (px >= t.ox1 || py >= t.oy1) continue;
+            const float wv = a.halo_w[((size_t)k * H + t.y0 + py) * W + t.x0 + px];
+#pragma unroll
+            for (int c = 0; c < 3; c++) acc[j][c] = k == 0 ? __fmul_rn(Lr[j][c], wv) : __fadd_rn(acc[j][c], __fmul_rn(wv, Lr[j][c]));
+            best[j] = k == 0 ? wv : __fadd_rn(best[j], wv);
+        }
+        __syncthreads();
+        return;
+    }
     float* eh = exph;
     if (R > 0) {
         for (int r = ty; r < lh; r += 8)
@@ -302,6 +323,7 @@ __device__ __forceinline__ void select_frame(const FoldArgs& a, float* __restric
         } else {
             e = yb[(py + t.y0 - t.yL0) * lw + px + t.x0 - t.xL0];
         }
+        if (a.halo_mode == 1) a.halo_w[((size_t)k * H + t.y0 + py) * W + t.x0 + px] = halo_weight(e, a.halo_p);
         if (e > best[j]) {
             best[j] = e;
             acc[j][0] = Lr[j][0];

@@ -86,6 +86,25 @@ def test_fuser_energy_variants(radius, chroma):
     assert_same(ri, di, "fused image")
 
 
+@pytest.mark.parametrize("hardness,depth_level,size", [(2.0, 1, (150, 100)), (8.0, 2, (257, 131)), (0.5, 0, (96, 64))])
+def test_fuser_halo_control_matches_oracle(hardness, depth_level, size):
+    """fuse.rs:112-136/453-510 halo control: the levels up to the guide select
+    as usual (winner map and shares exact); the coarser ones are the
+    guide-energy-weighted means. The weights go through the f32 ln and exp
+    (the platform libm in the oracle, CUDA's on the device), so the fused image
+    is held to 1e-5 instead of bit-exactness."""
+    w, h = size
+    frames = [blur(xorshift_img(w, h, 40 + k), 1 + k % 3, O) for k in range(5)]
+    p = L.FuseParams(levels=4, depth_level=depth_level, halo=hardness)
+    (ri, rw, rs), (di, dw, ds) = fuse_both(frames, p)
+    assert_same(rw, dw, "winner map")
+    assert_same(rs, ds, "shares")
+    assert np.max(np.abs(ri.astype(np.float64) - di.astype(np.float64))) <= 1e-5
+    # and halo control changes the result
+    (ni, _, _), _ = fuse_both(frames, L.FuseParams(levels=4, depth_level=depth_level))
+    assert np.max(np.abs(ni - ri)) > 1e-4
+
+
 def synth(w, h, n, **kw):
     return L.synth_stack(L.SynthSpec(w, h, n, **kw))[0]
 
