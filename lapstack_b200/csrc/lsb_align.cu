@@ -18,6 +18,7 @@
 #include <algorithm>
 #include <atomic>
 #include <cmath>
+#include <cstdlib>
 #include <functional>
 #include <vector>
 
@@ -40,17 +41,16 @@ __global__ void luma_u16_kernel(const uint16_t* __restrict__ f, size_t n, float*
     }
 }
 
-// align.rs:650 Burt's kernel, a = 0.33: [c, b, a, b, c]
-__device__ __forceinline__ float burt_k(int t) {
-    const float a = 0.33f, b = 0.25f, c = __fsub_rn(0.25f, __fdiv_rn(a, 2.0f));
-    return t == 2 ? a : ((t == 1 || t == 3) ? b : c);
-}
+// align.rs:650 Burt's kernel, a = 0.33: [c, b, a, b, c] with c = 0.25 - a/2 in f32
+// (set from the host, whose f32 division and subtraction round the same way).
+__constant__ float c_burt[5];
 // align.rs:658 `norm_full`: the in-bounds taps summed in order
 __device__ __forceinline__ float burt_norm(int i, int n) {
     float s = 0.f;
+#pragma unroll
     for (int t = 0; t < 5; t++) {
         int x = i + t - 2;
-        if (x >= 0 && x < n) s = __fadd_rn(s, burt_k(t));
+        if (x >= 0 && x < n) s = __fadd_rn(s, c_burt[t]);
     }
     return s;
 }
@@ -61,16 +61,27 @@ __global__ void reduce_burt_kernel(const float* __restrict__ src, int w, int h, 
     if (oj >= ow || oi >= oh) return;
     const int cx = 2 * oj, cy = 2 * oi;
     float v = 0.f;
-    for (int t = 0; t < 5; t++) {
-        const int y = cy + t - 2;
-        if (y < 0 || y >= h) continue;
-        const float* row = src + (size_t)y * w;
-        float a = 0.f;
-        for (int u = 0; u < 5; u++) {
-            const int x = cx + u - 2;
-            if (x >= 0 && x < w) a = __fadd_rn(a, __fmul_rn(burt_k(u), row[x]));
+    if (cx >= 2 && cx + 2 < w && cy >= 2 && cy + 2 < h) {
+        const float* row = src + (size_t)(cy - 2) * w + cx - 2;
+#pragma unroll
+        for (int t = 0; t < 5; t++, row += w) {
+            float a = 0.f;
+#pragma unroll
+            for (int u = 0; u < 5; u++) a = __fadd_rn(a, __fmul_rn(c_burt[u], row[u]));
+            v = __fadd_rn(v, __fmul_rn(c_burt[t], a));
         }
-        v = __fadd_rn(v, __fmul_rn(burt_k(t), a));
+    } else {
+        for (int t = 0; t < 5; t++) {
+            const int y = cy + t - 2;
+            if (y < 0 || y >= h) continue;
+            const float* row = src + (size_t)y * w;
+            float a = 0.f;
+            for (int u = 0; u < 5; u++) {
+                const int x = cx + u - 2;
+                if (x >= 0 && x < w) a = __fadd_rn(a, __fmul_rn(c_burt[u], row[x]));
+            }
+            v = __fadd_rn(v, __fmul_rn(c_burt[t], a));
+        }
     }
     out[(size_t)oi * ow + oj] = __fdiv_rn(v, __fmul_rn(burt_norm(cy, h), burt_norm(cx, w)));
 }
@@ -264,7 +275,24 @@ void gauss_dims(int w, int h, std::vector<std::pair<int, int>>& dims) {
     }
 }
 
+static cudaError_t set_burt(cudaStream_t s) {
+    static std::atomic<int> done[128];
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 0 || dev >= 128) return cudaErrorInvalidDevice;
+    if (done[dev].load()) return cudaSuccess;
+    volatile float a = 0.33f, two = 2.0f, q = 0.25f;  // f32 arithmetic, as the reference's const fn
+    const float c = q - a / two;
+    const float k[5] = {c, 0.25f, 0.33f, 0.25f, c};
+    cudaError_t e = cudaMemcpyToSymbol(c_burt, k, sizeof k);
+    if (e == cudaSuccess) done[dev].store(1);
+    (void)s;
+    return e;
+}
+
 cudaError_t gauss_levels(const float* y, int w, int h, const std::vector<float*>& lv, cudaStream_t s) {
+    cudaError_t e0 = set_burt(s);
+    if (e0 != cudaSuccess) return e0;
     std::vector<std::pair<int, int>> dims;
     gauss_dims(w, h, dims);
     const float* src = y;
@@ -831,32 +859,47 @@ __global__ void __launch_bounds__(NM_THREADS) nm_search_kernel(const NmJob J) {
                 dev_mat_inverse(m, cand[tid]);
             }
             __syncthreads();
-            for (int k = 0; k < nc; k++) {
-                double m[9];
-                for (int q = 0; q < 9; q++) m[q] = cand[k][q];
-                const bool aff = m[6] == 0.0 && m[7] == 0.0 && m[8] == 1.0;
-                double sd = 0.0, sd2 = 0.0, cnt = 0.0;
+            // the batch's candidates three at a time in one pass over this block's pixels: the
+            // reference value and the pixel's coordinates are shared, the three chains interleave
+            for (int k0 = 0; k0 < nc; k0 += 3) {
+                const int kn = min(3, nc - k0);
+                double sd[3] = {0.0, 0.0, 0.0}, sd2[3] = {0.0, 0.0, 0.0};
+                int cnt[3] = {0, 0, 0};
+                bool aff[3];
+#pragma unroll
+                for (int c = 0; c < 3; c++) {
+                    const double* m = cand[k0 + min(c, kn - 1)];
+                    aff[c] = m[6] == 0.0 && m[7] == 0.0 && m[8] == 1.0;
+                }
                 int x = x0s, y = y0s;
                 for (unsigned i = i0; i < npx; i += stride) {
-                    double sx, sy;
-                    src_point(m, aff, (double)x, (double)y, sx, sy);
-                    if (sx >= 0.0 && sx <= xmax && sy >= 0.0 && sy <= ymax) {
-                        const double fx = floor(sx), fy = floor(sy);
-                        const int xa = (int)fx, ya = (int)fy;
-                        float wx[4], wy[4];
-                        spline4f((float)__dsub_rn(sx, fx), wx);
-                        spline4f((float)__dsub_rn(sy, fy), wy);
-                        float acc = 0.f;
-                        for (int j = 0; j < 4; j++) {
-                            const float* row = lv.tg + (size_t)min(max(ya + j - 1, 0), lv.h - 1) * lv.w;
-                            float r = 0.f;
-                            for (int u = 0; u < 4; u++) r = __fadd_rn(r, __fmul_rn(wx[u], row[min(max(xa + u - 1, 0), lv.w - 1)]));
-                            acc = __fadd_rn(acc, __fmul_rn(wy[j], r));
+                    const float rv = lv.rf[i];
+#pragma unroll
+                    for (int c = 0; c < 3; c++) {
+                        if (c < kn) {
+                            double sx, sy;
+                            src_point(cand[k0 + c], aff[c], (double)x, (double)y, sx, sy);
+                            if (sx >= 0.0 && sx <= xmax && sy >= 0.0 && sy <= ymax) {
+                                const double fx = floor(sx), fy = floor(sy);
+                                const int xa = (int)fx, ya = (int)fy;
+                                float wx[4], wy[4];
+                                spline4f((float)__dsub_rn(sx, fx), wx);
+                                spline4f((float)__dsub_rn(sy, fy), wy);
+                                float acc = 0.f;
+#pragma unroll
+                                for (int j = 0; j < 4; j++) {
+                                    const float* row = lv.tg + (size_t)min(max(ya + j - 1, 0), lv.h - 1) * lv.w;
+                                    float r = 0.f;
+#pragma unroll
+                                    for (int u = 0; u < 4; u++) r = __fadd_rn(r, __fmul_rn(wx[u], row[min(max(xa + u - 1, 0), lv.w - 1)]));
+                                    acc = __fadd_rn(acc, __fmul_rn(wy[j], r));
+                                }
+                                const double d = (double)__fsub_rn(rv, acc);
+                                sd[c] += d;
+                                sd2[c] += d * d;
+                                cnt[c]++;
+                            }
                         }
-                        const double d = (double)__fsub_rn(lv.rf[i], acc);
-                        sd += d;
-                        sd2 += d * d;
-                        cnt += 1.0;
                     }
                     x += (int)sdx;
                     y += (int)sdy;
@@ -865,13 +908,15 @@ __global__ void __launch_bounds__(NM_THREADS) nm_search_kernel(const NmJob J) {
                         y++;
                     }
                 }
-                sd = warp_sum(sd);
-                sd2 = warp_sum(sd2);
-                cnt = warp_sum(cnt);
-                if (lane == 0) {
-                    wred[k][0][wid] = sd;
-                    wred[k][1][wid] = sd2;
-                    wred[k][2][wid] = cnt;
+#pragma unroll
+                for (int c = 0; c < 3; c++) {
+                    if (c >= kn) break;
+                    const double a = warp_sum(sd[c]), b = warp_sum(sd2[c]), n1 = warp_sum((double)cnt[c]);
+                    if (lane == 0) {
+                        wred[k0 + c][0][wid] = a;
+                        wred[k0 + c][1][wid] = b;
+                        wred[k0 + c][2][wid] = n1;
+                    }
                 }
             }
             __syncthreads();
@@ -974,7 +1019,9 @@ static cudaError_t nm_job(AlignCtx& C, const float* rf, const std::vector<float*
         cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, nm_search_kernel, NM_THREADS, 0);
         if (e != cudaSuccess) return e;
         if (per < 1) return cudaErrorCooperativeLaunchTooLarge;
-        g_nm_blocks = std::min(std::min(per, 2) * sms, NM_MAX_BLOCKS);
+        int want = 2;  // CTAs per SM: more warps hide the gathers, more CTAs make every barrier dearer
+        if (const char* v = getenv("LSB_NM_CTAS_PER_SM")) want = std::max(1, atoi(v));
+        g_nm_blocks = std::min(std::min(per, want) * sms, NM_MAX_BLOCKS);
     }
     J.part = C.nm_part;
     J.bar = (unsigned*)C.nm_ctl + 2;

@@ -9,7 +9,7 @@
 namespace lsb {
 
 constexpr int MAX_CAND = 9;
-constexpr int NM_MAX_BLOCKS = 148 * 2;
+constexpr int NM_MAX_BLOCKS = 148 * 4;
 
 // The inverse homographies of a batch of candidate transforms (row-major 3x3).
 struct CostBatch {

@@ -73,6 +73,7 @@ struct lsb_engine {
     cudaStream_t s;
     cudaStream_t cs = nullptr;  // host -> device frame copies, overlapped with the work on s
     cudaEvent_t s_mark = nullptr;  // recorded on s so that cs can wait for the work queued before it
+    cudaStream_t bs = nullptr;  // registration targets (luma + pyramid of the next frame) beside the search on s
     DevPool pool;
     unsigned *hist, *sel;
     float* scal;  // [floor, p90, max, ...]
@@ -136,6 +137,10 @@ struct lsb_stack {
     unsigned long long* evals_dev = nullptr;
     int aligned_upto = 0;        // frames already registered (at push time)
     std::vector<cudaEvent_t> copied;  // per frame: its host -> device copy is done
+    // two target buffers (luma + pyramid), filled on the side stream: frame i+1's while frame i searches
+    float* yt2[2] = {nullptr, nullptr};
+    std::vector<float*> pt2[2];
+    cudaEvent_t tdone[2] = {nullptr, nullptr}, tfree[2] = {nullptr, nullptr};
     WlsSolver* ws = nullptr;  // planes of the depth grid's solve, kept across runs
     lsb_unet* net = nullptr;  // learned warm start of the solves (not owned)
     float* x0 = nullptr;      // its prediction on the depth grid
@@ -145,6 +150,10 @@ struct lsb_stack {
         wls_destroy(ws);
         if (x0) cudaFree(x0);
         for (auto& v : copied) cudaEventDestroy(v);
+        for (int b = 0; b < 2; b++) {
+            if (tdone[b]) cudaEventDestroy(tdone[b]);
+            if (tfree[b]) cudaEventDestroy(tfree[b]);
+        }
     }
 };
 
@@ -223,6 +232,7 @@ char* lsb_engine_create(const lsb_config* cfg, lsb_engine** out) {
     TRY(cudaStreamCreateWithFlags(&e->s, cudaStreamNonBlocking));
     TRY(cudaStreamCreateWithFlags(&e->cs, cudaStreamNonBlocking));
     TRY(cudaEventCreateWithFlags(&e->s_mark, cudaEventDisableTiming));
+    TRY(cudaStreamCreateWithFlags(&e->bs, cudaStreamNonBlocking));
     TRY(e->pool.get(&e->hist, 65536));
     TRY(e->pool.get(&e->sel, 4));
     TRY(e->pool.get(&e->scal, 16));
@@ -251,6 +261,7 @@ void lsb_engine_destroy(lsb_engine* e) {
     e->pool.release();
     if (e->cs) cudaStreamSynchronize(e->cs), cudaStreamDestroy(e->cs);
     if (e->s_mark) cudaEventDestroy(e->s_mark);
+    if (e->bs) cudaStreamSynchronize(e->bs), cudaStreamDestroy(e->bs);
     cudaStreamDestroy(e->s);
     delete e;
 }
@@ -287,13 +298,14 @@ static std::vector<float> focus_taps(uint32_t r_in, uint32_t r_out) {
 static char* stack_alloc(lsb_stack* s) {
     DevPool& P = s->pool;
     const size_t W = s->w, H = s->h, N = s->n;
-    TRY(P.get(&s->frames, N * W * H * 3));
+    // fold inputs carry 64 bytes of tail padding: the async tile copies read whole words
+    TRY(P.get(&s->frames, N * W * H * 3 + 32));
     s->g.assign(s->levels + 1, nullptr);
     s->acc.assign(s->levels, nullptr);
     s->best.assign(s->levels, nullptr);
     for (int l = 1; l <= s->levels; l++) {
         void* p = nullptr;
-        TRY(cudaMalloc(&p, N * 3 * (size_t)s->lw[l] * s->lh[l] * gs_bytes(s)));
+        TRY(cudaMalloc(&p, N * 3 * (size_t)s->lw[l] * s->lh[l] * gs_bytes(s) + 64));
         P.ptrs.push_back(p);
         s->g[l] = p;
     }
@@ -336,7 +348,7 @@ static char* stack_alloc(lsb_stack* s) {
     if (s->ap.enabled && N > 1) {
         {
             void* p = nullptr;
-            TRY(cudaMalloc(&p, N * W * H * (s->storage == STORE_F32 ? 3 * sizeof(float) : 3 * sizeof(uint16_t))));
+            TRY(cudaMalloc(&p, N * W * H * (s->storage == STORE_F32 ? 3 * sizeof(float) : 3 * sizeof(uint16_t)) + 64));
             P.ptrs.push_back(p);
             s->warped = p;
         }
@@ -354,6 +366,18 @@ static char* stack_alloc(lsb_stack* s) {
         TRY(P.get(&s->bx_dev, N));
         TRY(P.get(&s->bpart, N * 64 * 7));
         TRY(P.get(&s->sims_dev, (size_t)N * 8));
+        s->yt2[0] = s->yt;
+        s->pt2[0] = s->pt;
+        TRY(P.get(&s->yt2[1], W * H));
+        for (auto& d : dims) {
+            float* a;
+            TRY(P.get(&a, (size_t)d.first * d.second));
+            s->pt2[1].push_back(a);
+        }
+        for (int b = 0; b < 2; b++) {
+            TRY(cudaEventCreateWithFlags(&s->tdone[b], cudaEventDisableTiming));
+            TRY(cudaEventCreateWithFlags(&s->tfree[b], cudaEventDisableTiming));
+        }
         TRY(P.get(&s->warp_dev, 16));
         TRY(P.get(&s->evals_dev, 1));
     }
@@ -538,14 +562,23 @@ static char* align_frame(lsb_stack* s, int i) {
     } else {
         bool freem[8];
         free_mask(s, freem);
-        TRY(luma_u16(f, W, H, s->yt, e->s));
-        TRY(gauss_levels(s->yt, W, H, s->pt, e->s));
-        TRY(multiscale_align_chain(C, s->yr, s->pr, s->yt, s->pt, W, H, s->sims_dev + 8 * (size_t)(i - 1), freem, (int)s->ap.coarsen,
+        // the target on the side stream, once its buffer's last reader on s is done
+        const int b = i & 1;
+        float* yt = s->yt2[b];
+        const std::vector<float*>& pt = s->pt2[b];
+        TRY(cudaStreamWaitEvent(e->bs, s->tfree[b], 0));
+        TRY(cudaStreamWaitEvent(e->bs, s->copied[i], 0));
+        TRY(luma_u16(f, W, H, yt, e->bs));
+        TRY(gauss_levels(yt, W, H, pt, e->bs));
+        TRY(cudaEventRecord(s->tdone[b], e->bs));
+        TRY(cudaStreamWaitEvent(e->s, s->tdone[b], 0));
+        TRY(multiscale_align_chain(C, s->yr, s->pr, yt, pt, W, H, s->sims_dev + 8 * (size_t)(i - 1), freem, (int)s->ap.coarsen,
                                    s->sims_dev + 8 * (size_t)i, s->warp_dev, s->evals_dev));
         if (i + 1 < n) {
-            TRY(warp_plane_dev(s->yt, W, H, s->warp_dev, (int)s->ap.interp, s->yr, e->s));
+            TRY(warp_plane_dev(yt, W, H, s->warp_dev, (int)s->ap.interp, s->yr, e->s));
             TRY(gauss_levels(s->yr, W, H, s->pr, e->s));
         }
+        TRY(cudaEventRecord(s->tfree[b], e->s));
     }
     s->aligned_upto = i + 1;
     return nullptr;
@@ -553,6 +586,9 @@ static char* align_frame(lsb_stack* s, int i) {
 
 static char* run_align(lsb_stack* s) {
     if (chained(s)) {
+        // the side stream reads frames the work stream may have written (a device-side fill)
+        TRY(cudaEventRecord(s->e->s_mark, s->e->s));
+        TRY(cudaStreamWaitEvent(s->e->bs, s->e->s_mark, 0));
         for (int i = s->aligned_upto; i < (int)s->count; i++)
             if (char* er = align_frame(s, i)) return er;
         size_t evals = 0;

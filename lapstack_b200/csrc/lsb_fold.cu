@@ -47,7 +47,7 @@ static cudaError_t with_smem(K k, size_t smem) {
 // One level: REDUCE every frame (and take the focus slices at level 0), then select.
 template <int SRC, class GS, int R, bool FOCUS, class SS>
 static cudaError_t launch_level(const FoldArgs& a, cudaStream_t s, int grid_limit) {
-    const size_t rsm = (size_t)RED_FLOATS * sizeof(float), ssm = (size_t)SEL_FLOATS * sizeof(float);
+    const size_t rsm = (size_t)RED_FLOATS * sizeof(float), ssm = Staging<SRC, GS, R>::SMEM;
     auto kr = reduce_level_kernel<SRC, GS, FOCUS, SS>;
     auto ks = select_level_kernel<SRC, GS, R>;
     cudaError_t e = with_smem(kr, rsm);
@@ -87,7 +87,11 @@ static cudaError_t pick_src(const FoldArgs& a, int src_kind, int r, bool focus, 
     }
 }
 
-cudaError_t fold_level(const FoldArgs& a, int src_kind, int storage, int radius, bool focus, cudaStream_t s, int grid_limit) {
+cudaError_t fold_level(const FoldArgs& a0, int src_kind, int storage, int radius, bool focus, cudaStream_t s, int grid_limit) {
+    FoldArgs a = a0;  // the select kernel's tiling
+    a.tiles_x = (a.W + TW - 1) / TW;
+    a.tiles_y = (a.H + TH - 1) / TH;
+    a.ntiles = a.tiles_x * a.tiles_y;
     if (a.ntiles <= 0) return cudaSuccess;
     switch (storage) {
         case STORE_UNORM16: return pick_src<unorm16>(a, src_kind, radius, focus, s, grid_limit);

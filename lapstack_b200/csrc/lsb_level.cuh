@@ -20,8 +20,19 @@
 #pragma once
 
 constexpr int NT = 256;
+// resident CTAs per SM the compiler keeps the register budget for
+#ifndef LSB_SEL_MINB
+#define LSB_SEL_MINB 2
+#endif
+#ifndef LSB_RED_MINB
+#define LSB_RED_MINB 1
+#endif
 // select: tile, own pixels per thread, windows
-constexpr int TW = 64, TH = 32, PPT = (TW * TH) / NT;
+#ifndef LSB_TH
+#define LSB_TH 32
+#endif
+constexpr int TW = 64, TH = LSB_TH, PPT = (TW * TH) / NT;
+static_assert(TH % 16 == 0 && PPT % 2 == 0, "thread (tx, ty) owns (tx + 32a, ty + 8b)");
 constexpr int RMAX = 2;
 constexpr int LW_MAX = TW + 2 * RMAX, LH_MAX = TH + 2 * RMAX;
 constexpr int AW_MAX = LW_MAX / 2 + 5, AH_MAX = LH_MAX / 2 + 5;
@@ -175,7 +186,7 @@ __device__ __forceinline__ void reduce_tile(const FoldArgs& a, float* __restrict
 }
 
 template <int SRC, class GS, bool FOCUS, class SS>
-__global__ void __launch_bounds__(NT) reduce_level_kernel(const FoldArgs a) {
+__global__ void __launch_bounds__(NT, LSB_RED_MINB) reduce_level_kernel(const FoldArgs a) {
     extern __shared__ float sm[];
     const int tiles_x = (a.W1 + RW - 1) / RW;
     const int gx0 = (blockIdx.x % tiles_x) * RW, gy0 = (blockIdx.x / tiles_x) * RH;
@@ -191,7 +202,7 @@ struct TileWin {
     int x0, y0, xL0, xL1, yL0, yL1, xA0, xA1, yA0, yA1, lw, lh, aw, ah, ox1, oy1;
 };
 
-template <int SRC, class GS, int R, bool IN>
+template <int SRC, class GS, int R, bool IN, bool STAGED = false>
 __device__ __forceinline__ void select_frame(const FoldArgs& a, float* __restrict__ sm, int k, const TileWin& t,
                                              float (&best)[PPT], float (&acc)[PPT][3], int (&win)[PPT]) {
     const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
@@ -207,7 +218,8 @@ __device__ __forceinline__ void select_frame(const FoldArgs& a, float* __restric
     const int lw = t.lw, lh = t.lh, aw = t.aw, ah = t.ah;
     const float2 sc = make_float2(a.gscale, a.ginv);
 
-    // ---- 1: stage G_l and G_{l+1}
+    // ---- 1: stage G_l and G_{l+1} (STAGED: already in gl / g1 from the async copies)
+    if (!STAGED) {
     for (int r = ty; r < lh; r += 8)
         for (int c = tx; c < lw; c += 32) {
             float v[3];
@@ -226,6 +238,7 @@ __device__ __forceinline__ void select_frame(const FoldArgs& a, float* __restric
             }
     }
     __syncthreads();
+    }
 
     // ---- 2: EXPAND along rows (pyramid.rs:147)
     for (int i = ty; i < ah; i += 8)
@@ -339,8 +352,118 @@ __device__ __forceinline__ void select_frame(const FoldArgs& a, float* __restric
 #undef RY1
 }
 
+// ------------------------------------------------------- async tile staging
+// For interior tiles the next frame's window rows (G_l over the tile +- R, and
+// G_{l+1} over what EXPAND reads) are copied global -> shared with cp.async
+// while the current frame computes, so the loads' latency is off the critical
+// path. Rows are copied as 4-byte words from the word boundary at or before
+// the row's first byte (`mis` bytes of slack in front); every fold input is
+// allocated with 64 bytes of tail padding for the word after a row's end.
+template <int R>
+struct InTile {  // interior-tile window sizes (x0, y0 multiples of TW, TH)
+    static constexpr int LW = TW + 2 * R, LH = TH + 2 * R;
+    static constexpr int AW = ((TW + R - 1) >> 1) + ((R + 1) >> 1) + 3;
+    static constexpr int AH = ((TH + R - 1) >> 1) + ((R + 1) >> 1) + 3;
+};
 template <int SRC, class GS, int R>
-__global__ void __launch_bounds__(NT, 2) select_level_kernel(const FoldArgs a) {
+struct Staging {
+    static constexpr bool INTERLEAVED = SRC == SRC_U16;
+    static constexpr int G0_EB = SRC == SRC_U16 ? 6 : (SRC == SRC_F32 ? 4 : (int)sizeof(GS));  // bytes per px in a row
+    static constexpr int G0_ROWS = INTERLEAVED ? InTile<R>::LH : 3 * InTile<R>::LH;
+    static constexpr int G0_WPR = (InTile<R>::LW * G0_EB + 2 + 3) / 4;  // words per row, with 2 bytes of slack
+    static constexpr int G1_ROWS = 3 * InTile<R>::AH;
+    static constexpr int G1_WPR = (InTile<R>::AW * (int)sizeof(GS) + 2 + 3) / 4;
+    static constexpr int WORDS = G0_ROWS * G0_WPR + G1_ROWS * G1_WPR;  // one stage
+    // two stages beside the compute buffers, if two CTAs still fit an SM
+    static constexpr bool ON = SRC != SRC_F32 && sizeof(GS) == 2 && (2 * WORDS + SEL_FLOATS) * 4 <= 110 * 1024;
+    static constexpr size_t SMEM = (size_t)(SEL_FLOATS + (ON ? 2 * WORDS : 0)) * 4;
+};
+
+__device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(d), "l"(gmem));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
+
+// Issue the copies of frame k's interior window into `raw` (one stage).
+template <int SRC, class GS, int R>
+__device__ __forceinline__ void stage_issue(const FoldArgs& a, int k, const TileWin& t, uint32_t* raw) {
+    using S = Staging<SRC, GS, R>;
+    const int W = a.W, H = a.H, W1 = a.W1, H1 = a.H1;
+    const size_t np = (size_t)W * H, np1 = (size_t)W1 * H1;
+    for (int i = threadIdx.x; i < S::G0_ROWS * S::G0_WPR; i += NT) {
+        const int row = i / S::G0_WPR, wd = i - row * S::G0_WPR;
+        size_t byte;
+        if (SRC == SRC_U16) {
+            byte = (((size_t)k * np + (size_t)(t.yL0 + row) * W + t.xL0) * 3) * 2;
+        } else {
+            const int c = row / InTile<R>::LH, r = row - c * InTile<R>::LH;
+            byte = ((((size_t)k * 3 + c) * H + t.yL0 + r) * W + t.xL0) * sizeof(GS);
+        }
+        const unsigned char* base = SRC == SRC_U16 ? (const unsigned char*)a.src_u16 : (const unsigned char*)a.src_g;
+        cp_async4(raw + i, base + (byte & ~(size_t)3) + 4 * wd);
+    }
+    uint32_t* raw1 = raw + S::G0_ROWS * S::G0_WPR;
+    for (int i = threadIdx.x; i < S::G1_ROWS * S::G1_WPR; i += NT) {
+        const int row = i / S::G1_WPR, wd = i - row * S::G1_WPR;
+        const int c = row / InTile<R>::AH, r = row - c * InTile<R>::AH;
+        const size_t byte = ((((size_t)k * 3 + c) * H1 + t.yA0 + r) * W1 + t.xA0) * sizeof(GS);
+        cp_async4(raw1 + i, (const unsigned char*)a.dst_g + (byte & ~(size_t)3) + 4 * wd);
+    }
+    (void)np1;
+}
+// The staged words of frame k -> the f32 windows gl / g1 select_frame reads
+// (level_px's conversion and gains, Store<GS>::ld for the stored levels).
+template <int SRC, class GS, int R>
+__device__ __forceinline__ void stage_convert(const FoldArgs& a, int k, const TileWin& t, const uint32_t* raw, float* sm) {
+    using S = Staging<SRC, GS, R>;
+    using T = InTile<R>;
+    const int W = a.W, H = a.H, W1 = a.W1, H1 = a.H1;
+    const size_t np = (size_t)W * H;
+    float* gl = sm;
+    float* g1 = gl + 3 * SEL_GL;
+    const float2 sc = make_float2(a.gscale, a.ginv);
+    int gon = 0;
+    float gain[3] = {1.f, 1.f, 1.f};
+    if (SRC == SRC_U16) {
+        gon = a.xf[k].gain_on;
+        for (int c = 0; c < 3; c++) gain[c] = a.xf[k].gain[c];
+    }
+    for (int i = threadIdx.x; i < T::LH * T::LW; i += NT) {
+        const int r = i / T::LW, x = i - r * T::LW;
+        float v[3];
+        if (SRC == SRC_U16) {
+            const size_t byte = (((size_t)k * np + (size_t)(t.yL0 + r) * W + t.xL0) * 3) * 2;
+            const uint16_t* p = (const uint16_t*)((const unsigned char*)(raw + r * S::G0_WPR) + (byte & 3)) + 3 * x;
+            for (int c = 0; c < 3; c++) {
+                v[c] = __fmul_rn((float)p[c], LSB_INV16);
+                if (gon & (1 << c)) v[c] = __fmul_rn(v[c], gain[c]);
+            }
+        } else {
+            for (int c = 0; c < 3; c++) {
+                const size_t byte = ((((size_t)k * 3 + c) * H + t.yL0 + r) * W + t.xL0) * sizeof(GS);
+                const GS* p = (const GS*)((const unsigned char*)(raw + (c * T::LH + r) * S::G0_WPR) + (byte & 3)) + x;
+                v[c] = Store<GS>::ld(p, sc);
+            }
+        }
+        const int o = r * T::LW + x;
+        gl[o] = v[0];
+        gl[SEL_GL + o] = v[1];
+        gl[2 * SEL_GL + o] = v[2];
+    }
+    const uint32_t* raw1 = raw + S::G0_ROWS * S::G0_WPR;
+    for (int i = threadIdx.x; i < 3 * T::AH * T::AW; i += NT) {
+        const int c = i / (T::AH * T::AW), rem = i - c * (T::AH * T::AW), r = rem / T::AW, x = rem - r * T::AW;
+        const size_t byte = ((((size_t)k * 3 + c) * H1 + t.yA0 + r) * W1 + t.xA0) * sizeof(GS);
+        const GS* p = (const GS*)((const unsigned char*)(raw1 + (c * T::AH + r) * S::G1_WPR) + (byte & 3)) + x;
+        g1[c * SEL_G1 + r * T::AW + x] = Store<GS>::ld(p, sc);
+    }
+}
+
+template <int SRC, class GS, int R>
+__global__ void __launch_bounds__(NT, LSB_SEL_MINB) select_level_kernel(const FoldArgs a) {
     extern __shared__ float sm[];
     const int W = a.W, H = a.H, W1 = a.W1, H1 = a.H1;
     const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
@@ -377,9 +500,34 @@ __global__ void __launch_bounds__(NT, 2) select_level_kernel(const FoldArgs a) {
             acc[j][0] = acc[j][1] = acc[j][2] = 0.f;
             win[j] = 0;
         }
-        for (int k = 0; k < a.nframes; k++) {
-            if (interior) select_frame<SRC, GS, R, true>(a, sm, k, t, best, acc, win);
-            else select_frame<SRC, GS, R, false>(a, sm, k, t, best, acc, win);
+        using S = Staging<SRC, GS, R>;
+        if (S::ON && interior) {
+            if (t.lw != InTile<R>::LW || t.lh != InTile<R>::LH || t.aw != InTile<R>::AW || t.ah != InTile<R>::AH) {
+                if (threadIdx.x == 0) atomicOr(a.status, LSB_ERR_SHAPE);
+                return;
+            }
+            uint32_t* raw = (uint32_t*)(sm + SEL_FLOATS);
+            stage_issue<SRC, GS, R>(a, 0, t, raw);
+            cp_async_commit();
+            for (int k = 0; k < a.nframes; k++) {
+                uint32_t* cur = raw + (k & 1) * S::WORDS;
+                if (k + 1 < a.nframes) {
+                    stage_issue<SRC, GS, R>(a, k + 1, t, raw + ((k + 1) & 1) * S::WORDS);
+                    cp_async_commit();
+                    cp_async_wait<1>();
+                } else {
+                    cp_async_wait<0>();
+                }
+                __syncthreads();
+                stage_convert<SRC, GS, R>(a, k, t, cur, sm);
+                __syncthreads();
+                select_frame<SRC, GS, R, true, true>(a, sm, k, t, best, acc, win);
+            }
+        } else {
+            for (int k = 0; k < a.nframes; k++) {
+                if (interior) select_frame<SRC, GS, R, true>(a, sm, k, t, best, acc, win);
+                else select_frame<SRC, GS, R, false>(a, sm, k, t, best, acc, win);
+            }
         }
 #pragma unroll
         for (int j = 0; j < PPT; j++) {
