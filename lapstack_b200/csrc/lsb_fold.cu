@@ -36,7 +36,16 @@ size_t fold_smem_bytes(int, bool) { return (size_t)SEL_FLOATS * sizeof(float); }
 
 cudaError_t set_focus_taps(const float* taps3, int ntaps, cudaStream_t s) {
     if (ntaps > 64) return cudaErrorInvalidValue;
-    return cudaMemcpyToSymbolAsync(c_taps, taps3, sizeof(float) * 3 * ntaps, 0, cudaMemcpyHostToDevice, s);
+    int off[64];
+    float wgt[64];
+    for (int q = 0; q < ntaps; q++) {
+        off[q] = (int)taps3[3 * q] * RGW + (int)taps3[3 * q + 1];
+        wgt[q] = taps3[3 * q + 2];
+    }
+    cudaError_t e = cudaMemcpyToSymbolAsync(c_taps, taps3, sizeof(float) * 3 * ntaps, 0, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaMemcpyToSymbolAsync(c_tapo, off, sizeof(int) * ntaps, 0, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaMemcpyToSymbolAsync(c_tapw, wgt, sizeof(float) * ntaps, 0, cudaMemcpyHostToDevice, s);
+    return e;
 }
 
 template <class K>

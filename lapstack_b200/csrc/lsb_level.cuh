@@ -49,6 +49,9 @@ constexpr int RED_FLOATS = 3 * RGW * RGH + RGW * RGH + 3 * RGH * RW;
 // conv_sparse taps (depth.rs:417) in the per-pixel accumulation order: rows
 // grouped by dy in order of first appearance, within a row in list order.
 __constant__ float c_taps[3 * 64];
+// the same taps for an interior window (rows RGW apart): offsets dy * RGW + dx and weights
+__constant__ int c_tapo[64];
+__constant__ float c_tapw[64];
 
 // binomial(R) of fuse.rs:139: C(2R, t) / 4^R, exact in f32.
 template <int R>
@@ -146,9 +149,14 @@ __device__ __forceinline__ void reduce_tile(const FoldArgs& a, float* __restrict
                         float m;
                         if (a.focus_kind == 0) {
                             float s = 0.f;
-                            for (int q = 0; q < a.ntaps; q++) {
-                                const int yy = RY(y + (int)c_taps[3 * q]) - yw0, xx = RX(x + (int)c_taps[3 * q + 1]) - xw0;
-                                s = __fadd_rn(s, __fmul_rn(c_taps[3 * q + 2], yl[yy * ww + xx]));
+                            if (IN) {
+                                const float* yc = yl + (y - yw0) * RGW + (x - xw0);
+                                for (int q = 0; q < a.ntaps; q++) s = __fadd_rn(s, __fmul_rn(c_tapw[q], yc[c_tapo[q]]));
+                            } else {
+                                for (int q = 0; q < a.ntaps; q++) {
+                                    const int yy = RY(y + (int)c_taps[3 * q]) - yw0, xx = RX(x + (int)c_taps[3 * q + 1]) - xw0;
+                                    s = __fadd_rn(s, __fmul_rn(c_taps[3 * q + 2], yl[yy * ww + xx]));
+                                }
                             }
                             m = fabsf(s);
                         } else {
