@@ -313,7 +313,86 @@ cudaError_t warp_plane(const float* src, int w, int h, const WarpXform& xf, floa
     return cudaGetLastError();
 }
 
+// The Spline4x4 form over 64x16 tiles: the tile's source footprint (its
+// corners' images, the taps' reach and a pixel of margin, clamped like the
+// taps) is staged in shared memory once; the taps, weights and sums are
+// warp_plane_px's. Identity warps copy; tiles whose footprint does not fit,
+// and projective warps, take the per-pixel path.
+constexpr int PT_W = 64, PT_H = 16, PB_W = PT_W + 16, PB_H = PT_H + 16;
+__global__ void __launch_bounds__(256) warp_plane_tile_kernel(const float* __restrict__ src, int w, int h, const double* __restrict__ wd,
+                                                              float* __restrict__ out) {
+    __shared__ float box[PB_H][PB_W];
+    const int x0 = blockIdx.x * PT_W, y0 = blockIdx.y * PT_H, tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+    const bool ident = wd[10] != 0.0, affine = wd[9] != 0.0;
+    double m[9];
+    for (int q = 0; q < 9; q++) m[q] = wd[q];
+    int bx0 = 0, by0 = 0, bw = 0, bh = 0;
+    bool fits = false;
+    if (!ident && affine) {
+        double mnx = 1e300, mxx = -1e300, mny = 1e300, mxy = -1e300;
+        const int cx[2] = {x0, min(x0 + PT_W - 1, w - 1)}, cy[2] = {y0, min(y0 + PT_H - 1, h - 1)};
+        for (int a = 0; a < 2; a++)
+            for (int b = 0; b < 2; b++) {
+                double sx, sy;
+                src_point(m, true, (double)cx[a], (double)cy[b], sx, sy);
+                mnx = fmin(mnx, sx);
+                mxx = fmax(mxx, sx);
+                mny = fmin(mny, sy);
+                mxy = fmax(mxy, sy);
+            }
+        if (mnx > -1e9 && mxx < 1e9 && mny > -1e9 && mxy < 1e9) {
+            bx0 = (int)floor(mnx) - 2;
+            by0 = (int)floor(mny) - 2;
+            bw = (int)floor(mxx) + 3 - bx0 + 1;
+            bh = (int)floor(mxy) + 3 - by0 + 1;
+            fits = bw <= PB_W && bh <= PB_H;
+        }
+    }
+    if (fits) {
+        for (int i = threadIdx.x; i < bw * bh; i += 256) {
+            const int r = i / bw, c = i - r * bw;
+            box[r][c] = src[(size_t)min(max(by0 + r, 0), h - 1) * w + min(max(bx0 + c, 0), w - 1)];
+        }
+        __syncthreads();
+    }
+#pragma unroll 1
+    for (int q = 0; q < 4; q++) {
+        const int x = x0 + tx + 32 * (q & 1), y = y0 + ty + 8 * (q >> 1);
+        if (x >= w || y >= h) continue;
+        const size_t k = (size_t)y * w + x;
+        if (ident) {
+            out[k] = src[k];
+            continue;
+        }
+        if (!fits) {
+            out[k] = warp_plane_px(src, w, h, m, affine, 3, x, y);
+            continue;
+        }
+        double sx, sy;
+        src_point(m, true, (double)x, (double)y, sx, sy);
+        const double fx = floor(sx), fy = floor(sy);
+        const int ix = (int)fx - 1 - bx0, iy = (int)fy - 1 - by0;
+        float wx[4], wy[4];
+        spline4_d(__dsub_rn(sx, fx), wx);
+        spline4_d(__dsub_rn(sy, fy), wy);
+        float acc = 0.f;
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            float r = 0.f;
+#pragma unroll
+            for (int i = 0; i < 4; i++) r = __fadd_rn(r, __fmul_rn(wx[i], box[iy + j][ix + i]));
+            acc = __fadd_rn(acc, __fmul_rn(wy[j], r));
+        }
+        out[k] = acc;
+    }
+}
+
 cudaError_t warp_plane_dev(const float* src, int w, int h, const double* warp_dev, int interp, float* out, cudaStream_t s) {
+    if (interp == 3) {
+        dim3 g((w + PT_W - 1) / PT_W, (h + PT_H - 1) / PT_H);
+        lsb_launched(), warp_plane_tile_kernel<<<g, 256, 0, s>>>(src, w, h, warp_dev, out);
+        return cudaGetLastError();
+    }
     dim3 b(32, 8), g((w + 31) / 32, (h + 7) / 8);
     lsb_launched(), warp_plane_dev_kernel<<<g, b, 0, s>>>(src, w, h, warp_dev, interp, out);
     return cudaGetLastError();

@@ -111,6 +111,12 @@ cudaError_t fold_level(const FoldArgs& a0, int src_kind, int storage, int radius
 
 cudaError_t warp_frames(const uint16_t* frames, const FrameXform* xf, int interp, int w, int h, int n, bool u16_out, void* out,
                         cudaStream_t s) {
+    if (interp == 3) {  // Spline4x4: the tiled form
+        dim3 g((w + WT_W - 1) / WT_W, (h + WT_H - 1) / WT_H, n);
+        if (u16_out) lsb_launched(), warp_tile_kernel<true><<<g, NT, 0, s>>>(frames, xf, w, h, out);
+        else lsb_launched(), warp_tile_kernel<false><<<g, NT, 0, s>>>(frames, xf, w, h, out);
+        return cudaGetLastError();
+    }
     dim3 g((w + 31) / 32, (h + 7) / 8, n);
     if (u16_out) lsb_launched(), warp_frames_kernel<true><<<g, NT, 0, s>>>(frames, xf, interp, w, h, out);
     else lsb_launched(), warp_frames_kernel<false><<<g, NT, 0, s>>>(frames, xf, interp, w, h, out);

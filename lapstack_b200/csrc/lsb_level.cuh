@@ -576,3 +576,119 @@ __global__ void __launch_bounds__(NT) warp_frames_kernel(const uint16_t* __restr
         p[2 * np] = v[2];
     }
 }
+
+// The same warp for the Spline4x4 kernel (align.rs:416, the default) over
+// 64x16 output tiles: the tile's source footprint (the images of its corners,
+// the taps' reach and a pixel of margin, clamped to the frame like the taps) is converted
+// to f32 once into shared memory, so each source sample is read and scaled
+// once instead of by every one of the 16 output pixels whose taps reach it.
+// The taps, weights and sums are those of load_px_core, in its order; a tile
+// whose footprint does not fit (a large rotation or magnification) takes the
+// direct path.
+constexpr int WT_W = 64, WT_H = 16, WB_W = WT_W + 16, WB_H = WT_H + 16;
+template <bool U16OUT>
+__global__ void __launch_bounds__(NT) warp_tile_kernel(const uint16_t* __restrict__ frames, const FrameXform* __restrict__ xf, int W,
+                                                       int H, void* __restrict__ out) {
+    __shared__ float4 box[WB_H][WB_W];
+    const int k = blockIdx.z, x0 = blockIdx.x * WT_W, y0 = blockIdx.y * WT_H;
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+    const size_t np = (size_t)W * H;
+    const uint16_t* f = frames + (size_t)k * np * 3;
+    const FrameXform X = xf[k];
+    int bx0 = 0, by0 = 0, bw = 0, bh = 0;
+    bool fits = false;
+    if (X.warp) {
+        double mnx = 1e300, mxx = -1e300, mny = 1e300, mxy = -1e300;
+        const int cx[2] = {x0, min(x0 + WT_W - 1, W - 1)}, cy[2] = {y0, min(y0 + WT_H - 1, H - 1)};
+        for (int a = 0; a < 2; a++)
+            for (int b = 0; b < 2; b++) {
+                double sx, sy;
+                const double* m = X.inv;
+                const double xd = (double)cx[a], yd = (double)cy[b];
+                if (X.affine) {
+                    sx = __dadd_rn(__dadd_rn(__dmul_rn(m[1], yd), m[2]), __dmul_rn(m[0], xd));
+                    sy = __dadd_rn(__dadd_rn(__dmul_rn(m[4], yd), m[5]), __dmul_rn(m[3], xd));
+                } else {
+                    const double d = __dadd_rn(__dadd_rn(__dmul_rn(m[6], xd), __dmul_rn(m[7], yd)), m[8]);
+                    sx = __ddiv_rn(__dadd_rn(__dadd_rn(__dmul_rn(m[0], xd), __dmul_rn(m[1], yd)), m[2]), d);
+                    sy = __ddiv_rn(__dadd_rn(__dadd_rn(__dmul_rn(m[3], xd), __dmul_rn(m[4], yd)), m[5]), d);
+                }
+                mnx = fmin(mnx, sx);
+                mxx = fmax(mxx, sx);
+                mny = fmin(mny, sy);
+                mxy = fmax(mxy, sy);
+            }
+        // only affine footprints are the corners' hull for sure; projective tiles go direct
+        if (X.affine && mnx > -1e9 && mxx < 1e9 && mny > -1e9 && mxy < 1e9) {
+            // one pixel of margin each side: an inner pixel's rounded source point may pass a corner's by an ulp
+            bx0 = (int)floor(mnx) - 2;
+            by0 = (int)floor(mny) - 2;
+            bw = (int)floor(mxx) + 3 - bx0 + 1;
+            bh = (int)floor(mxy) + 3 - by0 + 1;
+            fits = bw <= WB_W && bh <= WB_H;
+        }
+    }
+    if (fits) {
+        for (int i = threadIdx.x; i < bw * bh; i += NT) {
+            const int r = i / bw, c = i - r * bw;
+            const int yy = min(max(by0 + r, 0), H - 1), xx = min(max(bx0 + c, 0), W - 1);
+            const uint16_t* p = f + ((size_t)yy * W + xx) * 3;
+            box[r][c] = make_float4(__fmul_rn((float)p[0], LSB_INV16), __fmul_rn((float)p[1], LSB_INV16),
+                                    __fmul_rn((float)p[2], LSB_INV16), 0.f);
+        }
+        __syncthreads();
+    }
+#pragma unroll 1
+    for (int q = 0; q < 4; q++) {
+        const int x = x0 + tx + 32 * (q & 1), y = y0 + ty + 8 * (q >> 1);
+        if (x >= W || y >= H) continue;
+        float v[3];
+        if (fits) {
+            const double* m = X.inv;
+            const double xd = (double)x, yd = (double)y;
+            const double sx = __dadd_rn(__dadd_rn(__dmul_rn(m[1], yd), m[2]), __dmul_rn(m[0], xd));
+            const double sy = __dadd_rn(__dadd_rn(__dmul_rn(m[4], yd), m[5]), __dmul_rn(m[3], xd));
+            if (sx >= 0.0 && sx <= (double)(W - 1) && sy >= 0.0 && sy <= (double)(H - 1)) {
+                const double fx = floor(sx), fy = floor(sy);
+                const int ix = (int)fx - 1 - bx0, iy = (int)fy - 1 - by0;
+                float wx[4], wy[4];
+                spline4_d(__dsub_rn(sx, fx), wx);
+                spline4_d(__dsub_rn(sy, fy), wy);
+                float a0 = 0.f, a1 = 0.f, a2 = 0.f;
+#pragma unroll
+                for (int j = 0; j < 4; j++) {
+                    float r0 = 0.f, r1 = 0.f, r2 = 0.f;
+#pragma unroll
+                    for (int i = 0; i < 4; i++) {
+                        const float4 s4 = box[iy + j][ix + i];
+                        r0 = __fadd_rn(r0, __fmul_rn(wx[i], s4.x));
+                        r1 = __fadd_rn(r1, __fmul_rn(wx[i], s4.y));
+                        r2 = __fadd_rn(r2, __fmul_rn(wx[i], s4.z));
+                    }
+                    a0 = __fadd_rn(a0, __fmul_rn(wy[j], r0));
+                    a1 = __fadd_rn(a1, __fmul_rn(wy[j], r1));
+                    a2 = __fadd_rn(a2, __fmul_rn(wy[j], r2));
+                }
+                v[0] = a0;
+                v[1] = a1;
+                v[2] = a2;
+            } else {
+                const uint16_t* p = f + ((size_t)y * W + x) * 3;
+                for (int c = 0; c < 3; c++) v[c] = __fmul_rn((float)p[c], LSB_INV16);
+            }
+        } else {
+            load_px_core(f, X.inv, X.warp, X.affine, 3, W, H, x, y, v);
+        }
+        const size_t o = (size_t)y * W + x;
+        if (U16OUT) {
+            uint16_t* p = (uint16_t*)out + ((size_t)k * np + o) * 3;
+            for (int c = 0; c < 3; c++) p[c] = (uint16_t)fminf(fmaxf(__fadd_rn(__fmul_rn(v[c], 65535.f), 0.5f), 0.f), 65535.f);
+        } else {
+            float* p = (float*)out + (size_t)k * 3 * np + o;
+            p[0] = v[0];
+            p[np] = v[1];
+            p[2 * np] = v[2];
+        }
+    }
+}
+
