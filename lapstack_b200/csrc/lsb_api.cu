@@ -796,6 +796,7 @@ static char* run_pipeline(lsb_stack* s) {
             a.focus_kind = (int)s->dp.focus;
             a.sml_step = (int)s->dp.sml_step;
             a.ntaps = (int)focus_taps(s->dp.r_in, s->dp.r_out).size() / 3;
+            a.rdf13 = s->dp.focus == 0 && s->dp.r_in == 1 && s->dp.r_out == 3;
         }
         a.gscale = gscale;
         a.ginv = ginv;

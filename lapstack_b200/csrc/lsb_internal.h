@@ -46,6 +46,7 @@ struct FoldArgs {
     int focus_kind;  // 0 RDF, 1 SML
     int sml_step;
     int ntaps;
+    int rdf13;  // the taps are the default ring difference filter (r_in 1, r_out 3)
     int* status;  // device error word
     float gscale, ginv;  // the 16-bit fixed-point storage's scale and its inverse
     // halo control (fuse.rs:112-136, 453-475): 1 at the guide level (select, and write each frame's

@@ -53,6 +53,23 @@ __constant__ float c_taps[3 * 64];
 __constant__ int c_tapo[64];
 __constant__ float c_tapw[64];
 
+// The default ring difference filter (r_in 1, r_out 3: a 5-tap disk at +1/5,
+// a 24-tap ring at -1/24) in the order depth.rs:417 `conv_sparse` sums it
+// (rows in order of first appearance, each row's taps in list order), with
+// the offsets and weights as immediates. RDF_W* are the host's 1/|disk| and
+// -1/|ring| in f32.
+constexpr float RDF_WD = 1.0f / 5.0f, RDF_WR = -1.0f / 24.0f;
+__device__ __forceinline__ float rdf13(const float* __restrict__ yc) {
+    constexpr int T[29][3] = {{-1, 0, 0},  {-1, -2, 1}, {-1, -1, 1}, {-1, 1, 1}, {-1, 2, 1}, {0, -1, 0}, {0, 0, 0},  {0, 1, 0},
+                              {0, -3, 1},  {0, -2, 1},  {0, 2, 1},   {0, 3, 1},  {1, 0, 0},  {1, -2, 1}, {1, -1, 1}, {1, 1, 1},
+                              {1, 2, 1},   {-3, 0, 1},  {-2, -2, 1}, {-2, -1, 1}, {-2, 0, 1}, {-2, 1, 1}, {-2, 2, 1}, {2, -2, 1},
+                              {2, -1, 1},  {2, 0, 1},   {2, 1, 1},   {2, 2, 1},  {3, 0, 1}};
+    float s = 0.f;
+#pragma unroll
+    for (int q = 0; q < 29; q++) s = __fadd_rn(s, __fmul_rn(T[q][2] ? RDF_WR : RDF_WD, yc[T[q][0] * RGW + T[q][1]]));
+    return s;
+}
+
 // binomial(R) of fuse.rs:139: C(2R, t) / 4^R, exact in f32.
 template <int R>
 __device__ __forceinline__ float binw(int t) {
@@ -149,7 +166,9 @@ __device__ __forceinline__ void reduce_tile(const FoldArgs& a, float* __restrict
                         float m;
                         if (a.focus_kind == 0) {
                             float s = 0.f;
-                            if (IN) {
+                            if (IN && a.rdf13) {
+                                s = rdf13(yl + (y - yw0) * RGW + (x - xw0));
+                            } else if (IN) {
                                 const float* yc = yl + (y - yw0) * RGW + (x - xw0);
                                 for (int q = 0; q < a.ntaps; q++) s = __fadd_rn(s, __fmul_rn(c_tapw[q], yc[c_tapo[q]]));
                             } else {
