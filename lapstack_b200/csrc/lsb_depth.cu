@@ -135,12 +135,16 @@ __device__ __forceinline__ void peak_push(PeakState& p, float v, int m) {
     p.prev = v;
 }
 
-template <int TWD, int THD, class SS>
+// RT: the aggregation radius as a compile-time constant (0: a.r at run time).
+// Tiles whose windows stay inside the grid take fixed, unrolled 2R+1-tap
+// windows; border tiles clip them as BoxFilter does.
+template <int TWD, int THD, class SS, int RT>
 __global__ void __launch_bounds__(256, 2) aggregate_kernel(const AggArgs a) {
     constexpr int CPT = TWD * THD / 256;
     extern __shared__ float sm[];
-    const int R = a.r, w = a.dw, h = a.dh, tid = threadIdx.x;
+    const int R = RT > 0 ? RT : a.r, w = a.dw, h = a.dh, tid = threadIdx.x;
     const int PW = TWD + 4 * R, PH = THD + 4 * R, QW = TWD + 2 * R, QH = THD + 2 * R;
+    constexpr int NW = 2 * RT + 1;  // window taps when RT > 0
     float* P = sm;                 // [PH][PW] slice over tile +- 2R
     float* I = P + PW * PH;        // [PH][PW] guide
     float* MI = I + PW * PH;       // [QH][QW] mean_i
@@ -152,6 +156,8 @@ __global__ void __launch_bounds__(256, 2) aggregate_kernel(const AggArgs a) {
     for (int tile = blockIdx.x; tile < a.ntiles; tile += gridDim.x) {
         const int x0 = (tile % a.tiles_x) * TWD, y0 = (tile / a.tiles_x) * THD;
         const int px0 = x0 - 2 * R, py0 = y0 - 2 * R, qx0 = x0 - R, qy0 = y0 - R;
+        const bool inner = RT > 0 && px0 >= 0 && py0 >= 0 && px0 + PW <= w && py0 + PH <= h;
+        const float ic_in = box_inv_count(R, R, 4 * R + 1, 4 * R + 1, R);  // the interior's 1 / (2R+1)^2
         for (int i = tid; i < PW * PH; i += 256) {
             const int x = px0 + i % PW, y = py0 + i / PW;
             I[i] = (x >= 0 && x < w && y >= 0 && y < h) ? a.guide[(size_t)y * w + x] : 0.f;
@@ -168,20 +174,34 @@ __global__ void __launch_bounds__(256, 2) aggregate_kernel(const AggArgs a) {
         for (int m = 0; m < a.n; m++) {
             const SS* sl = (const SS*)a.slices + (size_t)m * w * h;
             __syncthreads();
-            for (int i = tid; i < PW * PH; i += 256) {
-                const int x = px0 + i % PW, y = py0 + i / PW;
-                P[i] = (x >= 0 && x < w && y >= 0 && y < h) ? lsb_ld<SS>(sl + (size_t)y * w + x) : 0.f;
+            if (inner) {
+                for (int i = tid; i < PW * PH; i += 256) P[i] = lsb_ld<SS>(sl + (size_t)(py0 + i / PW) * w + px0 + i % PW);
+            } else {
+                for (int i = tid; i < PW * PH; i += 256) {
+                    const int x = px0 + i % PW, y = py0 + i / PW;
+                    P[i] = (x >= 0 && x < w && y >= 0 && y < h) ? lsb_ld<SS>(sl + (size_t)y * w + x) : 0.f;
+                }
             }
             __syncthreads();
             // horizontal sums of p and I*p over rows of tile +- 2R, columns of tile +- R
             for (int i = tid; i < PH * QW; i += 256) {
                 const int r = i / QW, c = i % QW, x = qx0 + c;
                 double sp = 0.0, sq = 0.0;
-                const int lo = max(x - R, 0) - px0, hi = min(x + R, w - 1) - px0;
-                for (int t = lo; t <= hi; t++) {
-                    const float pv = P[r * PW + t];
-                    sp += (double)pv;
-                    sq += (double)__fmul_rn(I[r * PW + t], pv);
+                if (inner) {
+                    const float* pr = P + r * PW + c;
+                    const float* ir = I + r * PW + c;
+#pragma unroll
+                    for (int t = 0; t < NW; t++) {
+                        sp += (double)pr[t];
+                        sq += (double)__fmul_rn(ir[t], pr[t]);
+                    }
+                } else {
+                    const int lo = max(x - R, 0) - px0, hi = min(x + R, w - 1) - px0;
+                    for (int t = lo; t <= hi; t++) {
+                        const float pv = P[r * PW + t];
+                        sp += (double)pv;
+                        sq += (double)__fmul_rn(I[r * PW + t], pv);
+                    }
                 }
                 HP[i] = (float)sp;
                 HQ[i] = (float)sq;
@@ -190,18 +210,28 @@ __global__ void __launch_bounds__(256, 2) aggregate_kernel(const AggArgs a) {
             // vertical: mean_p, corr_Ip -> a, b over tile +- R
             for (int i = tid; i < QW * QH; i += 256) {
                 const int r = i / QW, c = i % QW, x = qx0 + c, y = qy0 + r;
-                if (x < 0 || x >= w || y < 0 || y >= h) {
+                if (!inner && (x < 0 || x >= w || y < 0 || y >= h)) {
                     A[i] = 0.f;
                     B[i] = 0.f;
                     continue;
                 }
                 double sp = 0.0, sq = 0.0;
-                const int lo = max(y - R, 0) - py0, hi = min(y + R, h - 1) - py0;
-                for (int t = lo; t <= hi; t++) {
-                    sp += (double)HP[t * QW + c];
-                    sq += (double)HQ[t * QW + c];
+                float ic;
+                if (inner) {
+#pragma unroll
+                    for (int t = 0; t < NW; t++) {
+                        sp += (double)HP[(r + t) * QW + c];
+                        sq += (double)HQ[(r + t) * QW + c];
+                    }
+                    ic = ic_in;
+                } else {
+                    const int lo = max(y - R, 0) - py0, hi = min(y + R, h - 1) - py0;
+                    for (int t = lo; t <= hi; t++) {
+                        sp += (double)HP[t * QW + c];
+                        sq += (double)HQ[t * QW + c];
+                    }
+                    ic = box_inv_count(x, y, w, h, R);
                 }
-                const float ic = box_inv_count(x, y, w, h, R);
                 const float mp = __fmul_rn((float)sp, ic), corr = __fmul_rn((float)sq, ic);
                 const float av = __fdiv_rn(__fsub_rn(corr, __fmul_rn(MI[i], mp)), __fadd_rn(VI[i], a.eps));
                 A[i] = av;
@@ -211,12 +241,20 @@ __global__ void __launch_bounds__(256, 2) aggregate_kernel(const AggArgs a) {
             // horizontal sums of a and b over rows of tile +- R, the tile's columns
             for (int i = tid; i < QH * TWD; i += 256) {
                 const int r = i / TWD, c = i % TWD, x = x0 + c;
-                if (x >= w) continue;
+                if (!inner && x >= w) continue;
                 double sa = 0.0, sb = 0.0;
-                const int lo = max(x - R, 0) - qx0, hi = min(x + R, w - 1) - qx0;
-                for (int t = lo; t <= hi; t++) {
-                    sa += (double)A[r * QW + t];
-                    sb += (double)B[r * QW + t];
+                if (inner) {
+#pragma unroll
+                    for (int t = 0; t < NW; t++) {
+                        sa += (double)A[r * QW + c + t];
+                        sb += (double)B[r * QW + c + t];
+                    }
+                } else {
+                    const int lo = max(x - R, 0) - qx0, hi = min(x + R, w - 1) - qx0;
+                    for (int t = lo; t <= hi; t++) {
+                        sa += (double)A[r * QW + t];
+                        sb += (double)B[r * QW + t];
+                    }
                 }
                 HP[i] = (float)sa;
                 HQ[i] = (float)sb;
@@ -225,14 +263,24 @@ __global__ void __launch_bounds__(256, 2) aggregate_kernel(const AggArgs a) {
 #pragma unroll
             for (int j = 0; j < CPT; j++) {
                 const int p = tid + 256 * j, c = p % TWD, r = p / TWD, x = x0 + c, y = y0 + r;
-                if (x >= w || y >= h) continue;
+                if (!inner && (x >= w || y >= h)) continue;
                 double sa = 0.0, sb = 0.0;
-                const int lo = max(y - R, 0) - qy0, hi = min(y + R, h - 1) - qy0;
-                for (int t = lo; t <= hi; t++) {
-                    sa += (double)HP[t * TWD + c];
-                    sb += (double)HQ[t * TWD + c];
+                float ic;
+                if (inner) {
+#pragma unroll
+                    for (int t = 0; t < NW; t++) {
+                        sa += (double)HP[(r + t) * TWD + c];
+                        sb += (double)HQ[(r + t) * TWD + c];
+                    }
+                    ic = ic_in;
+                } else {
+                    const int lo = max(y - R, 0) - qy0, hi = min(y + R, h - 1) - qy0;
+                    for (int t = lo; t <= hi; t++) {
+                        sa += (double)HP[t * TWD + c];
+                        sb += (double)HQ[t * TWD + c];
+                    }
+                    ic = box_inv_count(x, y, w, h, R);
                 }
-                const float ic = box_inv_count(x, y, w, h, R);
                 const float abar = __fmul_rn((float)sa, ic), bbar = __fmul_rn((float)sb, ic);
                 // depth.rs:404 q = a-bar * I + b-bar, then depth.rs:1146 max(q, 0)
                 const float q = fmaxf(__fadd_rn(__fmul_rn(abar, I[(r + 2 * R) * PW + c + 2 * R]), bbar), 0.f);
@@ -297,17 +345,26 @@ cudaError_t aggregate_peaks(AggArgs a, bool slice_fp16, cudaStream_t s, int grid
     if (smem > 227 * 1024) return cudaErrorInvalidValue;
     int grid = std::min(a.ntiles, std::max(1, grid_limit));
     cudaError_t e;
-#define LAUNCH_AGG(TWV, SST)                                                                               \
-    {                                                                                                      \
-        auto k = aggregate_kernel<TWV, 32, SST>;                                                           \
-        e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);               \
-        if (e != cudaSuccess) return e;                                                                    \
-        lsb_launched(), k<<<grid, 256, smem, s>>>(a);                                                                      \
+#define LAUNCH_AGG(TWV, SST, RTV)                                                              \
+    {                                                                                          \
+        auto k = aggregate_kernel<TWV, 32, SST, RTV>;                                          \
+        e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);   \
+        if (e != cudaSuccess) return e;                                                        \
+        lsb_launched(), k<<<grid, 256, smem, s>>>(a);                                          \
     }
+    // the reference's default radius (3) and the large-frame one (8) compiled in; others at run time
     if (TWD == 64) {
-        if (slice_fp16) LAUNCH_AGG(64, __half) else LAUNCH_AGG(64, float)
+        if (a.r == 3) {
+            if (slice_fp16) LAUNCH_AGG(64, __half, 3) else LAUNCH_AGG(64, float, 3)
+        } else {
+            if (slice_fp16) LAUNCH_AGG(64, __half, 0) else LAUNCH_AGG(64, float, 0)
+        }
     } else {
-        if (slice_fp16) LAUNCH_AGG(32, __half) else LAUNCH_AGG(32, float)
+        if (a.r == 8) {
+            if (slice_fp16) LAUNCH_AGG(32, __half, 8) else LAUNCH_AGG(32, float, 8)
+        } else {
+            if (slice_fp16) LAUNCH_AGG(32, __half, 0) else LAUNCH_AGG(32, float, 0)
+        }
     }
 #undef LAUNCH_AGG
     return cudaGetLastError();
