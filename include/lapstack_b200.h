@@ -222,6 +222,11 @@ char* lsb_unet_forward(lsb_unet* u, const void* in_dev, const float* d_in_dev, u
 /* forward, MSE of d_in + out0 against target_dev [B][H][W], backward, and Adam when lr > 0 */
 char* lsb_unet_train_step(lsb_unet* u, const void* in_dev, const float* d_in_dev, const float* target_dev, uint32_t B, uint32_t H,
                           uint32_t W, float lr, double* loss_out);
+/* Several stacks of uneven sizes and frame counts, one result each (the batch
+ * entry point of the boundary; stack.rs runs one stack per call). The stacks
+ * share one engine and run back to back on its stream; on an error every
+ * result is freed and the message names the stack. */
+char* lsb_batch_run(lsb_stack* const* stacks, uint32_t n_stacks, lsb_result* outs);
 /* Use the network's prediction as the x0 of this stack's WLS solves (NULL: the
  * reference's FGS start). The stack does not own the network. */
 char* lsb_stack_set_warm_start(lsb_stack* s, lsb_unet* u);

@@ -103,6 +103,7 @@ SIGNATURES = {
     "lsb_unet_forward": (ERR, [P, P, P, C.c_uint32, C.c_uint32, C.c_uint32, P]),
     "lsb_unet_train_step": (ERR, [P, P, P, P, C.c_uint32, C.c_uint32, C.c_uint32, C.c_float, C.POINTER(C.c_double)]),
     "lsb_stack_set_warm_start": (ERR, [P, P]),
+    "lsb_batch_run": (ERR, [C.POINTER(P), C.c_uint32, C.POINTER(Result)]),
     "lsb_stack_depth_planes": (ERR, [P, C.POINTER(P), C.POINTER(P), C.POINTER(P), C.POINTER(P), C.POINTER(C.c_uint32),
                                      C.POINTER(C.c_uint32)]),
 }

@@ -1342,3 +1342,22 @@ extern "C" char* lsb_stack_depth_planes(lsb_stack* s, const float** guide, const
     *dh = (uint32_t)s->dh;
     return nullptr;
 }
+
+extern "C" char* lsb_batch_run(lsb_stack* const* stacks, uint32_t n_stacks, lsb_result* outs) {
+    if (!stacks || !outs) return dup_err("null argument");
+    for (uint32_t i = 0; i < n_stacks; i++) memset(&outs[i], 0, sizeof(lsb_result));
+    for (uint32_t i = 0; i < n_stacks; i++) {
+        if (!stacks[i]) return dup_err(fmt("stack %u is null", i));
+        if (i > 0 && stacks[i]->e != stacks[0]->e) return dup_err("the stacks of a batch share one engine");
+    }
+    for (uint32_t i = 0; i < n_stacks; i++) {
+        char* err = lsb_stack_finish(stacks[i], &outs[i]);
+        if (err) {
+            for (uint32_t j = 0; j <= i; j++) lsb_result_free(&outs[j]);
+            char* msg = dup_err(fmt("stack %u: %s", i, err));
+            free(err);
+            return msg;
+        }
+    }
+    return nullptr;
+}

@@ -311,19 +311,40 @@ class Stack:
         r = Result()
         check(self._L.lsb_stack_finish(self._h, C.byref(r)))
         self._keep.clear()
-        own = _ResultOwner(self._L, r)  # the large planes are views of the library's buffers
-        w, h, n = r.w, r.h, r.n_frames
-        img = _view(own, r.image_f32, 3 * w * h, np.float32).reshape(3, h, w)
-        u16 = _view(own, r.image_u16, 3 * w * h, np.uint16).reshape(h, w, 3)
-        win = _view(own, r.winner, w * h, np.float32).reshape(h, w)
-        dm = None
-        if r.depth:
-            dm = DepthMap(_view(own, r.depth, w * h, np.float32).reshape(h, w), _view(own, r.conf, w * h, np.float32).reshape(h, w),
-                          w, h, r.dw, r.dh, _arr(r.floor_cells, r.dw * r.dh, np.float32).reshape(r.dh, r.dw), r.floor_value,
-                          r.p90, r.wls_rel, r.wls_rel64, r.wls_iters, r.wls_iters_first)
-        return Output(img, u16, win, dm, _arr(r.sims, 8 * n, np.float64).reshape(n, 8),
-                      _arr(r.gains, 3 * n, np.float32).reshape(n, 3), _arr(r.shares, n, np.float32), r.levels,
-                      tuple(r.crop), r.align_evals, dict(zip(STAGES, list(r.ms))))
+        return _output_of(self._L, r)
+
+
+def _output_of(lib, r) -> Output:
+    """An Output over an lsb_result; the large planes are views of the library's buffers."""
+    own = _ResultOwner(lib, r)
+    w, h, n = r.w, r.h, r.n_frames
+    img = _view(own, r.image_f32, 3 * w * h, np.float32).reshape(3, h, w)
+    u16 = _view(own, r.image_u16, 3 * w * h, np.uint16).reshape(h, w, 3)
+    win = _view(own, r.winner, w * h, np.float32).reshape(h, w)
+    dm = None
+    if r.depth:
+        dm = DepthMap(_view(own, r.depth, w * h, np.float32).reshape(h, w), _view(own, r.conf, w * h, np.float32).reshape(h, w),
+                      w, h, r.dw, r.dh, _arr(r.floor_cells, r.dw * r.dh, np.float32).reshape(r.dh, r.dw), r.floor_value,
+                      r.p90, r.wls_rel, r.wls_rel64, r.wls_iters, r.wls_iters_first)
+    return Output(img, u16, win, dm, _arr(r.sims, 8 * n, np.float64).reshape(n, 8),
+                  _arr(r.gains, 3 * n, np.float32).reshape(n, 3), _arr(r.shares, n, np.float32), r.levels,
+                  tuple(r.crop), r.align_evals, dict(zip(STAGES, list(r.ms))))
+
+
+def batch_run(stacks) -> list:
+    """Several pushed stacks of uneven sizes, one Output each (lsb_batch_run)."""
+    if not stacks:
+        return []
+    lib = stacks[0]._L
+    n = len(stacks)
+    hs = (C.c_void_p * n)(*[st._h.value for st in stacks])
+    rs = (Result * n)()
+    check(lib.lsb_batch_run(hs, n, rs))
+    outs = []
+    for i, st in enumerate(stacks):
+        st._keep.clear()
+        outs.append(_output_of(lib, rs[i]))
+    return outs
 
 
 class GpuFuser:

@@ -305,3 +305,25 @@ def test_16bit_storage_error_vs_oracles(storage):
         # both differ from FP64 mostly where a near-tie in the energies picks another frame
         assert e64["mean"] < 1.5 * f32_64["mean"] and e64["p99"] < 1.5 * f32_64["p99"]
         assert e32["mean"] < 2.0
+
+
+def test_batch_run_matches_single_stacks():
+    """lsb_batch_run over stacks of uneven sizes and frame counts gives each
+    stack the result it gets alone."""
+    eng = L.default_engine()
+    specs = [(160, 120, 4, 5), (320, 200, 7, 6), (96, 64, 3, 7)]
+    singles, stacks = [], []
+    for w, h, n, seed in specs:
+        fr = synth(w, h, n, seed=seed, warp=True, mag_step=0.0)
+        st = eng.stack(w, h, n, L.FuseParams(), L.AlignParams(coarsen=1), L.DepthParams())
+        for f in fr:
+            st.push_u16(f)
+        singles.append(st.finish())
+        st.set_count(0)
+        for f in fr:
+            st.push_u16(f)
+        stacks.append(st)
+    outs = L.batch_run(stacks)
+    for a, b in zip(singles, outs):
+        assert_same(a.image_u16, b.image_u16, "fused u16")
+        assert np.array_equal(a.align, b.align) and np.array_equal(a.depth.depth, b.depth.depth)
