@@ -84,16 +84,19 @@ __global__ void coarsen_edges_kernel(const float* __restrict__ ax, const float* 
     cay[(size_t)yy * cw + xx] = b;
 }
 // b_c = P^T r (depth.rs:911 `restrict`), the same block sum as the data weights
-__global__ void block_sum_kernel(const float* __restrict__ src, int w, int h, float* __restrict__ dst, int cw, int ch) {
-    const int xx = blockIdx.x * blockDim.x + threadIdx.x, yy = blockIdx.y * blockDim.y + threadIdx.y;
-    if (xx >= cw || yy >= ch) return;
+__device__ __forceinline__ float block_sum_at(const float* __restrict__ src, int w, int h, int xx, int yy) {
     float o = 0.f;
     for (int y = 2 * yy; y < min(2 * yy + 2, h); y++) {
         float rs = 0.f;
         for (int x = 2 * xx; x < min(2 * xx + 2, w); x++) rs = __fadd_rn(rs, src[(size_t)y * w + x]);
         o = __fadd_rn(o, rs);
     }
-    dst[(size_t)yy * cw + xx] = o;
+    return o;
+}
+__global__ void block_sum_kernel(const float* __restrict__ src, int w, int h, float* __restrict__ dst, int cw, int ch) {
+    const int xx = blockIdx.x * blockDim.x + threadIdx.x, yy = blockIdx.y * blockDim.y + threadIdx.y;
+    if (xx >= cw || yy >= ch) return;
+    dst[(size_t)yy * cw + xx] = block_sum_at(src, w, h, xx, yy);
 }
 // depth.rs:812 `set_dinv`
 __global__ void dinv_kernel(const float* __restrict__ wd, const float* __restrict__ ax, const float* __restrict__ ay, int w, int h,
@@ -109,6 +112,20 @@ __global__ void dinv_kernel(const float* __restrict__ wd, const float* __restric
     dinv[k] = __fdiv_rn(1.f, fmaxf(v, 1e-12f));
 }
 // depth.rs:786 `apply`: mode 0 out = A x; 1 out = b - A x; 2 out = x + w D^-1 (b - A x)
+__device__ __forceinline__ float stencil_at(const float* __restrict__ x, const float* __restrict__ b, const float* __restrict__ wd,
+                                            const float* __restrict__ ax, const float* __restrict__ ay, const float* __restrict__ dinv,
+                                            int w, int h, int i, int y, int mode) {
+    const size_t k = (size_t)y * w + i;
+    const float xk = x[k];
+    float v = __fmul_rn(wd[k], xk);
+    if (i > 0) v = __fadd_rn(v, __fmul_rn(ax[k - 1], __fsub_rn(xk, x[k - 1])));
+    if (i + 1 < w) v = __fadd_rn(v, __fmul_rn(ax[k], __fsub_rn(xk, x[k + 1])));
+    if (y > 0) v = __fadd_rn(v, __fmul_rn(ay[k - w], __fsub_rn(xk, x[k - w])));
+    if (y + 1 < h) v = __fadd_rn(v, __fmul_rn(ay[k], __fsub_rn(xk, x[k + w])));
+    if (mode == 0) return v;
+    if (mode == 1) return __fsub_rn(b[k], v);
+    return __fadd_rn(xk, __fmul_rn(__fmul_rn(MG_OMEGA, dinv[k]), __fsub_rn(b[k], v)));
+}
 __global__ void stencil_kernel(const float* __restrict__ x, const float* __restrict__ b, const float* __restrict__ wd,
                                const float* __restrict__ ax, const float* __restrict__ ay, const float* __restrict__ dinv,
                                float* __restrict__ out, int w, int h, int mode) {
@@ -136,6 +153,52 @@ __global__ void prolong_kernel(float* __restrict__ x, int w, int h, const float*
     if (i >= w || y >= h) return;
     const size_t k = (size_t)y * w + i;
     x[k] = __fadd_rn(x[k], xc[(size_t)(y / 2) * cw + i / 2]);
+}
+
+// The coarse end of the V-cycle (depth.rs:924 `vcycle` from level 0 of `T`
+// down) in ONE CTA: each level's zero-start Jacobi, residual, restriction,
+// the coarsest level's MG_COARSE sweeps, then prolongation and the smoothing
+// sweep back up; __syncthreads between steps. The per-element arithmetic is
+// the separate kernels'. Each level's solution ends in its lv[].x (a sweep
+// writes r, then copies back), as the host-driven levels above expect.
+constexpr int MG_TAIL_CELLS = 8192, MG_TAIL_MAX = 16;
+struct MgTail {
+    WlsLevel lv[MG_TAIL_MAX];
+    int n;
+};
+__device__ __forceinline__ void tail_sweep(const WlsLevel& L, bool zero) {
+    const int n = L.w * L.h;
+    if (zero) {
+        for (int k = threadIdx.x; k < n; k += blockDim.x) L.x[k] = __fmul_rn(__fmul_rn(MG_OMEGA, L.dinv[k]), L.b[k]);
+        __syncthreads();
+        return;
+    }
+    for (int k = threadIdx.x; k < n; k += blockDim.x) L.r[k] = stencil_at(L.x, L.b, L.wd, L.ax, L.ay, L.dinv, L.w, L.h, k % L.w, k / L.w, 2);
+    __syncthreads();
+    for (int k = threadIdx.x; k < n; k += blockDim.x) L.x[k] = L.r[k];
+    __syncthreads();
+}
+__global__ void __launch_bounds__(1024) vcycle_tail_kernel(const MgTail T) {
+    for (int l = 0; l + 1 < T.n; l++) {
+        const WlsLevel &L = T.lv[l], &C = T.lv[l + 1];
+        tail_sweep(L, true);
+        for (int k = threadIdx.x; k < L.w * L.h; k += blockDim.x)
+            L.r[k] = stencil_at(L.x, L.b, L.wd, L.ax, L.ay, L.dinv, L.w, L.h, k % L.w, k / L.w, 1);
+        __syncthreads();
+        for (int k = threadIdx.x; k < C.w * C.h; k += blockDim.x) C.b[k] = block_sum_at(L.r, L.w, L.h, k % C.w, k / C.w);
+        __syncthreads();
+    }
+    const WlsLevel& Z = T.lv[T.n - 1];
+    for (int it = 0; it < MG_COARSE; it++) tail_sweep(Z, it == 0);
+    for (int l = T.n - 2; l >= 0; l--) {
+        const WlsLevel &L = T.lv[l], &C = T.lv[l + 1];
+        for (int k = threadIdx.x; k < L.w * L.h; k += blockDim.x) {
+            const int i = k % L.w, y = k / L.w;
+            L.x[k] = __fadd_rn(L.x[k], C.x[(size_t)(y / 2) * C.w + i / 2]);
+        }
+        __syncthreads();
+        tail_sweep(L, false);
+    }
 }
 // depth.rs:994 wd = max(conf, 0) + 1e-4
 __global__ void wd_kernel(const float* __restrict__ conf, float* __restrict__ wd, size_t n) {
@@ -463,6 +526,13 @@ static void jacobi(WlsLevel& L, bool zero, cudaStream_t s) {
 // depth.rs:924 `vcycle`
 static void vcycle(WlsSolver* S, size_t l, cudaStream_t s) {
     WlsLevel& T = S->lv[l];
+    if ((size_t)T.w * T.h <= (size_t)MG_TAIL_CELLS && S->lv.size() - l <= (size_t)MG_TAIL_MAX) {
+        MgTail tl;
+        tl.n = (int)(S->lv.size() - l);
+        for (int q = 0; q < tl.n; q++) tl.lv[q] = S->lv[l + q];
+        lsb_launched(), vcycle_tail_kernel<<<1, 1024, 0, s>>>(tl);
+        return;
+    }
     if (l + 1 == S->lv.size()) {
         for (int k = 0; k < MG_COARSE; k++) jacobi(T, k == 0, s);
         return;
