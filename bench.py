@@ -238,6 +238,27 @@ def wls_report(L, eng, st, c):
     return out
 
 
+# ------------------------------------------------------------- replicas
+def replica_seed(rank):
+    """Each rank's stack: the same workload with its own seed (independent replicas)."""
+    return 0x1A957ACC ^ rank
+
+
+def max_over_ranks(x, dist=None, device="cpu"):
+    """The slowest rank's time (multi-GPU numbers are the max over ranks)."""
+    if dist is None:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_throughput(world, mp_per_rank_step, ms_max):
+    """Whole-job MP-frames/s: every rank's pixel-frames over the slowest rank's step time."""
+    return world * mp_per_rank_step / (ms_max / 1e3)
+
+
 def peaks():
     try:
         return json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))), "measured"
@@ -279,19 +300,15 @@ def main():
         if dist:
             dist.barrier()
 
-    def max_over_ranks(x):
-        if not dist:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    def max_ranks(x):
+        return max_over_ranks(x, dist, "cuda")
 
     eng = L.Engine(device=local, storage=c["storage"])
     fuse, align, depth = params_of(c, L)
     W, H, N = c["w"], c["h"], c["n"]
     st = eng.stack(W, H, N, fuse, align, depth)
     # independent stacks per rank (replicas): each its own seed
-    L.synth_stack_device(spec_of(c, seed=0x1A957ACC ^ rank), st.frames_device(), eng.stream)
+    L.synth_stack_device(spec_of(c, seed=replica_seed(rank)), st.frames_device(), eng.stream)
     st.set_count(N)
     stream = torch.cuda.ExternalStream(eng.stream)
 
@@ -311,9 +328,9 @@ def main():
     torch.cuda.synchronize()
     barrier()
     launches = L.load().lsb_launch_count() - l0
-    ms = max_over_ranks(e0.elapsed_time(e1) / args.steps)
+    ms = max_ranks(e0.elapsed_time(e1) / args.steps)
     mp_step = N * W * H / 1e6
-    value = world * mp_step / (ms / 1e3)
+    value = job_throughput(world, mp_step, ms)
     sel0 = statistics.mean(s["select_level0"] for s in stages)
     stage_ms = {k: statistics.mean(s[k] for s in stages) for k in stages[0]}
 
@@ -331,7 +348,7 @@ def main():
             st.push_u16(hnp[k])
         out = st.finish()
         torch.cuda.synchronize()
-        t = max_over_ranks((time.perf_counter() - t0) * 1e3)
+        t = max_ranks((time.perf_counter() - t0) * 1e3)
         if it > 0:
             e2e_ms.append(t)
         has_depth = out.depth is not None
@@ -370,7 +387,7 @@ def main():
             "dtype": "f32", "data": "synthetic (seeded generator: height field, band-limited texture, per-pixel defocus)",
             "config": {"workload": workload_name(c, args.config), "global_batch": N * world, "parallelism": f"replicas x{world}",
                        "l2": "inputs (frames) larger than L2 every step"},
-            "e2e": {"value": world * mp_step / (e2e_t / 1e3), "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+            "e2e": {"value": job_throughput(world, mp_step, e2e_t), "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "ms_per_step": e2e_t},
             "gpu_launches": launches,
             "roofline": {"bound": "hbm", "kernel": "select_level_kernel (level 0)", "achieved": achieved,
