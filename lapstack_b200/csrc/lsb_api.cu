@@ -28,6 +28,8 @@ using namespace lsb;
 
 static std::atomic<unsigned long long> g_launches{0};
 void lsb_launched() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+void lsb_launched_add(long long k) { g_launches.fetch_add((uint64_t)k, std::memory_order_relaxed); }
+uint64_t lsb_launched_now() { return g_launches.load(std::memory_order_relaxed); }
 extern "C" uint64_t lsb_launch_count(void) { return g_launches.load(); }
 
 static char* dup_err(const std::string& s) {

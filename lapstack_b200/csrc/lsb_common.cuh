@@ -13,6 +13,9 @@
 
 // Every kernel launch of the engine counts itself (lsb_launch_count in the C ABI).
 void lsb_launched();
+// Graph replays count the kernels they hold; a capture takes back the counts its launches added.
+void lsb_launched_add(long long k);
+uint64_t lsb_launched_now();
 
 // Reflect-101 into [0, n) (pyramid.rs:51 `reflect`): period 2(n-1); n == 1 maps to 0.
 LSB_HD int lsb_reflect(int i, int n) {

@@ -9,6 +9,7 @@
 #include <cuda_bf16.h>
 
 #include <algorithm>
+#include <functional>
 #include <vector>
 
 #include "lsb_common.cuh"
@@ -32,6 +33,12 @@ struct WlsSolver {
     float* alpha_beta;    // [alpha, beta]
     float* host_rel;      // pinned: [rel, stop]
     std::vector<void*> allocs;
+    // the CG iteration as two CUDA graphs (A: A p, alpha, the updates, |r|; B: the preconditioner,
+    // beta, the new direction), captured on the first solve for this u and V-cycle mode
+    cudaGraphExec_t gA = nullptr, gB = nullptr;
+    const float* g_u = nullptr;
+    int g_mode = -1;
+    long long kA = 0, kB = 0;
     float* alloc(size_t n, cudaError_t* e) {
         void* p = nullptr;
         cudaError_t r = cudaMalloc(&p, n * sizeof(float));
@@ -486,6 +493,8 @@ int wls_height(const WlsSolver* s) { return s->h; }
 
 void wls_destroy(WlsSolver* s) {
     if (!s) return;
+    if (s->gA) cudaGraphExecDestroy(s->gA);
+    if (s->gB) cudaGraphExecDestroy(s->gB);
     for (void* p : s->allocs) cudaFree(p);
     if (s->host_rel) cudaFreeHost(s->host_rel);
     delete s;
@@ -627,21 +636,69 @@ cudaError_t wls_solve(WlsSolver* S, const float* d, int max_iters, float* u, flo
     if (e != cudaSuccess) return e;
     float rel = S->host_rel[0];
     int iters = 0;
-    for (int it = 0; it < max_iters; it++) {
-        if (rel < 1e-5f) break;
-        iters++;
+    auto partA = [&]() {
         lsb_launched(), stencil_kernel<<<g2(w, h), B2, 0, s>>>(S->p, S->f, L0.wd, L0.ax, L0.ay, L0.dinv, S->ap, w, h, 0);
         dot(S, S->p, S->ap, n, 1, s);
         lsb_launched(), axpy2_kernel<<<g1(n), 256, 0, s>>>(u, S->p, S->r, S->ap, S->alpha_beta, n);
         dot(S, S->r, S->r, n, 3, s);
+    };
+    auto partB = [&]() {
+        precond();
+        dot(S, S->r, S->z, n, 2, s);
+        lsb_launched(), pupd_kernel<<<g1(n), 256, 0, s>>>(S->p, S->z, S->alpha_beta, n);
+    };
+    // Every V-cycle restarts each level from zero, so which of a level's two buffers holds x
+    // carries nothing from one cycle to the next: one captured cycle serves every iteration.
+    auto capture = [&](const std::function<void()>& part, cudaGraphExec_t* ex, long long* kcount) -> bool {
+        cudaGraph_t g = nullptr;
+        const uint64_t c0 = lsb_launched_now();
+        if (cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return false;
+        part();
+        const cudaError_t ec = cudaStreamEndCapture(s, &g);
+        *kcount = (long long)(lsb_launched_now() - c0);
+        lsb_launched_add(-*kcount);  // captured, not launched
+        bool ok = ec == cudaSuccess && g && cudaGraphInstantiate(ex, g, 0) == cudaSuccess;
+        if (g) cudaGraphDestroy(g);
+        return ok;
+    };
+    bool graphs = max_iters > 0;
+    if (graphs && (!S->gA || S->g_u != u || S->g_mode != mode)) {
+        if (S->gA) cudaGraphExecDestroy(S->gA);
+        if (S->gB) cudaGraphExecDestroy(S->gB);
+        S->gA = S->gB = nullptr;
+        graphs = capture(partA, &S->gA, &S->kA) && capture(partB, &S->gB, &S->kB);
+        if (!graphs) {  // launch directly instead
+            if (S->gA) cudaGraphExecDestroy(S->gA);
+            if (S->gB) cudaGraphExecDestroy(S->gB);
+            S->gA = S->gB = nullptr;
+            cudaGetLastError();
+        } else {
+            S->g_u = u;
+            S->g_mode = mode;
+        }
+    }
+    for (int it = 0; it < max_iters; it++) {
+        if (rel < 1e-5f) break;
+        iters++;
+        if (graphs) {
+            e = cudaGraphLaunch(S->gA, s);
+            if (e != cudaSuccess) return e;
+            lsb_launched_add(S->kA);
+        } else {
+            partA();
+        }
         e = cudaStreamSynchronize(s);
         if (e != cudaSuccess) return e;
         if (S->host_rel[1] != 0.f) break;  // p.Ap <= 0: alpha was 0, u and r are unchanged (depth.rs:1060)
         rel = S->host_rel[0];
         if (rel < 1e-5f) break;
-        precond();
-        dot(S, S->r, S->z, n, 2, s);
-        lsb_launched(), pupd_kernel<<<g1(n), 256, 0, s>>>(S->p, S->z, S->alpha_beta, n);
+        if (graphs) {
+            e = cudaGraphLaunch(S->gB, s);
+            if (e != cudaSuccess) return e;
+            lsb_launched_add(S->kB);
+        } else {
+            partB();
+        }
     }
     *rel_out = rel;
     *iters_out = iters;
