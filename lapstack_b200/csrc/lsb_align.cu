@@ -675,6 +675,7 @@ struct NmJob {
     const double* init_dev;        // if set, the initial transform (the previous frame's result) instead of init
     double* warp_dev;              // if set, the full-resolution warp of the result: inverse [9], affine, identity
     unsigned long long* evals_dev; // if set, evaluations are added here
+    double* costs;                 // [MAX_CAND] the batch's costs, published by the last CTA to arrive
 };
 
 __device__ void dev_sim_matrix(const double* v, int w, int h, double m[9]) {
@@ -759,140 +760,131 @@ __device__ int nm_level_start(const NmJob& J, NmState& S, int L) {
     S.it = 0;
     return n + 1;
 }
-// The top of align.rs:815's loop: returns the candidates pending, 0 when the level is done.
-__device__ int nm_iterate(const NmJob& J, NmState& S) {
+// One step of align.rs:796's loop (the top of align.rs:815's loop and the branch on the
+// batch's costs), run by one warp: lane q owns free
+// parameter q of every vertex, so the per-parameter arithmetic (centroid,
+// reflection, expansion, contraction, shrink, clamps, the convergence test)
+// runs in parallel in the reference's per-parameter operation order; the
+// scalar decisions are taken identically by every lane. The stable sort by
+// cost places vertex i at #{j: f_j < f_i} + #{j < i: f_j == f_i}, the
+// position the insertion sort gives it.
+__device__ int nm_iterate_warp(const NmJob& J, NmState& S, int lane) {
     const int n = J.nfree;
+    const bool lq = lane < n;
     bool done = S.it >= 200;
     if (!done) {
-        S.it++;
-        // stable sort by cost (align.rs:817)
-        for (int i = 1; i <= n; i++) {
-            double f = S.fv[i], v[8];
-            for (int q = 0; q < n; q++) v[q] = S.simplex[i][q];
-            int j = i - 1;
-            while (j >= 0 && S.fv[j] > f) {
-                S.fv[j + 1] = S.fv[j];
-                for (int q = 0; q < n; q++) S.simplex[j + 1][q] = S.simplex[j][q];
-                j--;
+        __syncwarp();
+        if (lane == 0) S.it++;
+        // stable sort: each lane i <= n moves its own vertex
+        double row[8], fi = 0.0;
+        int rank = 0;
+        if (lane <= n) {
+            fi = S.fv[lane];
+            for (int q = 0; q < n; q++) row[q] = S.simplex[lane][q];
+            for (int j = 0; j <= n; j++) {
+                const double fj = S.fv[j];
+                rank += (fj < fi) || (fj == fi && j < lane);
             }
-            S.fv[j + 1] = f;
-            for (int q = 0; q < n; q++) S.simplex[j + 1][q] = v[q];
         }
+        __syncwarp();
+        if (lane <= n) {
+            S.fv[rank] = fi;
+            for (int q = 0; q < n; q++) S.simplex[rank][q] = row[q];
+        }
+        __syncwarp();
         // align.rs:888 `converged`
         bool conv = fabs(__dsub_rn(S.fv[n], S.fv[0])) <= __dmul_rn(1e-4, __dadd_rn(1.0, fabs(S.fv[0])));
-        for (int i = 1; conv && i <= n; i++)
-            for (int q = 0; q < n; q++)
-                if (!(fabs(__dsub_rn(S.simplex[i][q], S.simplex[0][q])) <= S.tol[q])) {
-                    conv = false;
-                    break;
-                }
-        done = conv;
+        bool mine = true;
+        if (lq)
+            for (int i = 1; i <= n; i++) mine = mine && fabs(__dsub_rn(S.simplex[i][lane], S.simplex[0][lane])) <= S.tol[lane];
+        done = conv && __all_sync(0xffffffffu, mine);
     }
     if (done) {
         int best = 0;
         for (int i = 1; i <= n; i++)
             if (S.fv[i] < S.fv[best]) best = i;
-        for (int q = 0; q < n; q++) S.cur[J.free_idx[q]] = S.simplex[best][q];
+        __syncwarp();
+        if (lq) S.cur[J.free_idx[lane]] = S.simplex[best][lane];
+        __syncwarp();
         return 0;
     }
-    double c[8];
-    for (int q = 0; q < n; q++) c[q] = 0.0;
-    for (int i = 0; i < n; i++)
-        for (int q = 0; q < n; q++) c[q] = __dadd_rn(c[q], S.simplex[i][q]);
-    for (int q = 0; q < n; q++) c[q] = __ddiv_rn(c[q], (double)n);
-    for (int q = 0; q < n; q++) S.xr[q] = __dadd_rn(c[q], __dmul_rn(1.0, __dsub_rn(c[q], S.simplex[n][q])));
-    nm_clamp(S, n, S.xr);
-    for (int q = 0; q < n; q++) S.xe[q] = __dadd_rn(c[q], __dmul_rn(2.0, __dsub_rn(S.xr[q], c[q])));
-    nm_clamp(S, n, S.xe);
-    for (int q = 0; q < n; q++) S.xc[q] = __dadd_rn(c[q], __dmul_rn(0.5, __dsub_rn(S.simplex[n][q], c[q])));
-    nm_clamp(S, n, S.xc);
-    nm_put(S, n, 0, S.xr);
-    nm_put(S, n, 1, S.xe);
-    nm_put(S, n, 2, S.xc);
-    S.phase = NM_RXC;
+    if (lq) {
+        const int q = lane;
+        double c = 0.0;
+        for (int i = 0; i < n; i++) c = __dadd_rn(c, S.simplex[i][q]);
+        c = __ddiv_rn(c, (double)n);
+        const double xn = S.simplex[n][q];
+        double xr = __dadd_rn(c, __dmul_rn(1.0, __dsub_rn(c, xn)));
+        xr = fmin(fmax(xr, S.lo[q]), S.hi[q]);
+        double xe = __dadd_rn(c, __dmul_rn(2.0, __dsub_rn(xr, c)));
+        xe = fmin(fmax(xe, S.lo[q]), S.hi[q]);
+        double xc = __dadd_rn(c, __dmul_rn(0.5, __dsub_rn(xn, c)));
+        xc = fmin(fmax(xc, S.lo[q]), S.hi[q]);
+        S.xr[q] = xr;
+        S.xe[q] = xe;
+        S.xc[q] = xc;
+        S.pts[0][q] = xr;
+        S.pts[1][q] = xe;
+        S.pts[2][q] = xc;
+    }
+    if (lane == 0) S.phase = NM_RXC;
+    __syncwarp();
     return 3;
 }
-// Take the costs of the pending candidates; returns the candidates pending next.
-__device__ int nm_advance(const NmJob& J, NmState& S, const double* cost) {
+__device__ int nm_advance_warp(const NmJob& J, NmState& S, const double* cost, int lane) {
     const int n = J.nfree;
-    if (S.phase == NM_INIT) {
-        for (int i = 0; i <= n; i++) S.fv[i] = cost[i];
-        S.evals += n + 1;
-        return nm_iterate(J, S);
+    const bool lq = lane < n;
+    const int phase = S.phase;
+    __syncwarp();
+    if (phase == NM_INIT) {
+        if (lane <= n) S.fv[lane] = cost[lane];
+        if (lane == 0) S.evals += n + 1;
+        __syncwarp();
+        return nm_iterate_warp(J, S, lane);
     }
-    if (S.phase == NM_SHRINK) {
-        for (int i = 1; i <= n; i++) S.fv[i] = cost[i - 1];
-        S.evals += n;
-        return nm_iterate(J, S);
+    if (phase == NM_SHRINK) {
+        if (lane >= 1 && lane <= n) S.fv[lane] = cost[lane - 1];
+        if (lane == 0) S.evals += n;
+        __syncwarp();
+        return nm_iterate_warp(J, S, lane);
     }
     const double fr = cost[0], fe = cost[1], fc = cost[2];
-    S.evals += 1;
+    int evals = 1;
+    int take = -1;  // 0 xr, 1 xe, 2 xc, 3 shrink
     if (fr < S.fv[0]) {
-        S.evals += 1;
-        if (fe < fr) {
-            for (int q = 0; q < n; q++) S.simplex[n][q] = S.xe[q];
-            S.fv[n] = fe;
-        } else {
-            for (int q = 0; q < n; q++) S.simplex[n][q] = S.xr[q];
-            S.fv[n] = fr;
-        }
+        evals += 1;
+        take = fe < fr ? 1 : 0;
     } else if (fr < S.fv[n - 1]) {
-        for (int q = 0; q < n; q++) S.simplex[n][q] = S.xr[q];
-        S.fv[n] = fr;
+        take = 0;
     } else {
-        S.evals += 1;
-        if (fc < S.fv[n]) {
-            for (int q = 0; q < n; q++) S.simplex[n][q] = S.xc[q];
-            S.fv[n] = fc;
-        } else {
-            for (int i = 1; i <= n; i++) {
-                for (int q = 0; q < n; q++)
-                    S.simplex[i][q] = __dadd_rn(S.simplex[0][q], __dmul_rn(0.5, __dsub_rn(S.simplex[i][q], S.simplex[0][q])));
-                nm_clamp(S, n, S.simplex[i]);
-                nm_put(S, n, i - 1, S.simplex[i]);
-            }
-            S.phase = NM_SHRINK;
-            return n;
+        evals += 1;
+        take = fc < S.fv[n] ? 2 : 3;
+    }
+    __syncwarp();
+    if (lane == 0) S.evals += evals;
+    if (take < 3) {
+        if (lq) S.simplex[n][lane] = take == 0 ? S.xr[lane] : (take == 1 ? S.xe[lane] : S.xc[lane]);
+        if (lane == 0) S.fv[n] = take == 0 ? fr : (take == 1 ? fe : fc);
+        __syncwarp();
+        return nm_iterate_warp(J, S, lane);
+    }
+    if (lq) {
+        const int q = lane;
+        const double s0 = S.simplex[0][q];
+        for (int i = 1; i <= n; i++) {
+            double v = __dadd_rn(s0, __dmul_rn(0.5, __dsub_rn(S.simplex[i][q], s0)));
+            v = fmin(fmax(v, S.lo[q]), S.hi[q]);
+            S.simplex[i][q] = v;
+            S.pts[i - 1][q] = v;
         }
     }
-    return nm_iterate(J, S);
+    if (lane == 0) S.phase = NM_SHRINK;
+    __syncwarp();
+    return n;
 }
 
-// A grid barrier with a bounded wait (at least ~1 s of polling before it
-// gives up). Returns false when the wait ran out here or in another block.
-constexpr long long NM_SPIN_LIMIT = 1ll << 21;
-__device__ bool nm_barrier(unsigned* bar, int* err) {
-    __shared__ int ok;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        volatile unsigned* gen = bar + 1;
-        volatile int* verr = err;
-        int good = *verr == 0;
-        if (good) {
-            const unsigned g = *gen;
-            __threadfence();
-            if (atomicAdd(bar, 1u) == gridDim.x - 1) {
-                atomicExch(bar, 0u);
-                __threadfence();
-                atomicAdd(bar + 1, 1u);
-            } else {
-                long long t = 0;
-                while (*gen == g) {
-                    if (*verr != 0 || ++t > NM_SPIN_LIMIT) {
-                        good = 0;
-                        break;
-                    }
-                    __nanosleep(256);
-                }
-                if (!good) atomicCAS(err, 0, 1);
-            }
-            __threadfence();
-        }
-        ok = good;
-    }
-    __syncthreads();
-    return ok != 0;
-}
+// The bounded wait of the search's grid-wide hand-off (at least ~0.1 s of polling).
+constexpr long long NM_SPIN_LIMIT = 1ll << 22;
 
 __device__ __forceinline__ double warp_sum(double v) {
     for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
@@ -906,6 +898,8 @@ __global__ void __launch_bounds__(NM_THREADS) nm_search_kernel(const NmJob J) {
     __shared__ double wred[MAX_CAND][3][NM_WARPS];
     __shared__ double cost[MAX_CAND];
     __shared__ int pending;
+    __shared__ int s_last, s_ok;
+    __shared__ unsigned s_gen;
     const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
     if (tid == 0) {
         for (int q = 0; q < 8; q++) S.cur[q] = J.init_dev ? J.init_dev[q] : J.init[q];
@@ -1005,45 +999,93 @@ __global__ void __launch_bounds__(NM_THREADS) nm_search_kernel(const NmJob J) {
                 double s = 0.0;
                 for (int w8 = 0; w8 < NM_WARPS; w8++) s += wred[k][q][w8];
                 P[((size_t)k * gridDim.x + blockIdx.x) * 3 + q] = s;
+                __threadfence();  // visible to the CTA that sums the partials
             }
-            if (!nm_barrier(J.bar, J.ctl)) return;
-            // every block: every block's partials, in block order, then a fixed tree
-            for (int k = 0; k < nc; k++) {
-                double s0 = 0.0, s1 = 0.0, s2 = 0.0;
-                for (int b = tid; b < (int)gridDim.x; b += NM_THREADS) {
-                    const double* p = P + ((size_t)k * gridDim.x + b) * 3;
-                    s0 += __ldcg(p);
-                    s1 += __ldcg(p + 1);
-                    s2 += __ldcg(p + 2);
-                }
-                s0 = warp_sum(s0);
-                s1 = warp_sum(s1);
-                s2 = warp_sum(s2);
-                if (lane == 0) {
-                    wred[k][0][wid] = s0;
-                    wred[k][1][wid] = s1;
-                    wred[k][2][wid] = s2;
-                }
-            }
-            __syncthreads();
-            if (tid < nc) {
-                double sdv = 0.0, sd2v = 0.0, cn = 0.0;
-                for (int w8 = 0; w8 < NM_WARPS; w8++) {
-                    sdv += wred[tid][0][w8];
-                    sd2v += wred[tid][1][w8];
-                    cn += wred[tid][2][w8];
-                }
-                cost[tid] = cn < 16.0 ? 1e9 : sqrt(fmax(__ddiv_rn(__dsub_rn(sd2v, __ddiv_rn(__dmul_rn(sdv, sdv), cn)), cn), 0.0));
-            }
+            // The last CTA to arrive sums every CTA's partials (in CTA order, then a fixed tree),
+            // publishes the costs and releases the others, which only read the costs back.
             __syncthreads();
             if (tid == 0) {
-                int nx = nm_advance(J, S, cost);
-                // <= 200 iterations of at most two batches each, plus the first simplex
-                if (++passes > 402 && nx > 0) {
-                    nx = 0;
-                    if (blockIdx.x == 0) atomicCAS(J.ctl, 0, 2);
+                volatile unsigned* gen = J.bar + 1;
+                volatile int* verr = J.ctl;
+                s_ok = *verr == 0;
+                if (s_ok) {
+                    s_gen = *gen;
+                    __threadfence();
+                    s_last = atomicAdd(J.bar, 1u) == gridDim.x - 1;
                 }
-                pending = nx;
+            }
+            __syncthreads();
+            if (!s_ok) return;
+            if (s_last) {
+                __threadfence();
+                for (int k = 0; k < nc; k++) {
+                    double s0 = 0.0, s1 = 0.0, s2 = 0.0;
+                    for (int b = tid; b < (int)gridDim.x; b += NM_THREADS) {
+                        const double* p = P + ((size_t)k * gridDim.x + b) * 3;
+                        s0 += __ldcg(p);
+                        s1 += __ldcg(p + 1);
+                        s2 += __ldcg(p + 2);
+                    }
+                    s0 = warp_sum(s0);
+                    s1 = warp_sum(s1);
+                    s2 = warp_sum(s2);
+                    if (lane == 0) {
+                        wred[k][0][wid] = s0;
+                        wred[k][1][wid] = s1;
+                        wred[k][2][wid] = s2;
+                    }
+                }
+                __syncthreads();
+                if (tid < nc) {
+                    double sdv = 0.0, sd2v = 0.0, cn = 0.0;
+                    for (int w8 = 0; w8 < NM_WARPS; w8++) {
+                        sdv += wred[tid][0][w8];
+                        sd2v += wred[tid][1][w8];
+                        cn += wred[tid][2][w8];
+                    }
+                    const double cv = cn < 16.0 ? 1e9 : sqrt(fmax(__ddiv_rn(__dsub_rn(sd2v, __ddiv_rn(__dmul_rn(sdv, sdv), cn)), cn), 0.0));
+                    cost[tid] = cv;
+                    J.costs[tid] = cv;
+                }
+                __syncthreads();
+                if (tid == 0) {
+                    __threadfence();
+                    atomicExch(J.bar, 0u);
+                    __threadfence();
+                    atomicAdd(J.bar + 1, 1u);
+                }
+            } else {
+                if (tid == 0) {
+                    volatile unsigned* gen = J.bar + 1;
+                    volatile int* verr = J.ctl;
+                    long long t = 0;
+                    int good = 1;
+                    while (*gen == s_gen) {
+                        if (*verr != 0 || ++t > NM_SPIN_LIMIT) {
+                            good = 0;
+                            break;
+                        }
+                        __nanosleep(32);
+                    }
+                    if (!good) atomicCAS(J.ctl, 0, 1);
+                    __threadfence();
+                    s_ok = good;
+                }
+                __syncthreads();
+                if (!s_ok) return;
+                if (tid < nc) cost[tid] = __ldcg(J.costs + tid);
+            }
+            __syncthreads();
+            if (wid == 0) {
+                int nx = nm_advance_warp(J, S, cost, lane);
+                // <= 200 iterations of at most two batches each, plus the first simplex
+                if (lane == 0) {
+                    if (++passes > 402 && nx > 0) {
+                        nx = 0;
+                        if (blockIdx.x == 0) atomicCAS(J.ctl, 0, 2);
+                    }
+                    pending = nx;
+                }
             }
             batch++;
             __syncthreads();
@@ -1106,6 +1148,7 @@ static cudaError_t nm_job(AlignCtx& C, const float* rf, const std::vector<float*
     J.bar = (unsigned*)C.nm_ctl + 2;
     J.ctl = C.nm_ctl;
     J.out = C.nm_out;
+    J.costs = C.nm_out + 8;
     return cudaSuccess;
 }
 static cudaError_t nm_launch(AlignCtx& C, NmJob& J) {

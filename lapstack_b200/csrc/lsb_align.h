@@ -33,7 +33,7 @@ struct AlignCtx {
     // the search on the device (one cooperative launch per frame)
     double* nm_part;   // device, 2 * MAX_CAND * NM_MAX_BLOCKS * 3
     int* nm_ctl;       // device, 4: error, evaluations, barrier arrivals and generation
-    double* nm_out;    // device, 8
+    double* nm_out;    // device, 8 (the transform) + MAX_CAND (the batch costs)
     int device_search = 1;  // 0: the host drives the search, one launch per simplex step
     size_t evals = 0, launches = 0;
 };
