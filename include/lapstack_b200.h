@@ -222,6 +222,16 @@ char* lsb_unet_forward(lsb_unet* u, const void* in_dev, const float* d_in_dev, u
 /* forward, MSE of d_in + out0 against target_dev [B][H][W], backward, and Adam when lr > 0 */
 char* lsb_unet_train_step(lsb_unet* u, const void* in_dev, const float* d_in_dev, const float* target_dev, uint32_t B, uint32_t H,
                           uint32_t W, float lr, double* loss_out);
+/* The autotuner (no counterpart in the reference): the persistent kernels' grid
+ * sizes (the fold's select kernel, the depth aggregation) timed on this stack's
+ * frames (two full runs per candidate), the fastest kept by the engine for every
+ * later run. The grid size changes no result. */
+typedef struct {
+    uint32_t candidates[3];
+    double fold_ms[3], aggregate_ms[3];
+    uint32_t grid_select, grid_aggregate;
+} lsb_tuning;
+char* lsb_stack_autotune(lsb_stack* s, lsb_tuning* out);
 /* Several stacks of uneven sizes and frame counts, one result each (the batch
  * entry point of the boundary; stack.rs runs one stack per call). The stacks
  * share one engine and run back to back on its stream; on an error every

@@ -57,6 +57,11 @@ class Result(C.Structure):
                 ("align_evals", C.c_uint32), ("wls_rel64", C.c_double), ("ms", C.c_double * 12)]
 
 
+class Tuning(C.Structure):
+    _fields_ = [("candidates", C.c_uint32 * 3), ("fold_ms", C.c_double * 3), ("aggregate_ms", C.c_double * 3),
+                ("grid_select", C.c_uint32), ("grid_aggregate", C.c_uint32)]
+
+
 class SynthDesc(C.Structure):
     _fields_ = [("w", C.c_uint32), ("h", C.c_uint32), ("n", C.c_uint32), ("warp", C.c_uint32), ("seed", C.c_uint64),
                 ("mag_step", C.c_float), ("noise_std", C.c_float), ("blur_px", C.c_float), ("warp_scale", C.c_float),
@@ -104,6 +109,7 @@ SIGNATURES = {
     "lsb_unet_train_step": (ERR, [P, P, P, P, C.c_uint32, C.c_uint32, C.c_uint32, C.c_float, C.POINTER(C.c_double)]),
     "lsb_stack_set_warm_start": (ERR, [P, P]),
     "lsb_batch_run": (ERR, [C.POINTER(P), C.c_uint32, C.POINTER(Result)]),
+    "lsb_stack_autotune": (ERR, [P, C.POINTER(Tuning)]),
     "lsb_stack_depth_planes": (ERR, [P, C.POINTER(P), C.POINTER(P), C.POINTER(P), C.POINTER(P), C.POINTER(C.c_uint32),
                                      C.POINTER(C.c_uint32)]),
 }

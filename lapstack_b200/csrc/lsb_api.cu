@@ -71,6 +71,7 @@ struct DevPool {
 struct lsb_engine {
     lsb_config cfg;
     int device, sms, grid;
+    int grid_select = 0, grid_agg = 0;  // autotuned persistent grids (0: grid)
     int coop = 0;  // cooperative launch: the registration search runs on the device
     cudaStream_t s;
     cudaStream_t cs = nullptr;  // host -> device frame copies, overlapped with the work on s
@@ -805,7 +806,7 @@ static char* run_pipeline(lsb_stack* s) {
         const int src = l > 0 ? SRC_G : ((s->f32src || (warped && s->storage == STORE_F32)) ? SRC_F32 : SRC_U16);
         a.between = l == 0 ? ev[10] : nullptr;
         if (l == 0) TRY(cudaEventRecord(ev[8], st));
-        TRY(fold_level(a, src, s->storage, (int)s->fp.energy_radius, focus, st, e->grid));
+        TRY(fold_level(a, src, s->storage, (int)s->fp.energy_radius, focus, st, e->grid_select > 0 ? e->grid_select : e->grid));
         if (l == 0) TRY(cudaEventRecord(ev[9], st));
     }
     TRY(cudaEventRecord(ev[3], st));
@@ -845,7 +846,7 @@ static char* run_pipeline(lsb_stack* s) {
         TRY(luma_and_guide(s->img, W, H, k, s->yfull, s->guide, dw, dh, st));
         if (s->dp.agg_radius > 0) gf_stats(s->guide, dw, dh, (int)s->dp.agg_radius, s->tmp, s->mi, s->vi, st);
         AggArgs ag{s->slices, n, dw, dh, (int)s->dp.agg_radius, s->dp.agg_eps, s->guide, s->mi, s->vi, s->state, 0, 0};
-        TRY(aggregate_peaks(ag, s->storage != STORE_F32, st, e->grid));
+        TRY(aggregate_peaks(ag, s->storage != STORE_F32, st, e->grid_agg > 0 ? e->grid_agg : e->grid));
         TRY(cudaEventRecord(ev[5], st));
         const size_t cnt = (m + 6) / 7;
         TRY(select_kth(s->state + 7 * m, cnt, 7, cnt / 2, e->hist, e->sel, e->scal + 0, st));
@@ -1361,5 +1362,39 @@ extern "C" char* lsb_batch_run(lsb_stack* const* stacks, uint32_t n_stacks, lsb_
             return msg;
         }
     }
+    return nullptr;
+}
+
+// The project's autotuner: the persistent kernels' grid sizes (the fold's select
+// kernel and the depth aggregation; CTAs walk tiles, so any grid gives the same
+// results) timed on this stack's own frames, one full run per candidate, the
+// fastest kept in the engine for every later run.
+extern "C" char* lsb_stack_autotune(lsb_stack* s, lsb_tuning* out) {
+    if (!s || !out) return dup_err("null argument");
+    lsb_engine* e = s->e;
+    const int cand[3] = {e->sms, (3 * e->sms) / 2, 2 * e->sms};
+    double best_sel = 1e300, best_agg = 1e300;
+    int gs = cand[0], ga = cand[0];
+    memset(out, 0, sizeof *out);
+    for (int i = 0; i < 3; i++) {
+        e->grid_select = cand[i];
+        e->grid_agg = cand[i];
+        char* err = run_pipeline(s);
+        if (!err) err = run_pipeline(s);  // the second run is the one timed
+        if (err) {
+            e->grid_select = e->grid_agg = 0;
+            return err;
+        }
+        const double sel = s->ms[2], agg = s->ms[4];  // the fold, the aggregation
+        out->candidates[i] = (uint32_t)cand[i];
+        out->fold_ms[i] = sel;
+        out->aggregate_ms[i] = agg;
+        if (sel < best_sel) best_sel = sel, gs = cand[i];
+        if (agg < best_agg) best_agg = agg, ga = cand[i];
+    }
+    e->grid_select = gs;
+    e->grid_agg = ga;
+    out->grid_select = (uint32_t)gs;
+    out->grid_aggregate = (uint32_t)ga;
     return nullptr;
 }

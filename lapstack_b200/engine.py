@@ -279,6 +279,15 @@ class Stack:
         check(self._L.lsb_stack_set_warm_start(self._h, net._h if net is not None else None))
         self._net = net  # the stack does not own the network; keep it alive
 
+    def autotune(self):
+        """Time the persistent kernels' grid sizes on this stack's frames; the engine keeps the fastest."""
+        from ._lib import Tuning
+        t = Tuning()
+        check(self._L.lsb_stack_autotune(self._h, C.byref(t)))
+        self._keep.clear()
+        return dict(candidates=list(t.candidates), fold_ms=list(t.fold_ms), aggregate_ms=list(t.aggregate_ms),
+                    grid_select=t.grid_select, grid_aggregate=t.grid_aggregate)
+
     def depth_planes(self):
         """Device pointers of the last run's depth-grid planes: guide, d, conf, u, and (dw, dh)."""
         ps = [C.c_void_p() for _ in range(4)]

@@ -327,3 +327,20 @@ def test_batch_run_matches_single_stacks():
     for a, b in zip(singles, outs):
         assert_same(a.image_u16, b.image_u16, "fused u16")
         assert np.array_equal(a.align, b.align) and np.array_equal(a.depth.depth, b.depth.depth)
+
+
+def test_autotune_keeps_results():
+    """The autotuner changes only how many CTAs walk the tiles: the results stay bit for bit."""
+    fr = synth(512, 384, 6, seed=61, warp=True, mag_step=0.0)
+    eng = L.Engine()
+    st = eng.stack(512, 384, 6, L.FuseParams(), L.AlignParams(coarsen=1), L.DepthParams())
+    for f in fr:
+        st.push_u16(f)
+    before = st.finish()
+    tune = st.autotune()
+    assert tune["grid_select"] in tune["candidates"] and tune["grid_aggregate"] in tune["candidates"]
+    after = st.finish()
+    assert_same(before.image_u16, after.image_u16, "fused u16")
+    assert np.array_equal(before.depth.depth, after.depth.depth)
+    st.close()
+    eng.close()
