@@ -224,93 +224,124 @@ template <bool ROWS>
 __device__ __forceinline__ float& tl(float (*t)[TT + 1], int line, int e) {
     return ROWS ? t[line][e] : t[e][line];
 }
+__device__ __forceinline__ void cp_async4f(float* smem, const float* gmem) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(d), "l"(gmem));
+}
+__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
+
+// The 32 lines' elements e0 .. e0+31 of `src` into tile t (cp.async; `fill` where out of range).
+template <bool ROWS>
+__device__ __forceinline__ void tile_load(float (*t)[TT + 1], const float* __restrict__ src, int l0, int e0, int nlines, int len, int w,
+                                          float fill) {
+    const int lane = threadIdx.x;
+    for (int q = 0; q < TT; q++) {
+        const int ln = ROWS ? q : lane, e = ROWS ? e0 + lane : e0 + q;
+        float* d = &tl<ROWS>(t, ln, e - e0);
+        if (l0 + ln < nlines && e < len) cp_async4f(d, src + (ROWS ? (size_t)(l0 + ln) * w + e : (size_t)e * w + (l0 + ln)));
+        else *d = fill;
+    }
+}
+template <bool ROWS>
+__device__ __forceinline__ void tile_store(float (*t)[TT + 1], float* __restrict__ dst, int l0, int e0, int nlines, int len, int w) {
+    const int lane = threadIdx.x;
+    for (int q = 0; q < TT; q++) {
+        const int ln = ROWS ? q : lane, e = ROWS ? e0 + lane : e0 + q;
+        if (l0 + ln < nlines && e < len) dst[ROWS ? (size_t)(l0 + ln) * w + e : (size_t)e * w + (l0 + ln)] = tl<ROWS>(t, ln, e - e0);
+    }
+}
+
+// depth.rs:677 `solve_rows` / :707 `solve_cols`: the Thomas algorithm along
+// every line, one thread per line, 32 lines per warp (ROWS: a line is an image
+// row, the tile is [line][element]; else a line is a column, the tile is
+// [element][line]). The coefficient tiles of the next 32 elements stream into
+// shared memory (cp.async, two buffers) while the current 32 are eliminated,
+// and the back substitution streams cp / dp the same way; each thread walks
+// its line in the reference's order and arithmetic.
 template <bool ROWS>
 __global__ void __launch_bounds__(32) thomas_kernel(float* __restrict__ u, const float* __restrict__ f, const float* __restrict__ wd,
                                                     int unit_wd, const float* __restrict__ a, int w, int h, float lam,
                                                     float* __restrict__ cp, float* __restrict__ dp) {
-    __shared__ float ta[TT][TT + 1], tw[TT][TT + 1], tf[TT][TT + 1], tc[TT][TT + 1], td[TT][TT + 1];
+    __shared__ float ta[2][TT][TT + 1], tw[2][TT][TT + 1], tf[2][TT][TT + 1], tc[2][TT][TT + 1], td[2][TT][TT + 1];
     const int lane = threadIdx.x;
     const int nlines = ROWS ? h : w, len = ROWS ? w : h;
     const int l0 = blockIdx.x * TT;
     const int li = l0 + lane;
-    // global index of (line l0 + ln, element e)
-    auto gi = [&](int ln, int e) -> size_t { return ROWS ? (size_t)(l0 + ln) * w + e : (size_t)e * w + (l0 + ln); };
-    // the warp moves tile row q (q = line for ROWS, element otherwise): lane walks the contiguous axis
+    const int nch = (len + TT - 1) / TT;
+    auto issue_fwd = [&](int c) {
+        const int b = c & 1, e0 = c * TT;
+        tile_load<ROWS>(ta[b], a, l0, e0, nlines, len, w, 0.f);
+        tile_load<ROWS>(tf[b], f, l0, e0, nlines, len, w, 0.f);
+        if (!unit_wd) tile_load<ROWS>(tw[b], wd, l0, e0, nlines, len, w, 1.f);
+        cp_commit();
+    };
     float prev_a = 0.f, cprev = 0.f, dprev = 0.f;
     const float nl = -lam;
-    for (int e0 = 0; e0 < len; e0 += TT) {
-        const int ne = min(TT, len - e0);
-        for (int q = 0; q < TT; q++) {
-            int ln, e;
-            if (ROWS) ln = q, e = e0 + lane;
-            else ln = lane, e = e0 + q;
-            const bool ok = l0 + ln < nlines && e < e0 + ne;
-            const size_t k = ok ? gi(ln, e) : 0;
-            tl<ROWS>(ta, ln, e - e0) = ok && e + 1 < len ? a[k] : 0.f;
-            tl<ROWS>(tf, ln, e - e0) = ok ? f[k] : 0.f;
-            tl<ROWS>(tw, ln, e - e0) = ok && !unit_wd ? wd[k] : 1.f;
+    issue_fwd(0);
+    for (int c = 0; c < nch; c++) {
+        const int b = c & 1, e0 = c * TT, ne = min(TT, len - e0);
+        if (c + 1 < nch) {
+            issue_fwd(c + 1);
+            cp_wait<1>();
+        } else {
+            cp_wait<0>();
         }
         __syncwarp();
         if (li < nlines)
             for (int j = 0; j < ne; j++) {
                 const int i = e0 + j;
-                const float ai = tl<ROWS>(ta, lane, j);
-                const float wdi = tl<ROWS>(tw, lane, j);
+                const float ai = i + 1 < len ? tl<ROWS>(ta[b], lane, j) : 0.f;
+                const float wdi = unit_wd ? 1.f : tl<ROWS>(tw[b], lane, j);
                 const float diag = __fadd_rn(wdi, __fmul_rn(lam, __fadd_rn(prev_a, ai)));
                 const float lower = __fmul_rn(nl, prev_a), upper = __fmul_rn(nl, ai);
                 float m = __fsub_rn(diag, __fmul_rn(lower, i > 0 ? cprev : 0.f));
                 if (fabsf(m) < 1e-12f) m = 1e-12f;
                 cprev = __fdiv_rn(upper, m);
-                dprev = __fdiv_rn(__fsub_rn(__fmul_rn(wdi, tl<ROWS>(tf, lane, j)), __fmul_rn(lower, i > 0 ? dprev : 0.f)), m);
-                tl<ROWS>(tc, lane, j) = cprev;
-                tl<ROWS>(td, lane, j) = dprev;
+                dprev = __fdiv_rn(__fsub_rn(__fmul_rn(wdi, tl<ROWS>(tf[b], lane, j)), __fmul_rn(lower, i > 0 ? dprev : 0.f)), m);
+                tl<ROWS>(tc[b], lane, j) = cprev;
+                tl<ROWS>(td[b], lane, j) = dprev;
                 prev_a = ai;
             }
         __syncwarp();
-        for (int q = 0; q < TT; q++) {
-            int ln, e;
-            if (ROWS) ln = q, e = e0 + lane;
-            else ln = lane, e = e0 + q;
-            if (l0 + ln < nlines && e < e0 + ne) {
-                const size_t k = gi(ln, e);
-                cp[k] = tl<ROWS>(tc, ln, e - e0);
-                dp[k] = tl<ROWS>(td, ln, e - e0);
-            }
+        if (c + 1 < nch) {  // the last chunk stays in shared memory for the back substitution
+            tile_store<ROWS>(tc[b], cp, l0, e0, nlines, len, w);
+            tile_store<ROWS>(td[b], dp, l0, e0, nlines, len, w);
         }
         __syncwarp();
     }
-    // back substitution, tiles from the end; the last chunk's cp/dp are still in shared memory
+    __threadfence_block();
+    __syncwarp();
+    // back substitution, chunks from the end; chunk c-1's cp / dp stream in while chunk c runs
+    const int last = nch - 1;
+    auto issue_bwd = [&](int c) {
+        const int b = c & 1, e0 = c * TT;
+        tile_load<ROWS>(tc[b], cp, l0, e0, nlines, len, w, 0.f);
+        tile_load<ROWS>(td[b], dp, l0, e0, nlines, len, w, 0.f);
+        cp_commit();
+    };
     float nxt = 0.f;
-    const int last0 = ((len - 1) / TT) * TT;
-    for (int e0 = last0; e0 >= 0; e0 -= TT) {
-        const int ne = min(TT, len - e0);
-        if (e0 != last0) {
-            for (int q = 0; q < TT; q++) {
-                int ln, e;
-                if (ROWS) ln = q, e = e0 + lane;
-                else ln = lane, e = e0 + q;
-                const bool ok = l0 + ln < nlines;
-                const size_t k = ok ? gi(ln, e) : 0;
-                tl<ROWS>(tc, ln, e - e0) = ok ? cp[k] : 0.f;
-                tl<ROWS>(td, ln, e - e0) = ok ? dp[k] : 0.f;
-            }
-            __syncwarp();
+    for (int c = last; c >= 0; c--) {
+        const int b = c & 1, e0 = c * TT, ne = min(TT, len - e0);
+        if (c - 1 >= 0) {
+            issue_bwd(c - 1);
+            if (c != last) cp_wait<1>();
+        } else if (c != last) {
+            cp_wait<0>();
         }
+        __syncwarp();
         if (li < nlines)
             for (int j = ne - 1; j >= 0; j--) {
                 const int i = e0 + j;
-                nxt = i == len - 1 ? tl<ROWS>(td, lane, j) : __fsub_rn(tl<ROWS>(td, lane, j), __fmul_rn(tl<ROWS>(tc, lane, j), nxt));
-                tl<ROWS>(tf, lane, j) = nxt;
+                nxt = i == len - 1 ? tl<ROWS>(td[b], lane, j) : __fsub_rn(tl<ROWS>(td[b], lane, j), __fmul_rn(tl<ROWS>(tc[b], lane, j), nxt));
+                tl<ROWS>(tf[b], lane, j) = nxt;
             }
         __syncwarp();
-        for (int q = 0; q < TT; q++) {
-            int ln, e;
-            if (ROWS) ln = q, e = e0 + lane;
-            else ln = lane, e = e0 + q;
-            if (l0 + ln < nlines && e < e0 + ne) u[gi(ln, e)] = tl<ROWS>(tf, ln, e - e0);
-        }
+        tile_store<ROWS>(tf[b], u, l0, e0, nlines, len, w);
         __syncwarp();
     }
+    cp_wait<0>();
 }
 static void thomas(bool rows, float* u, const float* f, const float* wd, int unit_wd, const float* a, int w, int h, float lam,
                    float* cp, float* dp, cudaStream_t s) {
