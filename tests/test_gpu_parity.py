@@ -4,7 +4,7 @@ restatement of the reference's FP32 path, on the same seeded inputs.
 Bar (the north star's): selection / winner maps and the fused image
 bit-exact; gains bit-exact; the depth map within 1e-3 of the frame range
 except where a near-tie in the peak search falls the other way (the
-reference's own GPU test, gpu.rs:1480, allows 0.1 % of cells); WLS to the
+reference's own GPU test, gpu.rs:1524, allows 0.1 % of cells); WLS to the
 solver's own 1e-5 relative residual.
 """
 import numpy as np
