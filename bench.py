@@ -224,6 +224,22 @@ def wls_report(L, eng, st, c):
     losses = U.train(net, inp, d_in, tgt, steps=300, batch=8, crop=256, lr=1e-3)
     train_s = time.perf_counter() - t0
     del inp, d_in, tgt
+    # the network's forward pass on this stack's grid: tensor-core FLOPs against the measured bf16 peak
+    Hn, Wn = U.grid_of(dw, dh)
+    t_in = torch.zeros((1, Hn, Wn, U.CH), dtype=torch.bfloat16, device="cuda")
+    t_d = torch.zeros((1, Hn, Wn), dtype=torch.float32, device="cuda")
+    net.forward(t_in, t_d)
+    reps = 5
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        net.forward(t_in, t_d)
+    fwd_ms = (time.perf_counter() - t0) * 1e3 / reps
+    flops = U.forward_flops(Hn, Wn)
+    pk, pk_kind = peaks()
+    out["unet_forward"] = {"grid": [Wn, Hn], "ms": fwd_ms, "tflops": flops / (fwd_ms / 1e3) / 1e12,
+                           "frac": flops / (fwd_ms / 1e3) / 1e12 / pk["bf16_tflops"], "peak_tflops": pk["bf16_tflops"],
+                           "peak_kind": pk_kind, "timing": "host wall time of the synchronous call (copies of the input included)"}
+    del t_in, t_d
     res = {}
     for mode in ("plain", "learned", "plain", "learned"):
         st.set_warm_start(net if mode == "learned" else None)

@@ -25,6 +25,14 @@ from ._lib import check, load
 from .engine import DepthParams, Engine, FuseParams, SynthSpec, default_engine, synth_stack_device
 
 CH = 32  # channels of the network's input tensor (3 live)
+# the 15 convolutions as lsb_unet.cu runs them: (input channels, output channels, level)
+CONVS = [(32, 32, 0), (32, 32, 0), (32, 64, 1), (64, 64, 1), (64, 128, 2), (128, 128, 2), (128, 256, 3), (256, 256, 3),
+         (384, 128, 2), (128, 128, 2), (192, 64, 1), (64, 64, 1), (96, 32, 0), (32, 32, 0), (32, 32, 0)]
+
+
+def forward_flops(H, W, B=1):
+    """Tensor-core FLOPs of one forward pass on a B x H x W grid (as executed: padded channels included)."""
+    return 2 * sum(9 * ci * co * B * (H >> lv) * (W >> lv) for ci, co, lv in CONVS)
 
 
 def grid_of(dw, dh):
