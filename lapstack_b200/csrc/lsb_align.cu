@@ -650,8 +650,9 @@ cudaError_t cost_single(AlignCtx& C, const float* rf, int aw, int ah, const floa
 // Per batch it evaluates the pending candidates over its share of the
 // level's pixels (the cost of align.rs:581: f64 sums of d, d^2 and the
 // count), publishes its partial sums, meets the other blocks at a grid
-// barrier, sums every block's partials in one fixed order and advances its
-// copy of the search. Every copy sees the same sums and takes the same
+// barrier (only the blocks with pixels arrive; every block waits), sums
+// those blocks' partials in one fixed order and advances its copy of the
+// search. Every copy sees the same sums and takes the same
 // branches, so one barrier per batch suffices; the partials alternate
 // between two buffers, so a batch's writes never meet a slower block's reads
 // of the batch before. The barrier's wait is bounded: on a timeout the
@@ -667,15 +668,14 @@ struct NmJob {
     int W, H;  // full resolution
     double init[8];
     int free_idx[8], nfree;
-    double* part;   // [2][MAX_CAND][gridDim.x][3]
-    unsigned* bar;  // [0] arrivals, [1] generation; zero at launch
+    double* part;   // [2][MAX_CAND][3][gridDim.x]
+    unsigned* bar;  // [0] arrivals of every batch so far (zero at launch)
     int* ctl;       // [0] error (sticky): 1 barrier timeout, 2 batch limit; [1] evaluations (the reference's count)
     double* out;    // the transform found [8]
     // chained searches (no host round trip between frames):
     const double* init_dev;        // if set, the initial transform (the previous frame's result) instead of init
     double* warp_dev;              // if set, the full-resolution warp of the result: inverse [9], affine, identity
     unsigned long long* evals_dev; // if set, evaluations are added here
-    double* costs;                 // [MAX_CAND] the batch's costs, published by the last CTA to arrive
 };
 
 __device__ void dev_sim_matrix(const double* v, int w, int h, double m[9]) {
@@ -896,10 +896,10 @@ __global__ void __launch_bounds__(NM_THREADS) nm_search_kernel(const NmJob J) {
     __shared__ NmState S;
     __shared__ double cand[MAX_CAND][9];
     __shared__ double wred[MAX_CAND][3][NM_WARPS];
+    __shared__ double gred[NM_THREADS];
     __shared__ double cost[MAX_CAND];
     __shared__ int pending;
-    __shared__ int s_last, s_ok;
-    __shared__ unsigned s_gen;
+    __shared__ int s_ok;
     const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
     if (tid == 0) {
         for (int q = 0; q < 8; q++) S.cur[q] = J.init_dev ? J.init_dev[q] : J.init[q];
@@ -910,6 +910,7 @@ __global__ void __launch_bounds__(NM_THREADS) nm_search_kernel(const NmJob J) {
         S.evals = 0;
     }
     int batch = 0;
+    unsigned arrived = 0;  // the counter's value once this batch's arrivals are in
     const unsigned stride = gridDim.x * NM_THREADS;
     for (int L = 0; L < J.nlv; L++) {
         const NmLevel lv = J.lv[L];
@@ -918,6 +919,8 @@ __global__ void __launch_bounds__(NM_THREADS) nm_search_kernel(const NmJob J) {
         __syncthreads();
         const double xmax = (double)(lv.w - 1), ymax = (double)(lv.h - 1);
         const unsigned npx = (unsigned)lv.w * lv.h;  // < 2^32 (the host checks)
+        const int nown = (int)min((unsigned)gridDim.x, (npx + NM_THREADS - 1) / NM_THREADS);  // CTAs with pixels
+        const bool own = (int)blockIdx.x < nown;
         const unsigned sdy = stride / (unsigned)lv.w, sdx = stride - sdy * (unsigned)lv.w;
         const unsigned i0 = blockIdx.x * NM_THREADS + tid;
         const int y0s = (int)(i0 / (unsigned)lv.w), x0s = (int)(i0 - (unsigned)y0s * lv.w);
@@ -959,13 +962,25 @@ __global__ void __launch_bounds__(NM_THREADS) nm_search_kernel(const NmJob J) {
                                 spline4f((float)__dsub_rn(sx, fx), wx);
                                 spline4f((float)__dsub_rn(sy, fy), wy);
                                 float acc = 0.f;
+                                if (xa >= 1 && xa + 2 < lv.w && ya >= 1 && ya + 2 < lv.h) {
+                                    // the 4x4 footprint inside the plane: no clamps
+                                    const float* row = lv.tg + (size_t)(ya - 1) * lv.w + (xa - 1);
 #pragma unroll
-                                for (int j = 0; j < 4; j++) {
-                                    const float* row = lv.tg + (size_t)min(max(ya + j - 1, 0), lv.h - 1) * lv.w;
-                                    float r = 0.f;
+                                    for (int j = 0; j < 4; j++, row += lv.w) {
+                                        float r = 0.f;
 #pragma unroll
-                                    for (int u = 0; u < 4; u++) r = __fadd_rn(r, __fmul_rn(wx[u], row[min(max(xa + u - 1, 0), lv.w - 1)]));
-                                    acc = __fadd_rn(acc, __fmul_rn(wy[j], r));
+                                        for (int u = 0; u < 4; u++) r = __fadd_rn(r, __fmul_rn(wx[u], __ldg(row + u)));
+                                        acc = __fadd_rn(acc, __fmul_rn(wy[j], r));
+                                    }
+                                } else {
+#pragma unroll
+                                    for (int j = 0; j < 4; j++) {
+                                        const float* row = lv.tg + (size_t)min(max(ya + j - 1, 0), lv.h - 1) * lv.w;
+                                        float r = 0.f;
+#pragma unroll
+                                        for (int u = 0; u < 4; u++) r = __fadd_rn(r, __fmul_rn(wx[u], __ldg(row + min(max(xa + u - 1, 0), lv.w - 1))));
+                                        acc = __fadd_rn(acc, __fmul_rn(wy[j], r));
+                                    }
                                 }
                                 const double d = (double)__fsub_rn(rv, acc);
                                 sd[c] += d;
@@ -994,86 +1009,62 @@ __global__ void __launch_bounds__(NM_THREADS) nm_search_kernel(const NmJob J) {
             }
             __syncthreads();
             double* P = J.part + (size_t)(batch & 1) * MAX_CAND * gridDim.x * 3;
-            if (tid < 3 * nc) {
+            if (own && tid < 3 * nc) {
                 const int k = tid / 3, q = tid % 3;
                 double s = 0.0;
                 for (int w8 = 0; w8 < NM_WARPS; w8++) s += wred[k][q][w8];
-                P[((size_t)k * gridDim.x + blockIdx.x) * 3 + q] = s;
-                __threadfence();  // visible to the CTA that sums the partials
+                P[((size_t)k * 3 + q) * gridDim.x + blockIdx.x] = s;
             }
-            // The last CTA to arrive sums every CTA's partials (in CTA order, then a fixed tree),
-            // publishes the costs and releases the others, which only read the costs back.
+            // The hand-off: the CTAs with pixels arrive on a counter that only grows; every CTA
+            // waits until this batch's arrivals are in, then sums the partials itself.
+            arrived += (unsigned)nown;
             __syncthreads();
             if (tid == 0) {
-                volatile unsigned* gen = J.bar + 1;
-                volatile int* verr = J.ctl;
-                s_ok = *verr == 0;
-                if (s_ok) {
-                    s_gen = *gen;
-                    __threadfence();
-                    s_last = atomicAdd(J.bar, 1u) == gridDim.x - 1;
+                if (own) {
+                    __threadfence();  // this CTA's partials before its arrival
+                    atomicAdd(J.bar, 1u);
                 }
+                volatile unsigned* cnt = J.bar;
+                volatile int* verr = J.ctl;
+                long long t = 0;
+                int good = 1;
+                while ((int)(*cnt - arrived) < 0) {
+                    if (*verr != 0 || ++t > NM_SPIN_LIMIT) {
+                        good = 0;
+                        break;
+                    }
+                    __nanosleep(32);
+                }
+                if (!good) atomicCAS(J.ctl, 0, 1);
+                __threadfence();
+                s_ok = good;
             }
             __syncthreads();
             if (!s_ok) return;
-            if (s_last) {
-                __threadfence();
-                for (int k = 0; k < nc; k++) {
-                    double s0 = 0.0, s1 = 0.0, s2 = 0.0;
-                    for (int b = tid; b < (int)gridDim.x; b += NM_THREADS) {
-                        const double* p = P + ((size_t)k * gridDim.x + b) * 3;
-                        s0 += __ldcg(p);
-                        s1 += __ldcg(p + 1);
-                        s2 += __ldcg(p + 2);
-                    }
-                    s0 = warp_sum(s0);
-                    s1 = warp_sum(s1);
-                    s2 = warp_sum(s2);
-                    if (lane == 0) {
-                        wred[k][0][wid] = s0;
-                        wred[k][1][wid] = s1;
-                        wred[k][2][wid] = s2;
-                    }
+            // every CTA: each of the 3*nc sums over the CTAs with pixels, by gsz threads (thread r
+            // takes CTAs r, r + gsz, ...), then the threads' sums in order: the same order in every copy
+            {
+                const int np = 3 * nc, gsz = NM_THREADS / np;
+                const int pi = tid / gsz, r = tid - pi * gsz;
+                double sv = 0.0;
+                if (pi < np) {
+                    const double* row = P + (size_t)pi * gridDim.x;
+#pragma unroll 4
+                    for (int b = r; b < nown; b += gsz) sv += __ldcg(row + b);
                 }
+                gred[tid] = sv;
                 __syncthreads();
                 if (tid < nc) {
-                    double sdv = 0.0, sd2v = 0.0, cn = 0.0;
-                    for (int w8 = 0; w8 < NM_WARPS; w8++) {
-                        sdv += wred[tid][0][w8];
-                        sd2v += wred[tid][1][w8];
-                        cn += wred[tid][2][w8];
+                    double v3[3];
+                    for (int q = 0; q < 3; q++) {
+                        const double* g = gred + (size_t)(tid * 3 + q) * gsz;
+                        double a = 0.0;
+                        for (int i = 0; i < gsz; i++) a += g[i];
+                        v3[q] = a;
                     }
-                    const double cv = cn < 16.0 ? 1e9 : sqrt(fmax(__ddiv_rn(__dsub_rn(sd2v, __ddiv_rn(__dmul_rn(sdv, sdv), cn)), cn), 0.0));
-                    cost[tid] = cv;
-                    J.costs[tid] = cv;
+                    const double sdv = v3[0], sd2v = v3[1], cn = v3[2];
+                    cost[tid] = cn < 16.0 ? 1e9 : sqrt(fmax(__ddiv_rn(__dsub_rn(sd2v, __ddiv_rn(__dmul_rn(sdv, sdv), cn)), cn), 0.0));
                 }
-                __syncthreads();
-                if (tid == 0) {
-                    __threadfence();
-                    atomicExch(J.bar, 0u);
-                    __threadfence();
-                    atomicAdd(J.bar + 1, 1u);
-                }
-            } else {
-                if (tid == 0) {
-                    volatile unsigned* gen = J.bar + 1;
-                    volatile int* verr = J.ctl;
-                    long long t = 0;
-                    int good = 1;
-                    while (*gen == s_gen) {
-                        if (*verr != 0 || ++t > NM_SPIN_LIMIT) {
-                            good = 0;
-                            break;
-                        }
-                        __nanosleep(32);
-                    }
-                    if (!good) atomicCAS(J.ctl, 0, 1);
-                    __threadfence();
-                    s_ok = good;
-                }
-                __syncthreads();
-                if (!s_ok) return;
-                if (tid < nc) cost[tid] = __ldcg(J.costs + tid);
             }
             __syncthreads();
             if (wid == 0) {
@@ -1148,7 +1139,6 @@ static cudaError_t nm_job(AlignCtx& C, const float* rf, const std::vector<float*
     J.bar = (unsigned*)C.nm_ctl + 2;
     J.ctl = C.nm_ctl;
     J.out = C.nm_out;
-    J.costs = C.nm_out + 8;
     return cudaSuccess;
 }
 static cudaError_t nm_launch(AlignCtx& C, NmJob& J) {

@@ -32,8 +32,8 @@ struct AlignCtx {
     double* sums_host; // pinned, MAX_CAND * 3
     // the search on the device (one cooperative launch per frame)
     double* nm_part;   // device, 2 * MAX_CAND * NM_MAX_BLOCKS * 3
-    int* nm_ctl;       // device, 4: error, evaluations, barrier arrivals and generation
-    double* nm_out;    // device, 8 (the transform) + MAX_CAND (the batch costs)
+    int* nm_ctl;       // device, 4: error, evaluations, barrier arrivals, spare
+    double* nm_out;    // device, 8: the transform
     int device_search = 1;  // 0: the host drives the search, one launch per simplex step
     size_t evals = 0, launches = 0;
 };

@@ -245,7 +245,7 @@ char* lsb_engine_create(const lsb_config* cfg, lsb_engine** out) {
     TRY(cudaHostAlloc((void**)&e->actx.sums_host, sizeof(double) * MAX_CAND * 3, cudaHostAllocDefault));
     TRY(e->pool.get(&e->actx.nm_part, (size_t)2 * MAX_CAND * NM_MAX_BLOCKS * 3));
     TRY(e->pool.get(&e->actx.nm_ctl, 4));
-    TRY(e->pool.get(&e->actx.nm_out, 8 + MAX_CAND));
+    TRY(e->pool.get(&e->actx.nm_out, 8));
     {
         int coop = 0;
         TRY(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, e->cfg.device));
