@@ -219,8 +219,8 @@ __global__ void warp_plane_dev_kernel(const float* __restrict__ src, int w, int 
 // the warped frame's channels (the pixel as shot where the warp leaves the
 // frame) and frame 0's; f64 partials per block, then in order.
 __global__ void bright_kernel(const uint16_t* __restrict__ frames, int w, int h, const BrightXform* __restrict__ xf, int interp,
-                              int nparts, double* __restrict__ part) {
-    const int k = blockIdx.y + 1, pi = blockIdx.x;
+                              int nparts, double* __restrict__ part, int k0) {
+    const int k = k0 + (int)blockIdx.y, pi = blockIdx.x;
     const int gw = (w + 3) / 4, gh = (h + 3) / 4, ng = gw * gh;
     const int per = (ng + nparts - 1) / nparts, lo = pi * per, hi = min(ng, lo + per);
     const uint16_t* f = frames + (size_t)k * w * h * 3;
@@ -402,7 +402,13 @@ cudaError_t bright_sums(const uint16_t* frames, int n, int w, int h, const Brigh
                         cudaStream_t s) {
     if (n < 2) return cudaSuccess;
     dim3 g(nparts, n - 1);
-    lsb_launched(), bright_kernel<<<g, 128, 0, s>>>(frames, w, h, xf_dev, interp, nparts, part);
+    lsb_launched(), bright_kernel<<<g, 128, 0, s>>>(frames, w, h, xf_dev, interp, nparts, part, 1);
+    return cudaGetLastError();
+}
+cudaError_t bright_sums_frame(const uint16_t* frames, int k, int w, int h, const BrightXform* xf_dev, int interp, int nparts, double* part,
+                              cudaStream_t s) {
+    if (k < 1) return cudaSuccess;
+    lsb_launched(), bright_kernel<<<dim3(nparts, 1), 128, 0, s>>>(frames, w, h, xf_dev, interp, nparts, part, k);
     return cudaGetLastError();
 }
 

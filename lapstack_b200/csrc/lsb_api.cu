@@ -77,6 +77,8 @@ struct lsb_engine {
     cudaStream_t cs = nullptr;  // host -> device frame copies, overlapped with the work on s
     cudaEvent_t s_mark = nullptr;  // recorded on s so that cs can wait for the work queued before it
     cudaStream_t bs = nullptr;  // registration targets (luma + pyramid of the next frame) beside the search on s
+    cudaStream_t rs = nullptr;  // read-back of each frame's transform as its search ends
+    cudaStream_t ws = nullptr;  // each aligned frame's warp and brightness sums, behind the registration chain
     DevPool pool;
     unsigned *hist, *sel;
     float* scal;  // [floor, p90, max, ...]
@@ -140,6 +142,12 @@ struct lsb_stack {
     unsigned long long* evals_dev = nullptr;
     int aligned_upto = 0;        // frames already registered (at push time)
     std::vector<cudaEvent_t> copied;  // per frame: its host -> device copy is done
+    // per frame: its search is done (on s), its transform is back in sims_pin (on rs)
+    std::vector<cudaEvent_t> searched, sims_back;
+    double* sims_pin = nullptr;        // page-locked mirror of sims_dev
+    FrameXform* xf_pin = nullptr;      // page-locked: each frame's warp as the streamed warps read it
+    BrightXform* bx_pin = nullptr;
+    cudaEvent_t wdone = nullptr;       // the streamed warps and brightness sums are done (on ws)
     // two target buffers (luma + pyramid), filled on the side stream: frame i+1's while frame i searches
     float* yt2[2] = {nullptr, nullptr};
     std::vector<float*> pt2[2];
@@ -153,6 +161,12 @@ struct lsb_stack {
         wls_destroy(ws);
         if (x0) cudaFree(x0);
         for (auto& v : copied) cudaEventDestroy(v);
+        for (auto& v : searched) cudaEventDestroy(v);
+        for (auto& v : sims_back) cudaEventDestroy(v);
+        if (wdone) cudaEventDestroy(wdone);
+        if (sims_pin) cudaFreeHost(sims_pin);
+        if (xf_pin) cudaFreeHost(xf_pin);
+        if (bx_pin) cudaFreeHost(bx_pin);
         for (int b = 0; b < 2; b++) {
             if (tdone[b]) cudaEventDestroy(tdone[b]);
             if (tfree[b]) cudaEventDestroy(tfree[b]);
@@ -236,6 +250,8 @@ char* lsb_engine_create(const lsb_config* cfg, lsb_engine** out) {
     TRY(cudaStreamCreateWithFlags(&e->cs, cudaStreamNonBlocking));
     TRY(cudaEventCreateWithFlags(&e->s_mark, cudaEventDisableTiming));
     TRY(cudaStreamCreateWithFlags(&e->bs, cudaStreamNonBlocking));
+    TRY(cudaStreamCreateWithFlags(&e->rs, cudaStreamNonBlocking));
+    TRY(cudaStreamCreateWithFlags(&e->ws, cudaStreamNonBlocking));
     TRY(e->pool.get(&e->hist, 65536));
     TRY(e->pool.get(&e->sel, 4));
     TRY(e->pool.get(&e->scal, 16));
@@ -265,6 +281,8 @@ void lsb_engine_destroy(lsb_engine* e) {
     if (e->cs) cudaStreamSynchronize(e->cs), cudaStreamDestroy(e->cs);
     if (e->s_mark) cudaEventDestroy(e->s_mark);
     if (e->bs) cudaStreamSynchronize(e->bs), cudaStreamDestroy(e->bs);
+    if (e->rs) cudaStreamSynchronize(e->rs), cudaStreamDestroy(e->rs);
+    if (e->ws) cudaStreamSynchronize(e->ws), cudaStreamDestroy(e->ws);
     cudaStreamDestroy(e->s);
     delete e;
 }
@@ -383,6 +401,14 @@ static char* stack_alloc(lsb_stack* s) {
         }
         TRY(P.get(&s->warp_dev, 16));
         TRY(P.get(&s->evals_dev, 1));
+        TRY(cudaHostAlloc((void**)&s->sims_pin, sizeof(double) * 8 * N, cudaHostAllocDefault));
+        TRY(cudaHostAlloc((void**)&s->xf_pin, sizeof(FrameXform) * N, cudaHostAllocDefault));
+        TRY(cudaHostAlloc((void**)&s->bx_pin, sizeof(BrightXform) * N, cudaHostAllocDefault));
+        s->searched.assign(N, nullptr);
+        s->sims_back.assign(N, nullptr);
+        for (auto& v : s->searched) TRY(cudaEventCreateWithFlags(&v, cudaEventDisableTiming));
+        for (auto& v : s->sims_back) TRY(cudaEventCreateWithFlags(&v, cudaEventDisableTiming));
+        TRY(cudaEventCreateWithFlags(&s->wdone, cudaEventDisableTiming));
     }
     s->copied.assign(N, nullptr);
     for (auto& v : s->copied) TRY(cudaEventCreateWithFlags(&v, cudaEventDisableTiming));
@@ -560,6 +586,7 @@ static char* align_frame(lsb_stack* s, int i) {
         static const double id[8] = {0, 0, 1, 0, 1, 0, 0, 0};
         TRY(align_chain_begin(C, s->evals_dev));
         TRY(cudaMemcpyAsync(s->sims_dev, id, sizeof id, cudaMemcpyHostToDevice, e->s));
+        TRY(cudaEventRecord(s->searched[0], e->s));
         TRY(luma_u16(f, W, H, s->yr, e->s));
         TRY(gauss_levels(s->yr, W, H, s->pr, e->s));
     } else {
@@ -577,6 +604,7 @@ static char* align_frame(lsb_stack* s, int i) {
         TRY(cudaStreamWaitEvent(e->s, s->tdone[b], 0));
         TRY(multiscale_align_chain(C, s->yr, s->pr, yt, pt, W, H, s->sims_dev + 8 * (size_t)(i - 1), freem, (int)s->ap.coarsen,
                                    s->sims_dev + 8 * (size_t)i, s->warp_dev, s->evals_dev));
+        TRY(cudaEventRecord(s->searched[i], e->s));
         if (i + 1 < n) {
             TRY(warp_plane_dev(yt, W, H, s->warp_dev, (int)s->ap.interp, s->yr, e->s));
             TRY(gauss_levels(s->yr, W, H, s->pr, e->s));
@@ -587,6 +615,8 @@ static char* align_frame(lsb_stack* s, int i) {
     return nullptr;
 }
 
+// Queues the registration of the frames not yet registered; a chained
+// registration then finishes in stream_warps and align_finish.
 static char* run_align(lsb_stack* s) {
     if (chained(s)) {
         // the side stream reads frames the work stream may have written (a device-side fill)
@@ -594,14 +624,61 @@ static char* run_align(lsb_stack* s) {
         TRY(cudaStreamWaitEvent(s->e->bs, s->e->s_mark, 0));
         for (int i = s->aligned_upto; i < (int)s->count; i++)
             if (char* er = align_frame(s, i)) return er;
-        size_t evals = 0;
-        TRY(align_chain_end(s->e->actx, s->evals_dev, &evals));
-        TRY(cudaMemcpy(s->sims.data(), s->sims_dev, sizeof(double) * 8 * s->count, cudaMemcpyDeviceToHost));
-        s->align_evals = evals;
-        s->aligned_upto = 0;  // a later run registers the frames again
         return nullptr;
     }
     return run_align_host(s);
+}
+
+// The chained registration's end: its status and evaluation count.
+static char* align_finish(lsb_stack* s) {
+    size_t evals = 0;
+    TRY(align_chain_end(s->e->actx, s->evals_dev, &evals));
+    s->align_evals = evals;
+    s->aligned_upto = 0;  // a later run registers the frames again
+    return nullptr;
+}
+
+// Each frame's warp (align.rs:489, stack.rs:662-679) and brightness sums
+// (brightness.rs:67) as soon as its search is done, while the chain goes on:
+// the transforms come back on rs behind each search, their matrices are
+// built on the host (align.rs:200-294, as the host path builds them) and the
+// frame's warp and sums are queued on ws. The work stream waits for ws.
+static char* stream_warps(lsb_stack* s) {
+    lsb_engine* e = s->e;
+    const int W = (int)s->w, H = (int)s->h, n = (int)s->count;
+    const size_t np = (size_t)W * H;
+    const bool u16out = s->storage != STORE_F32, bright = s->brightness && n >= 2;
+    for (int i = 0; i < n; i++) {
+        TRY(cudaStreamWaitEvent(e->rs, s->searched[i], 0));
+        TRY(cudaMemcpyAsync(s->sims_pin + 8 * (size_t)i, s->sims_dev + 8 * (size_t)i, sizeof(double) * 8, cudaMemcpyDeviceToHost, e->rs));
+        TRY(cudaEventRecord(s->sims_back[i], e->rs));
+    }
+    for (int i = 0; i < n; i++) {
+        TRY(cudaEventSynchronize(s->sims_back[i]));
+        double* sim = &s->sims[8 * (size_t)i];
+        memcpy(sim, s->sims_pin + 8 * (size_t)i, sizeof(double) * 8);
+        FrameXform& X = s->xf_pin[i];
+        X = FrameXform{};
+        X.warp = !sim_is_id(sim);
+        double m[9];
+        sim_matrix(sim, W, H, m);
+        if (X.warp) mat_inverse(m, X.inv);
+        X.affine = X.inv[6] == 0.0 && X.inv[7] == 0.0 && X.inv[8] == 1.0;
+        TRY(cudaMemcpyAsync(s->xf_dev + i, &X, sizeof X, cudaMemcpyHostToDevice, e->ws));
+        void* out = u16out ? (void*)((uint16_t*)s->warped + (size_t)i * np * 3) : (void*)((float*)s->warped + (size_t)i * np * 3);
+        TRY(warp_frames(s->frames + (size_t)i * np * 3, s->xf_dev + i, (int)s->ap.interp, W, H, 1, u16out, out, e->ws));
+        if (bright && i >= 1) {
+            BrightXform& B = s->bx_pin[i];
+            mat_inverse(m, B.inv);
+            B.ident = sim_is_id(sim);
+            B.affine = B.inv[6] == 0.0 && B.inv[7] == 0.0 && B.inv[8] == 1.0;
+            TRY(cudaMemcpyAsync(s->bx_dev + i, &B, sizeof B, cudaMemcpyHostToDevice, e->ws));
+            TRY(bright_sums_frame(s->frames, i, W, H, s->bx_dev, (int)s->ap.interp, 64, s->bpart, e->ws));
+        }
+    }
+    TRY(cudaEventRecord(s->wdone, e->ws));
+    TRY(cudaStreamWaitEvent(e->s, s->wdone, 0));
+    return nullptr;
 }
 
 static char* run_align_host(lsb_stack* s) {
@@ -658,23 +735,25 @@ static void bratio(const double ref[3], const double frame[3], size_t n, float g
     }
 }
 
-static char* run_gains(lsb_stack* s, bool aligned) {
+static char* run_gains(lsb_stack* s, bool aligned, bool streamed) {
     lsb_engine* e = s->e;
     const int W = (int)s->w, H = (int)s->h, n = (int)s->count;
     for (int k = 0; k < n; k++)
         for (int c = 0; c < 3; c++) s->gains[3 * k + c] = 1.f;
     if (!s->brightness || n < 2 || s->f32src) return nullptr;
     if (aligned) {
-        std::vector<BrightXform> bx(n);
-        for (int k = 0; k < n; k++) {
-            double m[9];
-            sim_matrix(&s->sims[8 * (size_t)k], W, H, m);
-            mat_inverse(m, bx[k].inv);
-            bx[k].ident = sim_is_id(&s->sims[8 * (size_t)k]);
-            bx[k].affine = bx[k].inv[6] == 0.0 && bx[k].inv[7] == 0.0 && bx[k].inv[8] == 1.0;
+        if (!streamed) {  // else stream_warps has queued the sums
+            std::vector<BrightXform> bx(n);
+            for (int k = 0; k < n; k++) {
+                double m[9];
+                sim_matrix(&s->sims[8 * (size_t)k], W, H, m);
+                mat_inverse(m, bx[k].inv);
+                bx[k].ident = sim_is_id(&s->sims[8 * (size_t)k]);
+                bx[k].affine = bx[k].inv[6] == 0.0 && bx[k].inv[7] == 0.0 && bx[k].inv[8] == 1.0;
+            }
+            TRY(cudaMemcpyAsync(s->bx_dev, bx.data(), sizeof(BrightXform) * n, cudaMemcpyHostToDevice, e->s));
+            TRY(bright_sums(s->frames, n, W, H, s->bx_dev, (int)s->ap.interp, 64, s->bpart, e->s));
         }
-        TRY(cudaMemcpyAsync(s->bx_dev, bx.data(), sizeof(BrightXform) * n, cudaMemcpyHostToDevice, e->s));
-        TRY(bright_sums(s->frames, n, W, H, s->bx_dev, (int)s->ap.interp, 64, s->bpart, e->s));
         std::vector<double> part((size_t)n * 64 * 7);
         TRY(cudaMemcpyAsync(part.data(), s->bpart, sizeof(double) * part.size(), cudaMemcpyDeviceToHost, e->s));
         TRY(cudaStreamSynchronize(e->s));
@@ -715,8 +794,14 @@ static char* run_pipeline(lsb_stack* s) {
         if (err) return err;
     }
     TRY(cudaEventRecord(ev[1], st));
+    const bool streamed = aligned && chained(s);
+    if (streamed) {
+        char* err = stream_warps(s);
+        if (!err) err = align_finish(s);
+        if (err) return err;
+    }
     {
-        char* err = run_gains(s, aligned);
+        char* err = run_gains(s, aligned, streamed);
         if (err) return err;
     }
     // per-frame level-0 transforms
@@ -740,7 +825,7 @@ static char* run_pipeline(lsb_stack* s) {
     TRY(cudaMemcpyAsync(s->xf_dev, s->xf.data(), sizeof(FrameXform) * n, cudaMemcpyHostToDevice, st));
     // the aligned frames, written once (align.rs:489 with stack.rs:668's fallback); the fold reads them
     const bool warped = aligned;
-    if (warped) TRY(warp_frames(s->frames, s->xf_dev, (int)s->ap.interp, W, H, n, s->storage != STORE_F32, s->warped, st));
+    if (warped && !streamed) TRY(warp_frames(s->frames, s->xf_dev, (int)s->ap.interp, W, H, n, s->storage != STORE_F32, s->warped, st));
     TRY(cudaMemsetAsync(s->status, 0, sizeof(int), st));
     TRY(cudaEventRecord(ev[2], st));
     // ---- the fold, level by level over all frames
