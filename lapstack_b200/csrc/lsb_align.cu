@@ -256,7 +256,37 @@ __global__ void bright_kernel(const uint16_t* __restrict__ frames, int w, int h,
         for (int q = 0; q < 7; q++) part[((size_t)k * nparts + pi) * 7 + q] = red[q][0];
 }
 
+// brightness.rs:93 `ratio` of frame k from its partials (the host's bratio,
+// operation for operation), with the gain flags and the storage scale.
+__global__ void frame_gain_kernel(const double* __restrict__ part, int k, int nparts, FrameXform* __restrict__ xf) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    double sm[7] = {0, 0, 0, 0, 0, 0, 0};
+    for (int p = 0; p < nparts; p++)
+        for (int q = 0; q < 7; q++) sm[q] += part[((size_t)k * nparts + p) * 7 + q];
+    const size_t cnt = (size_t)sm[6];
+    float maxg = 1.f;
+    int on = 0;
+    for (int c = 0; c < 3; c++) {
+        float g = 1.0f;
+        if (cnt >= 64) {
+            const float v = sm[c] > 1e-9 ? (float)(sm[3 + c] / sm[c]) : 1.0f;
+            g = fminf(fmaxf(v, 0.25f), 4.0f);
+        }
+        xf->gain[c] = g;
+        if (fabsf(g - 1.0f) > 1e-6f) on |= 1 << c;
+        maxg = fmaxf(maxg, g);
+    }
+    xf->gain_on = on;
+    xf->gscale = (float)(65535.0 / maxg);
+    xf->ginv = (float)(maxg / 65535.0);
+}
+
 // ------------------------------------------------------------------- host
+cudaError_t frame_gain(const double* part, int k, int nparts, FrameXform* xf, cudaStream_t s) {
+    lsb_launched(), frame_gain_kernel<<<1, 32, 0, s>>>(part, k, nparts, xf);
+    return cudaGetLastError();
+}
+
 static int gsz(size_t n) { return (int)std::min<size_t>((n + 255) / 256, 148 * 16); }
 
 cudaError_t luma_u16(const uint16_t* f, int w, int h, float* y, cudaStream_t s) {

@@ -638,16 +638,67 @@ static char* align_finish(lsb_stack* s) {
     return nullptr;
 }
 
+// One level's fold arguments (halo control and timing events aside): every
+// frame's REDUCE and the selection.
+static FoldArgs level_args(const lsb_stack* s, int l, bool warped, bool depth_on, bool* focus, int* src) {
+    FoldArgs a{};
+    const int n = (int)s->count;
+    a.level = l;
+    a.nframes = n;
+    a.red_k0 = 0;
+    a.red_n = n;
+    a.select = 1;
+    a.W = s->lw[l];
+    a.H = s->lh[l];
+    a.W1 = s->lw[l + 1];
+    a.H1 = s->lh[l + 1];
+    a.tiles_x = (a.W + 63) / 64;
+    a.tiles_y = (a.H + 31) / 32;
+    a.ntiles = a.tiles_x * a.tiles_y;
+    a.src_u16 = warped && s->storage != STORE_F32 ? (const uint16_t*)s->warped : s->frames;
+    a.src_f32 = warped && s->storage == STORE_F32 ? (const float*)s->warped : s->frames_f32;
+    a.xf = s->xf_dev;
+    a.interp = (int)s->ap.interp;
+    a.src_g = l > 0 ? s->g[l] : nullptr;
+    a.dst_g = s->g[l + 1];
+    a.acc = s->acc[l];
+    a.best = s->best[l];
+    a.winner = l == s->depth_level ? s->winner : nullptr;
+    a.use_chroma = (int)s->fp.use_chroma;
+    a.status = s->status;
+    *focus = depth_on && l == 0;
+    if (*focus) {
+        a.slice = s->slices;
+        a.dw = s->dw;
+        a.dh = s->dh;
+        a.bk = s->bk;
+        a.focus_kind = (int)s->dp.focus;
+        a.sml_step = (int)s->dp.sml_step;
+        a.ntaps = (int)focus_taps(s->dp.r_in, s->dp.r_out).size() / 3;
+        a.rdf13 = s->dp.focus == 0 && s->dp.r_in == 1 && s->dp.r_out == 3;
+    }
+    *src = l > 0 ? SRC_G : ((s->f32src || (warped && s->storage == STORE_F32)) ? SRC_F32 : SRC_U16);
+    return a;
+}
+
 // Each frame's warp (align.rs:489, stack.rs:662-679) and brightness sums
 // (brightness.rs:67) as soon as its search is done, while the chain goes on:
 // the transforms come back on rs behind each search, their matrices are
 // built on the host (align.rs:200-294, as the host path builds them) and the
-// frame's warp and sums are queued on ws. The work stream waits for ws.
-static char* stream_warps(lsb_stack* s) {
+// frame's warp and sums are queued on ws, then its gains (brightness.rs:93)
+// and, with `reduce`, the REDUCE of every pyramid level (pyramid.rs:86, the
+// focus slice at level 0): all that depends on that frame alone. The work
+// stream waits for ws.
+static char* stream_warps(lsb_stack* s, bool reduce) {
     lsb_engine* e = s->e;
     const int W = (int)s->w, H = (int)s->h, n = (int)s->count;
     const size_t np = (size_t)W * H;
     const bool u16out = s->storage != STORE_F32, bright = s->brightness && n >= 2;
+    const bool depth_on = s->dp.enabled != 0;
+    if (depth_on && s->dp.focus == 0) {
+        std::vector<float> taps = focus_taps(s->dp.r_in, s->dp.r_out);
+        TRY(set_focus_taps(taps.data(), (int)(taps.size() / 3), e->ws));
+    }
     for (int i = 0; i < n; i++) {
         TRY(cudaStreamWaitEvent(e->rs, s->searched[i], 0));
         TRY(cudaMemcpyAsync(s->sims_pin + 8 * (size_t)i, s->sims_dev + 8 * (size_t)i, sizeof(double) * 8, cudaMemcpyDeviceToHost, e->rs));
@@ -664,6 +715,9 @@ static char* stream_warps(lsb_stack* s) {
         sim_matrix(sim, W, H, m);
         if (X.warp) mat_inverse(m, X.inv);
         X.affine = X.inv[6] == 0.0 && X.inv[7] == 0.0 && X.inv[8] == 1.0;
+        for (int c = 0; c < 3; c++) X.gain[c] = 1.f;  // frame_gain sets them when brightness is on
+        X.gscale = 65535.f;
+        X.ginv = (float)(1.0 / 65535.0);
         TRY(cudaMemcpyAsync(s->xf_dev + i, &X, sizeof X, cudaMemcpyHostToDevice, e->ws));
         void* out = u16out ? (void*)((uint16_t*)s->warped + (size_t)i * np * 3) : (void*)((float*)s->warped + (size_t)i * np * 3);
         TRY(warp_frames(s->frames + (size_t)i * np * 3, s->xf_dev + i, (int)s->ap.interp, W, H, 1, u16out, out, e->ws));
@@ -674,6 +728,16 @@ static char* stream_warps(lsb_stack* s) {
             B.affine = B.inv[6] == 0.0 && B.inv[7] == 0.0 && B.inv[8] == 1.0;
             TRY(cudaMemcpyAsync(s->bx_dev + i, &B, sizeof B, cudaMemcpyHostToDevice, e->ws));
             TRY(bright_sums_frame(s->frames, i, W, H, s->bx_dev, (int)s->ap.interp, 64, s->bpart, e->ws));
+            TRY(frame_gain(s->bpart, i, 64, s->xf_dev + i, e->ws));
+        }
+        for (int l = 0; l < s->levels && reduce; l++) {
+            bool focus = false;
+            int src = 0;
+            FoldArgs a = level_args(s, l, true, depth_on, &focus, &src);
+            a.red_k0 = i;
+            a.red_n = 1;
+            a.select = 0;
+            TRY(fold_level(a, src, s->storage, (int)s->fp.energy_radius, focus, e->ws, e->grid));
         }
     }
     TRY(cudaEventRecord(s->wdone, e->ws));
@@ -735,25 +799,23 @@ static void bratio(const double ref[3], const double frame[3], size_t n, float g
     }
 }
 
-static char* run_gains(lsb_stack* s, bool aligned, bool streamed) {
+static char* run_gains(lsb_stack* s, bool aligned) {
     lsb_engine* e = s->e;
     const int W = (int)s->w, H = (int)s->h, n = (int)s->count;
     for (int k = 0; k < n; k++)
         for (int c = 0; c < 3; c++) s->gains[3 * k + c] = 1.f;
     if (!s->brightness || n < 2 || s->f32src) return nullptr;
     if (aligned) {
-        if (!streamed) {  // else stream_warps has queued the sums
-            std::vector<BrightXform> bx(n);
-            for (int k = 0; k < n; k++) {
-                double m[9];
-                sim_matrix(&s->sims[8 * (size_t)k], W, H, m);
-                mat_inverse(m, bx[k].inv);
-                bx[k].ident = sim_is_id(&s->sims[8 * (size_t)k]);
-                bx[k].affine = bx[k].inv[6] == 0.0 && bx[k].inv[7] == 0.0 && bx[k].inv[8] == 1.0;
-            }
-            TRY(cudaMemcpyAsync(s->bx_dev, bx.data(), sizeof(BrightXform) * n, cudaMemcpyHostToDevice, e->s));
-            TRY(bright_sums(s->frames, n, W, H, s->bx_dev, (int)s->ap.interp, 64, s->bpart, e->s));
+        std::vector<BrightXform> bx(n);
+        for (int k = 0; k < n; k++) {
+            double m[9];
+            sim_matrix(&s->sims[8 * (size_t)k], W, H, m);
+            mat_inverse(m, bx[k].inv);
+            bx[k].ident = sim_is_id(&s->sims[8 * (size_t)k]);
+            bx[k].affine = bx[k].inv[6] == 0.0 && bx[k].inv[7] == 0.0 && bx[k].inv[8] == 1.0;
         }
+        TRY(cudaMemcpyAsync(s->bx_dev, bx.data(), sizeof(BrightXform) * n, cudaMemcpyHostToDevice, e->s));
+        TRY(bright_sums(s->frames, n, W, H, s->bx_dev, (int)s->ap.interp, 64, s->bpart, e->s));
         std::vector<double> part((size_t)n * 64 * 7);
         TRY(cudaMemcpyAsync(part.data(), s->bpart, sizeof(double) * part.size(), cudaMemcpyDeviceToHost, e->s));
         TRY(cudaStreamSynchronize(e->s));
@@ -789,6 +851,9 @@ static char* run_pipeline(lsb_stack* s) {
     const bool aligned = s->ap.enabled && n > 1 && !s->f32src;
     cudaEvent_t* ev = e->ev;
     TRY(cudaEventRecord(ev[0], st));
+    // Frames registered as they were pushed: the GPU waits on the host copies, so the REDUCEs
+    // fill that time too. Frames already on the device: the REDUCEs would only slow the chain.
+    const bool pushed = s->aligned_upto > 0;
     if (aligned) {
         char* err = run_align(s);
         if (err) return err;
@@ -796,17 +861,23 @@ static char* run_pipeline(lsb_stack* s) {
     TRY(cudaEventRecord(ev[1], st));
     const bool streamed = aligned && chained(s);
     if (streamed) {
-        char* err = stream_warps(s);
+        char* err = stream_warps(s, pushed);
         if (!err) err = align_finish(s);
         if (err) return err;
     }
-    {
-        char* err = run_gains(s, aligned, streamed);
+    if (streamed) {
+        // the transforms, gains and scales the streamed work used
+        s->xf.assign(n, FrameXform{});
+        TRY(cudaMemcpy(s->xf.data(), s->xf_dev, sizeof(FrameXform) * n, cudaMemcpyDeviceToHost));
+        for (int k = 0; k < n; k++)
+            for (int c = 0; c < 3; c++) s->gains[3 * (size_t)k + c] = s->xf[k].gain[c];
+    } else {
+        char* err = run_gains(s, aligned);
         if (err) return err;
     }
     // per-frame level-0 transforms
-    s->xf.assign(n, FrameXform{});
-    for (int k = 0; k < n; k++) {
+    if (!streamed) s->xf.assign(n, FrameXform{});
+    for (int k = 0; k < n && !streamed; k++) {
         FrameXform& X = s->xf[k];
         const double* sim = &s->sims[8 * (size_t)k];
         X.warp = aligned && !sim_is_id(sim);
@@ -817,12 +888,19 @@ static char* run_pipeline(lsb_stack* s) {
         }
         X.affine = X.inv[6] == 0.0 && X.inv[7] == 0.0 && X.inv[8] == 1.0;
         X.gain_on = 0;
+        float maxg = 1.f;
         for (int c = 0; c < 3; c++) {
             X.gain[c] = s->gains[3 * (size_t)k + c];
             if (fabsf(X.gain[c] - 1.0f) > 1e-6f) X.gain_on |= 1 << c;
+            maxg = std::max(maxg, X.gain[c]);
         }
+        // the frame's fixed-point levels span [0, its largest gain]: each is a convex
+        // combination of its gained inputs in [0, 1]
+        if (s->f32src) maxg = 1.f;
+        X.gscale = (float)(65535.0 / maxg);
+        X.ginv = (float)(maxg / 65535.0);
     }
-    TRY(cudaMemcpyAsync(s->xf_dev, s->xf.data(), sizeof(FrameXform) * n, cudaMemcpyHostToDevice, st));
+    if (!streamed) TRY(cudaMemcpyAsync(s->xf_dev, s->xf.data(), sizeof(FrameXform) * n, cudaMemcpyHostToDevice, st));
     // the aligned frames, written once (align.rs:489 with stack.rs:668's fallback); the fold reads them
     const bool warped = aligned;
     if (warped && !streamed) TRY(warp_frames(s->frames, s->xf_dev, (int)s->ap.interp, W, H, n, s->storage != STORE_F32, s->warped, st));
@@ -834,12 +912,6 @@ static char* run_pipeline(lsb_stack* s) {
         std::vector<float> taps = focus_taps(s->dp.r_in, s->dp.r_out);
         TRY(set_focus_taps(taps.data(), (int)(taps.size() / 3), st));
     }
-    // the fixed-point storage spans [0, the largest gain]: every Gaussian level
-    // is a convex combination of gained inputs in [0, 1]
-    float maxg = 1.f;
-    for (float g : s->gains) maxg = std::max(maxg, g);
-    if (s->f32src) maxg = 1.f;
-    const float gscale = (float)(65535.0 / maxg), ginv = (float)(maxg / 65535.0);
     // fuse.rs:120 halo_guide: the guide level and the hardness, when on (fuse.rs:112 HALO_MAX = 8)
     const bool halo = s->fp.halo > 0.f;
     const int guide = std::min((int)s->fp.depth_level, s->levels - 1);
@@ -848,47 +920,16 @@ static char* run_pipeline(lsb_stack* s) {
         for (int l = guide; l <= s->levels; l++) TRY(s->pool.get(&s->halo_w[l], (size_t)s->n * s->lw[l] * s->lh[l]));
     }
     for (int l = 0; l < s->levels; l++) {
-        FoldArgs a{};
-        a.level = l;
+        bool focus = false;
+        int src = 0;
+        FoldArgs a = level_args(s, l, warped, depth_on, &focus, &src);
+        if (streamed && pushed) a.red_n = 0;  // stream_warps has REDUCEd every frame
         if (halo && l >= guide) {
             a.halo_mode = l == guide ? 1 : 2;
             a.halo_p = std::min(s->fp.halo, 8.0f);
             a.halo_w = s->halo_w[l];
             if (l > guide) TRY(reduce_weights(s->halo_w[l - 1], s->lw[l - 1], s->lh[l - 1], n, s->halo_w[l], s->lw[l], s->lh[l], st));
         }
-        a.nframes = n;
-        a.W = s->lw[l];
-        a.H = s->lh[l];
-        a.W1 = s->lw[l + 1];
-        a.H1 = s->lh[l + 1];
-        a.tiles_x = (a.W + 63) / 64;
-        a.tiles_y = (a.H + 31) / 32;
-        a.ntiles = a.tiles_x * a.tiles_y;
-        a.src_u16 = warped && s->storage != STORE_F32 ? (const uint16_t*)s->warped : s->frames;
-        a.src_f32 = warped && s->storage == STORE_F32 ? (const float*)s->warped : s->frames_f32;
-        a.xf = s->xf_dev;
-        a.interp = (int)s->ap.interp;
-        a.src_g = l > 0 ? s->g[l] : nullptr;
-        a.dst_g = s->g[l + 1];
-        a.acc = s->acc[l];
-        a.best = s->best[l];
-        a.winner = l == s->depth_level ? s->winner : nullptr;
-        a.use_chroma = (int)s->fp.use_chroma;
-        a.status = s->status;
-        const bool focus = depth_on && l == 0;
-        if (focus) {
-            a.slice = s->slices;
-            a.dw = s->dw;
-            a.dh = s->dh;
-            a.bk = s->bk;
-            a.focus_kind = (int)s->dp.focus;
-            a.sml_step = (int)s->dp.sml_step;
-            a.ntaps = (int)focus_taps(s->dp.r_in, s->dp.r_out).size() / 3;
-            a.rdf13 = s->dp.focus == 0 && s->dp.r_in == 1 && s->dp.r_out == 3;
-        }
-        a.gscale = gscale;
-        a.ginv = ginv;
-        const int src = l > 0 ? SRC_G : ((s->f32src || (warped && s->storage == STORE_F32)) ? SRC_F32 : SRC_U16);
         a.between = l == 0 ? ev[10] : nullptr;
         if (l == 0) TRY(cudaEventRecord(ev[8], st));
         TRY(fold_level(a, src, s->storage, (int)s->fp.energy_radius, focus, st, e->grid_select > 0 ? e->grid_select : e->grid));
@@ -907,11 +948,11 @@ static char* run_pipeline(lsb_stack* s) {
             // fuse.rs:453-475 below the guide, fuse.rs:505-510 the weighted means
             const int L = s->levels;
             TRY(reduce_weights(s->halo_w[L - 1], s->lw[L - 1], s->lh[L - 1], n, s->halo_w[L], wt, ht, st));
-            TRY(halo_top(s->g[L], s->storage, ginv, s->halo_w[L], n, wt, ht, s->top, s->dev_s, st));
+            TRY(halo_top(s->g[L], s->storage, s->xf_dev, s->halo_w[L], n, wt, ht, s->top, s->dev_s, st));
             TRY(halo_divide(s->top, s->dev_s, wt, ht, st));
             for (int l = guide + 1; l < L; l++) TRY(halo_divide(s->acc[l], s->best[l], s->lw[l], s->lh[l], st));
         } else {
-            ResidualArgs ra{s->g[s->levels], n, wt, ht, (int)s->fp.top_rule, r, (int)s->fp.entropy_bins, s->dev_s, s->ent_s, s->top, ginv};
+            ResidualArgs ra{s->g[s->levels], n, wt, ht, (int)s->fp.top_rule, r, (int)s->fp.entropy_bins, s->dev_s, s->ent_s, s->top, s->xf_dev};
             TRY(fuse_residuals(ra, s->storage, s->lnp, st));
         }
         const float* coarse = s->top;

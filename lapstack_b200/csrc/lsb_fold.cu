@@ -53,7 +53,7 @@ static cudaError_t with_smem(K k, size_t smem) {
     return cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
 }
 
-// One level: REDUCE every frame (and take the focus slices at level 0), then select.
+// One level: REDUCE the frames asked for (and take their focus slices at level 0), then select.
 template <int SRC, class GS, int R, bool FOCUS, class SS>
 static cudaError_t launch_level(const FoldArgs& a, cudaStream_t s, int grid_limit) {
     const size_t rsm = (size_t)RED_FLOATS * sizeof(float), ssm = Staging<SRC, GS, R>::SMEM;
@@ -63,9 +63,9 @@ static cudaError_t launch_level(const FoldArgs& a, cudaStream_t s, int grid_limi
     if (e == cudaSuccess) e = with_smem(ks, ssm);
     if (e != cudaSuccess) return e;
     const int rtiles = ((a.W1 + RW - 1) / RW) * ((a.H1 + RH - 1) / RH);
-    lsb_launched(), kr<<<dim3(rtiles, a.nframes), NT, rsm, s>>>(a);
+    if (a.red_n > 0) lsb_launched(), kr<<<dim3(rtiles, a.red_n), NT, rsm, s>>>(a);
     if (a.between) cudaEventRecord(a.between, s);
-    lsb_launched(), ks<<<std::min(a.ntiles, std::max(grid_limit, 1)), NT, ssm, s>>>(a);
+    if (a.select) lsb_launched(), ks<<<std::min(a.ntiles, std::max(grid_limit, 1)), NT, ssm, s>>>(a);
     return cudaGetLastError();
 }
 
@@ -144,7 +144,7 @@ __global__ void dev_ent_kernel(const ResidualArgs a, const float* __restrict__ l
         const int yy = lsb_reflect(i + dy, a.h);
         for (int dx = -r; dx <= r; dx++) {
             const int o = yy * a.w + lsb_reflect(j + dx, a.w);
-            const float2 sc = make_float2(0.f, a.ginv);
+            const float2 sc = make_float2(0.f, a.xf[k].ginv);
             const float v = lsb_luma(Store<GS>::ld(t + o, sc), Store<GS>::ld(t + n2 + o, sc), Store<GS>::ld(t + 2 * n2 + o, sc));
             s = __fadd_rn(s, v);
             s2 = __fadd_rn(s2, __fmul_rn(v, v));
@@ -176,11 +176,12 @@ __global__ void pareto_kernel(const ResidualArgs a) {
     if (pix >= n2) return;
     float o[3] = {0.f, 0.f, 0.f};
     const GS* t = (const GS*)a.tops;
-    const float2 sc = make_float2(0.f, a.ginv);
     if (a.n == 1 || a.top_rule == 2) {
         const float inv = __fdiv_rn(1.f, (float)a.n);
-        for (int k = 0; k < a.n; k++)
+        for (int k = 0; k < a.n; k++) {
+            const float2 sc = make_float2(0.f, a.xf[k].ginv);
             for (int c = 0; c < 3; c++) o[c] = __fadd_rn(o[c], __fmul_rn(Store<GS>::ld(t + ((size_t)k * 3 + c) * n2 + pix, sc), inv));
+        }
     } else {
         const bool ent = a.top_rule == 0;
         auto dominated = [&](int x) {
@@ -197,8 +198,10 @@ __global__ void pareto_kernel(const ResidualArgs a) {
         for (int x = 0; x < a.n; x++) kept += !dominated(x);
         const float inv = __fdiv_rn(1.f, (float)max(kept, 1));
         for (int x = 0; x < a.n; x++)
-            if (!dominated(x))
+            if (!dominated(x)) {
+                const float2 sc = make_float2(0.f, a.xf[x].ginv);
                 for (int c = 0; c < 3; c++) o[c] = __fadd_rn(o[c], __fmul_rn(Store<GS>::ld(t + ((size_t)x * 3 + c) * n2 + pix, sc), inv));
+            }
     }
     for (int c = 0; c < 3; c++) a.out[(size_t)c * n2 + pix] = o[c];
 }
@@ -240,14 +243,14 @@ cudaError_t reduce_weights(const float* src, int w, int h, int n, float* dst, in
 }
 // fuse.rs:466-470 at the top level: acc = G * w for frame 0, then acc += w * G; best = sum w
 template <class GS>
-__global__ void halo_top_kernel(const GS* __restrict__ tops, float ginv, const float* __restrict__ wts, int n, int w, int h,
-                                float* __restrict__ acc, float* __restrict__ best) {
+__global__ void halo_top_kernel(const GS* __restrict__ tops, const FrameXform* __restrict__ xf, const float* __restrict__ wts, int n, int w,
+                                int h, float* __restrict__ acc, float* __restrict__ best) {
     const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
     if (x >= w || y >= h) return;
     const size_t n2 = (size_t)w * h, o = (size_t)y * w + x;
-    const float2 sc = make_float2(1.f / ginv, ginv);
     float a[3] = {0.f, 0.f, 0.f}, b = 0.f;
     for (int k = 0; k < n; k++) {
+        const float2 sc = make_float2(xf[k].gscale, xf[k].ginv);
         const float wv = wts[(size_t)k * n2 + o];
         for (int c = 0; c < 3; c++) {
             const float g = Store<GS>::ld(tops + ((size_t)k * 3 + c) * n2 + o, sc);
@@ -258,12 +261,12 @@ __global__ void halo_top_kernel(const GS* __restrict__ tops, float ginv, const f
     for (int c = 0; c < 3; c++) acc[c * n2 + o] = a[c];
     best[o] = b;
 }
-cudaError_t halo_top(const void* tops, int storage, float ginv, const float* wts, int n, int w, int h, float* acc, float* best,
+cudaError_t halo_top(const void* tops, int storage, const FrameXform* xf, const float* wts, int n, int w, int h, float* acc, float* best,
                      cudaStream_t s) {
     dim3 b(32, 8), g((w + 31) / 32, (h + 7) / 8);
-    if (storage == STORE_UNORM16) lsb_launched(), halo_top_kernel<unorm16><<<g, b, 0, s>>>((const unorm16*)tops, ginv, wts, n, w, h, acc, best);
-    else if (storage == STORE_F16) lsb_launched(), halo_top_kernel<__half><<<g, b, 0, s>>>((const __half*)tops, ginv, wts, n, w, h, acc, best);
-    else lsb_launched(), halo_top_kernel<float><<<g, b, 0, s>>>((const float*)tops, ginv, wts, n, w, h, acc, best);
+    if (storage == STORE_UNORM16) lsb_launched(), halo_top_kernel<unorm16><<<g, b, 0, s>>>((const unorm16*)tops, xf, wts, n, w, h, acc, best);
+    else if (storage == STORE_F16) lsb_launched(), halo_top_kernel<__half><<<g, b, 0, s>>>((const __half*)tops, xf, wts, n, w, h, acc, best);
+    else lsb_launched(), halo_top_kernel<float><<<g, b, 0, s>>>((const float*)tops, xf, wts, n, w, h, acc, best);
     return cudaGetLastError();
 }
 // fuse.rs:508: the weighted means

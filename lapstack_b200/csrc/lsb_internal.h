@@ -17,7 +17,9 @@ struct FrameXform {
     int warp;      // 1: resample through `inv` (the pixel as shot where it leaves the frame)
     int affine;    // inv's last row is [0, 0, 1] (align.rs:485 `affine_row`)
     int gain_on;   // bit c: multiply channel c by gain[c] (|g - 1| > 1e-6)
-    int pad;
+    // the frame's 16-bit fixed-point level storage: 65535 / max(1, largest gain) and its inverse
+    // (every Gaussian level of the frame is a convex combination of its gained inputs in [0, 1])
+    float gscale, ginv;
 };
 
 enum SrcKind { SRC_U16 = 0, SRC_F32 = 1, SRC_G = 2 };
@@ -48,7 +50,6 @@ struct FoldArgs {
     int ntaps;
     int rdf13;  // the taps are the default ring difference filter (r_in 1, r_out 3)
     int* status;  // device error word
-    float gscale, ginv;  // the 16-bit fixed-point storage's scale and its inverse
     // halo control (fuse.rs:112-136, 453-475): 1 at the guide level (select, and write each frame's
     // weight plane halo_w [n][H][W]); 2 at coarser levels (no selection: acc = sum w*L, best = sum w,
     // frames in order, with halo_w the weights REDUCEd to this level)
@@ -56,6 +57,9 @@ struct FoldArgs {
     float halo_p;
     float* halo_w;
     cudaEvent_t between;  // host side: recorded between the REDUCE and the select launch (may be null)
+    // what one fold_level call launches: the REDUCE of frames red_k0 .. red_k0 + red_n - 1
+    // (none if red_n is 0) and, if select is set, the selection over all frames
+    int red_k0, red_n, select;
 };
 
 // Storage of the Gaussian levels >= 1 and the focus slices.
@@ -70,6 +74,12 @@ cudaError_t warp_frames(const uint16_t* frames, const FrameXform* xf, int interp
 cudaError_t set_focus_taps(const float* taps3, int ntaps, cudaStream_t s);
 size_t fold_smem_bytes(int radius, bool focus);
 
+// brightness.rs:93 `ratio` on the device for frame k: its gains from its
+// brightness partials (part as bright_sums writes them, nparts per frame,
+// summed in order), the gain flags and the frame's fixed-point storage scale,
+// written into *xf (the frame's entry).
+cudaError_t frame_gain(const double* part, int k, int nparts, FrameXform* xf, cudaStream_t s);
+
 // Residual (top) level: fuse.rs:248 `fuse_residuals` over all frames' tops.
 struct ResidualArgs {
     const void* tops;  // [n][3][h][w] storage type
@@ -78,7 +88,7 @@ struct ResidualArgs {
     float* dev;  // scratch [n][h][w]
     float* ent;  // scratch [n][h][w]
     float* out;  // [3][h][w]
-    float ginv;  // fixed-point storage inverse scale
+    const FrameXform* xf;  // per frame: the fixed-point storage's scale
 };
 cudaError_t fuse_residuals(const ResidualArgs& a, int storage, const float* lnp, cudaStream_t s);
 
@@ -91,7 +101,7 @@ cudaError_t collapse_level(const float* acc, const float* coarse, float* out, in
 // top Gaussian level (acc [3][h][w] = sum w*G, best = sum w, frames in order);
 // and the weighted means acc /= best.
 cudaError_t reduce_weights(const float* src, int w, int h, int n, float* dst, int w1, int h1, cudaStream_t s);
-cudaError_t halo_top(const void* tops, int storage, float ginv, const float* wts, int n, int w, int h, float* acc, float* best,
+cudaError_t halo_top(const void* tops, int storage, const FrameXform* xf, const float* wts, int n, int w, int h, float* acc, float* best,
                      cudaStream_t s);
 cudaError_t halo_divide(float* acc, const float* best, int w, int h, cudaStream_t s);
 

@@ -101,7 +101,7 @@ __device__ __forceinline__ void level_px(const FoldArgs& a, int k, int x, int y,
         v[1] = p[np];
         v[2] = p[2 * np];
     } else {
-        const float2 sc = make_float2(a.gscale, a.ginv);
+        const float2 sc = make_float2(a.xf[k].gscale, a.xf[k].ginv);
         const GS* p = (const GS*)a.src_g + (size_t)k * 3 * np + o;
         v[0] = Store<GS>::ld(p, sc);
         v[1] = Store<GS>::ld(p + np, sc);
@@ -195,7 +195,7 @@ __device__ __forceinline__ void reduce_tile(const FoldArgs& a, float* __restrict
     }
     __syncthreads();
     // columns (pyramid.rs:104) -> G_{l+1}
-    const float2 sc = make_float2(a.gscale, a.ginv);
+    const float2 sc = make_float2(a.xf[k].gscale, a.xf[k].ginv);
     for (int i = ty; i < oh; i += 8) {
         const int cy = 2 * (gy0 + i);
         const int r0 = RY(cy - 2) - yw0, r1 = RY(cy - 1) - yw0, r2 = RY(cy) - yw0, r3 = RY(cy + 1) - yw0, r4 = RY(cy + 2) - yw0;
@@ -217,7 +217,7 @@ __global__ void __launch_bounds__(NT, LSB_RED_MINB) reduce_level_kernel(const Fo
     extern __shared__ float sm[];
     const int tiles_x = (a.W1 + RW - 1) / RW;
     const int gx0 = (blockIdx.x % tiles_x) * RW, gy0 = (blockIdx.x / tiles_x) * RH;
-    const int k = blockIdx.y;
+    const int k = a.red_k0 + (int)blockIdx.y;
     const bool interior = 2 * gx0 - FOC_R >= 0 && 2 * gx0 + 2 * RW + FOC_R <= a.W && 2 * gy0 - FOC_R >= 0 &&
                           2 * gy0 + 2 * RH + FOC_R <= a.H;
     if (interior) reduce_tile<SRC, GS, FOCUS, SS, true>(a, sm, k, gx0, gy0);
@@ -243,7 +243,7 @@ __device__ __forceinline__ void select_frame(const FoldArgs& a, float* __restric
     float* exph = g1 + 3 * SEL_G1;       // [3][ah][lw]   EXPAND along rows
     float* yb = exph + 3 * SEL_EXP;      // [lh][lw]      node energy
     const int lw = t.lw, lh = t.lh, aw = t.aw, ah = t.ah;
-    const float2 sc = make_float2(a.gscale, a.ginv);
+    const float2 sc = make_float2(a.xf[k].gscale, a.xf[k].ginv);
 
     // ---- 1: stage G_l and G_{l+1} (STAGED: already in gl / g1 from the async copies)
     if (!STAGED) {
@@ -451,7 +451,7 @@ __device__ __forceinline__ void stage_convert(const FoldArgs& a, int k, const Ti
     const size_t np = (size_t)W * H;
     float* gl = sm;
     float* g1 = gl + 3 * SEL_GL;
-    const float2 sc = make_float2(a.gscale, a.ginv);
+    const float2 sc = make_float2(a.xf[k].gscale, a.xf[k].ginv);
     int gon = 0;
     float gain[3] = {1.f, 1.f, 1.f};
     if (SRC == SRC_U16) {
