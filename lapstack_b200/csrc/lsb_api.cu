@@ -648,6 +648,8 @@ static FoldArgs level_args(const lsb_stack* s, int l, bool warped, bool depth_on
     a.red_k0 = 0;
     a.red_n = n;
     a.select = 1;
+    a.sel_k0 = 0;
+    a.sel_k1 = n;
     a.W = s->lw[l];
     a.H = s->lh[l];
     a.W1 = s->lw[l + 1];
@@ -687,9 +689,12 @@ static FoldArgs level_args(const lsb_stack* s, int l, bool warped, bool depth_on
 // built on the host (align.rs:200-294, as the host path builds them) and the
 // frame's warp and sums are queued on ws, then its gains (brightness.rs:93)
 // and, with `reduce`, the REDUCE of every pyramid level (pyramid.rs:86, the
-// focus slice at level 0): all that depends on that frame alone. The work
-// stream waits for ws.
-static char* stream_warps(lsb_stack* s, bool reduce) {
+// focus slice at level 0): all that depends on that frame alone. With
+// `select` too, every SEL_CHUNK frames the selection of every level folds
+// them in (fuse.rs:414-451, frames in order, resuming from the state the
+// chunk before left). The work stream waits for ws.
+constexpr int SEL_CHUNK = 10;
+static char* stream_warps(lsb_stack* s, bool reduce, bool select) {
     lsb_engine* e = s->e;
     const int W = (int)s->w, H = (int)s->h, n = (int)s->count;
     const size_t np = (size_t)W * H;
@@ -699,6 +704,8 @@ static char* stream_warps(lsb_stack* s, bool reduce) {
         std::vector<float> taps = focus_taps(s->dp.r_in, s->dp.r_out);
         TRY(set_focus_taps(taps.data(), (int)(taps.size() / 3), e->ws));
     }
+    TRY(cudaMemsetAsync(s->status, 0, sizeof(int), e->ws));
+    int sel_from = 0;
     for (int i = 0; i < n; i++) {
         TRY(cudaStreamWaitEvent(e->rs, s->searched[i], 0));
         TRY(cudaMemcpyAsync(s->sims_pin + 8 * (size_t)i, s->sims_dev + 8 * (size_t)i, sizeof(double) * 8, cudaMemcpyDeviceToHost, e->rs));
@@ -738,6 +745,19 @@ static char* stream_warps(lsb_stack* s, bool reduce) {
             a.red_n = 1;
             a.select = 0;
             TRY(fold_level(a, src, s->storage, (int)s->fp.energy_radius, focus, e->ws, e->grid));
+        }
+        if (reduce && select && (i + 1 - sel_from == SEL_CHUNK || i + 1 == n)) {
+            for (int l = 0; l < s->levels; l++) {
+                bool focus = false;
+                int src = 0;
+                FoldArgs a = level_args(s, l, true, depth_on, &focus, &src);
+                a.red_n = 0;
+                a.sel_k0 = sel_from;
+                a.sel_k1 = i + 1;
+                TRY(fold_level(a, src, s->storage, (int)s->fp.energy_radius, focus, e->ws,
+                               e->grid_select > 0 ? e->grid_select : e->grid));
+            }
+            sel_from = i + 1;
         }
     }
     TRY(cudaEventRecord(s->wdone, e->ws));
@@ -860,8 +880,9 @@ static char* run_pipeline(lsb_stack* s) {
     }
     TRY(cudaEventRecord(ev[1], st));
     const bool streamed = aligned && chained(s);
+    const bool sel_streamed = streamed && pushed && !(s->fp.halo > 0.f);  // the selection too (not with halo control)
     if (streamed) {
-        char* err = stream_warps(s, pushed);
+        char* err = stream_warps(s, pushed, sel_streamed);
         if (!err) err = align_finish(s);
         if (err) return err;
     }
@@ -904,7 +925,7 @@ static char* run_pipeline(lsb_stack* s) {
     // the aligned frames, written once (align.rs:489 with stack.rs:668's fallback); the fold reads them
     const bool warped = aligned;
     if (warped && !streamed) TRY(warp_frames(s->frames, s->xf_dev, (int)s->ap.interp, W, H, n, s->storage != STORE_F32, s->warped, st));
-    TRY(cudaMemsetAsync(s->status, 0, sizeof(int), st));
+    if (!streamed) TRY(cudaMemsetAsync(s->status, 0, sizeof(int), st));  // else stream_warps cleared it
     TRY(cudaEventRecord(ev[2], st));
     // ---- the fold, level by level over all frames
     const bool depth_on = s->dp.enabled != 0;
@@ -919,7 +940,9 @@ static char* run_pipeline(lsb_stack* s) {
         s->halo_w.assign(s->levels + 1, nullptr);
         for (int l = guide; l <= s->levels; l++) TRY(s->pool.get(&s->halo_w[l], (size_t)s->n * s->lw[l] * s->lh[l]));
     }
-    for (int l = 0; l < s->levels; l++) {
+    if (sel_streamed)  // the level-0 timings of a fold that ran on ws: none here
+        for (int q : {8, 10, 9}) TRY(cudaEventRecord(ev[q], st));
+    for (int l = 0; l < s->levels && !sel_streamed; l++) {
         bool focus = false;
         int src = 0;
         FoldArgs a = level_args(s, l, warped, depth_on, &focus, &src);

@@ -58,8 +58,9 @@ struct FoldArgs {
     float* halo_w;
     cudaEvent_t between;  // host side: recorded between the REDUCE and the select launch (may be null)
     // what one fold_level call launches: the REDUCE of frames red_k0 .. red_k0 + red_n - 1
-    // (none if red_n is 0) and, if select is set, the selection over all frames
-    int red_k0, red_n, select;
+    // (none if red_n is 0) and, if select is set, the selection over frames sel_k0 .. sel_k1 - 1
+    // (from sel_k0 > 0 it resumes from the acc / best / winner the frames before it left)
+    int red_k0, red_n, select, sel_k0, sel_k1;
 };
 
 // Storage of the Gaussian levels >= 1 and the focus slices.

@@ -526,6 +526,15 @@ __global__ void __launch_bounds__(NT, LSB_SEL_MINB) select_level_kernel(const Fo
             best[j] = -1.f;  // any energy (>= 0) beats it: frame 0 fills the accumulator (fuse.rs:409-412)
             acc[j][0] = acc[j][1] = acc[j][2] = 0.f;
             win[j] = 0;
+            const int px = tx + 32 * (j & 1), py = ty + 8 * (j >> 1);
+            if (a.sel_k0 > 0 && px < t.ox1 && py < t.oy1) {  // resume: the state the frames before left
+                const size_t o = (size_t)(t.y0 + py) * W + t.x0 + px;
+                acc[j][0] = a.acc[o];
+                acc[j][1] = a.acc[(size_t)W * H + o];
+                acc[j][2] = a.acc[2 * (size_t)W * H + o];
+                best[j] = a.best[o];
+                if (a.winner) win[j] = a.winner[o];
+            }
         }
         using S = Staging<SRC, GS, R>;
         if (S::ON && interior) {
@@ -534,12 +543,12 @@ __global__ void __launch_bounds__(NT, LSB_SEL_MINB) select_level_kernel(const Fo
                 return;
             }
             uint32_t* raw = (uint32_t*)(sm + SEL_FLOATS);
-            stage_issue<SRC, GS, R>(a, 0, t, raw);
+            stage_issue<SRC, GS, R>(a, a.sel_k0, t, raw);
             cp_async_commit();
-            for (int k = 0; k < a.nframes; k++) {
-                uint32_t* cur = raw + (k & 1) * S::WORDS;
-                if (k + 1 < a.nframes) {
-                    stage_issue<SRC, GS, R>(a, k + 1, t, raw + ((k + 1) & 1) * S::WORDS);
+            for (int k = a.sel_k0; k < a.sel_k1; k++) {
+                uint32_t* cur = raw + ((k - a.sel_k0) & 1) * S::WORDS;
+                if (k + 1 < a.sel_k1) {
+                    stage_issue<SRC, GS, R>(a, k + 1, t, raw + ((k + 1 - a.sel_k0) & 1) * S::WORDS);
                     cp_async_commit();
                     cp_async_wait<1>();
                 } else {
@@ -551,7 +560,7 @@ __global__ void __launch_bounds__(NT, LSB_SEL_MINB) select_level_kernel(const Fo
                 select_frame<SRC, GS, R, true, true>(a, sm, k, t, best, acc, win);
             }
         } else {
-            for (int k = 0; k < a.nframes; k++) {
+            for (int k = a.sel_k0; k < a.sel_k1; k++) {
                 if (interior) select_frame<SRC, GS, R, true>(a, sm, k, t, best, acc, win);
                 else select_frame<SRC, GS, R, false>(a, sm, k, t, best, acc, win);
             }

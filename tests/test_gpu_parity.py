@@ -258,6 +258,35 @@ def test_aligned_stack_matches_oracle():
     assert frac <= 1e-3
 
 
+@pytest.mark.parametrize("storage", ["f32", "unorm16"])
+def test_pushed_stack_streams_the_same_result(storage):
+    """Pushed frames are warped, gained, REDUCEd and folded (in chunks of 10
+    frames, each resuming the selection state the one before left) on a side
+    stream as their transforms land; the same frames folded from device memory
+    in one pass give the same result. Frames of uneven brightness exercise the
+    per-frame gains and storage scales; against the oracle too (FP32 storage)."""
+    n = 23
+    fr, _ = L.synth_stack(L.SynthSpec(192, 144, n, warp=True, mag_step=0.004, seed=29))
+    fr = np.stack([np.clip(f.astype(np.float64) * (1.0 - 0.03 * (k % 5)), 0, 65535).astype(np.uint16) for k, f in enumerate(fr)])
+    st = L.Engine(storage=storage).stack(192, 144, n, L.FuseParams(), L.AlignParams(coarsen=1), L.DepthParams(), brightness=True)
+    for f in fr:
+        st.push_u16(f)
+    pushed = st.finish()
+    st.set_count(n)  # the same frames, already on the device: one pass after the registration
+    resident = st.finish()
+    assert np.array_equal(pushed.align, resident.align)
+    assert_same(pushed.gains, resident.gains, "gains")
+    assert np.unique(pushed.gains).size > 1
+    assert_same(pushed.winner, resident.winner, "winner map")
+    assert_same(pushed.image_u16, resident.image_u16, "fused u16")
+    assert_same(pushed.depth.depth, resident.depth.depth, "depth")
+    if storage == "f32":
+        ref = O.run_stack(fr, O.StackParams(align=O.AlignParams(coarsen=1), depth=None))
+        assert np.max(np.abs(pushed.align - ref.sims)) < 1e-9
+        assert_same(ref.gains, pushed.gains, "gains vs oracle")
+        assert_same(ref.image_u16, pushed.image_u16, "fused u16 vs oracle")
+
+
 @pytest.mark.parametrize("model", ["similarity", "affine"])
 def test_device_search_matches_host_search(model):
     """The one-launch search on the device and the host-driven one take the
