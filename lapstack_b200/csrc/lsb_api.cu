@@ -156,6 +156,8 @@ struct lsb_stack {
     lsb_unet* net = nullptr;  // learned warm start of the solves (not owned)
     float* x0 = nullptr;      // its prediction on the depth grid
     float* winner_full = nullptr;  // the winner map at full size (finish)
+    lsb_result* early = nullptr;   // finish: the result whose fused planes leave on rs while the depth runs
+    cudaEvent_t fused_ev = nullptr;  // recorded on s once the fused planes and the winner map are written
     size_t x0_cells = 0;
     ~lsb_stack() {
         wls_destroy(ws);
@@ -164,6 +166,7 @@ struct lsb_stack {
         for (auto& v : searched) cudaEventDestroy(v);
         for (auto& v : sims_back) cudaEventDestroy(v);
         if (wdone) cudaEventDestroy(wdone);
+        if (fused_ev) cudaEventDestroy(fused_ev);
         if (sims_pin) cudaFreeHost(sims_pin);
         if (xf_pin) cudaFreeHost(xf_pin);
         if (bx_pin) cudaFreeHost(bx_pin);
@@ -988,6 +991,19 @@ static char* run_pipeline(lsb_stack* s) {
     }
     TRY(cudaEventRecord(ev[4], st));
     s->folded = true;
+    if (lsb_result* r = s->early) {
+        // the fused planes and the winner map go back on rs while the depth pass runs on s
+        const int dl = s->depth_level;
+        if (!s->winner_full) TRY(s->pool.get(&s->winner_full, (size_t)W * H));
+        if (!s->fused_ev) TRY(cudaEventCreateWithFlags(&s->fused_ev, cudaEventDisableTiming));
+        TRY(upsample_index(s->winner, s->lw[dl], s->lh[dl], 1 << dl, W, H, s->winner_full, st));
+        TRY(cudaEventRecord(s->fused_ev, st));
+        TRY(cudaStreamWaitEvent(e->rs, s->fused_ev, 0));
+        const size_t np = (size_t)W * H;
+        TRY(cudaMemcpyAsync(r->image_u16, s->img_u16, sizeof(uint16_t) * 3 * np, cudaMemcpyDeviceToHost, e->rs));
+        TRY(cudaMemcpyAsync(r->image_f32, s->img, sizeof(float) * 3 * np, cudaMemcpyDeviceToHost, e->rs));
+        TRY(cudaMemcpyAsync(r->winner, s->winner_full, sizeof(float) * np, cudaMemcpyDeviceToHost, e->rs));
+    }
     // ---- depth
     if (depth_on) {
         const int k = s->bk, dw = s->dw, dh = s->dh;
@@ -1233,26 +1249,27 @@ static void hb_release(void* p) {
 extern "C" char* lsb_stack_finish(lsb_stack* s, lsb_result* r) {
     if (!s || !r) return dup_err("null argument");
     memset(r, 0, sizeof *r);
-    char* err = run_pipeline(s);
-    if (err) return err;
-    const size_t W = s->w, H = s->h, N = s->count;
+    const size_t W = s->w, H = s->h;
     cudaStream_t st = s->e->s;
+    r->image_u16 = (uint16_t*)hb_get(sizeof(uint16_t) * 3 * W * H);
+    r->image_f32 = (float*)hb_get(sizeof(float) * 3 * W * H);
+    r->winner = (float*)hb_get(sizeof(float) * W * H);
+    s->early = r;  // run_pipeline sends the fused planes back as soon as they exist
+    char* err = run_pipeline(s);
+    s->early = nullptr;
+    if (err) {
+        cudaStreamSynchronize(s->e->rs);
+        lsb_result_free(r);
+        return err;
+    }
+    const size_t N = s->count;
     r->w = s->w;
     r->h = s->h;
     r->n_frames = s->count;
     r->levels = s->levels;
-    r->image_u16 = (uint16_t*)hb_get(sizeof(uint16_t) * 3 * W * H);
-    r->image_f32 = (float*)hb_get(sizeof(float) * 3 * W * H);
-    r->winner = (float*)hb_get(sizeof(float) * W * H);
     r->sims = (double*)malloc(sizeof(double) * 8 * N);
     r->gains = (float*)malloc(sizeof(float) * 3 * N);
     r->shares = (float*)malloc(sizeof(float) * N);
-    TRY(cudaMemcpyAsync(r->image_u16, s->img_u16, sizeof(uint16_t) * 3 * W * H, cudaMemcpyDeviceToHost, st));
-    TRY(cudaMemcpyAsync(r->image_f32, s->img, sizeof(float) * 3 * W * H, cudaMemcpyDeviceToHost, st));
-    const int dl = s->depth_level, dwl = s->lw[dl], dhl = s->lh[dl];
-    if (!s->winner_full) TRY(s->pool.get(&s->winner_full, W * H));
-    TRY(upsample_index(s->winner, dwl, dhl, 1 << dl, (int)W, (int)H, s->winner_full, st));
-    TRY(cudaMemcpyAsync(r->winner, s->winner_full, sizeof(float) * W * H, cudaMemcpyDeviceToHost, st));
     if (s->dp.enabled) {
         const size_t m = (size_t)s->dw * s->dh;
         r->dw = s->dw;
@@ -1265,6 +1282,7 @@ extern "C" char* lsb_stack_finish(lsb_stack* s, lsb_result* r) {
         TRY(cudaMemcpyAsync(r->floor_cells, s->mins, sizeof(float) * m, cudaMemcpyDeviceToHost, st));
     }
     TRY(cudaStreamSynchronize(st));
+    TRY(cudaStreamSynchronize(s->e->rs));
     memcpy(r->sims, s->sims.data(), sizeof(double) * 8 * N);
     memcpy(r->gains, s->gains.data(), sizeof(float) * 3 * N);
     err = shares_of(s, r->shares);
