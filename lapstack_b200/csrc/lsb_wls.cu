@@ -343,9 +343,129 @@ __global__ void __launch_bounds__(32) thomas_kernel(float* __restrict__ u, const
     }
     cp_wait<0>();
 }
+// The same systems (depth.rs:677 / :707), each line cut into P segments
+// (the partition method); a warp per segment holds 32 lines (lane = line).
+// (1) Each segment eliminates forward (pivots d', the spike g on the unknown
+// before the segment, the right-hand side r') and backward, leaving each of
+// its unknowns as rho + sigma * X_{s-1} + tau * X_s, X_s being the segment's
+// last unknown. (2) One thread per line solves the P-unknown tridiagonal
+// system that the segments' last equations make of the X_s. (3) Each segment
+// recovers its unknowns. A line's sequential chain shrinks P-fold and P times
+// as many threads run the lines; the result differs from the one-thread
+// Thomas sweep by rounding only (the systems are diagonally dominant), and
+// these sweeps only start the MG-PCG solve.
+template <bool ROWS, int P>
+__global__ void __launch_bounds__(32 * P) pthomas_kernel(float* __restrict__ u, const float* __restrict__ f, const float* __restrict__ wd,
+                                                         int unit_wd, const float* __restrict__ a, int w, int h, float lam,
+                                                         float* __restrict__ s0, float* __restrict__ s1, float* __restrict__ s2) {
+    __shared__ float cf[P][7][32];  // per segment and line: the first unknown's (rho, sigma, tau); the last equation's d', g, r', u
+    __shared__ float X[P][32];      // the segments' last unknowns
+    __shared__ float rc[P][32], rr[P][32];
+    const int lane = threadIdx.x & 31, seg = threadIdx.x >> 5;
+    const int nlines = ROWS ? h : w, len = ROWS ? w : h;
+    const int line = blockIdx.x * 32 + lane;
+    const bool live = line < nlines;
+    const int b = (int)((long long)seg * len / P), e = (int)((long long)(seg + 1) * len / P);  // len >= P: never empty
+    auto at = [&](int i) -> size_t { return ROWS ? (size_t)line * w + i : (size_t)i * w + line; };
+    const float nl = -lam;
+    if (live) {
+        float a_prev = b > 0 ? a[at(b - 1)] : 0.f;
+        float dprev = 1.f, gprev = 0.f, rprev = 0.f, uprev = 0.f;
+        for (int i = b; i < e; i++) {
+            const size_t k = at(i);
+            const float ai = i + 1 < len ? a[k] : 0.f;
+            const float wdi = unit_wd ? 1.f : wd[k];
+            const float diag = wdi + lam * (a_prev + ai);
+            const float lower = nl * a_prev, upper = nl * ai;
+            const float ri = wdi * f[k];
+            float dd = diag, gg = lower, rv = ri;
+            if (i > b) {
+                const float mlt = lower / dprev;
+                dd = diag - mlt * uprev;
+                gg = -(mlt * gprev);
+                rv = ri - mlt * rprev;
+            }
+            if (fabsf(dd) < 1e-12f) dd = 1e-12f;
+            s0[k] = dd;
+            s1[k] = gg;
+            s2[k] = rv;
+            dprev = dd;
+            gprev = gg;
+            rprev = rv;
+            uprev = upper;
+            a_prev = ai;
+        }
+        cf[seg][3][lane] = dprev;
+        cf[seg][4][lane] = gprev;
+        cf[seg][5][lane] = rprev;
+        cf[seg][6][lane] = uprev;
+        float rn = 0.f, sn = 0.f, tn = 1.f;  // the last unknown is X_s itself
+        {
+            const size_t k = at(e - 1);
+            s0[k] = 0.f;
+            s1[k] = 0.f;
+            s2[k] = 1.f;
+        }
+        for (int i = e - 2; i >= b; i--) {
+            const size_t k = at(i);
+            const float upper = nl * a[k];  // i + 1 < len here
+            const float inv = 1.f / s0[k];
+            const float rho = (s2[k] - upper * rn) * inv, sig = (-s1[k] - upper * sn) * inv, tau = -(upper * tn) * inv;
+            s0[k] = rho;
+            s1[k] = sig;
+            s2[k] = tau;
+            rn = rho;
+            sn = sig;
+            tn = tau;
+        }
+        cf[seg][0][lane] = rn;
+        cf[seg][1][lane] = sn;
+        cf[seg][2][lane] = tn;
+    }
+    __syncthreads();
+    if (seg == 0 && live) {
+        // segment q's last equation: g X_{q-1} + d' X_q + u x_first(q+1) = r', x_first(q+1) = rho + sigma X_q + tau X_{q+1}
+        float cprev = 0.f, rprev2 = 0.f;
+        for (int q = 0; q < P; q++) {
+            const bool nx = q + 1 < P;
+            const float uq = cf[q][6][lane];
+            const float A = q > 0 ? cf[q][4][lane] : 0.f;
+            const float B = nx ? cf[q][3][lane] + uq * cf[q + 1][1][lane] : cf[q][3][lane];
+            const float C = nx ? uq * cf[q + 1][2][lane] : 0.f;
+            const float R = nx ? cf[q][5][lane] - uq * cf[q + 1][0][lane] : cf[q][5][lane];
+            float den = B - A * cprev;
+            if (fabsf(den) < 1e-12f) den = 1e-12f;
+            cprev = C / den;
+            rprev2 = (R - A * rprev2) / den;
+            rc[q][lane] = cprev;
+            rr[q][lane] = rprev2;
+        }
+        float xn = 0.f;
+        for (int q = P - 1; q >= 0; q--) {
+            xn = q == P - 1 ? rr[q][lane] : rr[q][lane] - rc[q][lane] * xn;
+            X[q][lane] = xn;
+        }
+    }
+    __syncthreads();
+    if (live) {
+        const float xl = seg > 0 ? X[seg - 1][lane] : 0.f, xs = X[seg][lane];
+        for (int i = b; i < e; i++) {
+            const size_t k = at(i);
+            u[k] = s0[k] + s1[k] * xl + s2[k] * xs;
+        }
+    }
+}
+constexpr int PT_ROWS = 8, PT_COLS = 16;
+
 static void thomas(bool rows, float* u, const float* f, const float* wd, int unit_wd, const float* a, int w, int h, float lam,
-                   float* cp, float* dp, cudaStream_t s) {
-    const int nlines = rows ? h : w;
+                   float* cp, float* dp, float* sc, cudaStream_t s) {
+    const int nlines = rows ? h : w, len = rows ? w : h;
+    if (sc && len >= (rows ? PT_ROWS : PT_COLS) * 8) {
+        const int g = (nlines + 31) / 32;
+        if (rows) lsb_launched(), pthomas_kernel<true, PT_ROWS><<<g, 32 * PT_ROWS, 0, s>>>(u, f, wd, unit_wd, a, w, h, lam, cp, dp, sc);
+        else lsb_launched(), pthomas_kernel<false, PT_COLS><<<g, 32 * PT_COLS, 0, s>>>(u, f, wd, unit_wd, a, w, h, lam, cp, dp, sc);
+        return;
+    }
     if (rows) lsb_launched(), thomas_kernel<true><<<(nlines + TT - 1) / TT, TT, 0, s>>>(u, f, wd, unit_wd, a, w, h, lam, cp, dp);
     else lsb_launched(), thomas_kernel<false><<<(nlines + TT - 1) / TT, TT, 0, s>>>(u, f, wd, unit_wd, a, w, h, lam, cp, dp);
 }
@@ -624,8 +744,8 @@ cudaError_t wls_solve(WlsSolver* S, const float* d, int max_iters, float* u, flo
     const size_t n = (size_t)w * h;
     WlsLevel& L0 = S->lv[0];
     if (w == 1 || h == 1) {
-        if (h == 1) thomas(true, u, d, L0.wd, 0, S->ex, w, h, S->lambda, S->cp, S->dp, s);
-        else thomas(false, u, d, L0.wd, 0, S->ey, w, h, S->lambda, S->cp, S->dp, s);
+        if (h == 1) thomas(true, u, d, L0.wd, 0, S->ex, w, h, S->lambda, S->cp, S->dp, nullptr, s);
+        else thomas(false, u, d, L0.wd, 0, S->ey, w, h, S->lambda, S->cp, S->dp, nullptr, s);
         *rel_out = 0.f;
         *iters_out = 0;
         if (rel64) *rel64 = 0.0;
@@ -638,9 +758,9 @@ cudaError_t wls_solve(WlsSolver* S, const float* d, int max_iters, float* u, flo
             float p4 = 1.f;
             for (int q = 0; q < 3 - t; q++) p4 *= 4.f;
             const float lam_t = (1.5f * S->lambda * p4) / (64.f - 1.f);
-            thomas(true, u, S->f, L0.wd, t == 1 ? 0 : 1, S->ex, w, h, lam_t, S->cp, S->dp, s);
+            thomas(true, u, S->f, L0.wd, t == 1 ? 0 : 1, S->ex, w, h, lam_t, S->cp, S->dp, S->z, s);
             cudaMemcpyAsync(S->f, u, n * sizeof(float), cudaMemcpyDeviceToDevice, s);
-            thomas(false, u, S->f, L0.wd, 1, S->ey, w, h, lam_t, S->cp, S->dp, s);
+            thomas(false, u, S->f, L0.wd, 1, S->ey, w, h, lam_t, S->cp, S->dp, S->z, s);
             cudaMemcpyAsync(S->f, u, n * sizeof(float), cudaMemcpyDeviceToDevice, s);
         }
     }
