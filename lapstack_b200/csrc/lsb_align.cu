@@ -217,52 +217,64 @@ __global__ void warp_plane_dev_kernel(const float* __restrict__ src, int w, int 
 // brightness.rs:67 `sums` of every aligned frame against frame 0: over the
 // stride-4 grid points that the frame's map (align.rs:291) keeps inside,
 // the warped frame's channels (the pixel as shot where the warp leaves the
-// frame) and frame 0's; f64 partials per block, then in order.
+// frame) and frame 0's; f64 partials per part of the grid points, then in
+// order. A block takes parts blockIdx.x, + gridDim.x, ...: the partials do
+// not depend on how many blocks run.
 __global__ void bright_kernel(const uint16_t* __restrict__ frames, int w, int h, const BrightXform* __restrict__ xf, int interp,
                               int nparts, double* __restrict__ part, int k0) {
-    const int k = k0 + (int)blockIdx.y, pi = blockIdx.x;
+    const int k = k0 + (int)blockIdx.y;
     const int gw = (w + 3) / 4, gh = (h + 3) / 4, ng = gw * gh;
-    const int per = (ng + nparts - 1) / nparts, lo = pi * per, hi = min(ng, lo + per);
     const uint16_t* f = frames + (size_t)k * w * h * 3;
     const BrightXform X = xf[k];
-    double s[7] = {0, 0, 0, 0, 0, 0, 0};
-    for (int g = lo + threadIdx.x; g < hi; g += blockDim.x) {
-        const int x = (g % gw) * 4, y = (g / gw) * 4;
-        if (!X.ident) {
-            const double* m = X.inv;
-            const double d = __dadd_rn(__dadd_rn(__dmul_rn(m[6], (double)x), __dmul_rn(m[7], (double)y)), m[8]);
-            const double sx = __ddiv_rn(__dadd_rn(__dadd_rn(__dmul_rn(m[0], (double)x), __dmul_rn(m[1], (double)y)), m[2]), d);
-            const double sy = __ddiv_rn(__dadd_rn(__dadd_rn(__dmul_rn(m[3], (double)x), __dmul_rn(m[4], (double)y)), m[5]), d);
-            if (!(sx >= 0.0 && sx <= (double)(w - 1) && sy >= 0.0 && sy <= (double)(h - 1))) continue;
-        }
-        float v[3];
-        load_px_core(f, X.inv, !X.ident, X.affine, interp, w, h, x, y, v);
-        const uint16_t* r = frames + ((size_t)y * w + x) * 3;
-        for (int c = 0; c < 3; c++) {
-            s[c] += (double)v[c];
-            s[3 + c] += (double)__fmul_rn((float)r[c], LSB_INV16);
-        }
-        s[6] += 1.0;
-    }
     __shared__ double red[7][128];
-    for (int q = 0; q < 7; q++) red[q][threadIdx.x] = s[q];
-    __syncthreads();
-    for (int st = blockDim.x / 2; st > 0; st >>= 1) {
-        if (threadIdx.x < st)
-            for (int q = 0; q < 7; q++) red[q][threadIdx.x] += red[q][threadIdx.x + st];
+    for (int pi = blockIdx.x; pi < nparts; pi += gridDim.x) {
+        const int per = (ng + nparts - 1) / nparts, lo = pi * per, hi = min(ng, lo + per);
+        double s[7] = {0, 0, 0, 0, 0, 0, 0};
+        for (int g = lo + threadIdx.x; g < hi; g += blockDim.x) {
+            const int x = (g % gw) * 4, y = (g / gw) * 4;
+            if (!X.ident) {
+                const double* m = X.inv;
+                const double d = __dadd_rn(__dadd_rn(__dmul_rn(m[6], (double)x), __dmul_rn(m[7], (double)y)), m[8]);
+                const double sx = __ddiv_rn(__dadd_rn(__dadd_rn(__dmul_rn(m[0], (double)x), __dmul_rn(m[1], (double)y)), m[2]), d);
+                const double sy = __ddiv_rn(__dadd_rn(__dadd_rn(__dmul_rn(m[3], (double)x), __dmul_rn(m[4], (double)y)), m[5]), d);
+                if (!(sx >= 0.0 && sx <= (double)(w - 1) && sy >= 0.0 && sy <= (double)(h - 1))) continue;
+            }
+            float v[3];
+            load_px_core(f, X.inv, !X.ident, X.affine, interp, w, h, x, y, v);
+            const uint16_t* r = frames + ((size_t)y * w + x) * 3;
+            for (int c = 0; c < 3; c++) {
+                s[c] += (double)v[c];
+                s[3 + c] += (double)__fmul_rn((float)r[c], LSB_INV16);
+            }
+            s[6] += 1.0;
+        }
+        for (int q = 0; q < 7; q++) red[q][threadIdx.x] = s[q];
         __syncthreads();
+        for (int st = blockDim.x / 2; st > 0; st >>= 1) {
+            if (threadIdx.x < st)
+                for (int q = 0; q < 7; q++) red[q][threadIdx.x] += red[q][threadIdx.x + st];
+            __syncthreads();
+        }
+        if (threadIdx.x == 0)
+            for (int q = 0; q < 7; q++) part[((size_t)k * nparts + pi) * 7 + q] = red[q][0];
+        __syncthreads();  // red is reused by the next part
     }
-    if (threadIdx.x == 0)
-        for (int q = 0; q < 7; q++) part[((size_t)k * nparts + pi) * 7 + q] = red[q][0];
 }
 
 // brightness.rs:93 `ratio` of frame k from its partials (the host's bratio,
 // operation for operation), with the gain flags and the storage scale.
 __global__ void frame_gain_kernel(const double* __restrict__ part, int k, int nparts, FrameXform* __restrict__ xf) {
+    __shared__ double ssum[7];
+    if (threadIdx.x < 7) {  // one sum per thread, over the blocks in order
+        const int q = threadIdx.x;
+        double v = 0.0;
+        for (int p = 0; p < nparts; p++) v += part[((size_t)k * nparts + p) * 7 + q];
+        ssum[q] = v;
+    }
+    __syncthreads();
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
-    double sm[7] = {0, 0, 0, 0, 0, 0, 0};
-    for (int p = 0; p < nparts; p++)
-        for (int q = 0; q < 7; q++) sm[q] += part[((size_t)k * nparts + p) * 7 + q];
+    double sm[7];
+    for (int q = 0; q < 7; q++) sm[q] = ssum[q];
     const size_t cnt = (size_t)sm[6];
     float maxg = 1.f;
     int on = 0;
@@ -436,9 +448,9 @@ cudaError_t bright_sums(const uint16_t* frames, int n, int w, int h, const Brigh
     return cudaGetLastError();
 }
 cudaError_t bright_sums_frame(const uint16_t* frames, int k, int w, int h, const BrightXform* xf_dev, int interp, int nparts, double* part,
-                              cudaStream_t s) {
+                              int blocks, cudaStream_t s) {
     if (k < 1) return cudaSuccess;
-    lsb_launched(), bright_kernel<<<dim3(nparts, 1), 128, 0, s>>>(frames, w, h, xf_dev, interp, nparts, part, k);
+    lsb_launched(), bright_kernel<<<dim3(std::min(std::max(blocks, 1), nparts), 1), 128, 0, s>>>(frames, w, h, xf_dev, interp, nparts, part, k);
     return cudaGetLastError();
 }
 

@@ -44,9 +44,9 @@ cudaError_t gauss_levels(const float* y, int w, int h, const std::vector<float*>
 cudaError_t warp_plane(const float* src, int w, int h, const WarpXform& xf, float* out, cudaStream_t s);
 cudaError_t bright_sums(const uint16_t* frames, int n, int w, int h, const BrightXform* xf_dev, int interp, int nparts, double* part,
                         cudaStream_t s);
-// The same for frame k alone (k >= 1): its partials land where bright_sums puts them.
+// The same for frame k alone (k >= 1) on `blocks` blocks: its partials land where bright_sums puts them.
 cudaError_t bright_sums_frame(const uint16_t* frames, int k, int w, int h, const BrightXform* xf_dev, int interp, int nparts, double* part,
-                              cudaStream_t s);
+                              int blocks, cudaStream_t s);
 void sim_matrix(const double* v, int w, int h, double m[9]);
 void mat_inverse(const double m[9], double inv[9]);
 bool sim_is_id(const double* v);

@@ -68,6 +68,9 @@ struct DevPool {
     ~DevPool() { release(); }
 };
 
+// Blocks per frame of the brightness sums (brightness.rs:67): their f64 partials are summed in block order.
+constexpr int BRIGHT_PARTS = 512;
+
 struct lsb_engine {
     lsb_config cfg;
     int device, sms, grid;
@@ -388,7 +391,7 @@ static char* stack_alloc(lsb_stack* s) {
             s->pr.push_back(b);
         }
         TRY(P.get(&s->bx_dev, N));
-        TRY(P.get(&s->bpart, N * 64 * 7));
+        TRY(P.get(&s->bpart, N * BRIGHT_PARTS * 7));
         TRY(P.get(&s->sims_dev, (size_t)N * 8));
         s->yt2[0] = s->yt;
         s->pt2[0] = s->pt;
@@ -737,8 +740,10 @@ static char* stream_warps(lsb_stack* s, bool reduce, bool select) {
             B.ident = sim_is_id(sim);
             B.affine = B.inv[6] == 0.0 && B.inv[7] == 0.0 && B.inv[8] == 1.0;
             TRY(cudaMemcpyAsync(s->bx_dev + i, &B, sizeof B, cudaMemcpyHostToDevice, e->ws));
-            TRY(bright_sums_frame(s->frames, i, W, H, s->bx_dev, (int)s->ap.interp, 64, s->bpart, e->ws));
-            TRY(frame_gain(s->bpart, i, 64, s->xf_dev + i, e->ws));
+            // pushed frames: the whole GPU; frames in memory: a few blocks beside the registration chain
+            TRY(bright_sums_frame(s->frames, i, W, H, s->bx_dev, (int)s->ap.interp, BRIGHT_PARTS, s->bpart, reduce ? BRIGHT_PARTS : 64,
+                                  e->ws));
+            TRY(frame_gain(s->bpart, i, BRIGHT_PARTS, s->xf_dev + i, e->ws));
         }
         for (int l = 0; l < s->levels && reduce; l++) {
             bool focus = false;
@@ -838,14 +843,14 @@ static char* run_gains(lsb_stack* s, bool aligned) {
             bx[k].affine = bx[k].inv[6] == 0.0 && bx[k].inv[7] == 0.0 && bx[k].inv[8] == 1.0;
         }
         TRY(cudaMemcpyAsync(s->bx_dev, bx.data(), sizeof(BrightXform) * n, cudaMemcpyHostToDevice, e->s));
-        TRY(bright_sums(s->frames, n, W, H, s->bx_dev, (int)s->ap.interp, 64, s->bpart, e->s));
-        std::vector<double> part((size_t)n * 64 * 7);
+        TRY(bright_sums(s->frames, n, W, H, s->bx_dev, (int)s->ap.interp, BRIGHT_PARTS, s->bpart, e->s));
+        std::vector<double> part((size_t)n * BRIGHT_PARTS * 7);
         TRY(cudaMemcpyAsync(part.data(), s->bpart, sizeof(double) * part.size(), cudaMemcpyDeviceToHost, e->s));
         TRY(cudaStreamSynchronize(e->s));
         for (int k = 1; k < n; k++) {
             double sm[7] = {0, 0, 0, 0, 0, 0, 0};
-            for (int p = 0; p < 64; p++)
-                for (int q = 0; q < 7; q++) sm[q] += part[((size_t)k * 64 + p) * 7 + q];
+            for (int p = 0; p < BRIGHT_PARTS; p++)
+                for (int q = 0; q < 7; q++) sm[q] += part[((size_t)k * BRIGHT_PARTS + p) * 7 + q];
             double sf[3] = {sm[0], sm[1], sm[2]}, so[3] = {sm[3], sm[4], sm[5]};
             bratio(so, sf, (size_t)sm[6], &s->gains[3 * (size_t)k]);
         }
