@@ -145,6 +145,7 @@ __global__ void __launch_bounds__(256, 2) aggregate_kernel(const AggArgs a) {
     const int R = RT > 0 ? RT : a.r, w = a.dw, h = a.dh, tid = threadIdx.x;
     const int PW = TWD + 4 * R, PH = THD + 4 * R, QW = TWD + 2 * R, QH = THD + 2 * R;
     constexpr int NW = 2 * RT + 1;  // window taps when RT > 0
+    constexpr int KS = RT <= 4 ? 8 : 4;  // interior tiles: outputs per thread in a window pass
     float* P = sm;                 // [PH][PW] slice over tile +- 2R
     float* I = P + PW * PH;        // [PH][PW] guide
     float* MI = I + PW * PH;       // [QH][QW] mean_i
@@ -184,18 +185,42 @@ __global__ void __launch_bounds__(256, 2) aggregate_kernel(const AggArgs a) {
             }
             __syncthreads();
             // horizontal sums of p and I*p over rows of tile +- 2R, columns of tile +- R
+            if (inner) {
+                // a strip of KS outputs per thread: each input converted to f64 once, each
+                // output's window summed from zero in tap order
+                constexpr int NV = KS + 2 * RT;
+                const int nst = (QW + KS - 1) / KS;
+                for (int it = tid; it < PH * nst; it += 256) {
+                    const int r = it / nst, c0 = (it - r * nst) * KS;
+                    const float* pr = P + r * PW + c0;
+                    const float* ir = I + r * PW + c0;
+                    double v[NV];
+#pragma unroll
+                    for (int t = 0; t < NV; t++) v[t] = c0 + t < PW ? (double)pr[t] : 0.0;
+#pragma unroll
+                    for (int k = 0; k < KS; k++)
+                        if (c0 + k < QW) {
+                            double sp = 0.0;
+#pragma unroll
+                            for (int t = 0; t < NW; t++) sp += v[k + t];
+                            HP[r * QW + c0 + k] = (float)sp;
+                        }
+#pragma unroll
+                    for (int t = 0; t < NV; t++) v[t] = c0 + t < PW ? (double)__fmul_rn(ir[t], pr[t]) : 0.0;
+#pragma unroll
+                    for (int k = 0; k < KS; k++)
+                        if (c0 + k < QW) {
+                            double sq = 0.0;
+#pragma unroll
+                            for (int t = 0; t < NW; t++) sq += v[k + t];
+                            HQ[r * QW + c0 + k] = (float)sq;
+                        }
+                }
+            } else
             for (int i = tid; i < PH * QW; i += 256) {
                 const int r = i / QW, c = i % QW, x = qx0 + c;
                 double sp = 0.0, sq = 0.0;
-                if (inner) {
-                    const float* pr = P + r * PW + c;
-                    const float* ir = I + r * PW + c;
-#pragma unroll
-                    for (int t = 0; t < NW; t++) {
-                        sp += (double)pr[t];
-                        sq += (double)__fmul_rn(ir[t], pr[t]);
-                    }
-                } else {
+                {
                     const int lo = max(x - R, 0) - px0, hi = min(x + R, w - 1) - px0;
                     for (int t = lo; t <= hi; t++) {
                         const float pv = P[r * PW + t];
@@ -208,6 +233,39 @@ __global__ void __launch_bounds__(256, 2) aggregate_kernel(const AggArgs a) {
             }
             __syncthreads();
             // vertical: mean_p, corr_Ip -> a, b over tile +- R
+            if (inner) {
+                constexpr int NV = KS + 2 * RT;
+                const int nst = (QH + KS - 1) / KS;
+                for (int it = tid; it < QW * nst; it += 256) {
+                    const int c = it % QW, r0 = (it / QW) * KS;
+                    double v[NV];
+                    float sps[KS];  // the sums as f32, as the reference rounds them
+#pragma unroll
+                    for (int t = 0; t < NV; t++) v[t] = r0 + t < PH ? (double)HP[(r0 + t) * QW + c] : 0.0;
+#pragma unroll
+                    for (int k = 0; k < KS; k++) {
+                        double sp = 0.0;
+#pragma unroll
+                        for (int t = 0; t < NW; t++) sp += v[k + t];
+                        sps[k] = (float)sp;
+                    }
+#pragma unroll
+                    for (int t = 0; t < NV; t++) v[t] = r0 + t < PH ? (double)HQ[(r0 + t) * QW + c] : 0.0;
+#pragma unroll
+                    for (int k = 0; k < KS; k++) {
+                        const int r = r0 + k;
+                        if (r >= QH) break;
+                        double sq = 0.0;
+#pragma unroll
+                        for (int t = 0; t < NW; t++) sq += v[k + t];
+                        const int i = r * QW + c;
+                        const float mp = __fmul_rn(sps[k], ic_in), corr = __fmul_rn((float)sq, ic_in);
+                        const float av = __fdiv_rn(__fsub_rn(corr, __fmul_rn(MI[i], mp)), __fadd_rn(VI[i], a.eps));
+                        A[i] = av;
+                        B[i] = __fsub_rn(mp, __fmul_rn(av, MI[i]));
+                    }
+                }
+            } else
             for (int i = tid; i < QW * QH; i += 256) {
                 const int r = i / QW, c = i % QW, x = qx0 + c, y = qy0 + r;
                 if (!inner && (x < 0 || x >= w || y < 0 || y >= h)) {
@@ -239,6 +297,34 @@ __global__ void __launch_bounds__(256, 2) aggregate_kernel(const AggArgs a) {
             }
             __syncthreads();
             // horizontal sums of a and b over rows of tile +- R, the tile's columns
+            if (inner) {
+                constexpr int NV = KS + 2 * RT;
+                constexpr int nst = TWD / KS;
+                for (int it = tid; it < QH * nst; it += 256) {
+                    const int r = it / nst, c0 = (it - r * nst) * KS;
+                    const float* ar = A + r * QW + c0;
+                    const float* br = B + r * QW + c0;
+                    double v[NV];
+#pragma unroll
+                    for (int t = 0; t < NV; t++) v[t] = (double)ar[t];
+#pragma unroll
+                    for (int k = 0; k < KS; k++) {
+                        double sa = 0.0;
+#pragma unroll
+                        for (int t = 0; t < NW; t++) sa += v[k + t];
+                        HP[r * TWD + c0 + k] = (float)sa;
+                    }
+#pragma unroll
+                    for (int t = 0; t < NV; t++) v[t] = (double)br[t];
+#pragma unroll
+                    for (int k = 0; k < KS; k++) {
+                        double sb = 0.0;
+#pragma unroll
+                        for (int t = 0; t < NW; t++) sb += v[k + t];
+                        HQ[r * TWD + c0 + k] = (float)sb;
+                    }
+                }
+            } else
             for (int i = tid; i < QH * TWD; i += 256) {
                 const int r = i / TWD, c = i % TWD, x = x0 + c;
                 if (!inner && x >= w) continue;
@@ -260,6 +346,34 @@ __global__ void __launch_bounds__(256, 2) aggregate_kernel(const AggArgs a) {
                 HQ[i] = (float)sb;
             }
             __syncthreads();
+            if (inner) {
+                // the thread's CPT cells: column tid % TWD, rows (tid / TWD) * CPT + 0 .. CPT-1
+                constexpr int NV = CPT + 2 * RT;
+                const int c = tid % TWD, r0 = (tid / TWD) * CPT;
+                double v[NV];
+                float sas[CPT];
+#pragma unroll
+                for (int t = 0; t < NV; t++) v[t] = (double)HP[(r0 + t) * TWD + c];
+#pragma unroll
+                for (int k = 0; k < CPT; k++) {
+                    double sa = 0.0;
+#pragma unroll
+                    for (int t = 0; t < NW; t++) sa += v[k + t];
+                    sas[k] = (float)sa;
+                }
+#pragma unroll
+                for (int t = 0; t < NV; t++) v[t] = (double)HQ[(r0 + t) * TWD + c];
+#pragma unroll
+                for (int k = 0; k < CPT; k++) {
+                    double sb = 0.0;
+#pragma unroll
+                    for (int t = 0; t < NW; t++) sb += v[k + t];
+                    const float abar = __fmul_rn(sas[k], ic_in), bbar = __fmul_rn((float)sb, ic_in);
+                    const float q = fmaxf(__fadd_rn(__fmul_rn(abar, I[(r0 + k + 2 * R) * PW + c + 2 * R]), bbar), 0.f);
+                    peak_push(st[k], q, m);
+                }
+                continue;
+            }
 #pragma unroll
             for (int j = 0; j < CPT; j++) {
                 const int p = tid + 256 * j, c = p % TWD, r = p / TWD, x = x0 + c, y = y0 + r;
@@ -289,7 +403,8 @@ __global__ void __launch_bounds__(256, 2) aggregate_kernel(const AggArgs a) {
         }
 #pragma unroll
         for (int j = 0; j < CPT; j++) {
-            const int p = tid + 256 * j, c = p % TWD, r = p / TWD, x = x0 + c, y = y0 + r;
+            const int p = tid + 256 * j;
+            const int c = inner ? tid % TWD : p % TWD, r = inner ? (tid / TWD) * CPT + j : p / TWD, x = x0 + c, y = y0 + r;
             if (x >= w || y >= h) continue;
             const size_t o = (size_t)y * w + x, m = (size_t)w * h;
             float* S = a.state;
