@@ -25,7 +25,7 @@ constexpr int NT = 256;
 #define LSB_SEL_MINB 2
 #endif
 #ifndef LSB_RED_MINB
-#define LSB_RED_MINB 1
+#define LSB_RED_MINB 3
 #endif
 // select: tile, own pixels per thread, windows
 #ifndef LSB_TH
@@ -44,7 +44,8 @@ static_assert(LH_MAX * TW <= 3 * SEL_EXP, "the window rows fit the EXPAND scratc
 // reduce: tile of G_{l+1}, G_l window with the focus halo
 constexpr int RW = 32, RH = 16, FOC_R = 3;
 constexpr int RGW = 2 * RW + 2 * FOC_R, RGH = 2 * RH + 2 * FOC_R;  // 70 x 38
-constexpr int RED_FLOATS = 3 * RGW * RGH + RGW * RGH + 3 * RGH * RW;
+constexpr int RED_WPR = (RGW * 6 + 2 + 3) / 4;  // words per staged u16 window row (with 2 bytes of slack)
+constexpr int RED_FLOATS = 3 * RGW * RGH + RGW * RGH + 3 * RGH * RW + RGH * RED_WPR;
 
 // conv_sparse taps (depth.rs:417) in the per-pixel accumulation order: rows
 // grouped by dy in order of first appearance, within a row in list order.
@@ -115,6 +116,15 @@ __device__ __forceinline__ void level_px(const FoldArgs& a, int k, int x, int y,
     }
 }
 
+// 4-byte global -> shared copies that bypass the registers (cp.async)
+__device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(d), "l"(gmem));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
+
 // ------------------------------------------------------------------ REDUCE
 template <int SRC, class GS, bool FOCUS, class SS, bool IN>
 __device__ __forceinline__ void reduce_tile(const FoldArgs& a, float* __restrict__ sm, int k, int gx0, int gy0) {
@@ -128,6 +138,39 @@ __device__ __forceinline__ void reduce_tile(const FoldArgs& a, float* __restrict
     const int xw0 = max(0, 2 * gx0 - FOC_R), xw1 = min(W, 2 * gx0 + 2 * RW + FOC_R);
     const int yw0 = max(0, 2 * gy0 - FOC_R), yw1 = min(H, 2 * gy0 + 2 * RH + FOC_R);
     const int ww = xw1 - xw0, wh = yw1 - yw0;
+    if (SRC == SRC_U16 && IN) {
+        // the interleaved u16 window rows copied as words into shared memory (each row from the
+        // word at or before its first byte; fold inputs carry tail padding), then converted
+        uint32_t* raw = (uint32_t*)(tmph + 3 * RGH * RW);
+        const unsigned char* src = (const unsigned char*)a.src_u16;
+        for (int i = threadIdx.x; i < RGH * RED_WPR; i += NT) {
+            const int r = i / RED_WPR, wd = i - r * RED_WPR;
+            const size_t byte = (((size_t)k * H + yw0 + r) * W + xw0) * 6;
+            cp_async4(raw + i, src + (byte & ~(size_t)3) + 4 * wd);
+        }
+        cp_async_commit();
+        cp_async_wait<0>();
+        __syncthreads();
+        const int gon = a.xf[k].gain_on;
+        float gain[3];
+        for (int q = 0; q < 3; q++) gain[q] = a.xf[k].gain[q];
+        for (int r = ty; r < RGH; r += 8) {
+            const size_t byte = (((size_t)k * H + yw0 + r) * W + xw0) * 6;
+            const uint16_t* row = (const uint16_t*)((const unsigned char*)(raw + r * RED_WPR) + (byte & 3));
+            for (int c = tx; c < RGW; c += 32) {
+                float v[3];
+                for (int q = 0; q < 3; q++) {
+                    v[q] = __fmul_rn((float)row[3 * c + q], LSB_INV16);
+                    if (gon & (1 << q)) v[q] = __fmul_rn(v[q], gain[q]);
+                }
+                const int i = r * RGW + c;
+                g0[i] = v[0];
+                g0[RGW * RGH + i] = v[1];
+                g0[2 * RGW * RGH + i] = v[2];
+                if (FOCUS) yl[i] = lsb_luma(v[0], v[1], v[2]);
+            }
+        }
+    } else
     for (int r = ty; r < wh; r += 8)
         for (int c = tx; c < ww; c += 32) {
             float v[3];
@@ -406,13 +449,6 @@ struct Staging {
     static constexpr size_t SMEM = (size_t)(SEL_FLOATS + (ON ? 2 * WORDS : 0)) * 4;
 };
 
-__device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
-    const unsigned d = (unsigned)__cvta_generic_to_shared(smem);
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(d), "l"(gmem));
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
 
 // Issue the copies of frame k's interior window into `raw` (one stage).
 template <int SRC, class GS, int R>
