@@ -268,6 +268,12 @@ __global__ void __launch_bounds__(NT, LSB_RED_MINB) reduce_level_kernel(const Fo
 }
 
 // ------------------------------------------------------------------ select
+template <int R>
+struct InTile {  // interior-tile window sizes (x0, y0 multiples of TW, TH)
+    static constexpr int LW = TW + 2 * R, LH = TH + 2 * R;
+    static constexpr int AW = ((TW + R - 1) >> 1) + ((R + 1) >> 1) + 3;
+    static constexpr int AH = ((TH + R - 1) >> 1) + ((R + 1) >> 1) + 3;
+};
 struct TileWin {
     int x0, y0, xL0, xL1, yL0, yL1, xA0, xA1, yA0, yA1, lw, lh, aw, ah, ox1, oy1;
 };
@@ -285,7 +291,10 @@ __device__ __forceinline__ void select_frame(const FoldArgs& a, float* __restric
     float* g1 = gl + 3 * SEL_GL;         // [3][ah][aw]   G_{l+1} as stored
     float* exph = g1 + 3 * SEL_G1;       // [3][ah][lw]   EXPAND along rows
     float* yb = exph + 3 * SEL_EXP;      // [lh][lw]      node energy
-    const int lw = t.lw, lh = t.lh, aw = t.aw, ah = t.ah;
+    // staged tiles are interior: their window sizes and extents are the compile-time ones
+    const int lw = STAGED ? InTile<R>::LW : t.lw, lh = STAGED ? InTile<R>::LH : t.lh;
+    const int aw = STAGED ? InTile<R>::AW : t.aw, ah = STAGED ? InTile<R>::AH : t.ah;
+    const int ox1 = STAGED ? TW : t.ox1, oy1 = STAGED ? TH : t.oy1;
     const float2 sc = make_float2(a.xf[k].gscale, a.xf[k].ginv);
 
     // ---- 1: stage G_l and G_{l+1} (STAGED: already in gl / g1 from the async copies)
@@ -345,18 +354,18 @@ __device__ __forceinline__ void select_frame(const FoldArgs& a, float* __restric
     for (int j = 0; j < PPT; j++) {
         const int px = tx + 32 * (j & 1), py = ty + 8 * (j >> 1);
         Lr[j][0] = Lr[j][1] = Lr[j][2] = 0.f;
-        if (px < t.ox1 && py < t.oy1) {
+        if (px < ox1 && py < oy1) {
             const int x = t.x0 + px, y = t.y0 + py;
             yb[(y - t.yL0) * lw + x - t.xL0] = lpoint(x, y, Lr[j]);
         }
     }
     if (R > 0 && a.halo_mode != 2) {
         // the window's halo ring around the tile: energy only
-        const int left = t.x0 - t.xL0, right = t.xL1 - (t.x0 + t.ox1);
+        const int left = t.x0 - t.xL0, right = t.xL1 - (t.x0 + ox1);
         for (int yi = ty; yi < lh; yi += 8) {
             const int y = t.yL0 + yi;
             float L[3];
-            if (y < t.y0 || y >= t.y0 + t.oy1) {
+            if (y < t.y0 || y >= t.y0 + oy1) {
                 for (int xi = tx; xi < lw; xi += 32) yb[yi * lw + xi] = lpoint(t.xL0 + xi, y, L);
             } else if (tx < left + right) {
                 const int xi = tx < left ? tx : (lw - right) + (tx - left);
@@ -373,7 +382,7 @@ __device__ __forceinline__ void select_frame(const FoldArgs& a, float* __restric
 #pragma unroll
         for (int j = 0; j < PPT; j++) {
             const int px = tx + 32 * (j & 1), py = ty + 8 * (j >> 1);
-            if (px >= t.ox1 || py >= t.oy1) continue;
+            if (px >= ox1 || py >= oy1) continue;
             const float wv = a.halo_w[((size_t)k * H + t.y0 + py) * W + t.x0 + px];
 #pragma unroll
             for (int c = 0; c < 3; c++) acc[j][c] = k == 0 ? __fmul_rn(Lr[j][c], wv) : __fadd_rn(acc[j][c], __fmul_rn(wv, Lr[j][c]));
@@ -385,7 +394,7 @@ __device__ __forceinline__ void select_frame(const FoldArgs& a, float* __restric
     float* eh = exph;
     if (R > 0) {
         for (int r = ty; r < lh; r += 8)
-            for (int xo = tx; xo < t.ox1; xo += 32) {
+            for (int xo = tx; xo < ox1; xo += 32) {
                 const float* row = yb + r * lw - t.xL0;
                 float s = 0.f;
 #pragma unroll
@@ -397,7 +406,7 @@ __device__ __forceinline__ void select_frame(const FoldArgs& a, float* __restric
 #pragma unroll
     for (int j = 0; j < PPT; j++) {
         const int px = tx + 32 * (j & 1), py = ty + 8 * (j >> 1);
-        if (px >= t.ox1 || py >= t.oy1) continue;
+        if (px >= ox1 || py >= oy1) continue;
         float e;
         if (R > 0) {
             e = 0.f;
@@ -429,12 +438,6 @@ __device__ __forceinline__ void select_frame(const FoldArgs& a, float* __restric
 // path. Rows are copied as 4-byte words from the word boundary at or before
 // the row's first byte (`mis` bytes of slack in front); every fold input is
 // allocated with 64 bytes of tail padding for the word after a row's end.
-template <int R>
-struct InTile {  // interior-tile window sizes (x0, y0 multiples of TW, TH)
-    static constexpr int LW = TW + 2 * R, LH = TH + 2 * R;
-    static constexpr int AW = ((TW + R - 1) >> 1) + ((R + 1) >> 1) + 3;
-    static constexpr int AH = ((TH + R - 1) >> 1) + ((R + 1) >> 1) + 3;
-};
 template <int SRC, class GS, int R>
 struct Staging {
     static constexpr bool INTERLEAVED = SRC == SRC_U16;
