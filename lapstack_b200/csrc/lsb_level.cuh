@@ -137,7 +137,7 @@ __device__ __forceinline__ void reduce_tile(const FoldArgs& a, float* __restrict
     float* tmph = yl + RGW * RGH;        // [3][wh][RW]
     const int xw0 = max(0, 2 * gx0 - FOC_R), xw1 = min(W, 2 * gx0 + 2 * RW + FOC_R);
     const int yw0 = max(0, 2 * gy0 - FOC_R), yw1 = min(H, 2 * gy0 + 2 * RH + FOC_R);
-    const int ww = xw1 - xw0, wh = yw1 - yw0;
+    const int ww = IN ? RGW : xw1 - xw0, wh = IN ? RGH : yw1 - yw0;  // interior: the full window
     if (SRC == SRC_U16 && IN) {
         // the interleaved u16 window rows copied as words into shared memory (each row from the
         // word at or before its first byte; fold inputs carry tail padding), then converted
@@ -182,7 +182,7 @@ __device__ __forceinline__ void reduce_tile(const FoldArgs& a, float* __restrict
             if (FOCUS) yl[i] = lsb_luma(v[0], v[1], v[2]);
         }
     __syncthreads();
-    const int ow = min(RW, W1 - gx0), oh = min(RH, H1 - gy0);
+    const int ow = IN ? RW : min(RW, W1 - gx0), oh = IN ? RH : min(RH, H1 - gy0);
     // rows (pyramid.rs:90)
     for (int r = ty; r < wh; r += 8)
         for (int j = tx; j < ow; j += 32) {
