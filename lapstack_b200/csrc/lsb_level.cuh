@@ -198,6 +198,23 @@ __device__ __forceinline__ void reduce_tile(const FoldArgs& a, float* __restrict
         const int bk = a.bk;
         const int cx0 = (2 * gx0) / bk, cy0 = (2 * gy0) / bk;
         const int cw = min(2 * RW / bk, a.dw - cx0), chh = min(2 * RH / bk, a.dh - cy0);
+        if (IN && bk == 2 && a.rdf13 && a.focus_kind == 0) {
+            // the default filter over whole 2x2 blocks (interior tiles): the generic loop, unrolled
+            for (int cyy = ty; cyy < RH; cyy += 8)
+                for (int cxx = tx; cxx < RW; cxx += 32) {
+                    const int cx = cx0 + cxx, cy = cy0 + cyy;
+                    const float* yc = yl + (2 * cy - yw0) * RGW + (2 * cx - xw0);
+                    float o = 0.f;
+#pragma unroll
+                    for (int dy = 0; dy < 2; dy++) {
+                        float rs = 0.f;
+#pragma unroll
+                        for (int dx = 0; dx < 2; dx++) rs = __fadd_rn(rs, fabsf(rdf13(yc + dy * RGW + dx)));
+                        o = __fadd_rn(o, rs);
+                    }
+                    lsb_st<SS>((SS*)a.slice + ((size_t)k * a.dh + cy) * a.dw + cx, __fdiv_rn(o, 4.f));
+                }
+        } else
         for (int cyy = ty; cyy < chh; cyy += 8)
             for (int cxx = tx; cxx < cw; cxx += 32) {
                 const int cx = cx0 + cxx, cy = cy0 + cyy;
