@@ -14,6 +14,7 @@
 #include <array>
 #include <atomic>
 #include <map>
+#include <future>
 #include <mutex>
 #include <string>
 #include <unordered_map>
@@ -138,6 +139,7 @@ struct lsb_stack {
     float floor_v = 0.f, p90 = 0.f, rel = 0.f;
     double rel64 = 0.0;
     int iters = 0, iters_first = 0;
+    uint32_t crop_rect[4] = {0, 0, 0, 0};  // the common area of the last run (x, y, w, h)
     double ms[12] = {0};
     // registration chained on the device: per-frame transforms, the last warp, evaluations
     double* sims_dev = nullptr;  // n*8
@@ -871,6 +873,7 @@ static float ms_between(cudaEvent_t a, cudaEvent_t b) {
     return t;
 }
 
+static void common_area(const std::vector<double>& sims, int n, int w, int h, int interp, uint32_t rect[4]);
 static char* run_pipeline(lsb_stack* s) {
     lsb_engine* e = s->e;
     cudaStream_t st = e->s;
@@ -904,6 +907,15 @@ static char* run_pipeline(lsb_stack* s) {
         char* err = run_gains(s, aligned);
         if (err) return err;
     }
+    // align.rs:344 the common area, on a host thread (the transforms are known) while the GPU goes on;
+    // the future's destructor waits for it on every way out of this function
+    s->crop_rect[0] = 0;
+    s->crop_rect[1] = 0;
+    s->crop_rect[2] = s->w;
+    s->crop_rect[3] = s->h;
+    std::future<void> crop_job;
+    if (aligned && s->crop)
+        crop_job = std::async(std::launch::async, [s, n, W, H] { common_area(s->sims, n, W, H, (int)s->ap.interp, s->crop_rect); });
     // per-frame level-0 transforms
     if (!streamed) s->xf.assign(n, FrameXform{});
     for (int k = 0; k < n && !streamed; k++) {
@@ -1073,6 +1085,7 @@ static char* run_pipeline(lsb_stack* s) {
     }
     TRY(cudaEventRecord(ev[7], st));
     TRY(cudaEventSynchronize(ev[7]));
+    if (crop_job.valid()) crop_job.get();
     int status = 0;
     TRY(cudaMemcpy(&status, s->status, sizeof(int), cudaMemcpyDeviceToHost));
     if (status) return dup_err(fmt("device status 0x%x (a kernel met a shape it was not built for)", status));
@@ -1259,6 +1272,11 @@ extern "C" char* lsb_stack_finish(lsb_stack* s, lsb_result* r) {
     r->image_u16 = (uint16_t*)hb_get(sizeof(uint16_t) * 3 * W * H);
     r->image_f32 = (float*)hb_get(sizeof(float) * 3 * W * H);
     r->winner = (float*)hb_get(sizeof(float) * W * H);
+    if (s->dp.enabled) {  // page-locked, so that every copy back is asynchronous
+        r->depth = (float*)hb_get(sizeof(float) * W * H);
+        r->conf = (float*)hb_get(sizeof(float) * W * H);
+        r->floor_cells = (float*)hb_get(sizeof(float) * (size_t)s->dw * s->dh);
+    }
     s->early = r;  // run_pipeline sends the fused planes back as soon as they exist
     char* err = run_pipeline(s);
     s->early = nullptr;
@@ -1279,9 +1297,6 @@ extern "C" char* lsb_stack_finish(lsb_stack* s, lsb_result* r) {
         const size_t m = (size_t)s->dw * s->dh;
         r->dw = s->dw;
         r->dh = s->dh;
-        r->depth = (float*)hb_get(sizeof(float) * W * H);
-        r->conf = (float*)hb_get(sizeof(float) * W * H);
-        r->floor_cells = (float*)malloc(sizeof(float) * m);
         TRY(cudaMemcpyAsync(r->depth, s->dfull, sizeof(float) * W * H, cudaMemcpyDeviceToHost, st));
         TRY(cudaMemcpyAsync(r->conf, s->cfull, sizeof(float) * W * H, cudaMemcpyDeviceToHost, st));
         TRY(cudaMemcpyAsync(r->floor_cells, s->mins, sizeof(float) * m, cudaMemcpyDeviceToHost, st));
@@ -1292,11 +1307,7 @@ extern "C" char* lsb_stack_finish(lsb_stack* s, lsb_result* r) {
     memcpy(r->gains, s->gains.data(), sizeof(float) * 3 * N);
     err = shares_of(s, r->shares);
     if (err) return err;
-    r->crop[0] = 0;
-    r->crop[1] = 0;
-    r->crop[2] = s->w;
-    r->crop[3] = s->h;
-    if (s->ap.enabled && N > 1 && s->crop) common_area(s->sims, (int)N, (int)W, (int)H, (int)s->ap.interp, r->crop);
+    memcpy(r->crop, s->crop_rect, sizeof s->crop_rect);
     r->floor_value = s->floor_v;
     r->p90 = s->p90;
     r->wls_rel = s->rel;
@@ -1321,7 +1332,7 @@ extern "C" void lsb_result_free(lsb_result* r) {
     hb_release(r->winner);
     hb_release(r->depth);
     hb_release(r->conf);
-    free(r->floor_cells);
+    hb_release(r->floor_cells);
     free(r->sims);
     free(r->gains);
     free(r->shares);
