@@ -170,6 +170,20 @@ __device__ __forceinline__ void reduce_tile(const FoldArgs& a, float* __restrict
                 if (FOCUS) yl[i] = lsb_luma(v[0], v[1], v[2]);
             }
         }
+    } else if (SRC == SRC_G) {
+        // a stored level: the frame's scale read once, three planes
+        const float2 sc = make_float2(a.xf[k].gscale, a.xf[k].ginv);
+        const size_t np = (size_t)W * H;
+        const GS* f = (const GS*)a.src_g + (size_t)k * 3 * np;
+        for (int r = ty; r < wh; r += 8) {
+            const GS* row = f + (size_t)(yw0 + r) * W + xw0;
+            for (int c = tx; c < ww; c += 32) {
+                const int i = r * ww + c;
+                g0[i] = Store<GS>::ld(row + c, sc);
+                g0[RGW * RGH + i] = Store<GS>::ld(row + np + c, sc);
+                g0[2 * RGW * RGH + i] = Store<GS>::ld(row + 2 * np + c, sc);
+            }
+        }
     } else
     for (int r = ty; r < wh; r += 8)
         for (int c = tx; c < ww; c += 32) {
