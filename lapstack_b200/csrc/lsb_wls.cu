@@ -535,9 +535,18 @@ __global__ void dot_partial_kernel(const float* __restrict__ a, const float* __r
 }
 // mode: 0 rz; 1 pap -> alpha; 2 rz_new -> beta; 3 rr -> rel; 4 bb -> bnorm
 __global__ void dot_final_kernel(const double* part, int nparts, double* scal, float* ab, float* host_rel, int mode) {
+    // the partials summed by 256 threads (each a fixed stride of them), then a fixed tree
+    __shared__ double red[256];
+    double t = 0.0;
+    for (int i = threadIdx.x; i < nparts; i += 256) t += part[i];
+    red[threadIdx.x] = t;
+    __syncthreads();
+    for (int st = 128; st > 0; st >>= 1) {
+        if (threadIdx.x < st) red[threadIdx.x] += red[threadIdx.x + st];
+        __syncthreads();
+    }
     if (threadIdx.x != 0) return;
-    double s = 0.0;
-    for (int i = 0; i < nparts; i++) s += part[i];
+    const double s = red[0];
     if (mode == 0) scal[0] = s;
     else if (mode == 1) {
         scal[1] = s;
@@ -735,7 +744,7 @@ static void vcycle_h(WlsSolver* S, size_t l, cudaStream_t s) {
 static void dot(WlsSolver* S, const float* a, const float* b, size_t n, int mode, cudaStream_t s) {
     int nb = (int)std::min<size_t>(DOT_BLOCKS, (n + 255) / 256);
     lsb_launched(), dot_partial_kernel<<<nb, 256, 0, s>>>(a, b, n, S->part);
-    lsb_launched(), dot_final_kernel<<<1, 32, 0, s>>>(S->part, nb, S->scal, S->alpha_beta, S->host_rel, mode);
+    lsb_launched(), dot_final_kernel<<<1, 256, 0, s>>>(S->part, nb, S->scal, S->alpha_beta, S->host_rel, mode);
 }
 
 cudaError_t wls_solve(WlsSolver* S, const float* d, int max_iters, float* u, float* rel_out, int* iters_out, cudaStream_t s,
