@@ -724,6 +724,7 @@ struct NmJob {
     const double* init_dev;        // if set, the initial transform (the previous frame's result) instead of init
     double* warp_dev;              // if set, the full-resolution warp of the result: inverse [9], affine, identity
     unsigned long long* evals_dev; // if set, evaluations are added here
+    long long spin_limit;          // polls of the hand-off's wait before it gives up
 };
 
 __device__ void dev_sim_matrix(const double* v, int w, int h, double m[9]) {
@@ -931,8 +932,13 @@ __device__ int nm_advance_warp(const NmJob& J, NmState& S, const double* cost, i
     return n;
 }
 
-// The bounded wait of the search's grid-wide hand-off (at least ~0.1 s of polling).
+// The bounded wait of the search's grid-wide hand-off (at least ~0.1 s of polling);
+// LSB_NM_SPIN_LIMIT overrides it (tests shorten it to make the wait run out).
 constexpr long long NM_SPIN_LIMIT = 1ll << 22;
+static long long spin_limit() {
+    if (const char* v = getenv("LSB_NM_SPIN_LIMIT")) return std::max(1ll, atoll(v));
+    return NM_SPIN_LIMIT;
+}
 
 __device__ __forceinline__ double warp_sum(double v) {
     for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
@@ -1077,7 +1083,7 @@ __global__ void __launch_bounds__(NM_THREADS) nm_search_kernel(const NmJob J) {
                 long long t = 0;
                 int good = 1;
                 while ((int)(*cnt - arrived) < 0) {
-                    if (*verr != 0 || ++t > NM_SPIN_LIMIT) {
+                    if (*verr != 0 || ++t > J.spin_limit) {
                         good = 0;
                         break;
                     }
@@ -1183,6 +1189,7 @@ static cudaError_t nm_job(AlignCtx& C, const float* rf, const std::vector<float*
         if (const char* v = getenv("LSB_NM_CTAS_PER_SM")) want = std::max(1, atoi(v));
         g_nm_blocks = std::min(std::min(per, want) * sms, NM_MAX_BLOCKS);
     }
+    J.spin_limit = spin_limit();
     J.part = C.nm_part;
     J.bar = (unsigned*)C.nm_ctl + 2;
     J.ctl = C.nm_ctl;

@@ -146,6 +146,7 @@ struct lsb_stack {
     double* warp_dev = nullptr;  // inverse [9], affine, identity
     unsigned long long* evals_dev = nullptr;
     int aligned_upto = 0;        // frames already registered (at push time)
+    bool search_timed_out = false;  // the last chained registration gave up waiting
     std::vector<cudaEvent_t> copied;  // per frame: its host -> device copy is done
     // per frame: its search is done (on s), its transform is back in sims_pin (on rs)
     std::vector<cudaEvent_t> searched, sims_back;
@@ -640,7 +641,12 @@ static char* run_align(lsb_stack* s) {
 // The chained registration's end: its status and evaluation count.
 static char* align_finish(lsb_stack* s) {
     size_t evals = 0;
-    TRY(align_chain_end(s->e->actx, s->evals_dev, &evals));
+    const cudaError_t ce = align_chain_end(s->e->actx, s->evals_dev, &evals);
+    if (ce == cudaErrorLaunchTimeout) {  // the search's bounded wait ran out (no fault: the kernel returned)
+        s->search_timed_out = true;
+        return dup_err("the device search's hand-off wait ran out");
+    }
+    TRY(ce);
     s->align_evals = evals;
     s->aligned_upto = 0;  // a later run registers the frames again
     return nullptr;
@@ -874,7 +880,29 @@ static float ms_between(cudaEvent_t a, cudaEvent_t b) {
 }
 
 static void common_area(const std::vector<double>& sims, int n, int w, int h, int interp, uint32_t rect[4]);
+static char* run_pipeline_once(lsb_stack* s);
+// The pipeline, with one guard: if the device search's bounded wait runs out
+// (its cooperative blocks could not all be resident in time), the work queued
+// from its transforms is drained and the stack is registered again by the
+// host-driven search, which takes the same branches (same transforms and
+// evaluation count), then folded as usual.
 static char* run_pipeline(lsb_stack* s) {
+    s->search_timed_out = false;
+    char* err = run_pipeline_once(s);
+    if (!err || !s->search_timed_out) return err;
+    lsb_free_str(err);
+    lsb_engine* e = s->e;
+    e->log("registration: the device search's wait ran out; registering again with the host-driven search");
+    for (cudaStream_t q : {e->s, e->cs, e->bs, e->rs, e->ws}) TRY(cudaStreamSynchronize(q));
+    TRY(cudaMemsetAsync(e->actx.nm_ctl, 0, sizeof(int) * 4, e->s));
+    const auto hs = s->ap.host_search;
+    s->ap.host_search = 1;
+    s->aligned_upto = 0;
+    err = run_pipeline_once(s);
+    s->ap.host_search = hs;
+    return err;
+}
+static char* run_pipeline_once(lsb_stack* s) {
     lsb_engine* e = s->e;
     cudaStream_t st = e->s;
     const int W = (int)s->w, H = (int)s->h, n = (int)s->count;

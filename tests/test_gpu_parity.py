@@ -307,6 +307,40 @@ def test_device_search_matches_host_search(model):
     assert np.max(np.abs(outs[0].align - ref.sims)) < 1e-9
 
 
+def test_search_wait_running_out_falls_back_to_the_host_search(monkeypatch):
+    """The device search's hand-off wait is bounded. When it runs out (here
+    after one poll) the kernel returns, the stack is registered again by the
+    host-driven search and folded as usual: the result is the normal run's,
+    pushed frames and frames in device memory alike."""
+    n = 6
+    fr, _ = L.synth_stack(L.SynthSpec(192, 144, n, warp=True, mag_step=0.004, seed=37))
+    fr = np.stack([np.clip(f.astype(np.float64) * (1.0 - 0.03 * (k % 3)), 0, 65535).astype(np.uint16) for k, f in enumerate(fr)])
+
+    lines = []
+
+    def run(resident):
+        eng = L.Engine(storage="unorm16", log=lines.append)
+        st = eng.stack(192, 144, n, L.FuseParams(), L.AlignParams(coarsen=1), L.DepthParams(), brightness=True)
+        for f in fr:
+            st.push_u16(f)
+        if resident:
+            st.set_count(n)
+        return st.finish()
+
+    normal = run(False)
+    assert not any("registering again" in l for l in lines)
+    monkeypatch.setenv("LSB_NM_SPIN_LIMIT", "1")
+    for resident in (False, True):
+        lines.clear()
+        out = run(resident)
+        assert any("registering again" in l for l in lines), lines
+        assert np.array_equal(out.align, normal.align)
+        assert out.align_evals == normal.align_evals
+        assert_same(out.gains, normal.gains, "gains")
+        assert_same(out.image_u16, normal.image_u16, "fused u16")
+        assert_same(out.depth.depth, normal.depth.depth, "depth")
+
+
 # ---------------------------------------------------------------- precision
 def _errors(img, ref):
     e = np.abs(img.astype(np.float64) - ref.astype(np.float64)) * 65535
