@@ -457,9 +457,121 @@ __global__ void __launch_bounds__(32 * P) pthomas_kernel(float* __restrict__ u, 
 }
 constexpr int PT_ROWS = 8, PT_COLS = 16;
 
+// The row sweep with one row per warp held in shared memory (the partition
+// method of pthomas_kernel with 32 segments, lane = segment): a row's
+// coefficients are read once, coalesced, and every step of the segments'
+// sweeps hits shared memory (segments start w/32 floats apart: no bank
+// conflicts when that is odd, at most two-way otherwise). The reduced system
+// is solved by lane 0 from the segments' end coefficients gathered with
+// shuffles.
+constexpr int PTR_SEGS = 32;
+__global__ void __launch_bounds__(32) pthomas_rows_kernel(float* __restrict__ u, const float* __restrict__ f, const float* __restrict__ wd,
+                                                          int unit_wd, const float* __restrict__ a, int w, int h, float lam) {
+    extern __shared__ float sm[];
+    __shared__ float X[PTR_SEGS];
+    const int line = blockIdx.x, lane = threadIdx.x;
+    if (line >= h) return;
+    float* A = sm;
+    float* WD = A + w;
+    float* F = WD + w;
+    float* S0 = F + w;
+    float* S1 = S0 + w;
+    float* S2 = S1 + w;
+    const size_t row = (size_t)line * w;
+    for (int i = lane; i < w; i += 32) {
+        A[i] = a[row + i];
+        F[i] = f[row + i];
+        WD[i] = unit_wd ? 1.f : wd[row + i];
+    }
+    __syncwarp();
+    const int len = w, b = (int)((long long)lane * len / PTR_SEGS), e = (int)((long long)(lane + 1) * len / PTR_SEGS);
+    const float nl = -lam;
+    float a_prev = b > 0 ? A[b - 1] : 0.f;
+    float dprev = 1.f, gprev = 0.f, rprev = 0.f, uprev = 0.f;
+    for (int i = b; i < e; i++) {
+        const float ai = i + 1 < len ? A[i] : 0.f;
+        const float wdi = WD[i];
+        const float diag = wdi + lam * (a_prev + ai);
+        const float lower = nl * a_prev, upper = nl * ai;
+        const float ri = wdi * F[i];
+        float dd = diag, gg = lower, rv = ri;
+        if (i > b) {
+            const float mlt = lower / dprev;
+            dd = diag - mlt * uprev;
+            gg = -(mlt * gprev);
+            rv = ri - mlt * rprev;
+        }
+        if (fabsf(dd) < 1e-12f) dd = 1e-12f;
+        S0[i] = dd;
+        S1[i] = gg;
+        S2[i] = rv;
+        dprev = dd;
+        gprev = gg;
+        rprev = rv;
+        uprev = upper;
+        a_prev = ai;
+    }
+    const float dL = dprev, gL = gprev, rL = rprev, uL = uprev;  // the segment's last equation
+    float rn = 0.f, sn = 0.f, tn = 1.f;
+    S0[e - 1] = 0.f;
+    S1[e - 1] = 0.f;
+    S2[e - 1] = 1.f;
+    for (int i = e - 2; i >= b; i--) {
+        const float upper = nl * A[i];
+        const float inv = 1.f / S0[i];
+        const float rho = (S2[i] - upper * rn) * inv, sig = (-S1[i] - upper * sn) * inv, tau = -(upper * tn) * inv;
+        S0[i] = rho;
+        S1[i] = sig;
+        S2[i] = tau;
+        rn = rho;
+        sn = sig;
+        tn = tau;
+    }
+    // the reduced system on lane 0, the coefficients of segment q (and q + 1) by shuffle
+    float cprev = 0.f, rprev2 = 0.f;
+    float rc[PTR_SEGS], rr[PTR_SEGS];
+#pragma unroll
+    for (int q = 0; q < PTR_SEGS; q++) {
+        const float dq = __shfl_sync(0xffffffffu, dL, q), gq = __shfl_sync(0xffffffffu, gL, q);
+        const float rq = __shfl_sync(0xffffffffu, rL, q), uq = __shfl_sync(0xffffffffu, uL, q);
+        const int nq = q + 1 < PTR_SEGS ? q + 1 : q;
+        const float rF = __shfl_sync(0xffffffffu, rn, nq), sF = __shfl_sync(0xffffffffu, sn, nq), tF = __shfl_sync(0xffffffffu, tn, nq);
+        const bool nx = q + 1 < PTR_SEGS;
+        const float Aq = q > 0 ? gq : 0.f;
+        const float Bq = nx ? dq + uq * sF : dq;
+        const float Cq = nx ? uq * tF : 0.f;
+        const float Rq = nx ? rq - uq * rF : rq;
+        float den = Bq - Aq * cprev;
+        if (fabsf(den) < 1e-12f) den = 1e-12f;
+        cprev = Cq / den;
+        rprev2 = (Rq - Aq * rprev2) / den;
+        rc[q] = cprev;
+        rr[q] = rprev2;
+    }
+    if (lane == 0) {
+        float xn = 0.f;
+#pragma unroll
+        for (int q = PTR_SEGS - 1; q >= 0; q--) {
+            xn = q == PTR_SEGS - 1 ? rr[q] : rr[q] - rc[q] * xn;
+            X[q] = xn;
+        }
+    }
+    __syncwarp();
+    const float xl = lane > 0 ? X[lane - 1] : 0.f, xs = X[lane];
+    for (int i = b; i < e; i++) S0[i] = S0[i] + S1[i] * xl + S2[i] * xs;
+    __syncwarp();
+    for (int i = lane; i < w; i += 32) u[row + i] = S0[i];
+}
+
 static void thomas(bool rows, float* u, const float* f, const float* wd, int unit_wd, const float* a, int w, int h, float lam,
                    float* cp, float* dp, float* sc, cudaStream_t s) {
     const int nlines = rows ? h : w, len = rows ? w : h;
+    if (rows && len >= PTR_SEGS * 8 && (size_t)6 * len * sizeof(float) <= 200 * 1024) {
+        const size_t smem = (size_t)6 * len * sizeof(float);
+        cudaFuncSetAttribute(pthomas_rows_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        lsb_launched(), pthomas_rows_kernel<<<nlines, 32, smem, s>>>(u, f, wd, unit_wd, a, w, h, lam);
+        return;
+    }
     if (sc && len >= (rows ? PT_ROWS : PT_COLS) * 8) {
         const int g = (nlines + 31) / 32;
         if (rows) lsb_launched(), pthomas_kernel<true, PT_ROWS><<<g, 32 * PT_ROWS, 0, s>>>(u, f, wd, unit_wd, a, w, h, lam, cp, dp, sc);
