@@ -10,7 +10,7 @@ already in HBM; `e2e` times the public API (Stack.push_u16 from pinned host
 memory, Stack.finish reading the results back) per step.
 
 Workloads (seeded synthetic stacks with the shapes of the reference's
-published runs):
+published runs: a height field, band-limited texture, per-pixel defocus):
   c3  100 x 8256x5504 RGB u16, per-frame similarity warps, alignment at
       coarsen 3, 7 levels, 16-bit (UNORM16) pyramid storage   [default]
   c2  30 x 6000x4000, no alignment, 8 levels, aggregation radius 8, FP32
@@ -38,7 +38,7 @@ sys.path.insert(0, ROOT)
 
 METRIC = "stack MP-frames/s (align+fuse+depth)"
 UNIT = "MP-frames/s"
-# the reference's CUDA run of 100 x 45.7 MP frames (RTX 3060), 26 s wall
+# the reference's published CUDA run of 100 x 45.7 MP frames (RTX 3060), 26 s wall
 PUBLISHED_MPFS = 175.8
 
 CONFIGS = {
