@@ -140,6 +140,8 @@ struct lsb_stack {
     double rel64 = 0.0;
     int iters = 0, iters_first = 0;
     uint32_t crop_rect[4] = {0, 0, 0, 0};  // the common area of the last run (x, y, w, h)
+    float* gsel = nullptr;  // the frame groups' selection states of the small levels
+    size_t gsel_floats = 0;
     double ms[12] = {0};
     // registration chained on the device: per-frame transforms, the last warp, evaluations
     double* sims_dev = nullptr;  // n*8
@@ -357,6 +359,8 @@ static char* stack_alloc(lsb_stack* s) {
     TRY(P.get(&s->mpart, N * 64 * 3));
     TRY(P.get(&s->means, N * 3));
     TRY(P.get(&s->status, 4));
+    s->gsel_floats = (size_t)16 << 20;  // 64 MB: the small levels' frame-group states
+    TRY(P.get(&s->gsel, s->gsel_floats));
     TRY(P.get(&s->xf_dev, N));
     if (s->dp.enabled) {
         s->bk = 1 << s->dp.scale;
@@ -995,6 +999,20 @@ static char* run_pipeline_once(lsb_stack* s) {
         int src = 0;
         FoldArgs a = level_args(s, l, warped, depth_on, &focus, &src);
         if (streamed && pushed) a.red_n = 0;  // stream_warps has REDUCEd every frame
+        if (!(halo && l >= guide)) {
+            // levels with too few tiles to fill the GPU: the frames split into groups selected side
+            // by side, then merged in order (about 1.5 items per block, each group at least 2 frames)
+            const int gl = e->grid_select > 0 ? e->grid_select : e->grid;
+            const size_t np = (size_t)a.W * a.H;
+            int G = std::min((3 * gl / 2 + a.ntiles - 1) / std::max(a.ntiles, 1), std::max(1, n / 2));
+            while (G > 1 && (size_t)G * 5 * np > s->gsel_floats) G--;
+            if (G > 1) {
+                a.sel_groups = G;
+                a.gacc = s->gsel;
+                a.gbest = s->gsel + (size_t)G * 3 * np;
+                a.gwin = (int*)(s->gsel + (size_t)G * 4 * np);
+            }
+        }
         if (halo && l >= guide) {
             a.halo_mode = l == guide ? 1 : 2;
             a.halo_p = std::min(s->fp.halo, 8.0f);

@@ -53,6 +53,29 @@ static cudaError_t with_smem(K k, size_t smem) {
     return cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
 }
 
+// The frame groups' selection states merged in group order: the first group
+// holding the largest energy wins, and within it its first frame did.
+__global__ void select_merge_kernel(const FoldArgs a, int G) {
+    const size_t np = (size_t)a.W * a.H;
+    for (size_t o = blockIdx.x * (size_t)blockDim.x + threadIdx.x; o < np; o += (size_t)gridDim.x * blockDim.x) {
+        int bg = 0;
+        float best = a.gbest[o];
+        for (int g = 1; g < G; g++) {
+            const float b = a.gbest[(size_t)g * np + o];
+            if (b > best) {
+                best = b;
+                bg = g;
+            }
+        }
+        const float* ga = a.gacc + (size_t)bg * 3 * np;
+        a.acc[o] = ga[o];
+        a.acc[np + o] = ga[np + o];
+        a.acc[2 * np + o] = ga[2 * np + o];
+        a.best[o] = best;
+        if (a.winner) a.winner[o] = (uint16_t)a.gwin[(size_t)bg * np + o];
+    }
+}
+
 // One level: REDUCE the frames asked for (and take their focus slices at level 0), then select.
 template <int SRC, class GS, int R, bool FOCUS, class SS>
 static cudaError_t launch_level(const FoldArgs& a, cudaStream_t s, int grid_limit) {
@@ -65,7 +88,12 @@ static cudaError_t launch_level(const FoldArgs& a, cudaStream_t s, int grid_limi
     const int rtiles = ((a.W1 + RW - 1) / RW) * ((a.H1 + RH - 1) / RH);
     if (a.red_n > 0) lsb_launched(), kr<<<dim3(rtiles, a.red_n), NT, rsm, s>>>(a);
     if (a.between) cudaEventRecord(a.between, s);
-    if (a.select) lsb_launched(), ks<<<std::min(a.ntiles, std::max(grid_limit, 1)), NT, ssm, s>>>(a);
+    const int groups = std::max(a.sel_groups, 1);
+    if (a.select) lsb_launched(), ks<<<std::min(a.ntiles * groups, std::max(grid_limit, 1)), NT, ssm, s>>>(a);
+    if (a.select && groups > 1) {
+        const size_t np = (size_t)a.W * a.H;
+        lsb_launched(), select_merge_kernel<<<(unsigned)std::min<size_t>((np + 255) / 256, 148 * 8), 256, 0, s>>>(a, groups);
+    }
     return cudaGetLastError();
 }
 

@@ -61,6 +61,12 @@ struct FoldArgs {
     // (none if red_n is 0) and, if select is set, the selection over frames sel_k0 .. sel_k1 - 1
     // (from sel_k0 > 0 it resumes from the acc / best / winner the frames before it left)
     int red_k0, red_n, select, sel_k0, sel_k1;
+    // sel_groups > 1: the frames are split into that many groups selected side by side from a
+    // fresh state, each into its slice of gacc [g][3][H][W] / gbest [g][H][W] / gwin [g][H][W],
+    // then merged in group order (strict >, so the earliest frame with the largest energy wins)
+    int sel_groups;
+    float *gacc, *gbest;
+    int* gwin;
 };
 
 // Storage of the Gaussian levels >= 1 and the focus slices.

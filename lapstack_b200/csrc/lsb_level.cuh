@@ -564,7 +564,11 @@ __global__ void __launch_bounds__(NT, LSB_SEL_MINB) select_level_kernel(const Fo
     extern __shared__ float sm[];
     const int W = a.W, H = a.H, W1 = a.W1, H1 = a.H1;
     const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
-    for (int tile = blockIdx.x; tile < a.ntiles; tile += gridDim.x) {
+    const int G = a.sel_groups > 1 ? a.sel_groups : 1;
+    for (int wi = blockIdx.x; wi < a.ntiles * G; wi += gridDim.x) {
+        const int tile = wi % a.ntiles, g = wi / a.ntiles;
+        const int k0 = G > 1 ? a.sel_k0 + (a.sel_k1 - a.sel_k0) * g / G : a.sel_k0;
+        const int k1 = G > 1 ? a.sel_k0 + (a.sel_k1 - a.sel_k0) * (g + 1) / G : a.sel_k1;
         TileWin t;
         t.x0 = (tile % a.tiles_x) * TW;
         t.y0 = (tile / a.tiles_x) * TH;
@@ -597,7 +601,7 @@ __global__ void __launch_bounds__(NT, LSB_SEL_MINB) select_level_kernel(const Fo
             acc[j][0] = acc[j][1] = acc[j][2] = 0.f;
             win[j] = 0;
             const int px = tx + 32 * (j & 1), py = ty + 8 * (j >> 1);
-            if (a.sel_k0 > 0 && px < t.ox1 && py < t.oy1) {  // resume: the state the frames before left
+            if (G == 1 && a.sel_k0 > 0 && px < t.ox1 && py < t.oy1) {  // resume: the state the frames before left
                 const size_t o = (size_t)(t.y0 + py) * W + t.x0 + px;
                 acc[j][0] = a.acc[o];
                 acc[j][1] = a.acc[(size_t)W * H + o];
@@ -613,12 +617,12 @@ __global__ void __launch_bounds__(NT, LSB_SEL_MINB) select_level_kernel(const Fo
                 return;
             }
             uint32_t* raw = (uint32_t*)(sm + SEL_FLOATS);
-            stage_issue<SRC, GS, R>(a, a.sel_k0, t, raw);
+            stage_issue<SRC, GS, R>(a, k0, t, raw);
             cp_async_commit();
-            for (int k = a.sel_k0; k < a.sel_k1; k++) {
-                uint32_t* cur = raw + ((k - a.sel_k0) & 1) * S::WORDS;
-                if (k + 1 < a.sel_k1) {
-                    stage_issue<SRC, GS, R>(a, k + 1, t, raw + ((k + 1 - a.sel_k0) & 1) * S::WORDS);
+            for (int k = k0; k < k1; k++) {
+                uint32_t* cur = raw + ((k - k0) & 1) * S::WORDS;
+                if (k + 1 < k1) {
+                    stage_issue<SRC, GS, R>(a, k + 1, t, raw + ((k + 1 - k0) & 1) * S::WORDS);
                     cp_async_commit();
                     cp_async_wait<1>();
                 } else {
@@ -630,7 +634,7 @@ __global__ void __launch_bounds__(NT, LSB_SEL_MINB) select_level_kernel(const Fo
                 select_frame<SRC, GS, R, true, true>(a, sm, k, t, best, acc, win);
             }
         } else {
-            for (int k = a.sel_k0; k < a.sel_k1; k++) {
+            for (int k = k0; k < k1; k++) {
                 if (interior) select_frame<SRC, GS, R, true>(a, sm, k, t, best, acc, win);
                 else select_frame<SRC, GS, R, false>(a, sm, k, t, best, acc, win);
             }
@@ -639,10 +643,19 @@ __global__ void __launch_bounds__(NT, LSB_SEL_MINB) select_level_kernel(const Fo
         for (int j = 0; j < PPT; j++) {
             const int px = tx + 32 * (j & 1), py = ty + 8 * (j >> 1);
             if (px >= t.ox1 || py >= t.oy1) continue;
-            const size_t o = (size_t)(t.y0 + py) * W + t.x0 + px;
+            const size_t o = (size_t)(t.y0 + py) * W + t.x0 + px, np = (size_t)W * H;
+            if (G > 1) {  // this group's state, merged by select_merge_kernel
+                float* ga = a.gacc + (size_t)g * 3 * np;
+                ga[o] = acc[j][0];
+                ga[np + o] = acc[j][1];
+                ga[2 * np + o] = acc[j][2];
+                a.gbest[(size_t)g * np + o] = best[j];
+                a.gwin[(size_t)g * np + o] = win[j];
+                continue;
+            }
             a.acc[o] = acc[j][0];
-            a.acc[(size_t)W * H + o] = acc[j][1];
-            a.acc[2 * (size_t)W * H + o] = acc[j][2];
+            a.acc[np + o] = acc[j][1];
+            a.acc[2 * np + o] = acc[j][2];
             a.best[o] = best[j];
             if (a.winner) a.winner[o] = (uint16_t)win[j];
         }
