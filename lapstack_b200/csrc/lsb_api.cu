@@ -701,6 +701,24 @@ static FoldArgs level_args(const lsb_stack* s, int l, bool warped, bool depth_on
     return a;
 }
 
+// Levels with too few tiles to fill the GPU: the frames of the selection
+// split into groups selected side by side, then merged in order (about 1.5
+// work items per block, each group at least 2 frames; the first group resumes
+// the state of the frames before, if any).
+static void set_groups(const lsb_stack* s, FoldArgs& a) {
+    const lsb_engine* e = s->e;
+    const int gl = e->grid_select > 0 ? e->grid_select : e->grid;
+    const size_t np = (size_t)a.W * a.H;
+    int G = std::min((3 * gl / 2 + a.ntiles - 1) / std::max(a.ntiles, 1), std::max(1, (a.sel_k1 - a.sel_k0) / 2));
+    while (G > 1 && (size_t)G * 5 * np > s->gsel_floats) G--;
+    if (G > 1) {
+        a.sel_groups = G;
+        a.gacc = s->gsel;
+        a.gbest = s->gsel + (size_t)G * 3 * np;
+        a.gwin = (int*)(s->gsel + (size_t)G * 4 * np);
+    }
+}
+
 // Each frame's warp (align.rs:489, stack.rs:662-679) and brightness sums
 // (brightness.rs:67) as soon as its search is done, while the chain goes on:
 // the transforms come back on rs behind each search, their matrices are
@@ -774,6 +792,7 @@ static char* stream_warps(lsb_stack* s, bool reduce, bool select) {
                 a.red_n = 0;
                 a.sel_k0 = sel_from;
                 a.sel_k1 = i + 1;
+                set_groups(s, a);
                 TRY(fold_level(a, src, s->storage, (int)s->fp.energy_radius, focus, e->ws,
                                e->grid_select > 0 ? e->grid_select : e->grid));
             }
@@ -999,20 +1018,7 @@ static char* run_pipeline_once(lsb_stack* s) {
         int src = 0;
         FoldArgs a = level_args(s, l, warped, depth_on, &focus, &src);
         if (streamed && pushed) a.red_n = 0;  // stream_warps has REDUCEd every frame
-        if (!(halo && l >= guide)) {
-            // levels with too few tiles to fill the GPU: the frames split into groups selected side
-            // by side, then merged in order (about 1.5 items per block, each group at least 2 frames)
-            const int gl = e->grid_select > 0 ? e->grid_select : e->grid;
-            const size_t np = (size_t)a.W * a.H;
-            int G = std::min((3 * gl / 2 + a.ntiles - 1) / std::max(a.ntiles, 1), std::max(1, n / 2));
-            while (G > 1 && (size_t)G * 5 * np > s->gsel_floats) G--;
-            if (G > 1) {
-                a.sel_groups = G;
-                a.gacc = s->gsel;
-                a.gbest = s->gsel + (size_t)G * 3 * np;
-                a.gwin = (int*)(s->gsel + (size_t)G * 4 * np);
-            }
-        }
+        if (!(halo && l >= guide)) set_groups(s, a);
         if (halo && l >= guide) {
             a.halo_mode = l == guide ? 1 : 2;
             a.halo_p = std::min(s->fp.halo, 8.0f);

@@ -601,7 +601,7 @@ __global__ void __launch_bounds__(NT, LSB_SEL_MINB) select_level_kernel(const Fo
             acc[j][0] = acc[j][1] = acc[j][2] = 0.f;
             win[j] = 0;
             const int px = tx + 32 * (j & 1), py = ty + 8 * (j >> 1);
-            if (G == 1 && a.sel_k0 > 0 && px < t.ox1 && py < t.oy1) {  // resume: the state the frames before left
+            if (g == 0 && a.sel_k0 > 0 && px < t.ox1 && py < t.oy1) {  // resume: the state the frames before left
                 const size_t o = (size_t)(t.y0 + py) * W + t.x0 + px;
                 acc[j][0] = a.acc[o];
                 acc[j][1] = a.acc[(size_t)W * H + o];
