@@ -391,17 +391,21 @@ __device__ __forceinline__ void select_frame(const FoldArgs& a, float* __restric
         }
     }
     if (R > 0 && a.halo_mode != 2) {
-        // the window's halo ring around the tile: energy only
-        const int left = t.x0 - t.xL0, right = t.xL1 - (t.x0 + ox1);
-        for (int yi = ty; yi < lh; yi += 8) {
-            const int y = t.yL0 + yi;
+        // the window's halo ring around the tile, energy only, spread over all threads:
+        // the full-width rows above and below the tile, then the columns beside its rows
+        const int left = t.x0 - t.xL0, right = t.xL1 - (t.x0 + ox1), side = left + right;
+        const int top = t.y0 - t.yL0, bot = lh - top - oy1;
+        for (int m = threadIdx.x; m < (top + bot) * lw; m += NT) {
+            const int rr = m / lw, xi = m - rr * lw;
+            const int yi = rr < top ? rr : oy1 + rr;
             float L[3];
-            if (y < t.y0 || y >= t.y0 + oy1) {
-                for (int xi = tx; xi < lw; xi += 32) yb[yi * lw + xi] = lpoint(t.xL0 + xi, y, L);
-            } else if (tx < left + right) {
-                const int xi = tx < left ? tx : (lw - right) + (tx - left);
-                yb[yi * lw + xi] = lpoint(t.xL0 + xi, y, L);
-            }
+            yb[yi * lw + xi] = lpoint(t.xL0 + xi, t.yL0 + yi, L);
+        }
+        for (int m = threadIdx.x; m < oy1 * side; m += NT) {
+            const int rr = m / side, c = m - rr * side;
+            const int xi = c < left ? c : (lw - right) + (c - left);
+            float L[3];
+            yb[(top + rr) * lw + xi] = lpoint(t.xL0 + xi, t.yL0 + top + rr, L);
         }
     }
     __syncthreads();
