@@ -350,9 +350,10 @@ __device__ __forceinline__ void select_frame(const FoldArgs& a, float* __restric
     __syncthreads();
     }
 
-    // ---- 2: EXPAND along rows (pyramid.rs:147)
-    for (int i = ty; i < ah; i += 8)
-        for (int xi = tx; xi < lw; xi += 32) {
+    // ---- 2: EXPAND along rows (pyramid.rs:147), the ah x lw outputs spread over all threads
+    for (int m = threadIdx.x; m < ah * lw; m += NT) {
+        const int i = m / lw, xi = m - i * lw;
+        {
             const int x = t.xL0 + xi, cx = x >> 1;
             const bool even = (x & 1) == 0;
             const int ja = RX1(cx - 1) - t.xA0, jb = RX1(cx) - t.xA0, jc = RX1(cx + 1) - t.xA0;
@@ -362,6 +363,7 @@ __device__ __forceinline__ void select_frame(const FoldArgs& a, float* __restric
                 exph[c * SEL_EXP + i * lw + xi] = even ? lsb_exp_even(row[ja], row[jb], row[jc]) : lsb_exp_odd(row[jb], row[jc]);
             }
         }
+    }
     __syncthreads();
 
     // ---- 3: EXPAND along columns, L = G - EXPAND(G_{l+1}), node energy (fuse.rs:152)
@@ -428,14 +430,16 @@ __device__ __forceinline__ void select_frame(const FoldArgs& a, float* __restric
     }
     float* eh = exph;
     if (R > 0) {
-        for (int r = ty; r < lh; r += 8)
-            for (int xo = tx; xo < ox1; xo += 32) {
+        for (int m = threadIdx.x; m < lh * ox1; m += NT) {  // the lh x ox1 row sums over all threads
+            const int r = m / ox1, xo = m - r * ox1;
+            {
                 const float* row = yb + r * lw - t.xL0;
                 float s = 0.f;
 #pragma unroll
                 for (int q = 0; q <= 2 * R; q++) s = __fadd_rn(s, __fmul_rn(binw<R>(q), row[RX(t.x0 + xo + q - R)]));
                 eh[r * TW + xo] = s;
             }
+        }
         __syncthreads();
     }
 #pragma unroll
