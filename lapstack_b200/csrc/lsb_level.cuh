@@ -154,10 +154,12 @@ __device__ __forceinline__ void reduce_tile(const FoldArgs& a, float* __restrict
         const int gon = a.xf[k].gain_on;
         float gain[3];
         for (int q = 0; q < 3; q++) gain[q] = a.xf[k].gain[q];
-        for (int r = ty; r < RGH; r += 8) {
-            const size_t byte = (((size_t)k * H + yw0 + r) * W + xw0) * 6;
-            const uint16_t* row = (const uint16_t*)((const unsigned char*)(raw + r * RED_WPR) + (byte & 3));
-            for (int c = tx; c < RGW; c += 32) {
+        const unsigned mis0 = (unsigned)(((((size_t)k * H + yw0) * W + xw0) * 6) & 3), rowmis = (unsigned)((W * 6) & 3);
+        for (int m = threadIdx.x; m < RGH * RGW; m += NT) {  // the window's pixels over all threads
+            const int r = m / RGW, c = m - r * RGW;
+            const unsigned mis = (mis0 + (unsigned)r * rowmis) & 3;  // the row's first byte within its word
+            const uint16_t* row = (const uint16_t*)((const unsigned char*)(raw + r * RED_WPR) + mis);
+            {
                 float v[3];
                 for (int q = 0; q < 3; q++) {
                     v[q] = __fmul_rn((float)row[3 * c + q], LSB_INV16);
@@ -197,9 +199,10 @@ __device__ __forceinline__ void reduce_tile(const FoldArgs& a, float* __restrict
         }
     __syncthreads();
     const int ow = IN ? RW : min(RW, W1 - gx0), oh = IN ? RH : min(RH, H1 - gy0);
-    // rows (pyramid.rs:90)
-    for (int r = ty; r < wh; r += 8)
-        for (int j = tx; j < ow; j += 32) {
+    // rows (pyramid.rs:90), the wh x ow outputs over all threads
+    for (int m = threadIdx.x; m < wh * ow; m += NT) {
+        const int r = m / ow, j = m - r * ow;
+        {
             const int cc = 2 * (gx0 + j);
             const int i0 = RX(cc - 2) - xw0, i1 = RX(cc - 1) - xw0, i2 = RX(cc) - xw0, i3 = RX(cc + 1) - xw0, i4 = RX(cc + 2) - xw0;
 #pragma unroll
@@ -208,6 +211,7 @@ __device__ __forceinline__ void reduce_tile(const FoldArgs& a, float* __restrict
                 tmph[(c * RGH + r) * RW + j] = lsb_tap5(row[i0], row[i1], row[i2], row[i3], row[i4]);
             }
         }
+    }
     if (FOCUS) {
         const int bk = a.bk;
         const int cx0 = (2 * gx0) / bk, cy0 = (2 * gy0) / bk;
