@@ -177,9 +177,10 @@ __device__ __forceinline__ void reduce_tile(const FoldArgs& a, float* __restrict
         const float2 sc = make_float2(a.xf[k].gscale, a.xf[k].ginv);
         const size_t np = (size_t)W * H;
         const GS* f = (const GS*)a.src_g + (size_t)k * 3 * np;
-        for (int r = ty; r < wh; r += 8) {
+        for (int m = threadIdx.x; m < wh * ww; m += NT) {  // the window's pixels over all threads
+            const int r = m / ww, c = m - r * ww;
             const GS* row = f + (size_t)(yw0 + r) * W + xw0;
-            for (int c = tx; c < ww; c += 32) {
+            {
                 const int i = r * ww + c;
                 g0[i] = Store<GS>::ld(row + c, sc);
                 g0[RGW * RGH + i] = Store<GS>::ld(row + np + c, sc);
