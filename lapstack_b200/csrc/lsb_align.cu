@@ -391,9 +391,11 @@ __global__ void __launch_bounds__(256) warp_plane_tile_kernel(const float* __res
         }
     }
     if (fits) {
-        for (int r = ty; r < bh; r += 8) {  // a warp per footprint row, lanes along it
-            const float* row = src + (size_t)min(max(by0 + r, 0), h - 1) * w;
-            for (int c = tx; c < bw; c += 32) box[r][c] = row[min(max(bx0 + c, 0), w - 1)];
+        // the footprint's elements over all threads; m / bw by a multiply (exact for m < 2^16, bw <= 80)
+        const unsigned magic = (unsigned)((0xffffffffull + bw) / bw);
+        for (int m = threadIdx.x; m < bw * bh; m += 256) {
+            const int r = (int)__umulhi((unsigned)m, magic), c = m - r * bw;
+            box[r][c] = src[(size_t)min(max(by0 + r, 0), h - 1) * w + min(max(bx0 + c, 0), w - 1)];
         }
         __syncthreads();
     }

@@ -753,13 +753,13 @@ __global__ void __launch_bounds__(NT) warp_tile_kernel(const uint16_t* __restric
         }
     }
     if (fits) {
-        for (int r = ty; r < bh; r += NT / 32) {  // a warp per footprint row, lanes along it
-            const uint16_t* row = f + (size_t)min(max(by0 + r, 0), H - 1) * W * 3;
-            for (int c = tx; c < bw; c += 32) {
-                const uint16_t* p = row + (size_t)min(max(bx0 + c, 0), W - 1) * 3;
-                box[r][c] = make_float4(__fmul_rn((float)p[0], LSB_INV16), __fmul_rn((float)p[1], LSB_INV16),
-                                        __fmul_rn((float)p[2], LSB_INV16), 0.f);
-            }
+        // the footprint's elements over all threads; m / bw by a multiply (exact for m < 2^16, bw <= 80)
+        const unsigned magic = (unsigned)((0xffffffffull + bw) / bw);
+        for (int m = threadIdx.x; m < bw * bh; m += NT) {
+            const int r = (int)__umulhi((unsigned)m, magic), c = m - r * bw;
+            const uint16_t* p = f + ((size_t)min(max(by0 + r, 0), H - 1) * W + min(max(bx0 + c, 0), W - 1)) * 3;
+            box[r][c] = make_float4(__fmul_rn((float)p[0], LSB_INV16), __fmul_rn((float)p[1], LSB_INV16),
+                                    __fmul_rn((float)p[2], LSB_INV16), 0.f);
         }
         __syncthreads();
     }
