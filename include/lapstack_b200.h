@@ -147,7 +147,10 @@ void* lsb_engine_stream(lsb_engine* e);
 char* lsb_stack_begin(lsb_engine* e, uint32_t w, uint32_t h, uint32_t n_frames, const lsb_fuse_params* fuse,
                       const lsb_align_params* align, const lsb_depth_params* depth, int32_t brightness, int32_t crop,
                       lsb_stack** out);
-/* One decoded frame: interleaved RGB u16, rows stride_px pixels apart (host or device pointer). */
+/* One decoded frame: interleaved RGB u16, rows stride_px pixels apart (host or device pointer).
+   The copy is asynchronous for page-locked memory: keep it unchanged until finish/run returns.
+   The frame is registered on the device behind the next frame's copy; finish/run then warps,
+   gains, REDUCEs and folds each pushed frame as soon as its transform is known. */
 char* lsb_stack_push_u16(lsb_stack* s, const uint16_t* rgb, size_t stride_px);
 /* One frame as three planar f32 planes in [0,1] (host or device pointers); the frame is folded as given. */
 char* lsb_stack_push_f32(lsb_stack* s, const float* const planes[3]);
