@@ -232,29 +232,17 @@ static WlsSolver* stack_solver(lsb_stack* s, int dw, int dh, const lsb_depth_par
     return s->ws;
 }
 
-extern "C" {
-
-uint32_t lsb_abi(void) { return LSB_ABI_VERSION; }
-void lsb_free_str(char* s) { free(s); }
-
-char* lsb_engine_create(const lsb_config* cfg, lsb_engine** out) {
-    *out = nullptr;
-    lsb_engine* e = new lsb_engine();
-    e->cfg = cfg ? *cfg : lsb_config{0, 0, 0, 0, nullptr, nullptr};
-    e->device = e->cfg.device;
+// Everything lsb_engine_create makes; on an error the caller frees what was made with lsb_engine_destroy.
+static char* engine_init(lsb_engine* e) {
     int ndev = 0;
     cudaError_t r = cudaGetDeviceCount(&ndev);
-    if (r != cudaSuccess || ndev == 0) {
-        delete e;
+    if (r != cudaSuccess || ndev == 0)
         return dup_err(fmt("lapstack-b200 needs a CUDA device: %s", r != cudaSuccess ? cudaGetErrorString(r) : "none found"));
-    }
     TRY(cudaSetDevice(e->device));
     cudaDeviceProp prop;
     TRY(cudaGetDeviceProperties(&prop, e->device));
-    if (prop.major < 10) {
-        delete e;
+    if (prop.major < 10)
         return dup_err(fmt("lapstack-b200 is built for sm_100a; device %d is sm_%d%d", e->device, prop.major, prop.minor));
-    }
     e->sms = prop.multiProcessorCount;
     e->grid = e->cfg.grid_limit > 0 ? e->cfg.grid_limit : 2 * e->sms;
     TRY(cudaStreamCreateWithFlags(&e->s, cudaStreamNonBlocking));
@@ -279,22 +267,40 @@ char* lsb_engine_create(const lsb_config* cfg, lsb_engine** out) {
         e->coop = coop;
     }
     for (auto& v : e->ev) TRY(cudaEventCreate(&v));
+    return nullptr;
+}
+
+extern "C" {
+
+uint32_t lsb_abi(void) { return LSB_ABI_VERSION; }
+void lsb_free_str(char* s) { free(s); }
+
+char* lsb_engine_create(const lsb_config* cfg, lsb_engine** out) {
+    *out = nullptr;
+    lsb_engine* e = new lsb_engine();  // value-initialised: every stream, event and pointer starts null
+    e->cfg = cfg ? *cfg : lsb_config{0, 0, 0, 0, nullptr, nullptr};
+    e->device = e->cfg.device;
+    if (char* err = engine_init(e)) {
+        lsb_engine_destroy(e);
+        return err;
+    }
     *out = e;
     return nullptr;
 }
 
 void lsb_engine_destroy(lsb_engine* e) {
     if (!e) return;
-    cudaStreamSynchronize(e->s);
-    for (auto& v : e->ev) cudaEventDestroy(v);
-    cudaFreeHost(e->actx.sums_host);
+    if (e->s) cudaStreamSynchronize(e->s);
+    for (auto& v : e->ev)
+        if (v) cudaEventDestroy(v);
+    if (e->actx.sums_host) cudaFreeHost(e->actx.sums_host);
     e->pool.release();
     if (e->cs) cudaStreamSynchronize(e->cs), cudaStreamDestroy(e->cs);
     if (e->s_mark) cudaEventDestroy(e->s_mark);
     if (e->bs) cudaStreamSynchronize(e->bs), cudaStreamDestroy(e->bs);
     if (e->rs) cudaStreamSynchronize(e->rs), cudaStreamDestroy(e->rs);
     if (e->ws) cudaStreamSynchronize(e->ws), cudaStreamDestroy(e->ws);
-    cudaStreamDestroy(e->s);
+    if (e->s) cudaStreamDestroy(e->s);
     delete e;
 }
 

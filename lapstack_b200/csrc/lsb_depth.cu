@@ -79,8 +79,9 @@ __global__ void gf_var_kernel(const float* __restrict__ mean_i, float* __restric
         var_i[i] = fmaxf(__fsub_rn(var_i[i], __fmul_rn(mean_i[i], mean_i[i])), 0.f);
 }
 // depth.rs:385: a = (corr - mean_i * mean_p) / (var_i + eps), b = mean_p - a * mean_i
-__global__ void gf_ab_kernel(const float* __restrict__ mp, const float* __restrict__ corr, const float* __restrict__ mi,
-                             const float* __restrict__ vi, float eps, float* __restrict__ a, float* __restrict__ b, size_t n) {
+// b may be the corr buffer itself (gf_coeffs writes b over corr_Ip in place), so neither is __restrict__.
+__global__ void gf_ab_kernel(const float* __restrict__ mp, const float* corr, const float* __restrict__ mi,
+                             const float* __restrict__ vi, float eps, float* __restrict__ a, float* b, size_t n) {
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
         const float av = __fdiv_rn(__fsub_rn(corr[i], __fmul_rn(mi[i], mp[i])), __fadd_rn(vi[i], eps));
         a[i] = av;
