@@ -36,6 +36,26 @@ def test_library_exports_every_declared_symbol():
     assert lib.lsb_abi() == _lib.ABI_VERSION
 
 
+def test_header_is_plain_c_and_links(tmp_path):
+    """A C99 caller (cgo, bindgen, a C host) includes the header and links the library as is."""
+    import shutil
+    import subprocess
+    if shutil.which("gcc") is None:
+        pytest.skip("no gcc")
+    src = tmp_path / "abi.c"
+    src.write_text('#include "lapstack_b200.h"\n#include <stdio.h>\n'
+                   'int main(void) { printf("%u\\n", (unsigned)lsb_abi()); return 0; }\n')
+    exe = tmp_path / "abi"
+    libdir = os.path.dirname(_lib.LIB_PATH)
+    cc = subprocess.run(["gcc", "-std=c99", "-Wall", "-Wextra", "-pedantic", "-Werror", "-I", os.path.dirname(HEADER),
+                         str(src), "-L", libdir, "-llapstack_b200", f"-Wl,-rpath,{libdir}", "-o", str(exe)],
+                        capture_output=True, text=True)
+    assert cc.returncode == 0, cc.stderr
+    run = subprocess.run([str(exe)], capture_output=True, text=True, timeout=60)
+    assert run.returncode == 0, run.stderr
+    assert int(run.stdout) == _lib.ABI_VERSION
+
+
 def test_no_cpu_fallback_without_a_device():
     import torch
     if torch.cuda.is_available():
