@@ -56,6 +56,29 @@ def test_header_is_plain_c_and_links(tmp_path):
     assert int(run.stdout) == _lib.ABI_VERSION
 
 
+def header_arity():
+    src = re.sub(r"/\*.*?\*/", "", open(HEADER).read(), flags=re.S)
+    out = {}
+    for name, args in re.findall(r"\b(lsb_[a-z0-9_]+)\s*\(([^()]*)\)\s*;", src):
+        args = args.strip()
+        out[name] = 0 if args in ("", "void") else args.count(",") + 1
+    return out
+
+
+def test_rust_binding_in_the_guide_matches_the_header():
+    """Every `pub fn` of the Rust extern block in INTEGRATION.md is declared in the header with as many arguments."""
+    guide = open(os.path.join(os.path.dirname(HEADER), "..", "INTEGRATION.md")).read()
+    block = re.search(r'extern "C" \{(.*?)\n\}', guide, flags=re.S).group(1)
+    block = re.sub(r"//[^\n]*", "", block)
+    fns = re.findall(r"pub fn (lsb_[a-z0-9_]+)\(([^()]*)\)", block)
+    assert len(fns) >= 15
+    arity = header_arity()
+    for name, args in fns:
+        assert name in arity, name
+        n = 0 if not args.strip() else args.strip().rstrip(",").count(",") + 1
+        assert n == arity[name], (name, n, arity[name])
+
+
 def test_no_cpu_fallback_without_a_device():
     import torch
     if torch.cuda.is_available():
