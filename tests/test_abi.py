@@ -79,6 +79,12 @@ def test_rust_binding_in_the_guide_matches_the_header():
         assert n == arity[name], (name, n, arity[name])
 
 
+def test_ctypes_table_matches_the_header_arity():
+    arity = header_arity()
+    for name, (_res, args) in _lib.SIGNATURES.items():
+        assert len(args) == arity[name], (name, len(args), arity[name])
+
+
 def test_no_cpu_fallback_without_a_device():
     import torch
     if torch.cuda.is_available():
