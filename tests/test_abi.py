@@ -85,6 +85,34 @@ def test_ctypes_table_matches_the_header_arity():
         assert len(args) == arity[name], (name, len(args), arity[name])
 
 
+def test_ctypes_structs_have_the_header_layout(tmp_path):
+    """Size and every field offset of the ctypes mirrors, against what a C compiler makes of the header."""
+    import shutil
+    import subprocess
+    if shutil.which("gcc") is None:
+        pytest.skip("no gcc")
+    structs = {"lsb_config": _lib.Config, "lsb_fuse_params": _lib.FuseParamsC, "lsb_align_params": _lib.AlignParamsC,
+               "lsb_depth_params": _lib.DepthParamsC, "lsb_result": _lib.Result, "lsb_tuning": _lib.Tuning,
+               "lsb_synth_desc": _lib.SynthDesc}
+    rename = {"lam": "lambda"}
+    body, want = [], []
+    for cname, cls in structs.items():
+        body.append(f'printf("%zu\\n", sizeof({cname}));')
+        want.append(C.sizeof(cls))
+        for fname, *_ in cls._fields_:
+            body.append(f'printf("%zu\\n", offsetof({cname}, {rename.get(fname, fname)}));')
+            want.append(getattr(cls, fname).offset)
+    src = tmp_path / "layout.c"
+    src.write_text('#include "lapstack_b200.h"\n#include <stdio.h>\n#include <stddef.h>\nint main(void) {\n'
+                   + "\n".join(body) + "\nreturn 0;\n}\n")
+    exe = tmp_path / "layout"
+    cc = subprocess.run(["gcc", "-std=c99", "-I", os.path.dirname(HEADER), str(src), "-o", str(exe)],
+                        capture_output=True, text=True)
+    assert cc.returncode == 0, cc.stderr
+    got = [int(v) for v in subprocess.run([str(exe)], capture_output=True, text=True, timeout=60).stdout.split()]
+    assert got == want
+
+
 def test_no_cpu_fallback_without_a_device():
     import torch
     if torch.cuda.is_available():
