@@ -1,0 +1,40 @@
+"""The host mirror's parameter defaults are the reference's, so a caller that
+switches backends without naming a parameter gets the same stack. CPU only."""
+import lapstack_b200 as L
+from lapstack_b200 import _lib
+
+
+def test_fuse_defaults_are_the_reference_defaults():
+    # fuse.rs:94-107: levels None (auto), energy radius 1, DevEntropy top rule of radius 2 over 256 bins,
+    # no chroma, depth level 2, halo control off
+    p = L.FuseParams()
+    assert (p.levels, p.energy_radius, p.top_rule, p.top_radius, p.entropy_bins, p.use_chroma, p.depth_level,
+            p.halo) == (0, 1, "de", 2, 256, False, 2, 0.0)
+    c = p.c()
+    assert (c.levels, c.energy_radius, c.top_rule, c.top_radius, c.entropy_bins, c.use_chroma, c.depth_level) == \
+        (0, 1, 0, 2, 256, 0, 2)
+
+
+def test_align_defaults_are_the_reference_defaults():
+    # align.rs:66-70: shift, scale and rotation free, similarity model (align.rs:88), no coarsening,
+    # Spline4x4 interpolation (align.rs:137)
+    p = L.AlignParams()
+    assert (p.shift, p.scale, p.rotation, p.model, p.coarsen, p.interp) == (True, True, True, "similarity", 0, "spline4x4")
+    assert p.free() == [True, True, True, True, False, False, False, False]
+    c = p.c()
+    assert (c.enabled, c.shift, c.scale, c.rotation, c.model, c.coarsen, c.host_search) == (1, 1, 1, 1, 0, 0, 0)
+    assert L.engine.INTERPS[c.interp] == "spline4x4"
+
+
+def test_depth_defaults_are_the_reference_defaults():
+    # depth.rs:93-109: scale 1, RDF focus r_in 1 / r_out 3, aggregation radius 3 and eps 1e-4, lambda 3,
+    # sigma_c 0.04, 200 CG iterations, median on, guided upsampling radius 2 eps 1e-2, gate 1, robust 1
+    p = L.DepthParams()
+    assert (p.scale, p.focus, p.r_in, p.r_out, p.agg_radius, p.agg_eps, p.lam, p.sigma_c, p.cg_iters, p.median,
+            p.upsample, p.up_radius, p.up_eps, p.gate, p.robust) == \
+        (1, "rdf", 1, 3, 3, 1e-4, 3.0, 0.04, 200, True, "guided", 2, 1e-2, 1.0, 1.0)
+    # the two switches that leave the reference's formulas are off by default
+    assert (p.edge_mode, p.vcycle_mode) == (0, 0)
+    c = p.c()
+    assert isinstance(c, _lib.DepthParamsC)
+    assert (c.enabled, c.focus, c.upsample, c.median) == (1, 0, 1, 1)
