@@ -119,6 +119,7 @@ std::vector<T> expand(const T* coarse, size_t cw, size_t ch, size_t ow, size_t o
     return out;
 }
 
+// pyramid.rs:170 `reduce3`
 template <class T>
 Img3<T> reduce3(const Img3<T>& im) {
     Img3<T> o;
@@ -126,6 +127,7 @@ Img3<T> reduce3(const Img3<T>& im) {
     return o;
 }
 
+// pyramid.rs:177 `expand3`
 template <class T>
 Img3<T> expand3(const Img3<T>& im, size_t ow, size_t oh) {
     Img3<T> o;

@@ -433,6 +433,7 @@ void thomas_line(T* u, const T* f, const T* wd, const T* a, size_t n, size_t str
     u[(n - 1) * stride] = dp[n - 1];
     for (size_t i = n - 1; i-- > 0;) u[i * stride] = dp[i] - cp[i] * u[(i + 1) * stride];
 }
+// depth.rs:677 `solve_rows`
 template <class T>
 void solve_rows(T* u, const T* f, const T* wd, const T* a, size_t w, size_t h, T lam) {
 #pragma omp parallel for schedule(static)
@@ -442,6 +443,7 @@ void solve_rows(T* u, const T* f, const T* wd, const T* a, size_t w, size_t h, T
         thomas_line<T>(u + o, f + o, wd + o, a + o, w, 1, lam, cp.data(), dp.data());
     }
 }
+// depth.rs:707 `solve_cols`
 template <class T>
 void solve_cols(T* u, const T* f, const T* wd, const T* a, size_t w, size_t h, T lam) {
 #pragma omp parallel for schedule(static)
@@ -583,6 +585,8 @@ void vcycle(std::vector<MgLevel<T>>& lv, size_t l) {
     for (size_t k = 0; k < MG_POST; k++) top.jacobi(false);
 }
 
+// depth.rs:1037 the CG's `dot`: f64 products summed (here in index order; the reference's rayon
+// split only moves the sum at the 1e-16 level)
 template <class T>
 double dot(const T* a, const T* b, size_t n) {
     double s = 0.0;

@@ -49,6 +49,8 @@ inline uint16_t u16_of(T v) {
     return (uint16_t)(c * LIT(65535.0) + LIT(0.5));
 }
 
+// stack.rs:1011 `run_with` for frames already decoded: register and gain each frame, fold them
+// (stack.rs:740 `fuse_range`), then the depth pass (stack.rs:833 `fuse_and_depth`) and the crop
 template <class T>
 StackOutput<T> run_stack(const uint16_t* const* frames, size_t n, size_t w, size_t h, const StackParams& sp) {
     StackOutput<T> out;
