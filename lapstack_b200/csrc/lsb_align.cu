@@ -151,7 +151,7 @@ __global__ void cost_kernel(const float* __restrict__ rf, int aw, int ah, const 
     if (threadIdx.x == 0)
         for (int q = 0; q < 3; q++) part[((size_t)k * gridDim.x + blockIdx.x) * 3 + q] = red[q][0];
 }
-// The per-block partials of every candidate summed in a fixed order: one
+// align.rs:581 `warp_cost`, its f64 sums (align.rs:629): the per-block partials of every candidate summed in a fixed order: one
 // block per candidate, each thread a fixed stride of blocks, then a tree.
 __global__ void cost_final_kernel(const double* __restrict__ part, int nblocks, int ncand, double* __restrict__ out) {
     const int k = blockIdx.x;
@@ -192,12 +192,13 @@ __device__ __forceinline__ float warp_plane_px(const float* __restrict__ src, in
     }
     return acc;
 }
+// align.rs:542 `warp_plane`, one thread per output pixel.
 __global__ void warp_plane_kernel(const float* __restrict__ src, int w, int h, const WarpXform xf, float* __restrict__ out) {
     const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
     if (x >= w || y >= h) return;
     out[(size_t)y * w + x] = warp_plane_px(src, w, h, xf.inv, xf.affine, xf.interp, x, y);
 }
-// The same with the warp a search left in device memory: inverse [9],
+// align.rs:542 `warp_plane` with the warp a search left in device memory: inverse [9],
 // affine flag, identity flag (an identity result copies the plane, as the
 // host path does).
 __global__ void warp_plane_dev_kernel(const float* __restrict__ src, int w, int h, const double* __restrict__ wd, int interp,
@@ -355,7 +356,7 @@ cudaError_t warp_plane(const float* src, int w, int h, const WarpXform& xf, floa
     return cudaGetLastError();
 }
 
-// The Spline4x4 form over 64x16 tiles: the tile's source footprint (its
+// align.rs:542 `warp_plane` in its Spline4x4 form over 64x16 tiles: the tile's source footprint (its
 // corners' images, the taps' reach and a pixel of margin, clamped like the
 // taps) is staged in shared memory once; the taps, weights and sums are
 // warp_plane_px's. Identity warps copy; tiles whose footprint does not fit,
@@ -948,6 +949,7 @@ __device__ __forceinline__ double warp_sum(double v) {
 }
 
 constexpr int NM_THREADS = 256, NM_WARPS = NM_THREADS / 32;
+// align.rs:896 `multiscale_align` of one frame: the NmJob's whole coarse-to-fine search.
 __global__ void __launch_bounds__(NM_THREADS) nm_search_kernel(const NmJob J) {
     __shared__ NmState S;
     __shared__ double cand[MAX_CAND][9];

@@ -48,7 +48,7 @@ __device__ __forceinline__ float box_inv_count(int x, int y, int w, int h, int r
     return __fdiv_rn(1.f, __fmul_rn(cy, cx));
 }
 
-// Horizontal box sums (optionally of a*b), f64 window sum rounded to f32.
+// depth.rs:285 `BoxFilter::sum_into`, horizontal pass: box sums (optionally of a*b), f64 window sum rounded to f32.
 __global__ void box_h_kernel(const float* __restrict__ a, const float* __restrict__ b, float* __restrict__ out, int w, int h, int r) {
     const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
     if (x >= w || y >= h) return;
@@ -58,7 +58,7 @@ __global__ void box_h_kernel(const float* __restrict__ a, const float* __restric
     for (int t = max(x - r, 0); t <= min(x + r, w - 1); t++) s += rb ? (double)__fmul_rn(ra[t], rb[t]) : (double)ra[t];
     out[(size_t)y * w + x] = (float)s;
 }
-// Vertical box sums of the horizontal sums, rounded to f32, times the inverse count.
+// depth.rs:285/337 `BoxFilter::sum_into` / `mean_into`, vertical pass: box sums of the horizontal sums, rounded to f32, times the inverse count.
 __global__ void box_v_kernel(const float* __restrict__ hs, float* __restrict__ out, int w, int h, int r) {
     const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
     if (x >= w || y >= h) return;
@@ -136,6 +136,8 @@ __device__ __forceinline__ void peak_push(PeakState& p, float v, int m) {
     p.prev = v;
 }
 
+// depth.rs:1119 `depth_from_slices`: each focus slice's guided-filter aggregation (depth.rs:401
+// `GuidedFilter::filter_into`) fed straight to the peak tracker (depth.rs:547 `PeakTracker::push`).
 // RT: the aggregation radius as a compile-time constant (0: a.r at run time).
 // Tiles whose windows stay inside the grid take fixed, unrolled 2R+1-tap
 // windows; border tiles clip them as BoxFilter does.
@@ -423,7 +425,7 @@ __global__ void __launch_bounds__(256, 2) aggregate_kernel(const AggArgs a) {
     }
 }
 
-// Without aggregation (agg_radius 0) the slices go to the tracker as they are.
+// Without aggregation (agg_radius 0) the slices go to the tracker (depth.rs:547) as they are.
 template <class SS>
 __global__ void peaks_raw_kernel(const SS* __restrict__ slices, int n, size_t m, float* __restrict__ S) {
     for (size_t o = blockIdx.x * (size_t)blockDim.x + threadIdx.x; o < m; o += (size_t)gridDim.x * blockDim.x) {
@@ -487,6 +489,8 @@ cudaError_t aggregate_peaks(AggArgs a, bool slice_fp16, cudaStream_t s, int grid
 }
 
 // ------------------------------------------------------------- k-th value
+// depth.rs:580 and :618 `select_nth_unstable_by(total_cmp)` (the noise floor's median, p90):
+// the k-th value by a two-pass 16-bit radix histogram of total-order keys.
 // The key of a float in the total order (total_cmp): monotone as u32.
 __device__ __forceinline__ unsigned fkey(float f) {
     unsigned b = __float_as_uint(f);
@@ -659,7 +663,7 @@ __global__ void upsample_kernel(const float* __restrict__ abar, const float* __r
     depth[o] = fminf(fmaxf(d, 0.f), max_d);
     conf_full[o] = bil(conf, dw, x0, x1, y0, y1, tx, ty);
 }
-// The k == 1 case: q = a-bar * I + b-bar on the grid itself, clamped.
+// depth.rs:1184, guided upsampling when k == 1: q = a-bar * I + b-bar on the grid itself, clamped.
 __global__ void apply_grid_kernel(const float* __restrict__ abar, const float* __restrict__ bbar, const float* __restrict__ guide,
                                   size_t m, float max_d, int guided, float* __restrict__ depth) {
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < m; i += (size_t)gridDim.x * blockDim.x) {

@@ -53,7 +53,7 @@ static cudaError_t with_smem(K k, size_t smem) {
     return cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
 }
 
-// The frame groups' selection states merged in group order: the first group
+// fuse.rs:429 strict `>` across frame groups: the groups' selection states merged in group order: the first group
 // holding the largest energy wins, and within it its first frame did.
 __global__ void select_merge_kernel(const FoldArgs a, int G) {
     const size_t np = (size_t)a.W * a.H;
@@ -361,6 +361,8 @@ cudaError_t collapse_level(const float* acc, const float* coarse, float* out, in
 }
 
 // ------------------------------------------------------------ winner shares
+// fuse.rs:315 `winner_shares`: the plane's largest winning energy, then per frame the cells it
+// wins above 1% of that.
 __global__ void max_kernel(const float* __restrict__ v, int n, float* out) {
     float m = 0.f;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) m = fmaxf(m, v[i]);
@@ -407,6 +409,7 @@ __global__ void means_partial_kernel(const uint16_t* __restrict__ frames, int w,
     if (threadIdx.x == 0)
         for (int c = 0; c < 3; c++) partial[((size_t)k * nparts + part) * 3 + c] = red[c][0];
 }
+// brightness.rs:67: each frame's partials summed in part order.
 __global__ void means_final_kernel(const double* partial, int n, int nparts, int count, double* means) {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= n) return;

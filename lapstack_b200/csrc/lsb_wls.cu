@@ -100,6 +100,7 @@ __device__ __forceinline__ float block_sum_at(const float* __restrict__ src, int
     }
     return o;
 }
+// depth.rs:911 `restrict` (and the 2x2 aggregation of depth.rs:852 `coarsen`): 2x2 block sums.
 __global__ void block_sum_kernel(const float* __restrict__ src, int w, int h, float* __restrict__ dst, int cw, int ch) {
     const int xx = blockIdx.x * blockDim.x + threadIdx.x, yy = blockIdx.y * blockDim.y + threadIdx.y;
     if (xx >= cw || yy >= ch) return;
@@ -133,6 +134,7 @@ __device__ __forceinline__ float stencil_at(const float* __restrict__ x, const f
     if (mode == 1) return __fsub_rn(b[k], v);
     return __fadd_rn(xk, __fmul_rn(__fmul_rn(MG_OMEGA, dinv[k]), __fsub_rn(b[k], v)));
 }
+// depth.rs:786 `MgLevel::apply` (mode 0: A x; 1: b - A x) and :837 `jacobi` (mode 2).
 __global__ void stencil_kernel(const float* __restrict__ x, const float* __restrict__ b, const float* __restrict__ wd,
                                const float* __restrict__ ax, const float* __restrict__ ay, const float* __restrict__ dinv,
                                float* __restrict__ out, int w, int h, int mode) {
@@ -185,6 +187,7 @@ __device__ __forceinline__ void tail_sweep(const WlsLevel& L, bool zero) {
     for (int k = threadIdx.x; k < n; k += blockDim.x) L.x[k] = L.r[k];
     __syncthreads();
 }
+// depth.rs:924 `vcycle` from the first level small enough for one CTA down to the coarsest.
 __global__ void __launch_bounds__(1024) vcycle_tail_kernel(const MgTail T) {
     for (int l = 0; l + 1 < T.n; l++) {
         const WlsLevel &L = T.lv[l], &C = T.lv[l + 1];
@@ -457,7 +460,7 @@ __global__ void __launch_bounds__(32 * P) pthomas_kernel(float* __restrict__ u, 
 }
 constexpr int PT_ROWS = 8, PT_COLS = 16;
 
-// The row sweep with one row per warp held in shared memory (the partition
+// depth.rs:677 `solve_rows`: the row sweep with one row per warp held in shared memory (the partition
 // method of pthomas_kernel with 32 segments, lane = segment): a row's
 // coefficients are read once, coalesced, and every step of the segments'
 // sweeps hits shared memory (segments start w/32 floats apart: no bank
@@ -585,7 +588,8 @@ static void thomas(bool rows, float* u, const float* f, const float* wd, int uni
 // ------------------------------------------------ the BF16 V-cycle (mode 1)
 // The preconditioner's smoother, residual, restriction and prolongation on
 // BF16 copies of the level operators and vectors, arithmetic in FP32; the
-// outer CG stays FP32 with FP64 dot products.
+// outer CG stays FP32 with FP64 dot products. No reference counterpart: the
+// reference's V-cycle is FP32 (vcycle_mode 0 here).
 typedef __nv_bfloat16 bf;
 __device__ __forceinline__ float ldh(const uint16_t* p, size_t k) { return __bfloat162float(((const bf*)p)[k]); }
 __device__ __forceinline__ void sth(uint16_t* p, size_t k, float v) { ((bf*)p)[k] = __float2bfloat16_rn(v); }
@@ -631,7 +635,7 @@ __global__ void prolong_h_kernel(uint16_t* __restrict__ x, int w, int h, const u
     sth(x, k, ldh(x, k) + ldh(xc, (size_t)(y / 2) * cw + i / 2));
 }
 
-// f64 dot products: per-block partials, then the partials in order.
+// depth.rs:1037 `dot`, f64 products: per-block partials, then the partials in order.
 __global__ void dot_partial_kernel(const float* __restrict__ a, const float* __restrict__ b, size_t n, double* part) {
     double s = 0.0;
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
@@ -645,7 +649,7 @@ __global__ void dot_partial_kernel(const float* __restrict__ a, const float* __r
     }
     if (threadIdx.x == 0) part[blockIdx.x] = red[0];
 }
-// mode: 0 rz; 1 pap -> alpha; 2 rz_new -> beta; 3 rr -> rel; 4 bb -> bnorm
+// depth.rs:1039-1072, the CG scalars. mode: 0 rz; 1 pap -> alpha; 2 rz_new -> beta; 3 rr -> rel; 4 bb -> bnorm
 __global__ void dot_final_kernel(const double* part, int nparts, double* scal, float* ab, float* host_rel, int mode) {
     // the partials summed by 256 threads (each a fixed stride of them), then a fixed tree
     __shared__ double red[256];
@@ -676,6 +680,7 @@ __global__ void dot_final_kernel(const double* part, int nparts, double* scal, f
         scal[3] = fmax(sqrt(s), 1e-30);
     }
 }
+// depth.rs:1064-1065: u += alpha p, r -= alpha Ap.
 __global__ void axpy2_kernel(float* __restrict__ u, const float* __restrict__ p, float* __restrict__ r, const float* __restrict__ ap,
                              const float* ab, size_t n) {
     const float alpha = ab[0];
@@ -684,11 +689,13 @@ __global__ void axpy2_kernel(float* __restrict__ u, const float* __restrict__ p,
         r[i] = __fsub_rn(r[i], __fmul_rn(alpha, ap[i]));
     }
 }
+// depth.rs:1074: p = z + beta p.
 __global__ void pupd_kernel(float* __restrict__ p, const float* __restrict__ z, const float* ab, size_t n) {
     const float beta = ab[1];
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
         p[i] = __fadd_rn(z[i], __fmul_rn(beta, p[i]));
 }
+// depth.rs:1039: b = w d.
 __global__ void mul_kernel(const float* __restrict__ a, const float* __restrict__ b, float* __restrict__ o, size_t n) {
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
         o[i] = __fmul_rn(a[i], b[i]);
