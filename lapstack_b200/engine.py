@@ -25,6 +25,30 @@ from ._lib import (AlignParamsC, Config, DepthParamsC, FuseParamsC, LOG_FN, LsbE
 TOP_RULES = {"de": 0, "dev": 1, "avg": 2}
 INTERPS = ["nearest", "bilinear", "bicubic", "spline4x4", "spline6x6", "lanczos3"]
 MODELS = ["similarity", "affine", "projective"]
+FOCUS = ["rdf", "sml"]
+UPSAMPLE = ["bilinear", "guided"]
+# the other spellings the reference's parsers accept, by canonical name
+TOP_RULE_ALIASES = {"dev-entropy": "de", "deviation": "dev", "average": "avg"}  # fuse.rs:59
+MODEL_ALIASES = {"sim": "similarity", "perspective": "projective", "homography": "projective"}  # align.rs:95
+INTERP_ALIASES = {"nn": "nearest", "linear": "bilinear", "cubic": "bicubic", "spline16": "spline4x4",
+                  "spline36": "spline6x6", "lanczos": "lanczos3"}  # align.rs:148
+
+
+def _canon(name, names, what, aliases=None, fold=False):
+    """The canonical spelling of a named option. The reference's parsers (fuse.rs:59, align.rs:95 and
+    :148, which also trim and lower-case, depth.rs:112 and :127) return None for an unknown name: here
+    that is an LsbError naming the choices."""
+    key = name.strip().lower() if fold and isinstance(name, str) else name
+    key = (aliases or {}).get(key, key)
+    if key in names:
+        return key
+    raise LsbError(f"unknown {what} {name!r}: one of {', '.join(names)}")
+
+
+def _pick(name, names, what, aliases=None, fold=False):
+    """The C-ABI code of a named option (its index in `names`, or its value when `names` is a dict)."""
+    key = _canon(name, names, what, aliases, fold)
+    return names[key] if isinstance(names, dict) else names.index(key)
 
 
 @dataclass
@@ -39,7 +63,8 @@ class FuseParams:  # fuse.rs:70-107
     halo: float = 0.0
 
     def c(self):
-        return FuseParamsC(self.levels, self.energy_radius, TOP_RULES[self.top_rule], self.top_radius, self.entropy_bins,
+        return FuseParamsC(self.levels, self.energy_radius, _pick(self.top_rule, TOP_RULES, "top rule", TOP_RULE_ALIASES),
+                           self.top_radius, self.entropy_bins,
                            int(self.use_chroma), self.depth_level, self.halo)
 
 
@@ -54,11 +79,13 @@ class AlignParams:  # align.rs:52-70
     host_search: bool = False  # True: the host drives Nelder-Mead, one launch per simplex step
 
     def c(self, enabled=True):
-        return AlignParamsC(int(enabled), int(self.shift), int(self.scale), int(self.rotation), MODELS.index(self.model),
-                            self.coarsen, INTERPS.index(self.interp), int(self.host_search))
+        return AlignParamsC(int(enabled), int(self.shift), int(self.scale), int(self.rotation),
+                            _pick(self.model, MODELS, "alignment model", MODEL_ALIASES, fold=True), self.coarsen,
+                            _pick(self.interp, INTERPS, "interpolation", INTERP_ALIASES, fold=True), int(self.host_search))
 
     def free(self):
-        a, p = self.model != "similarity", self.model == "projective"
+        model = _canon(self.model, MODELS, "alignment model", MODEL_ALIASES, fold=True)
+        a, p = model != "similarity", model == "projective"
         return [self.shift, self.shift, self.scale, self.rotation, a, a, p, p]
 
 
@@ -84,10 +111,10 @@ class DepthParams:  # depth.rs:69-109
     vcycle_mode: int = 0  # 0: FP32 V-cycle as the reference; 1: BF16 smoother and restriction
 
     def c(self, enabled=True):
-        return DepthParamsC(int(enabled), self.scale, 0 if self.focus == "rdf" else 1, self.r_in, self.r_out, self.sml_step,
-                            self.agg_radius, self.agg_eps, self.lam, self.sigma_c, self.cg_iters, int(self.median),
-                            0 if self.upsample == "bilinear" else 1, self.up_radius, self.up_eps, self.gate, self.robust,
-                            self.edge_mode, self.vcycle_mode)
+        return DepthParamsC(int(enabled), self.scale, _pick(self.focus, FOCUS, "focus measure"), self.r_in, self.r_out,
+                            self.sml_step, self.agg_radius, self.agg_eps, self.lam, self.sigma_c, self.cg_iters,
+                            int(self.median), _pick(self.upsample, UPSAMPLE, "upsampling"), self.up_radius, self.up_eps,
+                            self.gate, self.robust, self.edge_mode, self.vcycle_mode)
 
 
 @dataclass

@@ -1,5 +1,8 @@
-"""The host mirror's parameter defaults are the reference's, so a caller that
-switches backends without naming a parameter gets the same stack. CPU only."""
+"""The host mirror's parameter defaults and option names are the reference's,
+so a caller that switches backends gets the same stack from the same settings,
+and a misspelt option is an error rather than another option. CPU only."""
+import pytest
+
 import lapstack_b200 as L
 from lapstack_b200 import _lib
 
@@ -38,3 +41,32 @@ def test_depth_defaults_are_the_reference_defaults():
     c = p.c()
     assert isinstance(c, _lib.DepthParamsC)
     assert (c.enabled, c.focus, c.upsample, c.median) == (1, 0, 1, 1)
+
+
+def test_option_names_take_the_reference_spellings():
+    # fuse.rs:59 TopRule::parse
+    for name, code in [("de", 0), ("dev-entropy", 0), ("dev", 1), ("deviation", 1), ("avg", 2), ("average", 2)]:
+        assert L.FuseParams(top_rule=name).c().top_rule == code
+    # align.rs:95 AlignModel::parse and align.rs:148 Interp::parse trim and lower-case
+    for name, code in [("similarity", 0), (" Sim ", 0), ("affine", 1), ("projective", 2), ("perspective", 2),
+                       ("HOMOGRAPHY", 2)]:
+        assert L.AlignParams(model=name).c().model == code
+    assert L.AlignParams(model="sim").free() == L.AlignParams().free()
+    assert L.AlignParams(model="homography").free() == [True] * 8
+    for name, code in [("nn", 0), ("linear", 1), ("cubic", 2), ("spline16", 3), ("Spline4x4", 3), ("spline36", 4),
+                       ("lanczos", 5)]:
+        assert L.AlignParams(interp=name).c().interp == code
+    assert (L.DepthParams(focus="sml").c().focus, L.DepthParams(upsample="bilinear").c().upsample) == (1, 0)
+
+
+@pytest.mark.parametrize("make", [lambda: L.FuseParams(top_rule="entropy").c(),
+                                  lambda: L.AlignParams(model="rigid").c(),
+                                  lambda: L.AlignParams(model="rigid").free(),
+                                  lambda: L.AlignParams(interp="spline8x8").c(),
+                                  lambda: L.DepthParams(focus="laplacian").c(),
+                                  lambda: L.DepthParams(upsample="nearest").c(),
+                                  lambda: L.DepthParams(upsample="Guided").c()])
+def test_unknown_option_names_are_errors(make):
+    """An unknown name is refused (the reference's parsers return None), never mapped to another option."""
+    with pytest.raises(L.LsbError, match="unknown"):
+        make()
