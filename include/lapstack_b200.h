@@ -144,6 +144,11 @@ void lsb_engine_destroy(lsb_engine* e);
 /* The engine's CUDA stream (cudaStream_t), for callers that share it. */
 void* lsb_engine_stream(lsb_engine* e);
 
+/* Checks settings without a device or an engine: NULL, or the error lsb_stack_begin would return
+   for them (any pointer may be NULL; align and depth settings count only when enabled). The
+   reference needs no counterpart: its options are typed enums, while a C caller passes codes. */
+char* lsb_check_params(const lsb_fuse_params* fuse, const lsb_align_params* align, const lsb_depth_params* depth);
+
 char* lsb_stack_begin(lsb_engine* e, uint32_t w, uint32_t h, uint32_t n_frames, const lsb_fuse_params* fuse,
                       const lsb_align_params* align, const lsb_depth_params* depth, int32_t brightness, int32_t crop,
                       lsb_stack** out);

@@ -79,6 +79,7 @@ SIGNATURES = {
     "lsb_engine_create": (ERR, [C.POINTER(Config), C.POINTER(P)]),
     "lsb_engine_destroy": (None, [P]),
     "lsb_engine_stream": (P, [P]),
+    "lsb_check_params": (ERR, [C.POINTER(FuseParamsC), C.POINTER(AlignParamsC), C.POINTER(DepthParamsC)]),
     "lsb_stack_begin": (ERR, [P, C.c_uint32, C.c_uint32, C.c_uint32, C.POINTER(FuseParamsC), C.POINTER(AlignParamsC),
                               C.POINTER(DepthParamsC), C.c_int32, C.c_int32, C.POINTER(P)]),
     "lsb_stack_push_u16": (ERR, [P, P, C.c_size_t]),

@@ -434,6 +434,40 @@ static char* stack_alloc(lsb_stack* s) {
     return nullptr;
 }
 
+// The settings' ranges: the codes the reference's typed options can take (fuse.rs:59 TopRule,
+// align.rs:95 AlignModel, align.rs:148 Interp, depth.rs:112 FocusMeasure, depth.rs:127 Upsample),
+// which a C caller could otherwise pass out of range and have read as another option, and the
+// radii this engine's kernels are built for. Align and depth settings count only when enabled.
+static const char* params_error(const lsb_fuse_params* f, const lsb_align_params* a, const lsb_depth_params* d) {
+    if (f) {
+        if (f->energy_radius > 2) return "energy_radius must be 0..2";
+        if (f->top_rule > 2) return "top_rule must be 0 (dev-entropy), 1 (deviation) or 2 (average)";
+        if (f->top_radius > 4) return "top_radius must be 0..4";
+    }
+    if (a && a->enabled) {
+        if (a->model > 2) return "align model must be 0 (similarity), 1 (affine) or 2 (projective)";
+        if (a->interp > 5) return "interp must be 0..5 (nearest, bilinear, bicubic, spline4x4, spline6x6, lanczos3)";
+    }
+    if (d && d->enabled) {
+        if (d->scale > 2) return "depth scale must be 0..2";
+        if (d->focus > 1) return "focus must be 0 (ring difference) or 1 (sum-modified Laplacian)";
+        if (d->focus == 0 && (d->r_out > 3 || d->r_out <= d->r_in)) return "rdf radii: r_in < r_out <= 3";
+        if (d->focus == 1 && (d->sml_step < 1 || d->sml_step > 3)) return "sml step must be 1..3";
+        // bounded first: the tile size below is computed in int
+        if (d->agg_radius > 64 || aggregate_smem_bytes((int)d->agg_radius) > 227 * 1024) return "agg_radius too large";
+        if (d->upsample > 1) return "upsample must be 0 (bilinear) or 1 (guided)";
+        if (d->up_radius > (1u << 20)) return "up_radius must be at most 2^20";
+        if (d->edge_mode > 1) return "edge_mode must be 0 or 1";
+        if (d->vcycle_mode > 1) return "vcycle_mode must be 0 or 1";
+    }
+    return nullptr;
+}
+
+extern "C" char* lsb_check_params(const lsb_fuse_params* fuse, const lsb_align_params* align, const lsb_depth_params* depth) {
+    const char* bad = params_error(fuse, align, depth);
+    return bad ? dup_err(bad) : nullptr;
+}
+
 extern "C" char* lsb_stack_begin(lsb_engine* e, uint32_t w, uint32_t h, uint32_t n_frames, const lsb_fuse_params* fuse,
                                  const lsb_align_params* align, const lsb_depth_params* depth, int32_t brightness, int32_t crop,
                                  lsb_stack** out) {
@@ -458,24 +492,9 @@ extern "C" char* lsb_stack_begin(lsb_engine* e, uint32_t w, uint32_t h, uint32_t
         return dup_err("storage must be 0 (FP32), 1 (UNORM16 levels, FP16 slices) or 2 (FP16)");
     }
     s->f32src = false;
-    if (s->fp.energy_radius > 2) {
+    if (const char* bad = params_error(&s->fp, &s->ap, &s->dp)) {
         delete s;
-        return dup_err("energy_radius must be 0..2");
-    }
-    if (s->fp.top_radius > 4) {
-        delete s;
-        return dup_err("top_radius must be 0..4");
-    }
-    if (s->dp.enabled) {
-        const char* bad = nullptr;
-        if (s->dp.scale > 2) bad = "depth scale must be 0..2";
-        else if (s->dp.focus == 0 && (s->dp.r_out > 3 || s->dp.r_out <= s->dp.r_in)) bad = "rdf radii: r_in < r_out <= 3";
-        else if (s->dp.focus == 1 && (s->dp.sml_step < 1 || s->dp.sml_step > 3)) bad = "sml step must be 1..3";
-        else if (aggregate_smem_bytes((int)s->dp.agg_radius) > 227 * 1024) bad = "agg_radius too large";
-        if (bad) {
-            delete s;
-            return dup_err(bad);
-        }
+        return dup_err(bad);
     }
     // pyramid.rs:191 auto_levels(w, h, 32); fuse.rs:372-373
     uint32_t levels = s->fp.levels;
@@ -1492,6 +1511,7 @@ extern "C" char* lsb_wls_solve(lsb_engine* e, const float* d, const float* conf,
                                float lambda, float sigma_c, uint32_t max_iters, uint32_t edge_mode, uint32_t vcycle_mode, float* u,
                                float* rel, uint32_t* iters, double* ms) {
     if (!e || !d || !conf || !guide || !u) return dup_err("null argument");
+    if (edge_mode > 1 || vcycle_mode > 1) return dup_err("edge_mode and vcycle_mode must be 0 or 1");
     cudaStream_t st = e->s;
     const size_t m = (size_t)w * h;
     DevPool P;

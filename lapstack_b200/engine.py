@@ -216,6 +216,16 @@ class Engine:
         return Stack(self, w, h, n, fuse, align, depth, brightness, crop)
 
 
+def check_params(fuse=None, align=None, depth=None):
+    """Raises LsbError for settings a stack would refuse (lsb_check_params); needs no device.
+    None stands for the defaults (fuse) or for the pass being off (align, depth), as in Engine.stack."""
+    L = load()
+    fp = (fuse or FuseParams()).c()
+    ap = (align or AlignParams()).c(enabled=align is not None)
+    dp = (depth or DepthParams()).c(enabled=depth is not None)
+    check(L.lsb_check_params(C.byref(fp), C.byref(ap), C.byref(dp)))
+
+
 _default = None
 
 

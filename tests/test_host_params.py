@@ -70,3 +70,65 @@ def test_unknown_option_names_are_errors(make):
     """An unknown name is refused (the reference's parsers return None), never mapped to another option."""
     with pytest.raises(L.LsbError, match="unknown"):
         make()
+
+
+def c_check(fp=None, ap=None, dp=None):
+    """lsb_check_params on raw C structs (codes the Python names cannot produce); None or the error text."""
+    import ctypes as C
+    lib = L.load()
+    err = lib.lsb_check_params(C.byref(fp or L.FuseParams().c()), C.byref(ap or L.AlignParams().c()),
+                               C.byref(dp or L.DepthParams().c()))
+    if not err:
+        return None
+    msg = C.cast(err, C.c_char_p).value.decode()
+    lib.lsb_free_str(err)
+    return msg
+
+
+def test_check_params_accepts_the_defaults_without_a_device():
+    L.check_params()
+    L.check_params(L.FuseParams(), L.AlignParams(), L.DepthParams())
+    L.check_params(L.FuseParams(energy_radius=2, top_rule="avg", top_radius=4),
+                   L.AlignParams(model="projective", interp="lanczos3"),
+                   L.DepthParams(focus="sml", sml_step=3, scale=2, agg_radius=19, upsample="bilinear", edge_mode=1,
+                                 vcycle_mode=1))
+    assert c_check() is None
+
+
+def with_field(struct, **kw):
+    for k, v in kw.items():
+        setattr(struct, k, v)
+    return struct
+
+
+@pytest.mark.parametrize("field,value,text", [
+    ("energy_radius", 3, "energy_radius"), ("top_rule", 3, "top_rule"), ("top_radius", 5, "top_radius")])
+def test_check_params_refuses_fuse_codes_out_of_range(field, value, text):
+    assert text in c_check(fp=with_field(L.FuseParams().c(), **{field: value}))
+
+
+@pytest.mark.parametrize("field,value,text", [("model", 3, "model"), ("interp", 6, "interp")])
+def test_check_params_refuses_align_codes_out_of_range(field, value, text):
+    assert text in c_check(ap=with_field(L.AlignParams().c(), **{field: value}))
+    # a disabled pass is not checked
+    assert c_check(ap=with_field(L.AlignParams().c(enabled=False), **{field: value})) is None
+
+
+@pytest.mark.parametrize("fields,text", [
+    ({"scale": 3}, "scale"), ({"focus": 2}, "focus"), ({"r_in": 3, "r_out": 3}, "rdf radii"),
+    ({"r_out": 4}, "rdf radii"), ({"focus": 1, "sml_step": 0}, "sml step"), ({"focus": 1, "sml_step": 4}, "sml step"),
+    ({"agg_radius": 20}, "agg_radius"), ({"agg_radius": 40000}, "agg_radius"), ({"agg_radius": 0xFFFFFFFF}, "agg_radius"),
+    ({"upsample": 2}, "upsample"), ({"up_radius": (1 << 20) + 1}, "up_radius"), ({"edge_mode": 2}, "edge_mode"),
+    ({"vcycle_mode": 2}, "vcycle_mode")])
+def test_check_params_refuses_depth_settings_out_of_range(fields, text):
+    assert text in c_check(dp=with_field(L.DepthParams().c(), **fields))
+    assert c_check(dp=with_field(L.DepthParams().c(enabled=False), **fields)) is None
+
+
+def test_check_params_largest_aggregation_radius_is_19():
+    # the aggregation tile with its halos must fit the 227 KiB of shared memory a CTA can have:
+    # 232,192 bytes at radius 19, 247,808 at 20
+    assert c_check(dp=with_field(L.DepthParams().c(), agg_radius=19)) is None
+    assert c_check(dp=with_field(L.DepthParams().c(), agg_radius=0)) is None
+    with pytest.raises(L.LsbError, match="agg_radius"):
+        L.check_params(depth=L.DepthParams(agg_radius=20))
