@@ -463,6 +463,15 @@ static const char* params_error(const lsb_fuse_params* f, const lsb_align_params
     return nullptr;
 }
 
+// Image sizes the kernels index safely: one grid row per image row in some launches (at most 65535),
+// and plane offsets within a frame (3 w h) in 32-bit ints.
+static const char* size_error(uint32_t w, uint32_t h) {
+    if (w == 0 || h == 0) return "width and height must be at least 1";
+    if (w > 65535 || h > 65535) return "width and height must be at most 65535";
+    if ((uint64_t)w * h * 3 > 0x7fffffffull) return "at most 715 Mpx per frame (3 w h must fit 31 bits)";
+    return nullptr;
+}
+
 extern "C" char* lsb_check_params(const lsb_fuse_params* fuse, const lsb_align_params* align, const lsb_depth_params* depth) {
     const char* bad = params_error(fuse, align, depth);
     return bad ? dup_err(bad) : nullptr;
@@ -475,6 +484,7 @@ extern "C" char* lsb_stack_begin(lsb_engine* e, uint32_t w, uint32_t h, uint32_t
     if (!e) return dup_err("no engine");
     if (w == 0 || h == 0 || n_frames == 0) return dup_err("a stack needs a size and at least one frame");
     if (n_frames > 65535) return dup_err("at most 65535 frames (the winner map is u16)");
+    if (const char* bad = size_error(w, h)) return dup_err(bad);
     lsb_stack* s = new lsb_stack();
     s->e = e;
     s->w = w;
@@ -1512,6 +1522,7 @@ extern "C" char* lsb_wls_solve(lsb_engine* e, const float* d, const float* conf,
                                float* rel, uint32_t* iters, double* ms) {
     if (!e || !d || !conf || !guide || !u) return dup_err("null argument");
     if (edge_mode > 1 || vcycle_mode > 1) return dup_err("edge_mode and vcycle_mode must be 0 or 1");
+    if (const char* bad = size_error(w, h)) return dup_err(bad);
     cudaStream_t st = e->s;
     const size_t m = (size_t)w * h;
     DevPool P;
@@ -1546,6 +1557,7 @@ extern "C" char* lsb_wls_solve(lsb_engine* e, const float* d, const float* conf,
 extern "C" char* lsb_align_pair(lsb_engine* e, const float* rf, const float* tg, uint32_t w, uint32_t h, const double* init8,
                                 const uint8_t* free8, uint32_t coarsen, double* out8, uint32_t* evals) {
     if (!e || !rf || !tg || !out8) return dup_err("null argument");
+    if (const char* bad = size_error(w, h)) return dup_err(bad);
     cudaStream_t st = e->s;
     DevPool P;
     float *a, *b;
@@ -1578,6 +1590,8 @@ extern "C" char* lsb_align_pair(lsb_engine* e, const float* rf, const float* tg,
 extern "C" char* lsb_warp_cost(lsb_engine* e, const float* rf, uint32_t aw, uint32_t ah, const float* tgt, uint32_t tw, uint32_t th,
                                const double* sim8, double* cost) {
     if (!e || !rf || !tgt || !sim8 || !cost) return dup_err("null argument");
+    if (const char* bad = size_error(aw, ah)) return dup_err(bad);
+    if (const char* bad = size_error(tw, th)) return dup_err(bad);
     cudaStream_t st = e->s;
     DevPool P;
     float *a, *b;
