@@ -53,6 +53,9 @@ def test_option_names_take_the_reference_spellings():
         assert L.AlignParams(model=name).c().model == code
     assert L.AlignParams(model="sim").free() == L.AlignParams().free()
     assert L.AlignParams(model="homography").free() == [True] * 8
+    # align.rs:1208-1209 free_mask
+    assert L.AlignParams(rotation=False, model="affine").free() == [True, True, True, False, True, True, False, False]
+    assert L.AlignParams(model="projective").free() == [True] * 8
     for name, code in [("nn", 0), ("linear", 1), ("cubic", 2), ("spline16", 3), ("Spline4x4", 3), ("spline36", 4),
                        ("lanczos", 5)]:
         assert L.AlignParams(interp=name).c().interp == code

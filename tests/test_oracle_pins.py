@@ -271,6 +271,30 @@ def test_homography_round_trip():  # align.rs:1154
     assert np.array_equal(O.mat_inverse(O.sim_matrix(O.SIM_ID, w, h)), np.eye(3))
 
 
+def test_projective_warp_and_common_area():  # align.rs:1187
+    w, h = 64, 48
+    ramp = np.array([(i % w) + 0.5 * (i // w) for i in range(w * h)], np.float32).reshape(h, w)
+    s = [0, 0, 1, 0, 1, 0.01, 0.04, -0.03]  # Sim { px: 0.04, py: -0.03, shear: 0.01, ..id }
+    o, valid = O.warp_plane(ramp, s, "bilinear")
+    inv = O.mat_inverse(O.sim_matrix(s, w, h))
+
+    def src(x, y):
+        d = inv[2] @ [x, y, 1.0]
+        return (inv[0] @ [x, y, 1.0]) / d, (inv[1] @ [x, y, 1.0]) / d
+
+    for y in range(4, h - 4):
+        for x in range(4, w - 4):
+            sx, sy = src(float(x), float(y))
+            assert valid[y, x] == 1
+            assert abs(float(o[y, x]) - (sx + 0.5 * sy)) < 1e-3, (x, y)
+    x0, y0, rw, rh = O.common_area([O.SIM_ID, s], w, h, "bilinear")
+    assert (rw, rh) != (w, h) and rw > w // 2 and rh > h // 2
+    m = 1.0  # Interp::Bilinear.margin(): half its 2 taps
+    for px, py in [(x0, y0), (x0 + rw - 1, y0), (x0, y0 + rh - 1), (x0 + rw - 1, y0 + rh - 1)]:
+        sx, sy = src(float(px), float(py))
+        assert m <= sx <= w - 1 - m and m <= sy <= h - 1 - m, (px, py, sx, sy)
+
+
 def test_multiscale_align_recovers_a_shift():
     """The search finds a known sub-pixel similarity on a textured plane."""
     w, h = 256, 192
