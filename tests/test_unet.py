@@ -1,5 +1,5 @@
 """The learned warm start's network: the numpy oracle's backward pass against
-finite differences (CPU), and the library's forward, backward and training
+finite differences, its layer table and grid rule (CPU), and the library's forward, backward and training
 kernels against the oracle on the same parameters and inputs (GPU)."""
 import numpy as np
 import pytest
@@ -57,6 +57,25 @@ def _to_gpu(inp, d_in, tgt):
     import torch
     t_in = torch.from_numpy(inp).to(torch.bfloat16).cuda()  # exact: inp is bf16-representable
     return t_in, torch.from_numpy(d_in).cuda(), torch.from_numpy(tgt).cuda()
+
+
+def test_flops_table_is_the_oracle_architecture():
+    """The convolution table behind the bench's U-Net FLOP count describes the oracle's network."""
+    from lapstack_b200 import unet as N
+    assert N.CONVS == [(c1 + c2, co, lv) for (_, _, c1, _, _, c2, co, lv, _) in U.LAYERS]
+    _, nw, _ = U.offsets()
+    assert nw == 9 * sum(ci * co for ci, co, _ in N.CONVS)
+    H, W = 64, 96
+    assert N.forward_flops(H, W, B=2) == 2 * 9 * sum(ci * co * 2 * (H >> lv) * (W >> lv) for ci, co, lv in N.CONVS)
+
+
+def test_network_grid_is_half_the_depth_grid_in_multiples_of_8():
+    from lapstack_b200 import unet as N
+    for dw, dh in [(1, 1), (15, 9), (16, 16), (17, 33), (4128, 2752), (4127, 2751)]:
+        H, W = N.grid_of(dw, dh)
+        hw, hh = (dw + 1) // 2, (dh + 1) // 2
+        assert W % 8 == 0 and H % 8 == 0  # three 2x2 poolings
+        assert hw <= W < hw + 8 and hh <= H < hh + 8
 
 
 @pytest.mark.gpu
