@@ -176,6 +176,8 @@ class DepthParams:  # depth.rs:69-109
     robust: float = 1.0
 
     def arr(self):
+        # a misspelt mode must not silently select the other one
+        assert self.focus in ("rdf", "sml") and self.upsample in ("bilinear", "guided"), (self.focus, self.upsample)
         return [self.scale, 0 if self.focus == "rdf" else 1, self.r_in, self.r_out, self.sml_step, self.agg_radius,
                 self.agg_eps, self.lam, self.sigma_c, self.cg_iters, float(self.median),
                 0 if self.upsample == "bilinear" else 1, self.up_radius, self.up_eps, self.gate, self.robust]
