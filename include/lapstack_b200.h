@@ -134,14 +134,18 @@ typedef struct {
     float warp_shift;       /* translation U(-a, a) px */
 } lsb_synth_desc;
 
+/* The ABI version (LSB_ABI_VERSION), as crates/lapstack-raw/src/ffi.rs:69 lapstack_raw_abi. */
 uint32_t lsb_abi(void);
+/* Frees an error string any entry point returned (ffi.rs:148 lapstack_raw_free_str). */
 void lsb_free_str(char* s);
-/* Kernel launches the library has issued since it was loaded. */
+/* Kernel launches the library has issued since it was loaded (no counterpart in the reference). */
 uint64_t lsb_launch_count(void);
 
+/* gpu.rs:308 `available` and the per-device context set-up (gpu.rs:312-324): one engine per device,
+   its streams and its small persistent buffers. */
 char* lsb_engine_create(const lsb_config* cfg, lsb_engine** out);
 void lsb_engine_destroy(lsb_engine* e);
-/* The engine's CUDA stream (cudaStream_t), for callers that share it. */
+/* The engine's CUDA stream (cudaStream_t), for callers that share it (no counterpart in the reference). */
 void* lsb_engine_stream(lsb_engine* e);
 
 /* Checks settings without a device or an engine: NULL, or the error lsb_stack_begin would return
@@ -149,26 +153,33 @@ void* lsb_engine_stream(lsb_engine* e);
    reference needs no counterpart: its options are typed enums, while a C caller passes codes. */
 char* lsb_check_params(const lsb_fuse_params* fuse, const lsb_align_params* align, const lsb_depth_params* depth);
 
+/* stack.rs:740 `fuse_range` creating its fuser (AnyFuser, stack.rs:123; GpuFuser::new, gpu.rs:359), with
+   the stack's registration and depth passes (align / depth NULL or not enabled: off) and the
+   brightness and crop switches of stack.rs:106-120 `Params`. */
 char* lsb_stack_begin(lsb_engine* e, uint32_t w, uint32_t h, uint32_t n_frames, const lsb_fuse_params* fuse,
                       const lsb_align_params* align, const lsb_depth_params* depth, int32_t brightness, int32_t crop,
                       lsb_stack** out);
-/* One decoded frame: interleaved RGB u16, rows stride_px pixels apart (host or device pointer).
+/* stack.rs:785-821 per frame: FrameSource::get_gpu, GpuFrames::process (gpu.rs:751) and
+   GpuFuser::push_device (gpu.rs:451). One decoded frame: interleaved RGB u16, rows stride_px pixels apart (host or device pointer).
    The copy is asynchronous for page-locked memory: keep it unchanged until finish/run returns.
    The frame is registered on the device behind the next frame's copy; finish/run then warps,
    gains, REDUCEs and folds each pushed frame as soon as its transform is known. */
 char* lsb_stack_push_u16(lsb_stack* s, const uint16_t* rgb, size_t stride_px);
-/* One frame as three planar f32 planes in [0,1] (host or device pointers); the frame is folded as given. */
+/* gpu.rs:432 GpuFuser::push (stack.rs:152 AnyFuser::push): one frame as three planar f32 planes in
+   [0,1] (host or device pointers); the frame is folded as given. */
 char* lsb_stack_push_f32(lsb_stack* s, const float* const planes[3]);
 /* The device buffer frames are pushed into ([n][h][w][3] u16), and a way to declare
-   frames written there directly (count = frames now present). */
+   frames written there directly (count = frames now present). No counterpart in the reference. */
 char* lsb_stack_frames_device(lsb_stack* s, uint16_t** frames_dev);
 char* lsb_stack_set_count(lsb_stack* s, uint32_t count);
 /* fuse.rs:315 shares of the frames pushed so far (runs the fold when needed); out_n holds n floats. */
 char* lsb_stack_shares(lsb_stack* s, float* out_n);
-/* Align, fold, depth: the whole pipeline over the frames pushed; may be called again. */
+/* stack.rs:181 AnyFuser::finish (gpu.rs:517), stack.rs:833 `fuse_and_depth` and align.rs:344
+   `common_area`. Align, fold, depth: the whole pipeline over the frames pushed; may be called again. */
 char* lsb_stack_finish(lsb_stack* s, lsb_result* out);
-/* lsb_stack_finish without copying results back (device-resident benchmarking). */
+/* lsb_stack_finish without copying results back (device-resident benchmarking; no counterpart). */
 char* lsb_stack_run(lsb_stack* s, double* ms_out12);
+/* Explicit frees, as ffi.rs:129 lapstack_raw_free_image. */
 void lsb_stack_destroy(lsb_stack* s);
 void lsb_result_free(lsb_result* r);
 
@@ -202,7 +213,7 @@ char* lsb_warp_cost(lsb_engine* e, const float* rf, uint32_t aw, uint32_t ah, co
 const char* lsb_warp_cost_noalloc(const float* rf_dev, uint32_t aw, uint32_t ah, const float* tgt_dev, uint32_t tw,
                                   uint32_t th, const double* sims8, uint32_t n_sims, double* costs, void* stream);
 
-/* Synthetic stacks: [n][h][w][3] u16 into host memory (OpenMP) or device memory. truth (n*4, may be NULL):
+/* Synthetic stacks (no counterpart in the reference; the benchmark inputs): [n][h][w][3] u16 into host memory (OpenMP) or device memory. truth (n*4, may be NULL):
    per frame scale, rotation (rad), tx, ty (px) applied. */
 const char* lsb_synth_stack_host(const lsb_synth_desc* d, uint16_t* out, double* truth);
 const char* lsb_synth_stack_device(const lsb_synth_desc* d, uint16_t* out_dev, double* truth, void* stream);
@@ -249,7 +260,7 @@ char* lsb_batch_run(lsb_stack* const* stacks, uint32_t n_stacks, lsb_result* out
  * reference's FGS start). The stack does not own the network. */
 char* lsb_stack_set_warm_start(lsb_stack* s, lsb_unet* u);
 /* Device planes of the last run's depth grid (dw x dh, valid until the next
- * run): the guide luma, the median-filtered raw depth, the normalised
+ * run; no counterpart in the reference): the guide luma, the median-filtered raw depth, the normalised
  * confidence and the WLS solution -- the network's inputs and target. */
 char* lsb_stack_depth_planes(lsb_stack* s, const float** guide, const float** d, const float** conf, const float** u,
                              uint32_t* dw, uint32_t* dh);
