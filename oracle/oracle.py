@@ -74,6 +74,7 @@ def _declare(L):
         ("orc_gauss_levels_f", sz, [P, sz, sz, P, P]),
         ("orc_level_steps", None, [P, sz, sz, sz, sz, P, P]),
         ("orc_multiscale_align_f", None, [P, P, sz, sz, P, P, sz, P, P]),
+        ("orc_nm_step_kinds", None, [P, C.c_int]),
         ("orc_common_area", None, [P, sz, sz, sz, C.c_int, P]),
         ("orc_brightness_gains_f", None, [P, P, sz, sz, P, P]),
         ("orc_brightness_gains_to_f", None, [P, P, sz, sz, P]),
@@ -412,6 +413,14 @@ def multiscale_align(rf, tg, init=None, free=None, coarsen=0):
     lib().orc_multiscale_align_f(_ptr(rf), _ptr(tg), w, h, _ptr(_arr(init or SIM_ID)), _ptr(fr), coarsen, _ptr(out),
                                  C.byref(ev))
     return out, ev.value
+
+
+def nm_step_kinds(reset=False):
+    """Nelder-Mead steps of every search since the last reset, by kind (the oracle's own counters):
+    accepted reflections, expansions evaluated, accepted contractions, shrinks, and searches run."""
+    k = np.zeros(5, np.uint64)
+    lib().orc_nm_step_kinds(_ptr(k), int(reset))
+    return dict(zip(("accepted", "expanded", "contracted", "shrunk", "searches"), (int(v) for v in k)))
 
 
 def common_area(sims, w, h, interp="spline4x4"):

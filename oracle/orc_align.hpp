@@ -1,6 +1,8 @@
 // Oracle (test infrastructure only; see orc_core.hpp): align.rs and
 // brightness.rs of crates/lapstack-core/src restated.
 #pragma once
+#include <atomic>
+
 #include "orc_core.hpp"
 
 namespace orc {
@@ -375,6 +377,11 @@ inline bool nm_converged(const std::vector<std::vector<double>>& s, const std::v
     return true;
 }
 
+// Nelder-Mead steps by kind over every search since the last reset: [0] reflection accepted,
+// [1] expansion evaluated, [2] contraction accepted, [3] shrink, [4] searches. Instrumentation
+// only: the search's arithmetic and branches do not depend on it.
+inline std::atomic<size_t> g_nm_steps[5];
+
 // align.rs:796 `nelder_mead` (bounded; stable sort of the vertices each iteration)
 inline std::vector<double> nelder_mead(const std::function<double(const std::vector<double>&)>& f, const std::vector<double>& x0,
                                        const std::vector<double>& lo, const std::vector<double>& hi, const std::vector<double>& step,
@@ -398,6 +405,7 @@ inline std::vector<double> nelder_mead(const std::function<double(const std::vec
     }
     std::vector<double> fv;
     for (auto& v : simplex) fv.push_back(F(v));
+    g_nm_steps[4]++;
     const double alpha = 1.0, gamma = 2.0, rho = 0.5, sigma = 0.5;
     for (int it = 0; it < 200; it++) {
         std::vector<size_t> idx(n + 1);
@@ -425,6 +433,7 @@ inline std::vector<double> nelder_mead(const std::function<double(const std::vec
             for (size_t k = 0; k < n; k++) xe[k] = c[k] + gamma * (xr[k] - c[k]);
             clampv(xe);
             double fe = F(xe);
+            g_nm_steps[1]++;
             if (fe < fr) {
                 simplex[n] = xe;
                 fv[n] = fe;
@@ -433,6 +442,7 @@ inline std::vector<double> nelder_mead(const std::function<double(const std::vec
                 fv[n] = fr;
             }
         } else if (fr < fv[n - 1]) {
+            g_nm_steps[0]++;
             simplex[n] = xr;
             fv[n] = fr;
         } else {
@@ -441,9 +451,11 @@ inline std::vector<double> nelder_mead(const std::function<double(const std::vec
             clampv(xc);
             double fc = F(xc);
             if (fc < fv[n]) {
+                g_nm_steps[2]++;
                 simplex[n] = xc;
                 fv[n] = fc;
             } else {
+                g_nm_steps[3]++;
                 for (size_t i = 1; i <= n; i++) {
                     for (size_t k = 0; k < n; k++) simplex[i][k] = simplex[0][k] + sigma * (simplex[i][k] - simplex[0][k]);
                     clampv(simplex[i]);

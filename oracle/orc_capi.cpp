@@ -206,6 +206,11 @@ void orc_nelder_mead(orc_cost_fn f, size_t n, const double* x0, const double* lo
     std::copy(r.begin(), r.end(), out);
     if (evals) *evals = ne;
 }
+// The oracle's Nelder-Mead step counts (orc::g_nm_steps) into out5; reset clears them after reading.
+void orc_nm_step_kinds(size_t* out5, int reset) {
+    for (int k = 0; k < 5; k++) out5[k] = reset ? orc::g_nm_steps[k].exchange(0) : orc::g_nm_steps[k].load();
+}
+
 void orc_multiscale_align_f(const float* rf, const float* tg, size_t w, size_t h, const double* init8, const uint8_t* free8,
                             size_t coarsen, double* out8, size_t* evals) {
     bool fr[8];

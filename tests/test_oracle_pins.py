@@ -316,6 +316,26 @@ def test_multiscale_align_recovers_a_shift():
         assert abs(q[0] / q[2] - x) < 0.15 and abs(q[1] / q[2] - y) < 0.15
 
 
+def test_nelder_mead_step_counts_add_up_to_the_evaluations():
+    """The oracle's step counters (used to size the device search's batches) account for every
+    evaluation: n+1 per search's first simplex, 1 per accepted reflection, 2 per expansion or
+    accepted contraction, 2+n per shrink (align.rs:796)."""
+    w, h = 256, 192
+    rng = np.random.default_rng(5)
+    base = rng.random((h, w)).astype(np.float32)
+    k = np.array([1, 4, 6, 4, 1], np.float32) / np.float32(16)
+    for _ in range(3):
+        base = O.window_sum(base, k)
+    tg, _ = O.warp_plane(base, [2.3 / w, 1.1 / h, 0.997, -0.002, 1, 0, 0, 0])
+    O.nm_step_kinds(reset=True)
+    _, evals = O.multiscale_align(tg, base)
+    s = O.nm_step_kinds(reset=True)
+    n = 4  # similarity: shift x, y, scale, rotation
+    assert s["searches"] >= 2
+    assert evals == s["searches"] * (n + 1) + s["accepted"] + 2 * (s["expanded"] + s["contracted"]) + (2 + n) * s["shrunk"]
+    assert O.nm_step_kinds() == dict(accepted=0, expanded=0, contracted=0, shrunk=0, searches=0)
+
+
 # --------------------------------------------------------------- brightness.rs
 def _bscene(w, h):  # brightness.rs:148 `scene`
     y, x = np.mgrid[0:h, 0:w]
