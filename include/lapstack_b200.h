@@ -175,7 +175,8 @@ char* lsb_stack_set_count(lsb_stack* s, uint32_t count);
 /* fuse.rs:315 shares of the frames pushed so far (runs the fold when needed); out_n holds n floats. */
 char* lsb_stack_shares(lsb_stack* s, float* out_n);
 /* stack.rs:181 AnyFuser::finish (gpu.rs:517), stack.rs:833 `fuse_and_depth` and align.rs:344
-   `common_area`. Align, fold, depth: the whole pipeline over the frames pushed; may be called again. */
+   `common_area`. Align, fold, depth: the whole pipeline over the frames pushed; may be called again.
+   On an error *out is left empty (every pointer NULL, nothing to free). */
 char* lsb_stack_finish(lsb_stack* s, lsb_result* out);
 /* lsb_stack_finish without copying results back (device-resident benchmarking; no counterpart). */
 char* lsb_stack_run(lsb_stack* s, double* ms_out12);
@@ -183,7 +184,8 @@ char* lsb_stack_run(lsb_stack* s, double* ms_out12);
 void lsb_stack_destroy(lsb_stack* s);
 void lsb_result_free(lsb_result* r);
 
-/* gpu.rs:1327 depth_from_slices: slices [n][dh][dw] f32, fused [3][h][w] f32 (host pointers). */
+/* gpu.rs:1327 depth_from_slices: slices [n][dh][dw] f32, fused [3][h][w] f32 (host pointers).
+   On an error *out is left empty. */
 char* lsb_depth_from_slices(lsb_engine* e, const float* slices, uint32_t n, const float* fused, uint32_t w, uint32_t h,
                             const lsb_depth_params* p, lsb_result* out);
 /* depth.rs:1081 wls_solve on the device (host pointers, w*h each). ms: device time from the edge
@@ -205,10 +207,13 @@ char* lsb_warp_cost(lsb_engine* e, const float* rf, uint32_t aw, uint32_t ah, co
  * (a cudaMalloc synchronises the device and may not be available at all to a
  * caller that only ever borrows memory). rf_dev (aw x ah) and tgt_dev
  * (tw x th) are device f32 planes; sims8 holds n_sims (1..9) Sim vectors;
- * costs (host, n_sims) receives the align.rs:581 costs. The scratch is a
- * fixed 64.9 KB array in the library's device image, per GPU: its address is
- * looked up on the first call on each device, so make that first call before
- * any stream capture. Calls that overlap on the GPU race on that scratch.
+ * costs (host, n_sims) receives the align.rs:581 costs. Planes follow the
+ * limits of the other entry points (sides at most 65535, 3 w h below 2^31).
+ * The scratch is a fixed 64,152-byte (62.6 KiB) array in the library's device
+ * image, per GPU; its address is looked up on the first call on each device.
+ * Every call is synchronous: it reads the costs back and waits for `stream`,
+ * so it cannot run inside a stream capture. Calls that overlap on the GPU
+ * (other threads, other streams) race on that scratch.
  * Returns NULL or a static error string (do not free it). */
 const char* lsb_warp_cost_noalloc(const float* rf_dev, uint32_t aw, uint32_t ah, const float* tgt_dev, uint32_t tw,
                                   uint32_t th, const double* sims8, uint32_t n_sims, double* costs, void* stream);

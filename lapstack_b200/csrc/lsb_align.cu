@@ -1271,7 +1271,7 @@ cudaError_t multiscale_align(AlignCtx& C, const float* rf, const std::vector<flo
 // ------------------------------------------ the cost without any allocation
 // Scratch of lsb_warp_cost_noalloc: the per-block partial sums (MAX_CAND
 // candidates x NOALLOC_BLOCKS blocks x 3 doubles) and the reduced sums
-// (MAX_CAND x 3): 64.9 KB, held by every GPU that loads the library until
+// (MAX_CAND x 3): 64,152 bytes (62.6 KiB), held by every GPU that loads the library until
 // the process exits. Each call writes every partial it later reads, so
 // nothing has to start at zero; calls that overlap on the GPU race on it.
 constexpr int NOALLOC_BLOCKS = 296;
@@ -1309,6 +1309,11 @@ extern "C" const char* lsb_warp_cost_noalloc(const float* rf_dev, uint32_t aw, u
                                              uint32_t th, const double* sims8, uint32_t n_sims, double* costs, void* stream) {
     if (!rf_dev || !tgt_dev || !sims8 || !costs) return "lsb_warp_cost_noalloc: null argument";
     if (aw == 0 || ah == 0 || tw == 0 || th == 0) return "lsb_warp_cost_noalloc: empty plane";
+    // the limits of the other entry points: the kernels index planes with 32-bit ints
+    for (const uint32_t* d : {&aw, &ah, &tw, &th})
+        if (*d > 65535u) return "lsb_warp_cost_noalloc: width and height must be at most 65535";
+    if ((uint64_t)aw * ah * 3 > 0x7fffffffull || (uint64_t)tw * th * 3 > 0x7fffffffull)
+        return "lsb_warp_cost_noalloc: at most 715 Mpx per plane (3 w h must fit 31 bits)";
     if (n_sims == 0 || n_sims > (uint32_t)MAX_CAND) return "lsb_warp_cost_noalloc: 1 to 9 transforms per call";
     double* scratch = nullptr;
     if (const char* e = noalloc_scratch(&scratch)) return e;

@@ -1351,27 +1351,24 @@ static void hb_release(void* p) {
     cudaFreeHost(p);
 }
 
-extern "C" char* lsb_stack_finish(lsb_stack* s, lsb_result* r) {
-    if (!s || !r) return dup_err("null argument");
-    memset(r, 0, sizeof *r);
+// lsb_stack_finish's body: every error return leaves the caller to free r.
+static char* stack_finish(lsb_stack* s, lsb_result* r) {
     const size_t W = s->w, H = s->h;
     cudaStream_t st = s->e->s;
     r->image_u16 = (uint16_t*)hb_get(sizeof(uint16_t) * 3 * W * H);
     r->image_f32 = (float*)hb_get(sizeof(float) * 3 * W * H);
     r->winner = (float*)hb_get(sizeof(float) * W * H);
+    if (!r->image_u16 || !r->image_f32 || !r->winner) return dup_err("out of host memory");
     if (s->dp.enabled) {  // page-locked, so that every copy back is asynchronous
         r->depth = (float*)hb_get(sizeof(float) * W * H);
         r->conf = (float*)hb_get(sizeof(float) * W * H);
         r->floor_cells = (float*)hb_get(sizeof(float) * (size_t)s->dw * s->dh);
+        if (!r->depth || !r->conf || !r->floor_cells) return dup_err("out of host memory");
     }
     s->early = r;  // run_pipeline sends the fused planes back as soon as they exist
     char* err = run_pipeline(s);
     s->early = nullptr;
-    if (err) {
-        cudaStreamSynchronize(s->e->rs);
-        lsb_result_free(r);
-        return err;
-    }
+    if (err) return err;
     const size_t N = s->count;
     r->w = s->w;
     r->h = s->h;
@@ -1380,6 +1377,7 @@ extern "C" char* lsb_stack_finish(lsb_stack* s, lsb_result* r) {
     r->sims = (double*)malloc(sizeof(double) * 8 * N);
     r->gains = (float*)malloc(sizeof(float) * 3 * N);
     r->shares = (float*)malloc(sizeof(float) * N);
+    if (!r->sims || !r->gains || !r->shares) return dup_err("out of host memory");
     if (s->dp.enabled) {
         const size_t m = (size_t)s->dw * s->dh;
         r->dw = s->dw;
@@ -1404,6 +1402,20 @@ extern "C" char* lsb_stack_finish(lsb_stack* s, lsb_result* r) {
     r->align_evals = (uint32_t)s->align_evals;
     memcpy(r->ms, s->ms, sizeof s->ms);
     return nullptr;
+}
+
+extern "C" char* lsb_stack_finish(lsb_stack* s, lsb_result* r) {
+    if (!s || !r) return dup_err("null argument");
+    memset(r, 0, sizeof *r);
+    char* err = stack_finish(s, r);
+    if (err) {
+        // copies into r may still be in flight on either stream: wait for them, then hand r's blocks back
+        cudaStreamSynchronize(s->e->s);
+        cudaStreamSynchronize(s->e->rs);
+        cudaGetLastError();
+        lsb_result_free(r);
+    }
+    return err;
 }
 
 extern "C" void lsb_stack_destroy(lsb_stack* s) {
@@ -1444,7 +1456,10 @@ extern "C" char* lsb_depth_from_slices(lsb_engine* e, const float* slices, uint3
     const int k = s->bk, dw = s->dw, dh = s->dh;
     const size_t m = (size_t)dw * dh;
     memset(out, 0, sizeof *out);
-    auto fail = [&](char* m_) {
+    auto fail = [&](char* m_) {  // out holds nothing on an error: copies into it are waited for, its buffers freed
+        cudaStreamSynchronize(st);
+        cudaGetLastError();
+        lsb_result_free(out);
         lsb_stack_destroy(s);
         return m_;
     };
@@ -1500,6 +1515,7 @@ extern "C" char* lsb_depth_from_slices(lsb_engine* e, const float* slices, uint3
     out->depth = (float*)malloc(sizeof(float) * w * h);
     out->conf = (float*)malloc(sizeof(float) * w * h);
     out->floor_cells = (float*)malloc(sizeof(float) * m);
+    if (!out->depth || !out->conf || !out->floor_cells) return fail(dup_err("out of host memory"));
     TRYS(cudaMemcpyAsync(out->depth, s->dfull, sizeof(float) * w * h, cudaMemcpyDeviceToHost, st));
     TRYS(cudaMemcpyAsync(out->conf, s->cfull, sizeof(float) * w * h, cudaMemcpyDeviceToHost, st));
     TRYS(cudaMemcpyAsync(out->floor_cells, s->mins, sizeof(float) * m, cudaMemcpyDeviceToHost, st));
