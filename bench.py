@@ -18,8 +18,12 @@ published runs: a height field, band-limited texture, per-pixel defocus):
   c3s 16 x 2048x1536 with c3's settings: the small case the ncu captures use
 
 --impl reference times the CPU restatement of the reference's path (the
-oracle; the Rust reference cannot be built here) on a bounded sample of the
-same workload with all host threads.
+oracle; the Rust reference cannot be built here) on the same workload with
+all host threads: per-frame work timed frame by frame over a sample of the
+stack's frames, the finish (depth pass over all N slices on the full grid)
+timed once, extrapolated to the whole stack; plus a 1-core per-frame figure.
+It loads no part of the CUDA library (the frames come from the oracle's twin
+of the generator).
 """
 from __future__ import annotations
 
@@ -43,14 +47,14 @@ PUBLISHED_MPFS = 175.8
 
 CONFIGS = {
     "c3": dict(w=8256, h=5504, n=100, warp=True, mag_step=0.0, noise_std=0.002, levels=0, align=True, coarsen=3,
-               agg_radius=3, storage="unorm16", sample=2, wls_report=True),
+               agg_radius=3, storage="unorm16", wls_report=True),
     "c2": dict(w=6000, h=4000, n=30, warp=False, mag_step=0.001, noise_std=0.002, levels=8, align=False, coarsen=0,
-               agg_radius=8, storage="f32", sample=2),
+               agg_radius=8, storage="f32"),
     "c1": dict(w=1024, h=768, n=8, warp=False, mag_step=0.002, noise_std=0.003, levels=6, align=False, coarsen=0,
-               agg_radius=3, storage="f32", sample=8),
+               agg_radius=3, storage="f32"),
     # c3's path at a size an ncu capture finishes quickly (frames still larger than L2)
     "c3s": dict(w=2048, h=1536, n=16, warp=True, mag_step=0.0, noise_std=0.002, levels=0, align=True, coarsen=3,
-                agg_radius=3, storage="unorm16", sample=4),
+                agg_radius=3, storage="unorm16"),
 }
 
 
@@ -116,63 +120,138 @@ class Clocks:
 
 
 # ------------------------------------------------------------- reference
-def run_oracle(frames, c, threads=None):
-    from oracle import oracle as O
-    fuse, align, depth = params_of(c, O)
-    sp = O.StackParams(fuse=fuse, align=align, depth=depth)
-    t0 = time.perf_counter()
-    O.run_stack(frames, sp)
-    return time.perf_counter() - t0
+class OracleStackTimer:
+    """The oracle (the C++ restatement of the reference's CPU path, OpenMP) on a sample of the workload's
+    frames, made by the oracle's twin of the seeded generator (no CUDA library is loaded).
+
+    push(): one frame's per-frame work, timed alone -- its registration to the previous frame, warp,
+    brightness gain, fold into the pyramid selection and focus slice (stack.rs:785-821). When the sample
+    wraps, a new stack starts and its first frame is pushed untimed, so every timed push registers.
+    finish(n): the stack's finish, timed once -- shares, residual and collapse, the depth pass over n
+    focus slices (the sample's slices in order, repeated) on the full working grid, the WLS solves, the
+    upsampling and the crop (stack.rs:833-853, 1047-1060)."""
+
+    def __init__(self, c, sample, w=None, h=None, seed=0x1A957ACC):
+        from oracle import oracle as O
+        self.O, self.c, self.sample = O, c, sample
+        self.w, self.h = w or c["w"], h or c["h"]
+        self.frames, _ = O.synth_stack(self.w, self.h, c["n"], seed=seed, mag_step=c["mag_step"], noise_std=c["noise_std"],
+                                       warp=c["warp"], frames=(0, sample))
+        fuse, align, depth = params_of(c, O)
+        self.sp = O.StackParams(fuse=fuse, align=align, depth=depth)
+        self.run, self.j = None, 0
+
+    def push(self):
+        if self.run is None or self.j == self.sample:
+            self.run = self.O.StackRun(self.c["n"], self.w, self.h, self.sp)
+            self.run.push(self.frames[0], last=False)
+            self.j = 1
+        t0 = time.perf_counter()
+        self.run.push(self.frames[self.j], last=False)
+        self.j += 1
+        return time.perf_counter() - t0
+
+    def finish(self, n_total):
+        self.run.cycle_slices(n_total)
+        t0 = time.perf_counter()
+        self.run.finish()
+        self.run = None
+        return time.perf_counter() - t0
 
 
-def sample_frames(c):
-    """A bounded sample of the workload: c['sample'] frames of the same size and recipe."""
-    import lapstack_b200 as L
-    n = c["sample"]
-    spec = spec_of(c, n=n, seed=0x1A957ACC ^ 0x5A)
+def repo_libs():
+    """The repository's shared libraries this process has mapped (what ran)."""
     try:
-        import torch
-        if torch.cuda.is_available():
-            buf = torch.empty((n, c["h"], c["w"], 3), dtype=torch.int16, device="cuda")
-            L.synth_stack_device(spec, buf.data_ptr())
-            torch.cuda.synchronize()
-            return buf.cpu().numpy().view(np.uint16)
+        maps = open("/proc/self/maps").read().split("\n")
     except Exception:
-        pass
-    return L.synth_stack(spec)[0]
+        return None
+    return sorted({os.path.relpath(l.split()[-1], ROOT) for l in maps if l.strip().endswith(".so") and ROOT in l})
 
 
-def cpu_baseline(c, frames=None):
-    frames = frames if frames is not None else sample_frames(c)
-    t = run_oracle(frames, c)
-    n = frames.shape[0]
-    mp = n * c["w"] * c["h"] / 1e6
-    return {"value": mp / t, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
-            "sample": f"{n} of the workload's frames ({c['w']}x{c['h']}), the whole path (align+fold+depth) in {t:.1f} s "
-                      f"on the oracle (C++ restatement of the reference's CPU path, OpenMP)"}
+def host_cores():
+    try:
+        return len(os.sched_getaffinity(0))
+    except Exception:
+        return os.cpu_count()
+
+
+def cpu_baseline(c):
+    """A bounded sample of the workload on the oracle (about 30 s of CPU): frames at a quarter of the
+    frame area from the same generator, two timed pushes and the finish over the workload's N slices on
+    the quarter-area grid, both scaled by the area ratio (the per-frame work, the depth pass and the WLS
+    solve grow with the pixel count). The reference arm (--impl reference) measures the full frame size."""
+    from oracle import oracle as O
+    threads = O.set_threads(0)
+    w, h = (c["w"] + 1) // 2, (c["h"] + 1) // 2
+    area = c["w"] * c["h"] / (w * h)
+    tm = OracleStackTimer(c, 3, w, h)
+    pushes = [tm.push() for _ in range(2)]
+    fin = tm.finish(c["n"])
+    per_frame, finish = statistics.mean(pushes) * area, fin * area
+    step = per_frame + finish / c["n"]
+    return {"value": c["w"] * c["h"] / 1e6 / step, "unit": UNIT, "cores": threads, "nproc": host_cores(), "kind": "port",
+            "extrapolated": True, "per_frame_s": per_frame, "finish_s": finish,
+            "sample": (f"the oracle (C++ restatement of the reference's CPU path, OpenMP on {threads} threads): frames at a "
+                       f"quarter of the area ({w}x{h}, same generator and settings), 2 registered frames pushed "
+                       f"({statistics.mean(pushes):.2f} s each) and the finish with the depth pass over {c['n']} slices "
+                       f"({fin:.1f} s), scaled by the area ratio {area:.2f}; MP-frames/s = N*W*H/(N*per_frame + finish)")}
 
 
 def reference_arm(args, c, name):
+    """The reference's CPU path (the oracle: the Rust reference cannot be built here) on this workload,
+    rank 0 only: each step is one frame's per-frame work (OracleStackTimer.push) on a sample of the
+    workload's first frames (at least 8 timed ones before the sample repeats); after the steps the stack's
+    finish, with the depth pass over all N slices on the full grid, is timed once and spread over the N
+    frames. ms_per_step = per-frame time + finish / N, so the value is the whole stack's extrapolated
+    MP-frames/s. One more push on a single thread gives the 1-core per-frame figure."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
-    frames = sample_frames(c)
-    n = frames.shape[0]
-    mp = n * c["w"] * c["h"] / 1e6
+    from oracle import oracle as O
+    threads = O.set_threads(0)
+    N, W, H = c["n"], c["w"], c["h"]
+    sample = min(N, 9)
+    tm = OracleStackTimer(c, sample)
+    t_begin = time.perf_counter()
     for _ in range(args.warmup):
-        run_oracle(frames, c)
-    ts = [run_oracle(frames, c) for _ in range(args.steps)]
-    t = sum(ts) / len(ts)
-    v = mp / t
+        tm.push()
+    pushes = [tm.push() for _ in range(args.steps)]
+    one_core = None
+    if tm.sample > 1:
+        O.set_threads(1)
+        try:
+            one_core = tm.push()
+        finally:
+            O.set_threads(0)
+    fin = tm.finish(N)
+    per_frame = statistics.mean(pushes)
+    step = per_frame + fin / N
+    v = W * H / 1e6 / step
+    world = int(os.environ.get("WORLD_SIZE", "1"))
     line = {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": t * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": v / PUBLISHED_MPFS,
-            "dtype": "f32", "data": "synthetic (seeded)", "impl": "reference",
-            "config": {"workload": workload_name(c, name), "sample_frames": n},
-            "cpu_baseline": {"value": v, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
-                             "sample": f"{n} frames of {c['w']}x{c['h']}, whole path per step"},
-            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+            "ms_per_step": step * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": v / PUBLISHED_MPFS,
+            "dtype": "f32", "data": "synthetic (seeded generator: height field, band-limited texture, per-pixel defocus)",
+            "impl": "reference", "config": bench_config(c, name, world),
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "nproc": host_cores(), "kind": "port",
+                             "extrapolated": True, "per_frame_s": per_frame, "finish_s": fin,
+                             "one_core": ({"per_frame_s": one_core, "per_frame_mpfs": W * H / 1e6 / one_core}
+                                          if one_core else None),
+                             "sample": (f"the oracle (C++ restatement of the reference's CPU path; the Rust reference "
+                                        f"cannot be built here) on {threads} threads: {args.steps} frames of the workload "
+                                        f"pushed one per step (registration, warp, gains, fold, focus slice; the first "
+                                        f"{sample} frames of the stack, repeated), then the finish with the depth pass over "
+                                        f"all {N} slices on the full grid ({fin:.1f} s), spread over the {N} frames; the "
+                                        f"whole run took {time.perf_counter() - t_begin:.0f} s")},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "native_so": repo_libs()}
     print(json.dumps(line), flush=True)
     return 0
+
+
+def bench_config(c, name, world):
+    """The workload as both arms name it."""
+    return {"workload": workload_name(c, name), "global_batch": c["n"] * world, "parallelism": f"replicas x{world}",
+            "l2": "inputs (frames) larger than L2 every step"}
 
 
 # ------------------------------------------------------------------- ours
@@ -403,10 +482,8 @@ def main():
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": value / PUBLISHED_MPFS,
             "dtype": "f32", "data": "synthetic (seeded generator: height field, band-limited texture, per-pixel defocus)",
-            "config": {"workload": workload_name(c, args.config), "global_batch": N * world, "parallelism": f"replicas x{world}",
-                       "l2": "inputs (frames) larger than L2 every step",
-                       "autotune": ({"grid_select": tune["grid_select"], "grid_aggregate": tune["grid_aggregate"]}
-                                    if tune else None)},
+            "config": bench_config(c, args.config, world),
+            "autotune": ({"grid_select": tune["grid_select"], "grid_aggregate": tune["grid_aggregate"]} if tune else None),
             "e2e": {"value": job_throughput(world, mp_step, e2e_t), "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "ms_per_step": e2e_t},
             "gpu_launches": launches,

@@ -100,6 +100,14 @@ def _declare(L):
         ("orc_stack_depth", None, [P, P, P, P]),
         ("orc_stack_stats", None, [P, P]),
         ("orc_stack_sims", None, [P, P, P, P]),
+        ("orc_stack_begin", P, [sz, sz, sz, P, C.c_int]),
+        ("orc_stack_push", None, [P, P, C.c_int]),
+        ("orc_stack_cycle_slices", None, [P, sz]),
+        ("orc_stack_end", P, [P]),
+        ("orc_stack_abort", None, [P]),
+        ("orc_set_threads", None, [C.c_int]),
+        ("orc_threads", C.c_int, []),
+        ("orc_synth_stack", C.c_int, [P, P, P, C.c_uint32, C.c_uint32]),
     ]:
         f = getattr(L, name)
         f.restype = res
@@ -588,8 +596,65 @@ def run_stack(frames_u16, params: StackParams | None = None, fp64=False) -> Stac
     p = params or StackParams()
     fr = np.ascontiguousarray(frames_u16, dtype=np.uint16)
     n, h, w, _ = fr.shape
+    return _result_of(lib().orc_run_stack(_ptr(fr), n, w, h, _ptr(p.arr()), int(fp64)), p, n, w, h)
+
+
+class StackRun:
+    """The same stack one frame at a time: push() registers, gains and folds a frame (the per-frame body
+    of stack.rs:785-821), finish() the shares, the fused image, the depth pass and the crop
+    (stack.rs:833, 1047-1060). n is the stack's frame count (registration is on only when n > 1)."""
+
+    def __init__(self, n, w, h, params: StackParams | None = None, fp64=False):
+        self.p, self.n, self.w, self.h, self.pushed = params or StackParams(), n, w, h, 0
+        self._h = lib().orc_stack_begin(n, w, h, _ptr(self.p.arr()), int(fp64))
+
+    def push(self, frame_u16, last=None):
+        f = np.ascontiguousarray(frame_u16, dtype=np.uint16)
+        assert f.shape == (self.h, self.w, 3)
+        last = self.pushed + 1 == self.n if last is None else last
+        lib().orc_stack_push(self._h, _ptr(f), int(last))
+        self.pushed += 1
+
+    def cycle_slices(self, n_total):
+        """For timing only: repeat the pushed frames' focus slices in order up to n_total, so that the
+        depth pass runs over a whole stack's worth of slices after a sample of its frames."""
+        lib().orc_stack_cycle_slices(self._h, n_total)
+
+    def finish(self) -> "StackResult":
+        h, self._h = self._h, None
+        return _result_of(lib().orc_stack_end(h), self.p, self.pushed, self.w, self.h)
+
+    def __del__(self):
+        try:
+            if self._h:
+                lib().orc_stack_abort(self._h)
+        except Exception:
+            pass
+
+
+def set_threads(n=0):
+    """OpenMP threads of every later oracle call (0: all the host's); returns the count now in use."""
+    lib().orc_set_threads(int(n))
+    return lib().orc_threads()
+
+
+def synth_stack(w, h, n, seed=0x1A957ACC, mag_step=0.002, noise_std=0.003, blur_px=6.0, warp=False, warp_scale=0.004,
+                warp_rot_deg=0.2, warp_shift=8.0, frames=None):
+    """The seeded synthetic stack (n, h, w, 3) u16 and the applied transforms (n, 4), made on the host by
+    the oracle's twin of the engine's generator (no CUDA library involved). frames=(k0, count): only
+    those frames of the n-frame stack."""
+    d = _arr([w, h, n, int(warp), seed & 0xFFFFFFFF, seed >> 32, mag_step, noise_std, blur_px, warp_scale, warp_rot_deg,
+              warp_shift])
+    k0, count = frames or (0, n)
+    out = np.empty((count, h, w, 3), np.uint16)
+    truth = np.empty((n, 4), F64)
+    if lib().orc_synth_stack(_ptr(d), _ptr(out), _ptr(truth), k0, count) != 0:
+        raise ValueError("synth_stack: bad description")
+    return out, truth
+
+
+def _result_of(r, p, n, w, h) -> "StackResult":
     L = lib()
-    r = L.orc_run_stack(_ptr(fr), n, w, h, _ptr(p.arr()), int(fp64))
     try:
         img = np.empty((3, h, w), F64)
         u16 = np.empty((h, w, 3), np.uint16)

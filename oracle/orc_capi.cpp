@@ -3,6 +3,8 @@
 // Parameter blocks are flat double arrays, laid out in oracle/oracle.py.
 #include <array>
 #include "orc_stack.hpp"
+#include "orc_synth.hpp"
+#include <omp.h>
 
 using namespace orc;
 
@@ -421,6 +423,86 @@ void orc_stack_sims(void* p, double* sims8, float* gains3, float* shares) {
     };
     if (r->dbl) fill(r->d);
     else fill(r->f);
+}
+
+// ---- the stack one frame at a time (the CPU baseline times the per-frame work and the finish apart)
+struct StackInc {
+    bool dbl;
+    size_t n, w, h;
+    StackRun<float>* f = nullptr;
+    StackRun<double>* d = nullptr;
+    ~StackInc() {
+        delete f;
+        delete d;
+    }
+};
+void* orc_stack_begin(size_t n, size_t w, size_t h, const double* sp, int fp64) {
+    StackInc* s = new StackInc();
+    s->dbl = fp64 != 0;
+    s->n = n;
+    s->w = w;
+    s->h = h;
+    if (s->dbl) s->d = new StackRun<double>(w, h, n, stack_params_of(sp));
+    else s->f = new StackRun<float>(w, h, n, stack_params_of(sp));
+    return s;
+}
+void orc_stack_push(void* p, const uint16_t* frame, int last) {
+    StackInc* s = (StackInc*)p;
+    if (s->dbl) s->d->push(frame, last != 0);
+    else s->f->push(frame, last != 0);
+}
+// For timing only: the focus slices pushed so far repeated in order until there are n_total, so that
+// the depth pass runs over a whole stack's slices after a sample of its frames was pushed.
+void orc_stack_cycle_slices(void* p, size_t n_total) {
+    StackInc* s = (StackInc*)p;
+    auto grow = [&](auto& sl) {
+        const size_t k = sl.size();
+        for (size_t i = k; i < n_total && k > 0; i++) sl.push_back(sl[i % k]);
+    };
+    if (s->dbl) grow(s->d->slices);
+    else grow(s->f->slices);
+}
+// Finishes and frees the handle; the result is read with the orc_stack_* accessors and freed by orc_stack_free.
+void* orc_stack_end(void* p) {
+    StackInc* s = (StackInc*)p;
+    StackRes* r = new StackRes();
+    r->dbl = s->dbl;
+    r->w = s->w;
+    r->h = s->h;
+    if (s->dbl) {
+        s->d->finish();
+        r->n = s->d->out.sims.size();
+        r->d = std::move(s->d->out);
+    } else {
+        s->f->finish();
+        r->n = s->f->out.sims.size();
+        r->f = std::move(s->f->out);
+    }
+    delete s;
+    return r;
+}
+void orc_stack_abort(void* p) { delete (StackInc*)p; }
+
+// OpenMP threads of every later oracle call (0: all the host's)
+void orc_set_threads(int n) { omp_set_num_threads(n > 0 ? n : omp_get_num_procs()); }
+int orc_threads(void) { return omp_get_max_threads(); }
+
+// the seeded synthetic stack (orc_synth.hpp): d = [w, h, n, warp, seed_lo, seed_hi, mag_step, noise_std,
+// blur_px, warp_scale, warp_rot_deg, warp_shift]; frames k0 .. k0+count-1 of the stack into out
+int orc_synth_stack(const double* d, uint16_t* out, double* truth, uint32_t k0, uint32_t count) {
+    SynthDesc sd;
+    sd.w = (uint32_t)d[0];
+    sd.h = (uint32_t)d[1];
+    sd.n = (uint32_t)d[2];
+    sd.warp = (uint32_t)d[3];
+    sd.seed = (uint64_t)d[4] | ((uint64_t)d[5] << 32);
+    sd.mag_step = (float)d[6];
+    sd.noise_std = (float)d[7];
+    sd.blur_px = (float)d[8];
+    sd.warp_scale = (float)d[9];
+    sd.warp_rot_deg = (float)d[10];
+    sd.warp_shift = (float)d[11];
+    return synth_stack(sd, out, truth, k0, count) ? 0 : 1;
 }
 
 }  // extern "C"

@@ -49,29 +49,38 @@ inline uint16_t u16_of(T v) {
     return (uint16_t)(c * LIT(65535.0) + LIT(0.5));
 }
 
-// stack.rs:1011 `run_with` for frames already decoded: register and gain each frame, fold them
-// (stack.rs:740 `fuse_range`), then the depth pass (stack.rs:833 `fuse_and_depth`) and the crop
+// stack.rs:1011 `run_with` for frames already decoded, one frame at a time:
+// push() registers and gains each frame and folds it (stack.rs:740 `fuse_range`,
+// the per-frame body of stack.rs:785-821), finish() takes the shares, the fused
+// image, the depth pass (stack.rs:833 `fuse_and_depth`) and the crop.
 template <class T>
-StackOutput<T> run_stack(const uint16_t* const* frames, size_t n, size_t w, size_t h, const StackParams& sp) {
+struct StackRun {
+    size_t w, h;
+    StackParams sp;
     StackOutput<T> out;
-    Fuser<T> fuser(w, h, sp.fuse);
-    out.levels = fuser.levels;
+    Fuser<T> fuser;
     std::vector<std::vector<T>> slices;
-    bool aligned = sp.align && n > 1;
+    bool aligned;
     bool freem[8];
-    free_mask(sp.al, freem);
     std::vector<T> prev_ref;
     BReference<T> bref;
     double ref_means[3] = {0, 0, 0};
-    for (size_t i = 0; i < n; i++) {
-        Img3<T> img = img_of_u16<T>(frames[i], w, h);
+    size_t i = 0;
+    StackRun(size_t w_, size_t h_, size_t n, const StackParams& sp_) : w(w_), h(h_), sp(sp_), fuser(w_, h_, sp_.fuse) {
+        out.levels = fuser.levels;
+        aligned = sp.align && n > 1;
+        free_mask(sp.al, freem);
+    }
+    // `last`: no frame follows (the next frame's reference is not made)
+    void push(const uint16_t* frame, bool last) {
+        Img3<T> img = img_of_u16<T>(frame, w, h);
         Sim sim;
         std::array<float, 3> gain{1.0f, 1.0f, 1.0f};
         if (aligned) {
             // stack.rs:513 `register`
             std::vector<T> y = luma(img);
             if (i > 0) sim = multiscale_align<T>(prev_ref.data(), y.data(), w, h, out.sims.back(), freem, sp.al.coarsen, &out.align_evals);
-            if (i + 1 < n) {
+            if (!last) {
                 if (sim.is_id()) prev_ref = y;
                 else warp_plane<T>(y.data(), w, h, sim, w, h, sp.al.interp, prev_ref, nullptr);
             }
@@ -117,13 +126,23 @@ StackOutput<T> run_stack(const uint16_t* const* frames, size_t n, size_t w, size
             size_t dw, dh;
             slices.push_back(focus_slice<T>(img, sp.dp, dw, dh));
         }
+        i++;
     }
-    out.shares = fuser.shares();
-    fuser.finish(out.image, out.winner);
-    if (sp.depth) out.dm = depth_from_slices<T>(slices, out.image, sp.dp);
-    out.crop = Rect{0, 0, w, h};
-    if (aligned && sp.crop) out.crop = common_area(out.sims, w, h, sp.al.interp);
-    return out;
+    void finish() {
+        out.shares = fuser.shares();
+        fuser.finish(out.image, out.winner);
+        if (sp.depth) out.dm = depth_from_slices<T>(slices, out.image, sp.dp);
+        out.crop = Rect{0, 0, w, h};
+        if (aligned && sp.crop) out.crop = common_area(out.sims, w, h, sp.al.interp);
+    }
+};
+
+template <class T>
+StackOutput<T> run_stack(const uint16_t* const* frames, size_t n, size_t w, size_t h, const StackParams& sp) {
+    StackRun<T> run(w, h, n, sp);
+    for (size_t i = 0; i < n; i++) run.push(frames[i], i + 1 == n);
+    run.finish();
+    return std::move(run.out);
 }
 
 }  // namespace orc

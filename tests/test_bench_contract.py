@@ -36,12 +36,17 @@ def test_reference_arm_prints_one_contract_line():
     assert j["unit"] == "MP-frames/s" and j["higher_is_better"] is True and j["scaling"] == "weak"
     assert j["steps"] == 1 and j["warmup"] == 0 and j["n_gpus"] == 1
     assert j["value"] > 0 and j["ms_per_step"] > 0
-    # one step is the whole 8-frame 1024x768 sample
-    assert j["value"] == pytest.approx(8 * 1024 * 768 / 1e6 / (j["ms_per_step"] / 1e3), rel=1e-9)
-    assert j["config"]["workload"].startswith("c1: 8 x 1024x768")
+    # one step is one frame's work plus its share of the stack's finish: the value is the whole
+    # 8-frame 1024x768 stack's, extrapolated from the per-frame time
     cb = j["cpu_baseline"]
+    assert j["ms_per_step"] == pytest.approx(1e3 * (cb["per_frame_s"] + cb["finish_s"] / 8), rel=1e-9)
+    assert j["value"] == pytest.approx(1024 * 768 / 1e6 / (j["ms_per_step"] / 1e3), rel=1e-9)
+    assert j["config"]["workload"].startswith("c1: 8 x 1024x768")
     assert cb["value"] == j["value"] and cb["unit"] == j["unit"] and cb["kind"] == "port" and cb["cores"] >= 1
-    assert cb["sample"]
+    assert cb["extrapolated"] is True and cb["sample"] and cb["one_core"]["per_frame_s"] > 0
+    # the CPU arm runs the oracle alone: no part of the CUDA library is loaded
+    assert j["native_so"] is not None and not any("liblapstack_b200" in p for p in j["native_so"]), j["native_so"]
+    assert any("liblsb_oracle" in p for p in j["native_so"])
     assert j["e2e"] == {"value": j["value"], "unit": j["unit"], "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
 
 
