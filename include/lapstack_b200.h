@@ -43,6 +43,10 @@ extern "C" {
 
 #define LSB_ABI_VERSION 1u
 
+/* lsb_config.flags: fold level 0 with the REDUCE and select kernels on every tile instead of the
+   fused level-0 kernel on the interior tiles (the same results; for cross-checks and timing) */
+#define LSB_FLAG_TWO_KERNEL_FOLD0 1
+
 typedef struct lsb_engine lsb_engine;
 typedef struct lsb_stack lsb_stack;
 
@@ -53,7 +57,7 @@ typedef struct {
     int32_t storage;       /* Gaussian levels >= 1 and focus slices: 0 FP32 (bit-exact with the reference
                               FP32 path); 1 16-bit: UNORM16 levels, FP16 slices; 2 FP16 levels and slices */
     int32_t grid_limit;    /* CTAs of the persistent kernels; 0 = 2 x the SM count */
-    int32_t reserved;
+    int32_t flags;         /* LSB_FLAG_* bits; 0 for the defaults */
     lsb_log_fn log;        /* optional progress lines (stack.rs:1014 `log`) */
     void* user;
 } lsb_config;
@@ -117,8 +121,9 @@ typedef struct {
     uint32_t wls_iters, wls_iters_first, align_evals;
     double wls_rel64;
     double ms[12];       /* device ms per stage: align, gains, fold, residual+collapse, focus agg, wls, upsample,
-                            total, fold level 0, its select kernel, its REDUCE kernel, the WLS solves
-                            (warm start included) */
+                            total, fold level 0, then its two parts: [9] the select kernel (with the fused
+                            level-0 kernel: the REDUCE and select of the border tiles after it) and [10] the
+                            REDUCE kernel (or the fused kernel), then the WLS solves (warm start included) */
 } lsb_result;
 
 /* Seeded synthetic stack description (no reference counterpart; the benchmark inputs). */

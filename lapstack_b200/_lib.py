@@ -25,7 +25,7 @@ LOG_FN = C.CFUNCTYPE(None, C.c_char_p, C.c_void_p)
 
 
 class Config(C.Structure):
-    _fields_ = [("device", C.c_int32), ("storage", C.c_int32), ("grid_limit", C.c_int32), ("reserved", C.c_int32),
+    _fields_ = [("device", C.c_int32), ("storage", C.c_int32), ("grid_limit", C.c_int32), ("flags", C.c_int32),
                 ("log", LOG_FN), ("user", C.c_void_p)]
 
 

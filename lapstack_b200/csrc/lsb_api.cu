@@ -721,6 +721,7 @@ static FoldArgs level_args(const lsb_stack* s, int l, bool warped, bool depth_on
     a.winner = l == s->depth_level ? s->winner : nullptr;
     a.use_chroma = (int)s->fp.use_chroma;
     a.status = s->status;
+    a.no_fused = (s->e->cfg.flags & LSB_FLAG_TWO_KERNEL_FOLD0) != 0;
     *focus = depth_on && l == 0;
     if (*focus) {
         a.slice = s->slices;

@@ -31,6 +31,7 @@
 namespace lsb {
 
 #include "lsb_level.cuh"
+#include "lsb_fold0.cuh"
 
 size_t fold_smem_bytes(int, bool) { return (size_t)SEL_FLOATS * sizeof(float); }
 
@@ -76,16 +77,43 @@ __global__ void select_merge_kernel(const FoldArgs a, int G) {
     }
 }
 
+// The fused level-0 kernel applies: 16-bit frames, one call doing the REDUCE and the selection of the
+// same frames, no halo control and no frame groups, no focus slice or the default one (ring difference
+// filter r 1..3 on 2x2 blocks), and a frame with interior tiles.
+static bool fold0_applies(const FoldArgs& a, int src, bool focus, int R) {
+    if (src != SRC_U16 || a.level != 0 || a.halo_mode != 0 || a.sel_groups > 1 || !a.select || a.red_n <= 0) return false;
+    if (a.red_k0 != a.sel_k0 || a.red_n != a.sel_k1 - a.sel_k0) return false;
+    if (focus && !(a.rdf13 && a.bk == 2 && a.focus_kind == 0)) return false;
+    return fold0_count(fold0_range(a.W, a.H, R)) > 0;
+}
+
 // One level: REDUCE the frames asked for (and take their focus slices at level 0), then select.
+// Level 0 of 16-bit frames: the fused kernel on the interior tiles, the two kernels on the others.
 template <int SRC, class GS, int R, bool FOCUS, class SS>
-static cudaError_t launch_level(const FoldArgs& a, cudaStream_t s, int grid_limit) {
+static cudaError_t launch_level(const FoldArgs& a0, cudaStream_t s, int grid_limit) {
     const size_t rsm = (size_t)RED_FLOATS * sizeof(float), ssm = Staging<SRC, GS, R>::SMEM;
     auto kr = reduce_level_kernel<SRC, GS, FOCUS, SS>;
     auto ks = select_level_kernel<SRC, GS, R>;
     cudaError_t e = with_smem(kr, rsm);
     if (e == cudaSuccess) e = with_smem(ks, ssm);
     if (e != cudaSuccess) return e;
-    const int rtiles = ((a.W1 + RW - 1) / RW) * ((a.H1 + RH - 1) / RH);
+    FoldArgs a = a0;
+    int rtiles = ((a.W1 + RW - 1) / RW) * ((a.H1 + RH - 1) / RH);
+    if (SRC == SRC_U16 && !a0.no_fused && fold0_applies(a0, SRC, FOCUS, R)) {
+        auto kf = fold0_kernel<GS, R, FOCUS, SS>;
+        e = with_smem(kf, f0::SMEM);
+        if (e != cudaSuccess) return e;
+        const Fold0Range rg = fold0_range(a.W, a.H, R);
+        const int nf = fold0_count(rg);
+        lsb_launched(), kf<<<std::min(nf, std::max(grid_limit, 1)), f0::NT0, f0::SMEM, s>>>(a);
+        if (a.between) cudaEventRecord(a.between, s);
+        a.between = nullptr;
+        a.fused0 = 1;
+        a.f0r = R;
+        a.ntiles = fold0_border_count(a.tiles_x, a.tiles_y, rg);
+        rtiles = a.ntiles;  // the REDUCE's tiles are the level-0 tiles' G_1 blocks
+        if (a.ntiles <= 0) return cudaGetLastError();
+    }
     if (a.red_n > 0) lsb_launched(), kr<<<dim3(rtiles, a.red_n), NT, rsm, s>>>(a);
     if (a.between) cudaEventRecord(a.between, s);
     const int groups = std::max(a.sel_groups, 1);

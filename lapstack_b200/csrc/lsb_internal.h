@@ -67,6 +67,10 @@ struct FoldArgs {
     int sel_groups;
     float *gacc, *gbest;
     int* gwin;
+    // level 0 only: fused0 set, the interior tiles (fold0_range(W, H, f0r)) are the fused kernel's, and
+    // reduce_level_kernel / select_level_kernel walk the other ntiles tiles (fold0_border_tile)
+    int fused0, f0r;
+    int no_fused;  // 1: level 0 runs the two kernels on every tile (the fused kernel's cross-check)
 };
 
 // Storage of the Gaussian levels >= 1 and the focus slices.

@@ -47,6 +47,41 @@ constexpr int RGW = 2 * RW + 2 * FOC_R, RGH = 2 * RH + 2 * FOC_R;  // 70 x 38
 constexpr int RED_WPR = (RGW * 6 + 2 + 3) / 4;  // words per staged u16 window row (with 2 bytes of slack)
 constexpr int RED_FLOATS = 3 * RGW * RGH + RGW * RGH + 3 * RGH * RW + RGH * RED_WPR;
 
+// ---- the level-0 tiles of the fused kernel (lsb_fold0.cuh) and the others
+// Tiles of level 0 the fused kernel takes: columns [1, ix1) and rows [1, iy1) of the 64x32 tile grid
+// (their windows, G_1 reads and slice cells lie inside the frame). 0 tiles when the frame is small.
+struct Fold0Range {
+    int ix1, iy1;
+};
+__host__ __device__ inline Fold0Range fold0_range(int W, int H, int R) {
+    Fold0Range r;
+    const int xs = W - 70 + (R & 1), ys = H - 38;
+    r.ix1 = xs >= 64 ? xs / 64 + 1 : 1;
+    r.iy1 = ys >= 32 ? ys / 32 + 1 : 1;
+    return r;
+}
+__host__ __device__ inline bool fold0_interior(int tx, int ty, const Fold0Range& r) {
+    return tx >= 1 && tx < r.ix1 && ty >= 1 && ty < r.iy1;
+}
+__host__ __device__ inline int fold0_count(const Fold0Range& r) { return (r.ix1 - 1) * (r.iy1 - 1); }
+
+// The tiles the fused kernel leaves (those whose window meets the frame border), enumerated for the
+// two-kernel path: row 0, then columns 0 and ix1.. of rows 1 .. iy1-1, then rows iy1.. . b < count.
+__host__ __device__ inline int fold0_border_count(int tiles_x, int tiles_y, const Fold0Range& r) {
+    return tiles_x * tiles_y - fold0_count(r);
+}
+__host__ __device__ inline int fold0_border_tile(int b, int tiles_x, const Fold0Range& r) {
+    if (r.ix1 <= 1 || r.iy1 <= 1) return b;  // no interior: every tile is a border tile
+    if (b < tiles_x) return b;
+    b -= tiles_x;
+    const int per = tiles_x - (r.ix1 - 1), mid = (r.iy1 - 1) * per;
+    if (b < mid) {
+        const int ty = 1 + b / per, j = b - (b / per) * per;
+        return ty * tiles_x + (j == 0 ? 0 : r.ix1 + j - 1);
+    }
+    return r.iy1 * tiles_x + (b - mid);
+}
+
 // conv_sparse taps (depth.rs:417) in the per-pixel accumulation order: rows
 // grouped by dy in order of first appearance, within a row in list order.
 __constant__ float c_taps[3 * 64];
@@ -294,8 +329,9 @@ __device__ __forceinline__ void reduce_tile(const FoldArgs& a, float* __restrict
 template <int SRC, class GS, bool FOCUS, class SS>
 __global__ void __launch_bounds__(NT, LSB_RED_MINB) reduce_level_kernel(const FoldArgs a) {
     extern __shared__ float sm[];
-    const int tiles_x = (a.W1 + RW - 1) / RW;
-    const int gx0 = (blockIdx.x % tiles_x) * RW, gy0 = (blockIdx.x / tiles_x) * RH;
+    const int tiles_x = (a.W1 + RW - 1) / RW;  // the level-0 64x32 tiles' grid
+    const int tile = a.fused0 ? fold0_border_tile(blockIdx.x, tiles_x, fold0_range(a.W, a.H, a.f0r)) : (int)blockIdx.x;
+    const int gx0 = (tile % tiles_x) * RW, gy0 = (tile / tiles_x) * RH;
     const int k = a.red_k0 + (int)blockIdx.y;
     const bool interior = 2 * gx0 - FOC_R >= 0 && 2 * gx0 + 2 * RW + FOC_R <= a.W && 2 * gy0 - FOC_R >= 0 &&
                           2 * gy0 + 2 * RH + FOC_R <= a.H;
@@ -579,7 +615,8 @@ __global__ void __launch_bounds__(NT, LSB_SEL_MINB) select_level_kernel(const Fo
     const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
     const int G = a.sel_groups > 1 ? a.sel_groups : 1;
     for (int wi = blockIdx.x; wi < a.ntiles * G; wi += gridDim.x) {
-        const int tile = wi % a.ntiles, g = wi / a.ntiles;
+        const int tile = a.fused0 ? fold0_border_tile(wi % a.ntiles, a.tiles_x, fold0_range(W, H, a.f0r)) : wi % a.ntiles;
+        const int g = wi / a.ntiles;
         const int k0 = G > 1 ? a.sel_k0 + (a.sel_k1 - a.sel_k0) * g / G : a.sel_k0;
         const int k1 = G > 1 ? a.sel_k0 + (a.sel_k1 - a.sel_k0) * (g + 1) / G : a.sel_k1;
         TileWin t;
