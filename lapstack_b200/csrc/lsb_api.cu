@@ -760,11 +760,11 @@ static void set_groups(const lsb_stack* s, FoldArgs& a) {
 // the transforms come back on rs behind each search, their matrices are
 // built on the host (align.rs:200-294, as the host path builds them) and the
 // frame's warp and sums are queued on ws, then its gains (brightness.rs:93)
-// and, with `reduce`, the REDUCE of every pyramid level (pyramid.rs:86, the
-// focus slice at level 0): all that depends on that frame alone. With
-// `select` too, every SEL_CHUNK frames the selection of every level folds
-// them in (fuse.rs:414-451, frames in order, resuming from the state the
-// chunk before left). The work stream waits for ws.
+// and, with `reduce` alone, the REDUCE of every pyramid level (pyramid.rs:86,
+// the focus slice at level 0): all that depends on that frame alone. With
+// `select` too, every SEL_CHUNK frames are folded in level by level, their
+// REDUCE then their selection (fuse.rs:414-451, frames in order, resuming
+// from the state the chunk before left). The work stream waits for ws.
 constexpr int SEL_CHUNK = 10;
 static char* stream_warps(lsb_stack* s, bool reduce, bool select) {
     lsb_engine* e = s->e;
@@ -811,7 +811,7 @@ static char* stream_warps(lsb_stack* s, bool reduce, bool select) {
                                   e->ws));
             TRY(frame_gain(s->bpart, i, BRIGHT_PARTS, s->xf_dev + i, e->ws));
         }
-        for (int l = 0; l < s->levels && reduce; l++) {
+        for (int l = 0; l < s->levels && reduce && !select; l++) {
             bool focus = false;
             int src = 0;
             FoldArgs a = level_args(s, l, true, depth_on, &focus, &src);
@@ -821,11 +821,14 @@ static char* stream_warps(lsb_stack* s, bool reduce, bool select) {
             TRY(fold_level(a, src, s->storage, (int)s->fp.energy_radius, focus, e->ws, e->grid));
         }
         if (reduce && select && (i + 1 - sel_from == SEL_CHUNK || i + 1 == n)) {
+            // the chunk's frames level by level: their REDUCE (and focus slices), then their selection
+            // (level 0: one fused kernel where it applies)
             for (int l = 0; l < s->levels; l++) {
                 bool focus = false;
                 int src = 0;
                 FoldArgs a = level_args(s, l, true, depth_on, &focus, &src);
-                a.red_n = 0;
+                a.red_k0 = sel_from;
+                a.red_n = i + 1 - sel_from;
                 a.sel_k0 = sel_from;
                 a.sel_k1 = i + 1;
                 set_groups(s, a);

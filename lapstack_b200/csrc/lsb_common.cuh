@@ -105,5 +105,21 @@ __device__ __forceinline__ void lsb_st<float>(float* p, float v) { *p = v; }
 template <>
 __device__ __forceinline__ void lsb_st<__half>(__half* p, float v) { *p = __float2half_rn(v); }
 
+// depth.rs:201 `upsample_bilinear` along one axis: the grid coordinate of output pixel x
+// ((x + 0.5) / k - 0.5, clamped), its two grid neighbours and the weight of the second.
+__device__ __forceinline__ void bil_axis(int x, float inv, int dn, int& x0, int& x1, float& t) {
+    const float f = fminf(fmaxf(__fsub_rn(__fmul_rn(__fadd_rn((float)x, 0.5f), inv), 0.5f), 0.f), (float)(dn - 1));
+    x0 = (int)f;
+    x1 = min(x0 + 1, dn - 1);
+    t = __fsub_rn(f, (float)x0);
+}
+// ... and the bilinear value of a grid plane g (dw wide) there, in the reference's order
+__device__ __forceinline__ float bil(const float* g, int dw, int x0, int x1, int y0, int y1, float tx, float ty) {
+    const float* r0 = g + (size_t)y0 * dw;
+    const float* r1 = g + (size_t)y1 * dw;
+    const float top = __fadd_rn(r0[x0], __fmul_rn(__fsub_rn(r0[x1], r0[x0]), tx));
+    const float bot = __fadd_rn(r1[x0], __fmul_rn(__fsub_rn(r1[x1], r1[x0]), tx));
+    return __fadd_rn(top, __fmul_rn(__fsub_rn(bot, top), ty));
+}
 // Error flag bits a kernel may raise in the engine's device status word.
 enum { LSB_ERR_BOUNDS = 1, LSB_ERR_TIMEOUT = 2, LSB_ERR_SHAPE = 4 };

@@ -91,6 +91,8 @@ __global__ void gf_ab_kernel(const float* __restrict__ mp, const float* corr, co
 
 static int grid1(size_t n) { return (int)std::min<size_t>((n + 255) / 256, 148 * 16); }
 
+void box_mean_plane(const float* src, float* tmp, float* out, int w, int h, int r, cudaStream_t s) { box_mean(src, nullptr, tmp, out, w, h, r, s); }
+
 void gf_stats(const float* guide, int w, int h, int r, float* tmp, float* mean_i, float* var_i, cudaStream_t s) {
     box_mean(guide, nullptr, tmp, mean_i, w, h, r, s);
     box_mean(guide, guide, tmp, var_i, w, h, r, s);
@@ -630,19 +632,6 @@ cudaError_t robust_weights(const float* conf, const float* d, const float* u, fl
 
 // ----------------------------------------------------------------- upsample
 // depth.rs:201 `upsample_bilinear` weights for an axis position.
-__device__ __forceinline__ void bil_axis(int x, float inv, int dn, int& x0, int& x1, float& t) {
-    const float f = fminf(fmaxf(__fsub_rn(__fmul_rn(__fadd_rn((float)x, 0.5f), inv), 0.5f), 0.f), (float)(dn - 1));
-    x0 = (int)f;
-    x1 = min(x0 + 1, dn - 1);
-    t = __fsub_rn(f, (float)x0);
-}
-__device__ __forceinline__ float bil(const float* g, int dw, int x0, int x1, int y0, int y1, float tx, float ty) {
-    const float* r0 = g + (size_t)y0 * dw;
-    const float* r1 = g + (size_t)y1 * dw;
-    const float top = __fadd_rn(r0[x0], __fmul_rn(__fsub_rn(r0[x1], r0[x0]), tx));
-    const float bot = __fadd_rn(r1[x0], __fmul_rn(__fsub_rn(r1[x1], r1[x0]), tx));
-    return __fadd_rn(top, __fmul_rn(__fsub_rn(bot, top), ty));
-}
 // depth.rs:1183-1197: depth = clamp(a-bar(x) * Y + b-bar(x), 0, n-1) with the
 // coefficients bilinear from the grid (a = 0, b = u for bilinear upsampling);
 // the confidence bilinear too.
@@ -681,6 +670,54 @@ cudaError_t upsample(const float* abar, const float* bbar, const float* yfull, c
     }
     dim3 b(32, 8), g((w + 31) / 32, (h + 7) / 8);
     lsb_launched(), upsample_kernel<<<g, b, 0, s>>>(abar, bbar, yfull, conf, w, h, dw, dh, k, max_d, guided ? 1 : 0, depth, conf_full);
+    return cudaGetLastError();
+}
+
+// ------------------------------------------------------ the weighted average
+// wav.rs:84 `weight` of every cell: (c - (1 + gate) f).max(0)^power + (1e-2 f)^power + 1e-30
+__global__ void wav_weight_kernel(const float* __restrict__ c, const float* __restrict__ floor, size_t m, float gate, float power,
+                                  float* __restrict__ out) {
+    const float g1 = __fadd_rn(1.f, gate);
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < m; i += (size_t)gridDim.x * blockDim.x) {
+        const float f = floor[i];
+        const float a = fmaxf(__fsub_rn(c[i], __fmul_rn(g1, f)), 0.f);
+        out[i] = __fadd_rn(__fadd_rn(powf(a, power), powf(__fmul_rn(1e-2f, f), power)), 1e-30f);
+    }
+}
+// wav.rs:140: the guided filter's output a-bar * I + b-bar, kept a weight (>= 1e-30)
+__global__ void wav_guided_kernel(const float* __restrict__ abar, const float* __restrict__ bbar, const float* __restrict__ guide, size_t m,
+                                  float* __restrict__ out) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < m; i += (size_t)gridDim.x * blockDim.x)
+        out[i] = fmaxf(__fadd_rn(__fmul_rn(abar[i], guide[i]), bbar[i]), 1e-30f);
+}
+__global__ void half_plane_kernel(const __half* __restrict__ src, size_t m, float* __restrict__ out) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < m; i += (size_t)gridDim.x * blockDim.x) out[i] = __half2float(src[i]);
+}
+
+// wav.rs:131-145 for one frame: its contrast on the grid (the focus slice the fold took), box-smoothed
+// (BoxFilter::mean, radius smooth), weighed against the floor cells, then smoothed again by the guided
+// filter (guide, mean_i, var_i of radius smooth, eps) or the box mean, into out.
+cudaError_t wav_weights(const void* slice, bool half, const float* floor, int dw, int dh, float gate, float power, int smooth, bool edge,
+                        const float* guide, const float* mean_i, const float* var_i, float eps, WavScratch& t, float* out, cudaStream_t s) {
+    const size_t m = (size_t)dw * dh;
+    const float* src = (const float*)slice;
+    if (half) {
+        lsb_launched(), half_plane_kernel<<<grid1(m), 256, 0, s>>>((const __half*)slice, m, t.s0);
+        src = t.s0;
+    }
+    if (smooth > 0) {
+        box_mean(src, nullptr, t.tmp, t.s1, dw, dh, smooth, s);
+        src = t.s1;
+    }
+    lsb_launched(), wav_weight_kernel<<<grid1(m), 256, 0, s>>>(src, floor, m, gate, power, t.s0);
+    if (edge && smooth > 0) {
+        gf_coeffs(guide, mean_i, var_i, t.s0, dw, dh, smooth, eps, t.t0, t.t1, t.t2, t.tmp, t.abar, t.bbar, s);
+        lsb_launched(), wav_guided_kernel<<<grid1(m), 256, 0, s>>>(t.abar, t.bbar, guide, m, out);
+    } else if (smooth > 0) {
+        box_mean(t.s0, nullptr, t.tmp, out, dw, dh, smooth, s);
+    } else {
+        return cudaMemcpyAsync(out, t.s0, sizeof(float) * m, cudaMemcpyDeviceToDevice, s);
+    }
     return cudaGetLastError();
 }
 

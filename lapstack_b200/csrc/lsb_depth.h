@@ -30,6 +30,13 @@ cudaError_t peak_finish(const float* state, size_t m, int n, const float* floor_
 cudaError_t median3(const float* src, float* out, int w, int h, cudaStream_t s);
 cudaError_t conf_scale(float* conf, size_t m, const float* p90, cudaStream_t s);
 cudaError_t robust_weights(const float* conf, const float* d, const float* u, float tau, float* w2, size_t m, cudaStream_t s);
+// the weighted average (wav.rs:92): scratch planes on the depth grid, one frame's weight plane
+struct WavScratch {
+    float *s0, *s1, *t0, *t1, *t2, *tmp, *abar, *bbar;
+};
+void box_mean_plane(const float* src, float* tmp, float* out, int w, int h, int r, cudaStream_t s);
+cudaError_t wav_weights(const void* slice, bool half, const float* floor, int dw, int dh, float gate, float power, int smooth, bool edge,
+                        const float* guide, const float* mean_i, const float* var_i, float eps, WavScratch& t, float* out, cudaStream_t s);
 cudaError_t upsample(const float* abar, const float* bbar, const float* yfull, const float* guide, const float* conf, int w,
                      int h, int dw, int dh, int k, float max_d, bool guided, float* depth, float* conf_full, cudaStream_t s);
 

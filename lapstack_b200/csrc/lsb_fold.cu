@@ -78,10 +78,11 @@ __global__ void select_merge_kernel(const FoldArgs a, int G) {
 }
 
 // The fused level-0 kernel applies: 16-bit frames, one call doing the REDUCE and the selection of the
-// same frames, no halo control and no frame groups, no focus slice or the default one (ring difference
-// filter r 1..3 on 2x2 blocks), and a frame with interior tiles.
+// same frames, no halo control, no focus slice or the default one (ring difference filter r 1..3 on
+// 2x2 blocks), and a frame with interior tiles. It walks all the frames per tile, so the level is then
+// selected without frame groups.
 static bool fold0_applies(const FoldArgs& a, int src, bool focus, int R) {
-    if (src != SRC_U16 || a.level != 0 || a.halo_mode != 0 || a.sel_groups > 1 || !a.select || a.red_n <= 0) return false;
+    if (src != SRC_U16 || a.level != 0 || a.halo_mode != 0 || !a.select || a.red_n <= 0) return false;
     if (a.red_k0 != a.sel_k0 || a.red_n != a.sel_k1 - a.sel_k0) return false;
     if (focus && !(a.rdf13 && a.bk == 2 && a.focus_kind == 0)) return false;
     return fold0_count(fold0_range(a.W, a.H, R)) > 0;
@@ -108,6 +109,7 @@ static cudaError_t launch_level(const FoldArgs& a0, cudaStream_t s, int grid_lim
         lsb_launched(), kf<<<std::min(nf, std::max(grid_limit, 1)), f0::NT0, f0::SMEM, s>>>(a);
         if (a.between) cudaEventRecord(a.between, s);
         a.between = nullptr;
+        a.sel_groups = 1;  // the border tiles too: a group merge would run over the whole level
         a.fused0 = 1;
         a.f0r = R;
         a.ntiles = fold0_border_count(a.tiles_x, a.tiles_y, rg);

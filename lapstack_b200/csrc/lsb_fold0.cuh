@@ -48,22 +48,37 @@ __device__ __forceinline__ float2 mul2(float2 a, float2 b) {
     return d;
 }
 __device__ __forceinline__ float2 splat(float v) { return make_float2(v, v); }
-// pyramid.rs:95 tap5 on two independent lanes
+// ptxas contracts a packed multiply that feeds a packed add into one fused multiply-add, whatever
+// the .rn modifiers, which changes the rounding. So a packed add follows a packed multiply only when
+// the product is exact (a power-of-two factor: 1/16, 1/4, 1/8, 1/2, where contraction changes
+// nothing); an inexact product is added lane by lane, with scalar round-to-nearest adds.
+__device__ __forceinline__ float2 addl(float2 a, float2 p) { return make_float2(__fadd_rn(a.x, p.x), __fadd_rn(a.y, p.y)); }
+// pyramid.rs:95 tap5 on two independent lanes (K0 = 1/16, K1 = 1/4 exact; K2 = 6/16 not)
 __device__ __forceinline__ float2 tap5x2(float2 s0, float2 s1, float2 s2, float2 s3, float2 s4) {
     float2 a = mul2(splat(LSB_K0), s0);
     a = add2(a, mul2(splat(LSB_K1), s1));
-    a = add2(a, mul2(splat(LSB_K2), s2));
+    a = addl(a, mul2(splat(LSB_K2), s2));
     a = add2(a, mul2(splat(LSB_K1), s3));
     return add2(a, mul2(splat(LSB_K0), s4));
 }
-// pyramid.rs:128-166 EXPAND taps on two lanes
+// pyramid.rs:128-166 EXPAND taps on two lanes (E0 = 1/8 and OD = 1/2 exact; E1 = 3/4 not)
 __device__ __forceinline__ float2 exp_even2(float2 a, float2 b, float2 c) {
-    return add2(add2(mul2(splat(LSB_E0), a), mul2(splat(LSB_E1), b)), mul2(splat(LSB_E0), c));
+    return add2(addl(mul2(splat(LSB_E0), a), mul2(splat(LSB_E1), b)), mul2(splat(LSB_E0), c));
 }
 __device__ __forceinline__ float2 exp_odd2(float2 a, float2 b) { return mul2(splat(LSB_OD), add2(a, b)); }
-// fuse.rs:160 luma on two lanes
+// fuse.rs:160 luma on two lanes (no weight is a power of two)
 __device__ __forceinline__ float2 luma2(float2 r, float2 g, float2 b) {
-    return add2(add2(mul2(splat(0.299f), r), mul2(splat(0.587f), g)), mul2(splat(0.114f), b));
+    return addl(addl(mul2(splat(0.299f), r), mul2(splat(0.587f), g)), mul2(splat(0.114f), b));
+}
+// w * v added to s, the product exact when w is a power of two
+template <bool EXACT>
+__device__ __forceinline__ float2 acc2(float2 s, float w, float2 v) {
+    return EXACT ? add2(s, mul2(splat(w), v)) : addl(s, mul2(splat(w), v));
+}
+// binw<R>(q) is a power of two except 6/16 (R = 2, q = 2)
+template <int R>
+__device__ __forceinline__ constexpr bool binw_exact(int q) {
+    return !(R == 2 && q == 2);
 }
 
 // ------------------------------------------------- bulk copies on an mbarrier
@@ -207,8 +222,8 @@ __device__ __forceinline__ void f0_focus(const FoldArgs& a, const float* __restr
                 const int dy = T[q][0], dx = T[q][1];
                 const float2 v = (dx & 1) ? *(const float2*)(Ly + (row + dy) * LYW + col + dx)
                                           : *(const float2*)(Ls + (row + dy) * LYW + col + dx - 1);
-                const float2 t = mul2(T[q][2] ? wr : wd, v);
-                s = q == 0 ? t : add2(s, t);
+                const float2 t = mul2(T[q][2] ? wr : wd, v);  // 1/5, -1/24: inexact products, added lane by lane
+                s = q == 0 ? t : addl(s, t);
             }
             const float rs = __fadd_rn(fabsf(s.x), fabsf(s.y));
             o = dy0 == 0 ? rs : __fadd_rn(o, rs);
@@ -325,7 +340,7 @@ __device__ __forceinline__ void f0_laplace(const float* __restrict__ exph, float
         }
         float2 en;
         if (chroma) {
-            en = add2(add2(mul2(L[0], L[0]), mul2(L[1], L[1])), mul2(L[2], L[2]));
+            en = addl(addl(mul2(L[0], L[0]), mul2(L[1], L[1])), mul2(L[2], L[2]));
         } else {
             const float2 y = luma2(L[0], L[1], L[2]);
             en = mul2(y, y);
@@ -351,7 +366,8 @@ __device__ __forceinline__ void f0_window_rows(const float* __restrict__ yb, flo
         for (int i = 0; i < 4; i++) {
             float2 s = mul2(splat(binw<R>(0)), v[i]);
 #pragma unroll
-            for (int q = 1; q <= 2 * R; q++) s = add2(s, mul2(splat(binw<R>(q)), v[i + q]));
+            for (int q = 1; q <= 2 * R; q++) s = binw_exact<R>(q) ? add2(s, mul2(splat(binw<R>(q)), v[i + q]))
+                                                                : addl(s, mul2(splat(binw<R>(q)), v[i + q]));
             eh[r0 * TW0 + xo0 + i] = s.x;
             eh[(r0 + 1) * TW0 + xo0 + i] = s.y;
         }
@@ -376,7 +392,8 @@ __device__ __forceinline__ void f0_select(const float* __restrict__ en, const fl
         if (R > 0) {
             e = mul2(splat(binw<R>(0)), v[j]);
 #pragma unroll
-            for (int q = 1; q <= 2 * R; q++) e = add2(e, mul2(splat(binw<R>(q)), v[j + q]));
+            for (int q = 1; q <= 2 * R; q++) e = binw_exact<R>(q) ? add2(e, mul2(splat(binw<R>(q)), v[j + q]))
+                                                                : addl(e, mul2(splat(binw<R>(q)), v[j + q]));
         }
         const int wr = 4 * ty + j + 6, wc = px + 6 + (R & 1);
 #pragma unroll

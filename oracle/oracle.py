@@ -108,6 +108,8 @@ def _declare(L):
         ("orc_set_threads", None, [C.c_int]),
         ("orc_threads", C.c_int, []),
         ("orc_synth_stack", C.c_int, [P, P, P, C.c_uint32, C.c_uint32]),
+        ("orc_stack_wav", C.c_int, [P, P]),
+        ("orc_weighted_average_f", None, [P, sz, sz, sz, P, P, P, P, P]),
     ]:
         f = getattr(L, name)
         f.restype = res
@@ -193,16 +195,27 @@ class DepthParams:  # depth.rs:69-109
 
 
 @dataclass
+class WavParams:  # wav.rs:52-80
+    power: float = 2.0
+    smooth: int = 3
+    gate: float = 0.5
+    edge: bool = True
+
+
+@dataclass
 class StackParams:  # stack.rs:27-71 (the hot-path subset)
     fuse: FuseParams = field(default_factory=FuseParams)
     align: AlignParams | None = field(default_factory=AlignParams)
     depth: DepthParams | None = field(default_factory=DepthParams)
     brightness: bool = True
     crop: bool = True
+    wav: WavParams | None = None  # stack.rs:857 the weighted average too (needs depth)
 
     def arr(self):
         a = self.fuse.arr() + (self.align or AlignParams()).arr() + (self.depth or DepthParams()).arr()
         a += [float(self.align is not None), float(self.depth is not None), float(self.brightness), float(self.crop)]
+        w = self.wav or WavParams()
+        a += [float(self.wav is not None), w.power, w.smooth, w.gate, float(w.edge)]
         return np.asarray(a, dtype=F64)
 
 
@@ -576,6 +589,21 @@ def depth_from_slices(slices, fused, params: DepthParams | None = None, fp64=Fal
     return depth, conf, floor_cells.reshape(int(st[6]), int(st[5])), stats
 
 
+def weighted_average(frames, params: DepthParams | None = None, wav: "WavParams | None" = None, floor=None, guide=None):
+    """wav.rs:92 `weighted_average` of (n, 3, h, w) f32 frames: floor on the depth grid (zeros: none),
+    guide the fused (3, h, w) image or None (the box mean)."""
+    p, wp = params or DepthParams(), wav or WavParams()
+    fr = c32(frames)
+    n, _, h, w = fr.shape
+    k = 1 << p.scale
+    fl = c32(floor if floor is not None else np.zeros((blocks(h, k), blocks(w, k)), F32))
+    g = c32(guide) if guide is not None else None
+    out = np.empty((3, h, w), F32)
+    lib().orc_weighted_average_f(_ptr(fr), n, w, h, _ptr(_arr(p.arr())), _ptr(_arr([wp.power, wp.smooth, wp.gate, float(wp.edge)])),
+                                 _ptr(fl), _ptr(g), _ptr(out))
+    return out
+
+
 # --------------------------------------------------------------------- stack
 @dataclass
 class StackResult:
@@ -589,6 +617,7 @@ class StackResult:
     gains: np.ndarray  # (n, 3)
     shares: np.ndarray
     stats: dict
+    wav: np.ndarray | None = None  # (3, h, w) float64, the weighted average when asked for
 
 
 def run_stack(frames_u16, params: StackParams | None = None, fp64=False) -> StackResult:
@@ -674,6 +703,9 @@ def _result_of(r, p, n, w, h) -> "StackResult":
         sims, gains = np.empty((n, 8), F64), np.empty((n, 3), F32)
         shares = np.zeros(n, F32)
         L.orc_stack_sims(r, _ptr(sims), _ptr(gains), _ptr(shares))
-        return StackResult(img, u16, win, depth, conf, floor_cells, sims, gains, shares, stats)
+        wav = np.empty((3, h, w), F64)
+        if not L.orc_stack_wav(r, _ptr(wav)):
+            wav = None
+        return StackResult(img, u16, win, depth, conf, floor_cells, sims, gains, shares, stats, wav)
     finally:
         L.orc_stack_free(r)

@@ -355,6 +355,11 @@ static StackParams stack_params_of(const double* sp) {
     p.depth = sp[31] != 0.0;
     p.brightness = sp[32] != 0.0;
     p.crop = sp[33] != 0.0;
+    p.wav = sp[34] != 0.0;
+    p.wp.power = (float)sp[35];
+    p.wp.smooth = (size_t)sp[36];
+    p.wp.gate = (float)sp[37];
+    p.wp.edge = sp[38] != 0.0;
     return p;
 }
 void* orc_run_stack(const uint16_t* frames, size_t n, size_t w, size_t h, const double* sp, int fp64) {
@@ -482,6 +487,41 @@ void* orc_stack_end(void* p) {
     return r;
 }
 void orc_stack_abort(void* p) { delete (StackInc*)p; }
+
+// wav.rs:92 weighted_average over n planar f32 frames [n][3][h][w]; dp as depth_of reads it; wp = [power,
+// smooth, gate, edge]; floor on the depth grid; guide planar [3][h][w] or null
+void orc_weighted_average_f(const float* frames, size_t n, size_t w, size_t h, const double* dp, const double* wp, const float* floor,
+                            const float* guide, float* out) {
+    std::vector<Img3<float>> fr(n, Img3<float>(w, h));
+    for (size_t k = 0; k < n; k++)
+        for (int c = 0; c < 3; c++) std::copy(frames + (k * 3 + c) * w * h, frames + (k * 3 + c + 1) * w * h, fr[k].p[c].begin());
+    DepthParams d = depth_of(dp);
+    WavParams p;
+    p.power = (float)wp[0];
+    p.smooth = (size_t)wp[1];
+    p.gate = (float)wp[2];
+    p.edge = wp[3] != 0.0;
+    const size_t k = (size_t)1 << d.scale;
+    std::vector<float> fl(floor, floor + blocks(w, k) * blocks(h, k));
+    Img3<float> g(w, h);
+    if (guide)
+        for (int c = 0; c < 3; c++) std::copy(guide + c * w * h, guide + (c + 1) * w * h, g.p[c].begin());
+    Img3<float> o = weighted_average<float>(fr, d, p, fl, guide ? &g : nullptr);
+    for (int c = 0; c < 3; c++) std::copy(o.p[c].begin(), o.p[c].end(), out + c * w * h);
+}
+
+// the weighted average (planar f64, exact for both precisions); 0 when the run made none
+int orc_stack_wav(void* p, double* planes) {
+    StackRes* r = (StackRes*)p;
+    auto fill = [&](auto& o) {
+        if (o.wav.w == 0) return 0;
+        const size_t n = o.wav.w * o.wav.h;
+        for (int c = 0; c < 3; c++)
+            for (size_t i = 0; i < n; i++) planes[c * n + i] = (double)o.wav.p[c][i];
+        return 1;
+    };
+    return r->dbl ? fill(r->d) : fill(r->f);
+}
 
 // OpenMP threads of every later oracle call (0: all the host's)
 void orc_set_threads(int n) { omp_set_num_threads(n > 0 ? n : omp_get_num_procs()); }

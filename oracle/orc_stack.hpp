@@ -6,6 +6,7 @@
 #pragma once
 #include "orc_align.hpp"
 #include "orc_depth.hpp"
+#include "orc_wav.hpp"
 
 namespace orc {
 
@@ -17,6 +18,8 @@ struct StackParams {
     DepthParams dp;
     bool brightness = true;
     bool crop = true;
+    bool wav = false;  // stack.rs:857 `weighted`: the weighted average too (needs the depth pass)
+    WavParams wp;
 };
 
 template <class T>
@@ -30,6 +33,7 @@ struct StackOutput {
     Rect crop;                     // the common area (full frame when nothing is cut)
     size_t levels = 0;
     size_t align_evals = 0;
+    Img3<T> wav;                   // the weighted average (wav.rs:92), when asked for
 };
 
 // io.rs:89-94 u16 -> f32 as v * (1/65535) (an f32 multiply by the f32 reciprocal)
@@ -66,6 +70,7 @@ struct StackRun {
     BReference<T> bref;
     double ref_means[3] = {0, 0, 0};
     size_t i = 0;
+    std::vector<Img3<T>> kept;  // the frames as folded, for the weighted average
     StackRun(size_t w_, size_t h_, size_t n, const StackParams& sp_) : w(w_), h(h_), sp(sp_), fuser(w_, h_, sp_.fuse) {
         out.levels = fuser.levels;
         aligned = sp.align && n > 1;
@@ -126,12 +131,14 @@ struct StackRun {
             size_t dw, dh;
             slices.push_back(focus_slice<T>(img, sp.dp, dw, dh));
         }
+        if (sp.wav && sp.depth) kept.push_back(img);
         i++;
     }
     void finish() {
         out.shares = fuser.shares();
         fuser.finish(out.image, out.winner);
         if (sp.depth) out.dm = depth_from_slices<T>(slices, out.image, sp.dp);
+        if (sp.wav && sp.depth && !kept.empty()) out.wav = weighted_average<T>(kept, sp.dp, sp.wp, out.dm.floor_cells, &out.image);
         out.crop = Rect{0, 0, w, h};
         if (aligned && sp.crop) out.crop = common_area(out.sims, w, h, sp.al.interp);
     }

@@ -70,6 +70,7 @@ def check_stack(frames, fuse, align, depth, depth_frac=1e-3):
     assert_same(ref.gains, out.gains, "gains")
     assert_same(ref.winner, out.winner, "winner map")
     assert_same(ref.image_u16, out.image_u16, "fused u16")
+    assert_same(ref.image.astype(np.float32), out.image, "fused f32 planes")
     assert_same(ref.shares, out.shares, "shares")
     if depth is not None:
         assert_same(ref.floor_cells.astype(np.float32), out.depth.floor, "floor cells (focus slices bit-exact)")

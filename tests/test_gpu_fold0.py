@@ -66,6 +66,24 @@ def test_fused_level0_odd_sizes(w, h):
              run(fr, storage, False, L.FuseParams(), depth=L.DepthParams()))
 
 
+@pytest.mark.parametrize("n,top", [(1, "avg"), (2, "de"), (3, "avg")])
+def test_fused_level0_few_frames_f32_planes_match_oracle(n, top):
+    """Few frames, gains of exactly 1 and a 1- or 2-level pyramid: the fused image's f32 planes equal
+    the oracle's bit for bit, so every rounding of the level-0 Laplacian is the reference's (a fused
+    multiply-add anywhere would move some of them by an ulp)."""
+    fr = L.synth_stack(L.SynthSpec(1024, 768, n, mag_step=0.0, noise_std=0.003, seed=5))[0]
+    for levels in (1, 2):
+        fuse = L.FuseParams(levels=levels, top_rule=top)
+        ref = O.run_stack(fr, O.StackParams(fuse=O.FuseParams(levels=levels, top_rule=top), align=None, depth=None, brightness=False))
+        eng = L.Engine(storage="f32")
+        st = eng.stack(1024, 768, n, fuse, None, None, brightness=False)
+        for f in fr:
+            st.push_u16(f)
+        out = st.finish()
+        assert np.array_equal(ref.image.astype(np.float32), out.image), (levels, np.count_nonzero(ref.image.astype(np.float32) != out.image))
+        assert np.array_equal(ref.winner, out.winner)
+
+
 def test_fused_level0_aligned_16bit_frames():
     """Aligned stacks with 16-bit storage fold their warped u16 frames through the fused kernel."""
     fr = L.synth_stack(L.SynthSpec(640, 480, 4, warp=True, mag_step=0.0, seed=47))[0]
@@ -81,5 +99,6 @@ def test_fused_level0_matches_oracle():
     out = run(fr, "f32", True, L.FuseParams(), depth=L.DepthParams())
     assert np.array_equal(ref.gains, out.gains)
     assert np.array_equal(ref.image_u16, out.image_u16)
+    assert np.array_equal(ref.image.astype(np.float32), out.image)
     assert np.array_equal(ref.winner, out.winner)
     assert np.array_equal(ref.floor_cells.astype(np.float32), out.depth.floor)
