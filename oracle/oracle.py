@@ -210,12 +210,15 @@ class StackParams:  # stack.rs:27-71 (the hot-path subset)
     brightness: bool = True
     crop: bool = True
     wav: WavParams | None = None  # stack.rs:857 the weighted average too (needs depth)
+    # the engine's 16-bit level storage to emulate ("f32": the reference itself; "unorm16", "f16")
+    storage: str = "f32"
 
     def arr(self):
         a = self.fuse.arr() + (self.align or AlignParams()).arr() + (self.depth or DepthParams()).arr()
         a += [float(self.align is not None), float(self.depth is not None), float(self.brightness), float(self.crop)]
         w = self.wav or WavParams()
         a += [float(self.wav is not None), w.power, w.smooth, w.gate, float(w.edge)]
+        a += [float(["f32", "unorm16", "f16"].index(self.storage))]
         return np.asarray(a, dtype=F64)
 
 

@@ -360,6 +360,7 @@ static StackParams stack_params_of(const double* sp) {
     p.wp.smooth = (size_t)sp[36];
     p.wp.gate = (float)sp[37];
     p.wp.edge = sp[38] != 0.0;
+    p.storage = (int)sp[39];
     return p;
 }
 void* orc_run_stack(const uint16_t* frames, size_t n, size_t w, size_t h, const double* sp, int fp64) {
@@ -521,6 +522,14 @@ int orc_stack_wav(void* p, double* planes) {
         return 1;
     };
     return r->dbl ? fill(r->d) : fill(r->f);
+}
+
+// f32 -> IEEE half bits (round to nearest even) and back, as the 16-bit storage emulation does them
+void orc_f16_round(const float* in, size_t n, uint16_t* bits, float* back) {
+    for (size_t i = 0; i < n; i++) {
+        bits[i] = f16_bits(in[i]);
+        back[i] = f16_value(bits[i]);
+    }
 }
 
 // OpenMP threads of every later oracle call (0: all the host's)

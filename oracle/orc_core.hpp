@@ -148,13 +148,20 @@ inline size_t auto_levels(size_t w, size_t h, size_t min_top) {
     return std::max<size_t>(n, 1);
 }
 
-// pyramid.rs:203 `build`: [L_0 .. L_{N-1}, G_N]
 template <class T>
-std::vector<Img3<T>> build(const Img3<T>& img, size_t levels) {
+inline T stored(T v, int storage, const float scale[2]);
+
+// pyramid.rs:203 `build`: [L_0 .. L_{N-1}, G_N]. With a 16-bit storage (the engine's, see `stored`)
+// every level >= 1 is rounded as stored before anything reads it.
+template <class T>
+std::vector<Img3<T>> build(const Img3<T>& img, size_t levels, int storage = 0, const float* scale = nullptr) {
     std::vector<Img3<T>> out;
     Img3<T> g = img;
     for (size_t l = 0; l < levels; l++) {
         Img3<T> next = reduce3(g);
+        if (storage != 0)
+            for (int c = 0; c < 3; c++)
+                for (auto& v : next.p[c]) v = stored(v, storage, scale);
         Img3<T> up = expand3(next, g.w, g.h);
         for (int c = 0; c < 3; c++)
             for (size_t i = 0; i < g.w * g.h; i++) g.p[c][i] -= up.p[c][i];
@@ -179,6 +186,55 @@ Img3<T> collapse(std::vector<Img3<T>> pyr) {
         g = std::move(l);
     }
     return g;
+}
+
+// ------------------------------------------- the engine's 16-bit level storage
+// Not the reference's: the rounding the CUDA engine applies when it stores Gaussian levels >= 1 in 16
+// bits, so that its 16-bit path can be checked against the reference algorithm run with the same
+// storage. STORE_UNORM16: a level of a frame whose largest gain is g (at least 1) is kept as
+// u = (u16) clamp(v * (65535 / g) + 0.5, 0, 65535) and read back as u * (g / 65535), both factors
+// rounded to f32 once; STORE_F16: IEEE half, round to nearest even.
+enum Storage { STORE_F32 = 0, STORE_UNORM16 = 1, STORE_F16 = 2 };
+
+// f32 -> f16 bits, round to nearest even (overflow to infinity, subnormal halves kept)
+inline uint16_t f16_bits(float f) {
+    uint32_t x;
+    std::memcpy(&x, &f, 4);
+    const uint32_t sign = (x >> 16) & 0x8000u, ax = x & 0x7fffffffu;
+    if (ax >= 0x7f800000u) return (uint16_t)(sign | 0x7c00u | (ax > 0x7f800000u ? 0x200u : 0u));  // inf, nan
+    if (ax >= 0x477ff000u) return (uint16_t)(sign | 0x7c00u);  // rounds past the largest half
+    if (ax >= 0x38800000u) {  // a normal half: drop 13 mantissa bits, nearest even
+        uint32_t m = ax - 0x38000000u;  // rebias the exponent (127 -> 15) in place
+        const uint32_t rest = m & 0x1fffu;
+        m >>= 13;
+        if (rest > 0x1000u || (rest == 0x1000u && (m & 1u))) m++;
+        return (uint16_t)(sign | m);
+    }
+    // a subnormal half (or zero): the value in units of 2^-24, nearest even
+    const int e = (int)(ax >> 23) - 127;  // the f32's exponent
+    if (e < -25) return (uint16_t)sign;
+    const uint32_t mant = (ax & 0x7fffffu) | 0x800000u;  // 24 significant bits, value = mant * 2^(e - 23)
+    const int shift = -e - 1;  // units of 2^-24: mant * 2^(e + 1) = mant >> (-(e + 1))
+    const uint32_t q = mant >> shift, rem = mant & ((1u << shift) - 1u), half = 1u << (shift - 1);
+    return (uint16_t)(sign | (q + ((rem > half || (rem == half && (q & 1u))) ? 1u : 0u)));
+}
+inline float f16_value(uint16_t h) {
+    const uint32_t sign = (uint32_t)(h & 0x8000u) << 16, e = (h >> 10) & 0x1fu, m = h & 0x3ffu;
+    float v;
+    if (e == 0) v = std::ldexp((float)m, -24);
+    else if (e == 31) v = m ? std::numeric_limits<float>::quiet_NaN() : std::numeric_limits<float>::infinity();
+    else v = std::ldexp((float)(m | 0x400u), (int)e - 25);
+    return sign ? -v : v;
+}
+// a level value as the storage gives it back; scale = (65535 / g, g / 65535) of the frame
+template <class T>
+inline T stored(T v, int storage, const float scale[2]) {
+    if (storage == STORE_UNORM16) {
+        const float u = std::min(std::max((float)v * scale[0] + 0.5f, 0.f), 65535.f);
+        return (T)((float)(uint16_t)u * scale[1]);
+    }
+    if (storage == STORE_F16) return (T)f16_value(f16_bits((float)v));
+    return v;
 }
 
 // -------------------------------------------------------------------- fuse.rs
@@ -428,6 +484,7 @@ struct Fuser {
     size_t halo_guide = 0;
     T halo_p = T(0);
     size_t count = 0;
+    int storage = 0;  // the engine's level storage to emulate (STORE_*; 0 = the reference's f32)
 
     Fuser(size_t w_, size_t h_, const FuseParams& p) : w(w_), h(h_), params(p) {
         levels = std::max<size_t>(p.levels ? p.levels : auto_levels(w, h, 32), 1);
@@ -440,9 +497,11 @@ struct Fuser {
     }
     size_t select_levels() const { return halo_on ? halo_guide + 1 : levels; }
 
-    // fuse.rs:401 `push`
-    void push(const Img3<T>& frame) {
-        std::vector<Img3<T>> pyr = build(frame, levels);
+    // fuse.rs:401 `push`; `max_gain`: the frame's largest brightness gain (the 16-bit storage's scale)
+    void push(const Img3<T>& frame, float max_gain = 1.0f) {
+        const float g = std::max(1.0f, max_gain);
+        const float scale[2] = {(float)(65535.0 / g), (float)(g / 65535.0)};
+        std::vector<Img3<T>> pyr = build(frame, levels, storage, scale);
         size_t nsel = select_levels();
         uint16_t idx = (uint16_t)count;
         bool first = count == 0;

@@ -20,6 +20,9 @@ struct StackParams {
     bool crop = true;
     bool wav = false;  // stack.rs:857 `weighted`: the weighted average too (needs the depth pass)
     WavParams wp;
+    // the engine's 16-bit storage to emulate (not the reference's): levels >= 1 rounded as stored
+    // (orc_core.hpp `stored`), focus slices as IEEE half, aligned frames as u16 after their warp
+    int storage = 0;
 };
 
 template <class T>
@@ -73,6 +76,7 @@ struct StackRun {
     std::vector<Img3<T>> kept;  // the frames as folded, for the weighted average
     StackRun(size_t w_, size_t h_, size_t n, const StackParams& sp_) : w(w_), h(h_), sp(sp_), fuser(w_, h_, sp_.fuse) {
         out.levels = fuser.levels;
+        fuser.storage = sp.storage;
         aligned = sp.align && n > 1;
         free_mask(sp.al, freem);
     }
@@ -101,6 +105,17 @@ struct StackRun {
                         if (!valid[k]) warped.p[c][k] = img.p[c][k];
                 img = std::move(warped);
             }
+            // 16-bit storage keeps the warped frame as u16 (the brightness sums read the warp itself)
+            Img3<T> as_stored;
+            if (sp.storage != 0 && !sim.is_id()) {
+                as_stored = img;
+                const T inv = std::is_same<T, float>::value ? (T)(1.0f / 65535.0f) : (T)(1.0 / 65535.0);
+                for (int c = 0; c < 3; c++)
+                    for (auto& v : as_stored.p[c]) {
+                        const float u = std::min(std::max((float)v * 65535.f + 0.5f, 0.f), 65535.f);
+                        v = (T)(uint16_t)u * inv;
+                    }
+            }
             // stack.rs:680-690 brightness against frame 0 over the covered pixels
             if (sp.brightness) {
                 if (i == 0) {
@@ -110,9 +125,10 @@ struct StackRun {
                     size_t cnt;
                     bsums<T>(img, &bref, sim, sf, so, cnt);
                     bratio(so, sf, cnt, gain.data());
-                    bapply<T>(img, gain.data());
                 }
             }
+            if (as_stored.w) img = std::move(as_stored);
+            if (sp.brightness && i > 0) bapply<T>(img, gain.data());
         } else if (sp.brightness) {
             // stack.rs LazyFrames: frame 0's channel means, gains_to for the others
             if (i == 0) {
@@ -126,10 +142,12 @@ struct StackRun {
         }
         out.sims.push_back(sim);
         out.gains.push_back(gain);
-        fuser.push(img);
+        fuser.push(img, std::max(gain[0], std::max(gain[1], gain[2])));
         if (sp.depth) {
             size_t dw, dh;
             slices.push_back(focus_slice<T>(img, sp.dp, dw, dh));
+            if (sp.storage != 0)
+                for (auto& v : slices.back()) v = (T)f16_value(f16_bits((float)v));
         }
         if (sp.wav && sp.depth) kept.push_back(img);
         i++;
