@@ -16,6 +16,8 @@ published runs: a height field, band-limited texture, per-pixel defocus):
   c2  30 x 6000x4000, no alignment, 8 levels, aggregation radius 8, FP32
   c1  8 x 1024x768, no alignment, 6 levels, FP32
   c3s 16 x 2048x1536 with c3's settings: the small case the ncu captures use
+  c3m 32 x 4096x2752, c3's depth settings without alignment: the capture case whose focus slices
+      exceed L2 (about 3 GB on the device)
 
 --impl reference times the CPU restatement of the reference's path (the
 oracle; the Rust reference cannot be built here) on the same workload with
@@ -52,7 +54,10 @@ CONFIGS = {
                agg_radius=8, storage="f32"),
     "c1": dict(w=1024, h=768, n=8, warp=False, mag_step=0.002, noise_std=0.003, levels=6, align=False, coarsen=0,
                agg_radius=3, storage="f32"),
-    # c3's path at a size an ncu capture finishes quickly (frames still larger than L2)
+    # c3's path at sizes an ncu capture finishes quickly: frames larger than L2 (c3s), and focus
+    # slices larger than L2 too (c3m)
+    "c3m": dict(w=4096, h=2752, n=32, warp=False, mag_step=0.002, noise_std=0.002, levels=0, align=False, coarsen=0,
+                agg_radius=3, storage="unorm16"),
     "c3s": dict(w=2048, h=1536, n=16, warp=True, mag_step=0.0, noise_std=0.002, levels=0, align=True, coarsen=3,
                 agg_radius=3, storage="unorm16"),
 }
