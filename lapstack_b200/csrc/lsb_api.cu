@@ -71,6 +71,8 @@ struct DevPool {
 
 // Blocks per frame of the brightness sums (brightness.rs:67): their f64 partials are summed in block order.
 constexpr int BRIGHT_PARTS = 512;
+// Frames per selection chunk when the fold runs on the side stream as the transforms land.
+constexpr int SEL_CHUNK = 10;
 
 struct lsb_engine {
     lsb_config cfg;
@@ -167,7 +169,10 @@ struct lsb_stack {
     lsb_result* early = nullptr;   // finish: the result whose fused planes leave on rs while the depth runs
     cudaEvent_t fused_ev = nullptr;  // recorded on s once the fused planes and the winner map are written
     size_t x0_cells = 0;
+    std::vector<cudaEvent_t> chunk_ev;  // per selection chunk folded on ws: [start, after the fused kernel, end] of level 0
+    int chunks = 0;                     // chunks the last streamed fold ran
     ~lsb_stack() {
+        for (auto& v : chunk_ev) cudaEventDestroy(v);
         wls_destroy(ws);
         if (x0) cudaFree(x0);
         for (auto& v : copied) cudaEventDestroy(v);
@@ -428,6 +433,8 @@ static char* stack_alloc(lsb_stack* s) {
         for (auto& v : s->searched) TRY(cudaEventCreateWithFlags(&v, cudaEventDisableTiming));
         for (auto& v : s->sims_back) TRY(cudaEventCreateWithFlags(&v, cudaEventDisableTiming));
         TRY(cudaEventCreateWithFlags(&s->wdone, cudaEventDisableTiming));
+        s->chunk_ev.assign(3 * ((N + SEL_CHUNK - 1) / SEL_CHUNK), nullptr);
+        for (auto& v : s->chunk_ev) TRY(cudaEventCreate(&v));
     }
     s->copied.assign(N, nullptr);
     for (auto& v : s->copied) TRY(cudaEventCreateWithFlags(&v, cudaEventDisableTiming));
@@ -765,8 +772,7 @@ static void set_groups(const lsb_stack* s, FoldArgs& a) {
 // `select` too, every SEL_CHUNK frames are folded in level by level, their
 // REDUCE then their selection (fuse.rs:414-451, frames in order, resuming
 // from the state the chunk before left). The work stream waits for ws.
-constexpr int SEL_CHUNK = 10;
-static char* stream_warps(lsb_stack* s, bool reduce, bool select) {
+static char* stream_warps(lsb_stack* s, bool pushed, bool reduce, bool select) {
     lsb_engine* e = s->e;
     const int W = (int)s->w, H = (int)s->h, n = (int)s->count;
     const size_t np = (size_t)W * H;
@@ -807,7 +813,7 @@ static char* stream_warps(lsb_stack* s, bool reduce, bool select) {
             B.affine = B.inv[6] == 0.0 && B.inv[7] == 0.0 && B.inv[8] == 1.0;
             TRY(cudaMemcpyAsync(s->bx_dev + i, &B, sizeof B, cudaMemcpyHostToDevice, e->ws));
             // pushed frames: the whole GPU; frames in memory: a few blocks beside the registration chain
-            TRY(bright_sums_frame(s->frames, i, W, H, s->bx_dev, (int)s->ap.interp, BRIGHT_PARTS, s->bpart, reduce ? BRIGHT_PARTS : 64,
+            TRY(bright_sums_frame(s->frames, i, W, H, s->bx_dev, (int)s->ap.interp, BRIGHT_PARTS, s->bpart, pushed ? BRIGHT_PARTS : 64,
                                   e->ws));
             TRY(frame_gain(s->bpart, i, BRIGHT_PARTS, s->xf_dev + i, e->ws));
         }
@@ -822,7 +828,9 @@ static char* stream_warps(lsb_stack* s, bool reduce, bool select) {
         }
         if (reduce && select && (i + 1 - sel_from == SEL_CHUNK || i + 1 == n)) {
             // the chunk's frames level by level: their REDUCE (and focus slices), then their selection
-            // (level 0: one fused kernel where it applies)
+            // (level 0: one fused kernel where it applies), beside the registration chain: one
+            // persistent CTA per SM, so that the chain's cooperative search keeps room on every SM
+            const int ch = sel_from / SEL_CHUNK;
             for (int l = 0; l < s->levels; l++) {
                 bool focus = false;
                 int src = 0;
@@ -831,10 +839,17 @@ static char* stream_warps(lsb_stack* s, bool reduce, bool select) {
                 a.red_n = i + 1 - sel_from;
                 a.sel_k0 = sel_from;
                 a.sel_k1 = i + 1;
+                a.beside = 1;
                 set_groups(s, a);
-                TRY(fold_level(a, src, s->storage, (int)s->fp.energy_radius, focus, e->ws,
-                               e->grid_select > 0 ? e->grid_select : e->grid));
+                if (l == 0) {  // the level-0 fold of the chunk, timed: [start, after the fused kernel, end]
+                    TRY(cudaEventRecord(s->chunk_ev[3 * ch], e->ws));
+                    TRY(cudaEventRecord(s->chunk_ev[3 * ch + 1], e->ws));
+                    a.after_fused = s->chunk_ev[3 * ch + 1];
+                }
+                TRY(fold_level(a, src, s->storage, (int)s->fp.energy_radius, focus, e->ws, e->sms));
+                if (l == 0) TRY(cudaEventRecord(s->chunk_ev[3 * ch + 2], e->ws));
             }
+            s->chunks = ch + 1;
             sel_from = i + 1;
         }
     }
@@ -981,9 +996,12 @@ static char* run_pipeline_once(lsb_stack* s) {
     }
     TRY(cudaEventRecord(ev[1], st));
     const bool streamed = aligned && chained(s);
-    const bool sel_streamed = streamed && pushed && !(s->fp.halo > 0.f);  // the selection too (not with halo control)
+    // the fold too, chunk by chunk beside the chain (not with halo control; frames in device memory
+    // unless LSB_FLAG_FOLD_AFTER_CHAIN asks for the fold after the chain)
+    const bool sel_streamed = streamed && !(s->fp.halo > 0.f) && (pushed || !(e->cfg.flags & LSB_FLAG_FOLD_AFTER_CHAIN));
+    s->chunks = 0;
     if (streamed) {
-        char* err = stream_warps(s, pushed, sel_streamed);
+        char* err = stream_warps(s, pushed, pushed || sel_streamed, sel_streamed);
         if (!err) err = align_finish(s);
         if (err) return err;
     }
@@ -1198,6 +1216,14 @@ static char* run_pipeline_once(lsb_stack* s) {
     s->ms[9] = ms_between(ev[10], ev[9]);   // select, level 0
     s->ms[10] = ms_between(ev[8], ev[10]);  // REDUCE (+ focus slices), level 0
     s->ms[11] = ms_between(ev[11], ev[6]);  // the WLS solves (warm start included)
+    if (sel_streamed) {  // the level-0 fold ran chunk by chunk on ws: the sums of its parts
+        s->ms[8] = s->ms[9] = s->ms[10] = 0.0;
+        for (int c = 0; c < s->chunks; c++) {
+            s->ms[8] += ms_between(s->chunk_ev[3 * c], s->chunk_ev[3 * c + 2]);
+            s->ms[10] += ms_between(s->chunk_ev[3 * c], s->chunk_ev[3 * c + 1]);
+            s->ms[9] += ms_between(s->chunk_ev[3 * c + 1], s->chunk_ev[3 * c + 2]);
+        }
+    }
     return nullptr;
 }
 

@@ -100,13 +100,18 @@ static cudaError_t launch_level(const FoldArgs& a0, cudaStream_t s, int grid_lim
     if (e != cudaSuccess) return e;
     FoldArgs a = a0;
     int rtiles = ((a.W1 + RW - 1) / RW) * ((a.H1 + RH - 1) / RH);
+    // beside the registration chain: one persistent CTA per SM at most
+    const size_t ssm_run = a.beside ? std::max(ssm, BESIDE_SMEM) : ssm;
+    if (a.beside && (e = with_smem(ks, ssm_run)) != cudaSuccess) return e;
     if (SRC == SRC_U16 && !a0.no_fused && fold0_applies(a0, SRC, FOCUS, R)) {
         auto kf = fold0_kernel<GS, R, FOCUS, SS>;
-        e = with_smem(kf, f0::SMEM);
+        const size_t fsm = a.beside ? std::max((size_t)f0::SMEM, BESIDE_SMEM) : (size_t)f0::SMEM;
+        e = with_smem(kf, fsm);
         if (e != cudaSuccess) return e;
         const Fold0Range rg = fold0_range(a.W, a.H, R);
         const int nf = fold0_count(rg);
-        lsb_launched(), kf<<<std::min(nf, std::max(grid_limit, 1)), f0::NT0, f0::SMEM, s>>>(a);
+        lsb_launched(), kf<<<std::min(nf, std::max(grid_limit, 1)), f0::NT0, fsm, s>>>(a);
+        if (a.after_fused) cudaEventRecord(a.after_fused, s);
         if (a.between) cudaEventRecord(a.between, s);
         a.between = nullptr;
         a.sel_groups = 1;  // the border tiles too: a group merge would run over the whole level
@@ -119,7 +124,7 @@ static cudaError_t launch_level(const FoldArgs& a0, cudaStream_t s, int grid_lim
     if (a.red_n > 0) lsb_launched(), kr<<<dim3(rtiles, a.red_n), NT, rsm, s>>>(a);
     if (a.between) cudaEventRecord(a.between, s);
     const int groups = std::max(a.sel_groups, 1);
-    if (a.select) lsb_launched(), ks<<<std::min(a.ntiles * groups, std::max(grid_limit, 1)), NT, ssm, s>>>(a);
+    if (a.select) lsb_launched(), ks<<<std::min(a.ntiles * groups, std::max(grid_limit, 1)), NT, ssm_run, s>>>(a);
     if (a.select && groups > 1) {
         const size_t np = (size_t)a.W * a.H;
         lsb_launched(), select_merge_kernel<<<(unsigned)std::min<size_t>((np + 255) / 256, 148 * 8), 256, 0, s>>>(a, groups);

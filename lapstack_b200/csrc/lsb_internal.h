@@ -71,7 +71,13 @@ struct FoldArgs {
     // reduce_level_kernel / select_level_kernel walk the other ntiles tiles (fold0_border_tile)
     int fused0, f0r;
     int no_fused;  // 1: level 0 runs the two kernels on every tile (the fused kernel's cross-check)
+    // 1: the level runs beside the registration chain: its persistent kernels take at most one CTA per
+    // SM (they ask for BESIDE_SMEM of shared memory), so the chain's cooperative search keeps room
+    int beside;
+    cudaEvent_t after_fused;  // host side: recorded right after the fused level-0 kernel (may be null)
 };
+// shared memory a persistent fold kernel asks for beside the registration chain: more than half an SM's
+constexpr size_t BESIDE_SMEM = 116 * 1024;
 
 // Storage of the Gaussian levels >= 1 and the focus slices.
 enum Storage { STORE_F32 = 0, STORE_UNORM16 = 1, STORE_F16 = 2 };

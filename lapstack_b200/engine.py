@@ -183,14 +183,18 @@ class Engine:
 
     STORAGE = {"f32": 0, "unorm16": 1, "f16": 2}
 
-    def __init__(self, device: int = 0, storage: str = "f32", grid_limit: int = 0, log=None, fused_fold0: bool = True):
+    def __init__(self, device: int = 0, storage: str = "f32", grid_limit: int = 0, log=None, fused_fold0: bool = True,
+                 fold_beside_chain: bool = True):
         """storage: "f32" (bit-exact with the reference FP32 path), "unorm16" (16-bit
         Gaussian levels, FP16 slices) or "f16" (IEEE half levels and slices).
         fused_fold0=False folds level 0 with the separate REDUCE and select kernels on
-        every tile (LSB_FLAG_TWO_KERNEL_FOLD0): the same results, for cross-checks."""
+        every tile (LSB_FLAG_TWO_KERNEL_FOLD0); fold_beside_chain=False folds an aligned
+        stack in device memory after its registration chain instead of chunk by chunk
+        beside it (LSB_FLAG_FOLD_AFTER_CHAIN). Neither changes a result."""
         self._L = load()
         self._logcb = LOG_FN(lambda line, _u: log(line.decode())) if log else LOG_FN()
-        cfg = Config(device, self.STORAGE[storage], grid_limit, 0 if fused_fold0 else 1, self._logcb, None)
+        flags = (0 if fused_fold0 else 1) | (0 if fold_beside_chain else 2)
+        cfg = Config(device, self.STORAGE[storage], grid_limit, flags, self._logcb, None)
         h = C.c_void_p()
         check(self._L.lsb_engine_create(C.byref(cfg), C.byref(h)))
         self._h = h
