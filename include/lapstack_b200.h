@@ -129,6 +129,14 @@ typedef struct {
                             REDUCE kernel (or the fused kernel), then the WLS solves (warm start included) */
 } lsb_result;
 
+/* wav.rs:52-80 WavParams: the weighted average's settings (defaults 2, 3, 0.5, 1). */
+typedef struct {
+    float power;     /* the contrast above the floor raised to this */
+    uint32_t smooth; /* box radius of the contrast, then of the weights, on the working grid (0: none) */
+    float gate;      /* a contrast counts above (1 + gate) x the cell's noise floor */
+    uint32_t edge;   /* 1: the weights smoothed by the guided filter with the fused luma as guide */
+} lsb_wav_params;
+
 /* Seeded synthetic stack description (no reference counterpart; the benchmark inputs). */
 typedef struct {
     uint32_t w, h, n;
@@ -186,6 +194,11 @@ char* lsb_stack_shares(lsb_stack* s, float* out_n);
    `common_area`. Align, fold, depth: the whole pipeline over the frames pushed; may be called again.
    On an error *out is left empty (every pointer NULL, nothing to free). */
 char* lsb_stack_finish(lsb_stack* s, lsb_result* out);
+/* stack.rs:857 `weighted` / wav.rs:92 `weighted_average`: every frame of the last finish (or run),
+   as folded (aligned, gains applied), averaged with weights that follow its contrast above the depth
+   pass's per-cell noise floor; out receives 3*w*h planar f32 in [0,1] (host pointer). Needs a run
+   with the depth pass. The stack's fold and depth results stay as they were. */
+char* lsb_stack_weighted_average(lsb_stack* s, const lsb_wav_params* p, float* out);
 /* lsb_stack_finish without copying results back (device-resident benchmarking; no counterpart). */
 char* lsb_stack_run(lsb_stack* s, double* ms_out12);
 /* Explicit frees, as ffi.rs:129 lapstack_raw_free_image. */

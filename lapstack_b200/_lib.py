@@ -62,6 +62,10 @@ class Tuning(C.Structure):
                 ("grid_select", C.c_uint32), ("grid_aggregate", C.c_uint32)]
 
 
+class WavParamsC(C.Structure):
+    _fields_ = [("power", C.c_float), ("smooth", C.c_uint32), ("gate", C.c_float), ("edge", C.c_uint32)]
+
+
 class SynthDesc(C.Structure):
     _fields_ = [("w", C.c_uint32), ("h", C.c_uint32), ("n", C.c_uint32), ("warp", C.c_uint32), ("seed", C.c_uint64),
                 ("mag_step", C.c_float), ("noise_std", C.c_float), ("blur_px", C.c_float), ("warp_scale", C.c_float),
@@ -109,6 +113,7 @@ SIGNATURES = {
     "lsb_unet_forward": (ERR, [P, P, P, C.c_uint32, C.c_uint32, C.c_uint32, P]),
     "lsb_unet_train_step": (ERR, [P, P, P, P, C.c_uint32, C.c_uint32, C.c_uint32, C.c_float, C.POINTER(C.c_double)]),
     "lsb_stack_set_warm_start": (ERR, [P, P]),
+    "lsb_stack_weighted_average": (ERR, [P, C.POINTER(WavParamsC), P]),
     "lsb_batch_run": (ERR, [C.POINTER(P), C.c_uint32, C.POINTER(Result)]),
     "lsb_stack_autotune": (ERR, [P, C.POINTER(Tuning)]),
     "lsb_stack_depth_planes": (ERR, [P, C.POINTER(P), C.POINTER(P), C.POINTER(P), C.POINTER(P), C.POINTER(C.c_uint32),

@@ -169,10 +169,13 @@ struct lsb_stack {
     lsb_result* early = nullptr;   // finish: the result whose fused planes leave on rs while the depth runs
     cudaEvent_t fused_ev = nullptr;  // recorded on s once the fused planes and the winner map are written
     size_t x0_cells = 0;
+    float* wav_w = nullptr;  // the weighted average's weight planes [n][dh][dw]
+    int wav_frames = 0;
     std::vector<cudaEvent_t> chunk_ev;  // per selection chunk folded on ws: [start, after the fused kernel, end] of level 0
     int chunks = 0;                     // chunks the last streamed fold ran
     ~lsb_stack() {
         for (auto& v : chunk_ev) cudaEventDestroy(v);
+        if (wav_w) cudaFree(wav_w);
         wls_destroy(ws);
         if (x0) cudaFree(x0);
         for (auto& v : copied) cudaEventDestroy(v);
@@ -1646,6 +1649,43 @@ extern "C" char* lsb_warp_cost(lsb_engine* e, const float* rf, uint32_t aw, uint
     TRY(cudaMemcpyAsync(a, rf, sizeof(float) * aw * ah, cudaMemcpyHostToDevice, st));
     TRY(cudaMemcpyAsync(b, tgt, sizeof(float) * tw * th, cudaMemcpyHostToDevice, st));
     TRY(cost_single(e->actx, a, (int)aw, (int)ah, b, (int)tw, (int)th, sim8, cost));
+    return nullptr;
+}
+
+// stack.rs:857 `weighted` -> wav.rs:92 `weighted_average` over the frames of the last run
+extern "C" char* lsb_stack_weighted_average(lsb_stack* s, const lsb_wav_params* p, float* out) {
+    if (!s || !p || !out) return dup_err("null argument");
+    if (!s->folded || !s->dp.enabled) return dup_err("the weighted average needs a run with the depth pass (its focus measure and noise floor)");
+    if (!(p->power >= 0.f) || !(p->gate >= 0.f) || p->smooth > 64) return dup_err("wav: power and gate must be >= 0, smooth at most 64");
+    lsb_engine* e = s->e;
+    cudaStream_t st = e->s;
+    const int n = (int)s->count, dw = s->dw, dh = s->dh;
+    const size_t m = (size_t)dw * dh;
+    if (s->wav_frames < n) {
+        if (s->wav_w) cudaFree(s->wav_w);
+        s->wav_w = nullptr;
+        s->wav_frames = 0;
+        TRY(cudaMalloc(&s->wav_w, sizeof(float) * m * n));
+        s->wav_frames = n;
+    }
+    // the guided filter's statistics for radius `smooth` on the depth pass's guide (the fused luma's block mean)
+    const int r = (int)p->smooth;
+    const bool edge = p->edge != 0 && r > 0;
+    if (edge) gf_stats(s->guide, dw, dh, r, s->tmp, s->mi, s->vi, st);
+    WavScratch t{s->w2, s->draw, s->t0, s->t1, s->t2, s->tmp, s->abar, s->bbar};
+    const bool half = s->storage != STORE_F32;
+    for (int k = 0; k < n; k++) {
+        const void* slice = (const char*)s->slices + (size_t)k * m * gs_bytes(s);
+        TRY(wav_weights(slice, half, s->mins, dw, dh, p->gate, p->power, r, edge, s->guide, s->mi, s->vi, s->dp.agg_eps, t,
+                        s->wav_w + (size_t)k * m, st));
+    }
+    bool focus = false;
+    int src = 0;
+    const bool aligned = s->ap.enabled && n > 1 && !s->f32src;
+    FoldArgs a = level_args(s, 0, aligned, false, &focus, &src);
+    TRY(wav_accumulate(a, src, s->wav_w, n, dw, dh, s->bk, s->img_tmp, st));
+    TRY(cudaMemcpyAsync(out, s->img_tmp, sizeof(float) * 3 * (size_t)s->w * s->h, cudaMemcpyDeviceToHost, st));
+    TRY(cudaStreamSynchronize(st));
     return nullptr;
 }
 

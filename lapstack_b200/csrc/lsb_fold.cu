@@ -159,6 +159,41 @@ static cudaError_t pick_src(const FoldArgs& a, int src_kind, int r, bool focus, 
     }
 }
 
+// wav.rs:146-161 the weighted average's accumulation over the frames as folded (level 0's source and
+// gains): per pixel, frame by frame in order, w = the frame's weight plane taken bilinearly to the pixel
+// (depth.rs:201 upsample_bilinear), acc += w * v per channel, wsum += w; then acc / wsum clamped to [0, 1].
+template <int SRC>
+__global__ void wav_accumulate_kernel(const FoldArgs a, const float* __restrict__ wts, int n, int dw, int dh, int k,
+                                      float* __restrict__ out) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
+    if (x >= a.W || y >= a.H) return;
+    const float inv = __fdiv_rn(1.f, (float)k);
+    int x0, x1, y0, y1;
+    float tx, ty;
+    bil_axis(x, inv, dw, x0, x1, tx);
+    bil_axis(y, inv, dh, y0, y1, ty);
+    const size_t m = (size_t)dw * dh, np = (size_t)a.W * a.H, o = (size_t)y * a.W + x;
+    float acc[3] = {0.f, 0.f, 0.f}, ws = 0.f;
+    for (int f = 0; f < n; f++) {
+        const float wv = bil(wts + (size_t)f * m, dw, x0, x1, y0, y1, tx, ty);
+        float v[3];
+        level_px<SRC, float>(a, f, x, y, v);
+#pragma unroll
+        for (int c = 0; c < 3; c++) acc[c] = __fadd_rn(acc[c], __fmul_rn(wv, v[c]));
+        ws = __fadd_rn(ws, wv);
+    }
+#pragma unroll
+    for (int c = 0; c < 3; c++) out[c * np + o] = fminf(fmaxf(__fdiv_rn(acc[c], ws), 0.f), 1.f);
+}
+
+cudaError_t wav_accumulate(const FoldArgs& a, int src_kind, const float* wts, int n, int dw, int dh, int k, float* out, cudaStream_t s) {
+    dim3 b(32, 8), g((a.W + 31) / 32, (a.H + 7) / 8);
+    if (src_kind == SRC_F32) lsb_launched(), wav_accumulate_kernel<SRC_F32><<<g, b, 0, s>>>(a, wts, n, dw, dh, k, out);
+    else if (src_kind == SRC_U16) lsb_launched(), wav_accumulate_kernel<SRC_U16><<<g, b, 0, s>>>(a, wts, n, dw, dh, k, out);
+    else return cudaErrorInvalidValue;
+    return cudaGetLastError();
+}
+
 cudaError_t fold_level(const FoldArgs& a0, int src_kind, int storage, int radius, bool focus, cudaStream_t s, int grid_limit) {
     FoldArgs a = a0;  // the select kernel's tiling
     a.tiles_x = (a.W + TW - 1) / TW;

@@ -84,6 +84,9 @@ enum Storage { STORE_F32 = 0, STORE_UNORM16 = 1, STORE_F16 = 2 };
 
 // Launchers (lsb_fold.cu).
 cudaError_t fold_level(const FoldArgs& a, int src_kind, int storage, int radius, bool focus, cudaStream_t s, int grid_limit);
+// The weighted average's accumulation (wav.rs:146-161): frames as level 0 of `a` reads them, weight planes
+// wts [n][dh][dw] (grid scale k), out [3][H][W].
+cudaError_t wav_accumulate(const FoldArgs& a, int src_kind, const float* wts, int n, int dw, int dh, int k, float* out, cudaStream_t s);
 // Every frame through its warp (the pixel as shot where it leaves the frame):
 // f32 planar [n][3][h][w], or u16 interleaved [n][h][w][3] rounded to the u16 step.
 cudaError_t warp_frames(const uint16_t* frames, const FrameXform* xf, int interp, int w, int h, int n, bool u16_out, void* out,

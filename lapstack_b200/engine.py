@@ -20,7 +20,7 @@ from dataclasses import dataclass, field
 
 import numpy as np
 
-from ._lib import (AlignParamsC, Config, DepthParamsC, FuseParamsC, LOG_FN, LsbError, Result, SynthDesc, check, load)
+from ._lib import (AlignParamsC, Config, DepthParamsC, FuseParamsC, LOG_FN, LsbError, Result, SynthDesc, WavParamsC, check, load)
 
 TOP_RULES = {"de": 0, "dev": 1, "avg": 2}
 INTERPS = ["nearest", "bilinear", "bicubic", "spline4x4", "spline6x6", "lanczos3"]
@@ -115,6 +115,17 @@ class DepthParams:  # depth.rs:69-109
                             self.sml_step, self.agg_radius, self.agg_eps, self.lam, self.sigma_c, self.cg_iters,
                             int(self.median), _pick(self.upsample, UPSAMPLE, "upsampling"), self.up_radius, self.up_eps,
                             self.gate, self.robust, self.edge_mode, self.vcycle_mode)
+
+
+@dataclass
+class WavParams:  # wav.rs:52-80
+    power: float = 2.0
+    smooth: int = 3
+    gate: float = 0.5
+    edge: bool = True
+
+    def c(self):
+        return WavParamsC(self.power, self.smooth, self.gate, int(self.edge))
 
 
 @dataclass
@@ -316,6 +327,14 @@ class Stack:
         check(self._L.lsb_stack_push_f32(self._h, arr))
 
     push = push_f32
+
+    def weighted_average(self, wav: WavParams | None = None) -> np.ndarray:
+        """stack.rs:857 / wav.rs:92 the weighted average of the frames of the last finish (or run), with
+        its depth pass's noise floor: (3, h, w) float32 in [0, 1]."""
+        out = np.empty((3, self.h, self.w), np.float32)
+        p = (wav or WavParams()).c()
+        check(self._L.lsb_stack_weighted_average(self._h, C.byref(p), C.c_void_p(out.ctypes.data)))
+        return out
 
     def set_warm_start(self, net):
         """Start this stack's WLS solves from the U-Net's prediction (None: the reference's FGS start)."""

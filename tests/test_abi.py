@@ -93,7 +93,7 @@ def test_ctypes_structs_have_the_header_layout(tmp_path):
         pytest.skip("no gcc")
     structs = {"lsb_config": _lib.Config, "lsb_fuse_params": _lib.FuseParamsC, "lsb_align_params": _lib.AlignParamsC,
                "lsb_depth_params": _lib.DepthParamsC, "lsb_result": _lib.Result, "lsb_tuning": _lib.Tuning,
-               "lsb_synth_desc": _lib.SynthDesc}
+               "lsb_synth_desc": _lib.SynthDesc, "lsb_wav_params": _lib.WavParamsC}
     rename = {"lam": "lambda"}
     body, want = [], []
     for cname, cls in structs.items():

@@ -209,3 +209,40 @@ def test_sml_focus_measure_matches_oracle(step):
     filter: the focus slices bit-exact (so the noise floor cells are), the depth within 1e-3."""
     fr = synth(256, 192, 6, seed=75)
     check_stack(fr, L.FuseParams(), None, L.DepthParams(focus="sml", sml_step=step))
+
+
+# ------------------------------------------------------ the weighted average
+@pytest.mark.parametrize("aligned,storage,wav", [(False, "f32", dict()), (False, "f32", dict(edge=False)),
+                                                  (False, "f32", dict(smooth=0, power=1.0)), (True, "f32", dict()),
+                                                  (True, "unorm16", dict())])
+def test_weighted_average_matches_oracle(aligned, storage, wav):
+    """stack.rs:857 / wav.rs:92 over the frames as folded, with the depth pass's floor cells and the fused
+    luma as guide. The weights go through powf (the platform's in the oracle, CUDA's on the device) and
+    f64 box sums, so the image is held to 2e-6 of full scale (about 1/8 of a 16-bit step) and its u16
+    rounding to 1 step; with 16-bit storage the oracle emulates the storage."""
+    if aligned:
+        fr = synth(320, 240, 4, warp=True, mag_step=0.0, seed=17)
+        al = L.AlignParams(coarsen=1)
+    else:
+        fr = synth(256, 192, 8, seed=9)
+        al = None
+    fuse, dp, wp = L.FuseParams(), L.DepthParams(), L.WavParams(**wav)
+    sp = oracle_params(fuse, al, dp)
+    sp.wav = O.WavParams(**wav)
+    sp.storage = storage
+    ref = O.run_stack(fr, sp)
+    n, h, w, _ = fr.shape
+    eng = L.Engine(storage=storage)
+    st = eng.stack(w, h, n, fuse, al, dp)
+    for f in fr:
+        st.push_u16(f)
+    out = st.finish()
+    got = st.weighted_average(wp)
+    d = np.abs(got.astype(np.float64) - ref.wav)
+    print(f"weighted average vs oracle: max {d.max():.3e}, mean {d.mean():.3e}")
+    assert d.max() <= 2e-6, d.max()
+    # the stack's own results are untouched by it
+    again = st.finish()
+    assert np.array_equal(again.image_u16, out.image_u16) and np.array_equal(again.depth.depth, out.depth.depth)
+    # and it is not the fused image: no pixel is picked outright
+    assert np.mean(np.abs(got - out.image)) > 1e-4
