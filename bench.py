@@ -379,7 +379,7 @@ def main():
     ap.add_argument("--no-wls-report", action="store_true")
     ap.add_argument("--no-autotune", action="store_true")
     ap.add_argument("--two-kernel-fold0", action="store_true", help="fold level 0 with the separate REDUCE and select kernels")
-    ap.add_argument("--fold-after-chain", action="store_true", help="fold device-resident frames after the registration chain")
+    ap.add_argument("--fold-beside-chain", action="store_true", help="fold device-resident frames beside the registration chain")
     args = ap.parse_args()
     c = dict(CONFIGS[args.config])
     if args.storage:
@@ -407,7 +407,7 @@ def main():
         return max_over_ranks(x, dist, "cuda")
 
     eng = L.Engine(device=local, storage=c["storage"], fused_fold0=not args.two_kernel_fold0,
-                   fold_beside_chain=not args.fold_after_chain)
+                   fold_beside_chain=args.fold_beside_chain)
     fuse, align, depth = params_of(c, L)
     W, H, N = c["w"], c["h"], c["n"]
     st = eng.stack(W, H, N, fuse, align, depth)

@@ -46,9 +46,9 @@ extern "C" {
 /* lsb_config.flags: fold level 0 with the REDUCE and select kernels on every tile instead of the
    fused level-0 kernel on the interior tiles (the same results; for cross-checks and timing) */
 #define LSB_FLAG_TWO_KERNEL_FOLD0 1
-/* lsb_config.flags: with frames already in device memory, fold the stack after its registration chain
-   instead of chunk by chunk beside it (the same results; for timing) */
-#define LSB_FLAG_FOLD_AFTER_CHAIN 2
+/* lsb_config.flags: with frames already in device memory, fold an aligned stack chunk by chunk beside
+   its registration chain instead of after it (the same results; pushed frames always fold beside it) */
+#define LSB_FLAG_FOLD_BESIDE_CHAIN 2
 
 typedef struct lsb_engine lsb_engine;
 typedef struct lsb_stack lsb_stack;

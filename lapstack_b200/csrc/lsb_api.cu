@@ -999,9 +999,11 @@ static char* run_pipeline_once(lsb_stack* s) {
     }
     TRY(cudaEventRecord(ev[1], st));
     const bool streamed = aligned && chained(s);
-    // the fold too, chunk by chunk beside the chain (not with halo control; frames in device memory
-    // unless LSB_FLAG_FOLD_AFTER_CHAIN asks for the fold after the chain)
-    const bool sel_streamed = streamed && !(s->fp.halo > 0.f) && (pushed || !(e->cfg.flags & LSB_FLAG_FOLD_AFTER_CHAIN));
+    // the fold too, chunk by chunk beside the chain, for pushed frames (not with halo control): the GPU
+    // waits on the host copies anyway. Frames already in device memory fold after the chain unless
+    // LSB_FLAG_FOLD_BESIDE_CHAIN asks otherwise: beside it (one fold CTA per SM) the fold ran at half its
+    // speed and the chain slowed, 572 ms against 530 ms for the C3 step.
+    const bool sel_streamed = streamed && !(s->fp.halo > 0.f) && (pushed || (e->cfg.flags & LSB_FLAG_FOLD_BESIDE_CHAIN));
     s->chunks = 0;
     if (streamed) {
         char* err = stream_warps(s, pushed, pushed || sel_streamed, sel_streamed);
