@@ -14,9 +14,10 @@
 //      depth.rs:1097 / :417 / :174),
 //   4. REDUCEs the window to G_1 over what EXPAND needs (pyramid.rs:86) and
 //      writes the tile's own G_1 in the storage type,
-//   5. EXPANDs back, forms L = G - EXPAND(G_1 as stored) in place of G, the
-//      luma energy (fuse.rs:152), its binomial window (fuse.rs:168), and keeps
-//      the strict-> selection (fuse.rs:429) in registers.
+//   5. EXPANDs back, forms L = G - EXPAND(G_1 as stored) in place of G and the
+//      luma energy (fuse.rs:152); each thread takes the binomial window
+//      (fuse.rs:168) of the pixels it owns and keeps their strict-> selection
+//      (fuse.rs:429) in registers.
 // The arithmetic is the reference's, op for op and in its order (round-to-
 // nearest f32 adds and multiplies, never contracted); pairs of independent
 // results (two rows, or two neighbouring pixels) go through one packed
@@ -134,12 +135,11 @@ constexpr int OFF_RAW = 192;
 constexpr int OFF_G0 = OFF_RAW + WH * RAW_ROW;                 // [3][WH][WW] f32: G, then L
 constexpr int OFF_LY = OFF_G0 + 3 * WH * WW * 4;               // [LYH][LYW] luma and [LYH][LYW] luma shifted by one
 constexpr int OFF_YB = OFF_LY;                                 // [YBH][YBW] energies  (after the filter)
-constexpr int OFF_EH = OFF_YB + YBH * YBW * 4;                 // [YBH][TW0] their row sums
 constexpr int OFF_TMP = OFF_LY + 2 * LYH * LYW * 4;            // [3][WH][36] REDUCE rows; then [3][G1H][EXW] EXPAND rows
 constexpr int TMPW = 36;
 constexpr int OFF_G1 = OFF_TMP + 3 * WH * TMPW * 4;            // [3][G1H][G1W] G_1 as stored
 constexpr int SMEM = OFF_G1 + 3 * G1H * G1W * 4;
-static_assert(OFF_EH + YBH * TW0 * 4 <= OFF_TMP, "energies and their row sums fit the luma planes");
+static_assert(OFF_YB + YBH * YBW * 4 <= OFF_TMP, "the energies fit the luma planes");
 static_assert(3 * G1H * EXW <= 3 * WH * TMPW, "the EXPAND rows fit the REDUCE rows' space");
 static_assert(OFF_RAW % 16 == 0 && RAW_ROW % 16 == 0, "bulk copy destinations are 16-byte aligned");
 static_assert(SMEM <= 113 * 1024, "two CTAs per SM");
@@ -233,27 +233,39 @@ __device__ __forceinline__ void f0_focus(const FoldArgs& a, const float* __restr
 }
 
 // ---- phase 3: REDUCE along rows (pyramid.rs:90) of every window row, at the G_1 columns
-// x0/2 - 2 + a, a < 36: tmp[c][r][a]. Two rows per thread as lanes, four outputs from 11 loads.
+// x0/2 - 2 + a, a < 36: tmp[c][r][a]. Two rows per thread as lanes; the lanes of a warp take consecutive
+// outputs, so their taps (window columns 2a .. 2a + 4, read as two 8-byte pairs and one word) are
+// contiguous in shared memory.
 template <int R>
 __device__ __forceinline__ void f0_reduce_rows(const float* __restrict__ G, float* __restrict__ tmp) {
     using namespace f0;
-    constexpr int GROUPS = TMPW / 4, ITEMS = (WH / 2) * GROUPS;
+    constexpr int ITEMS = 3 * (WH / 2) * TMPW;
     for (int it = threadIdx.x; it < ITEMS; it += NT0) {
-        const int rp = it / GROUPS, g = it - rp * GROUPS;
-        const int r0 = 2 * rp, a0 = 4 * g, cs = 2 * a0 + (R & 1);
-#pragma unroll
-        for (int c = 0; c < 3; c++) {
-            const float* p0 = G + (c * WH + r0) * WW + cs;
-            float2 v[11];
-#pragma unroll
-            for (int t = 0; t < 11; t++) v[t] = make_float2(p0[t], p0[WW + t]);
-#pragma unroll
-            for (int i = 0; i < 4; i++) {
-                const float2 o = tap5x2(v[2 * i], v[2 * i + 1], v[2 * i + 2], v[2 * i + 3], v[2 * i + 4]);
-                tmp[(c * WH + r0) * TMPW + a0 + i] = o.x;
-                tmp[(c * WH + r0 + 1) * TMPW + a0 + i] = o.y;
-            }
+        const int c = it / ((WH / 2) * TMPW), rem = it - c * ((WH / 2) * TMPW);
+        const int rp = rem / TMPW, a = rem - rp * TMPW;
+        const int r0 = 2 * rp;
+        const float* p0 = G + (c * WH + r0) * WW + 2 * a + (R & 1);
+        float2 v[5];
+        if (R & 1) {  // odd columns: one word, then two pairs
+            v[0] = make_float2(p0[0], p0[WW]);
+            const float2 a1 = *(const float2*)(p0 + 1), b1 = *(const float2*)(p0 + WW + 1);
+            const float2 a3 = *(const float2*)(p0 + 3), b3 = *(const float2*)(p0 + WW + 3);
+            v[1] = make_float2(a1.x, b1.x);
+            v[2] = make_float2(a1.y, b1.y);
+            v[3] = make_float2(a3.x, b3.x);
+            v[4] = make_float2(a3.y, b3.y);
+        } else {  // even columns: two pairs, then one word
+            const float2 a0 = *(const float2*)(p0), b0 = *(const float2*)(p0 + WW);
+            const float2 a2 = *(const float2*)(p0 + 2), b2 = *(const float2*)(p0 + WW + 2);
+            v[0] = make_float2(a0.x, b0.x);
+            v[1] = make_float2(a0.y, b0.y);
+            v[2] = make_float2(a2.x, b2.x);
+            v[3] = make_float2(a2.y, b2.y);
+            v[4] = make_float2(p0[4], p0[WW + 4]);
         }
+        const float2 o = tap5x2(v[0], v[1], v[2], v[3], v[4]);
+        tmp[(c * WH + r0) * TMPW + a] = o.x;
+        tmp[(c * WH + r0 + 1) * TMPW + a] = o.y;
     }
 }
 
@@ -290,24 +302,27 @@ __device__ __forceinline__ void f0_reduce_cols(const FoldArgs& a, const float* _
 }
 
 // ---- phase 5: EXPAND along rows (pyramid.rs:147) of G_1 as stored: exph[c][b][x'] at level-0
-// columns x0 - R + x', x' < 64 + 2R. Two G_1 rows per thread as lanes, eight outputs from six loads.
+// columns x0 - R + x', x' < 64 + 2R. Two G_1 rows per thread as lanes, eight outputs from eight loads;
+// the last column group also takes the 2R columns past 64, so that the 240 items take one round.
 template <int R>
 __device__ __forceinline__ void f0_expand_rows(const float* __restrict__ G1s, float* __restrict__ exph) {
     using namespace f0;
-    constexpr int EW = TW0 + 2 * R, NG = (EW + 7) / 8, ITEMS = 3 * (G1H / 2) * NG;
+    constexpr int NG = TW0 / 8, ITEMS = 3 * (G1H / 2) * NG;
     constexpr int A0 = R == 2 ? 0 : 1;  // the group's first G_1 column, less 4g
     for (int it = threadIdx.x; it < ITEMS; it += NT0) {
         const int c = it / ((G1H / 2) * NG), rem = it - c * ((G1H / 2) * NG);
         const int bp = rem / NG, g = rem - bp * NG;
         const int b0 = 2 * bp;
         const float* src = G1s + (c * G1H + b0) * G1W + 4 * g + A0;
-        float2 u[6];
+        float2 u[8];
 #pragma unroll
-        for (int t = 0; t < 6; t++) u[t] = make_float2(src[t], src[G1W + t]);
+        for (int t = 0; t < 8; t++) u[t] = make_float2(src[t], src[G1W + t]);
         float* d0 = exph + (c * G1H + b0) * EXW + 8 * g;
+        const int ni = g == NG - 1 ? 8 + 2 * R : 8;
 #pragma unroll
-        for (int i = 0; i < 8; i++) {
-            const int m = i - R;                   // x - x0 + ... : its parity is x's
+        for (int i = 0; i < 8 + 2 * R; i++) {
+            if (i >= ni) break;
+            const int m = i - R;                   // its parity is that of the level-0 column
             const int j = ((m >> 1) + 2) - A0;     // the G_1 column of x >> 1 within u
             const float2 o = (m & 1) == 0 ? exp_even2(u[j - 1], u[j], u[j + 1]) : exp_odd2(u[j], u[j + 1]);
             d0[i] = o.x;
@@ -349,43 +364,38 @@ __device__ __forceinline__ void f0_laplace(const float* __restrict__ exph, float
     }
 }
 
-// ---- phase 7: the binomial window (fuse.rs:168) along rows: eh[r][xo] = sum_q binw(q) yb[r][xo + q],
-// in order. Two rows per thread as lanes, four outputs from 4 + 2R loads.
+// ---- phase 7: the binomial window (fuse.rs:168) and the strict-> selection (fuse.rs:429): thread
+// (tx, ty) owns the pixel pairs (x0 + 2tx, +1) of rows y0 + 4ty .. +3. It forms the row sums of the
+// 4 + 2R energy rows it needs itself (sum_q binw(q) yb[r][x' + q], in order), then the column sums, and
+// reads the winning coefficients from L only when a frame wins. R = 0: the node energy itself.
 template <int R>
-__device__ __forceinline__ void f0_window_rows(const float* __restrict__ yb, float* __restrict__ eh) {
-    using namespace f0;
-    constexpr int EH = TH0 + 2 * R, GR = TW0 / 4, ITEMS = (EH / 2) * GR, NV = 4 + 2 * R;
-    for (int it = threadIdx.x; it < ITEMS; it += NT0) {
-        const int rp = it / GR, g = it - rp * GR;
-        const int r0 = 2 * rp, xo0 = 4 * g;
-        const float* src = yb + r0 * YBW + xo0;
-        float2 v[NV];
-#pragma unroll
-        for (int t = 0; t < NV; t++) v[t] = make_float2(src[t], src[YBW + t]);
-#pragma unroll
-        for (int i = 0; i < 4; i++) {
-            float2 s = mul2(splat(binw<R>(0)), v[i]);
-#pragma unroll
-            for (int q = 1; q <= 2 * R; q++) s = binw_exact<R>(q) ? add2(s, mul2(splat(binw<R>(q)), v[i + q]))
-                                                                : addl(s, mul2(splat(binw<R>(q)), v[i + q]));
-            eh[r0 * TW0 + xo0 + i] = s.x;
-            eh[(r0 + 1) * TW0 + xo0 + i] = s.y;
-        }
-    }
-}
-
-// ---- phase 8: the binomial window along columns and the strict-> selection (fuse.rs:429): thread
-// (tx, ty) owns the pixel pairs (x0 + 2tx, +1) of rows y0 + 4ty .. +3; the winning coefficients are
-// read from L only when a frame wins. R = 0: the node energy itself.
-template <int R>
-__device__ __forceinline__ void f0_select(const float* __restrict__ en, const float* __restrict__ G, int k, float (&best)[8],
+__device__ __forceinline__ void f0_select(const float* __restrict__ yb, const float* __restrict__ G, int k, float (&best)[8],
                                           float (&acc)[8][3], int (&win)[8]) {
     using namespace f0;
-    constexpr int NV = 4 + 2 * R, STRIDE = R > 0 ? TW0 : YBW;
+    constexpr int NV = 4 + 2 * R;
     const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5, px = 2 * tx;
     float2 v[NV];
 #pragma unroll
-    for (int t = 0; t < NV; t++) v[t] = *(const float2*)(en + (4 * ty + t) * STRIDE + px);
+    for (int t = 0; t < NV; t++) {
+        const float* row = yb + (4 * ty + t) * YBW + px;
+        if (R == 0) {
+            v[t] = *(const float2*)row;
+        } else {
+            float y[2 + 2 * R];
+#pragma unroll
+            for (int q = 0; q < 2 + 2 * R; q += 2) {
+                const float2 p2 = *(const float2*)(row + q);
+                y[q] = p2.x;
+                y[q + 1] = p2.y;
+            }
+            float2 h = mul2(splat(binw<R>(0)), make_float2(y[0], y[1]));
+#pragma unroll
+            for (int q = 1; q <= 2 * R; q++)
+                h = binw_exact<R>(q) ? add2(h, mul2(splat(binw<R>(q)), make_float2(y[q], y[q + 1])))
+                                     : addl(h, mul2(splat(binw<R>(q)), make_float2(y[q], y[q + 1])));
+            v[t] = h;
+        }
+    }
 #pragma unroll
     for (int j = 0; j < 4; j++) {
         float2 e = v[j];
@@ -464,7 +474,6 @@ __global__ void __launch_bounds__(f0::NT0, 2) fold0_kernel(const FoldArgs a) {
     float* Ly = (float*)(smem + OFF_LY);
     float* Ls = Ly + LYH * LYW;
     float* yb = (float*)(smem + OFF_YB);
-    float* eh = (float*)(smem + OFF_EH);
     float* tmp = (float*)(smem + OFF_TMP);
     float* G1s = (float*)(smem + OFF_G1);
     const int W = a.W, H = a.H;
@@ -526,11 +535,7 @@ __global__ void __launch_bounds__(f0::NT0, 2) fold0_kernel(const FoldArgs a) {
             __syncthreads();
             f0_laplace<R>(tmp, G, yb, a.use_chroma);
             __syncthreads();
-            if (R > 0) {
-                f0_window_rows<R>(yb, eh);
-                __syncthreads();
-            }
-            f0_select<R>(R > 0 ? eh : yb, G, k, best, acc, win);
+            f0_select<R>(yb, G, k, best, acc, win);
             __syncthreads();  // the next frame's conversion overwrites G and the luma planes
         }
 #pragma unroll
