@@ -199,6 +199,25 @@ char* lsb_stack_finish(lsb_stack* s, lsb_result* out);
    pass's per-cell noise floor; out receives 3*w*h planar f32 in [0,1] (host pointer). Needs a run
    with the depth pass. The stack's fold and depth results stay as they were. */
 char* lsb_stack_weighted_average(lsb_stack* s, const lsb_wav_params* p, float* out);
+/* stack.rs:76 `slab_ranges`: the slabs of a count-frame stack, size frames each (clamped to
+   [1, count]), consecutive slabs overlapping by overlap (at most size - 1), the last cut short at the
+   last frame. Writes the first max_slabs (lo, hi) pairs (inclusive frame indices) into lohi (may be
+   NULL) and returns how many slabs there are (0 for an empty stack). Needs no device. */
+uint32_t lsb_slab_ranges(uint32_t count, uint32_t size, uint32_t overlap, uint32_t* lohi, uint32_t max_slabs);
+/* stack.rs:740 `fuse_range` with stack.rs:872 `fuse_slabs`'s cut and resize: frames lo..hi (inclusive)
+   of the last finish (or run), as folded (aligned, gains applied), fused on their own with the stack's
+   fusion settings, as a fresh fuser of those frames would fuse them; the stack's own results stay as
+   they were. rect = {x, y, w, h} (NULL: the whole frame) cuts the fused image (pyramid.rs:31
+   Img3::crop); out_w x out_h (both 0: rect's size) resamples the cut through prep.rs:46 `resize` with
+   interpolation `interp` (align.rs:148 code; stack.rs:889 uses 3, Spline4x4). out receives
+   3*ow*oh planar f32 (host pointer). */
+char* lsb_stack_fuse_range(lsb_stack* s, uint32_t lo, uint32_t hi, const uint32_t* rect, uint32_t out_w, uint32_t out_h,
+                           uint32_t interp, float* out);
+/* prep.rs:46 `resize` / :63 `resize_plane` (stack.rs:951 `restretched`): `planes` host planes of
+   pw x ph resampled to w x h through the scaling warp with pixel centres kept (output pixel o reads
+   source (o + 1/2) / k - 1/2 on each axis), taps clamped at the edge; equal sizes copy. */
+char* lsb_resize(lsb_engine* e, const float* src, uint32_t planes, uint32_t pw, uint32_t ph, uint32_t w, uint32_t h, uint32_t interp,
+                 float* out);
 /* lsb_stack_finish without copying results back (device-resident benchmarking; no counterpart). */
 char* lsb_stack_run(lsb_stack* s, double* ms_out12);
 /* Explicit frees, as ffi.rs:129 lapstack_raw_free_image. */

@@ -114,6 +114,9 @@ SIGNATURES = {
     "lsb_unet_train_step": (ERR, [P, P, P, P, C.c_uint32, C.c_uint32, C.c_uint32, C.c_float, C.POINTER(C.c_double)]),
     "lsb_stack_set_warm_start": (ERR, [P, P]),
     "lsb_stack_weighted_average": (ERR, [P, C.POINTER(WavParamsC), P]),
+    "lsb_slab_ranges": (C.c_uint32, [C.c_uint32, C.c_uint32, C.c_uint32, P, C.c_uint32]),
+    "lsb_stack_fuse_range": (ERR, [P, C.c_uint32, C.c_uint32, P, C.c_uint32, C.c_uint32, C.c_uint32, P]),
+    "lsb_resize": (ERR, [P, P, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, P]),
     "lsb_batch_run": (ERR, [C.POINTER(P), C.c_uint32, C.POINTER(Result)]),
     "lsb_stack_autotune": (ERR, [P, C.POINTER(Tuning)]),
     "lsb_stack_depth_planes": (ERR, [P, C.POINTER(P), C.POINTER(P), C.POINTER(P), C.POINTER(P), C.POINTER(C.c_uint32),

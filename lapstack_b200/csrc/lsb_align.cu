@@ -172,9 +172,10 @@ __global__ void cost_final_kernel(const double* __restrict__ part, int nblocks, 
 }
 
 // align.rs:489 `warp_with` on an f32 plane (edge-clamped; no fallback), the
-// interpolation weights as in the fold's level-0 warp.
-__device__ __forceinline__ float warp_plane_px(const float* __restrict__ src, int w, int h, const double* inv, bool affine, int interp,
-                                               int x, int y) {
+// interpolation weights as in the fold's level-0 warp. The plane is w x h
+// with rows `stride` floats apart.
+__device__ __forceinline__ float warp_window_px(const float* __restrict__ src, size_t stride, int w, int h, const double* inv, bool affine,
+                                                int interp, int x, int y) {
     double sx, sy;
     src_point(inv, affine, (double)x, (double)y, sx, sy);
     const double fx = floor(sx), fy = floor(sy);
@@ -185,12 +186,28 @@ __device__ __forceinline__ float warp_plane_px(const float* __restrict__ src, in
     const int start = 1 - n / 2;
     float acc = 0.f;
     for (int j = 0; j < n; j++) {
-        const float* row = src + (size_t)min(max(y0 + start + j, 0), h - 1) * w;
+        const float* row = src + (size_t)min(max(y0 + start + j, 0), h - 1) * stride;
         float r = 0.f;
         for (int i = 0; i < n; i++) r = __fadd_rn(r, __fmul_rn(wx[i], row[min(max(x0 + start + i, 0), w - 1)]));
         acc = __fadd_rn(acc, __fmul_rn(wy[j], r));
     }
     return acc;
+}
+__device__ __forceinline__ float warp_plane_px(const float* __restrict__ src, int w, int h, const double* inv, bool affine, int interp,
+                                               int x, int y) {
+    return warp_window_px(src, (size_t)w, w, h, inv, affine, interp, x, y);
+}
+// prep.rs:46 `resize` / :63 `resize_plane` of a window (x0, y0, sw x sh) of planes `stride` floats
+// wide, `pstride` floats apart: align.rs:542 `warp_plane` of the window through the scaling Sim the
+// host turned into `inv`, onto ow x oh (blockIdx.z the plane). Without `inv` (the sizes agree) the
+// window is copied, as the reference returns the plane unchanged.
+__global__ void resize_kernel(const float* __restrict__ src, size_t stride, size_t pstride, int x0, int y0, int sw, int sh,
+                              const WarpXform xf, int scaled, int ow, int oh, float* __restrict__ out) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
+    if (x >= ow || y >= oh) return;
+    const float* p = src + (size_t)blockIdx.z * pstride + (size_t)y0 * stride + x0;
+    out[(size_t)blockIdx.z * ow * oh + (size_t)y * ow + x] =
+        scaled ? warp_window_px(p, stride, sw, sh, xf.inv, xf.affine, xf.interp, x, y) : p[(size_t)y * stride + x];
 }
 // align.rs:542 `warp_plane`, one thread per output pixel.
 __global__ void warp_plane_kernel(const float* __restrict__ src, int w, int h, const WarpXform xf, float* __restrict__ out) {
@@ -353,6 +370,27 @@ cudaError_t gauss_levels(const float* y, int w, int h, const std::vector<float*>
 cudaError_t warp_plane(const float* src, int w, int h, const WarpXform& xf, float* out, cudaStream_t s) {
     dim3 b(32, 8), g((w + 31) / 32, (h + 7) / 8);
     lsb_launched(), warp_plane_kernel<<<g, b, 0, s>>>(src, w, h, xf, out);
+    return cudaGetLastError();
+}
+
+// prep.rs:63 `resize_plane`: the Sim that maps the sw x sh source onto ow x oh with pixel centres
+// corresponding (output pixel o reads source (o + 1/2) / k - 1/2, k = ow / sw on each axis).
+cudaError_t resize_planes(const float* src, size_t stride, size_t pstride, int planes, int x0, int y0, int sw, int sh, int ow, int oh,
+                          int interp, float* out, cudaStream_t s) {
+    if (planes <= 0 || ow <= 0 || oh <= 0) return cudaSuccess;
+    WarpXform xf{};
+    xf.interp = interp;
+    const bool scaled = sw != ow || sh != oh;
+    if (scaled) {
+        const double fw = (double)sw, fh = (double)sh, kx = (double)ow / fw, ky = (double)oh / fh;
+        const double v[8] = {(kx - 1.0) * (fw + 1.0) / (2.0 * fw), (ky - 1.0) * (fh + 1.0) / (2.0 * fh), kx, 0.0, ky / kx, 0.0, 0.0, 0.0};
+        double m[9];
+        sim_matrix(v, sw, sh, m);
+        mat_inverse(m, xf.inv);
+        xf.affine = xf.inv[6] == 0.0 && xf.inv[7] == 0.0 && xf.inv[8] == 1.0;
+    }
+    dim3 b(32, 8), g((ow + 31) / 32, (oh + 7) / 8, planes);
+    lsb_launched(), resize_kernel<<<g, b, 0, s>>>(src, stride, pstride, x0, y0, sw, sh, xf, scaled ? 1 : 0, ow, oh, out);
     return cudaGetLastError();
 }
 

@@ -42,6 +42,10 @@ cudaError_t luma_u16(const uint16_t* f, int w, int h, float* y, cudaStream_t s);
 void gauss_dims(int w, int h, std::vector<std::pair<int, int>>& dims);
 cudaError_t gauss_levels(const float* y, int w, int h, const std::vector<float*>& lv, cudaStream_t s);
 cudaError_t warp_plane(const float* src, int w, int h, const WarpXform& xf, float* out, cudaStream_t s);
+// prep.rs:46 `resize` / :63 `resize_plane` of the window (x0, y0, sw x sh) of `planes` planes (rows `stride`
+// floats, planes `pstride` floats apart) onto ow x oh planar out; a copy of the window when the sizes agree.
+cudaError_t resize_planes(const float* src, size_t stride, size_t pstride, int planes, int x0, int y0, int sw, int sh, int ow, int oh,
+                          int interp, float* out, cudaStream_t s);
 cudaError_t bright_sums(const uint16_t* frames, int n, int w, int h, const BrightXform* xf_dev, int interp, int nparts, double* part,
                         cudaStream_t s);
 // The same for frame k alone (k >= 1) on `blocks` blocks: its partials land where bright_sums puts them.

@@ -173,7 +173,13 @@ struct lsb_stack {
     int wav_frames = 0;
     std::vector<cudaEvent_t> chunk_ev;  // per selection chunk folded on ws: [start, after the fused kernel, end] of level 0
     int chunks = 0;                     // chunks the last streamed fold ran
+    // a frame range fused on its own (stack.rs:740 `fuse_range`): its accumulators, residual and image, made
+    // on first use so that the stack's own fold results stay as they were; its cut and resized output
+    std::vector<float*> slab_acc, slab_best;
+    float *slab_top = nullptr, *slab_img = nullptr, *slab_out = nullptr;
+    size_t slab_out_floats = 0;
     ~lsb_stack() {
+        if (slab_out) cudaFree(slab_out);
         for (auto& v : chunk_ev) cudaEventDestroy(v);
         if (wav_w) cudaFree(wav_w);
         wls_destroy(ws);
@@ -1688,6 +1694,160 @@ extern "C" char* lsb_stack_weighted_average(lsb_stack* s, const lsb_wav_params* 
     TRY(wav_accumulate(a, src, s->wav_w, n, dw, dh, s->bk, s->img_tmp, st));
     TRY(cudaMemcpyAsync(out, s->img_tmp, sizeof(float) * 3 * (size_t)s->w * s->h, cudaMemcpyDeviceToHost, st));
     TRY(cudaStreamSynchronize(st));
+    return nullptr;
+}
+
+// stack.rs:76 `slab_ranges`
+extern "C" uint32_t lsb_slab_ranges(uint32_t count, uint32_t size, uint32_t overlap, uint32_t* lohi, uint32_t max_slabs) {
+    if (count == 0) return 0;
+    size = std::min(std::max(size, 1u), count);
+    overlap = std::min(overlap, size - 1);
+    uint32_t k = 0, lo = 0;
+    for (;;) {
+        const uint32_t hi = std::min(lo + size - 1, count - 1);
+        if (lohi && k < max_slabs) {
+            lohi[2 * k] = lo;
+            lohi[2 * k + 1] = hi;
+        }
+        k++;
+        if (hi + 1 >= count) return k;
+        lo = hi + 1 - overlap;
+    }
+}
+
+// stack.rs:740 `fuse_range` over frames lo..hi of the last run, as a fuser of their own would fold them:
+// every level's selection over those frames alone from a fresh state (their Gaussian levels and level-0
+// frames are the run's, which a fresh fuser would build the same), the residual over their tops and the
+// collapse, into slab_img. The run's accumulators, residual, winner map and image are left as they were.
+static char* slab_fold(lsb_stack* s, int lo, int hi) {
+    lsb_engine* e = s->e;
+    cudaStream_t st = e->s;
+    const int n = hi - lo + 1, L = s->levels;
+    const size_t gsb = gs_bytes(s);
+    if (s->slab_acc.empty()) {
+        s->slab_acc.assign(L, nullptr);
+        s->slab_best.assign(L, nullptr);
+        for (int l = 0; l < L; l++) {
+            TRY(s->pool.get(&s->slab_acc[l], 3 * (size_t)s->lw[l] * s->lh[l]));
+            TRY(s->pool.get(&s->slab_best[l], (size_t)s->lw[l] * s->lh[l]));
+        }
+        TRY(s->pool.get(&s->slab_top, 3 * (size_t)s->lw[L] * s->lh[L]));
+        TRY(s->pool.get(&s->slab_img, 3 * (size_t)s->w * s->h));
+    }
+    const bool aligned = s->ap.enabled && s->count > 1 && !s->f32src;
+    const bool halo = s->fp.halo > 0.f;
+    const int guide = std::min((int)s->fp.depth_level, L - 1);
+    auto frame_g = [&](int l) { return (size_t)lo * 3 * s->lw[l] * s->lh[l] * gsb; };
+    auto frame_w = [&](int l) { return (size_t)lo * s->lw[l] * s->lh[l]; };
+    TRY(cudaMemsetAsync(s->status, 0, sizeof(int), st));
+    for (int l = 0; l < L; l++) {
+        bool focus = false;
+        int src = 0;
+        FoldArgs a = level_args(s, l, aligned, false, &focus, &src);
+        // frames lo..hi as a stack of their own: sources, transforms and levels offset to frame lo
+        a.nframes = n;
+        a.red_n = 0;
+        a.sel_k0 = 0;
+        a.sel_k1 = n;
+        if (l == 0) {
+            if (a.src_u16) a.src_u16 += (size_t)lo * s->w * s->h * 3;
+            if (a.src_f32) a.src_f32 += (size_t)lo * 3 * s->w * s->h;
+        } else {
+            a.src_g = (const char*)a.src_g + frame_g(l);
+        }
+        a.dst_g = (char*)a.dst_g + frame_g(l + 1);
+        a.xf = s->xf_dev + lo;
+        a.acc = s->slab_acc[l];
+        a.best = s->slab_best[l];
+        a.winner = nullptr;
+        if (halo && l >= guide) {
+            a.halo_mode = l == guide ? 1 : 2;
+            a.halo_p = std::min(s->fp.halo, 8.0f);
+            a.halo_w = s->halo_w[l] + frame_w(l);
+            if (l > guide)
+                TRY(reduce_weights(s->halo_w[l - 1] + frame_w(l - 1), s->lw[l - 1], s->lh[l - 1], n, a.halo_w, s->lw[l], s->lh[l], st));
+        } else {
+            set_groups(s, a);
+        }
+        TRY(fold_level(a, src, s->storage, (int)s->fp.energy_radius, false, st, e->grid_select > 0 ? e->grid_select : e->grid));
+    }
+    const int wt = s->lw[L], ht = s->lh[L];
+    const void* tops = (const char*)s->g[L] + frame_g(L);
+    if (halo) {
+        TRY(reduce_weights(s->halo_w[L - 1] + frame_w(L - 1), s->lw[L - 1], s->lh[L - 1], n, s->halo_w[L] + frame_w(L), wt, ht, st));
+        TRY(halo_top(tops, s->storage, s->xf_dev + lo, s->halo_w[L] + frame_w(L), n, wt, ht, s->slab_top, s->dev_s, st));
+        TRY(halo_divide(s->slab_top, s->dev_s, wt, ht, st));
+        for (int l = guide + 1; l < L; l++) TRY(halo_divide(s->slab_acc[l], s->slab_best[l], s->lw[l], s->lh[l], st));
+    } else {
+        // the log table of the top rule's entropy window is the run's (lnp, written for the same radius)
+        ResidualArgs ra{tops, n, wt, ht, (int)s->fp.top_rule, (int)s->fp.top_radius, (int)s->fp.entropy_bins, s->dev_s, s->ent_s,
+                        s->slab_top, s->xf_dev + lo};
+        TRY(fuse_residuals(ra, s->storage, s->lnp, st));
+    }
+    const float* coarse = s->slab_top;
+    for (int l = L - 1; l >= 0; l--) {
+        float* out = (l % 2 == 0) ? s->slab_img : s->img_tmp;
+        TRY(collapse_level(s->slab_acc[l], coarse, out, s->lw[l], s->lh[l], s->lw[l + 1], s->lh[l + 1], l == 0, nullptr, st));
+        coarse = out;
+    }
+    return nullptr;
+}
+
+// stack.rs:872 `fuse_slabs` for one slab: fuse_range, the cut (pyramid.rs:31) and the resize (prep.rs:46)
+extern "C" char* lsb_stack_fuse_range(lsb_stack* s, uint32_t lo, uint32_t hi, const uint32_t* rect, uint32_t out_w, uint32_t out_h,
+                                      uint32_t interp, float* out) {
+    if (!s || !out) return dup_err("null argument");
+    if (!s->folded) return dup_err("fuse_range needs a finished (or run) stack: it fuses the frames as that run folded them");
+    if (lo > hi || hi >= s->count) return dup_err(fmt("fuse_range: frames %u..%u of a %u-frame stack", lo, hi, s->count));
+    if (interp > 5) return dup_err(fmt("fuse_range: interp %u out of range (0..5)", interp));
+    uint32_t r[4] = {0, 0, s->w, s->h};
+    if (rect) memcpy(r, rect, sizeof r);
+    if (r[2] == 0 || r[3] == 0 || r[0] >= s->w || r[1] >= s->h || r[2] > s->w - r[0] || r[3] > s->h - r[1])
+        return dup_err(fmt("fuse_range: the rectangle %u,%u %ux%u is not inside the %ux%u frame", r[0], r[1], r[2], r[3], s->w, s->h));
+    if ((out_w == 0) != (out_h == 0)) return dup_err("fuse_range: give both output dimensions or neither");
+    const uint32_t ow = out_w ? out_w : r[2], oh = out_h ? out_h : r[3];
+    if (const char* why = size_error(ow, oh)) return dup_err(fmt("fuse_range output: %s", why));
+    if (s->fp.halo > 0.f && s->halo_w.empty()) return dup_err("fuse_range: the halo weights of the run are missing");
+    char* err = slab_fold(s, (int)lo, (int)hi);
+    if (err) return err;
+    cudaStream_t st = s->e->s;
+    const size_t of = 3 * (size_t)ow * oh;
+    if (s->slab_out_floats < of) {
+        if (s->slab_out) cudaFree(s->slab_out);
+        s->slab_out = nullptr;
+        s->slab_out_floats = 0;
+        TRY(cudaMalloc(&s->slab_out, sizeof(float) * of));
+        s->slab_out_floats = of;
+    }
+    TRY(resize_planes(s->slab_img, s->w, (size_t)s->w * s->h, 3, (int)r[0], (int)r[1], (int)r[2], (int)r[3], (int)ow, (int)oh, (int)interp,
+                      s->slab_out, st));
+    TRY(cudaMemcpyAsync(out, s->slab_out, sizeof(float) * of, cudaMemcpyDeviceToHost, st));
+    TRY(cudaStreamSynchronize(st));
+    int status = 0;
+    TRY(cudaMemcpy(&status, s->status, sizeof(int), cudaMemcpyDeviceToHost));
+    if (status) return dup_err(fmt("device status 0x%x (a kernel met a shape it was not built for)", status));
+    return nullptr;
+}
+
+// prep.rs:46 `resize` / :63 `resize_plane` of host planes, on the engine's stream
+extern "C" char* lsb_resize(lsb_engine* e, const float* src, uint32_t planes, uint32_t pw, uint32_t ph, uint32_t w, uint32_t h,
+                            uint32_t interp, float* out) {
+    if (!e || !src || !out) return dup_err("null argument");
+    if (interp > 5) return dup_err(fmt("resize: interp %u out of range (0..5)", interp));
+    if (planes == 0 || planes > 64) return dup_err("resize: 1 to 64 planes");
+    if (const char* why = size_error(pw, ph)) return dup_err(fmt("resize source: %s", why));
+    if (const char* why = size_error(w, h)) return dup_err(fmt("resize output: %s", why));
+    const size_t ni = (size_t)planes * pw * ph, no = (size_t)planes * w * h;
+    float *di = nullptr, *dout = nullptr;
+    cudaError_t ce = cudaMalloc(&di, sizeof(float) * ni);
+    if (ce == cudaSuccess) ce = cudaMalloc(&dout, sizeof(float) * no);
+    if (ce == cudaSuccess) ce = cudaMemcpyAsync(di, src, sizeof(float) * ni, cudaMemcpyHostToDevice, e->s);
+    if (ce == cudaSuccess) ce = resize_planes(di, pw, (size_t)pw * ph, (int)planes, 0, 0, (int)pw, (int)ph, (int)w, (int)h, (int)interp, dout, e->s);
+    if (ce == cudaSuccess) ce = cudaMemcpyAsync(out, dout, sizeof(float) * no, cudaMemcpyDeviceToHost, e->s);
+    if (ce == cudaSuccess) ce = cudaStreamSynchronize(e->s);
+    cudaFree(di);
+    cudaFree(dout);
+    if (ce != cudaSuccess) return dup_err(fmt("resize: %s", cudaGetErrorString(ce)));
     return nullptr;
 }
 

@@ -405,7 +405,7 @@ __global__ void collapse_kernel(const float* __restrict__ acc, const float* __re
         float v = __fadd_rn(acc[o], up);
         if (last) {
             v = fminf(fmaxf(v, 0.f), 1.f);
-            rgb[((size_t)y * w + x) * 3 + c] = (uint16_t)__fadd_rn(__fmul_rn(v, 65535.f), 0.5f);
+            if (rgb) rgb[((size_t)y * w + x) * 3 + c] = (uint16_t)__fadd_rn(__fmul_rn(v, 65535.f), 0.5f);
         }
         out[o] = v;
     }

@@ -232,6 +232,28 @@ class Engine:
     def stack(self, w, h, n, fuse=None, align=None, depth=None, brightness=True, crop=True):
         return Stack(self, w, h, n, fuse, align, depth, brightness, crop)
 
+    def resize(self, planes, w: int, h: int, interp: int = 3) -> np.ndarray:
+        """prep.rs:46 `resize` / :63 `resize_plane` on the device: (p, ph, pw) or (ph, pw) float32 planes
+        resampled to (..., h, w) with pixel centres kept (interp: align.rs:148 code, 3 = Spline4x4)."""
+        a = np.ascontiguousarray(planes, dtype=np.float32)
+        one = a.ndim == 2
+        if one:
+            a = a[None]
+        out = np.empty((a.shape[0], h, w), np.float32)
+        check(self._L.lsb_resize(self._h, C.c_void_p(a.ctypes.data), a.shape[0], a.shape[2], a.shape[1], w, h, interp,
+                                 C.c_void_p(out.ctypes.data)))
+        return out[0] if one else out
+
+
+def slab_ranges(count: int, size: int, overlap: int = 0) -> list:
+    """stack.rs:76 `slab_ranges`: (lo, hi) inclusive frame ranges of `size` frames (clamped to
+    [1, count]), consecutive ones overlapping by `overlap` (at most size - 1), the last cut short."""
+    L = load()
+    k = L.lsb_slab_ranges(count, size, overlap, None, 0)
+    buf = (C.c_uint32 * (2 * max(k, 1)))()
+    L.lsb_slab_ranges(count, size, overlap, buf, k)
+    return [(buf[2 * i], buf[2 * i + 1]) for i in range(k)]
+
 
 def check_params(fuse=None, align=None, depth=None):
     """Raises LsbError for settings a stack would refuse (lsb_check_params); needs no device.
@@ -295,6 +317,7 @@ class Stack:
                                       C.byref(hnd)))
         self._h = hnd
         self._keep = []
+        self.count = 0  # frames pushed (or declared with set_count)
         _live_stacks.add(self)
 
     def close(self):
@@ -314,6 +337,7 @@ class Stack:
         """One decoded frame, (h, w, 3) uint16 (numpy or CUDA tensor)."""
         p, keep = _ptr(rgb)
         check(self._L.lsb_stack_push_u16(self._h, p, stride_px))
+        self.count += 1
         self._keep.append(keep)  # async copies from host memory complete before the next sync
 
     def push_f32(self, planes):
@@ -325,6 +349,7 @@ class Stack:
             self._keep.append(keep)
         arr = (C.c_void_p * 3)(*ps)
         check(self._L.lsb_stack_push_f32(self._h, arr))
+        self.count += 1
 
     push = push_f32
 
@@ -335,6 +360,27 @@ class Stack:
         p = (wav or WavParams()).c()
         check(self._L.lsb_stack_weighted_average(self._h, C.byref(p), C.c_void_p(out.ctypes.data)))
         return out
+
+    def fuse_range(self, lo: int, hi: int, rect=None, size=None, interp: int = 3) -> np.ndarray:
+        """stack.rs:740 `fuse_range` over frames lo..hi (inclusive) of the last finish (or run), fused on
+        their own, cut to rect = (x, y, w, h) and resized to size = (w, h) as stack.rs:872 `fuse_slabs`
+        does (Spline4x4 by default): (3, oh, ow) float32. The stack's own results stay as they were."""
+        r = None
+        if rect is not None:
+            r = (C.c_uint32 * 4)(*[int(v) for v in rect])
+        ow, oh = (int(size[0]), int(size[1])) if size is not None else (0, 0)
+        w, h = (ow, oh) if size is not None else ((int(rect[2]), int(rect[3])) if rect is not None else (self.w, self.h))
+        out = np.empty((3, h, w), np.float32)
+        check(self._L.lsb_stack_fuse_range(self._h, lo, hi, r, ow, oh, interp, C.c_void_p(out.ctypes.data)))
+        return out
+
+    def slabs(self, size: int, overlap: int = 0, rect=None, restretch=None, interp: int = 3):
+        """stack.rs:872 `fuse_slabs` after a finish: (index, count, lo, hi, image) for each slab of
+        slab_ranges(count, size, overlap), each fused on its own, cut to rect and, with restretch = (w, h),
+        resized to that size; one at a time, none kept."""
+        ranges = slab_ranges(self.count, size, overlap)
+        for k, (lo, hi) in enumerate(ranges):
+            yield k, len(ranges), lo, hi, self.fuse_range(lo, hi, rect, restretch, interp)
 
     def set_warm_start(self, net):
         """Start this stack's WLS solves from the U-Net's prediction (None: the reference's FGS start)."""
@@ -364,6 +410,7 @@ class Stack:
 
     def set_count(self, count):
         check(self._L.lsb_stack_set_count(self._h, count))
+        self.count = count
 
     def shares(self):
         out = np.zeros(self.n, np.float32)

@@ -110,6 +110,9 @@ def _declare(L):
         ("orc_synth_stack", C.c_int, [P, P, P, C.c_uint32, C.c_uint32]),
         ("orc_stack_wav", C.c_int, [P, P]),
         ("orc_weighted_average_f", None, [P, sz, sz, sz, P, P, P, P, P]),
+        ("orc_stack_slabs", sz, [P, P, P]),
+        ("orc_slab_ranges", sz, [sz, sz, sz, P, sz]),
+        ("orc_resize_f", None, [P, sz, sz, sz, sz, sz, C.c_int, P]),
     ]:
         f = getattr(L, name)
         f.restype = res
@@ -212,6 +215,8 @@ class StackParams:  # stack.rs:27-71 (the hot-path subset)
     wav: WavParams | None = None  # stack.rs:857 the weighted average too (needs depth)
     # the engine's 16-bit level storage to emulate ("f32": the reference itself; "unorm16", "f16")
     storage: str = "f32"
+    # stack.rs:55 `slabs`: (size, overlap), each slab fused on its own after the result
+    slabs: tuple | None = None
 
     def arr(self):
         a = self.fuse.arr() + (self.align or AlignParams()).arr() + (self.depth or DepthParams()).arr()
@@ -219,6 +224,7 @@ class StackParams:  # stack.rs:27-71 (the hot-path subset)
         w = self.wav or WavParams()
         a += [float(self.wav is not None), w.power, w.smooth, w.gate, float(w.edge)]
         a += [float(["f32", "unorm16", "f16"].index(self.storage))]
+        a += [float(self.slabs[0]), float(self.slabs[1])] if self.slabs else [0.0, 0.0]
         return np.asarray(a, dtype=F64)
 
 
@@ -621,6 +627,28 @@ class StackResult:
     shares: np.ndarray
     stats: dict
     wav: np.ndarray | None = None  # (3, h, w) float64, the weighted average when asked for
+    # stack.rs:872 the slabs when asked for: (lo, hi) and each one's fused image (3, h, w) float64, uncut
+    slab_ranges: list | None = None
+    slabs: np.ndarray | None = None
+
+
+def slab_ranges(count, size, overlap=0):
+    """stack.rs:76 `slab_ranges`: inclusive (lo, hi) frame ranges."""
+    k = lib().orc_slab_ranges(count, size, overlap, None, 0)
+    buf = np.zeros(2 * max(k, 1), np.uint64)
+    lib().orc_slab_ranges(count, size, overlap, _ptr(buf), k)
+    return [(int(buf[2 * i]), int(buf[2 * i + 1])) for i in range(k)]
+
+
+def resize(planes, w, h, interp=3):
+    """prep.rs:46 `resize` / :63 `resize_plane` in f32: (p, ph, pw) or (ph, pw) planes to (..., h, w)."""
+    a = c32(planes)
+    one = a.ndim == 2
+    if one:
+        a = a[None]
+    out = np.empty((a.shape[0], h, w), F32)
+    lib().orc_resize_f(_ptr(a), a.shape[0], a.shape[2], a.shape[1], w, h, int(interp), _ptr(out))
+    return out[0] if one else out
 
 
 def run_stack(frames_u16, params: StackParams | None = None, fp64=False) -> StackResult:
@@ -709,6 +737,13 @@ def _result_of(r, p, n, w, h) -> "StackResult":
         wav = np.empty((3, h, w), F64)
         if not L.orc_stack_wav(r, _ptr(wav)):
             wav = None
-        return StackResult(img, u16, win, depth, conf, floor_cells, sims, gains, shares, stats, wav)
+        ranges = slabs = None
+        k = L.orc_stack_slabs(r, None, None)
+        if k:
+            lohi = np.zeros(2 * k, np.uint64)
+            slabs = np.empty((k, 3, h, w), F64)
+            L.orc_stack_slabs(r, _ptr(lohi), _ptr(slabs))
+            ranges = [(int(lohi[2 * i]), int(lohi[2 * i + 1])) for i in range(k)]
+        return StackResult(img, u16, win, depth, conf, floor_cells, sims, gains, shares, stats, wav, ranges, slabs)
     finally:
         L.orc_stack_free(r)

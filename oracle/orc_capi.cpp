@@ -361,6 +361,8 @@ static StackParams stack_params_of(const double* sp) {
     p.wp.gate = (float)sp[37];
     p.wp.edge = sp[38] != 0.0;
     p.storage = (int)sp[39];
+    p.slab_size = (size_t)sp[40];
+    p.slab_overlap = (size_t)sp[41];
     return p;
 }
 void* orc_run_stack(const uint16_t* frames, size_t n, size_t w, size_t h, const double* sp, int fp64) {
@@ -522,6 +524,44 @@ int orc_stack_wav(void* p, double* planes) {
         return 1;
     };
     return r->dbl ? fill(r->d) : fill(r->f);
+}
+
+// the slabs of the run: their count; with lohi, (lo, hi) pairs; with planes, each slab's fused image
+// (planar f64 [k][3][h][w], exact for both precisions)
+size_t orc_stack_slabs(void* p, uint64_t* lohi, double* planes) {
+    StackRes* r = (StackRes*)p;
+    auto fill = [&](auto& o) {
+        const size_t n = r->w * r->h;
+        for (size_t k = 0; k < o.slabs.size(); k++) {
+            if (lohi) {
+                lohi[2 * k] = o.slab_rng[k][0];
+                lohi[2 * k + 1] = o.slab_rng[k][1];
+            }
+            if (planes)
+                for (int c = 0; c < 3; c++)
+                    for (size_t i = 0; i < n; i++) planes[(k * 3 + c) * n + i] = (double)o.slabs[k].p[c][i];
+        }
+        return o.slabs.size();
+    };
+    return r->dbl ? fill(r->d) : fill(r->f);
+}
+
+// stack.rs:76 slab_ranges: the count; the first max (lo, hi) pairs into lohi
+size_t orc_slab_ranges(size_t count, size_t size, size_t overlap, uint64_t* lohi, size_t max) {
+    auto v = slab_ranges(count, size, overlap);
+    for (size_t k = 0; k < v.size() && k < max; k++) {
+        lohi[2 * k] = v[k][0];
+        lohi[2 * k + 1] = v[k][1];
+    }
+    return v.size();
+}
+
+// prep.rs:63 resize_plane (f32) of `planes` planes pw x ph -> w x h
+void orc_resize_f(const float* src, size_t planes, size_t pw, size_t ph, size_t w, size_t h, int interp, float* out) {
+    for (size_t c = 0; c < planes; c++) {
+        std::vector<float> o = resize_plane<float>(src + c * pw * ph, pw, ph, w, h, interp);
+        std::copy(o.begin(), o.end(), out + c * w * h);
+    }
 }
 
 // f32 -> IEEE half bits (round to nearest even) and back, as the 16-bit storage emulation does them

@@ -23,7 +23,40 @@ struct StackParams {
     // the engine's 16-bit storage to emulate (not the reference's): levels >= 1 rounded as stored
     // (orc_core.hpp `stored`), focus slices as IEEE half, aligned frames as u16 after their warp
     int storage = 0;
+    // stack.rs:55 `slabs`: (size, overlap) of the slabs fused after the result (size 0: none)
+    size_t slab_size = 0, slab_overlap = 0;
 };
+
+// stack.rs:76 `slab_ranges`
+inline std::vector<std::array<size_t, 2>> slab_ranges(size_t count, size_t size, size_t overlap) {
+    std::vector<std::array<size_t, 2>> out;
+    if (count == 0) return out;
+    size = std::min(std::max(size, (size_t)1), count);
+    overlap = std::min(overlap, size - 1);
+    size_t lo = 0;
+    for (;;) {
+        const size_t hi = std::min(lo + size - 1, count - 1);
+        out.push_back({lo, hi});
+        if (hi + 1 >= count) return out;
+        lo = hi + 1 - overlap;
+    }
+}
+
+// prep.rs:63 `resize_plane`: the plane through the Sim that scales it onto w x h with pixel centres
+// corresponding (offset (k - 1)(s + 1) / 2s of the source size on each axis)
+template <class T>
+std::vector<T> resize_plane(const T* p, size_t pw, size_t ph, size_t w, size_t h, int interp) {
+    if (pw == w && ph == h) return std::vector<T>(p, p + w * h);
+    const double sw = (double)pw, sh = (double)ph, kx = (double)w / sw, ky = (double)h / sh;
+    Sim sim;
+    sim.v[0] = (kx - 1.0) * (sw + 1.0) / (2.0 * sw);
+    sim.v[1] = (ky - 1.0) * (sh + 1.0) / (2.0 * sh);
+    sim.v[2] = kx;
+    sim.v[4] = ky / kx;
+    std::vector<T> out;
+    warp_plane<T>(p, pw, ph, sim, w, h, interp, out, nullptr);
+    return out;
+}
 
 template <class T>
 struct StackOutput {
@@ -37,6 +70,9 @@ struct StackOutput {
     size_t levels = 0;
     size_t align_evals = 0;
     Img3<T> wav;                   // the weighted average (wav.rs:92), when asked for
+    // stack.rs:872 `fuse_slabs`: each slab's frames and its fused image (full frame, before any cut)
+    std::vector<std::array<size_t, 2>> slab_rng;
+    std::vector<Img3<T>> slabs;
 };
 
 // io.rs:89-94 u16 -> f32 as v * (1/65535) (an f32 multiply by the f32 reciprocal)
@@ -149,7 +185,7 @@ struct StackRun {
             if (sp.storage != 0)
                 for (auto& v : slices.back()) v = (T)f16_value(f16_bits((float)v));
         }
-        if (sp.wav && sp.depth) kept.push_back(img);
+        if ((sp.wav && sp.depth) || sp.slab_size > 0) kept.push_back(img);
         i++;
     }
     void finish() {
@@ -157,6 +193,22 @@ struct StackRun {
         fuser.finish(out.image, out.winner);
         if (sp.depth) out.dm = depth_from_slices<T>(slices, out.image, sp.dp);
         if (sp.wav && sp.depth && !kept.empty()) out.wav = weighted_average<T>(kept, sp.dp, sp.wp, out.dm.floor_cells, &out.image);
+        if (sp.slab_size > 0) {
+            // stack.rs:740 `fuse_range` for each slab: a fresh fuser over the slab's frames as folded
+            out.slab_rng = slab_ranges(kept.size(), sp.slab_size, sp.slab_overlap);
+            for (const auto& r : out.slab_rng) {
+                Fuser<T> f(w, h, sp.fuse);
+                f.storage = sp.storage;
+                for (size_t k = r[0]; k <= r[1]; k++) {
+                    const auto& g = out.gains[k];
+                    f.push(kept[k], std::max(g[0], std::max(g[1], g[2])));
+                }
+                Img3<T> im;
+                std::vector<float> win;
+                f.finish(im, win);
+                out.slabs.push_back(std::move(im));
+            }
+        }
         out.crop = Rect{0, 0, w, h};
         if (aligned && sp.crop) out.crop = common_area(out.sims, w, h, sp.al.interp);
     }
