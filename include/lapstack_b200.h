@@ -137,6 +137,33 @@ typedef struct {
     uint32_t edge;   /* 1: the weights smoothed by the guided filter with the fused luma as guide */
 } lsb_wav_params;
 
+/* dust.rs:85 Spot: a window (x, y, w, h) of the frame, its mask (w*h bytes, nonzero = dust) and, for
+   flat mode, its attenuation (w*h floats, >= 1; may be NULL in fill mode). */
+typedef struct {
+    uint32_t x, y, w, h;
+    const uint8_t* mask;
+    const float* gain;
+} lsb_dust_spot;
+
+/* dust.rs:105 DustMap: the frame size it was made at, dust.rs:42 DustMode (0 fill: pull-push from the
+   surroundings; 1 flat: times the attenuation) and the spots, taken out in order. */
+typedef struct {
+    uint32_t w, h;
+    uint32_t mode;
+    uint32_t n_spots;
+    const lsb_dust_spot* spots;
+} lsb_dust_map;
+
+/* What every decoded frame goes through before it is registered and folded (stack.rs:52-58 Params::dust,
+   rotate, reduce; lapstack-web lib.rs:766-784 on 16-bit frames): the dust map (NULL: none; frames of its
+   size only), quarter turns clockwise (0..3), the draft block mean by 2^draft (0..8); then a frame of
+   another size than the stack's is resampled to it (decode.rs:125). */
+typedef struct {
+    const lsb_dust_map* dust;
+    uint32_t rotate;
+    uint32_t draft;
+} lsb_frame_prep;
+
 /* Seeded synthetic stack description (no reference counterpart; the benchmark inputs). */
 typedef struct {
     uint32_t w, h, n;
@@ -184,6 +211,19 @@ char* lsb_stack_push_u16(lsb_stack* s, const uint16_t* rgb, size_t stride_px);
 /* gpu.rs:432 GpuFuser::push (stack.rs:152 AnyFuser::push): one frame as three planar f32 planes in
    [0,1] (host or device pointers); the frame is folded as given. */
 char* lsb_stack_push_f32(lsb_stack* s, const float* const planes[3]);
+/* The frame preparation of every frame pushed from now on (stack.rs:291-305 LazyFrames' dust, rotate and
+   reduce; lapstack-web lib.rs:766-784), on the device as each frame lands: set it before the first push
+   (the map is copied; p NULL clears it). The stack's w x h is the size the frames are brought to. */
+char* lsb_stack_set_prep(lsb_stack* s, const lsb_frame_prep* p);
+/* A decoded 16-bit frame of any size w x h (interleaved, host or device pointer), prepared as set
+   (lsb_stack_set_prep) and brought to the stack's size (lapstack-web lib.rs:784 decode_for_run). With a
+   preparation set, lsb_stack_push_u16 is this call with the stack's own size. */
+char* lsb_stack_push_u16_sized(lsb_stack* s, const uint16_t* rgb, uint32_t w, uint32_t h);
+/* The same preparation on one frame, on its own (host or device pointers; synchronous): in is w x h,
+   out receives run_w x run_h (both 0: the prepared size, written to out_wh[0..1] in any case; out may be
+   NULL to ask the size only). */
+char* lsb_prep_frame_u16(lsb_engine* e, const lsb_frame_prep* p, const uint16_t* in, uint32_t w, uint32_t h, uint32_t run_w,
+                         uint32_t run_h, uint16_t* out, uint32_t* out_wh);
 /* The device buffer frames are pushed into ([n][h][w][3] u16), and a way to declare
    frames written there directly (count = frames now present). No counterpart in the reference. */
 char* lsb_stack_frames_device(lsb_stack* s, uint16_t** frames_dev);

@@ -66,6 +66,20 @@ class WavParamsC(C.Structure):
     _fields_ = [("power", C.c_float), ("smooth", C.c_uint32), ("gate", C.c_float), ("edge", C.c_uint32)]
 
 
+class DustSpotC(C.Structure):
+    _fields_ = [("x", C.c_uint32), ("y", C.c_uint32), ("w", C.c_uint32), ("h", C.c_uint32), ("mask", C.c_void_p),
+                ("gain", C.c_void_p)]
+
+
+class DustMapC(C.Structure):
+    _fields_ = [("w", C.c_uint32), ("h", C.c_uint32), ("mode", C.c_uint32), ("n_spots", C.c_uint32),
+                ("spots", C.POINTER(DustSpotC))]
+
+
+class FramePrepC(C.Structure):
+    _fields_ = [("dust", C.POINTER(DustMapC)), ("rotate", C.c_uint32), ("draft", C.c_uint32)]
+
+
 class SynthDesc(C.Structure):
     _fields_ = [("w", C.c_uint32), ("h", C.c_uint32), ("n", C.c_uint32), ("warp", C.c_uint32), ("seed", C.c_uint64),
                 ("mag_step", C.c_float), ("noise_std", C.c_float), ("blur_px", C.c_float), ("warp_scale", C.c_float),
@@ -114,6 +128,10 @@ SIGNATURES = {
     "lsb_unet_train_step": (ERR, [P, P, P, P, C.c_uint32, C.c_uint32, C.c_uint32, C.c_float, C.POINTER(C.c_double)]),
     "lsb_stack_set_warm_start": (ERR, [P, P]),
     "lsb_stack_weighted_average": (ERR, [P, C.POINTER(WavParamsC), P]),
+    "lsb_stack_set_prep": (ERR, [P, C.POINTER(FramePrepC)]),
+    "lsb_stack_push_u16_sized": (ERR, [P, P, C.c_uint32, C.c_uint32]),
+    "lsb_prep_frame_u16": (ERR, [P, C.POINTER(FramePrepC), P, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, P,
+                                 C.POINTER(C.c_uint32)]),
     "lsb_slab_ranges": (C.c_uint32, [C.c_uint32, C.c_uint32, C.c_uint32, P, C.c_uint32]),
     "lsb_stack_fuse_range": (ERR, [P, C.c_uint32, C.c_uint32, P, C.c_uint32, C.c_uint32, C.c_uint32, P]),
     "lsb_resize": (ERR, [P, P, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, P]),

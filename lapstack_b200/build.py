@@ -20,7 +20,7 @@ ROOT = os.path.dirname(PKG)
 CSRC = os.path.join(PKG, "csrc")
 OUT_DIR = os.path.join(PKG, "_build")
 LIB = os.path.join(OUT_DIR, "liblapstack_b200.so")
-SOURCES = ["lsb_fold.cu", "lsb_depth.cu", "lsb_wls.cu", "lsb_align.cu", "lsb_synth.cu", "lsb_unet.cu", "lsb_api.cu"]
+SOURCES = ["lsb_fold.cu", "lsb_depth.cu", "lsb_wls.cu", "lsb_align.cu", "lsb_synth.cu", "lsb_unet.cu", "lsb_prep.cu", "lsb_api.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

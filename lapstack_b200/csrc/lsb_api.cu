@@ -24,6 +24,7 @@
 #include "lsb_align.h"
 #include "lsb_depth.h"
 #include "lsb_internal.h"
+#include "lsb_prep.h"
 
 using namespace lsb;
 
@@ -178,7 +179,23 @@ struct lsb_stack {
     std::vector<float*> slab_acc, slab_best;
     float *slab_top = nullptr, *slab_img = nullptr, *slab_out = nullptr;
     size_t slab_out_floats = 0;
+    // the frame preparation (lsb_stack_set_prep): the uploaded dust map, the turn and the draft level,
+    // two staging buffers for frames as decoded (frame i uses i & 1) and one for a turned frame to resize
+    bool prep_on = false;
+    DustDev* dust = nullptr;
+    int prep_rot = 0, prep_draft = 0;
+    uint16_t* stage[2] = {nullptr, nullptr};
+    size_t stage_px = 0;
+    uint16_t* stage_mid = nullptr;
+    size_t mid_px = 0;
+    cudaEvent_t stage_free[2] = {nullptr, nullptr};
     ~lsb_stack() {
+        delete dust;
+        for (int b = 0; b < 2; b++) {
+            if (stage[b]) cudaFree(stage[b]);
+            if (stage_free[b]) cudaEventDestroy(stage_free[b]);
+        }
+        if (stage_mid) cudaFree(stage_mid);
         if (slab_out) cudaFree(slab_out);
         for (auto& v : chunk_ev) cudaEventDestroy(v);
         if (wav_w) cudaFree(wav_w);
@@ -565,10 +582,15 @@ static bool is_device_ptr(const void* p) {
     return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
 }
 
+extern "C" char* lsb_stack_push_u16_sized(lsb_stack* s, const uint16_t* rgb, uint32_t w, uint32_t h);
 extern "C" char* lsb_stack_push_u16(lsb_stack* s, const uint16_t* rgb, size_t stride_px) {
     if (!s || !rgb) return dup_err("null argument");
     if (s->f32src) return dup_err("this stack takes f32 frames");
     if (s->count >= s->n) return dup_err(fmt("the stack holds %u frames", s->n));
+    if (s->prep_on) {
+        if (stride_px != 0 && stride_px != s->w) return dup_err("a prepared frame is pushed without a row stride");
+        return lsb_stack_push_u16_sized(s, rgb, s->w, s->h);
+    }
     if (stride_px == 0) stride_px = s->w;
     if (stride_px < s->w) return dup_err("stride_px < width");
     uint16_t* dst = s->frames + (size_t)s->count * s->w * s->h * 3;
@@ -589,6 +611,149 @@ extern "C" char* lsb_stack_push_u16(lsb_stack* s, const uint16_t* rgb, size_t st
     // register this frame now, behind the copy of the next one (stack.rs:785-821 does it per frame too)
     if (s->ap.enabled && s->n > 1 && chained(s) && s->aligned_upto == i)
         if (char* er = align_frame(s, i)) return er;
+    return nullptr;
+}
+
+// stack.rs:52-58 / 291-305 (LazyFrames' dust, rotate, reduce) as lapstack-web lib.rs:766-784 does them on
+// 16-bit frames: the map is uploaded once, the rest is set per stack
+extern "C" char* lsb_stack_set_prep(lsb_stack* s, const lsb_frame_prep* p) {
+    if (!s) return dup_err("null stack");
+    if (s->count > 0) return dup_err("set the frame preparation before the first push");
+    if (s->f32src) return dup_err("this stack takes f32 frames");
+    if (p && p->rotate > 3) return dup_err("prep: rotate must be 0..3 quarter turns");
+    if (p && p->draft > 8) return dup_err("prep: draft must be 0..8");
+    DustDev* d = nullptr;
+    if (p && p->dust) {
+        std::string why = dust_create(p->dust, &d);
+        if (!why.empty()) return dup_err(why);
+    }
+    delete s->dust;
+    s->dust = d;
+    s->prep_on = p != nullptr;
+    s->prep_rot = p ? (int)p->rotate : 0;
+    s->prep_draft = p ? (int)p->draft : 0;
+    for (int b = 0; b < 2; b++)
+        if (!s->stage_free[b]) TRY(cudaEventCreateWithFlags(&s->stage_free[b], cudaEventDisableTiming));
+    return nullptr;
+}
+
+// A buffer of at least px pixels (3 u16 each), grown once nothing on the copy stream still uses it.
+static cudaError_t grow_u16(uint16_t** buf, size_t* have, size_t px, cudaStream_t cs) {
+    if (*have >= px) return cudaSuccess;
+    cudaError_t e = cudaStreamSynchronize(cs);
+    if (e != cudaSuccess) return e;
+    if (*buf) cudaFree(*buf);
+    *buf = nullptr;
+    *have = 0;
+    e = cudaMalloc(buf, sizeof(uint16_t) * 3 * px);
+    if (e == cudaSuccess) *have = px;
+    return e;
+}
+
+// lapstack-web lib.rs:766-784 `decode` + `decode_for_run` on the device, on the copy stream: the frame as
+// decoded into a staging buffer, the dust map (frames of its size only), the turn and draft block mean in
+// one gather, and a frame of another size resampled to the stack's (decode.rs:125), into frame i's slot.
+extern "C" char* lsb_stack_push_u16_sized(lsb_stack* s, const uint16_t* rgb, uint32_t w, uint32_t h) {
+    if (!s || !rgb) return dup_err("null argument");
+    if (s->f32src) return dup_err("this stack takes f32 frames");
+    if (s->count >= s->n) return dup_err(fmt("the stack holds %u frames", s->n));
+    if (const char* why = size_error(w, h)) return dup_err(fmt("frame: %s", why));
+    if (!s->prep_on && w == s->w && h == s->h) return lsb_stack_push_u16(s, rgb, 0);
+    if (!s->prep_on) {  // only a resize: a preparation without steps
+        lsb_frame_prep none{nullptr, 0, 0};
+        if (char* er = lsb_stack_set_prep(s, &none)) return er;
+    }
+    lsb_engine* e = s->e;
+    const int i = (int)s->count, b = i & 1;
+    cudaStream_t cs = e->cs;
+    if (i == 0) {  // the frame store is rewritten: wait for whatever still reads it on the work stream
+        TRY(cudaEventRecord(e->s_mark, e->s));
+        TRY(cudaStreamWaitEvent(cs, e->s_mark, 0));
+    }
+    const size_t px = (size_t)w * h;
+    if (s->stage_px < px) {
+        // both staging buffers, grown together once the copy stream is idle
+        TRY(cudaStreamSynchronize(cs));
+        for (int k = 0; k < 2; k++) {
+            size_t have = 0;
+            TRY(grow_u16(&s->stage[k], &have, px, cs));
+        }
+        s->stage_px = px;
+    }
+    TRY(cudaStreamWaitEvent(cs, s->stage_free[b], 0));
+    uint16_t* raw = s->stage[b];
+    cudaMemcpyKind kind = is_device_ptr(rgb) ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+    TRY(cudaMemcpyAsync(raw, rgb, sizeof(uint16_t) * 3 * px, kind, cs));
+    if (s->dust && (int)w == s->dust->W && (int)h == s->dust->H) TRY(dust_apply_rgb16(s->dust, raw, cs));
+    int pw = (int)w, ph = (int)h;
+    const uint16_t* cur = raw;
+    uint16_t* dst = s->frames + (size_t)i * s->w * s->h * 3;
+    const bool turn = s->prep_rot != 0 || s->prep_draft != 0;
+    if (turn) turn_draft_dims((int)w, (int)h, s->prep_rot, s->prep_draft, &pw, &ph);
+    const bool resize = pw != (int)s->w || ph != (int)s->h;
+    if (turn) {
+        uint16_t* o = dst;
+        if (resize) {
+            TRY(grow_u16(&s->stage_mid, &s->mid_px, (size_t)pw * ph, cs));
+            o = s->stage_mid;
+        }
+        TRY(turn_draft_rgb16(raw, (int)w, (int)h, s->prep_rot, s->prep_draft, o, cs));
+        cur = o;
+    }
+    if (resize) TRY(resize_rgb16(cur, pw, ph, dst, (int)s->w, (int)s->h, cs));
+    else if (!turn) TRY(cudaMemcpyAsync(dst, raw, sizeof(uint16_t) * 3 * px, cudaMemcpyDeviceToDevice, cs));
+    TRY(cudaEventRecord(s->stage_free[b], cs));
+    TRY(cudaEventRecord(s->copied[i], cs));
+    TRY(cudaStreamWaitEvent(e->s, s->copied[i], 0));
+    s->count++;
+    s->folded = false;
+    if (s->ap.enabled && s->n > 1 && chained(s) && s->aligned_upto == i)
+        if (char* er = align_frame(s, i)) return er;
+    return nullptr;
+}
+
+// One frame through lsb_frame_prep on its own, synchronously on the engine's copy stream.
+extern "C" char* lsb_prep_frame_u16(lsb_engine* e, const lsb_frame_prep* p, const uint16_t* in, uint32_t w, uint32_t h, uint32_t run_w,
+                                    uint32_t run_h, uint16_t* out, uint32_t* out_wh) {
+    if (!e || !p || !in || !out_wh) return dup_err("null argument");
+    if (const char* why = size_error(w, h)) return dup_err(fmt("frame: %s", why));
+    if (p->rotate > 3) return dup_err("prep: rotate must be 0..3 quarter turns");
+    if (p->draft > 8) return dup_err("prep: draft must be 0..8");
+    if ((run_w == 0) != (run_h == 0)) return dup_err("prep: give both run dimensions or neither");
+    int pw = (int)w, ph = (int)h;
+    turn_draft_dims((int)w, (int)h, (int)p->rotate, (int)p->draft, &pw, &ph);
+    const int ow = run_w ? (int)run_w : pw, oh = run_h ? (int)run_h : ph;
+    if (const char* why = size_error((uint32_t)ow, (uint32_t)oh)) return dup_err(fmt("prep output: %s", why));
+    out_wh[0] = (uint32_t)ow;
+    out_wh[1] = (uint32_t)oh;
+    if (!out) return nullptr;
+    DustDev* d = nullptr;
+    if (p->dust) {
+        std::string why = dust_create(p->dust, &d);
+        if (!why.empty()) return dup_err(why);
+    }
+    cudaStream_t cs = e->cs;
+    uint16_t *raw = nullptr, *mid = nullptr, *res = nullptr;
+    cudaError_t ce = cudaMalloc(&raw, sizeof(uint16_t) * 3 * (size_t)w * h);
+    if (ce == cudaSuccess) ce = cudaMalloc(&mid, sizeof(uint16_t) * 3 * (size_t)pw * ph);
+    if (ce == cudaSuccess) ce = cudaMalloc(&res, sizeof(uint16_t) * 3 * (size_t)ow * oh);
+    const cudaMemcpyKind ki = is_device_ptr(in) ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+    const cudaMemcpyKind ko = is_device_ptr(out) ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+    if (ce == cudaSuccess) ce = cudaMemcpyAsync(raw, in, sizeof(uint16_t) * 3 * (size_t)w * h, ki, cs);
+    if (ce == cudaSuccess && d && (int)w == d->W && (int)h == d->H) ce = dust_apply_rgb16(d, raw, cs);
+    if (ce == cudaSuccess) ce = turn_draft_rgb16(raw, (int)w, (int)h, (int)p->rotate, (int)p->draft, mid, cs);
+    if (ce == cudaSuccess) {
+        if (ow != pw || oh != ph) ce = resize_rgb16(mid, pw, ph, res, ow, oh, cs);
+        else ce = cudaMemcpyAsync(res, mid, sizeof(uint16_t) * 3 * (size_t)ow * oh, cudaMemcpyDeviceToDevice, cs);
+    }
+    if (ce == cudaSuccess) ce = cudaMemcpyAsync(out, res, sizeof(uint16_t) * 3 * (size_t)ow * oh, ko, cs);
+    if (ce == cudaSuccess) ce = cudaStreamSynchronize(cs);
+    cudaStreamSynchronize(cs);
+    cudaFree(raw);
+    cudaFree(mid);
+    cudaFree(res);
+    delete d;
+    if (ce != cudaSuccess) return dup_err(fmt("prep: %s", cudaGetErrorString(ce)));
     return nullptr;
 }
 

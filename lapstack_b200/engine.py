@@ -20,7 +20,8 @@ from dataclasses import dataclass, field
 
 import numpy as np
 
-from ._lib import (AlignParamsC, Config, DepthParamsC, FuseParamsC, LOG_FN, LsbError, Result, SynthDesc, WavParamsC, check, load)
+from ._lib import (AlignParamsC, Config, DepthParamsC, DustMapC, DustSpotC, FramePrepC, FuseParamsC, LOG_FN, LsbError, Result,
+                   SynthDesc, WavParamsC, check, load)
 
 TOP_RULES = {"de": 0, "dev": 1, "avg": 2}
 INTERPS = ["nearest", "bilinear", "bicubic", "spline4x4", "spline6x6", "lanczos3"]
@@ -129,6 +130,51 @@ class WavParams:  # wav.rs:52-80
 
 
 @dataclass
+class DustSpot:  # dust.rs:85 Spot: its window at (x, y), mask (h, w) nonzero = dust, gain (h, w) for flat mode
+    x: int
+    y: int
+    mask: np.ndarray
+    gain: np.ndarray | None = None
+
+
+DUST_MODES = ("fill", "flat")
+
+
+@dataclass
+class DustMap:  # dust.rs:105 DustMap; mode dust.rs:42 ("fill": pull-push, "flat": times the attenuation)
+    w: int
+    h: int
+    spots: list
+    mode: str = "fill"
+
+
+@dataclass
+class FramePrep:  # stack.rs:52-58 Params::dust, rotate, reduce
+    dust: DustMap | None = None
+    rotate: int = 0
+    draft: int = 0
+
+    def c(self):
+        """The C struct and the arrays it points into (keep both alive while it is used)."""
+        keep = []
+        dm = None
+        if self.dust is not None:
+            d = self.dust
+            spots = (DustSpotC * max(len(d.spots), 1))()
+            for k, sp in enumerate(d.spots):
+                m = np.ascontiguousarray(sp.mask, dtype=np.uint8)
+                g = None if sp.gain is None else np.ascontiguousarray(sp.gain, dtype=np.float32)
+                keep += [m, g]
+                spots[k] = DustSpotC(sp.x, sp.y, m.shape[1], m.shape[0], m.ctypes.data, None if g is None else g.ctypes.data)
+            mode = _pick(d.mode, DUST_MODES, "dust mode") if isinstance(d.mode, str) else int(d.mode)
+            dm = DustMapC(d.w, d.h, mode, len(d.spots), spots)
+            keep += [spots, dm]
+        p = FramePrepC(C.pointer(dm) if dm is not None else None, self.rotate, self.draft)
+        keep.append(p)
+        return p, keep
+
+
+@dataclass
 class DepthMap:  # depth.rs:141
     depth: np.ndarray
     conf: np.ndarray
@@ -232,6 +278,19 @@ class Engine:
     def stack(self, w, h, n, fuse=None, align=None, depth=None, brightness=True, crop=True):
         return Stack(self, w, h, n, fuse, align, depth, brightness, crop)
 
+    def prep_frame(self, rgb, prep: FramePrep, size=None) -> np.ndarray:
+        """lapstack-web lib.rs:766-784 on one (h, w, 3) uint16 frame on the device: the dust map (frames of
+        its size only), the quarter turns, the draft block mean and, with size = (w, h), the run's size."""
+        a = np.ascontiguousarray(rgb, dtype=np.uint16)
+        p, keep = prep.c()
+        rw, rh = (int(size[0]), int(size[1])) if size is not None else (0, 0)
+        wh = (C.c_uint32 * 2)()
+        check(self._L.lsb_prep_frame_u16(self._h, C.byref(p), C.c_void_p(a.ctypes.data), a.shape[1], a.shape[0], rw, rh, None, wh))
+        out = np.empty((wh[1], wh[0], 3), np.uint16)
+        check(self._L.lsb_prep_frame_u16(self._h, C.byref(p), C.c_void_p(a.ctypes.data), a.shape[1], a.shape[0], rw, rh,
+                                         C.c_void_p(out.ctypes.data), wh))
+        return out
+
     def resize(self, planes, w: int, h: int, interp: int = 3) -> np.ndarray:
         """prep.rs:46 `resize` / :63 `resize_plane` on the device: (p, ph, pw) or (ph, pw) float32 planes
         resampled to (..., h, w) with pixel centres kept (interp: align.rs:148 code, 3 = Spline4x4)."""
@@ -318,6 +377,7 @@ class Stack:
         self._h = hnd
         self._keep = []
         self.count = 0  # frames pushed (or declared with set_count)
+        self._prep = None
         _live_stacks.add(self)
 
     def close(self):
@@ -334,11 +394,27 @@ class Stack:
             pass
 
     def push_u16(self, rgb, stride_px: int = 0):
-        """One decoded frame, (h, w, 3) uint16 (numpy or CUDA tensor)."""
+        """One decoded frame, (h, w, 3) uint16 (numpy or CUDA tensor). A frame of another size than the
+        stack's (or any frame, with a preparation set) goes through the preparation and is brought to
+        the stack's size (lsb_stack_push_u16_sized)."""
         p, keep = _ptr(rgb)
-        check(self._L.lsb_stack_push_u16(self._h, p, stride_px))
+        h, w = int(rgb.shape[0]), int(rgb.shape[1])
+        if stride_px == 0 and (self._prep is not None or (w, h) != (self.w, self.h)):
+            check(self._L.lsb_stack_push_u16_sized(self._h, p, w, h))
+        else:
+            check(self._L.lsb_stack_push_u16(self._h, p, stride_px))
         self.count += 1
         self._keep.append(keep)  # async copies from host memory complete before the next sync
+
+    def set_prep(self, prep: FramePrep | None):
+        """stack.rs:52-58 the dust map, quarter turns and draft level every decoded frame goes through
+        (lapstack-web lib.rs:766-784), on the device as each frame lands; before the first push."""
+        if prep is None:
+            check(self._L.lsb_stack_set_prep(self._h, None))
+        else:
+            p, keep = prep.c()
+            check(self._L.lsb_stack_set_prep(self._h, C.byref(p)))
+        self._prep = prep
 
     def push_f32(self, planes):
         """AnyFuser::push(&Img3): (3, h, w) float32 planes in [0, 1]."""

@@ -111,6 +111,12 @@ def _declare(L):
         ("orc_stack_wav", C.c_int, [P, P]),
         ("orc_weighted_average_f", None, [P, sz, sz, sz, P, P, P, P, P]),
         ("orc_stack_slabs", sz, [P, P, P]),
+        ("orc_dust_apply_rgb16", None, [P, sz, P, P, sz, sz, C.c_int, P, sz, sz]),
+        ("orc_dust_apply_f", None, [P, sz, P, P, sz, sz, C.c_int, P, sz, sz]),
+        ("orc_pull_push_f", None, [P, P, sz, sz, P]),
+        ("orc_rotate_f", None, [P, sz, sz, C.c_int, C.c_int, P]),
+        ("orc_draft_reduce_f", None, [P, sz, sz, C.c_int, P]),
+        ("orc_prep_rgb16", None, [P, sz, P, P, sz, sz, C.c_int, C.c_int, C.c_int, P, sz, sz, sz, sz, P, P]),
         ("orc_slab_ranges", sz, [sz, sz, sz, P, sz]),
         ("orc_resize_f", None, [P, sz, sz, sz, sz, sz, C.c_int, P]),
     ]:
@@ -747,3 +753,97 @@ def _result_of(r, p, n, w, h) -> "StackResult":
         return StackResult(img, u16, win, depth, conf, floor_cells, sims, gains, shares, stats, wav, ranges, slabs)
     finally:
         L.orc_stack_free(r)
+
+
+# --------------------------------------------------------------- frame prep
+@dataclass
+class DustSpot:  # dust.rs:85 Spot: its window at (x, y), mask (h, w) 1 = dust, gain (h, w) for flat mode
+    x: int
+    y: int
+    mask: np.ndarray
+    gain: np.ndarray | None = None
+
+
+@dataclass
+class DustMap:  # dust.rs:105 DustMap; mode dust.rs:42 "fill" (pull-push) or "flat"
+    w: int
+    h: int
+    spots: list
+    mode: str = "fill"
+
+
+def _dust_arrays(m: DustMap):
+    n = len(m.spots)
+    rects = np.zeros((max(n, 1), 4), np.uint64)
+    masks, gains = [], []
+    for k, s in enumerate(m.spots):
+        mk = np.ascontiguousarray(s.mask, dtype=np.uint8)
+        rects[k] = (s.x, s.y, mk.shape[1], mk.shape[0])
+        masks.append(mk.ravel())
+        g = np.ones(mk.shape, F32) if s.gain is None else np.asarray(s.gain, F32)
+        gains.append(np.ascontiguousarray(g).ravel())
+    masks = np.concatenate(masks) if masks else np.zeros(1, np.uint8)
+    gains = np.concatenate(gains) if gains else np.zeros(1, F32)
+    return rects, n, masks, gains, {"fill": 0, "flat": 1}[m.mode]
+
+
+def dust_apply_rgb16(m: DustMap, rgb):
+    """dust.rs:487 `apply_rgb16` on a copy of an interleaved (h, w, 3) u16 frame."""
+    out = np.array(rgb, dtype=np.uint16, copy=True, order="C")
+    rects, n, masks, gains, mode = _dust_arrays(m)
+    lib().orc_dust_apply_rgb16(_ptr(rects), n, _ptr(masks), _ptr(gains), m.w, m.h, mode, _ptr(out), out.shape[1], out.shape[0])
+    return out
+
+
+def dust_apply(m: DustMap, planes):
+    """dust.rs:478 `apply` on a copy of (3, h, w) f32 planes."""
+    out = np.array(planes, dtype=F32, copy=True, order="C")
+    rects, n, masks, gains, mode = _dust_arrays(m)
+    lib().orc_dust_apply_f(_ptr(rects), n, _ptr(masks), _ptr(gains), m.w, m.h, mode, _ptr(out), out.shape[2], out.shape[1])
+    return out
+
+
+def pull_push(v, wt):
+    """dust.rs:591 `pull_push` of (h, w) f32 values with weights in [0, 1]."""
+    v, wt = c32(v), c32(wt)
+    out = np.empty_like(v)
+    lib().orc_pull_push_f(_ptr(v), _ptr(wt), v.shape[1], v.shape[0], _ptr(out))
+    return out
+
+
+def rotate(planes, quarters, flip=False):
+    """prep.rs:16 `rotate` of (3, h, w) f32 planes: quarter turns clockwise after an optional mirror."""
+    a = c32(planes)
+    h, w = a.shape[1:]
+    out = np.empty((3, w, h) if quarters % 2 else (3, h, w), F32)
+    lib().orc_rotate_f(_ptr(a), w, h, int(quarters), int(flip), _ptr(out))
+    return out
+
+
+def draft_reduce(planes, levels):
+    """prep.rs:77 `reduce`: (3, h, w) f32 planes block-averaged by 2^levels."""
+    a = c32(planes)
+    h, w = a.shape[1:]
+    k = 1 << levels
+    out = np.empty((3, max(-(-h // k), 1), max(-(-w // k), 1)), F32)
+    lib().orc_draft_reduce_f(_ptr(a), w, h, int(levels), _ptr(out))
+    return out
+
+
+def prep_rgb16(rgb, dust: DustMap | None = None, rotate=0, draft=0, size=None):
+    """lapstack-web lib.rs:766-784 on an interleaved (h, w, 3) u16 frame: the dust map (frames of its size
+    only), the quarter turns, the draft block mean (decode.rs:68, 92) and, with size = (w, h), the run's
+    size (decode.rs:125 bilinear)."""
+    f = np.ascontiguousarray(rgb, dtype=np.uint16)
+    h, w = f.shape[:2]
+    rects, n, masks, gains, mode = _dust_arrays(dust) if dust is not None else (np.zeros((1, 4), np.uint64), 0, np.zeros(1, np.uint8),
+                                                                                  np.zeros(1, F32), 0)
+    mw, mh = (dust.w, dust.h) if dust is not None else (0, 0)
+    rw, rh = size if size is not None else (0, 0)
+    dims = np.zeros(2, np.uint64)
+    L = lib()
+    L.orc_prep_rgb16(_ptr(rects), n, _ptr(masks), _ptr(gains), mw, mh, mode, int(rotate), int(draft), _ptr(f), w, h, rw, rh, None, _ptr(dims))
+    out = np.empty((int(dims[1]), int(dims[0]), 3), np.uint16)
+    L.orc_prep_rgb16(_ptr(rects), n, _ptr(masks), _ptr(gains), mw, mh, mode, int(rotate), int(draft), _ptr(f), w, h, rw, rh, _ptr(out),
+                     _ptr(dims))
+    return out

@@ -4,6 +4,7 @@
 #include <array>
 #include "orc_stack.hpp"
 #include "orc_synth.hpp"
+#include "orc_dust.hpp"
 #include <omp.h>
 
 using namespace orc;
@@ -562,6 +563,76 @@ void orc_resize_f(const float* src, size_t planes, size_t pw, size_t ph, size_t 
         std::vector<float> o = resize_plane<float>(src + c * pw * ph, pw, ph, w, h, interp);
         std::copy(o.begin(), o.end(), out + c * w * h);
     }
+}
+
+// a dust map from flat arrays: rects [n][4] (x, y, w, h), the masks and (flat mode) the gains concatenated
+static DustMap dust_of(const uint64_t* rects, size_t n, const uint8_t* masks, const float* gains, size_t mw, size_t mh, int mode) {
+    DustMap m;
+    m.w = mw;
+    m.h = mh;
+    m.mode = mode;
+    size_t off = 0;
+    for (size_t k = 0; k < n; k++) {
+        DustSpot s;
+        s.x = rects[4 * k];
+        s.y = rects[4 * k + 1];
+        s.w = rects[4 * k + 2];
+        s.h = rects[4 * k + 3];
+        s.mask.assign(masks + off, masks + off + s.w * s.h);
+        if (gains) s.gain.assign(gains + off, gains + off + s.w * s.h);
+        else s.gain.assign(s.w * s.h, 1.0f);
+        off += s.w * s.h;
+        m.spots.push_back(std::move(s));
+    }
+    return m;
+}
+
+// dust.rs:487 apply_rgb16 in place on an interleaved u16 frame (w x h; a frame of another size is left alone)
+void orc_dust_apply_rgb16(const uint64_t* rects, size_t n, const uint8_t* masks, const float* gains, size_t mw, size_t mh, int mode,
+                          uint16_t* rgb, size_t w, size_t h) {
+    dust_apply_rgb16(dust_of(rects, n, masks, gains, mw, mh, mode), rgb, w, h);
+}
+
+// dust.rs:478 apply in place on planar f32 planes [3][h][w]
+void orc_dust_apply_f(const uint64_t* rects, size_t n, const uint8_t* masks, const float* gains, size_t mw, size_t mh, int mode,
+                      float* planes, size_t w, size_t h) {
+    Img3<float> f(w, h);
+    for (int c = 0; c < 3; c++) std::copy(planes + c * w * h, planes + (c + 1) * w * h, f.p[c].begin());
+    dust_apply(dust_of(rects, n, masks, gains, mw, mh, mode), f);
+    for (int c = 0; c < 3; c++) std::copy(f.p[c].begin(), f.p[c].end(), planes + c * w * h);
+}
+
+// dust.rs:591 pull_push (f32)
+void orc_pull_push_f(const float* v, const float* wt, size_t w, size_t h, float* out) {
+    std::vector<float> a(v, v + w * h), b(wt, wt + w * h);
+    std::vector<float> f = pull_push<float>(a, b, w, h);
+    std::copy(f.begin(), f.end(), out);
+}
+
+// prep.rs:16 rotate and prep.rs:77 reduce of planar f32 planes; out sized by the caller
+void orc_rotate_f(const float* planes, size_t w, size_t h, int quarters, int flip, float* out) {
+    Img3<float> f(w, h);
+    for (int c = 0; c < 3; c++) std::copy(planes + c * w * h, planes + (c + 1) * w * h, f.p[c].begin());
+    Img3<float> o = rotate(f, quarters, flip != 0);
+    for (int c = 0; c < 3; c++) std::copy(o.p[c].begin(), o.p[c].end(), out + c * o.w * o.h);
+}
+void orc_draft_reduce_f(const float* planes, size_t w, size_t h, int levels, float* out) {
+    Img3<float> f(w, h);
+    for (int c = 0; c < 3; c++) std::copy(planes + c * w * h, planes + (c + 1) * w * h, f.p[c].begin());
+    Img3<float> o = draft_reduce(f, levels);
+    for (int c = 0; c < 3; c++) std::copy(o.p[c].begin(), o.p[c].end(), out + c * o.w * o.h);
+}
+
+// lapstack-web lib.rs:766-784 on an interleaved u16 frame: the dust map (n_spots 0: none), the turn, the draft
+// reduction and the run's size (rw, rh; 0: as prepared); out sized by the caller, its dims into odims[2]
+void orc_prep_rgb16(const uint64_t* rects, size_t n, const uint8_t* masks, const float* gains, size_t mw, size_t mh, int mode, int quarters,
+                    int draft, const uint16_t* in, size_t w, size_t h, size_t rw, size_t rh, uint16_t* out, uint64_t* odims) {
+    DustMap m = dust_of(rects, n, masks, gains, mw, mh, mode);
+    size_t ow, oh;
+    std::vector<uint16_t> f = prep_rgb16(n ? &m : nullptr, quarters, draft, std::vector<uint16_t>(in, in + w * h * 3), w, h, rw, rh, ow, oh);
+    if (out) std::copy(f.begin(), f.end(), out);
+    odims[0] = ow;
+    odims[1] = oh;
 }
 
 // f32 -> IEEE half bits (round to nearest even) and back, as the 16-bit storage emulation does them
