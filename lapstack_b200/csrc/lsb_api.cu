@@ -276,12 +276,16 @@ static char* engine_init(lsb_engine* e) {
         return dup_err(fmt("lapstack-b200 is built for sm_100a; device %d is sm_%d%d", e->device, prop.major, prop.minor));
     e->sms = prop.multiProcessorCount;
     e->grid = e->cfg.grid_limit > 0 ? e->cfg.grid_limit : 2 * e->sms;
-    TRY(cudaStreamCreateWithFlags(&e->s, cudaStreamNonBlocking));
+    // The registration chain (on s, its targets on bs) sets the pace of an aligned stack: its blocks go
+    // first when the per-frame warps, sums and fold chunks on ws wait for room on the SMs.
+    int prio_low = 0, prio_high = 0;
+    TRY(cudaDeviceGetStreamPriorityRange(&prio_low, &prio_high));
+    TRY(cudaStreamCreateWithPriority(&e->s, cudaStreamNonBlocking, prio_high));
     TRY(cudaStreamCreateWithFlags(&e->cs, cudaStreamNonBlocking));
     TRY(cudaEventCreateWithFlags(&e->s_mark, cudaEventDisableTiming));
-    TRY(cudaStreamCreateWithFlags(&e->bs, cudaStreamNonBlocking));
+    TRY(cudaStreamCreateWithPriority(&e->bs, cudaStreamNonBlocking, prio_high));
     TRY(cudaStreamCreateWithFlags(&e->rs, cudaStreamNonBlocking));
-    TRY(cudaStreamCreateWithFlags(&e->ws, cudaStreamNonBlocking));
+    TRY(cudaStreamCreateWithPriority(&e->ws, cudaStreamNonBlocking, prio_low));
     TRY(e->pool.get(&e->hist, 65536));
     TRY(e->pool.get(&e->sel, 4));
     TRY(e->pool.get(&e->scal, 16));
