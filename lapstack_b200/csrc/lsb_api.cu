@@ -990,9 +990,8 @@ static char* stream_warps(lsb_stack* s, bool pushed, bool reduce, bool select) {
             B.ident = sim_is_id(sim);
             B.affine = B.inv[6] == 0.0 && B.inv[7] == 0.0 && B.inv[8] == 1.0;
             TRY(cudaMemcpyAsync(s->bx_dev + i, &B, sizeof B, cudaMemcpyHostToDevice, e->ws));
-            // pushed frames: the whole GPU; frames in memory: a few blocks beside the registration chain
-            TRY(bright_sums_frame(s->frames, i, W, H, s->bx_dev, (int)s->ap.interp, BRIGHT_PARTS, s->bpart, pushed ? BRIGHT_PARTS : 64,
-                                  e->ws));
+            // one short block per part: on the low-priority stream, freed SMs go to the chain's search first
+            TRY(bright_sums_frame(s->frames, i, W, H, s->bx_dev, (int)s->ap.interp, BRIGHT_PARTS, s->bpart, BRIGHT_PARTS, e->ws));
             TRY(frame_gain(s->bpart, i, BRIGHT_PARTS, s->xf_dev + i, e->ws));
         }
         for (int l = 0; l < s->levels && reduce && !select; l++) {
