@@ -316,6 +316,9 @@ void lsb_unet_sizes(const lsb_unet* u, uint64_t* n_weights, uint64_t* n_biases);
 /* host copies of the FP32 master weights/biases and of the last step's gradients (any may be NULL) */
 char* lsb_unet_get_params(lsb_unet* u, float* w, float* b, float* gw, float* gb);
 char* lsb_unet_set_params(lsb_unet* u, const float* w, const float* b);
+/* The 3x3 convolutions' tensor-core path: 0 (the default) tcgen05 MMAs with TMEM accumulators, 1 the
+   mma.sync path (the same products, another summation order; kept for comparison). */
+char* lsb_unet_set_conv(lsb_unet* u, uint32_t path);
 /* network grid of a dw x dh depth grid: ceil(d/2) rounded up to a multiple of 8 */
 void lsb_unet_grid(uint32_t dw, uint32_t dh, uint32_t* H, uint32_t* W);
 /* device planes (dw x dh) -> batch entry b of in_dev [B][H][W][32] bf16 and d_in_dev [B][H][W] f32 (= d / dmax) */

@@ -122,6 +122,7 @@ SIGNATURES = {
     "lsb_unet_sizes": (None, [P, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
     "lsb_unet_get_params": (ERR, [P, P, P, P, P]),
     "lsb_unet_set_params": (ERR, [P, P, P]),
+    "lsb_unet_set_conv": (ERR, [P, C.c_uint32]),
     "lsb_unet_grid": (None, [C.c_uint32, C.c_uint32, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]),
     "lsb_unet_prepare": (ERR, [P, P, P, C.c_uint32, C.c_uint32, C.c_float, P, P, C.c_uint32, P]),
     "lsb_unet_forward": (ERR, [P, P, P, C.c_uint32, C.c_uint32, C.c_uint32, P]),

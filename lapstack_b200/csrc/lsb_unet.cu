@@ -196,6 +196,166 @@ __global__ void __launch_bounds__(UN_THREADS) conv3x3_kernel(const ConvArgs a) {
     }
 }
 
+// ------------------------------------------------- the same conv on tcgen05
+// conv3x3_tc_kernel: the implicit GEMM on the 5th-generation tensor cores. A CTA of 4 warps owns a
+// 16 x 8 tile of output pixels (M = 128, one TMEM lane per pixel) and N = cout output channels (one
+// fp32 TMEM column each). Per 32-channel input chunk every thread stages the 18 x 10 input halo and
+// the chunk's 9 x N x 32 weights in shared memory in the canonical no-swizzle K-major layout of the
+// UMMA operand descriptors (8 rows of 16 bytes per core matrix): the halo as [k8][pixel][8 channels],
+// so that the tap (ky, kx) of the A operand is the same layout started (ky * 10 + kx) pixels later
+// (rows of 8 pixels 10 pixels apart: SBO = 160 B, the next 8 channels LBO = 180 pixels further);
+// the weights as [tap][k8][n][8]. One thread issues the 9 taps x 2 K-steps of tcgen05.mma
+// (kind::f16, BF16 x BF16 -> FP32 in TMEM) and commits them to an mbarrier that every thread waits
+// on (bounded) before the staging of the next chunk; the epilogue reads the accumulator with
+// tcgen05.ld (warp w: lanes 32w..32w+31), adds the bias, applies ReLU and stores NHWC.
+constexpr int TC_TH = 16, TC_TW = 8;
+constexpr int TC_HP = TC_TH + 2, TC_WP = TC_TW + 2, TC_PIX = TC_HP * TC_WP;  // 18 x 10 halo
+constexpr unsigned TC_SPIN_LIMIT = 1u << 24;
+
+__host__ __device__ constexpr size_t tc_a_bytes() { return (size_t)4 * TC_PIX * 16; }
+__host__ __device__ constexpr size_t tc_b_bytes(int n) { return (size_t)9 * 4 * n * 16; }
+// A, B, the mbarrier and the TMEM address slot
+__host__ __device__ constexpr size_t tc_smem_bytes(int n) { return tc_a_bytes() + tc_b_bytes(n) + 16; }
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+// the UMMA shared-memory descriptor, no swizzle (layout type 0), version 1; addresses and offsets in bytes
+__device__ __forceinline__ uint64_t umma_desc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
+    return (uint64_t)((addr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) | ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) |
+           (1ull << 46);
+}
+// the instruction descriptor of kind::f16: D f32, A and B bf16, both K-major, M = 128, N
+__host__ __device__ constexpr uint32_t umma_idesc_bf16(int n) {
+    return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(128 >> 4) << 24);
+}
+
+template <int N>
+__global__ void __launch_bounds__(UN_THREADS) conv3x3_tc_kernel(const ConvArgs a, int* status) {
+    extern __shared__ __align__(128) unsigned char tc_smem[];
+    unsigned char* As = tc_smem;
+    unsigned char* Bs = tc_smem + tc_a_bytes();
+    uint64_t* mbar = reinterpret_cast<uint64_t*>(Bs + tc_b_bytes(N));
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(mbar + 1);
+    const int tiles_x = (a.W + TC_TW - 1) / TC_TW;
+    const int x0 = (blockIdx.x % tiles_x) * TC_TW, y0 = (blockIdx.x / tiles_x) * TC_TH;
+    const int n0 = blockIdx.y * N, b = blockIdx.z;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    constexpr uint32_t COLS = N < 32 ? 32 : N;
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tslot)), "r"(COLS));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    if (tid == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(mbar)), "r"(1));
+        asm volatile("fence.mbarrier_init.release.cluster;");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;");
+    const uint32_t tmem = *tslot;
+    const uint32_t a_base = smem_u32(As), b_base = smem_u32(Bs);
+    constexpr uint32_t IDESC = umma_idesc_bf16(N);
+    bool ok = true;
+    int chunk = 0;
+    for (int c0 = 0; c0 < a.cin; c0 += UN_CH, chunk++) {
+        const bool first = c0 < a.c1;
+        const __nv_bfloat16* src = first ? a.src1 : a.src2;
+        const int cs = first ? a.c1s : a.c2s, mode = first ? a.mode1 : a.mode2, cb = first ? c0 : c0 - a.c1;
+        // the halo: [k8][pixel][8 channels], zero outside the image
+        for (int i = tid; i < TC_PIX * 4; i += UN_THREADS) {
+            const int pix = i >> 2, v = i & 3;
+            const int yy = y0 - 1 + pix / TC_WP, xx = x0 - 1 + pix % TC_WP;
+            uint4 val = make_uint4(0u, 0u, 0u, 0u);
+            if (yy >= 0 && yy < a.H && xx >= 0 && xx < a.W) val = load8(src, cs, mode, b, yy, xx, a.H, a.W, cb + 8 * v);
+            *reinterpret_cast<uint4*>(As + ((size_t)v * TC_PIX + pix) * 16) = val;
+        }
+        // the weights: [tap][k8][n][8]
+        for (int i = tid; i < 9 * N * 4; i += UN_THREADS) {
+            const int v = i & 3, row = i >> 2, tap = row / N, n = row % N;
+            const uint4 val = *reinterpret_cast<const uint4*>(a.w + ((size_t)tap * a.cout + n0 + n) * a.cin + c0 + 8 * v);
+            *reinterpret_cast<uint4*>(Bs + (((size_t)tap * 4 + v) * N + n) * 16) = val;
+        }
+        // the generic-proxy stores, visible to the tensor cores' async proxy
+        asm volatile("fence.proxy.async.shared::cta;");
+        __syncthreads();
+        if (tid == 0) {
+            asm volatile("tcgen05.fence::after_thread_sync;");
+#pragma unroll 1
+            for (int tap = 0; tap < 9; tap++) {
+                const int ky = tap / 3, kx = tap % 3;
+#pragma unroll
+                for (int j = 0; j < 2; j++) {
+                    const uint64_t da = umma_desc(a_base + (uint32_t)((2 * j * TC_PIX + ky * TC_WP + kx) * 16), TC_PIX * 16, TC_WP * 16);
+                    const uint64_t db = umma_desc(b_base + (uint32_t)(((tap * 4 + 2 * j) * N) * 16), N * 16, 8 * 16);
+                    const uint32_t acc = (chunk > 0 || tap > 0 || j > 0) ? 1u : 0u;
+                    asm volatile(
+                        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+                        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem),
+                        "l"(da), "l"(db), "r"(IDESC), "r"(acc));
+                }
+            }
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(mbar)) : "memory");
+        }
+        // every thread: the chunk's MMAs are done (their shared-memory reads too) before the next staging
+        uint32_t done = 0;
+        for (unsigned it = 0; it < TC_SPIN_LIMIT && !done; it++)
+            asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}\n"
+                         : "=r"(done)
+                         : "r"(smem_u32(mbar)), "r"((uint32_t)(chunk & 1)));
+        if (!done) {
+            ok = false;
+            break;
+        }
+    }
+    if (!ok) {
+        // the wait ran out: flag it, give the MMAs in flight a second bounded wait, free the TMEM, return
+        if (tid == 0) atomicOr(status, 0x100);
+        uint32_t done = 0;
+        for (unsigned it = 0; it < TC_SPIN_LIMIT && !done; it++)
+            asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}\n"
+                         : "=r"(done)
+                         : "r"(smem_u32(mbar)), "r"((uint32_t)(chunk & 1)));
+    } else {
+        asm volatile("tcgen05.fence::after_thread_sync;");
+        // epilogue: pixel m = 32 warp + lane = (row m / 8, column m % 8); 8 channels per load
+        const int m = 32 * warp + lane, y = y0 + m / TC_TW, x = x0 + m % TC_TW;
+        const bool in = y < a.H && x < a.W;
+        const size_t pix = ((size_t)b * a.H + y) * a.W + x;
+#pragma unroll 1
+        for (int c = 0; c < N; c += 8) {
+            uint32_t r[8];
+            asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+                         : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
+                         : "r"(tmem + ((uint32_t)(32 * warp) << 16) + (uint32_t)c));
+            asm volatile("tcgen05.wait::ld.sync.aligned;");
+            if (!in) continue;
+            float v[8];
+#pragma unroll
+            for (int q = 0; q < 8; q++) {
+                v[q] = __uint_as_float(r[q]);
+                if (a.bias) v[q] += a.bias[n0 + c + q];
+                if (a.relu) v[q] = fmaxf(v[q], 0.f);
+            }
+            const int n = n0 + c;
+            if (a.out) {
+                uint4 o;
+                __nv_bfloat162* h = reinterpret_cast<__nv_bfloat162*>(&o);
+#pragma unroll
+                for (int q = 0; q < 4; q++) h[q] = __floats2bfloat162_rn(v[2 * q], v[2 * q + 1]);
+                *reinterpret_cast<uint4*>(a.out + pix * a.cout + n) = o;
+            }
+            if (a.out_f32) {
+                float4* o = reinterpret_cast<float4*>(a.out_f32 + pix * a.cout + n);
+                o[0] = make_float4(v[0], v[1], v[2], v[3]);
+                o[1] = make_float4(v[4], v[5], v[6], v[7]);
+            }
+            if (a.out_c0 && n == 0) a.out_c0[pix] = v[0];
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;");
+    __syncthreads();
+    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(COLS));
+}
+
 // ------------------------------------------------------------ backward parts
 // dZ = dY * (Y > 0) rounded to bf16 (the operand of the dX conv and dW)
 __global__ void relu_grad_kernel(const float* __restrict__ dy, const __nv_bfloat16* __restrict__ y, __nv_bfloat16* __restrict__ dz,
@@ -448,6 +608,8 @@ struct lsb_unet {
     double* loss = nullptr;
     double* loss_host = nullptr;
     std::vector<void*> shape_allocs;
+    int* status = nullptr;  // device error word of the tcgen05 convolution (a bounded wait ran out)
+    bool tc = true;         // the 3x3 convolutions on tcgen05 (false: mma.sync, for comparison)
 };
 
 static char* un_err(const std::string& s) {
@@ -519,7 +681,27 @@ static cudaError_t ensure_shape(lsb_unet* u, int B, int H, int W, bool train) {
     return cudaSuccess;
 }
 
-static cudaError_t conv_launch(const ConvArgs& a, cudaStream_t s) {
+template <int N>
+static cudaError_t conv_tc_launch(const ConvArgs& a, int* status, cudaStream_t s) {
+    const size_t smem = tc_smem_bytes(N);
+    cudaError_t e = cudaFuncSetAttribute(conv3x3_tc_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    const dim3 grid(((a.W + TC_TW - 1) / TC_TW) * ((a.H + TC_TH - 1) / TC_TH), a.cout / N, a.B);
+    lsb_launched(), conv3x3_tc_kernel<N><<<grid, UN_THREADS, smem, s>>>(a, status);
+    return cudaGetLastError();
+}
+
+static cudaError_t conv_launch(const ConvArgs& a, cudaStream_t s, int* status = nullptr, bool tc = false) {
+    // tcgen05: every layer's cin is a multiple of 32 and its cout 32, 64, 128 or 256 (one CTA takes them all)
+    if (tc && status && a.cin % UN_CH == 0) {
+        switch (a.cout) {
+            case 32: return conv_tc_launch<32>(a, status, s);
+            case 64: return conv_tc_launch<64>(a, status, s);
+            case 128: return conv_tc_launch<128>(a, status, s);
+            case 256: return conv_tc_launch<256>(a, status, s);
+            default: break;
+        }
+    }
     const int NT = a.cout % 64 == 0 ? 64 : 32;
     const size_t smem = (size_t)(UN_HP * UN_WP + 9 * NT) * UN_LD * sizeof(__nv_bfloat16);
     const dim3 grid(((a.W + UN_TW - 1) / UN_TW) * ((a.H + UN_TH - 1) / UN_TH), a.cout / NT, a.B);
@@ -561,7 +743,7 @@ static cudaError_t unet_forward(lsb_unet* u) {
         a.out = last ? nullptr : u->act[i + 1];
         a.out_c0 = last ? u->out0 : nullptr;
         if (last) a.out = u->act[i + 1];
-        cudaError_t e = conv_launch(a, u->s);
+        cudaError_t e = conv_launch(a, u->s, u->status, u->tc);
         if (e != cudaSuccess) return e;
     }
     return cudaSuccess;
@@ -616,7 +798,8 @@ extern "C" char* lsb_unet_create(int32_t device, uint64_t seed, lsb_unet** out) 
               alloc((void**)&u->vw, u->nw * 4) && alloc((void**)&u->b, u->nb * 4) && alloc((void**)&u->gb, u->nb * 4) &&
               alloc((void**)&u->mb, u->nb * 4) && alloc((void**)&u->vb, u->nb * 4) && alloc((void**)&u->wmask, u->nw) &&
               alloc((void**)&u->bmask, u->nb) && alloc((void**)&u->wb, u->nw * 2) && alloc((void**)&u->wt, u->nw * 2) &&
-              alloc((void**)&u->loss, 8) && cudaHostAlloc((void**)&u->loss_host, 8, cudaHostAllocDefault) == cudaSuccess &&
+              alloc((void**)&u->loss, 8) && alloc((void**)&u->status, 4) &&
+              cudaHostAlloc((void**)&u->loss_host, 8, cudaHostAllocDefault) == cudaSuccess &&
               cudaStreamCreateWithFlags(&u->s, cudaStreamNonBlocking) == cudaSuccess;
     if (!ok) {
         lsb_unet_destroy(u);
@@ -641,11 +824,29 @@ extern "C" void lsb_unet_destroy(lsb_unet* u) {
     if (u->s) cudaStreamSynchronize(u->s);
     free_shape(u);
     for (void* p : {(void*)u->w, (void*)u->gw, (void*)u->mw, (void*)u->vw, (void*)u->b, (void*)u->gb, (void*)u->mb, (void*)u->vb,
-                    (void*)u->wmask, (void*)u->bmask, (void*)u->wb, (void*)u->wt, (void*)u->loss})
+                    (void*)u->wmask, (void*)u->bmask, (void*)u->wb, (void*)u->wt, (void*)u->loss, (void*)u->status})
         if (p) cudaFree(p);
     if (u->loss_host) cudaFreeHost(u->loss_host);
     if (u->s) cudaStreamDestroy(u->s);
     delete u;
+}
+
+// The device error word: a tcgen05 convolution whose bounded wait ran out (its output is not written).
+static char* conv_status(lsb_unet* u) {
+    int st = 0;
+    UTRY(cudaMemcpy(&st, u->status, sizeof st, cudaMemcpyDeviceToHost));
+    if (st) {
+        cudaMemset(u->status, 0, sizeof st);
+        return un_err("unet: a tensor-core convolution's wait for its MMAs ran out");
+    }
+    return nullptr;
+}
+
+extern "C" char* lsb_unet_set_conv(lsb_unet* u, uint32_t path) {
+    if (!u) return un_err("unet: null network");
+    if (path > 1) return un_err("unet: conv path must be 0 (tcgen05) or 1 (mma.sync)");
+    u->tc = path == 0;
+    return nullptr;
 }
 
 extern "C" void lsb_unet_sizes(const lsb_unet* u, uint64_t* n_weights, uint64_t* n_biases) {
@@ -686,7 +887,7 @@ extern "C" char* lsb_unet_forward(lsb_unet* u, const void* in_dev, const float* 
     UTRY(unet_forward(u));
     if (out0_dev) UTRY(cudaMemcpyAsync(out0_dev, u->out0, (size_t)B * H * W * 4, cudaMemcpyDeviceToDevice, u->s));
     UTRY(cudaStreamSynchronize(u->s));
-    return nullptr;
+    return conv_status(u);
 }
 
 static cudaError_t unet_backward(lsb_unet* u) {
@@ -722,7 +923,7 @@ static cudaError_t unet_backward(lsb_unet* u) {
         d.B = a.B;
         d.H = a.H;
         d.W = a.W;
-        cudaError_t e = conv_launch(d, u->s);
+        cudaError_t e = conv_launch(d, u->s, u->status, u->tc);
         if (e != cudaSuccess) return e;
         const size_t s1px = (size_t)a.B * (u->H >> act_level(u, l.src1)) * (u->W >> act_level(u, l.src1));
         lsb_launched(), route_kernel<<<ugrid(s1px * l.c1), 256, 0, u->s>>>(u->dxbuf, cin, 0, l.c1, u->grad[l.src1],
@@ -758,7 +959,7 @@ extern "C" char* lsb_unet_train_step(lsb_unet* u, const void* in_dev, const floa
     UTRY(cudaMemcpyAsync(u->loss_host, u->loss, 8, cudaMemcpyDeviceToHost, u->s));
     UTRY(cudaStreamSynchronize(u->s));
     if (loss_out) *loss_out = *u->loss_host;
-    return nullptr;
+    return conv_status(u);
 }
 
 // The network input of one depth grid (device planes dw x dh): in [H][W][32]

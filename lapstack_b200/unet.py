@@ -82,6 +82,11 @@ class UNet:
         assert w.size == self.n_weights and b.size == self.n_biases
         check(self._L.lsb_unet_set_params(self._h, C.c_void_p(w.ctypes.data), C.c_void_p(b.ctypes.data)))
 
+    def set_conv(self, path: str = "tcgen05"):
+        """The 3x3 convolutions' tensor-core path: "tcgen05" (the default; TMEM accumulators) or
+        "mma.sync" (the same products summed in another order, for comparison)."""
+        check(self._L.lsb_unet_set_conv(self._h, {"tcgen05": 0, "mma.sync": 1}[path]))
+
     def save(self, path):
         w, b = self.params()
         np.savez(path, w=w, b=b)

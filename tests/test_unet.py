@@ -142,3 +142,34 @@ def test_training_fits_a_fixed_batch():
     for _ in range(150):
         last = net.train_step(*t, lr=2e-3)
     assert last < 0.2 * first, (first, last)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("shape", [(1, 8, 8), (2, 40, 56), (1, 64, 128)])
+def test_tcgen05_convolutions_match_the_mma_sync_path(shape):
+    """The 3x3 convolutions on tcgen05 (TMEM accumulators, the default) against the mma.sync path on the
+    same parameters and inputs: the same bf16 products summed in another order, so the forward output
+    agrees to bf16 rounding (partial 16 x 8 tiles at every level of the shapes here) and the gradients
+    of one step too; both are held to the oracle as above."""
+    import lapstack_b200 as L
+    B, H, W = shape
+    w, b = U.init_params(17)
+    inp, d_in, tgt = _case(19, B, H, W)
+    outs, grads = {}, {}
+    for path in ("tcgen05", "mma.sync"):
+        net = L.UNet(seed=0)
+        net.set_conv(path)
+        net.set_params(w, b)
+        t = _to_gpu(inp, d_in, tgt)
+        outs[path] = net.forward(*t[:2]).cpu().numpy()
+        net.train_step(*t, lr=0.0)
+        grads[path] = net.grads()[0]
+        net.close()
+    a, m = outs["tcgen05"], outs["mma.sync"]
+    scale = max(float(np.abs(m).max()), 1e-3)
+    assert np.abs(a - m).max() <= 1e-2 * scale, (np.abs(a - m).max(), scale)
+    assert np.corrcoef(a.ravel(), m.ravel())[0, 1] > 0.9999
+    ga, gm = grads["tcgen05"], grads["mma.sync"]
+    assert np.linalg.norm(ga - gm) <= 2e-2 * np.linalg.norm(gm)
+    _, ref = U.forward(inp, w, b)
+    assert np.abs(a - ref).max() <= 2e-2 * max(float(np.abs(ref).max()), 1e-3)
