@@ -74,6 +74,8 @@ struct DevPool {
 constexpr int BRIGHT_PARTS = 512;
 // Frames per selection chunk when the fold runs on the side stream as the transforms land.
 constexpr int SEL_CHUNK = 10;
+// Frames of the last selection chunk (it folds after the last frame lands).
+constexpr int SEL_TAIL = 4;
 
 struct lsb_engine {
     lsb_config cfg;
@@ -463,7 +465,7 @@ static char* stack_alloc(lsb_stack* s) {
         for (auto& v : s->searched) TRY(cudaEventCreateWithFlags(&v, cudaEventDisableTiming));
         for (auto& v : s->sims_back) TRY(cudaEventCreateWithFlags(&v, cudaEventDisableTiming));
         TRY(cudaEventCreateWithFlags(&s->wdone, cudaEventDisableTiming));
-        s->chunk_ev.assign(3 * ((N + SEL_CHUNK - 1) / SEL_CHUNK), nullptr);
+        s->chunk_ev.assign(3 * ((N + SEL_CHUNK - 1) / SEL_CHUNK + 1), nullptr);
         for (auto& v : s->chunk_ev) TRY(cudaEventCreate(&v));
     }
     s->copied.assign(N, nullptr);
@@ -1003,11 +1005,16 @@ static char* stream_warps(lsb_stack* s, bool pushed, bool reduce, bool select) {
             a.select = 0;
             TRY(fold_level(a, src, s->storage, (int)s->fp.energy_radius, focus, e->ws, e->grid));
         }
-        if (reduce && select && (i + 1 - sel_from == SEL_CHUNK || i + 1 == n)) {
+        // chunks of SEL_CHUNK frames, the stack's last SEL_TAIL frames a chunk of their own: what is left
+        // to fold once the last frame lands is small
+        const bool cut = i + 1 - sel_from == SEL_CHUNK || i + 1 == n || (n > 2 * SEL_TAIL && i + 1 == n - SEL_TAIL);
+        if (reduce && select && cut) {
             // the chunk's frames level by level: their REDUCE (and focus slices), then their selection
             // (level 0: one fused kernel where it applies), beside the registration chain: one
-            // persistent CTA per SM, so that the chain's cooperative search keeps room on every SM
-            const int ch = sel_from / SEL_CHUNK;
+            // persistent CTA per SM, so that the chain's cooperative search keeps room on every SM;
+            // the last chunk, after the chain, on the whole GPU
+            const int ch = s->chunks;
+            const bool last = i + 1 == n;
             for (int l = 0; l < s->levels; l++) {
                 bool focus = false;
                 int src = 0;
@@ -1016,14 +1023,14 @@ static char* stream_warps(lsb_stack* s, bool pushed, bool reduce, bool select) {
                 a.red_n = i + 1 - sel_from;
                 a.sel_k0 = sel_from;
                 a.sel_k1 = i + 1;
-                a.beside = 1;
+                a.beside = last ? 0 : 1;
                 set_groups(s, a);
                 if (l == 0) {  // the level-0 fold of the chunk, timed: [start, after the fused kernel, end]
                     TRY(cudaEventRecord(s->chunk_ev[3 * ch], e->ws));
                     TRY(cudaEventRecord(s->chunk_ev[3 * ch + 1], e->ws));
                     a.after_fused = s->chunk_ev[3 * ch + 1];
                 }
-                TRY(fold_level(a, src, s->storage, (int)s->fp.energy_radius, focus, e->ws, e->sms));
+                TRY(fold_level(a, src, s->storage, (int)s->fp.energy_radius, focus, e->ws, last ? e->grid : e->sms));
                 if (l == 0) TRY(cudaEventRecord(s->chunk_ev[3 * ch + 2], e->ws));
             }
             s->chunks = ch + 1;
