@@ -210,7 +210,9 @@ __global__ void __launch_bounds__(UN_THREADS) conv3x3_kernel(const ConvArgs a) {
 // tcgen05.ld (warp w: lanes 32w..32w+31), adds the bias, applies ReLU and stores NHWC.
 constexpr int TC_TH = 16, TC_TW = 8;
 constexpr int TC_HP = TC_TH + 2, TC_WP = TC_TW + 2, TC_PIX = TC_HP * TC_WP;  // 18 x 10 halo
-constexpr unsigned TC_SPIN_LIMIT = 1u << 24;
+// try_wait polls per wait: far beyond a chunk's MMAs (microseconds); a CTA that meets a set error word
+// (an earlier wait ran out) does nothing
+constexpr unsigned TC_SPIN_LIMIT = 1u << 20;
 
 __host__ __device__ constexpr size_t tc_a_bytes() { return (size_t)4 * TC_PIX * 16; }
 __host__ __device__ constexpr size_t tc_b_bytes(int n) { return (size_t)9 * 4 * n * 16; }
@@ -240,6 +242,7 @@ __global__ void __launch_bounds__(UN_THREADS) conv3x3_tc_kernel(const ConvArgs a
     const int n0 = blockIdx.y * N, b = blockIdx.z;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     constexpr uint32_t COLS = N < 32 ? 32 : N;
+    if (*(volatile int*)status) return;  // an earlier CTA's wait ran out: nothing is allocated yet
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tslot)), "r"(COLS));
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");

@@ -164,6 +164,58 @@ __global__ void prolong_kernel(float* __restrict__ x, int w, int h, const float*
     x[k] = __fadd_rn(x[k], xc[(size_t)(y / 2) * cw + i / 2]);
 }
 
+// One fine level's way down the V-cycle in one pass (depth.rs:924-930): the zero-start Jacobi sweep
+// x = w D^-1 b (depth.rs:840), the residual b - A x (depth.rs:786) and its restriction to the coarse
+// right-hand side (depth.rs:911), one thread per coarse cell and its 2x2 fine cells; the neighbours'
+// x are recomputed from b and D^-1 by the same product, so every value is the separate kernels' own.
+__device__ __forceinline__ float jac0_at(const float* __restrict__ b, const float* __restrict__ dinv, size_t k) {
+    return __fmul_rn(__fmul_rn(MG_OMEGA, dinv[k]), b[k]);
+}
+__global__ void vc_down_kernel(const float* __restrict__ b, const float* __restrict__ wd, const float* __restrict__ ax,
+                               const float* __restrict__ ay, const float* __restrict__ dinv, float* __restrict__ x, int w, int h,
+                               float* __restrict__ cb, int cw, int ch) {
+    const int xx = blockIdx.x * blockDim.x + threadIdx.x, yy = blockIdx.y * blockDim.y + threadIdx.y;
+    if (xx >= cw || yy >= ch) return;
+    float o = 0.f;
+    for (int y = 2 * yy; y < min(2 * yy + 2, h); y++) {
+        float rs = 0.f;
+        for (int i = 2 * xx; i < min(2 * xx + 2, w); i++) {
+            const size_t k = (size_t)y * w + i;
+            const float xk = jac0_at(b, dinv, k);
+            x[k] = xk;
+            float v = __fmul_rn(wd[k], xk);
+            if (i > 0) v = __fadd_rn(v, __fmul_rn(ax[k - 1], __fsub_rn(xk, jac0_at(b, dinv, k - 1))));
+            if (i + 1 < w) v = __fadd_rn(v, __fmul_rn(ax[k], __fsub_rn(xk, jac0_at(b, dinv, k + 1))));
+            if (y > 0) v = __fadd_rn(v, __fmul_rn(ay[k - w], __fsub_rn(xk, jac0_at(b, dinv, k - w))));
+            if (y + 1 < h) v = __fadd_rn(v, __fmul_rn(ay[k], __fsub_rn(xk, jac0_at(b, dinv, k + w))));
+            rs = __fadd_rn(rs, __fsub_rn(b[k], v));
+        }
+        o = __fadd_rn(o, rs);
+    }
+    cb[(size_t)yy * cw + xx] = o;
+}
+// ... and its way up in one pass (depth.rs:932-946): the prolongation x += P x_c (depth.rs:901) and the
+// damped Jacobi sweep (depth.rs:837) on the corrected x, the neighbours' corrected x recomputed by the
+// same addition; into out (another buffer than x).
+__device__ __forceinline__ float prolonged_at(const float* __restrict__ x, const float* __restrict__ xc, int w, int cw, size_t k) {
+    const int y = (int)(k / w), i = (int)(k - (size_t)y * w);
+    return __fadd_rn(x[k], xc[(size_t)(y / 2) * cw + i / 2]);
+}
+__global__ void vc_up_kernel(const float* __restrict__ x, const float* __restrict__ xc, int cw, const float* __restrict__ b,
+                             const float* __restrict__ wd, const float* __restrict__ ax, const float* __restrict__ ay,
+                             const float* __restrict__ dinv, float* __restrict__ out, int w, int h) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
+    if (i >= w || y >= h) return;
+    const size_t k = (size_t)y * w + i;
+    const float xk = prolonged_at(x, xc, w, cw, k);
+    float v = __fmul_rn(wd[k], xk);
+    if (i > 0) v = __fadd_rn(v, __fmul_rn(ax[k - 1], __fsub_rn(xk, prolonged_at(x, xc, w, cw, k - 1))));
+    if (i + 1 < w) v = __fadd_rn(v, __fmul_rn(ax[k], __fsub_rn(xk, prolonged_at(x, xc, w, cw, k + 1))));
+    if (y > 0) v = __fadd_rn(v, __fmul_rn(ay[k - w], __fsub_rn(xk, prolonged_at(x, xc, w, cw, k - w))));
+    if (y + 1 < h) v = __fadd_rn(v, __fmul_rn(ay[k], __fsub_rn(xk, prolonged_at(x, xc, w, cw, k + w))));
+    out[k] = __fadd_rn(xk, __fmul_rn(__fmul_rn(MG_OMEGA, dinv[k]), __fsub_rn(b[k], v)));
+}
+
 // The coarse end of the V-cycle (depth.rs:924 `vcycle` from level 0 of `T`
 // down) in ONE CTA: each level's zero-start Jacobi, residual, restriction,
 // the coarsest level's MG_COARSE sweeps, then prolongation and the smoothing
@@ -811,10 +863,30 @@ static void jacobi(WlsLevel& L, bool zero, cudaStream_t s) {
     std::swap(L.x, L.r);
 }
 
-// depth.rs:924 `vcycle`
+static bool tail_level(const WlsSolver* S, size_t l) {
+    return (size_t)S->lv[l].w * S->lv[l].h <= (size_t)MG_TAIL_CELLS && S->lv.size() - l <= (size_t)MG_TAIL_MAX;
+}
+// depth.rs:924 `vcycle` on a level with a coarser one (MG_PRE = MG_POST = 1): down and up in one pass
+// each. The right-hand side is bin (null: the level's b); the result lands in xout (null: the level's
+// x, through its r buffer).
+static void vcycle(WlsSolver* S, size_t l, cudaStream_t s);
+static void vcycle_fused(WlsSolver* S, size_t l, const float* bin, float* xout, cudaStream_t s) {
+    WlsLevel& T = S->lv[l];
+    WlsLevel& C = S->lv[l + 1];
+    const float* b = bin ? bin : T.b;
+    lsb_launched(), vc_down_kernel<<<g2(C.w, C.h), B2, 0, s>>>(b, T.wd, T.ax, T.ay, T.dinv, T.x, T.w, T.h, C.b, C.w, C.h);
+    vcycle(S, l + 1, s);
+    float* out = xout ? xout : T.r;
+    lsb_launched(), vc_up_kernel<<<g2(T.w, T.h), B2, 0, s>>>(T.x, C.x, C.w, b, T.wd, T.ax, T.ay, T.dinv, out, T.w, T.h);
+    if (!xout) std::swap(T.x, T.r);
+}
 static void vcycle(WlsSolver* S, size_t l, cudaStream_t s) {
     WlsLevel& T = S->lv[l];
-    if ((size_t)T.w * T.h <= (size_t)MG_TAIL_CELLS && S->lv.size() - l <= (size_t)MG_TAIL_MAX) {
+    if (l + 1 < S->lv.size() && !tail_level(S, l)) {
+        vcycle_fused(S, l, nullptr, nullptr, s);
+        return;
+    }
+    if (tail_level(S, l)) {
         MgTail tl;
         tl.n = (int)(S->lv.size() - l);
         for (int q = 0; q < tl.n; q++) tl.lv[q] = S->lv[l + q];
@@ -901,6 +973,10 @@ cudaError_t wls_solve(WlsSolver* S, const float* d, int max_iters, float* u, flo
             lsb_launched(), to_bf16_kernel<<<g1(n), 256, 0, s>>>(S->r, L0.hb, n);
             vcycle_h(S, 0, s);
             lsb_launched(), from_bf16_kernel<<<g1(n), 256, 0, s>>>(S->lv[0].hx, S->z, n);
+            return;
+        }
+        if (S->lv.size() > 1 && !tail_level(S, 0)) {  // r in, z out: no copies
+            vcycle_fused(S, 0, S->r, S->z, s);
             return;
         }
         cudaMemcpyAsync(L0.b, S->r, n * sizeof(float), cudaMemcpyDeviceToDevice, s);
