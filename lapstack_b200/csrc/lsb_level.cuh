@@ -170,9 +170,11 @@ __device__ __forceinline__ void reduce_tile(const FoldArgs& a, float* __restrict
     float* g0 = sm;                      // [3][wh][ww]
     float* yl = g0 + 3 * RGW * RGH;      // [wh][ww] focus luma
     float* tmph = yl + RGW * RGH;        // [3][wh][RW]
-    const int xw0 = max(0, 2 * gx0 - FOC_R), xw1 = min(W, 2 * gx0 + 2 * RW + FOC_R);
-    const int yw0 = max(0, 2 * gy0 - FOC_R), yw1 = min(H, 2 * gy0 + 2 * RH + FOC_R);
-    const int ww = IN ? RGW : xw1 - xw0, wh = IN ? RGH : yw1 - yw0;  // interior: the full window
+    // the window of the tile's outputs and the focus taps' reach: RGW x RGH from (xw0, yw0); a border
+    // tile's window is staged with its coordinates reflected into the level (pyramid.rs:51 reflect-101,
+    // the same reflect every tap applies), so every tap below indexes it directly
+    const int xw0 = 2 * gx0 - FOC_R, yw0 = 2 * gy0 - FOC_R;
+    constexpr int ww = RGW, wh = RGH;
     if (SRC == SRC_U16 && IN) {
         // the interleaved u16 window rows copied as words into shared memory (each row from the
         // word at or before its first byte; fold inputs carry tail padding), then converted
@@ -214,19 +216,19 @@ __device__ __forceinline__ void reduce_tile(const FoldArgs& a, float* __restrict
         const GS* f = (const GS*)a.src_g + (size_t)k * 3 * np;
         for (int m = threadIdx.x; m < wh * ww; m += NT) {  // the window's pixels over all threads
             const int r = m / ww, c = m - r * ww;
-            const GS* row = f + (size_t)(yw0 + r) * W + xw0;
+            const GS* px = f + (size_t)RY(yw0 + r) * W + RX(xw0 + c);
             {
                 const int i = r * ww + c;
-                g0[i] = Store<GS>::ld(row + c, sc);
-                g0[RGW * RGH + i] = Store<GS>::ld(row + np + c, sc);
-                g0[2 * RGW * RGH + i] = Store<GS>::ld(row + 2 * np + c, sc);
+                g0[i] = Store<GS>::ld(px, sc);
+                g0[RGW * RGH + i] = Store<GS>::ld(px + np, sc);
+                g0[2 * RGW * RGH + i] = Store<GS>::ld(px + 2 * np, sc);
             }
         }
     } else
     for (int r = ty; r < wh; r += 8)
         for (int c = tx; c < ww; c += 32) {
             float v[3];
-            level_px<SRC, GS>(a, k, xw0 + c, yw0 + r, v);
+            level_px<SRC, GS>(a, k, RX(xw0 + c), RY(yw0 + r), v);
             const int i = r * ww + c;
             g0[i] = v[0];
             g0[RGW * RGH + i] = v[1];
@@ -240,7 +242,7 @@ __device__ __forceinline__ void reduce_tile(const FoldArgs& a, float* __restrict
         const int r = m / ow, j = m - r * ow;
         {
             const int cc = 2 * (gx0 + j);
-            const int i0 = RX(cc - 2) - xw0, i1 = RX(cc - 1) - xw0, i2 = RX(cc) - xw0, i3 = RX(cc + 1) - xw0, i4 = RX(cc + 2) - xw0;
+            const int i0 = cc - 2 - xw0, i1 = i0 + 1, i2 = i0 + 2, i3 = i0 + 3, i4 = i0 + 4;
 #pragma unroll
             for (int c = 0; c < 3; c++) {
                 const float* row = g0 + c * RGW * RGH + r * ww;
@@ -252,7 +254,7 @@ __device__ __forceinline__ void reduce_tile(const FoldArgs& a, float* __restrict
         const int bk = a.bk;
         const int cx0 = (2 * gx0) / bk, cy0 = (2 * gy0) / bk;
         const int cw = min(2 * RW / bk, a.dw - cx0), chh = min(2 * RH / bk, a.dh - cy0);
-        if (IN && bk == 2 && a.rdf13 && a.focus_kind == 0) {
+        if (IN && bk == 2 && a.rdf13 && a.focus_kind == 0) {  // whole 2x2 blocks (interior tiles)
             // the default filter over whole 2x2 blocks (interior tiles): the generic loop, unrolled
             for (int cyy = ty; cyy < RH; cyy += 8)
                 for (int cxx = tx; cxx < RW; cxx += 32) {
@@ -280,23 +282,18 @@ __device__ __forceinline__ void reduce_tile(const FoldArgs& a, float* __restrict
                         float m;
                         if (a.focus_kind == 0) {
                             float s = 0.f;
-                            if (IN && a.rdf13) {
+                            if (a.rdf13) {
                                 s = rdf13(yl + (y - yw0) * RGW + (x - xw0));
-                            } else if (IN) {
+                            } else {
                                 const float* yc = yl + (y - yw0) * RGW + (x - xw0);
                                 for (int q = 0; q < a.ntaps; q++) s = __fadd_rn(s, __fmul_rn(c_tapw[q], yc[c_tapo[q]]));
-                            } else {
-                                for (int q = 0; q < a.ntaps; q++) {
-                                    const int yy = RY(y + (int)c_taps[3 * q]) - yw0, xx = RX(x + (int)c_taps[3 * q + 1]) - xw0;
-                                    s = __fadd_rn(s, __fmul_rn(c_taps[3 * q + 2], yl[yy * ww + xx]));
-                                }
                             }
                             m = fabsf(s);
                         } else {
                             const int st = a.sml_step;
                             const float c = yl[(y - yw0) * ww + x - xw0];
-                            const float l = yl[(y - yw0) * ww + RX(x - st) - xw0], r = yl[(y - yw0) * ww + RX(x + st) - xw0];
-                            const float u = yl[(RY(y - st) - yw0) * ww + x - xw0], d = yl[(RY(y + st) - yw0) * ww + x - xw0];
+                            const float l = yl[(y - yw0) * ww + x - st - xw0], r = yl[(y - yw0) * ww + x + st - xw0];
+                            const float u = yl[(y - st - yw0) * ww + x - xw0], d = yl[(y + st - yw0) * ww + x - xw0];
                             const float c2 = __fmul_rn(2.f, c);
                             m = __fadd_rn(fabsf(__fsub_rn(__fsub_rn(c2, l), r)), fabsf(__fsub_rn(__fsub_rn(c2, u), d)));
                         }
@@ -312,7 +309,7 @@ __device__ __forceinline__ void reduce_tile(const FoldArgs& a, float* __restrict
     const float2 sc = make_float2(a.xf[k].gscale, a.xf[k].ginv);
     for (int i = ty; i < oh; i += 8) {
         const int cy = 2 * (gy0 + i);
-        const int r0 = RY(cy - 2) - yw0, r1 = RY(cy - 1) - yw0, r2 = RY(cy) - yw0, r3 = RY(cy + 1) - yw0, r4 = RY(cy + 2) - yw0;
+        const int r0 = cy - 2 - yw0, r1 = r0 + 1, r2 = r0 + 2, r3 = r0 + 3, r4 = r0 + 4;
         for (int j = tx; j < ow; j += 32) {
 #pragma unroll
             for (int c = 0; c < 3; c++) {
