@@ -49,6 +49,9 @@ extern "C" {
 /* lsb_config.flags: with frames already in device memory, fold an aligned stack chunk by chunk beside
    its registration chain instead of after it (the same results; pushed frames always fold beside it) */
 #define LSB_FLAG_FOLD_BESIDE_CHAIN 2
+/* lsb_config.flags: aggregate the focus slices with direct window sums of 2R+1 taps instead of moving
+   sums at radii 3 and 8 (the same results whenever the f64 sums are exact; for cross-checks and timing) */
+#define LSB_FLAG_DIRECT_WINDOW_SUMS 4
 
 typedef struct lsb_engine lsb_engine;
 typedef struct lsb_stack lsb_stack;

@@ -1323,7 +1323,8 @@ static char* run_pipeline_once(lsb_stack* s) {
         TRY(luma_and_guide(s->img, W, H, k, s->yfull, s->guide, dw, dh, st));
         if (s->dp.agg_radius > 0) gf_stats(s->guide, dw, dh, (int)s->dp.agg_radius, s->tmp, s->mi, s->vi, st);
         AggArgs ag{s->slices, n, dw, dh, (int)s->dp.agg_radius, s->dp.agg_eps, s->guide, s->mi, s->vi, s->state, 0, 0};
-        TRY(aggregate_peaks(ag, s->storage != STORE_F32, st, e->grid_agg > 0 ? e->grid_agg : e->grid));
+        TRY(aggregate_peaks(ag, s->storage != STORE_F32, st, e->grid_agg > 0 ? e->grid_agg : e->grid,
+                            !(e->cfg.flags & LSB_FLAG_DIRECT_WINDOW_SUMS)));
         TRY(cudaEventRecord(ev[5], st));
         const size_t cnt = (m + 6) / 7;
         TRY(select_kth(s->state + 7 * m, cnt, 7, cnt / 2, e->hist, e->sel, e->scal + 0, st));
@@ -1689,7 +1690,7 @@ extern "C" char* lsb_depth_from_slices(lsb_engine* e, const float* slices, uint3
     TRYS(luma_and_guide(s->img, (int)w, (int)h, k, s->yfull, s->guide, dw, dh, st));
     if (dp.agg_radius > 0) gf_stats(s->guide, dw, dh, (int)dp.agg_radius, s->tmp, s->mi, s->vi, st);
     AggArgs ag{s->slices, (int)n, dw, dh, (int)dp.agg_radius, dp.agg_eps, s->guide, s->mi, s->vi, s->state, 0, 0};
-    TRYS(aggregate_peaks(ag, false, st, e->grid));
+    TRYS(aggregate_peaks(ag, false, st, e->grid, !(e->cfg.flags & LSB_FLAG_DIRECT_WINDOW_SUMS)));
     const size_t cnt = (m + 6) / 7;
     TRYS(select_kth(s->state + 7 * m, cnt, 7, cnt / 2, e->hist, e->sel, e->scal + 0, st));
     TRYS(peak_finish(s->state, m, (int)n, e->scal + 0, dp.gate, s->draw, s->conf, s->mins, st));

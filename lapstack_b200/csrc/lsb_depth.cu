@@ -427,6 +427,250 @@ __global__ void __launch_bounds__(256, 2) aggregate_kernel(const AggArgs a) {
     }
 }
 
+// --------------------------- aggregation by moving sums, one slice ahead
+// 16-byte global -> shared copies (cp.async.cg), zero-filled where the source lies outside the grid
+__device__ __forceinline__ void agg_cp16(void* sdst, const void* gsrc, bool in) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(sdst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(d), "l"(gsrc), "r"(in ? 16 : 0));
+}
+__device__ __forceinline__ void agg_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+__device__ __forceinline__ void agg_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::); }
+template <class S>
+__device__ __forceinline__ float agg_f(S v);
+template <>
+__device__ __forceinline__ float agg_f<float>(float v) { return v; }
+template <>
+__device__ __forceinline__ float agg_f<__half>(__half v) { return __half2float(v); }
+template <class S>
+__device__ __forceinline__ S agg_zero();
+template <>
+__device__ __forceinline__ float agg_zero<float>() { return 0.f; }
+template <>
+__device__ __forceinline__ __half agg_zero<__half>() { return __ushort_as_half((unsigned short)0); }
+
+// Run length of a pass over `lines` lines of `len` outputs, so that the lines' runs fit 256 threads once.
+__host__ __device__ constexpr int agg_run(int lines, int len) {
+    return (len + (256 / lines > 0 ? 256 / lines : 1) - 1) / (256 / lines > 0 ? 256 / lines : 1);
+}
+
+// depth.rs:1119 `depth_from_slices` over tiles of TW x TH cells, with the window sums of the
+// guided filter (depth.rs:379-406) formed as depth.rs:285 `BoxFilter::sum_into` forms them:
+// moving f64 sums along runs of a line (the entering value added, then the leaving one subtracted),
+// rounded to f32 after the horizontal and after the vertical pass. A run converts each input to
+// f64 once and keeps it in a register until it leaves the window. The sums are the reference's
+// whenever its f64 sums are exact (true unless a window spans more than 2^29 in magnitude).
+// A CTA stages slice m+1's window (tile +- 2R) by cp.async while it filters slice m; the
+// window is zero outside the grid, so the sums there equal BoxFilter's border-clipped ones,
+// and a (a, b) outside the grid is zero. Each thread keeps the peak tracker (depth.rs:547) of
+// CPT cells of one column in registers.
+template <int R, int TW, int TH, class SS, int MINB>
+__global__ void __launch_bounds__(256, MINB) guided_peaks_kernel(const AggArgs a) {
+    constexpr int NT = 256, CPT = TW * TH / NT;
+    constexpr int PW = TW + 4 * R, PH = TH + 4 * R, QW = TW + 2 * R, QH = TH + 2 * R, NW = 2 * R + 1;
+    constexpr int CE = 16 / (int)sizeof(SS);            // elements of one 16-byte copy
+    constexpr int LEAD = (2 * R + CE - 1) / CE * CE;    // staged columns left of the tile
+    constexpr int T0 = LEAD - 2 * R;                    // the window's first column in a staged row
+    constexpr int PS = (T0 + PW + CE - 1) / CE * CE;    // staged row length
+    constexpr int NCH = PS / CE;
+    constexpr int PWI = PW | 1;                         // guide row pitch
+    constexpr int L1 = agg_run(PH, QW), NS1 = (QW + L1 - 1) / L1;  // horizontal runs of p and I*p
+    constexpr int L2 = agg_run(QW, QH), NS2 = (QH + L2 - 1) / L2;  // vertical runs -> a, b
+    constexpr int L3 = agg_run(QH, TW), NS3 = (TW + L3 - 1) / L3;  // horizontal runs of a and b
+    static_assert(TW % CE == 0 && CPT * NT == TW * TH, "tile");
+    extern __shared__ __align__(16) unsigned char agg_sm[];
+    SS* P0 = (SS*)agg_sm;                                           // [2][PH][PS] slice windows
+    float* I = (float*)(agg_sm + sizeof(SS) * 2 * PH * PS);         // [PH][PWI] guide
+    float* MI = I + PH * PWI;                                       // [QH][QW] mean_i
+    float* VE = MI + QH * QW;                                       // [QH][QW] var_i + eps
+    float* HP = VE + QH * QW;                                       // [PH][QW] sums of p; then [QH][TW] of a
+    float* HQ = HP + PH * QW;                                       // [PH][QW] sums of I*p; then [QH][TW] of b
+    float* A = HQ + PH * QW;                                        // [QH][QW]
+    float* B = A + QH * QW;                                         // [QH][QW]
+    const int w = a.dw, h = a.dh, tid = threadIdx.x;
+    const float ic_in = box_inv_count(R, R, 4 * R + 1, 4 * R + 1, R);  // 1 / (2R+1)^2
+    for (int tile = blockIdx.x; tile < a.ntiles; tile += gridDim.x) {
+        const int x0 = (tile % a.tiles_x) * TW, y0 = (tile / a.tiles_x) * TH;
+        const int px0 = x0 - 2 * R, py0 = y0 - 2 * R, qx0 = x0 - R, qy0 = y0 - R, xs0 = x0 - LEAD;
+        const bool inner = px0 >= 0 && py0 >= 0 && px0 + PW <= w && py0 + PH <= h;
+        auto stage = [&](int m, SS* buf) {
+            const SS* sl = (const SS*)a.slices + (size_t)m * w * h;
+            if (a.async16) {
+                // xs0 and the copies are CE-aligned and w % CE == 0: a copy lies wholly inside or outside
+                for (int i = tid; i < PH * NCH; i += NT) {
+                    const int r = i / NCH, k = i - r * NCH, y = py0 + r, x = xs0 + k * CE;
+                    const bool in = y >= 0 && y < h && x >= 0 && x < w;
+                    agg_cp16(buf + r * PS + k * CE, in ? (const void*)(sl + (size_t)y * w + x) : a.slices, in);
+                }
+                agg_commit();
+            } else {
+                for (int i = tid; i < PH * PS; i += NT) {
+                    const int r = i / PS, t = i - r * PS, y = py0 + r, x = xs0 + t;
+                    buf[i] = (y >= 0 && y < h && x >= 0 && x < w) ? sl[(size_t)y * w + x] : agg_zero<SS>();
+                }
+            }
+        };
+        __syncthreads();  // the previous tile is done with every buffer
+        stage(0, P0);
+        for (int i = tid; i < PH * PW; i += NT) {
+            const int r = i / PW, c = i - r * PW, x = px0 + c, y = py0 + r;
+            I[r * PWI + c] = (x >= 0 && x < w && y >= 0 && y < h) ? a.guide[(size_t)y * w + x] : 0.f;
+        }
+        for (int i = tid; i < QW * QH; i += NT) {
+            const int x = qx0 + i % QW, y = qy0 + i / QW;
+            const bool in = x >= 0 && x < w && y >= 0 && y < h;
+            MI[i] = in ? a.mean_i[(size_t)y * w + x] : 0.f;
+            VE[i] = in ? __fadd_rn(a.var_i[(size_t)y * w + x], a.eps) : 1.f;
+        }
+        PeakState st[CPT];
+#pragma unroll
+        for (int j = 0; j < CPT; j++) st[j] = PeakState{-1.f, -1.f, -1.f, -1.f, 0.f, 0.f, 0.f, __int_as_float(0x7f800000), 0};
+        const int vc = tid % TW, vr0 = (tid / TW) * CPT;  // this thread's cells: column vc, rows vr0 ..
+        for (int m = 0; m < a.n; m++) {
+            const SS* P = P0 + (m & 1) * PH * PS;
+            if (a.async16) agg_wait_all();
+            __syncthreads();  // slice m staged; the last pass of slice m-1 is done with HP and HQ
+            if (m + 1 < a.n) stage(m + 1, P0 + ((m + 1) & 1) * PH * PS);
+            // horizontal runs: sums of p and of I*p over rows of tile +- 2R, columns of tile +- R
+            for (int it = tid; it < PH * NS1; it += NT) {
+                const int r = it / NS1, c0 = (it - r * NS1) * L1;
+                const SS* pr = P + r * PS + T0 + c0;
+                const float* ir = I + r * PWI + c0;
+                float* hp = HP + r * QW + c0;
+                float* hq = HQ + r * QW + c0;
+                double vp[L1 + 2 * R], vq[L1 + 2 * R], sp = 0.0, sq = 0.0;
+#pragma unroll
+                for (int t = 0; t < L1 + 2 * R; t++) {
+                    if (QW % L1 != 0 && c0 + t - 2 * R >= QW) break;
+                    const float pv = agg_f<SS>(pr[t]);
+                    vp[t] = (double)pv;
+                    vq[t] = (double)__fmul_rn(ir[t], pv);
+                    sp += vp[t];
+                    sq += vq[t];
+                    if (t > 2 * R) {
+                        sp -= vp[t - NW];
+                        sq -= vq[t - NW];
+                    }
+                    if (t >= 2 * R) {
+                        hp[t - 2 * R] = (float)sp;
+                        hq[t - 2 * R] = (float)sq;
+                    }
+                }
+            }
+            __syncthreads();
+            // vertical runs: mean_p and corr_Ip over tile +- R, then a and b (depth.rs:385-390)
+            for (int it = tid; it < QW * NS2; it += NT) {
+                const int j = it / QW, c = it - j * QW, r0 = j * L2;
+                const float* hp = HP + r0 * QW + c;
+                const float* hq = HQ + r0 * QW + c;
+                double vp[L2 + 2 * R], vq[L2 + 2 * R], sp = 0.0, sq = 0.0;
+#pragma unroll
+                for (int t = 0; t < L2 + 2 * R; t++) {
+                    if (QH % L2 != 0 && r0 + t - 2 * R >= QH) break;
+                    vp[t] = (double)hp[t * QW];
+                    vq[t] = (double)hq[t * QW];
+                    sp += vp[t];
+                    sq += vq[t];
+                    if (t > 2 * R) {
+                        sp -= vp[t - NW];
+                        sq -= vq[t - NW];
+                    }
+                    if (t >= 2 * R) {
+                        const int k = t - 2 * R, i = (r0 + k) * QW + c;
+                        float ic = ic_in;
+                        bool in = true;
+                        if (!inner) {
+                            const int x = qx0 + c, y = qy0 + r0 + k;
+                            in = x >= 0 && x < w && y >= 0 && y < h;
+                            if (in) ic = box_inv_count(x, y, w, h, R);
+                        }
+                        const float mp = __fmul_rn((float)sp, ic), corr = __fmul_rn((float)sq, ic), mi = MI[i];
+                        const float av = __fdiv_rn(__fsub_rn(corr, __fmul_rn(mi, mp)), VE[i]);
+                        A[i] = in ? av : 0.f;
+                        B[i] = in ? __fsub_rn(mp, __fmul_rn(av, mi)) : 0.f;
+                    }
+                }
+            }
+            __syncthreads();
+            // horizontal runs: sums of a and b over rows of tile +- R, the tile's columns
+            for (int it = tid; it < QH * NS3; it += NT) {
+                const int r = it / NS3, c0 = (it - r * NS3) * L3;
+                const float* ar = A + r * QW + c0;
+                const float* br = B + r * QW + c0;
+                float* ha = HP + r * TW + c0;
+                float* hb = HQ + r * TW + c0;
+                double va[L3 + 2 * R], vb[L3 + 2 * R], sa = 0.0, sb = 0.0;
+#pragma unroll
+                for (int t = 0; t < L3 + 2 * R; t++) {
+                    if (TW % L3 != 0 && c0 + t - 2 * R >= TW) break;
+                    va[t] = (double)ar[t];
+                    vb[t] = (double)br[t];
+                    sa += va[t];
+                    sb += vb[t];
+                    if (t > 2 * R) {
+                        sa -= va[t - NW];
+                        sb -= vb[t - NW];
+                    }
+                    if (t >= 2 * R) {
+                        ha[t - 2 * R] = (float)sa;
+                        hb[t - 2 * R] = (float)sb;
+                    }
+                }
+            }
+            __syncthreads();
+            // vertical run down this thread's column: a-bar, b-bar, q = a-bar I + b-bar (depth.rs:404),
+            // max(q, 0) (depth.rs:1146) into the tracker
+            {
+                const float* ha = HP + vr0 * TW + vc;
+                const float* hb = HQ + vr0 * TW + vc;
+                double va[CPT + 2 * R], vb[CPT + 2 * R], sa = 0.0, sb = 0.0;
+#pragma unroll
+                for (int t = 0; t < CPT + 2 * R; t++) {
+                    va[t] = (double)ha[t * TW];
+                    vb[t] = (double)hb[t * TW];
+                    sa += va[t];
+                    sb += vb[t];
+                    if (t > 2 * R) {
+                        sa -= va[t - NW];
+                        sb -= vb[t - NW];
+                    }
+                    if (t >= 2 * R) {
+                        const int k = t - 2 * R, x = x0 + vc, y = y0 + vr0 + k;
+                        if (inner || (x < w && y < h)) {
+                            const float ic = inner ? ic_in : box_inv_count(x, y, w, h, R);
+                            const float abar = __fmul_rn((float)sa, ic), bbar = __fmul_rn((float)sb, ic);
+                            const float q = fmaxf(__fadd_rn(__fmul_rn(abar, I[(vr0 + k + 2 * R) * PWI + vc + 2 * R]), bbar), 0.f);
+                            peak_push(st[k], q, m);
+                        }
+                    }
+                }
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < CPT; j++) {
+            const int x = x0 + vc, y = y0 + vr0 + j;
+            if (x >= w || y >= h) continue;
+            const size_t o = (size_t)y * w + x, m = (size_t)w * h;
+            float* S = a.state;
+            S[o] = st[j].c1;
+            S[m + o] = st[j].l1;
+            S[2 * m + o] = st[j].r1;
+            S[3 * m + o] = st[j].c2;
+            S[4 * m + o] = st[j].prev;
+            S[5 * m + o] = st[j].prev2;
+            S[6 * m + o] = st[j].sum;
+            S[7 * m + o] = st[j].cmin;
+            S[8 * m + o] = __int_as_float(st[j].i1);
+        }
+    }
+}
+
+template <int R, int TW, int TH, class SS>
+constexpr size_t guided_peaks_smem() {
+    constexpr int PW = TW + 4 * R, PH = TH + 4 * R, QW = TW + 2 * R, QH = TH + 2 * R;
+    constexpr int CE = 16 / (int)sizeof(SS), LEAD = (2 * R + CE - 1) / CE * CE, PS = (LEAD - 2 * R + PW + CE - 1) / CE * CE;
+    return sizeof(SS) * 2 * PH * PS + sizeof(float) * ((size_t)PH * (PW | 1) + 4 * QH * QW + 2 * PH * QW);
+}
+
 // Without aggregation (agg_radius 0) the slices go to the tracker (depth.rs:547) as they are.
 template <class SS>
 __global__ void peaks_raw_kernel(const SS* __restrict__ slices, int n, size_t m, float* __restrict__ S) {
@@ -451,13 +695,33 @@ size_t aggregate_smem_bytes(int r) {
     return sizeof(float) * (size_t)(2 * PW * PH + 4 * QW * QH + 2 * PH * QW);
 }
 
-cudaError_t aggregate_peaks(AggArgs a, bool slice_fp16, cudaStream_t s, int grid_limit) {
+template <int R, int TW, int TH, class SS>
+static cudaError_t launch_guided_peaks(AggArgs a, cudaStream_t s, int grid_limit) {
+    constexpr size_t smem = guided_peaks_smem<R, TW, TH, SS>();
+    constexpr int minb = smem <= 110 * 1024 ? 2 : 1;
+    static_assert(smem <= 227 * 1024, "shared memory");
+    a.tiles_x = (a.dw + TW - 1) / TW;
+    a.ntiles = a.tiles_x * ((a.dh + TH - 1) / TH);
+    a.async16 = a.dw % (16 / (int)sizeof(SS)) == 0 && (reinterpret_cast<uintptr_t>(a.slices) & 15) == 0;
+    auto k = guided_peaks_kernel<R, TW, TH, SS, minb>;
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    lsb_launched(), k<<<std::min(a.ntiles, std::max(1, grid_limit)), 256, smem, s>>>(a);
+    return cudaGetLastError();
+}
+
+cudaError_t aggregate_peaks(AggArgs a, bool slice_fp16, cudaStream_t s, int grid_limit, bool running) {
     size_t m = (size_t)a.dw * a.dh;
     if (a.r == 0) {
         if (slice_fp16) lsb_launched(), peaks_raw_kernel<__half><<<grid1(m), 256, 0, s>>>((const __half*)a.slices, a.n, m, a.state);
         else lsb_launched(), peaks_raw_kernel<float><<<grid1(m), 256, 0, s>>>((const float*)a.slices, a.n, m, a.state);
         return cudaGetLastError();
     }
+    // the reference's default radius (3) and the large-frame one (8) by moving sums
+    if (running && a.r == 3)
+        return slice_fp16 ? launch_guided_peaks<3, 64, 32, __half>(a, s, grid_limit) : launch_guided_peaks<3, 64, 32, float>(a, s, grid_limit);
+    if (running && a.r == 8)
+        return slice_fp16 ? launch_guided_peaks<8, 64, 32, __half>(a, s, grid_limit) : launch_guided_peaks<8, 64, 32, float>(a, s, grid_limit);
     const int TWD = a.r <= 4 ? 64 : 32, THD = 32;
     a.tiles_x = (a.dw + TWD - 1) / TWD;
     a.ntiles = a.tiles_x * ((a.dh + THD - 1) / THD);

@@ -15,6 +15,7 @@ struct AggArgs {
     const float* var_i;
     float* state;  // [9][dh][dw] peak tracker state
     int tiles_x, ntiles;
+    int async16;  // set by aggregate_peaks: slice rows start on 16-byte boundaries
 };
 
 cudaError_t luma_and_guide(const float* img, int w, int h, int k, float* yfull, float* guide, int dw, int dh, cudaStream_t s);
@@ -22,7 +23,8 @@ void gf_stats(const float* guide, int w, int h, int r, float* tmp, float* mean_i
 void gf_coeffs(const float* guide, const float* mean_i, const float* var_i, const float* p, int w, int h, int r, float eps,
                float* t0, float* t1, float* t2, float* tmp, float* abar, float* bbar, cudaStream_t s);
 size_t aggregate_smem_bytes(int r);
-cudaError_t aggregate_peaks(AggArgs a, bool slice_fp16, cudaStream_t s, int grid_limit);
+// running: moving window sums (radius 3 and 8) rather than the direct window sums of the general kernel
+cudaError_t aggregate_peaks(AggArgs a, bool slice_fp16, cudaStream_t s, int grid_limit, bool running = true);
 cudaError_t select_kth(const float* v, size_t cnt, int stride, size_t rank, unsigned* hist, unsigned* sel, float* out,
                        cudaStream_t s);
 cudaError_t peak_finish(const float* state, size_t m, int n, const float* floor_p, float gate, float* depth, float* conf,

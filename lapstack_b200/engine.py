@@ -241,16 +241,18 @@ class Engine:
     STORAGE = {"f32": 0, "unorm16": 1, "f16": 2}
 
     def __init__(self, device: int = 0, storage: str = "f32", grid_limit: int = 0, log=None, fused_fold0: bool = True,
-                 fold_beside_chain: bool = False):
+                 fold_beside_chain: bool = False, direct_window_sums: bool = False):
         """storage: "f32" (bit-exact with the reference FP32 path), "unorm16" (16-bit
         Gaussian levels, FP16 slices) or "f16" (IEEE half levels and slices).
         fused_fold0=False folds level 0 with the separate REDUCE and select kernels on
         every tile (LSB_FLAG_TWO_KERNEL_FOLD0); fold_beside_chain=True folds an aligned
         stack in device memory chunk by chunk beside its registration chain instead of
-        after it (LSB_FLAG_FOLD_BESIDE_CHAIN). Neither changes a result."""
+        after it (LSB_FLAG_FOLD_BESIDE_CHAIN); direct_window_sums=True forms the depth
+        pass's guided-filter window sums tap by tap instead of as moving sums
+        (LSB_FLAG_DIRECT_WINDOW_SUMS). None changes a result."""
         self._L = load()
         self._logcb = LOG_FN(lambda line, _u: log(line.decode())) if log else LOG_FN()
-        flags = (0 if fused_fold0 else 1) | (2 if fold_beside_chain else 0)
+        flags = (0 if fused_fold0 else 1) | (2 if fold_beside_chain else 0) | (4 if direct_window_sums else 0)
         cfg = Config(device, self.STORAGE[storage], grid_limit, flags, self._logcb, None)
         h = C.c_void_p()
         check(self._L.lsb_engine_create(C.byref(cfg), C.byref(h)))
