@@ -8,10 +8,11 @@
 //   order and keeps every cell's profile state in registers, so a slice is read
 //   from HBM once (plus its halo) and the tracker state never round-trips.
 // * Box sums follow depth.rs:285 `BoxFilter::sum_into`: border-clipped, f64
-//   sums rounded to f32 after the horizontal and after the vertical pass; the
-//   window sums are formed directly in f64 (equal to the reference's f64
-//   running sums whenever those are exact, which they are unless a window
-//   spans more than 2^29 in magnitude).
+//   sums rounded to f32 after the horizontal and after the vertical pass; at
+//   radii 3 and 8 the window sums are moving f64 sums along short runs, at
+//   other radii direct sums of 2R+1 taps (both equal to the reference's f64
+//   running sums whenever those are exact, which they are unless a window's
+//   values span more than about 2^24 in magnitude).
 // * The two medians of a subsample (noise floor depth.rs:578, p90
 //   depth.rs:616) are exact k-th-value selections on the device (two 16-bit
 //   radix passes over the total-order key of each float).
@@ -453,12 +454,30 @@ __host__ __device__ constexpr int agg_run(int lines, int len) {
     return (len + (256 / lines > 0 ? 256 / lines : 1) - 1) / (256 / lines > 0 ? 256 / lines : 1);
 }
 
+// One step of a moving window sum of NW = 2R+1 values along a run (t: the entering value's
+// index): the first window is summed as two interleaved partial sums, then each step adds the
+// entering value less the leaving one. Every partial sum of up to 18 f32 values is exact in f64
+// unless their magnitudes span more than about 2^24, so the window sum is then the exact sum,
+// whatever the order of the adds, as the reference's moving sums give it while they are exact.
+template <int R, int NV>
+__device__ __forceinline__ void agg_step_t(double& s, double& s2, const double (&v)[NV], int t) {
+    if (t < 2 * R) {
+        if (t & 1) s2 += v[t];
+        else s += v[t];
+    } else if (t == 2 * R) {
+        s = (s + s2) + v[t];
+    } else {
+        s += v[t] - v[t - 2 * R - 1];
+    }
+}
+#define agg_step(s, s2, v, t) agg_step_t<R>(s, s2, v, t)
+
 // depth.rs:1119 `depth_from_slices` over tiles of TW x TH cells, with the window sums of the
 // guided filter (depth.rs:379-406) formed as depth.rs:285 `BoxFilter::sum_into` forms them:
 // moving f64 sums along runs of a line (the entering value added, then the leaving one subtracted),
 // rounded to f32 after the horizontal and after the vertical pass. A run converts each input to
 // f64 once and keeps it in a register until it leaves the window. The sums are the reference's
-// whenever its f64 sums are exact (true unless a window spans more than 2^29 in magnitude).
+// whenever its f64 sums are exact (true unless a window's values span more than about 2^24).
 // A CTA stages slice m+1's window (tile +- 2R) by cp.async while it filters slice m; the
 // window is zero outside the grid, so the sums there equal BoxFilter's border-clipped ones,
 // and a (a, b) outside the grid is zero. Each thread keeps the peak tracker (depth.rs:547) of
@@ -537,19 +556,15 @@ __global__ void __launch_bounds__(256, MINB) guided_peaks_kernel(const AggArgs a
                 const float* ir = I + r * PWI + c0;
                 float* hp = HP + r * QW + c0;
                 float* hq = HQ + r * QW + c0;
-                double vp[L1 + 2 * R], vq[L1 + 2 * R], sp = 0.0, sq = 0.0;
+                double vp[L1 + 2 * R], vq[L1 + 2 * R], sp = 0.0, sp2 = 0.0, sq = 0.0, sq2 = 0.0;
 #pragma unroll
                 for (int t = 0; t < L1 + 2 * R; t++) {
                     if (QW % L1 != 0 && c0 + t - 2 * R >= QW) break;
                     const float pv = agg_f<SS>(pr[t]);
                     vp[t] = (double)pv;
                     vq[t] = (double)__fmul_rn(ir[t], pv);
-                    sp += vp[t];
-                    sq += vq[t];
-                    if (t > 2 * R) {
-                        sp -= vp[t - NW];
-                        sq -= vq[t - NW];
-                    }
+                    agg_step(sp, sp2, vp, t);
+                    agg_step(sq, sq2, vq, t);
                     if (t >= 2 * R) {
                         hp[t - 2 * R] = (float)sp;
                         hq[t - 2 * R] = (float)sq;
@@ -562,18 +577,14 @@ __global__ void __launch_bounds__(256, MINB) guided_peaks_kernel(const AggArgs a
                 const int j = it / QW, c = it - j * QW, r0 = j * L2;
                 const float* hp = HP + r0 * QW + c;
                 const float* hq = HQ + r0 * QW + c;
-                double vp[L2 + 2 * R], vq[L2 + 2 * R], sp = 0.0, sq = 0.0;
+                double vp[L2 + 2 * R], vq[L2 + 2 * R], sp = 0.0, sp2 = 0.0, sq = 0.0, sq2 = 0.0;
 #pragma unroll
                 for (int t = 0; t < L2 + 2 * R; t++) {
                     if (QH % L2 != 0 && r0 + t - 2 * R >= QH) break;
                     vp[t] = (double)hp[t * QW];
                     vq[t] = (double)hq[t * QW];
-                    sp += vp[t];
-                    sq += vq[t];
-                    if (t > 2 * R) {
-                        sp -= vp[t - NW];
-                        sq -= vq[t - NW];
-                    }
+                    agg_step(sp, sp2, vp, t);
+                    agg_step(sq, sq2, vq, t);
                     if (t >= 2 * R) {
                         const int k = t - 2 * R, i = (r0 + k) * QW + c;
                         float ic = ic_in;
@@ -598,18 +609,14 @@ __global__ void __launch_bounds__(256, MINB) guided_peaks_kernel(const AggArgs a
                 const float* br = B + r * QW + c0;
                 float* ha = HP + r * TW + c0;
                 float* hb = HQ + r * TW + c0;
-                double va[L3 + 2 * R], vb[L3 + 2 * R], sa = 0.0, sb = 0.0;
+                double va[L3 + 2 * R], vb[L3 + 2 * R], sa = 0.0, sa2 = 0.0, sb = 0.0, sb2 = 0.0;
 #pragma unroll
                 for (int t = 0; t < L3 + 2 * R; t++) {
                     if (TW % L3 != 0 && c0 + t - 2 * R >= TW) break;
                     va[t] = (double)ar[t];
                     vb[t] = (double)br[t];
-                    sa += va[t];
-                    sb += vb[t];
-                    if (t > 2 * R) {
-                        sa -= va[t - NW];
-                        sb -= vb[t - NW];
-                    }
+                    agg_step(sa, sa2, va, t);
+                    agg_step(sb, sb2, vb, t);
                     if (t >= 2 * R) {
                         ha[t - 2 * R] = (float)sa;
                         hb[t - 2 * R] = (float)sb;
@@ -622,17 +629,13 @@ __global__ void __launch_bounds__(256, MINB) guided_peaks_kernel(const AggArgs a
             {
                 const float* ha = HP + vr0 * TW + vc;
                 const float* hb = HQ + vr0 * TW + vc;
-                double va[CPT + 2 * R], vb[CPT + 2 * R], sa = 0.0, sb = 0.0;
+                double va[CPT + 2 * R], vb[CPT + 2 * R], sa = 0.0, sa2 = 0.0, sb = 0.0, sb2 = 0.0;
 #pragma unroll
                 for (int t = 0; t < CPT + 2 * R; t++) {
                     va[t] = (double)ha[t * TW];
                     vb[t] = (double)hb[t * TW];
-                    sa += va[t];
-                    sb += vb[t];
-                    if (t > 2 * R) {
-                        sa -= va[t - NW];
-                        sb -= vb[t - NW];
-                    }
+                    agg_step(sa, sa2, va, t);
+                    agg_step(sb, sb2, vb, t);
                     if (t >= 2 * R) {
                         const int k = t - 2 * R, x = x0 + vc, y = y0 + vr0 + k;
                         if (inner || (x < w && y < h)) {
