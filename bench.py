@@ -63,6 +63,13 @@ CONFIGS = {
 }
 
 
+# Several stacks of uneven sizes and frame counts (12, 24 and 45 MP; 8 to 24 frames), aligned,
+# 16-bit storage, depth on: run one after another on the whole GPU, then side by side on engines
+# that each take a share of the SMs (lsb_batch_run). Not the headline: its own JSON line.
+BATCH = [(4240, 2832, 16), (6000, 4000, 12), (8256, 5504, 8), (4240, 2832, 24), (6000, 4000, 20), (8256, 5504, 12),
+         (4240, 2832, 10), (6000, 4000, 8)]
+
+
 def params_of(cfg, mod):
     fuse = mod.FuseParams(levels=cfg["levels"])
     align = mod.AlignParams(coarsen=cfg["coarsen"]) if cfg["align"] else None
@@ -380,7 +387,11 @@ def main():
     ap.add_argument("--no-autotune", action="store_true")
     ap.add_argument("--two-kernel-fold0", action="store_true", help="fold level 0 with the separate REDUCE and select kernels")
     ap.add_argument("--fold-beside-chain", action="store_true", help="fold device-resident frames beside the registration chain")
+    ap.add_argument("--batch", action="store_true", help="time the uneven batch of stacks instead (its own JSON line)")
+    ap.add_argument("--engines", type=int, default=2, help="engines the batch runs on side by side")
     args = ap.parse_args()
+    if args.batch:
+        return batch_bench(args)
     c = dict(CONFIGS[args.config])
     if args.storage:
         c["storage"] = args.storage
@@ -514,6 +525,79 @@ def main():
     eng.close()
     if dist:
         dist.destroy_process_group()
+    return 0
+
+
+def batch_bench(args):
+    """The uneven batch: each stack alone on an engine with the whole GPU (the sum of their times),
+    then the batch on `--engines` engines with an equal share of the SMs each, side by side
+    (lsb_batch_run). Frames are generated in each stack's frame store on the device; a run is
+    lsb_stack_finish (results copied to the host). Wall clock around device-synchronised runs."""
+    import torch
+    import lapstack_b200 as L
+
+    torch.cuda.set_device(0)
+    sms = torch.cuda.get_device_properties(0).multi_processor_count
+    fuse, align, depth = L.FuseParams(), L.AlignParams(coarsen=3), L.DepthParams()
+
+    def stacks_on(engines):
+        out = []
+        for i, (w, h, n) in enumerate(BATCH):
+            e = engines[i % len(engines)]
+            st = e.stack(w, h, n, fuse, align, depth)
+            L.synth_stack_device(L.SynthSpec(w, h, n, seed=0xBA7C + i, warp=True, mag_step=0.0, noise_std=0.002),
+                                 st.frames_device(), e.stream)
+            st.set_count(n)
+            out.append(st)
+        torch.cuda.synchronize()
+        return out
+
+    def timed(fn):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        r = fn()
+        torch.cuda.synchronize()
+        return (time.perf_counter() - t0) * 1e3, r
+
+    whole = L.Engine(storage="unorm16")
+    stacks = stacks_on([whole])
+    single = []
+    for st in stacks:
+        for it in range(1 + max(1, args.steps)):
+            ms, out = timed(st.finish)
+            del out
+            if it > 0:
+                single.append((st.w, st.h, st.n, ms))
+    per_stack = [statistics.median(m for (w, h, n, m) in single if (w, h, n) == key) for key in BATCH]
+    for st in stacks:
+        st.close()
+    whole.close()
+
+    k = max(1, args.engines)
+    engines = [L.Engine(storage="unorm16", grid_limit=max(1, 2 * sms // k)) for _ in range(k)]
+    stacks = stacks_on(engines)
+    batch = []
+    for it in range(max(1, args.warmup) + max(1, args.steps)):
+        ms, outs = timed(lambda: L.batch_run(stacks))
+        del outs
+        if it >= max(1, args.warmup):
+            batch.append(ms)
+    for st in stacks:
+        st.close()
+    for e in engines:
+        e.close()
+    mpf = sum(w * h * n for (w, h, n) in BATCH) / 1e6
+    b = statistics.median(batch)
+    print(json.dumps({
+        "metric": "uneven batch of stacks MP-frames/s (align+fuse+depth)", "value": mpf / (b / 1e3), "unit": "MP-frames/s",
+        "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_batch": b, "higher_is_better": True,
+        "dtype": "f32", "data": "synthetic (seeded generator, frames generated on the device)",
+        "config": {"workload": "batch: " + ", ".join(f"{n} x {w}x{h}" for (w, h, n) in BATCH) +
+                   "; aligned (coarsen 3), unorm16 storage, guided-filter DfF r=3, WLS MG-PCG", "engines": k,
+                   "grid_limit": max(1, 2 * sms // k)},
+        "sum_single_ms": sum(per_stack), "single_ms": per_stack, "batch_ms": batch,
+        "speedup_vs_one_after_another": sum(per_stack) / b, "timing": "wall clock around device-synchronised runs",
+    }))
     return 0
 
 

@@ -62,7 +62,8 @@ typedef struct {
     int32_t device;        /* CUDA device ordinal */
     int32_t storage;       /* Gaussian levels >= 1 and focus slices: 0 FP32 (bit-exact with the reference
                               FP32 path); 1 16-bit: UNORM16 levels, FP16 slices; 2 FP16 levels and slices */
-    int32_t grid_limit;    /* CTAs of the persistent kernels; 0 = 2 x the SM count */
+    int32_t grid_limit;    /* CTAs of the persistent kernels and of the device registration search;
+                              0 = 2 x the SM count */
     int32_t flags;         /* LSB_FLAG_* bits; 0 for the defaults */
     lsb_log_fn log;        /* optional progress lines (stack.rs:1014 `log`) */
     void* user;
@@ -343,9 +344,14 @@ typedef struct {
 } lsb_tuning;
 char* lsb_stack_autotune(lsb_stack* s, lsb_tuning* out);
 /* Several stacks of uneven sizes and frame counts, one result each (the batch
- * entry point of the boundary; stack.rs runs one stack per call). The stacks
- * share one engine and run back to back on its stream; on an error every
- * result is freed and the message names the stack. */
+ * entry point of the boundary; stack.rs runs one stack per call). Stacks of one
+ * engine run back to back on its streams; stacks of different engines on one
+ * device run side by side, one host thread per engine (so a log callback may be
+ * called from several threads). Engines made with a share of the SMs each
+ * (lsb_config.grid_limit, which bounds the registration search's CTAs too) fill
+ * the GPU together. Stacks of different engines with depth on must share the
+ * focus measure and its radii. On an error every result is freed and the
+ * message names the stack. */
 char* lsb_batch_run(lsb_stack* const* stacks, uint32_t n_stacks, lsb_result* outs);
 /* Use the network's prediction as the x0 of this stack's WLS solves (NULL: the
  * reference's FGS start). The stack does not own the network. */

@@ -1243,7 +1243,8 @@ static cudaError_t nm_launch(AlignCtx& C, NmJob& J) {
     if (e != cudaSuccess) return e;
     void* args[] = {(void*)&J};
     lsb_launched();
-    return cudaLaunchCooperativeKernel((void*)nm_search_kernel, dim3(g_nm_blocks), dim3(NM_THREADS), args, 0, C.s);
+    const int blocks = C.max_blocks > 0 ? std::min(g_nm_blocks, C.max_blocks) : g_nm_blocks;
+    return cudaLaunchCooperativeKernel((void*)nm_search_kernel, dim3(blocks), dim3(NM_THREADS), args, 0, C.s);
 }
 
 static cudaError_t multiscale_align_dev(AlignCtx& C, const float* rf, const std::vector<float*>& pr, const float* tg,

@@ -35,6 +35,7 @@ struct AlignCtx {
     int* nm_ctl;       // device, 4: error, evaluations, barrier arrivals, spare
     double* nm_out;    // device, 8: the transform
     int device_search = 1;  // 0: the host drives the search, one launch per simplex step
+    int max_blocks = 0;     // CTAs of the device search at most (0: two per SM); the engine's grid limit
     size_t evals = 0, launches = 0;
 };
 

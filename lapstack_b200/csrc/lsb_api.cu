@@ -292,6 +292,7 @@ static char* engine_init(lsb_engine* e) {
     TRY(e->pool.get(&e->sel, 4));
     TRY(e->pool.get(&e->scal, 16));
     e->actx.s = e->s;
+    e->actx.max_blocks = e->cfg.grid_limit > 0 ? e->cfg.grid_limit : 0;
     TRY(e->pool.get(&e->actx.part, MAX_CAND * 296 * 3));
     TRY(e->pool.get(&e->actx.sums_dev, MAX_CAND * 3));
     TRY(cudaHostAlloc((void**)&e->actx.sums_host, sizeof(double) * MAX_CAND * 3, cudaHostAllocDefault));
@@ -2045,21 +2046,54 @@ extern "C" char* lsb_stack_depth_planes(lsb_stack* s, const float** guide, const
     return nullptr;
 }
 
+// Several stacks at once (no counterpart in the reference, whose caller loops over stacks,
+// stack.rs:1011): the stacks of one engine run back to back on its streams; the stacks of
+// different engines on the same device run side by side, one host thread per engine. Each
+// engine's persistent kernels and device search take the CTAs its grid limit allows, so that
+// engines created with a share of the SMs each (lsb_config.grid_limit) fill the GPU together:
+// one stack's registration chain, which leaves most of the GPU idle, beside another's fold.
 extern "C" char* lsb_batch_run(lsb_stack* const* stacks, uint32_t n_stacks, lsb_result* outs) {
     if (!stacks || !outs) return dup_err("null argument");
     for (uint32_t i = 0; i < n_stacks; i++) memset(&outs[i], 0, sizeof(lsb_result));
+    std::vector<lsb_engine*> engines;
+    std::vector<std::vector<uint32_t>> work;
     for (uint32_t i = 0; i < n_stacks; i++) {
-        if (!stacks[i]) return dup_err(fmt("stack %u is null", i));
-        if (i > 0 && stacks[i]->e != stacks[0]->e) return dup_err("the stacks of a batch share one engine");
+        const lsb_stack* s = stacks[i];
+        if (!s) return dup_err(fmt("stack %u is null", i));
+        if (s->e->device != stacks[0]->e->device) return dup_err("the stacks of a batch run on one device");
+        // the focus measure's taps are one constant-memory copy per device
+        if (s->dp.enabled && stacks[0]->dp.enabled && s->e != stacks[0]->e &&
+            (s->dp.focus != stacks[0]->dp.focus || s->dp.r_in != stacks[0]->dp.r_in || s->dp.r_out != stacks[0]->dp.r_out))
+            return dup_err(fmt("stack %u: stacks of different engines in one batch share the focus measure and its radii", i));
+        const size_t k = std::find(engines.begin(), engines.end(), s->e) - engines.begin();
+        if (k == engines.size()) engines.push_back(s->e), work.emplace_back();
+        work[k].push_back(i);
+    }
+    std::vector<char*> errs(n_stacks, nullptr);
+    auto run = [&](size_t k) {
+        if (cudaSetDevice(engines[k]->device) != cudaSuccess) {
+            errs[work[k][0]] = dup_err("cudaSetDevice failed");
+            return;
+        }
+        for (uint32_t i : work[k])
+            if ((errs[i] = lsb_stack_finish(stacks[i], &outs[i])) != nullptr) break;
+    };
+    if (engines.size() == 1) {
+        run(0);
+    } else {
+        std::vector<std::future<void>> th;
+        for (size_t k = 1; k < engines.size(); k++) th.push_back(std::async(std::launch::async, run, k));
+        run(0);
+        for (auto& t : th) t.get();
     }
     for (uint32_t i = 0; i < n_stacks; i++) {
-        char* err = lsb_stack_finish(stacks[i], &outs[i]);
-        if (err) {
-            for (uint32_t j = 0; j <= i; j++) lsb_result_free(&outs[j]);
-            char* msg = dup_err(fmt("stack %u: %s", i, err));
-            free(err);
-            return msg;
+        if (!errs[i]) continue;
+        char* msg = dup_err(fmt("stack %u: %s", i, errs[i]));
+        for (uint32_t j = 0; j < n_stacks; j++) {
+            lsb_result_free(&outs[j]);
+            free(errs[j]);
         }
+        return msg;
     }
     return nullptr;
 }

@@ -485,7 +485,7 @@ __device__ __forceinline__ void agg_step_t(double& s, double& s2, const double (
 template <int R, int TW, int TH, class SS, int MINB>
 __global__ void __launch_bounds__(256, MINB) guided_peaks_kernel(const AggArgs a) {
     constexpr int NT = 256, CPT = TW * TH / NT;
-    constexpr int PW = TW + 4 * R, PH = TH + 4 * R, QW = TW + 2 * R, QH = TH + 2 * R, NW = 2 * R + 1;
+    constexpr int PW = TW + 4 * R, PH = TH + 4 * R, QW = TW + 2 * R, QH = TH + 2 * R;
     constexpr int CE = 16 / (int)sizeof(SS);            // elements of one 16-byte copy
     constexpr int LEAD = (2 * R + CE - 1) / CE * CE;    // staged columns left of the tile
     constexpr int T0 = LEAD - 2 * R;                    // the window's first column in a staged row

@@ -23,6 +23,9 @@
 // intrinsic in the reference's association order, so selection maps and
 // coefficients are bit-identical to the reference FP32 CPU path.
 #include <algorithm>
+#include <map>
+#include <mutex>
+#include <vector>
 
 #include "lsb_common.cuh"
 #include "lsb_internal.h"
@@ -35,8 +38,27 @@ namespace lsb {
 
 size_t fold_smem_bytes(int, bool) { return (size_t)SEL_FLOATS * sizeof(float); }
 
+// The taps live in constant memory, one copy per device for every engine on it: they are written
+// (stream-ordered on s) only when they change, and an engine that finds them already requested
+// makes its stream wait for that write. Engines that run at the same time must ask for the same taps.
+static std::mutex g_taps_mu;
+static std::map<int, std::pair<std::vector<float>, cudaEvent_t>> g_taps;
 cudaError_t set_focus_taps(const float* taps3, int ntaps, cudaStream_t s) {
     if (ntaps > 64) return cudaErrorInvalidValue;
+    int dev = 0;
+    cudaError_t de = cudaGetDevice(&dev);
+    if (de != cudaSuccess) return de;
+    std::lock_guard<std::mutex> lk(g_taps_mu);
+    auto& cur = g_taps[dev];
+    const std::vector<float> want(taps3, taps3 + 3 * ntaps);
+    if (cur.second && cur.first == want) return cudaStreamWaitEvent(s, cur.second, 0);
+    if (!cur.second) {
+        de = cudaEventCreateWithFlags(&cur.second, cudaEventDisableTiming);
+        if (de != cudaSuccess) {
+            cur.second = nullptr;
+            return de;
+        }
+    }
     int off[64];
     float wgt[64];
     for (int q = 0; q < ntaps; q++) {
@@ -46,6 +68,8 @@ cudaError_t set_focus_taps(const float* taps3, int ntaps, cudaStream_t s) {
     cudaError_t e = cudaMemcpyToSymbolAsync(c_taps, taps3, sizeof(float) * 3 * ntaps, 0, cudaMemcpyHostToDevice, s);
     if (e == cudaSuccess) e = cudaMemcpyToSymbolAsync(c_tapo, off, sizeof(int) * ntaps, 0, cudaMemcpyHostToDevice, s);
     if (e == cudaSuccess) e = cudaMemcpyToSymbolAsync(c_tapw, wgt, sizeof(float) * ntaps, 0, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaEventRecord(cur.second, s);
+    cur.first = e == cudaSuccess ? want : std::vector<float>();
     return e;
 }
 

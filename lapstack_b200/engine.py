@@ -528,7 +528,9 @@ def _output_of(lib, r) -> Output:
 
 
 def batch_run(stacks) -> list:
-    """Several pushed stacks of uneven sizes, one Output each (lsb_batch_run)."""
+    """Several pushed stacks of uneven sizes, one Output each (lsb_batch_run). Stacks of one
+    engine run back to back; stacks of different engines on the device run side by side (give
+    each engine a share of the SMs through grid_limit)."""
     if not stacks:
         return []
     lib = stacks[0]._L
