@@ -330,6 +330,9 @@ char* lsb_unet_prepare(const float* guide, const float* d, const float* conf, ui
                        float* d_in_dev, uint32_t b, void* stream);
 /* out0_dev [B][H][W]: the network's correction; the prediction is d_in + out0 */
 char* lsb_unet_forward(lsb_unet* u, const void* in_dev, const float* d_in_dev, uint32_t B, uint32_t H, uint32_t W, float* out0_dev);
+/* the last forward pass's device time: CUDA events around its layers on the network's stream (the
+   input copies excluded) */
+char* lsb_unet_forward_ms(lsb_unet* u, float* ms);
 /* forward, MSE of d_in + out0 against target_dev [B][H][W], backward, and Adam when lr > 0 */
 char* lsb_unet_train_step(lsb_unet* u, const void* in_dev, const float* d_in_dev, const float* target_dev, uint32_t B, uint32_t H,
                           uint32_t W, float lr, double* loss_out);

@@ -126,6 +126,7 @@ SIGNATURES = {
     "lsb_unet_grid": (None, [C.c_uint32, C.c_uint32, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]),
     "lsb_unet_prepare": (ERR, [P, P, P, C.c_uint32, C.c_uint32, C.c_float, P, P, C.c_uint32, P]),
     "lsb_unet_forward": (ERR, [P, P, P, C.c_uint32, C.c_uint32, C.c_uint32, P]),
+    "lsb_unet_forward_ms": (ERR, [P, P]),
     "lsb_unet_train_step": (ERR, [P, P, P, P, C.c_uint32, C.c_uint32, C.c_uint32, C.c_float, C.POINTER(C.c_double)]),
     "lsb_stack_set_warm_start": (ERR, [P, P]),
     "lsb_stack_weighted_average": (ERR, [P, C.POINTER(WavParamsC), P]),

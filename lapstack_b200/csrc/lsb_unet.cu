@@ -613,6 +613,8 @@ struct lsb_unet {
     std::vector<void*> shape_allocs;
     int* status = nullptr;  // device error word of the tcgen05 convolution (a bounded wait ran out)
     bool tc = true;         // the 3x3 convolutions on tcgen05 (false: mma.sync, for comparison)
+    cudaEvent_t fev[2] = {nullptr, nullptr};  // around the last forward pass's layers on s
+    float fwd_ms = 0.f;
 };
 
 static char* un_err(const std::string& s) {
@@ -830,6 +832,8 @@ extern "C" void lsb_unet_destroy(lsb_unet* u) {
                     (void*)u->wmask, (void*)u->bmask, (void*)u->wb, (void*)u->wt, (void*)u->loss, (void*)u->status})
         if (p) cudaFree(p);
     if (u->loss_host) cudaFreeHost(u->loss_host);
+    for (cudaEvent_t v : u->fev)
+        if (v) cudaEventDestroy(v);
     if (u->s) cudaStreamDestroy(u->s);
     delete u;
 }
@@ -887,10 +891,21 @@ static char* stage_batch(lsb_unet* u, const void* in, const float* d_in, int B, 
 extern "C" char* lsb_unet_forward(lsb_unet* u, const void* in_dev, const float* d_in_dev, uint32_t B, uint32_t H, uint32_t W,
                                   float* out0_dev) {
     if (char* er = stage_batch(u, in_dev, d_in_dev, (int)B, (int)H, (int)W, false)) return er;
+    for (cudaEvent_t& v : u->fev)
+        if (!v) UTRY(cudaEventCreate(&v));
+    UTRY(cudaEventRecord(u->fev[0], u->s));
     UTRY(unet_forward(u));
+    UTRY(cudaEventRecord(u->fev[1], u->s));
     if (out0_dev) UTRY(cudaMemcpyAsync(out0_dev, u->out0, (size_t)B * H * W * 4, cudaMemcpyDeviceToDevice, u->s));
     UTRY(cudaStreamSynchronize(u->s));
+    UTRY(cudaEventElapsedTime(&u->fwd_ms, u->fev[0], u->fev[1]));
     return conv_status(u);
+}
+
+extern "C" char* lsb_unet_forward_ms(lsb_unet* u, float* ms) {
+    if (!u || !ms) return un_err("unet: null argument");
+    *ms = u->fwd_ms;
+    return nullptr;
 }
 
 static cudaError_t unet_backward(lsb_unet* u) {

@@ -106,6 +106,12 @@ class UNet:
                                        C.c_void_p(out.data_ptr())))
         return out
 
+    def forward_ms(self):
+        """The last forward pass's device time (CUDA events around its layers)."""
+        ms = C.c_float()
+        check(self._L.lsb_unet_forward_ms(self._h, C.byref(ms)))
+        return ms.value
+
     def train_step(self, inp, d_in, target, lr):
         """One step on a batch; lr = 0 computes the gradients only. Returns the batch MSE."""
         import torch

@@ -75,8 +75,8 @@ def test_two_engines_side_by_side_match_single_runs_and_the_oracle():
 
 def test_stacks_of_two_engines_must_share_the_focus_measure():
     e1, e2 = L.Engine(), L.Engine()
-    a = e1.stack(64, 48, 2, L.FuseParams(), None, L.DepthParams(r_out=3))
-    b = e2.stack(64, 48, 2, L.FuseParams(), None, L.DepthParams(r_out=4))
+    a = e1.stack(64, 48, 2, L.FuseParams(), None, L.DepthParams(r_in=1))
+    b = e2.stack(64, 48, 2, L.FuseParams(), None, L.DepthParams(r_in=2))
     try:
         fr = frames_of(64, 48, 2, False, 7)
         for st in (a, b):
