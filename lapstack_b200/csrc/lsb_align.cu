@@ -1144,9 +1144,17 @@ __global__ void __launch_bounds__(NM_THREADS) nm_search_kernel(const NmJob J) {
                 const int pi = tid / gsz, r = tid - pi * gsz;
                 double sv = 0.0;
                 if (pi < np) {
+                    // the first 12 partials loaded at once (one round of L2 latency), then added in
+                    // the order of b, as the rest
                     const double* row = P + (size_t)pi * gridDim.x;
-#pragma unroll 4
-                    for (int b = r; b < nown; b += gsz) sv += __ldcg(row + b);
+                    constexpr int PRE = 12;
+                    double pv[PRE];
+#pragma unroll
+                    for (int u = 0; u < PRE; u++) pv[u] = r + u * gsz < nown ? __ldcg(row + r + u * gsz) : 0.0;
+#pragma unroll
+                    for (int u = 0; u < PRE; u++)
+                        if (r + u * gsz < nown) sv += pv[u];
+                    for (int b = r + PRE * gsz; b < nown; b += gsz) sv += __ldcg(row + b);
                 }
                 gred[tid] = sv;
                 __syncthreads();
