@@ -1116,15 +1116,16 @@ __global__ void __launch_bounds__(NM_THREADS) nm_search_kernel(const NmJob J) {
             arrived += (unsigned)nown;
             __syncthreads();
             if (tid == 0) {
-                if (own) {
-                    __threadfence();  // this CTA's partials before its arrival
-                    atomicAdd(J.bar, 1u);
-                }
-                volatile unsigned* cnt = J.bar;
+                // the arrival releases this CTA's partials (written before the barrier above); the
+                // wait acquires everyone's once the count is in: no fence, no returning atomic
+                if (own) asm volatile("red.release.gpu.global.add.u32 [%0], 1;" ::"l"(J.bar) : "memory");
                 volatile int* verr = J.ctl;
                 long long t = 0;
                 int good = 1;
-                while ((int)(*cnt - arrived) < 0) {
+                for (;;) {
+                    unsigned c;
+                    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(c) : "l"(J.bar) : "memory");
+                    if ((int)(c - arrived) >= 0) break;
                     if (*verr != 0 || ++t > J.spin_limit) {
                         good = 0;
                         break;
@@ -1132,7 +1133,6 @@ __global__ void __launch_bounds__(NM_THREADS) nm_search_kernel(const NmJob J) {
                     __nanosleep(32);
                 }
                 if (!good) atomicCAS(J.ctl, 0, 1);
-                __threadfence();
                 s_ok = good;
             }
             __syncthreads();
