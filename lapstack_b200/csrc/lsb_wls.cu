@@ -688,10 +688,24 @@ __global__ void prolong_h_kernel(uint16_t* __restrict__ x, int w, int h, const u
 }
 
 // depth.rs:1037 `dot`, f64 products: per-block partials, then the partials in order.
+// Each thread's products (exact in f64) summed in a fixed order: 16-byte loads of four elements
+// at a time when both planes allow them (more bytes in flight), the elements past the last four
+// by the first threads.
 __global__ void dot_partial_kernel(const float* __restrict__ a, const float* __restrict__ b, size_t n, double* part) {
     double s = 0.0;
-    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
-        s += (double)a[i] * (double)b[i];
+    const size_t t0 = blockIdx.x * (size_t)blockDim.x + threadIdx.x, nt = (size_t)gridDim.x * blockDim.x;
+    const bool vec = ((reinterpret_cast<uintptr_t>(a) | reinterpret_cast<uintptr_t>(b)) & 15) == 0;
+    const size_t n4 = vec ? n / 4 : 0;
+    const float4* a4 = reinterpret_cast<const float4*>(a);
+    const float4* b4 = reinterpret_cast<const float4*>(b);
+    for (size_t i = t0; i < n4; i += nt) {
+        const float4 x = __ldg(a4 + i), y = __ldg(b4 + i);
+        s += (double)x.x * (double)y.x;
+        s += (double)x.y * (double)y.y;
+        s += (double)x.z * (double)y.z;
+        s += (double)x.w * (double)y.w;
+    }
+    for (size_t i = 4 * n4 + t0; i < n; i += nt) s += (double)a[i] * (double)b[i];
     __shared__ double red[256];
     red[threadIdx.x] = s;
     __syncthreads();
