@@ -398,82 +398,125 @@ cudaError_t resize_planes(const float* src, size_t stride, size_t pstride, int p
 // corners' images, the taps' reach and a pixel of margin, clamped like the
 // taps) is staged in shared memory once; the taps, weights and sums are
 // warp_plane_px's. Identity warps copy; tiles whose footprint does not fit,
-// and projective warps, take the per-pixel path.
+// and projective warps, take the per-pixel path. The CTAs are persistent: the
+// next tile's footprint arrives by cp.async into the other buffer while this
+// one is warped.
 constexpr int PT_W = 64, PT_H = 16, PB_W = PT_W + 16, PB_H = PT_H + 16;
+__device__ __forceinline__ void wp_cp4(float* sdst, const float* gsrc) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"((unsigned)__cvta_generic_to_shared(sdst)), "l"(gsrc));
+}
+// The footprint of tile t (affine warps): its origin and extent, and whether it fits the buffer.
+__device__ __forceinline__ bool wp_footprint(const double* m, int w, int h, int tiles_x, int t, int& bx0, int& by0, int& bw, int& bh) {
+    const int x0 = (t % tiles_x) * PT_W, y0 = (t / tiles_x) * PT_H;
+    double mnx = 1e300, mxx = -1e300, mny = 1e300, mxy = -1e300;
+    const int cx[2] = {x0, min(x0 + PT_W - 1, w - 1)}, cy[2] = {y0, min(y0 + PT_H - 1, h - 1)};
+    for (int a = 0; a < 2; a++)
+        for (int b = 0; b < 2; b++) {
+            double sx, sy;
+            src_point(m, true, (double)cx[a], (double)cy[b], sx, sy);
+            mnx = fmin(mnx, sx);
+            mxx = fmax(mxx, sx);
+            mny = fmin(mny, sy);
+            mxy = fmax(mxy, sy);
+        }
+    if (!(mnx > -1e9 && mxx < 1e9 && mny > -1e9 && mxy < 1e9)) return false;
+    bx0 = (int)floor(mnx) - 2;
+    by0 = (int)floor(mny) - 2;
+    bw = (int)floor(mxx) + 3 - bx0 + 1;
+    bh = (int)floor(mxy) + 3 - by0 + 1;
+    return bw <= PB_W && bh <= PB_H;
+}
 __global__ void __launch_bounds__(256) warp_plane_tile_kernel(const float* __restrict__ src, int w, int h, const double* __restrict__ wd,
                                                               float* __restrict__ out) {
-    __shared__ float box[PB_H][PB_W];
-    const int x0 = blockIdx.x * PT_W, y0 = blockIdx.y * PT_H, tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+    __shared__ float box[2][PB_H][PB_W];
+    __shared__ int fp[2][5];  // per buffer: fits, bx0, by0, bw, bh
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+    const int tiles_x = (w + PT_W - 1) / PT_W, ntiles = tiles_x * ((h + PT_H - 1) / PT_H);
     const bool ident = wd[10] != 0.0, affine = wd[9] != 0.0;
     double m[9];
     for (int q = 0; q < 9; q++) m[q] = wd[q];
-    int bx0 = 0, by0 = 0, bw = 0, bh = 0;
-    bool fits = false;
-    if (!ident && affine) {
-        double mnx = 1e300, mxx = -1e300, mny = 1e300, mxy = -1e300;
-        const int cx[2] = {x0, min(x0 + PT_W - 1, w - 1)}, cy[2] = {y0, min(y0 + PT_H - 1, h - 1)};
-        for (int a = 0; a < 2; a++)
-            for (int b = 0; b < 2; b++) {
-                double sx, sy;
-                src_point(m, true, (double)cx[a], (double)cy[b], sx, sy);
-                mnx = fmin(mnx, sx);
-                mxx = fmax(mxx, sx);
-                mny = fmin(mny, sy);
-                mxy = fmax(mxy, sy);
-            }
-        if (mnx > -1e9 && mxx < 1e9 && mny > -1e9 && mxy < 1e9) {
-            bx0 = (int)floor(mnx) - 2;
-            by0 = (int)floor(mny) - 2;
-            bw = (int)floor(mxx) + 3 - bx0 + 1;
-            bh = (int)floor(mxy) + 3 - by0 + 1;
-            fits = bw <= PB_W && bh <= PB_H;
-        }
-    }
-    if (fits) {
-        // the footprint's elements over all threads; m / bw by a multiply (exact for m < 2^16, bw <= 80)
-        const unsigned magic = (unsigned)((0xffffffffull + bw) / bw);
-        for (int m = threadIdx.x; m < bw * bh; m += 256) {
-            const int r = (int)__umulhi((unsigned)m, magic), c = m - r * bw;
-            box[r][c] = src[(size_t)min(max(by0 + r, 0), h - 1) * w + min(max(bx0 + c, 0), w - 1)];
+    // tile t's footprint into buffer b (thread 0 decides, every thread copies its share)
+    auto stage = [&](int t, int b) {
+        if (threadIdx.x == 0) {
+            int bx0 = 0, by0 = 0, bw = 0, bh = 0;
+            const bool f = t < ntiles && !ident && affine && wp_footprint(m, w, h, tiles_x, t, bx0, by0, bw, bh);
+            fp[b][0] = f;
+            fp[b][1] = bx0;
+            fp[b][2] = by0;
+            fp[b][3] = bw;
+            fp[b][4] = bh;
         }
         __syncthreads();
-    }
+        if (fp[b][0]) {
+            const int bx0 = fp[b][1], by0 = fp[b][2], bw = fp[b][3], bh = fp[b][4];
+            // m / bw by a multiply (exact for m < 2^16, bw <= 80)
+            const unsigned magic = (unsigned)((0xffffffffull + bw) / bw);
+            for (int e = threadIdx.x; e < bw * bh; e += 256) {
+                const int r = (int)__umulhi((unsigned)e, magic), c = e - r * bw;
+                wp_cp4(&box[b][r][c], src + (size_t)min(max(by0 + r, 0), h - 1) * w + min(max(bx0 + c, 0), w - 1));
+            }
+        }
+        asm volatile("cp.async.commit_group;\n" ::);
+    };
+    int b = 0;
+    stage(blockIdx.x, 0);
+    for (int t = blockIdx.x; t < ntiles; t += gridDim.x, b ^= 1) {
+        stage(t + gridDim.x, b ^ 1);  // the other buffer's last reader finished before the loop's last barrier
+        asm volatile("cp.async.wait_group 1;\n" ::);
+        __syncthreads();  // tile t's footprint is in
+        const int x0 = (t % tiles_x) * PT_W, y0 = (t / tiles_x) * PT_H;
+        const bool fits = fp[b][0] != 0;
+        const int bx0 = fp[b][1], by0 = fp[b][2];
 #pragma unroll 1
-    for (int q = 0; q < 4; q++) {
-        const int x = x0 + tx + 32 * (q & 1), y = y0 + ty + 8 * (q >> 1);
-        if (x >= w || y >= h) continue;
-        const size_t k = (size_t)y * w + x;
-        if (ident) {
-            out[k] = src[k];
-            continue;
-        }
-        if (!fits) {
-            out[k] = warp_plane_px(src, w, h, m, affine, 3, x, y);
-            continue;
-        }
-        double sx, sy;
-        src_point(m, true, (double)x, (double)y, sx, sy);
-        const double fx = floor(sx), fy = floor(sy);
-        const int ix = (int)fx - 1 - bx0, iy = (int)fy - 1 - by0;
-        float wx[4], wy[4];
-        spline4_d(__dsub_rn(sx, fx), wx);
-        spline4_d(__dsub_rn(sy, fy), wy);
-        float acc = 0.f;
+        for (int q = 0; q < 4; q++) {
+            const int x = x0 + tx + 32 * (q & 1), y = y0 + ty + 8 * (q >> 1);
+            if (x >= w || y >= h) continue;
+            const size_t k = (size_t)y * w + x;
+            if (ident) {
+                out[k] = src[k];
+                continue;
+            }
+            if (!fits) {
+                out[k] = warp_plane_px(src, w, h, m, affine, 3, x, y);
+                continue;
+            }
+            double sx, sy;
+            src_point(m, true, (double)x, (double)y, sx, sy);
+            const double fx = floor(sx), fy = floor(sy);
+            const int ix = (int)fx - 1 - bx0, iy = (int)fy - 1 - by0;
+            float wx[4], wy[4];
+            spline4_d(__dsub_rn(sx, fx), wx);
+            spline4_d(__dsub_rn(sy, fy), wy);
+            float acc = 0.f;
 #pragma unroll
-        for (int j = 0; j < 4; j++) {
-            float r = 0.f;
+            for (int j = 0; j < 4; j++) {
+                float r = 0.f;
 #pragma unroll
-            for (int i = 0; i < 4; i++) r = __fadd_rn(r, __fmul_rn(wx[i], box[iy + j][ix + i]));
-            acc = __fadd_rn(acc, __fmul_rn(wy[j], r));
+                for (int i = 0; i < 4; i++) r = __fadd_rn(r, __fmul_rn(wx[i], box[b][iy + j][ix + i]));
+                acc = __fadd_rn(acc, __fmul_rn(wy[j], r));
+            }
+            out[k] = acc;
         }
-        out[k] = acc;
+        __syncthreads();  // buffer b and its footprint record are free for tile t + 2 grid
     }
+    asm volatile("cp.async.wait_group 0;\n" ::);
+}
+
+static int warp_plane_grid(int ntiles) {
+    static const int resident = [] {  // once per process, whichever thread comes first
+        int dev = 0, sms = 1, per_sm = 1;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, warp_plane_tile_kernel, 256, 0) != cudaSuccess || per_sm < 1) per_sm = 1;
+        return per_sm * std::max(sms, 1);
+    }();
+    return std::max(1, std::min(ntiles, resident));
 }
 
 cudaError_t warp_plane_dev(const float* src, int w, int h, const double* warp_dev, int interp, float* out, cudaStream_t s) {
     if (interp == 3) {
-        dim3 g((w + PT_W - 1) / PT_W, (h + PT_H - 1) / PT_H);
-        lsb_launched(), warp_plane_tile_kernel<<<g, 256, 0, s>>>(src, w, h, warp_dev, out);
+        const int ntiles = ((w + PT_W - 1) / PT_W) * ((h + PT_H - 1) / PT_H);
+        lsb_launched(), warp_plane_tile_kernel<<<warp_plane_grid(ntiles), 256, 0, s>>>(src, w, h, warp_dev, out);
         return cudaGetLastError();
     }
     dim3 b(32, 8), g((w + 31) / 32, (h + 7) / 8);
@@ -1205,7 +1248,7 @@ __global__ void __launch_bounds__(NM_THREADS) nm_search_kernel(const NmJob J) {
     }
 }
 
-static int g_nm_blocks = 0;
+static std::atomic<int> g_nm_blocks{0};  // the search's grid on this device (set once, by any thread)
 
 // One frame's search job: the levels searched (coarsest first) and the free parameters.
 static cudaError_t nm_job(AlignCtx& C, const float* rf, const std::vector<float*>& pr, const float* tg, const std::vector<float*>& pt,
@@ -1228,7 +1271,7 @@ static cudaError_t nm_job(AlignCtx& C, const float* rf, const std::vector<float*
     J.H = h;
     for (int q = 0; q < 8; q++)
         if (freem[q]) J.free_idx[J.nfree++] = q;
-    if (g_nm_blocks == 0) {
+    if (g_nm_blocks.load() == 0) {
         int dev = 0, sms = 0, per = 0;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
@@ -1237,7 +1280,7 @@ static cudaError_t nm_job(AlignCtx& C, const float* rf, const std::vector<float*
         if (per < 1) return cudaErrorCooperativeLaunchTooLarge;
         int want = 2;  // CTAs per SM: more warps hide the gathers, more CTAs make every barrier dearer
         if (const char* v = getenv("LSB_NM_CTAS_PER_SM")) want = std::max(1, atoi(v));
-        g_nm_blocks = std::min(std::min(per, want) * sms, NM_MAX_BLOCKS);
+        g_nm_blocks.store(std::min(std::min(per, want) * sms, NM_MAX_BLOCKS));
     }
     J.spin_limit = spin_limit();
     J.part = C.nm_part;
@@ -1251,7 +1294,7 @@ static cudaError_t nm_launch(AlignCtx& C, NmJob& J) {
     if (e != cudaSuccess) return e;
     void* args[] = {(void*)&J};
     lsb_launched();
-    const int blocks = C.max_blocks > 0 ? std::min(g_nm_blocks, C.max_blocks) : g_nm_blocks;
+    const int blocks = C.max_blocks > 0 ? std::min(g_nm_blocks.load(), C.max_blocks) : g_nm_blocks.load();
     return cudaLaunchCooperativeKernel((void*)nm_search_kernel, dim3(blocks), dim3(NM_THREADS), args, 0, C.s);
 }
 

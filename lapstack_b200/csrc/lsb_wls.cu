@@ -197,9 +197,8 @@ __global__ void vc_down_kernel(const float* __restrict__ b, const float* __restr
 // ... and its way up in one pass (depth.rs:932-946): the prolongation x += P x_c (depth.rs:901) and the
 // damped Jacobi sweep (depth.rs:837) on the corrected x, the neighbours' corrected x recomputed by the
 // same addition; into out (another buffer than x).
-__device__ __forceinline__ float prolonged_at(const float* __restrict__ x, const float* __restrict__ xc, int w, int cw, size_t k) {
-    const int y = (int)(k / w), i = (int)(k - (size_t)y * w);
-    return __fadd_rn(x[k], xc[(size_t)(y / 2) * cw + i / 2]);
+__device__ __forceinline__ float prolonged_at(const float* __restrict__ x, const float* __restrict__ xc, int w, int cw, int i, int y) {
+    return __fadd_rn(x[(size_t)y * w + i], xc[(size_t)(y >> 1) * cw + (i >> 1)]);
 }
 __global__ void vc_up_kernel(const float* __restrict__ x, const float* __restrict__ xc, int cw, const float* __restrict__ b,
                              const float* __restrict__ wd, const float* __restrict__ ax, const float* __restrict__ ay,
@@ -207,12 +206,12 @@ __global__ void vc_up_kernel(const float* __restrict__ x, const float* __restric
     const int i = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
     if (i >= w || y >= h) return;
     const size_t k = (size_t)y * w + i;
-    const float xk = prolonged_at(x, xc, w, cw, k);
+    const float xk = prolonged_at(x, xc, w, cw, i, y);
     float v = __fmul_rn(wd[k], xk);
-    if (i > 0) v = __fadd_rn(v, __fmul_rn(ax[k - 1], __fsub_rn(xk, prolonged_at(x, xc, w, cw, k - 1))));
-    if (i + 1 < w) v = __fadd_rn(v, __fmul_rn(ax[k], __fsub_rn(xk, prolonged_at(x, xc, w, cw, k + 1))));
-    if (y > 0) v = __fadd_rn(v, __fmul_rn(ay[k - w], __fsub_rn(xk, prolonged_at(x, xc, w, cw, k - w))));
-    if (y + 1 < h) v = __fadd_rn(v, __fmul_rn(ay[k], __fsub_rn(xk, prolonged_at(x, xc, w, cw, k + w))));
+    if (i > 0) v = __fadd_rn(v, __fmul_rn(ax[k - 1], __fsub_rn(xk, prolonged_at(x, xc, w, cw, i - 1, y))));
+    if (i + 1 < w) v = __fadd_rn(v, __fmul_rn(ax[k], __fsub_rn(xk, prolonged_at(x, xc, w, cw, i + 1, y))));
+    if (y > 0) v = __fadd_rn(v, __fmul_rn(ay[k - w], __fsub_rn(xk, prolonged_at(x, xc, w, cw, i, y - 1))));
+    if (y + 1 < h) v = __fadd_rn(v, __fmul_rn(ay[k], __fsub_rn(xk, prolonged_at(x, xc, w, cw, i, y + 1))));
     out[k] = __fadd_rn(xk, __fmul_rn(__fmul_rn(MG_OMEGA, dinv[k]), __fsub_rn(b[k], v)));
 }
 
