@@ -10,6 +10,7 @@
 
 #include <algorithm>
 #include <functional>
+#include <type_traits>
 #include <vector>
 
 #include "lsb_common.cuh"
@@ -651,12 +652,15 @@ __global__ void to_bf16_kernel(const float* __restrict__ a, uint16_t* __restrict
 __global__ void from_bf16_kernel(const uint16_t* __restrict__ a, float* __restrict__ o, size_t n) {
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) o[i] = ldh(a, i);
 }
-// mode 1: out = b - A x; mode 2: out = x + w D^-1 (b - A x)
-__global__ void stencil_h_kernel(const uint16_t* __restrict__ x, const uint16_t* __restrict__ b, const uint16_t* __restrict__ wd,
-                                 const uint16_t* __restrict__ ax, const uint16_t* __restrict__ ay, const uint16_t* __restrict__ dinv,
-                                 uint16_t* __restrict__ out, int w, int h, int mode) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
-    if (i >= w || y >= h) return;
+// A level's right-hand side and a sweep's output are BF16 (uint16_t) below level 0; at level 0 the
+// right-hand side is the CG's FP32 residual and the last sweep writes the FP32 z.
+__device__ __forceinline__ float ldv(const uint16_t* p, size_t k) { return ldh(p, k); }
+__device__ __forceinline__ float ldv(const float* p, size_t k) { return p[k]; }
+__device__ __forceinline__ void stv(uint16_t* p, size_t k, float v) { sth(p, k, v); }
+__device__ __forceinline__ void stv(float* p, size_t k, float v) { p[k] = v; }
+__device__ __forceinline__ float stencil_h_at(const uint16_t* __restrict__ x, float bk, const uint16_t* __restrict__ wd,
+                                              const uint16_t* __restrict__ ax, const uint16_t* __restrict__ ay,
+                                              const uint16_t* __restrict__ dinv, int w, int h, int i, int y, int mode) {
     const size_t k = (size_t)y * w + i;
     const float xk = ldh(x, k);
     float v = ldh(wd, k) * xk;
@@ -664,12 +668,58 @@ __global__ void stencil_h_kernel(const uint16_t* __restrict__ x, const uint16_t*
     if (i + 1 < w) v += ldh(ax, k) * (xk - ldh(x, k + 1));
     if (y > 0) v += ldh(ay, k - w) * (xk - ldh(x, k - w));
     if (y + 1 < h) v += ldh(ay, k) * (xk - ldh(x, k + w));
-    const float r = ldh(b, k) - v;
-    sth(out, k, mode == 1 ? r : xk + MG_OMEGA * ldh(dinv, k) * r);
+    const float r = bk - v;
+    return mode == 1 ? r : xk + MG_OMEGA * ldh(dinv, k) * r;
 }
-__global__ void jac0_h_kernel(const uint16_t* __restrict__ b, const uint16_t* __restrict__ dinv, uint16_t* __restrict__ x, size_t n) {
+// mode 1: out = b - A x; mode 2: out = x + w D^-1 (b - A x)
+template <class BT, class OT>
+__global__ void stencil_h_kernel(const uint16_t* __restrict__ x, const BT* __restrict__ b, const uint16_t* __restrict__ wd,
+                                 const uint16_t* __restrict__ ax, const uint16_t* __restrict__ ay, const uint16_t* __restrict__ dinv,
+                                 OT* __restrict__ out, int w, int h, int mode) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
+    if (i >= w || y >= h) return;
+    const size_t k = (size_t)y * w + i;
+    stv(out, k, stencil_h_at(x, ldv(b, k), wd, ax, ay, dinv, w, h, i, y, mode));
+}
+template <class BT>
+__global__ void jac0_h_kernel(const BT* __restrict__ b, const uint16_t* __restrict__ dinv, uint16_t* __restrict__ x, size_t n) {
     for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x)
-        sth(x, k, MG_OMEGA * ldh(dinv, k) * ldh(b, k));
+        sth(x, k, MG_OMEGA * ldh(dinv, k) * ldv(b, k));
+}
+// The coarsest level's sweeps in one CTA of 32 x 32 threads with the level's planes in shared memory:
+// the zero-start sweep, then sweeps - 1 damped Jacobi sweeps between two buffers, __syncthreads
+// between them; the result is written to x.
+constexpr int COARSE_H_PLANES = 7;
+__global__ void __launch_bounds__(1024) coarse_h_kernel(uint16_t* __restrict__ x, const uint16_t* __restrict__ b,
+                                                        const uint16_t* __restrict__ wd, const uint16_t* __restrict__ ax,
+                                                        const uint16_t* __restrict__ ay, const uint16_t* __restrict__ dinv, int w,
+                                                        int h, int sweeps) {
+    extern __shared__ uint16_t csm[];
+    const int n = w * h, tid = threadIdx.y * 32 + threadIdx.x;
+    uint16_t *sb = csm, *swd = sb + n, *sax = swd + n, *say = sax + n, *sdi = say + n, *s0 = sdi + n, *s1 = s0 + n;
+    for (int k = tid; k < n; k += 1024) {
+        sb[k] = b[k];
+        swd[k] = wd[k];
+        sax[k] = ax[k];
+        say[k] = ay[k];
+        sdi[k] = dinv[k];
+    }
+    __syncthreads();
+    for (int k = tid; k < n; k += 1024) sth(s0, k, MG_OMEGA * ldh(sdi, k) * ldh(sb, k));
+    uint16_t *src = s0, *dst = s1;
+    for (int sw = 1; sw < sweeps; sw++) {
+        __syncthreads();
+        for (int y = threadIdx.y; y < h; y += 32)
+            for (int i = threadIdx.x; i < w; i += 32) {
+                const size_t k = (size_t)y * w + i;
+                sth(dst, k, stencil_h_at(src, ldh(sb, k), swd, sax, say, sdi, w, h, i, y, 2));
+            }
+        uint16_t* t = src;
+        src = dst;
+        dst = t;
+    }
+    __syncthreads();
+    for (int k = tid; k < n; k += 1024) x[k] = src[k];
 }
 __global__ void block_sum_h_kernel(const uint16_t* __restrict__ src, int w, int h, uint16_t* __restrict__ dst, int cw, int ch) {
     const int xx = blockIdx.x * blockDim.x + threadIdx.x, yy = blockIdx.y * blockDim.y + threadIdx.y;
@@ -771,6 +821,12 @@ __global__ void fill_kernel(float* o, float v, size_t n) {
 
 WlsSolver* wls_alloc(int w, int h, cudaError_t* err) {
     *err = cudaSuccess;
+    // set here, outside the graph captures of the CG iteration that launch it
+    static const cudaError_t coarse_attr = cudaFuncSetAttribute(coarse_h_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+    if (coarse_attr != cudaSuccess) {
+        *err = coarse_attr;
+        return nullptr;
+    }
     WlsSolver* S = new WlsSolver();
     S->w = w;
     S->h = h;
@@ -919,30 +975,50 @@ static void vcycle(WlsSolver* S, size_t l, cudaStream_t s) {
     jacobi(T, false, s);
 }
 
-static void jacobi_h(WlsLevel& L, bool zero, cudaStream_t s) {
+// A damped Jacobi sweep on level L (zero: the zero-start one) against the right-hand side b
+// (BF16, or level 0's FP32 residual); z32: the sweep's output goes there as FP32 instead of x.
+template <class BT>
+static void jacobi_h(WlsLevel& L, const BT* b, bool zero, cudaStream_t s, float* z32 = nullptr) {
     if (zero) {
-        lsb_launched(), jac0_h_kernel<<<g1((size_t)L.w * L.h), 256, 0, s>>>(L.hb, L.hdinv, L.hx, (size_t)L.w * L.h);
+        lsb_launched(), jac0_h_kernel<BT><<<g1((size_t)L.w * L.h), 256, 0, s>>>(b, L.hdinv, L.hx, (size_t)L.w * L.h);
         return;
     }
-    lsb_launched(), stencil_h_kernel<<<g2(L.w, L.h), B2, 0, s>>>(L.hx, L.hb, L.hwd, L.hax, L.hay, L.hdinv, L.hr, L.w, L.h, 2);
+    if (z32) {
+        lsb_launched(), stencil_h_kernel<BT, float><<<g2(L.w, L.h), B2, 0, s>>>(L.hx, b, L.hwd, L.hax, L.hay, L.hdinv, z32, L.w, L.h, 2);
+        return;
+    }
+    lsb_launched(), stencil_h_kernel<BT, uint16_t><<<g2(L.w, L.h), B2, 0, s>>>(L.hx, b, L.hwd, L.hax, L.hay, L.hdinv, L.hr, L.w, L.h, 2);
     std::swap(L.hx, L.hr);
 }
-// the mixed-precision V-cycle: MG_H_SWEEPS pre/post sweeps, MG_H_LEVELS levels,
-// MG_COARSE sweeps on the coarsest
-static void vcycle_h(WlsSolver* S, size_t l, cudaStream_t s) {
+static size_t coarse_h_smem(const WlsLevel& L) { return sizeof(uint16_t) * COARSE_H_PLANES * (size_t)L.w * L.h; }
+static bool coarse_h_fits(const WlsLevel& L) { return coarse_h_smem(L) <= 227 * 1024; }
+// the mixed-precision V-cycle: MG_H_SWEEPS pre/post sweeps, MG_H_LEVELS levels, MG_COARSE sweeps on
+// the coarsest (one CTA). b32 / z32: level 0 takes the CG's FP32 residual as its right-hand side and
+// its last sweep writes the FP32 z (no conversion passes).
+static void vcycle_h(WlsSolver* S, size_t l, cudaStream_t s, const float* b32 = nullptr, float* z32 = nullptr) {
     WlsLevel& T = S->lv[l];
     const size_t last = std::min(S->lv.size(), (size_t)MG_H_LEVELS) - 1;
     if (l == last) {
-        for (int k = 0; k < MG_COARSE; k++) jacobi_h(T, k == 0, s);
+        if (coarse_h_fits(T)) {
+            const size_t smem = coarse_h_smem(T);  // at most 227 KB (wls_alloc raised the kernel's limit)
+            lsb_launched(), coarse_h_kernel<<<1, dim3(32, 32), smem, s>>>(T.hx, T.hb, T.hwd, T.hax, T.hay, T.hdinv, T.w, T.h, MG_COARSE);
+        } else {
+            for (int k = 0; k < MG_COARSE; k++) jacobi_h(T, (const uint16_t*)T.hb, k == 0, s);
+        }
         return;
     }
-    for (int k = 0; k < MG_H_SWEEPS; k++) jacobi_h(T, k == 0, s);
-    lsb_launched(), stencil_h_kernel<<<g2(T.w, T.h), B2, 0, s>>>(T.hx, T.hb, T.hwd, T.hax, T.hay, T.hdinv, T.hr, T.w, T.h, 1);
-    WlsLevel& C = S->lv[l + 1];
-    lsb_launched(), block_sum_h_kernel<<<g2(C.w, C.h), B2, 0, s>>>(T.hr, T.w, T.h, C.hb, C.w, C.h);
-    vcycle_h(S, l + 1, s);
-    lsb_launched(), prolong_h_kernel<<<g2(T.w, T.h), B2, 0, s>>>(T.hx, T.w, T.h, C.hx, C.w);
-    for (int k = 0; k < MG_H_SWEEPS; k++) jacobi_h(T, false, s);
+    auto down_up = [&](auto* b) {
+        for (int k = 0; k < MG_H_SWEEPS; k++) jacobi_h(T, b, k == 0, s);
+        using BT = std::remove_cv_t<std::remove_pointer_t<decltype(b)>>;
+        lsb_launched(), stencil_h_kernel<BT, uint16_t><<<g2(T.w, T.h), B2, 0, s>>>(T.hx, b, T.hwd, T.hax, T.hay, T.hdinv, T.hr, T.w, T.h, 1);
+        WlsLevel& C = S->lv[l + 1];
+        lsb_launched(), block_sum_h_kernel<<<g2(C.w, C.h), B2, 0, s>>>(T.hr, T.w, T.h, C.hb, C.w, C.h);
+        vcycle_h(S, l + 1, s);
+        lsb_launched(), prolong_h_kernel<<<g2(T.w, T.h), B2, 0, s>>>(T.hx, T.w, T.h, C.hx, C.w);
+        for (int k = 0; k < MG_H_SWEEPS; k++) jacobi_h(T, b, false, s, k + 1 == MG_H_SWEEPS ? z32 : nullptr);
+    };
+    if (b32) down_up(b32);
+    else down_up((const uint16_t*)T.hb);
 }
 
 static void dot(WlsSolver* S, const float* a, const float* b, size_t n, int mode, cudaStream_t s) {
@@ -983,6 +1059,10 @@ cudaError_t wls_solve(WlsSolver* S, const float* d, int max_iters, float* u, flo
     lsb_launched(), stencil_kernel<<<g2(w, h), B2, 0, s>>>(u, S->f, L0.wd, L0.ax, L0.ay, L0.dinv, S->r, w, h, 1);
     auto precond = [&]() {
         if (mode == 1) {
+            if (std::min(S->lv.size(), (size_t)MG_H_LEVELS) > 1) {  // r in, z out, no conversion passes
+                vcycle_h(S, 0, s, S->r, S->z);
+                return;
+            }
             lsb_launched(), to_bf16_kernel<<<g1(n), 256, 0, s>>>(S->r, L0.hb, n);
             vcycle_h(S, 0, s);
             lsb_launched(), from_bf16_kernel<<<g1(n), 256, 0, s>>>(S->lv[0].hx, S->z, n);
