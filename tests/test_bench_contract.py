@@ -64,3 +64,14 @@ def test_cuda_arm_stops_without_a_device():
     p = run_bench("--config", "c1", "--steps", "1", "--warmup", "0")
     assert p.returncode != 0
     assert json_lines(p.stdout) == []
+
+
+def test_batch_mode_stops_without_a_device():
+    """The uneven-batch line (--batch) comes from the CUDA engine only: without a device it stops with an
+    error and prints no line."""
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a CUDA device is present")
+    p = run_bench("--batch", "--steps", "1", "--warmup", "0")
+    assert p.returncode != 0
+    assert json_lines(p.stdout) == []
