@@ -172,23 +172,35 @@ __global__ void prolong_kernel(float* __restrict__ x, int w, int h, const float*
 __device__ __forceinline__ float jac0_at(const float* __restrict__ b, const float* __restrict__ dinv, size_t k) {
     return __fmul_rn(__fmul_rn(MG_OMEGA, dinv[k]), b[k]);
 }
-__global__ void vc_down_kernel(const float* __restrict__ b, const float* __restrict__ wd, const float* __restrict__ ax,
-                               const float* __restrict__ ay, const float* __restrict__ dinv, float* __restrict__ x, int w, int h,
-                               float* __restrict__ cb, int cw, int ch) {
+// A 32 x 8 block of coarse cells covers 64 x 16 fine cells: their x and a one-cell ring are
+// computed once into shared memory, and every fine cell's residual reads its neighbours there.
+constexpr int VC_FW = 2 * 32 + 2, VC_FH = 2 * 8 + 2;
+__global__ void __launch_bounds__(256) vc_down_kernel(const float* __restrict__ b, const float* __restrict__ wd, const float* __restrict__ ax,
+                                                      const float* __restrict__ ay, const float* __restrict__ dinv, float* __restrict__ x,
+                                                      int w, int h, float* __restrict__ cb, int cw, int ch) {
+    __shared__ float J[VC_FH][VC_FW];
+    const int fx0 = 2 * blockIdx.x * blockDim.x - 1, fy0 = 2 * blockIdx.y * blockDim.y - 1;
+    for (int e = threadIdx.y * blockDim.x + threadIdx.x; e < VC_FW * VC_FH; e += blockDim.x * blockDim.y) {
+        const int r = e / VC_FW, c = e - r * VC_FW, gx = fx0 + c, gy = fy0 + r;
+        J[r][c] = gx >= 0 && gx < w && gy >= 0 && gy < h ? jac0_at(b, dinv, (size_t)gy * w + gx) : 0.f;
+    }
+    __syncthreads();
     const int xx = blockIdx.x * blockDim.x + threadIdx.x, yy = blockIdx.y * blockDim.y + threadIdx.y;
     if (xx >= cw || yy >= ch) return;
     float o = 0.f;
     for (int y = 2 * yy; y < min(2 * yy + 2, h); y++) {
         float rs = 0.f;
+        const int jr = y - fy0;
         for (int i = 2 * xx; i < min(2 * xx + 2, w); i++) {
             const size_t k = (size_t)y * w + i;
-            const float xk = jac0_at(b, dinv, k);
+            const int jc = i - fx0;
+            const float xk = J[jr][jc];
             x[k] = xk;
             float v = __fmul_rn(wd[k], xk);
-            if (i > 0) v = __fadd_rn(v, __fmul_rn(ax[k - 1], __fsub_rn(xk, jac0_at(b, dinv, k - 1))));
-            if (i + 1 < w) v = __fadd_rn(v, __fmul_rn(ax[k], __fsub_rn(xk, jac0_at(b, dinv, k + 1))));
-            if (y > 0) v = __fadd_rn(v, __fmul_rn(ay[k - w], __fsub_rn(xk, jac0_at(b, dinv, k - w))));
-            if (y + 1 < h) v = __fadd_rn(v, __fmul_rn(ay[k], __fsub_rn(xk, jac0_at(b, dinv, k + w))));
+            if (i > 0) v = __fadd_rn(v, __fmul_rn(ax[k - 1], __fsub_rn(xk, J[jr][jc - 1])));
+            if (i + 1 < w) v = __fadd_rn(v, __fmul_rn(ax[k], __fsub_rn(xk, J[jr][jc + 1])));
+            if (y > 0) v = __fadd_rn(v, __fmul_rn(ay[k - w], __fsub_rn(xk, J[jr - 1][jc])));
+            if (y + 1 < h) v = __fadd_rn(v, __fmul_rn(ay[k], __fsub_rn(xk, J[jr + 1][jc])));
             rs = __fadd_rn(rs, __fsub_rn(b[k], v));
         }
         o = __fadd_rn(o, rs);
@@ -201,18 +213,28 @@ __global__ void vc_down_kernel(const float* __restrict__ b, const float* __restr
 __device__ __forceinline__ float prolonged_at(const float* __restrict__ x, const float* __restrict__ xc, int w, int cw, int i, int y) {
     return __fadd_rn(x[(size_t)y * w + i], xc[(size_t)(y >> 1) * cw + (i >> 1)]);
 }
-__global__ void vc_up_kernel(const float* __restrict__ x, const float* __restrict__ xc, int cw, const float* __restrict__ b,
-                             const float* __restrict__ wd, const float* __restrict__ ax, const float* __restrict__ ay,
-                             const float* __restrict__ dinv, float* __restrict__ out, int w, int h) {
+// The block's 32 x 8 corrected x and a one-cell ring are computed once into shared memory.
+__global__ void __launch_bounds__(256) vc_up_kernel(const float* __restrict__ x, const float* __restrict__ xc, int cw,
+                                                    const float* __restrict__ b, const float* __restrict__ wd,
+                                                    const float* __restrict__ ax, const float* __restrict__ ay,
+                                                    const float* __restrict__ dinv, float* __restrict__ out, int w, int h) {
+    __shared__ float X[8 + 2][32 + 2];
+    const int x0 = blockIdx.x * blockDim.x - 1, y0 = blockIdx.y * blockDim.y - 1;
+    for (int e = threadIdx.y * blockDim.x + threadIdx.x; e < 10 * 34; e += blockDim.x * blockDim.y) {
+        const int r = e / 34, c = e - r * 34, gx = x0 + c, gy = y0 + r;
+        X[r][c] = gx >= 0 && gx < w && gy >= 0 && gy < h ? prolonged_at(x, xc, w, cw, gx, gy) : 0.f;
+    }
+    __syncthreads();
     const int i = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
     if (i >= w || y >= h) return;
     const size_t k = (size_t)y * w + i;
-    const float xk = prolonged_at(x, xc, w, cw, i, y);
+    const int r = threadIdx.y + 1, c = threadIdx.x + 1;
+    const float xk = X[r][c];
     float v = __fmul_rn(wd[k], xk);
-    if (i > 0) v = __fadd_rn(v, __fmul_rn(ax[k - 1], __fsub_rn(xk, prolonged_at(x, xc, w, cw, i - 1, y))));
-    if (i + 1 < w) v = __fadd_rn(v, __fmul_rn(ax[k], __fsub_rn(xk, prolonged_at(x, xc, w, cw, i + 1, y))));
-    if (y > 0) v = __fadd_rn(v, __fmul_rn(ay[k - w], __fsub_rn(xk, prolonged_at(x, xc, w, cw, i, y - 1))));
-    if (y + 1 < h) v = __fadd_rn(v, __fmul_rn(ay[k], __fsub_rn(xk, prolonged_at(x, xc, w, cw, i, y + 1))));
+    if (i > 0) v = __fadd_rn(v, __fmul_rn(ax[k - 1], __fsub_rn(xk, X[r][c - 1])));
+    if (i + 1 < w) v = __fadd_rn(v, __fmul_rn(ax[k], __fsub_rn(xk, X[r][c + 1])));
+    if (y > 0) v = __fadd_rn(v, __fmul_rn(ay[k - w], __fsub_rn(xk, X[r - 1][c])));
+    if (y + 1 < h) v = __fadd_rn(v, __fmul_rn(ay[k], __fsub_rn(xk, X[r + 1][c])));
     out[k] = __fadd_rn(xk, __fmul_rn(__fmul_rn(MG_OMEGA, dinv[k]), __fsub_rn(b[k], v)));
 }
 
