@@ -708,6 +708,87 @@ __global__ void jac0_h_kernel(const BT* __restrict__ b, const uint16_t* __restri
     for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x)
         sth(x, k, MG_OMEGA * ldh(dinv, k) * ldv(b, k));
 }
+// A fine level's way down and way up in one pass each, on tiles in shared memory: the same values
+// as the separate kernels (every sweep's output rounded to BF16 where they store it), the
+// neighbours' values computed once per block over a ring around the tile.
+__device__ __forceinline__ float rbf(float v) { return __bfloat162float(__float2bfloat16_rn(v)); }
+// stencil_h_at with x read from a shared tile: (r, c) the cell's place in the tile
+template <int PITCH>
+__device__ __forceinline__ float sweep_tile(const float* X, int r, int c, float bk, const uint16_t* __restrict__ wd,
+                                            const uint16_t* __restrict__ ax, const uint16_t* __restrict__ ay,
+                                            const uint16_t* __restrict__ dinv, int w, int h, int i, int y, int mode) {
+    const size_t k = (size_t)y * w + i;
+    const float xk = X[r * PITCH + c];
+    float v = ldh(wd, k) * xk;
+    if (i > 0) v += ldh(ax, k - 1) * (xk - X[r * PITCH + c - 1]);
+    if (i + 1 < w) v += ldh(ax, k) * (xk - X[r * PITCH + c + 1]);
+    if (y > 0) v += ldh(ay, k - w) * (xk - X[(r - 1) * PITCH + c]);
+    if (y + 1 < h) v += ldh(ay, k) * (xk - X[(r + 1) * PITCH + c]);
+    const float rr = bk - v;
+    return mode == 1 ? rr : xk + MG_OMEGA * ldh(dinv, k) * rr;
+}
+// Down: x0 = w D^-1 b, x1 = one sweep, r = b - A x1, its 2x2 block sums; x1 -> x, the sums -> cb.
+// A 32 x 8 block of coarse cells: x0 over its 64 x 16 fine cells and a 2-cell ring, x1 with a 1-cell ring.
+constexpr int VH_D0W = 64 + 4, VH_D0H = 16 + 4, VH_D1W = 64 + 2, VH_D1H = 16 + 2;
+template <class BT>
+__global__ void __launch_bounds__(256) vc_down_h_kernel(const BT* __restrict__ b, const uint16_t* __restrict__ wd,
+                                                        const uint16_t* __restrict__ ax, const uint16_t* __restrict__ ay,
+                                                        const uint16_t* __restrict__ dinv, uint16_t* __restrict__ x, int w, int h,
+                                                        uint16_t* __restrict__ cb, int cw, int ch) {
+    __shared__ float X0[VH_D0H * VH_D0W], X1[VH_D1H * VH_D1W];
+    const int tid = threadIdx.y * 32 + threadIdx.x, fx = 64 * blockIdx.x, fy = 16 * blockIdx.y;
+    for (int e = tid; e < VH_D0W * VH_D0H; e += 256) {
+        const int r = e / VH_D0W, c = e - r * VH_D0W, gx = fx - 2 + c, gy = fy - 2 + r;
+        X0[e] = gx >= 0 && gx < w && gy >= 0 && gy < h ? rbf(MG_OMEGA * ldh(dinv, (size_t)gy * w + gx) * ldv(b, (size_t)gy * w + gx)) : 0.f;
+    }
+    __syncthreads();
+    for (int e = tid; e < VH_D1W * VH_D1H; e += 256) {
+        const int r = e / VH_D1W, c = e - r * VH_D1W, gx = fx - 1 + c, gy = fy - 1 + r;
+        X1[e] = gx >= 0 && gx < w && gy >= 0 && gy < h
+                    ? rbf(sweep_tile<VH_D0W>(X0, r + 1, c + 1, ldv(b, (size_t)gy * w + gx), wd, ax, ay, dinv, w, h, gx, gy, 2))
+                    : 0.f;
+    }
+    __syncthreads();
+    const int xx = blockIdx.x * 32 + threadIdx.x, yy = blockIdx.y * 8 + threadIdx.y;
+    if (xx >= cw || yy >= ch) return;
+    float o = 0.f;
+    for (int y = 2 * yy; y < min(2 * yy + 2, h); y++)
+        for (int i = 2 * xx; i < min(2 * xx + 2, w); i++) {
+            const size_t k = (size_t)y * w + i;
+            const int r = y - fy + 1, c = i - fx + 1;
+            sth(x, k, X1[r * VH_D1W + c]);
+            o += rbf(sweep_tile<VH_D1W>(X1, r, c, ldv(b, k), wd, ax, ay, dinv, w, h, i, y, 1));
+        }
+    sth(cb, (size_t)yy * cw + xx, o);
+}
+// Up: x2 = x1 + P x_c, then two sweeps; the result -> out (BF16, or level 0's FP32 z).
+// A 32 x 8 block of fine cells: x2 with a 2-cell ring, the first sweep with a 1-cell ring.
+constexpr int VH_U2W = 32 + 4, VH_U2H = 8 + 4, VH_U3W = 32 + 2, VH_U3H = 8 + 2;
+template <class BT, class OT>
+__global__ void __launch_bounds__(256) vc_up_h_kernel(const uint16_t* __restrict__ x, const uint16_t* __restrict__ xc, int cw,
+                                                      const BT* __restrict__ b, const uint16_t* __restrict__ wd,
+                                                      const uint16_t* __restrict__ ax, const uint16_t* __restrict__ ay,
+                                                      const uint16_t* __restrict__ dinv, OT* __restrict__ out, int w, int h) {
+    __shared__ float X2[VH_U2H * VH_U2W], X3[VH_U3H * VH_U3W];
+    const int tid = threadIdx.y * 32 + threadIdx.x, fx = 32 * blockIdx.x, fy = 8 * blockIdx.y;
+    for (int e = tid; e < VH_U2W * VH_U2H; e += 256) {
+        const int r = e / VH_U2W, c = e - r * VH_U2W, gx = fx - 2 + c, gy = fy - 2 + r;
+        X2[e] = gx >= 0 && gx < w && gy >= 0 && gy < h ? rbf(ldh(x, (size_t)gy * w + gx) + ldh(xc, (size_t)(gy / 2) * cw + gx / 2)) : 0.f;
+    }
+    __syncthreads();
+    for (int e = tid; e < VH_U3W * VH_U3H; e += 256) {
+        const int r = e / VH_U3W, c = e - r * VH_U3W, gx = fx - 1 + c, gy = fy - 1 + r;
+        X3[e] = gx >= 0 && gx < w && gy >= 0 && gy < h
+                    ? rbf(sweep_tile<VH_U2W>(X2, r + 1, c + 1, ldv(b, (size_t)gy * w + gx), wd, ax, ay, dinv, w, h, gx, gy, 2))
+                    : 0.f;
+    }
+    __syncthreads();
+    const int i = fx + threadIdx.x, y = fy + threadIdx.y;
+    if (i >= w || y >= h) return;
+    const size_t k = (size_t)y * w + i;
+    stv(out, k, sweep_tile<VH_U3W>(X3, threadIdx.y + 1, threadIdx.x + 1, ldv(b, k), wd, ax, ay, dinv, w, h, i, y, 2));
+}
+
 // The coarsest level's sweeps in one CTA of 32 x 32 threads with the level's planes in shared memory:
 // the zero-start sweep, then sweeps - 1 damped Jacobi sweeps between two buffers, __syncthreads
 // between them; the result is written to x.
@@ -743,21 +824,6 @@ __global__ void __launch_bounds__(1024) coarse_h_kernel(uint16_t* __restrict__ x
     __syncthreads();
     for (int k = tid; k < n; k += 1024) x[k] = src[k];
 }
-__global__ void block_sum_h_kernel(const uint16_t* __restrict__ src, int w, int h, uint16_t* __restrict__ dst, int cw, int ch) {
-    const int xx = blockIdx.x * blockDim.x + threadIdx.x, yy = blockIdx.y * blockDim.y + threadIdx.y;
-    if (xx >= cw || yy >= ch) return;
-    float o = 0.f;
-    for (int y = 2 * yy; y < min(2 * yy + 2, h); y++)
-        for (int x = 2 * xx; x < min(2 * xx + 2, w); x++) o += ldh(src, (size_t)y * w + x);
-    sth(dst, (size_t)yy * cw + xx, o);
-}
-__global__ void prolong_h_kernel(uint16_t* __restrict__ x, int w, int h, const uint16_t* __restrict__ xc, int cw) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
-    if (i >= w || y >= h) return;
-    const size_t k = (size_t)y * w + i;
-    sth(x, k, ldh(x, k) + ldh(xc, (size_t)(y / 2) * cw + i / 2));
-}
-
 // depth.rs:1037 `dot`, f64 products: per-block partials, then the partials in order.
 // Each thread's products (exact in f64) summed in a fixed order: 16-byte loads of four elements
 // at a time when both planes allow them (more bytes in flight), the elements past the last four
@@ -997,19 +1063,15 @@ static void vcycle(WlsSolver* S, size_t l, cudaStream_t s) {
     jacobi(T, false, s);
 }
 
-// A damped Jacobi sweep on level L (zero: the zero-start one) against the right-hand side b
-// (BF16, or level 0's FP32 residual); z32: the sweep's output goes there as FP32 instead of x.
-template <class BT>
-static void jacobi_h(WlsLevel& L, const BT* b, bool zero, cudaStream_t s, float* z32 = nullptr) {
+// A damped Jacobi sweep on level L (zero: the zero-start one) against its BF16 right-hand side:
+// the coarsest level's sweeps when it does not fit one CTA's shared memory.
+static void jacobi_h(WlsLevel& L, bool zero, cudaStream_t s) {
     if (zero) {
-        lsb_launched(), jac0_h_kernel<BT><<<g1((size_t)L.w * L.h), 256, 0, s>>>(b, L.hdinv, L.hx, (size_t)L.w * L.h);
+        lsb_launched(), jac0_h_kernel<uint16_t><<<g1((size_t)L.w * L.h), 256, 0, s>>>(L.hb, L.hdinv, L.hx, (size_t)L.w * L.h);
         return;
     }
-    if (z32) {
-        lsb_launched(), stencil_h_kernel<BT, float><<<g2(L.w, L.h), B2, 0, s>>>(L.hx, b, L.hwd, L.hax, L.hay, L.hdinv, z32, L.w, L.h, 2);
-        return;
-    }
-    lsb_launched(), stencil_h_kernel<BT, uint16_t><<<g2(L.w, L.h), B2, 0, s>>>(L.hx, b, L.hwd, L.hax, L.hay, L.hdinv, L.hr, L.w, L.h, 2);
+    lsb_launched(), stencil_h_kernel<uint16_t, uint16_t><<<g2(L.w, L.h), B2, 0, s>>>(L.hx, L.hb, L.hwd, L.hax, L.hay, L.hdinv, L.hr, L.w,
+                                                                                   L.h, 2);
     std::swap(L.hx, L.hr);
 }
 static size_t coarse_h_smem(const WlsLevel& L) { return sizeof(uint16_t) * COARSE_H_PLANES * (size_t)L.w * L.h; }
@@ -1025,19 +1087,23 @@ static void vcycle_h(WlsSolver* S, size_t l, cudaStream_t s, const float* b32 = 
             const size_t smem = coarse_h_smem(T);  // at most 227 KB (wls_alloc raised the kernel's limit)
             lsb_launched(), coarse_h_kernel<<<1, dim3(32, 32), smem, s>>>(T.hx, T.hb, T.hwd, T.hax, T.hay, T.hdinv, T.w, T.h, MG_COARSE);
         } else {
-            for (int k = 0; k < MG_COARSE; k++) jacobi_h(T, (const uint16_t*)T.hb, k == 0, s);
+            for (int k = 0; k < MG_COARSE; k++) jacobi_h(T, k == 0, s);
         }
         return;
     }
-    auto down_up = [&](auto* b) {
-        for (int k = 0; k < MG_H_SWEEPS; k++) jacobi_h(T, b, k == 0, s);
+    static_assert(MG_H_SWEEPS == 2, "the fused BF16 passes run the zero-start sweep and one more down, two up");
+    auto down_up = [&](auto* b) {  // the way down and the way up in one pass each
         using BT = std::remove_cv_t<std::remove_pointer_t<decltype(b)>>;
-        lsb_launched(), stencil_h_kernel<BT, uint16_t><<<g2(T.w, T.h), B2, 0, s>>>(T.hx, b, T.hwd, T.hax, T.hay, T.hdinv, T.hr, T.w, T.h, 1);
         WlsLevel& C = S->lv[l + 1];
-        lsb_launched(), block_sum_h_kernel<<<g2(C.w, C.h), B2, 0, s>>>(T.hr, T.w, T.h, C.hb, C.w, C.h);
+        lsb_launched(), vc_down_h_kernel<BT><<<g2(C.w, C.h), B2, 0, s>>>(b, T.hwd, T.hax, T.hay, T.hdinv, T.hx, T.w, T.h, C.hb, C.w, C.h);
         vcycle_h(S, l + 1, s);
-        lsb_launched(), prolong_h_kernel<<<g2(T.w, T.h), B2, 0, s>>>(T.hx, T.w, T.h, C.hx, C.w);
-        for (int k = 0; k < MG_H_SWEEPS; k++) jacobi_h(T, b, false, s, k + 1 == MG_H_SWEEPS ? z32 : nullptr);
+        if (z32) {
+            lsb_launched(), vc_up_h_kernel<BT, float><<<g2(T.w, T.h), B2, 0, s>>>(T.hx, C.hx, C.w, b, T.hwd, T.hax, T.hay, T.hdinv, z32, T.w, T.h);
+        } else {
+            lsb_launched(), vc_up_h_kernel<BT, uint16_t><<<g2(T.w, T.h), B2, 0, s>>>(T.hx, C.hx, C.w, b, T.hwd, T.hax, T.hay, T.hdinv, T.hr, T.w,
+                                                                                    T.h);
+            std::swap(T.hx, T.hr);
+        }
     };
     if (b32) down_up(b32);
     else down_up((const uint16_t*)T.hb);
